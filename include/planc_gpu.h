@@ -1,0 +1,169 @@
+/* planc_gpu.h -- C ABI of the B200 (sm_100a) implementation of PLANC's
+ * shared-memory NTF iteration (AUNTF with MU / HALS / ANLS-BPP updates and the
+ * dimension-tree MTTKRP).
+ *
+ * Plain C types only: pointers, sizes and status codes. One context owns one
+ * device-resident tensor, one set of CP factors and one CUDA stream. A
+ * context is not thread-safe; distinct contexts are independent.
+ *
+ * Layouts (the reference's own memory layouts):
+ *   tensor X : dense, column-major with mode 0 fastest
+ *              (reference common/tensor.hpp:22-28, Tensor::m_data).
+ *   factors  : row-major I_n x k, rank index fastest. This is the memory of
+ *              the reference's ncp_mttkrp_t[n] (k x I_n column-major,
+ *              ntf/auntf.hpp:95) and of the dimension-tree factors
+ *              (dimtree/ddt.hpp:84-88); an Armadillo I_n x k factor
+ *              (NCPFactors::factor) is its transpose in memory.
+ *   k x k    : symmetric.
+ *
+ * Every function returns PLANC_GPU_OK (0) or a negative status; the message
+ * of the last failure on the calling thread is planc_gpu_last_error(). The
+ * reference reports the same failures with exit() (dimtree/dimtrees.hpp:48-64,
+ * nnls/bppnnls.hpp:185-188) and assert (common/ncpfactors.hpp:113).
+ */
+#ifndef PLANC_GPU_H_
+#define PLANC_GPU_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define PLANC_GPU_ABI_VERSION 1
+
+/* status codes */
+#define PLANC_GPU_OK 0
+#define PLANC_GPU_ERR_ARG (-1)         /* bad argument / shape */
+#define PLANC_GPU_ERR_CUDA (-2)        /* CUDA runtime or driver error */
+#define PLANC_GPU_ERR_STATE (-3)       /* call out of order (no tensor, no factors) */
+#define PLANC_GPU_ERR_BPP_MAXITER (-4) /* BPP hit its 5k iteration cap ("BPP failed") */
+#define PLANC_GPU_ERR_NONFINITE (-5)   /* NaN/Inf met in a solve */
+#define PLANC_GPU_ERR_TIMEOUT (-6)     /* a bounded device wait ran out */
+#define PLANC_GPU_ERR_UNSUPPORTED (-7) /* shape/rank outside what the kernels take */
+#define PLANC_GPU_ERR_OOM (-8)         /* device allocation failed */
+#define PLANC_GPU_ERR_SINGULAR (-9)    /* a normal-equation solve found no pivot */
+
+/* MTTKRP precision. The Gram matrices, the factor updates, the BPP solves and
+ * the error are FP64 in every mode. */
+#define PLANC_GPU_PREC_FP64 0   /* FP64 tensor, FP64 contraction (plain path) */
+#define PLANC_GPU_PREC_BF16 1   /* BF16 tensor, split-BF16 (hi+lo) factors, FP32 accumulate */
+#define PLANC_GPU_PREC_BF16X2 2 /* tensor split into BF16 hi+lo, 3 products, FP32 accumulate */
+
+/* update algorithms: values of the reference's algotype (common/utils.h:10) */
+#define PLANC_GPU_MU 0
+#define PLANC_GPU_HALS 1
+#define PLANC_GPU_ANLSBPP 2
+
+/* element types of a tensor handed to planc_gpu_set_tensor */
+#define PLANC_GPU_F64 0
+#define PLANC_GPU_F32 1
+
+typedef struct planc_gpu_ctx planc_gpu_ctx;
+
+/* ABI version (PLANC_GPU_ABI_VERSION of the built library). */
+int planc_gpu_abi_version(void);
+
+/* Message of the last failing call on this thread ("" if none). */
+const char* planc_gpu_last_error(void);
+
+/* Creates a context on `device`. `cuda_stream` is a cudaStream_t to run on
+ * (NULL: the context creates and owns a non-blocking stream). */
+int planc_gpu_create(planc_gpu_ctx** out, int device, int precision, void* cuda_stream);
+
+/* Releases all device memory of the context. NULL is accepted. */
+int planc_gpu_destroy(planc_gpu_ctx* ctx);
+
+/* The CUDA stream the context launches on (as a cudaStream_t). */
+void* planc_gpu_stream(planc_gpu_ctx* ctx);
+
+/* Uploads the tensor (replaces Tensor(dims) / Tensor::read as the input of
+ * AUNTF(const Tensor&, ...), ntf/auntf.hpp:83-105). X has prod(dims)
+ * elements of `dtype`, column-major with mode 0 fastest; `x_on_device` != 0
+ * means X is a device pointer on the context's device. ||X||^2 is computed in
+ * FP64 from the values given (Tensor::norm, common/tensor.hpp:350-356). */
+int planc_gpu_set_tensor(planc_gpu_ctx* ctx, const void* X, int dtype,
+                         const int64_t* dims, int nmodes, int x_on_device);
+
+/* Injects CP factors as AUNTF::reset(new_factors, false) does
+ * (ntf/auntf.hpp:186-198): each mode is column-normalised
+ * (NCPFactors::normalize(int), common/ncpfactors.hpp:346-351), then lambda is
+ * set to `lambda` (k values; NULL means all ones). F[n] is row-major
+ * I_n x k (host memory). Sets the rank k (1 <= k <= 64). */
+int planc_gpu_set_factors(planc_gpu_ctx* ctx, const double* const* F,
+                          const double* lambda, int k);
+
+/* Runs `iters` outer iterations of AUNTF::computeNTF (ntf/auntf.hpp:128-177)
+ * with update `algo` (PLANC_GPU_MU / HALS / ANLSBPP). `dimtree` != 0 uses
+ * the dimension tree (N in {3,4}; ddt.hpp:134-243), else the direct MTTKRP
+ * (common/tensor.hpp:246-327). With `compute_error` != 0, errs_out[it]
+ * receives the relative error after iteration it (auntf.hpp:165-170), in the
+ * FP64 Gram form ||X||^2 - 2<X,M> + ||M||^2. errs_out may be NULL. */
+int planc_gpu_run(planc_gpu_ctx* ctx, int algo, int iters, int dimtree,
+                  int compute_error, double* errs_out);
+
+/* Copies the current (normalised) factors and lambda to host memory
+ * (AUNTF::ncp_factors(), ntf/auntf.hpp:118). F[n]: row-major I_n x k; either
+ * argument may be NULL. */
+int planc_gpu_get_factors(planc_gpu_ctx* ctx, double* const* F, double* lambda);
+
+/* MTTKRP of mode n with the current factors, row-major I_n x k (host):
+ * with `dimtree` != 0 through the dimension tree (the partial MTTKRP is
+ * recomputed from the current factors), else the direct form
+ * (ntf_utils.hpp:49-53 / tensor.hpp:246-327). */
+int planc_gpu_mttkrp(planc_gpu_ctx* ctx, int mode, int dimtree, double* out);
+
+/* Hadamard product of the Grams of all modes except n, k x k (host):
+ * NCPFactors::gram_leave_out_one, common/ncpfactors.hpp:139-148. */
+int planc_gpu_gram_loo(planc_gpu_ctx* ctx, int mode, double* out);
+
+/* Relative error of the current factors and lambda
+ * (AUNTF::computeObjectiveError, ntf/auntf.hpp:200-246), FP64 Gram form. */
+int planc_gpu_objective_error(planc_gpu_ctx* ctx, double* err);
+
+/* Per-mode extension point for host-side factor updates (the reference's
+ * virtual MAT AUNTF::update(int mode), ntf/auntf.hpp:45): mode_begin computes
+ * the leave-one-out Gram and the MTTKRP of `mode` from the current factors
+ * (the steps of auntf.hpp:132-151) and copies them to the host (either
+ * pointer may be NULL); mode_end takes the new, unnormalised factor (row-major
+ * I_n x k, host) and applies AUNTF::update_factor_mode (auntf.hpp:66-79). */
+int planc_gpu_mode_begin(planc_gpu_ctx* ctx, int mode, int dimtree,
+                         double* gram_out, double* mttkrp_out);
+int planc_gpu_mode_end(planc_gpu_ctx* ctx, int mode, const double* factor);
+
+/* BPP NNLS on the device for host inputs: solves min ||A x - b|| s.t. x >= 0
+ * for `ncols` right-hand sides from the normal equations, as
+ * BPPNNLS<MAT,VEC>(AtA, AtB, true).solveNNLS() (nnls/bppnnls.hpp:67-191,
+ * nnls/nnls.hpp:100-131). AtA: n x n; AtB and X: column-major n x ncols;
+ * passive (may be NULL): n x ncols final passive-set mask; iters (may be
+ * NULL): per-column BPP iteration counts. 1 <= n <= 64. */
+int planc_gpu_bpp_solve(planc_gpu_ctx* ctx, const double* AtA, const double* AtB,
+                        int n, int64_t ncols, double* X, int32_t* passive,
+                        int32_t* iters);
+
+/* Kernel timing, for roofline measurement: while enabled, CUDA events bracket
+ * every launch of each kernel class on the context's stream. Class ids:
+ *   0 partial MTTKRP (tensor contraction), 1 multi-TTV, 2 factor update,
+ *   3 normalise + Gram, 4 error, 5 split-K reduction, 6 BPP.
+ * get_kernel_times fills ms[c] and launches[c] for c < n and resets them. */
+int planc_gpu_set_timing(planc_gpu_ctx* ctx, int enable);
+int planc_gpu_get_kernel_times(planc_gpu_ctx* ctx, double* ms, int64_t* launches, int n);
+
+/* Number of kernel launches the library issued on this context so far. */
+int64_t planc_gpu_launch_count(planc_gpu_ctx* ctx);
+
+/* Synthetic input: writes into device memory `X_dev` (prod(dims) elements of
+ * `dtype`, mode 0 fastest) the CP model [[A_0, ..., A_{N-1}]] of rank k from
+ * host factors A[n] (row-major I_n x k), plus i.i.d. Gaussian noise of
+ * standard deviation `sigma` (counter-based Philox stream of `seed`),
+ * clipped at >= 0 when `clip` != 0. This is the reference's Gen_Tensor noise
+ * model (dimtree/ddttensor.hpp:899-985) with a reproducible generator. */
+int planc_gpu_synth_cp_tensor(int device, void* X_dev, int dtype, const int64_t* dims,
+                              int nmodes, const double* const* A, int k, double sigma,
+                              uint64_t seed, int clip, void* cuda_stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PLANC_GPU_H_ */

@@ -1,0 +1,236 @@
+"""ctypes binding of the CPU oracle (test infrastructure only).
+
+Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline legs of
+``bench.py`` import this package; the product path never does.
+
+Two libraries are loaded:
+  * ``liboracle.so``: the CPU restatement of the reference NTF path
+    (``ntf_oracle.cpp``; every function cites the reference lines it follows);
+  * ``_ref/libref_dimtree.so``: the reference's own dimension-tree MTTKRP
+    kernels (``dimtree/dimtrees.hpp``, ``dimtree/ddttensor.hpp``) compiled
+    unmodified by ``oracle/Makefile``, driven by ``ref_dimtree_driver.cpp``.
+
+Array conventions: tensors are numpy arrays in Fortran order (mode 0
+fastest, ``common/tensor.hpp:22-28``); factors are C-order ``(I_n, k)``
+float64 arrays (row-major, the layout of ``ncp_mttkrp_t`` and the dimension
+tree's factors).
+"""
+import ctypes
+import glob
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ALGO = {"mu": 0, "hals": 1, "anlsbpp": 2}
+
+_lib = None
+_ref = None
+
+
+def find_openblas():
+    """Locate an LP64 OpenBLAS (with LAPACK) shipped inside the Python env."""
+    import numpy  # noqa: F401  (only to find site-packages)
+    site = os.path.dirname(os.path.dirname(np.__file__))
+    cands = sorted(glob.glob(os.path.join(site, "opencv_python_headless.libs", "libopenblas*.so*")))
+    if not cands:
+        raise RuntimeError("no LP64 OpenBLAS found for the CPU oracle")
+    return cands[0]
+
+
+def build(reference_dir=None):
+    """Compile liboracle.so (and _ref/libref_dimtree.so when the reference
+    tree is present)."""
+    cmd = ["make", "-s", "-C", HERE, "OPENBLAS=" + find_openblas()]
+    if reference_dir and os.path.isdir(reference_dir):
+        cmd.append("REFERENCE_DIR=" + reference_dir)
+    subprocess.run(cmd, check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            build()
+        L = ctypes.CDLL(path)
+        P = ctypes.POINTER
+        d, i64, i32 = ctypes.c_double, ctypes.c_int64, ctypes.c_int
+        pd, pi64, pi = P(d), P(i64), P(i32)
+        ppd = P(pd)
+        L.orc_gram_loo.argtypes = [ppd, pi64, i32, i32, i32, pd]
+        L.orc_krp_leave_out_one.argtypes = [ppd, pi64, i32, i32, i32, pd]
+        L.orc_mttkrp_direct.argtypes = [pd, pi64, i32, ppd, i32, i32, pd]
+        L.orc_mttkrp_dimtree_all.argtypes = [pd, pi64, i32, ppd, i32, ppd]
+        L.orc_mttkrp_dimtree_all.restype = i32
+        L.orc_normalize.argtypes = [pd, i64, i32, pd]
+        L.orc_hals_update.argtypes = [pd, i64, i32, pd, pd]
+        L.orc_mu_update.argtypes = [pd, i64, i32, pd, pd]
+        L.orc_bpp_update.argtypes = [pd, i64, i32, pd, pd, pi]
+        L.orc_bpp_update.restype = i32
+        L.orc_bpp_solve.argtypes = [pd, pd, i32, i64, pd, pi]
+        L.orc_bpp_solve.restype = i32
+        L.orc_explicit_error.argtypes = [pd, pi64, i32, ppd, pd, i32]
+        L.orc_explicit_error.restype = d
+        L.orc_ntf_run.argtypes = [pd, pi64, i32, i32, ppd, pd, i32, i32, i32, i32, pd]
+        L.orc_ntf_run.restype = i32
+        L.orc_tensor_randu.argtypes = [i64, ctypes.c_uint, pd]
+        _lib = L
+    return _lib
+
+
+def ref_available():
+    return os.path.exists(os.path.join(HERE, "_ref", "libref_dimtree.so"))
+
+
+def ref():
+    global _ref
+    if _ref is None:
+        path = os.path.join(HERE, "_ref", "libref_dimtree.so")
+        R = ctypes.CDLL(path)
+        P = ctypes.POINTER
+        pd = P(ctypes.c_double)
+        li = ctypes.c_long
+        R.ref_dimtree_create.argtypes = [pd, P(li), li, li, P(pd), li]
+        R.ref_dimtree_create.restype = ctypes.c_void_p
+        R.ref_dimtree_set_factor.argtypes = [ctypes.c_void_p, li, pd]
+        R.ref_dimtree_mttkrp.argtypes = [ctypes.c_void_p, li, pd]
+        R.ref_dimtree_destroy.argtypes = [ctypes.c_void_p]
+        _ref = R
+    return _ref
+
+
+# ---------------------------------------------------------------- helpers
+def _pd(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _dims(X):
+    return (ctypes.c_int64 * X.ndim)(*X.shape)
+
+
+def _fptrs(F):
+    arr = (ctypes.POINTER(ctypes.c_double) * len(F))()
+    for i, f in enumerate(F):
+        assert f.dtype == np.float64 and f.flags.c_contiguous
+        arr[i] = _pd(f)
+    return arr
+
+
+def _xf(X):
+    X = np.asarray(X, dtype=np.float64)
+    return np.asfortranarray(X)
+
+
+def tensor_randu(dims, seed=103):
+    """Tensor(dims) fill: std::mt19937(seed) + uniform_real_distribution<>(0,1)
+    in linear order (common/tensor.hpp:86-93, 219-235, single-threaded)."""
+    n = int(np.prod(dims))
+    flat = np.empty(n, dtype=np.float64)
+    lib().orc_tensor_randu(n, seed, _pd(flat))
+    return flat.reshape(tuple(dims), order="F")
+
+
+def gram_loo(F, n):
+    k = F[0].shape[1]
+    G = np.zeros((k, k))
+    dims = (ctypes.c_int64 * len(F))(*[f.shape[0] for f in F])
+    lib().orc_gram_loo(_fptrs(F), dims, len(F), k, n, _pd(G))
+    return G
+
+
+def mttkrp_direct(X, F, n):
+    X = _xf(X)
+    k = F[0].shape[1]
+    out = np.zeros((X.shape[n], k))
+    lib().orc_mttkrp_direct(_pd(X), _dims(X), X.ndim, _fptrs(F), k, n, _pd(out))
+    return out
+
+
+def mttkrp_dimtree_all(X, F):
+    X = _xf(X)
+    k = F[0].shape[1]
+    outs = [np.zeros((X.shape[n], k)) for n in range(X.ndim)]
+    rc = lib().orc_mttkrp_dimtree_all(_pd(X), _dims(X), X.ndim, _fptrs(F), k, _fptrs(outs))
+    if rc != 0:
+        raise ValueError("dimension tree needs N in {3,4}")
+    return outs
+
+
+def ref_mttkrp_dimtree_all(X, F, nthreads=1):
+    """All-mode MTTKRP through the reference's compiled dimension-tree kernels,
+    with fixed factors (the factor slot overwritten by each MTTKRP is restored
+    as AUNTF's set_factor would, ntf/auntf.hpp:70-73)."""
+    X = _xf(X)
+    k = F[0].shape[1]
+    R = ref()
+    dims = (ctypes.c_long * X.ndim)(*X.shape)
+    h = R.ref_dimtree_create(_pd(X), dims, X.ndim, k, _fptrs(F), nthreads)
+    outs = []
+    try:
+        for n in range(X.ndim):
+            o = np.zeros((X.shape[n], k))
+            R.ref_dimtree_mttkrp(h, n, _pd(o))
+            R.ref_dimtree_set_factor(h, n, _pd(F[n]))
+            outs.append(o)
+    finally:
+        R.ref_dimtree_destroy(h)
+    return outs
+
+
+def normalize(F):
+    F = np.ascontiguousarray(F, dtype=np.float64).copy()
+    lam = np.zeros(F.shape[1])
+    lib().orc_normalize(_pd(F), F.shape[0], F.shape[1], _pd(lam))
+    return F, lam
+
+
+def hals_update(H, M, G):
+    H = np.ascontiguousarray(H, dtype=np.float64).copy()
+    M = np.ascontiguousarray(M, dtype=np.float64)
+    G = np.ascontiguousarray(G, dtype=np.float64)
+    lib().orc_hals_update(_pd(H), H.shape[0], H.shape[1], _pd(M), _pd(G))
+    return H
+
+
+def mu_update(H, M, G):
+    H = np.ascontiguousarray(H, dtype=np.float64).copy()
+    M = np.ascontiguousarray(M, dtype=np.float64)
+    G = np.ascontiguousarray(G, dtype=np.float64)
+    lib().orc_mu_update(_pd(H), H.shape[0], H.shape[1], _pd(M), _pd(G))
+    return H
+
+
+def bpp_update(M, G):
+    """Returns (H row-major I x k, passive mask I x k, iterations)."""
+    M = np.ascontiguousarray(M, dtype=np.float64)
+    G = np.ascontiguousarray(G, dtype=np.float64)
+    I, k = M.shape
+    H = np.zeros((I, k))
+    mask = np.zeros((I, k), dtype=np.int32)
+    it = lib().orc_bpp_update(_pd(H), I, k, _pd(M), _pd(G),
+                              mask.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
+    return H, mask, it
+
+
+def explicit_error(X, F, lam):
+    X = _xf(X)
+    return lib().orc_explicit_error(_pd(X), _dims(X), X.ndim, _fptrs(F),
+                                    _pd(np.ascontiguousarray(lam, dtype=np.float64)), F[0].shape[1])
+
+
+def ntf_run(X, F_init, algo, iters, dimtree=True, compute_error=True, lam=None):
+    """The AUNTF loop (ntf/auntf.hpp:128-177) from injected initial factors.
+    Returns (factors, lambda, errors)."""
+    X = _xf(X)
+    k = F_init[0].shape[1]
+    F = [np.ascontiguousarray(f, dtype=np.float64).copy() for f in F_init]
+    lam = np.ones(k) if lam is None else np.asarray(lam, dtype=np.float64).copy()
+    errs = np.zeros(max(iters, 1))
+    rc = lib().orc_ntf_run(_pd(X), _dims(X), X.ndim, k, _fptrs(F), _pd(lam),
+                           ALGO[algo] if isinstance(algo, str) else int(algo),
+                           iters, int(dimtree), int(compute_error), _pd(errs))
+    if rc != 0:
+        raise RuntimeError("oracle ntf_run failed with code %d" % rc)
+    return F, lam, errs[:iters]

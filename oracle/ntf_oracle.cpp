@@ -1,0 +1,609 @@
+// ntf_oracle.cpp -- CPU oracle for PLANC's shared-memory NTF iteration.
+//
+// TEST INFRASTRUCTURE ONLY. This file is the checker the CUDA path is compared
+// against; nothing in the product (libplanc_gpu.so, the C++ API, the Python
+// binding) links, loads or calls it. Only tests/, __graft_entry__.smoke() and
+// the cpu_baseline / --impl reference legs of bench.py use it.
+//
+// It restates, in plain C++ over OpenBLAS (the same BLAS family the reference
+// links through Armadillo), the algorithm of the reference files below. Every
+// function names the reference lines it follows. Armadillo is not available
+// here, so Armadillo expressions are written out as loops with the same
+// semantics; `arma::solve(..., likely_sympd)` is restated as a Cholesky solve
+// (LAPACK dposv) with an LU (dgesv) fallback when the Cholesky fails.
+//
+// Layout conventions (all buffers owned by the caller):
+//   X        : dense tensor, column-major with mode 0 fastest
+//              (common/tensor.hpp:22-28).
+//   factors  : row-major I_n x k ("r fastest"); this is the memory layout of
+//              the reference's ncp_mttkrp_t[n] (k x I_n column-major,
+//              ntf/auntf.hpp:95) and of the dimension-tree factors
+//              (dimtree/ddt.hpp:84-88).
+//   k x k    : symmetric, layout irrelevant.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <random>
+#include <vector>
+
+extern "C" {
+// OpenBLAS / LAPACK prototypes (LP64).
+enum { CblasRowMajor = 101, CblasColMajor = 102 };
+enum { CblasNoTrans = 111, CblasTrans = 112 };
+void cblas_dgemm(int order, int ta, int tb, int m, int n, int k, double alpha,
+                 const double* a, int lda, const double* b, int ldb,
+                 double beta, double* c, int ldc);
+void dposv_(const char* uplo, const int* n, const int* nrhs, double* a,
+            const int* lda, double* b, const int* ldb, int* info);
+void dgesv_(const int* n, const int* nrhs, double* a, const int* lda,
+            int* ipiv, double* b, const int* ldb, int* info);
+}
+
+namespace {
+
+// common/utils.h:46-49
+constexpr double kEps17 = 0.00000000000000001;  // EPSILON_1EMINUS16 (= 1e-17)
+constexpr double kEps6 = 0.000001;               // EPSILON
+constexpr double kEps12 = 1e-12;                 // EPSILON_1EMINUS12
+// ntf/ntfanlsbpp.hpp:11
+constexpr int64_t kChunk = 2000;                 // ONE_THREAD_MATRIX_SIZE
+
+enum Algo { MU = 0, HALS = 1, ANLSBPP = 2 };  // common/utils.h:10
+
+int64_t prod(const int64_t* d, int a, int b) {
+  int64_t p = 1;
+  for (int i = a; i < b; ++i) p *= d[i];
+  return p;
+}
+
+// Gram F^T F of a row-major I x k factor. common/ncpfactors.hpp:144
+void gram(const double* F, int64_t I, int k, double* G) {
+  cblas_dgemm(CblasColMajor, CblasNoTrans, CblasTrans, k, k, (int)I, 1.0, F, k,
+              F, k, 0.0, G, k);
+}
+
+// Leave-one-out Hadamard product of Grams. common/ncpfactors.hpp:139-148
+void gram_loo(const double* const* F, const int64_t* dims, int N, int k, int n,
+              double* G) {
+  std::vector<double> cur((size_t)k * k);
+  for (int i = 0; i < k * k; ++i) G[i] = 1.0;
+  for (int m = 0; m < N; ++m) {
+    if (m == n) continue;
+    gram(F[m], dims[m], k, cur.data());
+    for (int i = 0; i < k * k; ++i) G[i] *= cur[i];
+  }
+}
+
+// Reverse Khatri-Rao product of all factors except n, stored column-major
+// (prod_{m!=n} I_m) x k. Row index is the column-major linear index over the
+// remaining modes with the lowest mode fastest.
+// common/ncpfactors.hpp:171-233 (per-column outer products, matorder
+// reversed).
+void krp_leave_out_one(const double* const* F, const int64_t* dims, int N,
+                       int k, int n, double* KRP) {
+  int64_t rows = 1;
+  for (int m = 0; m < N; ++m)
+    if (m != n) rows *= dims[m];
+  std::vector<int> order;
+  for (int m = N - 1; m >= 0; --m)
+    if (m != n) order.push_back(m);
+  std::vector<double> ab, nab;
+  for (int r = 0; r < k; ++r) {
+    int m0 = order[0];
+    ab.resize(dims[m0]);
+    for (int64_t i = 0; i < dims[m0]; ++i) ab[i] = F[m0][i * k + r];
+    for (size_t t = 1; t < order.size(); ++t) {
+      int m = order[t];
+      int64_t Im = dims[m];
+      nab.resize((size_t)Im * ab.size());
+      // ab = currentvec * oldabvec.t(), vectorised column-major
+      for (size_t b = 0; b < ab.size(); ++b)
+        for (int64_t a = 0; a < Im; ++a)
+          nab[a + Im * b] = F[m][a * k + r] * ab[b];
+      ab.swap(nab);
+    }
+    std::memcpy(KRP + (size_t)r * rows, ab.data(), sizeof(double) * rows);
+  }
+}
+
+// Direct MTTKRP with a materialised KRP. common/tensor.hpp:246-327.
+// out is row-major I_n x k.
+void mttkrp_direct(const double* X, const int64_t* dims, int N,
+                   const double* const* F, int k, int n, double* out) {
+  int64_t In = dims[n];
+  int64_t krows = prod(dims, 0, N) / In;
+  std::vector<double> KRP((size_t)krows * k);
+  krp_leave_out_one(F, dims, N, k, n, KRP.data());
+  if (n == 0) {
+    // tensor.hpp:279-281: out(I0 x k, row-major) = X_(0) * KRP
+    cblas_dgemm(CblasRowMajor, CblasTrans, CblasTrans, (int)In, k, (int)krows,
+                1.0, X, (int)In, KRP.data(), (int)krows, 0.0, out, k);
+  } else {
+    int64_t ncols = prod(dims, 0, n);
+    int64_t nmats = prod(dims, n + 1, N);
+    // tensor.hpp:298-325: one dgemm per trailing slice, beta = 1 after the
+    // first.
+    for (int64_t i = 0; i < nmats; ++i) {
+      cblas_dgemm(CblasRowMajor, CblasNoTrans, CblasTrans, (int)In, k,
+                  (int)ncols, 1.0, X + i * ncols * In, (int)ncols,
+                  KRP.data() + i * ncols, (int)(ncols * nmats),
+                  i == 0 ? 0.0 : 1.0, out, k);
+    }
+  }
+}
+
+// Dimension-tree state, restating DenseDimensionTree (dimtree/ddt.hpp) for
+// N in {3, 4} with split s = N/2 (ntf/auntf.hpp:122-123). P holds the
+// right-contracted partial MTTKRP (prod_{i<=s} I_i) x k, column-major with
+// the left modes' linear index fastest (dimtrees.hpp:281-306, ColMajor).
+// Q holds P contracted with the updated F_0 (N = 4 only,
+// ddt.hpp:218-226).
+struct DimTree {
+  int N, k, s;
+  const int64_t* dims;
+  int64_t L, R;
+  std::vector<double> P, Q;
+};
+
+// ddt.hpp:134-243 restated. Writes the mode-n MTTKRP row-major I_n x k.
+void dimtree_mttkrp(DimTree& t, const double* X, const double* const* F, int n,
+                    double* out) {
+  const int N = t.N, k = t.k, s = t.s;
+  const int64_t* d = t.dims;
+  if (n == 0) {
+    // partial_MTTKRP_with_KRP_output_T(s, right, ...): P = X_(L x R) * KRP_right
+    int64_t R = t.R, L = t.L;
+    // For N in {3, 4} and s = N/2 the right group is the single last mode.
+    const double* B = F[N - 1];  // row-major R x k
+    // C(L x k, col-major) = X(L x R col-major) * B^T  where B is k x R col-major
+    cblas_dgemm(CblasColMajor, CblasNoTrans, CblasTrans, (int)L, k, (int)R, 1.0,
+                X, (int)L, B, k, 0.0, t.P.data(), (int)L);
+    // multi_TTV right over modes 1..s: M0[i0,r] = sum_{rest} P[i0,rest,r] *
+    // prod_{1<=m<=s} F_m[i_m, r]   (dimtrees.hpp:464-479)
+    int64_t I0 = d[0];
+    int64_t rest = t.L / I0;
+    std::fill(out, out + I0 * k, 0.0);
+    std::vector<double> w((size_t)rest);
+    for (int r = 0; r < k; ++r) {
+      for (int64_t q = 0; q < rest; ++q) {
+        int64_t idx = q;
+        double v = 1.0;
+        for (int m = 1; m <= s; ++m) {
+          int64_t im = idx % d[m];
+          idx /= d[m];
+          v *= F[m][im * k + r];
+        }
+        w[q] = v;
+      }
+      const double* Pr = t.P.data() + (size_t)r * t.L;
+      for (int64_t i0 = 0; i0 < I0; ++i0) {
+        double acc = 0.0;
+        for (int64_t q = 0; q < rest; ++q) acc += Pr[i0 + I0 * q] * w[q];
+        out[i0 * k + r] = acc;
+      }
+    }
+    return;
+  }
+  if (n == s + 1) {
+    // partial_MTTKRP_with_KRP_output_FM(left, ...): M = X^T * KRP_left
+    // (dimtrees.hpp:250-271, KRP from ddttensor.hpp:872-897)
+    int64_t L = t.L, R = t.R;
+    std::vector<double> colmaj((size_t)L * k);
+    std::vector<const double*> sub(F, F + s + 1);
+    krp_leave_out_one(sub.data(), d, s + 2, k, s + 1, colmaj.data());
+    // out(R x k row-major) = X^T (R x L) * KRP (L x k)
+    // as col-major: out^T (k x R) = KRP^T (k x L) * X (L x R)
+    cblas_dgemm(CblasColMajor, CblasTrans, CblasNoTrans, k, (int)R, (int)L, 1.0,
+                colmaj.data(), (int)L, X, (int)L, 0.0, out, k);
+    return;
+  }
+  // 1 <= n <= s: multi-TTV on P (and Q for N = 4).
+  if (N == 3) {
+    // n == 1, s == 1: M1[i1,r] = sum_{i0} P[i0,i1,r] F0[i0,r]
+    // (ddt.hpp:207-212, multi_TTV left)
+    int64_t I0 = d[0], I1 = d[1];
+    for (int r = 0; r < k; ++r) {
+      const double* Pr = t.P.data() + (size_t)r * t.L;
+      for (int64_t i1 = 0; i1 < I1; ++i1) {
+        double acc = 0.0;
+        for (int64_t i0 = 0; i0 < I0; ++i0)
+          acc += Pr[i0 + I0 * i1] * F[0][i0 * k + r];
+        out[i1 * k + r] = acc;
+      }
+    }
+    return;
+  }
+  // N == 4, s == 2
+  int64_t I0 = d[0], I1 = d[1], I2 = d[2];
+  if (n == 1) {
+    // Q[i1,i2,r] = sum_{i0} P[i0,i1,i2,r] F0[i0,r]   (ddt.hpp:218-226)
+    t.Q.assign((size_t)I1 * I2 * k, 0.0);
+    for (int r = 0; r < k; ++r) {
+      const double* Pr = t.P.data() + (size_t)r * t.L;
+      double* Qr = t.Q.data() + (size_t)r * I1 * I2;
+      for (int64_t q = 0; q < I1 * I2; ++q) {
+        double acc = 0.0;
+        for (int64_t i0 = 0; i0 < I0; ++i0)
+          acc += Pr[i0 + I0 * q] * F[0][i0 * k + r];
+        Qr[q] = acc;
+      }
+    }
+    // M1[i1,r] = sum_{i2} Q[i1,i2,r] F2[i2,r]   (ddt.hpp:231-232)
+    for (int r = 0; r < k; ++r) {
+      const double* Qr = t.Q.data() + (size_t)r * I1 * I2;
+      for (int64_t i1 = 0; i1 < I1; ++i1) {
+        double acc = 0.0;
+        for (int64_t i2 = 0; i2 < I2; ++i2)
+          acc += Qr[i1 + I1 * i2] * F[2][i2 * k + r];
+        out[i1 * k + r] = acc;
+      }
+    }
+    return;
+  }
+  // n == 2: M2[i2,r] = sum_{i1} Q[i1,i2,r] F1[i1,r]   (ddt.hpp:207-212)
+  for (int r = 0; r < k; ++r) {
+    const double* Qr = t.Q.data() + (size_t)r * I1 * I2;
+    for (int64_t i2 = 0; i2 < I2; ++i2) {
+      double acc = 0.0;
+      for (int64_t i1 = 0; i1 < I1; ++i1)
+        acc += Qr[i1 + I1 * i2] * F[1][i1 * k + r];
+      out[i2 * k + r] = acc;
+    }
+  }
+}
+
+// Column normalisation of mode n; replaces lambda. ncpfactors.hpp:346-351
+void normalize_mode(double* F, int64_t I, int k, double* lambda) {
+  for (int r = 0; r < k; ++r) {
+    double ss = 0.0;
+    for (int64_t i = 0; i < I; ++i) ss += F[i * k + r] * F[i * k + r];
+    double nrm = std::sqrt(ss);
+    lambda[r] = nrm;
+    if (nrm > 0)
+      for (int64_t i = 0; i < I; ++i) F[i * k + r] /= nrm;
+  }
+}
+
+// HALS update, ntf/ntfhals.hpp:13-29 with fixNumericalError
+// (common/utils.hpp:59-64): u = H(:,i) + (M(i,:)^T - H*G(:,i)); u[u<1e-17] =
+// 1e-17; if ||u||^2 > 0: H(:,i) = u. H is updated in place (Gauss-Seidel).
+void hals_update(double* H, int64_t I, int k, const double* M,
+                 const double* G) {
+  std::vector<double> u((size_t)I);
+  for (int i = 0; i < k; ++i) {
+    for (int64_t row = 0; row < I; ++row) {
+      double hg = 0.0;
+      for (int j = 0; j < k; ++j) hg += H[row * k + j] * G[j + (size_t)k * i];
+      double v = H[row * k + i] + (M[row * k + i] - hg);
+      u[row] = (v < kEps17) ? kEps17 : v;
+    }
+    double nrm2 = 0.0;
+    for (int64_t row = 0; row < I; ++row) nrm2 += u[row] * u[row];
+    if (nrm2 > 0)
+      for (int64_t row = 0; row < I; ++row) H[row * k + i] = u[row];
+  }
+}
+
+// MU update, ntf/ntfmu.hpp:11-16: H = (H % M^T) / (H*G + 1e-6).
+void mu_update(double* H, int64_t I, int k, const double* M, const double* G) {
+  std::vector<double> t((size_t)k);
+  for (int64_t row = 0; row < I; ++row) {
+    for (int c = 0; c < k; ++c) {
+      double acc = 0.0;
+      for (int j = 0; j < k; ++j) acc += H[row * k + j] * G[j + (size_t)k * c];
+      t[c] = acc + kEps6;
+    }
+    for (int c = 0; c < k; ++c)
+      H[row * k + c] = (H[row * k + c] * M[row * k + c]) / t[c];
+  }
+}
+
+// Solve A(P,P) x = b(P) for one column (arma::solve likely_sympd restated:
+// Cholesky, then LU on failure). Returns 0 on success.
+int solve_subset(const double* AtA, int n, const std::vector<int>& pset,
+                 const double* b, double* x) {
+  int m = (int)pset.size();
+  if (m == 0) return 0;
+  std::vector<double> A((size_t)m * m), A2, rhs(m), rhs2;
+  for (int c = 0; c < m; ++c)
+    for (int r = 0; r < m; ++r) A[r + (size_t)m * c] = AtA[pset[r] + (size_t)n * pset[c]];
+  for (int r = 0; r < m; ++r) rhs[r] = b[pset[r]];
+  A2 = A;
+  rhs2 = rhs;
+  int one = 1, info = 0;
+  char uplo = 'L';
+  dposv_(&uplo, &m, &one, A.data(), &m, rhs.data(), &m, &info);
+  if (info != 0) {
+    std::vector<int> ipiv(m);
+    dgesv_(&m, &one, A2.data(), &m, ipiv.data(), rhs2.data(), &m, &info);
+    if (info != 0) return -1;
+    rhs = rhs2;
+  }
+  for (int r = 0; r < m; ++r) x[pset[r]] = rhs[r];
+  return 0;
+}
+
+// Block principal pivoting NNLS for multiple RHS, nnls/bppnnls.hpp:67-191.
+// AtA: n x n, AtB: n x ncols column-major; X (out): n x ncols column-major.
+// The reference groups columns with identical passive sets
+// (bppnnls.hpp:204-287) only to share one factorisation; every column's
+// values are the same as a per-column solve, which is what is done here.
+// Returns the iteration count, or -1 if the iteration cap (5n) was hit
+// (the reference prints "BPP failed" and exits, bppnnls.hpp:185-188).
+int bpp_solve(const double* AtA, const double* AtB, int n, int64_t ncols,
+              double* X, int* passive_out) {
+  const unsigned MAX_IT = 5u * (unsigned)n;
+  const int pbar = 3;
+  std::vector<double> Y((size_t)n * ncols);
+  std::vector<unsigned char> PS((size_t)n * ncols, 0), NonOpt((size_t)n * ncols),
+      Infea((size_t)n * ncols);
+  std::vector<int> P(ncols, pbar), Ninf(ncols, n + 1), NotGood(ncols);
+  std::vector<unsigned char> NotOpt(ncols);
+  std::fill(X, X + (size_t)n * ncols, 0.0);
+  for (size_t i = 0; i < (size_t)n * ncols; ++i) Y[i] = -AtB[i];  // AtA*0 - AtB
+  auto classify = [&](int64_t c) {
+    int ng = 0;
+    for (int r = 0; r < n; ++r) {
+      size_t e = r + (size_t)n * c;
+      NonOpt[e] = (Y[e] < 0) && !PS[e];
+      Infea[e] = (X[e] < 0) && PS[e];
+      ng += NonOpt[e] + Infea[e];
+    }
+    NotGood[c] = ng;
+    NotOpt[c] = ng > 0;
+  };
+  int64_t numNonOpt = 0;
+  for (int64_t c = 0; c < ncols; ++c) {
+    classify(c);
+    numNonOpt += NotOpt[c];
+  }
+  unsigned iter = 0;
+  std::vector<int> pset;
+  std::vector<double> xs(n);
+  while (numNonOpt > 0) {
+    ++iter;
+    if (MAX_IT > 0 && iter > MAX_IT) return -1;
+    for (int64_t c = 0; c < ncols; ++c) {
+      if (!NotOpt[c]) continue;
+      bool c1 = NotGood[c] < Ninf[c];
+      bool c2 = !c1 && (NotGood[c] >= Ninf[c]) && (P[c] >= 1);
+      if (c1) {  // bppnnls.hpp:115-129
+        P[c] = pbar;
+        Ninf[c] = NotGood[c];
+      } else if (c2) {  // bppnnls.hpp:133-146
+        P[c] -= 1;
+      }
+      if (c1 || c2) {
+        for (int r = 0; r < n; ++r) {
+          size_t e = r + (size_t)n * c;
+          if (NonOpt[e]) PS[e] = 1;
+          if (Infea[e]) PS[e] = 0;
+        }
+      } else {  // backup rule, bppnnls.hpp:149-160: flip the largest index
+        int rowidx = -1;
+        for (int r = 0; r < n; ++r) {
+          size_t e = r + (size_t)n * c;
+          if (NonOpt[e] + Infea[e]) rowidx = r;
+        }
+        size_t e = rowidx + (size_t)n * c;
+        PS[e] = PS[e] ? 0 : 1;
+      }
+    }
+    // solve on passive sets, bppnnls.hpp:163-168 / 204-259
+    for (int64_t c = 0; c < ncols; ++c) {
+      if (!NotOpt[c]) continue;
+      pset.clear();
+      for (int r = 0; r < n; ++r)
+        if (PS[r + (size_t)n * c]) pset.push_back(r);
+      std::fill(xs.begin(), xs.end(), 0.0);
+      if (solve_subset(AtA, n, pset, AtB + (size_t)n * c, xs.data()) != 0)
+        return -2;
+      for (int r = 0; r < n; ++r) X[r + (size_t)n * c] = xs[r];
+      for (int r = 0; r < n; ++r) {
+        double acc = 0.0;
+        for (int j = 0; j < n; ++j) acc += AtA[r + (size_t)n * j] * xs[j];
+        Y[r + (size_t)n * c] = acc - AtB[r + (size_t)n * c];
+      }
+    }
+    // bppnnls.hpp:170-172: zero |.| < 1e-12 in all of X and Y
+    for (size_t i = 0; i < (size_t)n * ncols; ++i) {
+      if (std::fabs(X[i]) < kEps12) X[i] = 0.0;
+      if (std::fabs(Y[i]) < kEps12) Y[i] = 0.0;
+    }
+    numNonOpt = 0;
+    for (int64_t c = 0; c < ncols; ++c) {
+      classify(c);
+      numNonOpt += NotOpt[c];
+    }
+  }
+  if (passive_out)
+    for (size_t i = 0; i < (size_t)n * ncols; ++i) passive_out[i] = PS[i];
+  return (int)iter;
+}
+
+// ANLS/BPP update, ntf/ntfanlsbpp.hpp:15-57: chunks of 2000 RHS, X0 = 0.
+// M is row-major I x k == column-major k x I (ncp_mttkrp_t); H (out) row-major.
+int bpp_update(double* H, int64_t I, int k, const double* M, const double* G,
+               int* passive_out) {
+  int maxit = 0;
+  for (int64_t start = 0; start < I; start += kChunk) {
+    int64_t cnt = std::min(kChunk, I - start);
+    int it = bpp_solve(G, M + start * k, k, cnt, H + start * k,
+                       passive_out ? passive_out + start * k : nullptr);
+    if (it < 0) return it;
+    maxit = std::max(maxit, it);
+  }
+  return maxit;
+}
+
+// Relative error by explicit reconstruction, ntf/auntf.hpp:200-246:
+// lowrank = (F0 diag(lambda)) * KRP_{-0}^T, err = sqrt(||X - lowrank||^2 /
+// ||X||^2) with the squared norms of common/tensor.hpp:350-369.
+double explicit_error(const double* X, const int64_t* dims, int N,
+                      const double* const* F, const double* lambda, int k,
+                      double normA) {
+  int64_t I0 = dims[0];
+  int64_t rest = prod(dims, 1, N);
+  std::vector<double> KRP((size_t)rest * k);
+  krp_leave_out_one(F, dims, N, k, 0, KRP.data());
+  std::vector<double> U((size_t)I0 * k);  // column-major I0 x k
+  for (int64_t i = 0; i < I0; ++i)
+    for (int r = 0; r < k; ++r) U[i + I0 * r] = F[0][i * k + r] * lambda[r];
+  double err = 0.0;
+  const int64_t blk = 4096;
+  std::vector<double> low((size_t)I0 * blk);
+  for (int64_t c0 = 0; c0 < rest; c0 += blk) {
+    int64_t nc = std::min(blk, rest - c0);
+    cblas_dgemm(CblasColMajor, CblasNoTrans, CblasTrans, (int)I0, (int)nc, k,
+                1.0, U.data(), (int)I0, KRP.data() + c0, (int)rest, 0.0,
+                low.data(), (int)I0);
+    const double* Xb = X + c0 * I0;
+    for (int64_t i = 0; i < I0 * nc; ++i) {
+      double dlt = Xb[i] - low[i];
+      err += dlt * dlt;
+    }
+  }
+  return std::sqrt(err / normA);
+}
+
+}  // namespace
+
+extern "C" {
+
+int orc_version() { return 1; }
+
+// Tensor(dims) uniform fill: one std::mt19937(seed) and
+// std::uniform_real_distribution<>(0, 1) drawn in linear (mode-0-fastest)
+// order, common/tensor.hpp:86-93 and 219-235 (the single-threaded order; the
+// reference's OpenMP loop shares one generator across threads).
+void orc_tensor_randu(int64_t numel, unsigned seed, double* out) {
+  std::uniform_real_distribution<> dis(0, 1);
+  std::mt19937 gen(seed);
+  for (int64_t i = 0; i < numel; ++i) out[i] = dis(gen);
+}
+
+void orc_gram_loo(const double* const* F, const int64_t* dims, int N, int k,
+                  int n, double* G) {
+  gram_loo(F, dims, N, k, n, G);
+}
+
+void orc_krp_leave_out_one(const double* const* F, const int64_t* dims, int N,
+                           int k, int n, double* KRP_colmajor) {
+  krp_leave_out_one(F, dims, N, k, n, KRP_colmajor);
+}
+
+void orc_mttkrp_direct(const double* X, const int64_t* dims, int N,
+                       const double* const* F, int k, int n, double* out) {
+  mttkrp_direct(X, dims, N, F, k, n, out);
+}
+
+// All-mode dimension-tree MTTKRP with fixed factors (no updates between
+// modes), for comparison with the direct form.
+int orc_mttkrp_dimtree_all(const double* X, const int64_t* dims, int N,
+                           const double* const* F, int k, double* const* out) {
+  if (N != 3 && N != 4) return -1;
+  DimTree t;
+  t.N = N;
+  t.k = k;
+  t.s = N / 2;
+  t.dims = dims;
+  t.L = prod(dims, 0, t.s + 1);
+  t.R = prod(dims, t.s + 1, N);
+  t.P.assign((size_t)t.L * k, 0.0);
+  for (int n = 0; n < N; ++n) dimtree_mttkrp(t, X, F, n, out[n]);
+  return 0;
+}
+
+void orc_normalize(double* F, int64_t I, int k, double* lambda) {
+  normalize_mode(F, I, k, lambda);
+}
+
+void orc_hals_update(double* H, int64_t I, int k, const double* M,
+                     const double* G) {
+  hals_update(H, I, k, M, G);
+}
+
+void orc_mu_update(double* H, int64_t I, int k, const double* M,
+                   const double* G) {
+  mu_update(H, I, k, M, G);
+}
+
+int orc_bpp_update(double* H, int64_t I, int k, const double* M,
+                   const double* G, int* passive_out) {
+  return bpp_update(H, I, k, M, G, passive_out);
+}
+
+int orc_bpp_solve(const double* AtA, const double* AtB, int n, int64_t ncols,
+                  double* X, int* passive_out) {
+  return bpp_solve(AtA, AtB, n, ncols, X, passive_out);
+}
+
+double orc_explicit_error(const double* X, const int64_t* dims, int N,
+                          const double* const* F, const double* lambda, int k) {
+  int64_t numel = prod(dims, 0, N);
+  double normA = 0.0;
+  for (int64_t i = 0; i < numel; ++i) normA += X[i] * X[i];
+  return explicit_error(X, dims, N, F, lambda, k, normA);
+}
+
+// The AUNTF loop, ntf/auntf.hpp:128-177, starting from injected factors as
+// AUNTF::reset(init, false) leaves them (auntf.hpp:186-198): every mode
+// column-normalised by update_factor_mode (auntf.hpp:66-79), lambda := the
+// injected lambda.
+//   F (in/out): N row-major I_n x k factors (initial values in, final out)
+//   lambda (in/out): k
+//   errs: iters entries (relative error per iteration, if compute_error)
+// Returns 0, or a negative code on BPP failure (-1 iteration cap).
+int orc_ntf_run(const double* X, const int64_t* dims, int N, int k,
+                double* const* F, double* lambda, int algo, int iters,
+                int dimtree, int compute_error, double* errs) {
+  std::vector<double> tmp(k);
+  for (int n = 0; n < N; ++n) normalize_mode(F[n], dims[n], k, tmp.data());
+  int64_t numel = prod(dims, 0, N);
+  double normA = 0.0;  // Tensor::norm (squared), tensor.hpp:350-356
+  for (int64_t i = 0; i < numel; ++i) normA += X[i] * X[i];
+  bool use_dt = dimtree && (N == 3 || N == 4);
+  DimTree t;
+  if (use_dt) {
+    t.N = N;
+    t.k = k;
+    t.s = N / 2;
+    t.dims = dims;
+    t.L = prod(dims, 0, t.s + 1);
+    t.R = prod(dims, t.s + 1, N);
+    t.P.assign((size_t)t.L * k, 0.0);
+  }
+  std::vector<double> G((size_t)k * k);
+  int64_t maxI = 0;
+  for (int n = 0; n < N; ++n) maxI = std::max(maxI, dims[n]);
+  std::vector<double> M((size_t)maxI * k);
+  const double* const* Fc = F;
+  for (int it = 0; it < iters; ++it) {
+    for (int n = 0; n < N; ++n) {
+      gram_loo(Fc, dims, N, k, n, G.data());
+      if (use_dt)
+        dimtree_mttkrp(t, X, Fc, n, M.data());
+      else
+        mttkrp_direct(X, dims, N, Fc, k, n, M.data());
+      if (algo == HALS) {
+        hals_update(F[n], dims[n], k, M.data(), G.data());
+      } else if (algo == MU) {
+        mu_update(F[n], dims[n], k, M.data(), G.data());
+      } else if (algo == ANLSBPP) {
+        int rc = bpp_update(F[n], dims[n], k, M.data(), G.data(), nullptr);
+        if (rc < 0) return rc;
+      } else {
+        return -3;
+      }
+      normalize_mode(F[n], dims[n], k, lambda);
+    }
+    if (compute_error)
+      errs[it] = explicit_error(X, dims, N, Fc, lambda, k, normA);
+  }
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,250 @@
+"""planc_b200 -- B200 (sm_100a) implementation of PLANC's shared-memory NTF.
+
+Python binding of the C ABI in ``include/planc_gpu.h`` (``libplanc_gpu.so``,
+built in-tree by ``planc_b200/build.py``). There is no CPU fallback: every
+call goes to the CUDA library, and importing fails loudly if the library is
+missing.
+
+Conventions follow the reference (see ``include/planc_gpu.h``): tensors are
+column-major with mode 0 fastest (numpy Fortran order), factors are C-order
+``(I_n, k)`` float64 arrays.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libplanc_gpu.so")
+
+OK = 0
+ERR = {
+    -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_STATE", -4: "ERR_BPP_MAXITER",
+    -5: "ERR_NONFINITE", -6: "ERR_TIMEOUT", -7: "ERR_UNSUPPORTED", -8: "ERR_OOM",
+    -9: "ERR_SINGULAR",
+}
+PREC = {"fp64": 0, "bf16": 1, "bf16x2": 2}
+ALGO = {"mu": 0, "hals": 1, "anlsbpp": 2}
+F64, F32 = 0, 1
+KERNEL_CLASSES = ["contract", "ttv", "update", "normgram", "error", "reduce", "bpp"]
+
+# Every symbol declared in include/planc_gpu.h.
+EXPORTS = [
+    "planc_gpu_abi_version", "planc_gpu_last_error", "planc_gpu_create", "planc_gpu_destroy",
+    "planc_gpu_stream", "planc_gpu_set_tensor", "planc_gpu_set_factors", "planc_gpu_run",
+    "planc_gpu_get_factors", "planc_gpu_mttkrp", "planc_gpu_gram_loo",
+    "planc_gpu_objective_error", "planc_gpu_mode_begin", "planc_gpu_mode_end",
+    "planc_gpu_bpp_solve", "planc_gpu_set_timing", "planc_gpu_get_kernel_times",
+    "planc_gpu_launch_count", "planc_gpu_synth_cp_tensor",
+]
+
+
+class PlancGpuError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("%s (%d): %s" % (ERR.get(code, "ERR"), code, msg))
+        self.code = code
+
+
+_lib = None
+
+
+def load():
+    """Load libplanc_gpu.so (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise ImportError("libplanc_gpu.so is not built; run `python -m planc_b200.build`")
+    L = ctypes.CDLL(LIB_PATH)
+    P = ctypes.POINTER
+    i32, i64, d, vp = ctypes.c_int, ctypes.c_int64, ctypes.c_double, ctypes.c_void_p
+    pd, pi64, pi32 = P(d), P(i64), P(ctypes.c_int32)
+    L.planc_gpu_abi_version.restype = i32
+    L.planc_gpu_last_error.restype = ctypes.c_char_p
+    L.planc_gpu_create.argtypes = [P(vp), i32, i32, vp]
+    L.planc_gpu_destroy.argtypes = [vp]
+    L.planc_gpu_stream.argtypes = [vp]
+    L.planc_gpu_stream.restype = vp
+    L.planc_gpu_set_tensor.argtypes = [vp, vp, i32, pi64, i32, i32]
+    L.planc_gpu_set_factors.argtypes = [vp, P(pd), pd, i32]
+    L.planc_gpu_run.argtypes = [vp, i32, i32, i32, i32, pd]
+    L.planc_gpu_get_factors.argtypes = [vp, P(pd), pd]
+    L.planc_gpu_mttkrp.argtypes = [vp, i32, i32, pd]
+    L.planc_gpu_gram_loo.argtypes = [vp, i32, pd]
+    L.planc_gpu_objective_error.argtypes = [vp, pd]
+    L.planc_gpu_mode_begin.argtypes = [vp, i32, i32, pd, pd]
+    L.planc_gpu_mode_end.argtypes = [vp, i32, pd]
+    L.planc_gpu_bpp_solve.argtypes = [vp, pd, pd, i32, i64, pd, pi32, pi32]
+    L.planc_gpu_set_timing.argtypes = [vp, i32]
+    L.planc_gpu_get_kernel_times.argtypes = [vp, pd, pi64, i32]
+    L.planc_gpu_launch_count.argtypes = [vp]
+    L.planc_gpu_launch_count.restype = i64
+    L.planc_gpu_synth_cp_tensor.argtypes = [i32, vp, i32, pi64, i32, P(pd), i32, d, ctypes.c_uint64,
+                                            i32, vp]
+    for name in EXPORTS:
+        getattr(L, name).restype = getattr(L, name).restype or i32
+    L.planc_gpu_last_error.restype = ctypes.c_char_p
+    L.planc_gpu_stream.restype = vp
+    L.planc_gpu_launch_count.restype = i64
+    _lib = L
+    return L
+
+
+def _check(rc):
+    if rc != OK:
+        raise PlancGpuError(rc, load().planc_gpu_last_error().decode())
+
+
+def _pd(a):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _fptrs(F):
+    arr = (ctypes.POINTER(ctypes.c_double) * len(F))()
+    for i, f in enumerate(F):
+        arr[i] = _pd(f)
+    return arr
+
+
+def _c64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Context:
+    """One device-resident tensor + CP factors + stream (planc_gpu_ctx)."""
+
+    def __init__(self, device=0, precision="fp64", stream=None):
+        L = load()
+        h = ctypes.c_void_p()
+        _check(L.planc_gpu_create(ctypes.byref(h), device, PREC[precision], stream))
+        self.h = h
+        self.precision = precision
+        self.device = device
+        self.dims = None
+        self.k = None
+
+    def close(self):
+        if self.h:
+            load().planc_gpu_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def stream(self):
+        return load().planc_gpu_stream(self.h)
+
+    def set_tensor(self, X, dims=None, dtype=None):
+        """X: numpy array (any shape; Fortran order = mode 0 fastest), or a
+        device pointer (int) with explicit dims and dtype ('f32'/'f64')."""
+        L = load()
+        if isinstance(X, np.ndarray):
+            dims = X.shape
+            if X.dtype == np.float32:
+                dt, arr = F32, np.asfortranarray(X)
+            else:
+                dt, arr = F64, np.asfortranarray(X, dtype=np.float64)
+            ptr, on_dev = arr.ctypes.data_as(ctypes.c_void_p), 0
+            self._keep = arr
+        else:
+            dt = F32 if dtype == "f32" else F64
+            ptr, on_dev = ctypes.c_void_p(int(X)), 1
+        d = (ctypes.c_int64 * len(dims))(*dims)
+        _check(L.planc_gpu_set_tensor(self.h, ptr, dt, d, len(dims), on_dev))
+        self._keep = None
+        self.dims = tuple(int(x) for x in dims)
+
+    def set_factors(self, F, lam=None):
+        F = [_c64(f) for f in F]
+        k = F[0].shape[1]
+        lamp = _pd(_c64(lam)) if lam is not None else None
+        if lam is not None:
+            lam_arr = _c64(lam)
+            lamp = _pd(lam_arr)
+        _check(load().planc_gpu_set_factors(self.h, _fptrs(F), lamp, k))
+        self.k = k
+
+    def run(self, algo, iters, dimtree=True, compute_error=True):
+        errs = np.zeros(max(iters, 1))
+        _check(load().planc_gpu_run(self.h, ALGO[algo] if isinstance(algo, str) else int(algo),
+                                    iters, int(dimtree), int(compute_error), _pd(errs)))
+        return errs[:iters]
+
+    def get_factors(self):
+        F = [np.zeros((d, self.k)) for d in self.dims]
+        lam = np.zeros(self.k)
+        _check(load().planc_gpu_get_factors(self.h, _fptrs(F), _pd(lam)))
+        return F, lam
+
+    def mttkrp(self, mode, dimtree=True):
+        out = np.zeros((self.dims[mode], self.k))
+        _check(load().planc_gpu_mttkrp(self.h, mode, int(dimtree), _pd(out)))
+        return out
+
+    def gram_loo(self, mode):
+        out = np.zeros((self.k, self.k))
+        _check(load().planc_gpu_gram_loo(self.h, mode, _pd(out)))
+        return out
+
+    def objective_error(self):
+        e = ctypes.c_double()
+        _check(load().planc_gpu_objective_error(self.h, ctypes.byref(e)))
+        return e.value
+
+    def mode_begin(self, mode, dimtree=True):
+        G = np.zeros((self.k, self.k))
+        M = np.zeros((self.dims[mode], self.k))
+        _check(load().planc_gpu_mode_begin(self.h, mode, int(dimtree), _pd(G), _pd(M)))
+        return G, M
+
+    def mode_end(self, mode, factor):
+        f = _c64(factor)
+        _check(load().planc_gpu_mode_end(self.h, mode, _pd(f)))
+
+    def bpp_solve(self, AtA, AtB):
+        """AtA n x n, AtB n x ncols -> (X n x ncols, passive n x ncols, iters)."""
+        AtA = _c64(AtA)
+        n, ncols = AtB.shape
+        B = np.ascontiguousarray(np.asarray(AtB, dtype=np.float64).T)  # column-major n x ncols
+        X = np.zeros((ncols, n))
+        P = np.zeros((ncols, n), dtype=np.int32)
+        it = np.zeros(ncols, dtype=np.int32)
+        _check(load().planc_gpu_bpp_solve(
+            self.h, _pd(AtA), _pd(B), n, ncols, _pd(X),
+            P.ctypes.data_as(ctypes.POINTER(ctypes.c_int32)),
+            it.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))
+        return X.T.copy(), P.T.copy(), it
+
+    def set_timing(self, on):
+        _check(load().planc_gpu_set_timing(self.h, int(on)))
+
+    def kernel_times(self):
+        ms = np.zeros(len(KERNEL_CLASSES))
+        n = np.zeros(len(KERNEL_CLASSES), dtype=np.int64)
+        _check(load().planc_gpu_get_kernel_times(self.h, _pd(ms),
+                                                 n.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                                 len(KERNEL_CLASSES)))
+        return {c: (float(ms[i]), int(n[i])) for i, c in enumerate(KERNEL_CLASSES)}
+
+    def launch_count(self):
+        return int(load().planc_gpu_launch_count(self.h))
+
+
+def synth_cp_tensor(device, x_dev_ptr, dtype, dims, A, sigma, seed, clip=True, stream=None):
+    """Fill device memory with a CP model + Gaussian noise (see planc_gpu.h)."""
+    A = [_c64(a) for a in A]
+    d = (ctypes.c_int64 * len(dims))(*dims)
+    _check(load().planc_gpu_synth_cp_tensor(device, ctypes.c_void_p(int(x_dev_ptr)),
+                                            F32 if dtype == "f32" else F64, d, len(dims),
+                                            _fptrs(A), A[0].shape[1], float(sigma), int(seed),
+                                            int(clip), stream))

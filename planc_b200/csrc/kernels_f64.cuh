@@ -1,0 +1,486 @@
+// kernels_f64.cuh -- FP64 kernels of the NTF iteration: tensor contractions
+// (partial / direct MTTKRP), multi-TTV, split-K reduction, MU / HALS row
+// sweeps, normalisation + Gram, Gram-form error, tensor norm, synthetic data.
+#pragma once
+#include "common.cuh"
+
+namespace pg {
+
+// ---------------------------------------------------------------------------
+// Tensor contraction with a generated Khatri-Rao operand (FP64 DFMA).
+//
+//   RIGHT  (partial MTTKRP right contraction, dimtree/dimtrees.hpp:106-138,
+//           and the direct mode-0 MTTKRP, common/tensor.hpp:279-281):
+//             out[m, r] = sum_j X[m + ldx * j] * W(j, r),       j < K
+//   LEFT   (partial MTTKRP left contraction, dimtrees.hpp:72-105, and the
+//           direct mode-n MTTKRP as a batch over trailing slices,
+//           tensor.hpp:298-325):
+//             out[m, r] = sum_b sum_a X[a + ldx*m + ldb*b] * W(a + A*b, r)
+//
+// out is row-major (m, r) with row stride k; with a split-K grid
+// (gridDim.y > 1) each y-slice writes its partial to out + y*split_stride and
+// k_reduce_splits sums them in a fixed order (deterministic).
+// CTA tile: 128 rows x KP ranks x 32 reduction steps, 256 threads, each
+// thread owns 4 rows x KP/8 ranks.
+// ---------------------------------------------------------------------------
+constexpr int CT_BM = 128;
+constexpr int CT_BK = 32;  // reduction tile (16 at KP = 64 to stay within 48 KB of shared memory)
+template <int KP>
+constexpr int ct_bk() { return KP == 64 ? 16 : 32; }
+
+struct ContractGeom {
+  int64_t M;        // output rows
+  int64_t ldx;      // RIGHT: column stride of X; LEFT: row (m) stride
+  int64_t A;        // RIGHT: K (reduction length); LEFT: contiguous extent a
+  int64_t B;        // LEFT: number of batches b (1 for a plain 2-D view)
+  int64_t ldb;      // LEFT: batch stride of X
+  int64_t ktiles;   // total reduction tiles
+  int64_t tiles_per_split;
+  int64_t split_stride;
+};
+
+template <int KP, bool LEFT>
+__global__ void __launch_bounds__(256) k_contract_f64(const double* __restrict__ X,
+                                                      ContractGeom g, WGen wg, int k,
+                                                      double* __restrict__ out) {
+  constexpr int TN = KP / 8;
+  constexpr int BK = ct_bk<KP>();
+  constexpr int XPT = BK * CT_BM / 256;  // X elements per thread per tile
+  __shared__ double Xs[BK][CT_BM + 1];
+  __shared__ double Ws[BK][KP];
+  const int tid = threadIdx.x;
+  const int tr = tid & 7, tm = tid >> 3;
+  const int64_t m0 = (int64_t)blockIdx.x * CT_BM;
+  const int64_t t_begin = (int64_t)blockIdx.y * g.tiles_per_split;
+  int64_t t_end = t_begin + g.tiles_per_split;
+  if (t_end > g.ktiles) t_end = g.ktiles;
+  const int64_t tilesA = (g.A + BK - 1) / BK;
+
+  double acc[4][TN];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < TN; ++j) acc[i][j] = 0.0;
+
+  double xr[XPT];
+  double wr[(BK * KP + 255) / 256];
+
+  auto load_tile = [&](int64_t t) {
+    if constexpr (!LEFT) {
+      const int64_t j0 = t * BK;
+      const int mm = tid & 127;
+      const int64_t gm = m0 + mm;
+#pragma unroll
+      for (int i = 0; i < XPT; ++i) {
+        int kk = (tid >> 7) + 2 * i;
+        int64_t gj = j0 + kk;
+        xr[i] = (gm < g.M && gj < g.A) ? X[gm + g.ldx * gj] : 0.0;
+      }
+#pragma unroll
+      for (int i = 0; i < (BK * KP + 255) / 256; ++i) {
+        int e = tid + 256 * i;
+        double v = 0.0;
+        if (e < BK * KP) {
+          int kk = e / KP, r = e % KP;
+          int64_t gj = j0 + kk;
+          if (r < k && gj < g.A) v = wgen_eval(wg, gj, r, k);
+        }
+        wr[i] = v;
+      }
+    } else {
+      const int64_t b = t / tilesA;
+      const int64_t a0 = (t % tilesA) * BK;
+      const int aa = tid % BK;
+      const int64_t ga = a0 + aa;
+#pragma unroll
+      for (int i = 0; i < XPT; ++i) {
+        int mm = tid / BK + (256 / BK) * i;
+        int64_t gm = m0 + mm;
+        xr[i] = (gm < g.M && ga < g.A) ? X[ga + g.ldx * gm + g.ldb * b] : 0.0;
+      }
+#pragma unroll
+      for (int i = 0; i < (BK * KP + 255) / 256; ++i) {
+        int e = tid + 256 * i;
+        double v = 0.0;
+        if (e < BK * KP) {
+          int kk = e / KP, r = e % KP;
+          int64_t gaa = a0 + kk;
+          if (r < k && gaa < g.A) v = wgen_eval(wg, gaa + g.A * b, r, k);
+        }
+        wr[i] = v;
+      }
+    }
+  };
+  auto store_tile = [&]() {
+    if constexpr (!LEFT) {
+      const int mm = tid & 127;
+#pragma unroll
+      for (int i = 0; i < XPT; ++i) Xs[(tid >> 7) + 2 * i][mm] = xr[i];
+    } else {
+      const int aa = tid % BK;
+#pragma unroll
+      for (int i = 0; i < XPT; ++i) Xs[aa][tid / BK + (256 / BK) * i] = xr[i];
+    }
+#pragma unroll
+    for (int i = 0; i < (BK * KP + 255) / 256; ++i) {
+      int e = tid + 256 * i;
+      if (e < BK * KP) Ws[e / KP][e % KP] = wr[i];
+    }
+  };
+
+  if (t_begin < t_end) load_tile(t_begin);
+  for (int64_t t = t_begin; t < t_end; ++t) {
+    __syncthreads();
+    store_tile();
+    __syncthreads();
+    if (t + 1 < t_end) load_tile(t + 1);
+#pragma unroll 8
+    for (int kk = 0; kk < BK; ++kk) {
+      double xv[4], wv[TN];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) xv[i] = Xs[kk][tm + 32 * i];
+#pragma unroll
+      for (int j = 0; j < TN; ++j) wv[j] = Ws[kk][tr + 8 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < TN; ++j) acc[i][j] = fma(xv[i], wv[j], acc[i][j]);
+    }
+  }
+  double* o = out + (int64_t)blockIdx.y * g.split_stride;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    int64_t gm = m0 + tm + 32 * i;
+    if (gm >= g.M) continue;
+#pragma unroll
+    for (int j = 0; j < TN; ++j) {
+      int r = tr + 8 * j;
+      if (r < k) o[gm * k + r] = acc[i][j];
+    }
+  }
+}
+
+// out[i] = sum_{s < nsplit} part[s * stride + i], fixed order.
+__global__ void k_reduce_splits(const double* __restrict__ part, int nsplit, int64_t stride,
+                                int64_t n, double* __restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int p = 0; p < nsplit; ++p) s += part[p * stride + i];
+    out[i] = s;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Multi-TTV on a row-major (A*B) x k intermediate T (rank index fastest),
+// dimtree/dimtrees.hpp:315-410:
+//   left : out[b, r] = sum_a T[(a + A*b)*k + r] * F[a*k + r]
+//   right: out[a, r] = sum_b T[(a + A*b)*k + r] * W(b, r)
+// ---------------------------------------------------------------------------
+template <typename TT>
+__global__ void __launch_bounds__(256) k_ttv_left(const TT* __restrict__ T, int64_t A, int64_t B,
+                                                  int k, const double* __restrict__ F,
+                                                  double* __restrict__ out) {
+  __shared__ double red[256];
+  const int lanes = 256 / k;
+  const int tid = threadIdx.x;
+  const int r = tid % k, lane = tid / k;
+  for (int64_t b = blockIdx.x; b < B; b += gridDim.x) {
+    double s = 0.0;
+    if (lane < lanes) {
+      const TT* Tb = T + (A * b) * k;
+      for (int64_t a = lane; a < A; a += lanes) s = fma((double)Tb[a * k + r], F[a * k + r], s);
+    }
+    red[tid] = s;
+    __syncthreads();
+    if (tid < k) {
+      double t = 0.0;
+      for (int l = 0; l < lanes; ++l) t += red[l * k + tid];
+      out[b * k + tid] = t;
+    }
+    __syncthreads();
+  }
+}
+
+template <typename TT>
+__global__ void __launch_bounds__(256) k_ttv_right(const TT* __restrict__ T, int64_t A, int64_t B,
+                                                   int k, WGen wg, int64_t b_per_split,
+                                                   int64_t split_stride,
+                                                   double* __restrict__ out) {
+  const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= A * k) return;
+  const int64_t a = e / k;
+  const int r = (int)(e % k);
+  int64_t b0 = (int64_t)blockIdx.y * b_per_split;
+  int64_t b1 = b0 + b_per_split;
+  if (b1 > B) b1 = B;
+  double s = 0.0;
+  for (int64_t b = b0; b < b1; ++b)
+    s = fma((double)T[(a + A * b) * k + r], wgen_eval(wg, b, r, k), s);
+  out[(int64_t)blockIdx.y * split_stride + e] = s;
+}
+
+// ---------------------------------------------------------------------------
+// Factor updates, one thread per factor row (each row's recurrence reads only
+// that row of H and M, and G).
+// ---------------------------------------------------------------------------
+// HALS, ntf/ntfhals.hpp:13-29 + common/utils.hpp:59-64:
+//   for i < k: u = h_i + (m_i - sum_j h_j G[j,i]);  h_i = (u < 1e-17) ? 1e-17 : u
+// Column i of H is replaced in place before column i+1 is computed; the
+// reference's ||u||^2 > 0 guard always holds once every entry is >= 1e-17.
+template <int KP>
+__global__ void __launch_bounds__(128) k_hals_rows(double* __restrict__ H, const double* __restrict__ M,
+                                                   const double* __restrict__ G, int64_t I, int k) {
+  __shared__ double Gs[KP * KP];
+  for (int e = threadIdx.x; e < k * k; e += blockDim.x) Gs[e] = G[e];
+  __syncthreads();
+  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= I) return;
+  double h[KP], m[KP];
+#pragma unroll
+  for (int j = 0; j < KP; ++j) {
+    h[j] = j < k ? H[row * k + j] : 0.0;
+    m[j] = j < k ? M[row * k + j] : 0.0;
+  }
+#pragma unroll
+  for (int i = 0; i < KP; ++i) {
+    if (i < k) {
+      double hg = 0.0;
+#pragma unroll
+      for (int j = 0; j < KP; ++j)
+        if (j < k) hg = fma(h[j], Gs[j * k + i], hg);
+      double u = h[i] + (m[i] - hg);
+      h[i] = (u < kEps17) ? kEps17 : u;
+    }
+  }
+#pragma unroll
+  for (int j = 0; j < KP; ++j)
+    if (j < k) H[row * k + j] = h[j];
+}
+
+// MU, ntf/ntfmu.hpp:11-16: H = (H % M^T) / (H*G + 1e-6), H*G from the old H.
+template <int KP>
+__global__ void __launch_bounds__(128) k_mu_rows(double* __restrict__ H, const double* __restrict__ M,
+                                                 const double* __restrict__ G, int64_t I, int k) {
+  __shared__ double Gs[KP * KP];
+  for (int e = threadIdx.x; e < k * k; e += blockDim.x) Gs[e] = G[e];
+  __syncthreads();
+  const int64_t row = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (row >= I) return;
+  double h[KP], t[KP];
+#pragma unroll
+  for (int j = 0; j < KP; ++j) h[j] = j < k ? H[row * k + j] : 0.0;
+#pragma unroll
+  for (int c = 0; c < KP; ++c) {
+    double acc = 0.0;
+#pragma unroll
+    for (int j = 0; j < KP; ++j)
+      if (j < k && c < k) acc = fma(h[j], Gs[j * k + c], acc);
+    t[c] = acc + kEps6;
+  }
+#pragma unroll
+  for (int c = 0; c < KP; ++c)
+    if (c < k) H[row * k + c] = (h[c] * M[row * k + c]) / t[c];
+}
+
+// ---------------------------------------------------------------------------
+// Normalise mode n (NCPFactors::normalize(int), common/ncpfactors.hpp:346-351:
+// lambda_r = ||F(:,r)||, F(:,r) /= lambda_r when > 0), then G_n = F^T F of the
+// normalised factor (ncpfactors.hpp:144) and, if next >= 0, the leave-one-out
+// Hadamard product for mode `next` (ncpfactors.hpp:139-148, modes in
+// increasing order starting from ones). One CTA of 1024 threads.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(1024) k_normalize_gram(double* __restrict__ F, int64_t I, int k,
+                                                         double* __restrict__ lambda,
+                                                         double* __restrict__ Gall, int N, int n,
+                                                         int next, double* __restrict__ Gloo) {
+  __shared__ double red[1024];
+  __shared__ double lam[kMaxRank];
+  const int tid = threadIdx.x;
+  const int lanes = 1024 / k;
+  const int r = tid % k, lane = tid / k;
+  double ss = 0.0;
+  if (lane < lanes)
+    for (int64_t i = lane; i < I; i += lanes) {
+      double v = F[i * k + r];
+      ss = fma(v, v, ss);
+    }
+  red[tid] = ss;
+  __syncthreads();
+  if (tid < k) {
+    double t = 0.0;
+    for (int l = 0; l < lanes; ++l) t += red[l * k + tid];
+    double nrm = sqrt(t);
+    lam[tid] = nrm;
+    if (lambda) lambda[tid] = nrm;
+  }
+  __syncthreads();
+  for (int64_t e = tid; e < I * k; e += 1024) {
+    double nrm = lam[e % k];
+    if (nrm > 0) F[e] = F[e] / nrm;
+  }
+  __syncthreads();
+  double* Gn = Gall + (int64_t)n * k * k;
+  for (int e = tid; e < k * k; e += 1024) {
+    int a = e / k, b = e % k;
+    double s = 0.0;
+    for (int64_t i = 0; i < I; ++i) s = fma(F[i * k + a], F[i * k + b], s);
+    Gn[e] = s;
+  }
+  if (next < 0) return;
+  __syncthreads();
+  for (int e = tid; e < k * k; e += 1024) {
+    double g = 1.0;
+    for (int i = 0; i < N; ++i)
+      if (i != next) g = g * Gall[(int64_t)i * k * k + e];
+    Gloo[e] = g;
+  }
+}
+
+// Leave-one-out Hadamard product from cached Grams.
+__global__ void k_gram_loo(const double* __restrict__ Gall, int N, int k, int n,
+                           double* __restrict__ Gloo) {
+  for (int e = threadIdx.x; e < k * k; e += blockDim.x) {
+    double g = 1.0;
+    for (int i = 0; i < N; ++i)
+      if (i != n) g = g * Gall[(int64_t)i * k * k + e];
+    Gloo[e] = g;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Relative error in FP64 Gram form (the form of distntf/distauntf.hpp:685-727;
+// value of AUNTF::computeObjectiveError, ntf/auntf.hpp:200-246):
+//   ||X - [[lambda; F]]||^2 = ||X||^2 - 2 sum_r lambda_r <M_last(:,r), F_last(:,r)>
+//                             + lambda^T (*_i G_i) lambda
+// M_last is the MTTKRP of the last mode, computed from the final F_0..F_{N-2}.
+// Writes errs[*counter] and increments *counter (so one captured graph can be
+// replayed across iterations). One CTA of 256 threads.
+// ---------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_error(const double* __restrict__ Mlast,
+                                               const double* __restrict__ Flast, int64_t I,
+                                               const double* __restrict__ lambda,
+                                               const double* __restrict__ Gall, int N, int k,
+                                               const double* __restrict__ normX2,
+                                               double* __restrict__ errs, int* __restrict__ counter) {
+  __shared__ double red[256];
+  __shared__ double red2[256];
+  const int tid = threadIdx.x;
+  double inner = 0.0;
+  for (int64_t e = tid; e < I * k; e += 256) inner = fma(Mlast[e] * Flast[e], lambda[e % k], inner);
+  double mn = 0.0;
+  for (int e = tid; e < k * k; e += 256) {
+    double g = 1.0;
+    for (int i = 0; i < N; ++i) g = g * Gall[(int64_t)i * k * k + e];
+    mn = fma(lambda[e / k] * lambda[e % k], g, mn);
+  }
+  red[tid] = inner;
+  red2[tid] = mn;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (tid < s) {
+      red[tid] += red[tid + s];
+      red2[tid] += red2[tid + s];
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    double nx = *normX2;
+    double e2 = nx - 2.0 * red[0] + red2[0];
+    double err = sqrt(fabs(e2) / nx);
+    int c = *counter;
+    errs[c] = err;
+    *counter = c + 1;
+  }
+}
+
+// Sum of squares in FP64 (Tensor::norm, common/tensor.hpp:350-356), per-block
+// partials; k_reduce_splits with nsplit = blocks finishes it.
+template <typename T>
+__global__ void __launch_bounds__(256) k_sumsq_partial(const T* __restrict__ X, int64_t n,
+                                                       double* __restrict__ part) {
+  __shared__ double red[256];
+  double s = 0.0;
+  for (int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256) {
+    double v = (double)X[i];
+    s = fma(v, v, s);
+  }
+  red[threadIdx.x] = s;
+  __syncthreads();
+  for (int st = 128; st > 0; st >>= 1) {
+    if (threadIdx.x < st) red[threadIdx.x] += red[threadIdx.x + st];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+template <typename T>
+__global__ void k_copy_to_f64(const T* __restrict__ in, int64_t n, double* __restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = (double)in[i];
+}
+
+// ---------------------------------------------------------------------------
+// Synthetic CP tensor: X = [[A_0..A_{N-1}]] + sigma * N(0,1), optionally
+// clipped at 0. Normals come from Philox-4x32-10 (Salmon et al., SC'11) keyed
+// by `seed` and counted by the element index, through the Box-Muller
+// transform, so the tensor is a pure function of (factors, sigma, seed).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void philox4x32_10(uint32_t ctr[4], uint32_t key[2]) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+  const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+#pragma unroll
+  for (int round = 0; round < 10; ++round) {
+    uint32_t hi0 = __umulhi(M0, ctr[0]), lo0 = M0 * ctr[0];
+    uint32_t hi1 = __umulhi(M1, ctr[2]), lo1 = M1 * ctr[2];
+    uint32_t n0 = hi1 ^ ctr[1] ^ key[0];
+    uint32_t n1 = lo1;
+    uint32_t n2 = hi0 ^ ctr[3] ^ key[1];
+    uint32_t n3 = lo0;
+    ctr[0] = n0; ctr[1] = n1; ctr[2] = n2; ctr[3] = n3;
+    key[0] += W0;
+    key[1] += W1;
+  }
+}
+
+struct SynthDesc {
+  const double* A[kMaxModes];
+  int64_t dims[kMaxModes];
+  int N, k;
+  double sigma;
+  uint64_t seed;
+  int clip;
+};
+
+template <typename T>
+__global__ void __launch_bounds__(256) k_synth_cp(SynthDesc d, int64_t numel, T* __restrict__ X) {
+  for (int64_t idx = (int64_t)blockIdx.x * 256 + threadIdx.x; idx < numel;
+       idx += (int64_t)gridDim.x * 256) {
+    int64_t rem = idx;
+    int64_t sub[kMaxModes];
+    for (int m = 0; m < d.N; ++m) {
+      sub[m] = rem % d.dims[m];
+      rem /= d.dims[m];
+    }
+    double v = 0.0;
+    for (int r = 0; r < d.k; ++r) {
+      double p = 1.0;
+      for (int m = d.N - 1; m >= 0; --m) p = d.A[m][sub[m] * d.k + r] * p;
+      v += p;
+    }
+    if (d.sigma > 0) {
+      uint32_t ctr[4] = {(uint32_t)idx, (uint32_t)(idx >> 32), 0x5eedu, 0u};
+      uint32_t key[2] = {(uint32_t)d.seed, (uint32_t)(d.seed >> 32)};
+      philox4x32_10(ctr, key);
+      double u1 = ((double)ctr[0] + 1.0) * (1.0 / 4294967296.0);  // (0, 1]
+      double u2 = (double)ctr[1] * (1.0 / 4294967296.0);          // [0, 1)
+      double z = sqrt(-2.0 * log(u1)) * cospi(2.0 * u2);
+      v += d.sigma * z;
+    }
+    if (d.clip && v < 0) v = 0;
+    X[idx] = (T)v;
+  }
+}
+
+}  // namespace pg

@@ -1,0 +1,1056 @@
+// planc_gpu.cu -- context, orchestration and C ABI of the B200 NTF library.
+//
+// One context = one device-resident tensor + CP factors + one stream. The
+// AUNTF outer iteration (ntf/auntf.hpp:128-177) is issued as a fixed launch
+// sequence per mode: [MTTKRP] -> [update] -> [normalise + Gram + next
+// leave-one-out Gram], then the Gram-form error; it is captured once into a
+// CUDA graph and replayed for every iteration.
+#include <cuda.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/planc_gpu.h"
+#include "bpp.cuh"
+#include "common.cuh"
+#include "kernels_f64.cuh"
+#include "tc_mttkrp.cuh"
+
+using namespace pg;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct Fail {
+  int code;
+};
+
+[[noreturn]] void fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  throw Fail{code};
+}
+
+void cuda_check(cudaError_t e, const char* what) {
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    fail(e == cudaErrorMemoryAllocation ? PLANC_GPU_ERR_OOM : PLANC_GPU_ERR_CUDA,
+         std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+#define CK(x) cuda_check((x), #x)
+
+template <typename F>
+int guarded(F&& f) {
+  try {
+    f();
+    return PLANC_GPU_OK;
+  } catch (const Fail& e) {
+    return e.code;
+  } catch (...) {
+    g_last_error = "unexpected host exception";
+    return PLANC_GPU_ERR_CUDA;
+  }
+}
+
+int kpad(int k) { return k <= 8 ? 8 : k <= 16 ? 16 : k <= 32 ? 32 : 64; }
+
+}  // namespace
+
+struct planc_gpu_ctx {
+  int device = 0;
+  int precision = PLANC_GPU_PREC_FP64;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  int sm_count = 148;
+
+  int N = 0;
+  int64_t dims[kMaxModes] = {0};
+  int64_t numel = 0;
+  int s = 0;
+  int64_t L = 0, R = 0;
+  int k = 0;
+  bool have_tensor = false, have_factors = false;
+
+  double* X64 = nullptr;         // FP64 tensor (plain path)
+  TcTensor tct;                  // tensor-core operand copy (BF16 paths)
+  double* normX2 = nullptr;      // device scalar ||X||^2
+  double* F[kMaxModes] = {nullptr};
+  double* M[kMaxModes] = {nullptr};
+  double* Gall = nullptr;
+  double* Gloo = nullptr;
+  double* lambda = nullptr;
+  double* P = nullptr;           // right-contracted partial MTTKRP, row-major L x k
+  float* P32 = nullptr;          // same, FP32, for the tensor-core paths
+  double* Q = nullptr;           // N = 4: P contracted with F_0, row-major (I1*I2) x k
+  double* scratch = nullptr;
+  size_t scratch_elems = 0;
+  double* errs_dev = nullptr;
+  int errs_cap = 0;
+  int* counter_dev = nullptr;
+  int* status_dev = nullptr;
+  int64_t factor_cap[kMaxModes] = {0};
+
+  cudaGraphExec_t gexec = nullptr;
+  int g_algo = -1, g_dimtree = -1, g_err = -1;
+
+  bool timing = false;
+  bool capturing = false;
+  struct Pending {
+    int cls;
+    cudaEvent_t a, b;
+  };
+  std::vector<Pending> pending;
+  std::vector<cudaEvent_t> ev_pool;
+  double kms[KC_COUNT] = {0};
+  int64_t klaunch[KC_COUNT] = {0};
+  int64_t launch_count = 0;
+};
+
+namespace {
+
+void set_device(planc_gpu_ctx* c) { CK(cudaSetDevice(c->device)); }
+
+template <typename T>
+void dalloc(T** p, size_t n) {
+  if (*p) {
+    cudaFree(*p);
+    *p = nullptr;
+  }
+  if (n == 0) return;
+  CK(cudaMalloc((void**)p, n * sizeof(T)));
+}
+
+cudaEvent_t get_event(planc_gpu_ctx* c) {
+  if (!c->ev_pool.empty()) {
+    cudaEvent_t e = c->ev_pool.back();
+    c->ev_pool.pop_back();
+    return e;
+  }
+  cudaEvent_t e;
+  CK(cudaEventCreate(&e));
+  return e;
+}
+
+void drain_timing(planc_gpu_ctx* c) {
+  if (c->pending.empty()) return;
+  CK(cudaStreamSynchronize(c->stream));
+  for (auto& p : c->pending) {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, p.a, p.b));
+    c->kms[p.cls] += ms;
+    c->klaunch[p.cls] += 1;
+    c->ev_pool.push_back(p.a);
+    c->ev_pool.push_back(p.b);
+  }
+  c->pending.clear();
+}
+
+// Launch wrapper: counts launches, checks the launch error, optionally
+// brackets the launch with events of its kernel class.
+template <typename Fn>
+void launch(planc_gpu_ctx* c, int cls, Fn&& fn) {
+  cudaEvent_t a = nullptr, b = nullptr;
+  bool timed = c->timing && !c->capturing;
+  if (timed) {
+    a = get_event(c);
+    b = get_event(c);
+    CK(cudaEventRecord(a, c->stream));
+  }
+  fn();
+  CK(cudaGetLastError());
+  if (timed) {
+    CK(cudaEventRecord(b, c->stream));
+    c->pending.push_back({cls, a, b});
+    if (c->pending.size() > 4096) drain_timing(c);
+  }
+  c->launch_count++;
+}
+
+WGen make_wgen(planc_gpu_ctx* c, const std::vector<int>& modes) {
+  WGen g;
+  memset(&g, 0, sizeof(g));
+  g.nf = (int)modes.size();
+  int64_t stride = 1;
+  for (int t = 0; t < g.nf; ++t) {
+    g.f[t] = c->F[modes[t]];
+    g.dim[t] = c->dims[modes[t]];
+    g.stride[t] = stride;
+    stride *= c->dims[modes[t]];
+  }
+  return g;
+}
+
+// ---------------------------------------------------------------- planning
+struct ContractPlan {
+  ContractGeom g;
+  int nsplit;
+  dim3 grid;
+};
+
+ContractPlan plan_contract(planc_gpu_ctx* c, bool left, int64_t M, int64_t ldx, int64_t A,
+                           int64_t B, int64_t ldb) {
+  ContractPlan p;
+  memset(&p, 0, sizeof(p));
+  p.g.M = M;
+  p.g.ldx = ldx;
+  p.g.A = A;
+  p.g.B = B;
+  p.g.ldb = ldb;
+  const int bk = c->k > 32 ? ct_bk<64>() : ct_bk<32>();
+  int64_t tilesA = (A + bk - 1) / bk;
+  p.g.ktiles = left ? tilesA * B : tilesA;
+  int64_t mtiles = (M + CT_BM - 1) / CT_BM;
+  int64_t target = 2 * (int64_t)c->sm_count;
+  int64_t ns = (target + mtiles - 1) / mtiles;
+  ns = std::max<int64_t>(1, std::min<int64_t>(ns, p.g.ktiles));
+  ns = std::min<int64_t>(ns, 1024);
+  p.g.tiles_per_split = (p.g.ktiles + ns - 1) / ns;
+  ns = (p.g.ktiles + p.g.tiles_per_split - 1) / p.g.tiles_per_split;
+  if (ns < 1) ns = 1;
+  p.nsplit = (int)ns;
+  p.g.split_stride = M * c->k;
+  p.grid = dim3((unsigned)mtiles, (unsigned)ns, 1);
+  return p;
+}
+
+size_t contract_scratch(const ContractPlan& p) {
+  return p.nsplit > 1 ? (size_t)p.nsplit * p.g.split_stride : 0;
+}
+
+struct TtvRightPlan {
+  int64_t bper;
+  int nsplit;
+  dim3 grid;
+};
+
+TtvRightPlan plan_ttv_right(planc_gpu_ctx* c, int64_t A, int64_t B) {
+  TtvRightPlan p;
+  int64_t gx = (A * c->k + 255) / 256;
+  int64_t target = 2 * (int64_t)c->sm_count;
+  int64_t ns = std::max<int64_t>(1, std::min<int64_t>((target + gx - 1) / gx, B));
+  ns = std::min<int64_t>(ns, 256);
+  p.bper = (B + ns - 1) / ns;
+  ns = (B + p.bper - 1) / p.bper;
+  p.nsplit = (int)ns;
+  p.grid = dim3((unsigned)gx, (unsigned)ns, 1);
+  return p;
+}
+
+void direct_geom(planc_gpu_ctx* c, int n, int64_t* A, int64_t* B) {
+  *A = 1;
+  *B = 1;
+  for (int m = 0; m < n; ++m) *A *= c->dims[m];
+  for (int m = n + 1; m < c->N; ++m) *B *= c->dims[m];
+}
+
+// Computes the largest scratch any MTTKRP path needs and (re)allocates.
+void ensure_buffers(planc_gpu_ctx* c) {
+  const int k = c->k;
+  size_t need = 0;
+  if (c->N == 3 || c->N == 4) {
+    ContractPlan pl = plan_contract(c, true, c->R, c->L, c->L, 1, 0);
+    need = std::max(need, contract_scratch(pl));
+    TtvRightPlan tr = plan_ttv_right(c, c->dims[0], c->L / c->dims[0]);
+    need = std::max(need, (size_t)tr.nsplit * c->dims[0] * k);
+    if (c->N == 4) {
+      TtvRightPlan t2 = plan_ttv_right(c, c->dims[1], c->dims[2]);
+      need = std::max(need, (size_t)t2.nsplit * c->dims[1] * k);
+    }
+    need = std::max(need, tc_scratch_elems(c->tct, c->sm_count, k));
+  }
+  for (int n = 0; n < c->N; ++n) {
+    int64_t A, B;
+    direct_geom(c, n, &A, &B);
+    ContractPlan pl = n == 0 ? plan_contract(c, false, c->dims[0], c->dims[0], B, 1, 0)
+                             : plan_contract(c, true, c->dims[n], A, A, B, A * c->dims[n]);
+    need = std::max(need, contract_scratch(pl));
+  }
+  need = std::max<size_t>(need, 4096);
+  if (need > c->scratch_elems) {
+    dalloc(&c->scratch, need);
+    c->scratch_elems = need;
+  }
+  if ((c->N == 3 || c->N == 4)) {
+    if (c->precision == PLANC_GPU_PREC_FP64) {
+      if (!c->P) dalloc(&c->P, (size_t)c->L * k);
+    } else {
+      if (!c->P32) dalloc(&c->P32, (size_t)c->L * k);
+    }
+    if (c->N == 4 && !c->Q) dalloc(&c->Q, (size_t)c->dims[1] * c->dims[2] * k);
+  }
+}
+
+void run_contract(planc_gpu_ctx* c, const ContractPlan& p, bool left, const double* X,
+                  const WGen& wg, double* out) {
+  const int k = c->k;
+  double* dst = p.nsplit > 1 ? c->scratch : out;
+  launch(c, KC_CONTRACT, [&] {
+    switch (kpad(k)) {
+#define CASE(KP)                                                                      \
+  case KP:                                                                            \
+    if (left)                                                                         \
+      k_contract_f64<KP, true><<<p.grid, 256, 0, c->stream>>>(X, p.g, wg, k, dst);    \
+    else                                                                              \
+      k_contract_f64<KP, false><<<p.grid, 256, 0, c->stream>>>(X, p.g, wg, k, dst);   \
+    break;
+      CASE(8) CASE(16) CASE(32) CASE(64)
+#undef CASE
+    }
+  });
+  if (p.nsplit > 1) {
+    int64_t n = p.g.M * k;
+    launch(c, KC_REDUCE, [&] {
+      k_reduce_splits<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, c->stream>>>(
+          c->scratch, p.nsplit, p.g.split_stride, n, out);
+    });
+  }
+}
+
+template <typename TT>
+void run_ttv_right(planc_gpu_ctx* c, const TT* T, int64_t A, int64_t B, const WGen& wg,
+                   double* out) {
+  TtvRightPlan p = plan_ttv_right(c, A, B);
+  double* dst = p.nsplit > 1 ? c->scratch : out;
+  int k = c->k;
+  launch(c, KC_TTV, [&] {
+    k_ttv_right<TT><<<p.grid, 256, 0, c->stream>>>(T, A, B, k, wg, p.bper, A * k, dst);
+  });
+  if (p.nsplit > 1) {
+    int64_t n = A * k;
+    launch(c, KC_REDUCE, [&] {
+      k_reduce_splits<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, c->stream>>>(
+          c->scratch, p.nsplit, n, n, out);
+    });
+  }
+}
+
+template <typename TT>
+void run_ttv_left(planc_gpu_ctx* c, const TT* T, int64_t A, int64_t B, const double* Fa,
+                  double* out) {
+  int k = c->k;
+  launch(c, KC_TTV, [&] {
+    k_ttv_left<TT><<<(unsigned)std::min<int64_t>(B, 65535), 256, 0, c->stream>>>(T, A, B, k, Fa, out);
+  });
+}
+
+// ---------------------------------------------------------------- MTTKRP
+// Direct MTTKRP of mode n (common/tensor.hpp:246-327), FP64.
+void mttkrp_direct(planc_gpu_ctx* c, int n, double* out) {
+  if (!c->X64) fail(PLANC_GPU_ERR_UNSUPPORTED, "direct MTTKRP needs the FP64 tensor copy");
+  std::vector<int> modes;
+  for (int m = 0; m < c->N; ++m)
+    if (m != n) modes.push_back(m);
+  WGen wg = make_wgen(c, modes);
+  int64_t A, B;
+  direct_geom(c, n, &A, &B);
+  if (n == 0) {
+    ContractPlan p = plan_contract(c, false, c->dims[0], c->dims[0], B, 1, 0);
+    run_contract(c, p, false, c->X64, wg, out);
+  } else {
+    ContractPlan p = plan_contract(c, true, c->dims[n], A, A, B, A * c->dims[n]);
+    run_contract(c, p, true, c->X64, wg, out);
+  }
+}
+
+// Right contraction P = X_(L x R) * F_{N-1} (dimtrees.hpp:281-306).
+void partial_right(planc_gpu_ctx* c) {
+  if (c->precision == PLANC_GPU_PREC_FP64) {
+    WGen wg = make_wgen(c, {c->N - 1});
+    ContractPlan p = plan_contract(c, false, c->L, c->L, c->R, 1, 0);
+    run_contract(c, p, false, c->X64, wg, c->P);
+  } else {
+    launch(c, KC_CONTRACT, [&] { tc_right(c->tct, c->F[c->N - 1], c->k, c->P32, c->stream); });
+  }
+}
+
+// Left contraction M_{N-1} = X^T * KRP(F_0..F_s) (dimtrees.hpp:250-271).
+void partial_left(planc_gpu_ctx* c, double* out) {
+  std::vector<int> modes;
+  for (int m = 0; m <= c->s; ++m) modes.push_back(m);
+  if (c->precision == PLANC_GPU_PREC_FP64) {
+    WGen wg = make_wgen(c, modes);
+    ContractPlan p = plan_contract(c, true, c->R, c->L, c->L, 1, 0);
+    run_contract(c, p, true, c->X64, wg, out);
+  } else {
+    WGen wg = make_wgen(c, modes);
+    int nsplit = 0;
+    launch(c, KC_CONTRACT, [&] {
+      nsplit = tc_left(c->tct, wg, c->k, c->scratch, c->sm_count, c->stream);
+    });
+    int64_t n = c->R * c->k;
+    launch(c, KC_REDUCE, [&] {
+      k_reduce_splits<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, c->stream>>>(
+          c->scratch, nsplit, n, n, out);
+    });
+  }
+}
+
+// Dimension-tree MTTKRP of mode n (DenseDimensionTree::in_order_reuse_MTTKRP,
+// dimtree/ddt.hpp:134-243). Mode 0 recomputes P from the current F_{N-1};
+// modes 1..s reuse it with the freshly updated F_0 (.. F_{n-1}).
+void mttkrp_dimtree(planc_gpu_ctx* c, int n, double* out) {
+  const int N = c->N;
+  const bool f64 = c->precision == PLANC_GPU_PREC_FP64;
+  if (n == 0) {
+    partial_right(c);
+    std::vector<int> modes;
+    for (int m = 1; m <= c->s; ++m) modes.push_back(m);
+    WGen wg = make_wgen(c, modes);
+    if (f64)
+      run_ttv_right<double>(c, c->P, c->dims[0], c->L / c->dims[0], wg, out);
+    else
+      run_ttv_right<float>(c, c->P32, c->dims[0], c->L / c->dims[0], wg, out);
+    return;
+  }
+  if (n == c->s + 1) {
+    partial_left(c, out);
+    return;
+  }
+  if (N == 3) {  // n == 1
+    if (f64)
+      run_ttv_left<double>(c, c->P, c->dims[0], c->dims[1], c->F[0], out);
+    else
+      run_ttv_left<float>(c, c->P32, c->dims[0], c->dims[1], c->F[0], out);
+    return;
+  }
+  // N == 4
+  if (n == 1) {
+    if (f64)
+      run_ttv_left<double>(c, c->P, c->dims[0], c->dims[1] * c->dims[2], c->F[0], c->Q);
+    else
+      run_ttv_left<float>(c, c->P32, c->dims[0], c->dims[1] * c->dims[2], c->F[0], c->Q);
+    WGen wg = make_wgen(c, {2});
+    run_ttv_right<double>(c, c->Q, c->dims[1], c->dims[2], wg, out);
+    return;
+  }
+  // n == 2
+  run_ttv_left<double>(c, c->Q, c->dims[1], c->dims[2], c->F[1], out);
+}
+
+void mttkrp_any(planc_gpu_ctx* c, int n, bool dimtree, double* out) {
+  if (dimtree && (c->N == 3 || c->N == 4))
+    mttkrp_dimtree(c, n, out);
+  else
+    mttkrp_direct(c, n, out);
+}
+
+// ---------------------------------------------------------------- updates
+void run_update(planc_gpu_ctx* c, int algo, int n) {
+  const int k = c->k;
+  const int64_t I = c->dims[n];
+  if (algo == PLANC_GPU_HALS || algo == PLANC_GPU_MU) {
+    unsigned blocks = (unsigned)((I + 127) / 128);
+    launch(c, KC_UPDATE, [&] {
+      switch (kpad(k)) {
+#define CASE(KP)                                                                              \
+  case KP:                                                                                    \
+    if (algo == PLANC_GPU_HALS)                                                               \
+      k_hals_rows<KP><<<blocks, 128, 0, c->stream>>>(c->F[n], c->M[n], c->Gloo, I, k);        \
+    else                                                                                      \
+      k_mu_rows<KP><<<blocks, 128, 0, c->stream>>>(c->F[n], c->M[n], c->Gloo, I, k);          \
+    break;
+        CASE(8) CASE(16) CASE(32) CASE(64)
+#undef CASE
+      }
+    });
+  } else if (algo == PLANC_GPU_ANLSBPP) {
+    // NTFANLSBPP::update (ntf/ntfanlsbpp.hpp:15-57): all I_n right-hand sides
+    // in one launch; the 2000-column chunking does not change values.
+    unsigned blocks = (unsigned)((I + BPP_WARPS - 1) / BPP_WARPS);
+    launch(c, KC_BPP, [&] {
+      switch (kpad(k)) {
+#define CASE(KP)                                                                                   \
+  case KP:                                                                                         \
+    k_bpp<KP><<<blocks, 32 * BPP_WARPS, 0, c->stream>>>(c->Gloo, c->M[n], k, I, c->F[n], nullptr, \
+                                                        nullptr, c->status_dev);                   \
+    break;
+        CASE(8) CASE(16) CASE(32) CASE(64)
+#undef CASE
+      }
+    });
+  } else {
+    fail(PLANC_GPU_ERR_ARG, "unknown algorithm " + std::to_string(algo));
+  }
+}
+
+void normalize_gram(planc_gpu_ctx* c, int n, int next, double* lambda) {
+  launch(c, KC_NORMGRAM, [&] {
+    k_normalize_gram<<<1, 1024, 0, c->stream>>>(c->F[n], c->dims[n], c->k, lambda, c->Gall, c->N,
+                                                n, next, c->Gloo);
+  });
+}
+
+void gram_loo(planc_gpu_ctx* c, int n) {
+  launch(c, KC_NORMGRAM, [&] { k_gram_loo<<<1, 1024, 0, c->stream>>>(c->Gall, c->N, c->k, n, c->Gloo); });
+}
+
+void error_kernel(planc_gpu_ctx* c) {
+  const int last = c->N - 1;
+  launch(c, KC_ERROR, [&] {
+    k_error<<<1, 256, 0, c->stream>>>(c->M[last], c->F[last], c->dims[last], c->lambda, c->Gall,
+                                      c->N, c->k, c->normX2, c->errs_dev, c->counter_dev);
+  });
+}
+
+// One AUNTF outer iteration (ntf/auntf.hpp:131-170).
+void one_iteration(planc_gpu_ctx* c, int algo, bool dimtree, bool err) {
+  for (int n = 0; n < c->N; ++n) {
+    mttkrp_any(c, n, dimtree, c->M[n]);
+    run_update(c, algo, n);
+    normalize_gram(c, n, (n + 1) % c->N, c->lambda);
+  }
+  if (err) error_kernel(c);
+}
+
+void require_ready(planc_gpu_ctx* c) {
+  if (!c) fail(PLANC_GPU_ERR_ARG, "null context");
+  if (!c->have_tensor) fail(PLANC_GPU_ERR_STATE, "no tensor set");
+  if (!c->have_factors) fail(PLANC_GPU_ERR_STATE, "no factors set");
+}
+
+void check_status(planc_gpu_ctx* c) {
+  int st = 0;
+  CK(cudaMemcpyAsync(&st, c->status_dev, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (st != 0) {
+    CK(cudaMemsetAsync(c->status_dev, 0, sizeof(int), c->stream));
+    const char* what = st == kStBppMaxIter ? "BPP failed (iteration cap 5k reached)"
+                       : st == kStNonFinite ? "non-finite value in a BPP solve"
+                       : st == kStSingular  ? "singular normal-equation matrix"
+                       : st == kStTimeout   ? "bounded device wait timed out"
+                                            : "device status error";
+    fail(st, what);
+  }
+}
+
+void reset_graph(planc_gpu_ctx* c) {
+  if (c->gexec) {
+    cudaGraphExecDestroy(c->gexec);
+    c->gexec = nullptr;
+  }
+  c->g_algo = c->g_dimtree = c->g_err = -1;
+}
+
+void free_all(planc_gpu_ctx* c) {
+  reset_graph(c);
+  auto f = [](auto*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+  };
+  f(c->X64);
+  tc_free(c->tct);
+  f(c->normX2);
+  for (int n = 0; n < kMaxModes; ++n) {
+    f(c->F[n]);
+    f(c->M[n]);
+    c->factor_cap[n] = 0;
+  }
+  f(c->Gall);
+  f(c->Gloo);
+  f(c->lambda);
+  f(c->P);
+  f(c->P32);
+  f(c->Q);
+  f(c->scratch);
+  c->scratch_elems = 0;
+  f(c->errs_dev);
+  c->errs_cap = 0;
+  f(c->counter_dev);
+  f(c->status_dev);
+}
+
+}  // namespace
+
+// ===================================================================== ABI
+extern "C" {
+
+int planc_gpu_abi_version(void) { return PLANC_GPU_ABI_VERSION; }
+
+const char* planc_gpu_last_error(void) { return g_last_error.c_str(); }
+
+int planc_gpu_create(planc_gpu_ctx** out, int device, int precision, void* cuda_stream) {
+  return guarded([&] {
+    if (!out) fail(PLANC_GPU_ERR_ARG, "out is null");
+    *out = nullptr;
+    if (precision < PLANC_GPU_PREC_FP64 || precision > PLANC_GPU_PREC_BF16X2)
+      fail(PLANC_GPU_ERR_ARG, "unknown precision " + std::to_string(precision));
+    int ndev = 0;
+    CK(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) fail(PLANC_GPU_ERR_ARG, "bad device index");
+    CK(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, device));
+    if (precision != PLANC_GPU_PREC_FP64 && prop.major < 10)
+      fail(PLANC_GPU_ERR_UNSUPPORTED, "tensor-core precisions need an sm_100 device");
+    planc_gpu_ctx* c = new planc_gpu_ctx();
+    c->device = device;
+    c->precision = precision;
+    c->sm_count = prop.multiProcessorCount;
+    if (cuda_stream) {
+      c->stream = (cudaStream_t)cuda_stream;
+    } else {
+      cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+      if (e != cudaSuccess) {
+        delete c;
+        cuda_check(e, "cudaStreamCreateWithFlags");
+      }
+      c->own_stream = true;
+    }
+    try {
+      CK(cudaMalloc(&c->normX2, sizeof(double)));
+      CK(cudaMalloc(&c->counter_dev, sizeof(int)));
+      CK(cudaMalloc(&c->status_dev, sizeof(int)));
+      CK(cudaMemsetAsync(c->status_dev, 0, sizeof(int), c->stream));
+    } catch (...) {
+      free_all(c);
+      if (c->own_stream) cudaStreamDestroy(c->stream);
+      delete c;
+      throw;
+    }
+    *out = c;
+  });
+}
+
+int planc_gpu_destroy(planc_gpu_ctx* c) {
+  if (!c) return PLANC_GPU_OK;
+  return guarded([&] {
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    for (auto& p : c->pending) {
+      cudaEventDestroy(p.a);
+      cudaEventDestroy(p.b);
+    }
+    for (auto e : c->ev_pool) cudaEventDestroy(e);
+    free_all(c);
+    if (c->own_stream) cudaStreamDestroy(c->stream);
+    delete c;
+  });
+}
+
+void* planc_gpu_stream(planc_gpu_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+int planc_gpu_set_tensor(planc_gpu_ctx* c, const void* X, int dtype, const int64_t* dims,
+                         int nmodes, int x_on_device) {
+  return guarded([&] {
+    if (!c || !X || !dims) fail(PLANC_GPU_ERR_ARG, "null argument");
+    if (nmodes < 2 || nmodes > kMaxModes)
+      fail(PLANC_GPU_ERR_ARG, "nmodes must be in [2, " + std::to_string(kMaxModes) + "]");
+    if (dtype != PLANC_GPU_F64 && dtype != PLANC_GPU_F32) fail(PLANC_GPU_ERR_ARG, "bad dtype");
+    int64_t numel = 1;
+    for (int i = 0; i < nmodes; ++i) {
+      if (dims[i] < 1) fail(PLANC_GPU_ERR_ARG, "every mode size must be >= 1");
+      numel *= dims[i];
+    }
+    set_device(c);
+    reset_graph(c);
+    // drop everything shaped by the previous tensor
+    bool same = c->have_tensor && c->N == nmodes;
+    for (int i = 0; same && i < nmodes; ++i) same = c->dims[i] == dims[i];
+    if (!same) {
+      c->have_factors = false;
+      auto f = [](auto*& p) {
+        if (p) cudaFree(p);
+        p = nullptr;
+      };
+      f(c->P);
+      f(c->P32);
+      f(c->Q);
+    }
+    c->N = nmodes;
+    for (int i = 0; i < nmodes; ++i) c->dims[i] = dims[i];
+    c->numel = numel;
+    c->s = nmodes / 2;  // ntf/auntf.hpp:122-123
+    c->L = 1;
+    c->R = 1;
+    for (int i = 0; i < nmodes; ++i) (i <= c->s ? c->L : c->R) *= dims[i];
+    size_t esz = dtype == PLANC_GPU_F64 ? 8 : 4;
+    const void* src = X;
+    void* staged = nullptr;
+    if (!x_on_device) {
+      CK(cudaMalloc(&staged, numel * esz));
+      cudaError_t e = cudaMemcpyAsync(staged, X, numel * esz, cudaMemcpyHostToDevice, c->stream);
+      if (e != cudaSuccess) {
+        cudaFree(staged);
+        cuda_check(e, "upload tensor");
+      }
+      src = staged;
+    }
+    try {
+      // ||X||^2 in FP64 from the values given
+      const int nb = 1184;
+      double* part = nullptr;
+      CK(cudaMalloc(&part, nb * sizeof(double)));
+      if (dtype == PLANC_GPU_F64)
+        k_sumsq_partial<double><<<nb, 256, 0, c->stream>>>((const double*)src, numel, part);
+      else
+        k_sumsq_partial<float><<<nb, 256, 0, c->stream>>>((const float*)src, numel, part);
+      k_reduce_splits<<<1, 32, 0, c->stream>>>(part, nb, 1, 1, c->normX2);
+      CK(cudaGetLastError());
+      if (c->precision == PLANC_GPU_PREC_FP64) {
+        dalloc(&c->X64, (size_t)numel);
+        if (dtype == PLANC_GPU_F64)
+          CK(cudaMemcpyAsync(c->X64, src, numel * 8, cudaMemcpyDeviceToDevice, c->stream));
+        else
+          k_copy_to_f64<float><<<4096, 256, 0, c->stream>>>((const float*)src, numel, c->X64);
+      } else {
+        if (c->X64) {
+          cudaFree(c->X64);
+          c->X64 = nullptr;
+        }
+        tc_set_tensor(c->tct, src, dtype == PLANC_GPU_F64, c->L, c->R, c->precision, c->stream);
+      }
+      CK(cudaGetLastError());
+      CK(cudaStreamSynchronize(c->stream));
+      cudaFree(part);
+    } catch (...) {
+      if (staged) cudaFree(staged);
+      throw;
+    }
+    if (staged) cudaFree(staged);
+    c->have_tensor = true;
+  });
+}
+
+int planc_gpu_set_factors(planc_gpu_ctx* c, const double* const* F, const double* lambda, int k) {
+  return guarded([&] {
+    if (!c || !F) fail(PLANC_GPU_ERR_ARG, "null argument");
+    if (!c->have_tensor) fail(PLANC_GPU_ERR_STATE, "set the tensor before the factors");
+    if (k < 1 || k > kMaxRank)
+      fail(PLANC_GPU_ERR_UNSUPPORTED, "rank must be in [1, " + std::to_string(kMaxRank) + "]");
+    if (c->precision != PLANC_GPU_PREC_FP64 && (c->N != 3 && c->N != 4))
+      fail(PLANC_GPU_ERR_UNSUPPORTED, "tensor-core precisions run the dimension tree (N in {3,4})");
+    set_device(c);
+    reset_graph(c);
+    if (k != c->k) {
+      auto f = [](auto*& p) {
+        if (p) cudaFree(p);
+        p = nullptr;
+      };
+      f(c->P);
+      f(c->P32);
+      f(c->Q);
+      for (int n = 0; n < kMaxModes; ++n) c->factor_cap[n] = 0;
+    }
+    c->k = k;
+    for (int n = 0; n < c->N; ++n) {
+      if (!F[n]) fail(PLANC_GPU_ERR_ARG, "null factor");
+      size_t need = (size_t)c->dims[n] * k;
+      if (c->factor_cap[n] != (int64_t)need) {
+        dalloc(&c->F[n], need);
+        dalloc(&c->M[n], need);
+        c->factor_cap[n] = (int64_t)need;
+      }
+      CK(cudaMemcpyAsync(c->F[n], F[n], need * 8, cudaMemcpyHostToDevice, c->stream));
+    }
+    dalloc(&c->Gall, (size_t)c->N * k * k);
+    dalloc(&c->Gloo, (size_t)k * k);
+    dalloc(&c->lambda, (size_t)k);
+    // AUNTF::reset: update_factor_mode on every mode (normalise, Gram), then
+    // set_lambda(new lambda)
+    for (int n = 0; n < c->N; ++n) normalize_gram(c, n, n == c->N - 1 ? 0 : -1, c->lambda);
+    std::vector<double> lam(k, 1.0);
+    if (lambda) std::copy(lambda, lambda + k, lam.begin());
+    CK(cudaMemcpyAsync(c->lambda, lam.data(), k * 8, cudaMemcpyHostToDevice, c->stream));
+    ensure_buffers(c);
+    CK(cudaStreamSynchronize(c->stream));
+    c->have_factors = true;
+  });
+}
+
+int planc_gpu_run(planc_gpu_ctx* c, int algo, int iters, int dimtree, int compute_error,
+                  double* errs_out) {
+  return guarded([&] {
+    require_ready(c);
+    if (iters < 0) fail(PLANC_GPU_ERR_ARG, "iters < 0");
+    if (algo != PLANC_GPU_MU && algo != PLANC_GPU_HALS && algo != PLANC_GPU_ANLSBPP)
+      fail(PLANC_GPU_ERR_ARG, "unknown algorithm " + std::to_string(algo));
+    bool dt = dimtree && (c->N == 3 || c->N == 4);
+    if (c->precision != PLANC_GPU_PREC_FP64 && !dt)
+      fail(PLANC_GPU_ERR_UNSUPPORTED, "tensor-core precisions run the dimension tree only");
+    if (iters == 0) return;
+    set_device(c);
+    ensure_buffers(c);
+    if (compute_error && iters > c->errs_cap) {
+      dalloc(&c->errs_dev, (size_t)iters);
+      c->errs_cap = iters;
+    }
+    if (!c->errs_dev) {
+      dalloc(&c->errs_dev, 1);
+      c->errs_cap = 1;
+    }
+    CK(cudaMemsetAsync(c->counter_dev, 0, sizeof(int), c->stream));
+    gram_loo(c, 0);
+    bool use_graph = !c->timing;
+    if (use_graph) {
+      if (!c->gexec || c->g_algo != algo || c->g_dimtree != (int)dt || c->g_err != compute_error) {
+        reset_graph(c);
+        cudaGraph_t graph;
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        c->capturing = true;
+        try {
+          one_iteration(c, algo, dt, compute_error != 0);
+        } catch (...) {
+          c->capturing = false;
+          cudaStreamEndCapture(c->stream, &graph);
+          if (graph) cudaGraphDestroy(graph);
+          throw;
+        }
+        c->capturing = false;
+        CK(cudaStreamEndCapture(c->stream, &graph));
+        cudaError_t e = cudaGraphInstantiate(&c->gexec, graph, 0);
+        cudaGraphDestroy(graph);
+        cuda_check(e, "cudaGraphInstantiate");
+        c->g_algo = algo;
+        c->g_dimtree = (int)dt;
+        c->g_err = compute_error;
+      }
+      for (int it = 0; it < iters; ++it) CK(cudaGraphLaunch(c->gexec, c->stream));
+    } else {
+      for (int it = 0; it < iters; ++it) one_iteration(c, algo, dt, compute_error != 0);
+    }
+    if (compute_error && errs_out)
+      CK(cudaMemcpyAsync(errs_out, c->errs_dev, iters * sizeof(double), cudaMemcpyDeviceToHost,
+                         c->stream));
+    check_status(c);
+    drain_timing(c);
+  });
+}
+
+int planc_gpu_get_factors(planc_gpu_ctx* c, double* const* F, double* lambda) {
+  return guarded([&] {
+    require_ready(c);
+    set_device(c);
+    if (F)
+      for (int n = 0; n < c->N; ++n)
+        if (F[n])
+          CK(cudaMemcpyAsync(F[n], c->F[n], (size_t)c->dims[n] * c->k * 8, cudaMemcpyDeviceToHost,
+                             c->stream));
+    if (lambda)
+      CK(cudaMemcpyAsync(lambda, c->lambda, c->k * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int planc_gpu_mttkrp(planc_gpu_ctx* c, int mode, int dimtree, double* out) {
+  return guarded([&] {
+    require_ready(c);
+    if (mode < 0 || mode >= c->N || !out) fail(PLANC_GPU_ERR_ARG, "bad mode or null output");
+    set_device(c);
+    ensure_buffers(c);
+    bool dt = dimtree && (c->N == 3 || c->N == 4);
+    if (c->precision != PLANC_GPU_PREC_FP64 && !dt)
+      fail(PLANC_GPU_ERR_UNSUPPORTED, "tensor-core precisions run the dimension tree only");
+    if (dt) {
+      // the tree state for `mode` comes from the current factors
+      if (mode >= 1) mttkrp_dimtree(c, 0, c->M[0]);
+      if (c->N == 4 && mode == 2) mttkrp_dimtree(c, 1, c->M[1]);
+      mttkrp_dimtree(c, mode, c->M[mode]);
+    } else {
+      mttkrp_direct(c, mode, c->M[mode]);
+    }
+    CK(cudaMemcpyAsync(out, c->M[mode], (size_t)c->dims[mode] * c->k * 8, cudaMemcpyDeviceToHost,
+                       c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    drain_timing(c);
+  });
+}
+
+int planc_gpu_gram_loo(planc_gpu_ctx* c, int mode, double* out) {
+  return guarded([&] {
+    require_ready(c);
+    if (mode < 0 || mode >= c->N || !out) fail(PLANC_GPU_ERR_ARG, "bad mode or null output");
+    set_device(c);
+    gram_loo(c, mode);
+    CK(cudaMemcpyAsync(out, c->Gloo, (size_t)c->k * c->k * 8, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int planc_gpu_objective_error(planc_gpu_ctx* c, double* err) {
+  return guarded([&] {
+    require_ready(c);
+    if (!err) fail(PLANC_GPU_ERR_ARG, "null output");
+    set_device(c);
+    ensure_buffers(c);
+    if (!c->errs_dev) {
+      dalloc(&c->errs_dev, 1);
+      c->errs_cap = 1;
+    }
+    const int last = c->N - 1;
+    // <X, model> needs the MTTKRP of the last mode from the current factors
+    if (c->precision == PLANC_GPU_PREC_FP64 || c->N == 3 || c->N == 4) {
+      if (c->precision == PLANC_GPU_PREC_FP64)
+        mttkrp_direct(c, last, c->M[last]);
+      else
+        partial_left(c, c->M[last]);
+    }
+    CK(cudaMemsetAsync(c->counter_dev, 0, sizeof(int), c->stream));
+    error_kernel(c);
+    CK(cudaMemcpyAsync(err, c->errs_dev, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    drain_timing(c);
+  });
+}
+
+int planc_gpu_mode_begin(planc_gpu_ctx* c, int mode, int dimtree, double* gram_out,
+                         double* mttkrp_out) {
+  return guarded([&] {
+    require_ready(c);
+    if (mode < 0 || mode >= c->N) fail(PLANC_GPU_ERR_ARG, "bad mode");
+    set_device(c);
+    ensure_buffers(c);
+    bool dt = dimtree && (c->N == 3 || c->N == 4);
+    if (c->precision != PLANC_GPU_PREC_FP64 && !dt)
+      fail(PLANC_GPU_ERR_UNSUPPORTED, "tensor-core precisions run the dimension tree only");
+    gram_loo(c, mode);
+    mttkrp_any(c, mode, dt, c->M[mode]);
+    if (gram_out)
+      CK(cudaMemcpyAsync(gram_out, c->Gloo, (size_t)c->k * c->k * 8, cudaMemcpyDeviceToHost,
+                         c->stream));
+    if (mttkrp_out)
+      CK(cudaMemcpyAsync(mttkrp_out, c->M[mode], (size_t)c->dims[mode] * c->k * 8,
+                         cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int planc_gpu_mode_end(planc_gpu_ctx* c, int mode, const double* factor) {
+  return guarded([&] {
+    require_ready(c);
+    if (mode < 0 || mode >= c->N || !factor) fail(PLANC_GPU_ERR_ARG, "bad mode or null factor");
+    set_device(c);
+    reset_graph(c);
+    CK(cudaMemcpyAsync(c->F[mode], factor, (size_t)c->dims[mode] * c->k * 8,
+                       cudaMemcpyHostToDevice, c->stream));
+    normalize_gram(c, mode, (mode + 1) % c->N, c->lambda);
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int planc_gpu_bpp_solve(planc_gpu_ctx* c, const double* AtA, const double* AtB, int n,
+                        int64_t ncols, double* X, int32_t* passive, int32_t* iters) {
+  return guarded([&] {
+    if (!c || !AtA || !AtB || !X) fail(PLANC_GPU_ERR_ARG, "null argument");
+    if (n < 1 || n > kMaxRank) fail(PLANC_GPU_ERR_UNSUPPORTED, "n must be in [1, 64]");
+    if (ncols < 0) fail(PLANC_GPU_ERR_ARG, "ncols < 0");
+    if (ncols == 0) return;
+    set_device(c);
+    double *dA = nullptr, *dB = nullptr, *dX = nullptr;
+    int *dP = nullptr, *dI = nullptr;
+    auto cleanup = [&] {
+      cudaFree(dA);
+      cudaFree(dB);
+      cudaFree(dX);
+      cudaFree(dP);
+      cudaFree(dI);
+    };
+    try {
+      CK(cudaMalloc(&dA, (size_t)n * n * 8));
+      CK(cudaMalloc(&dB, (size_t)n * ncols * 8));
+      CK(cudaMalloc(&dX, (size_t)n * ncols * 8));
+      CK(cudaMalloc(&dP, (size_t)n * ncols * 4));
+      CK(cudaMalloc(&dI, (size_t)ncols * 4));
+      CK(cudaMemcpyAsync(dA, AtA, (size_t)n * n * 8, cudaMemcpyHostToDevice, c->stream));
+      CK(cudaMemcpyAsync(dB, AtB, (size_t)n * ncols * 8, cudaMemcpyHostToDevice, c->stream));
+      unsigned blocks = (unsigned)((ncols + BPP_WARPS - 1) / BPP_WARPS);
+      launch(c, KC_BPP, [&] {
+        switch (kpad(n)) {
+#define CASE(KP)                                                                            \
+  case KP:                                                                                  \
+    k_bpp<KP><<<blocks, 32 * BPP_WARPS, 0, c->stream>>>(dA, dB, n, ncols, dX, dP, dI,      \
+                                                        c->status_dev);                     \
+    break;
+          CASE(8) CASE(16) CASE(32) CASE(64)
+#undef CASE
+        }
+      });
+      CK(cudaMemcpyAsync(X, dX, (size_t)n * ncols * 8, cudaMemcpyDeviceToHost, c->stream));
+      if (passive)
+        CK(cudaMemcpyAsync(passive, dP, (size_t)n * ncols * 4, cudaMemcpyDeviceToHost, c->stream));
+      if (iters) CK(cudaMemcpyAsync(iters, dI, (size_t)ncols * 4, cudaMemcpyDeviceToHost, c->stream));
+      check_status(c);
+      drain_timing(c);
+    } catch (...) {
+      cleanup();
+      throw;
+    }
+    cleanup();
+  });
+}
+
+int planc_gpu_set_timing(planc_gpu_ctx* c, int enable) {
+  return guarded([&] {
+    if (!c) fail(PLANC_GPU_ERR_ARG, "null context");
+    set_device(c);
+    drain_timing(c);
+    c->timing = enable != 0;
+  });
+}
+
+int planc_gpu_get_kernel_times(planc_gpu_ctx* c, double* ms, int64_t* launches, int n) {
+  return guarded([&] {
+    if (!c) fail(PLANC_GPU_ERR_ARG, "null context");
+    set_device(c);
+    drain_timing(c);
+    for (int i = 0; i < n && i < KC_COUNT; ++i) {
+      if (ms) ms[i] = c->kms[i];
+      if (launches) launches[i] = c->klaunch[i];
+    }
+    for (int i = 0; i < KC_COUNT; ++i) {
+      c->kms[i] = 0;
+      c->klaunch[i] = 0;
+    }
+  });
+}
+
+int64_t planc_gpu_launch_count(planc_gpu_ctx* c) { return c ? c->launch_count : -1; }
+
+int planc_gpu_synth_cp_tensor(int device, void* X_dev, int dtype, const int64_t* dims, int nmodes,
+                              const double* const* A, int k, double sigma, uint64_t seed, int clip,
+                              void* cuda_stream) {
+  return guarded([&] {
+    if (!X_dev || !dims || !A) fail(PLANC_GPU_ERR_ARG, "null argument");
+    if (nmodes < 1 || nmodes > kMaxModes || k < 1) fail(PLANC_GPU_ERR_ARG, "bad shape");
+    if (dtype != PLANC_GPU_F64 && dtype != PLANC_GPU_F32) fail(PLANC_GPU_ERR_ARG, "bad dtype");
+    CK(cudaSetDevice(device));
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    SynthDesc d;
+    memset(&d, 0, sizeof(d));
+    d.N = nmodes;
+    d.k = k;
+    d.sigma = sigma;
+    d.seed = seed;
+    d.clip = clip;
+    int64_t numel = 1;
+    std::vector<double*> bufs;
+    try {
+      for (int m = 0; m < nmodes; ++m) {
+        d.dims[m] = dims[m];
+        numel *= dims[m];
+        double* p = nullptr;
+        CK(cudaMalloc(&p, (size_t)dims[m] * k * 8));
+        bufs.push_back(p);
+        CK(cudaMemcpyAsync(p, A[m], (size_t)dims[m] * k * 8, cudaMemcpyHostToDevice, st));
+        d.A[m] = p;
+      }
+      if (dtype == PLANC_GPU_F32)
+        k_synth_cp<float><<<8192, 256, 0, st>>>(d, numel, (float*)X_dev);
+      else
+        k_synth_cp<double><<<8192, 256, 0, st>>>(d, numel, (double*)X_dev);
+      CK(cudaGetLastError());
+      CK(cudaStreamSynchronize(st));
+    } catch (...) {
+      for (auto p : bufs) cudaFree(p);
+      throw;
+    }
+    for (auto p : bufs) cudaFree(p);
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,169 @@
+"""GPU parity of the FP64 plain path against the CPU oracle, through the C ABI.
+
+Tolerance: the north-star bar for FP64, 1e-10 relative (max-abs error over
+max-abs value) for factors, MTTKRPs, Grams and relative errors."""
+import numpy as np
+import pytest
+
+from helpers import cp_tensor, einsum_mttkrp, init_factors, rel
+
+pytestmark = pytest.mark.gpu
+TOL = 1e-10
+
+
+def _ctx(gpu, X, F, prec="fp64"):
+    c = gpu.Context(0, prec)
+    c.set_tensor(X)
+    c.set_factors(F)
+    return c
+
+
+def _normalized(F):
+    return [f / np.linalg.norm(f, axis=0) for f in F]
+
+
+@pytest.mark.parametrize("dims,k", [((64, 64, 64), 8), ((17, 23, 9), 5), ((12, 10, 8, 6), 12),
+                                    ((40, 33, 21), 32), ((9, 8, 7, 10), 64), ((30, 20, 10), 1)])
+def test_mttkrp_and_gram(gpu, oracle_lib, dims, k):
+    X, _ = cp_tensor(dims, 3, seed=1)
+    F = init_factors(dims, k, seed=2)
+    with _ctx(gpu, X, F) as c:
+        Fn = _normalized(F)  # set_factors normalises like AUNTF::reset
+        for n in range(len(dims)):
+            ref = oracle_lib.mttkrp_direct(X, Fn, n)
+            assert rel(c.mttkrp(n, dimtree=False), ref) < TOL
+            if len(dims) in (3, 4):
+                assert rel(c.mttkrp(n, dimtree=True), ref) < TOL
+            assert rel(c.gram_loo(n), oracle_lib.gram_loo(Fn, n)) < TOL
+
+
+def test_direct_mttkrp_five_modes(gpu, oracle_lib):
+    dims, k = (5, 4, 6, 3, 4), 6
+    X, _ = cp_tensor(dims, 2, seed=3)
+    F = init_factors(dims, k, seed=4)
+    with _ctx(gpu, X, F) as c:
+        Fn = _normalized(F)
+        for n in range(5):
+            assert rel(c.mttkrp(n, dimtree=False), einsum_mttkrp(X, Fn, n)) < TOL
+
+
+@pytest.mark.parametrize("algo", ["hals", "mu", "anlsbpp"])
+@pytest.mark.parametrize("dims,k,iters", [((64, 64, 64), 8, 20), ((20, 31, 17, 9), 6, 6)])
+def test_ntf_run_matches_oracle(gpu, oracle_lib, algo, dims, k, iters):
+    X, _ = cp_tensor(dims, k, noise=0.01, seed=7)
+    F0 = init_factors(dims, k, seed=8)
+    Fo, lamo, eo = oracle_lib.ntf_run(X, F0, algo, iters, dimtree=True)
+    for dimtree in (True, False):
+        with _ctx(gpu, X, F0) as c:
+            e = c.run(algo, iters, dimtree=dimtree, compute_error=True)
+            F, lam = c.get_factors()
+        assert rel(e, eo) < TOL, (e, eo)
+        for a, b in zip(F, Fo):
+            assert rel(a, b) < TOL
+        assert rel(lam, lamo) < TOL
+
+
+def test_run_in_pieces_equals_one_run(gpu, oracle_lib):
+    X, _ = cp_tensor((30, 25, 20), 5, seed=9)
+    F0 = init_factors(X.shape, 5, seed=10)
+    with _ctx(gpu, X, F0) as c:
+        e1 = np.concatenate([c.run("hals", 3), c.run("hals", 4)])
+        F1, _ = c.get_factors()
+    with _ctx(gpu, X, F0) as c:
+        e2 = c.run("hals", 7)
+        F2, _ = c.get_factors()
+    assert rel(e1, e2) < 1e-14
+    assert all(rel(a, b) < 1e-14 for a, b in zip(F1, F2))
+
+
+def test_objective_error_matches_explicit(gpu, oracle_lib):
+    X, _ = cp_tensor((25, 20, 15), 4, seed=11)
+    F0 = init_factors(X.shape, 4, seed=12)
+    Fo, lamo, eo = oracle_lib.ntf_run(X, F0, "hals", 3)
+    with _ctx(gpu, X, F0) as c:
+        c.run("hals", 3, compute_error=False)
+        err = c.objective_error()
+    assert abs(err - eo[-1]) / eo[-1] < TOL
+
+
+def test_host_update_extension_point(gpu, oracle_lib):
+    # A host-side update (the reference's virtual AUNTF::update) driven by
+    # mode_begin / mode_end reproduces the oracle's HALS iteration.
+    X, _ = cp_tensor((16, 14, 12), 4, seed=13)
+    F0 = init_factors(X.shape, 4, seed=14)
+    Fo, lamo, eo = oracle_lib.ntf_run(X, F0, "hals", 2)
+    with _ctx(gpu, X, F0) as c:
+        F, _ = c.get_factors()
+        for it in range(2):
+            for n in range(3):
+                G, M = c.mode_begin(n)
+                H = oracle_lib.hals_update(F[n], M, G)
+                c.mode_end(n, H)
+                F, _ = c.get_factors()
+        err = c.objective_error()
+        F, lam = c.get_factors()
+    assert all(rel(a, b) < TOL for a, b in zip(F, Fo))
+    assert abs(err - eo[-1]) / eo[-1] < TOL
+
+
+@pytest.mark.parametrize("n", [3, 8, 17, 40, 64])
+def test_bpp_solve_masks_and_values(gpu, oracle_lib, n):
+    rng = np.random.default_rng(100 + n)
+    A = rng.random((2 * n, n))
+    A[:, rng.random(n) < 0.3] *= 0.1
+    AtA = A.T @ A
+    B = rng.standard_normal((n, 300)) + 0.2
+    Xo, Po, ito = oracle_lib.bpp_update(B.T.copy(), AtA)
+    with gpu.Context(0, "fp64") as c:
+        Xg, Pg, itg = c.bpp_solve(AtA, B)
+    assert rel(Xg.T, Xo) < 1e-9
+    assert np.array_equal(Pg.T, Po)
+    assert itg.max() <= 5 * n
+
+
+def test_bpp_singular_normal_equations_reports_status(gpu):
+    # AtA with a zero row/column at an index that enters the passive set:
+    # the solve has no pivot; the call returns ERR_SINGULAR and the context
+    # stays usable.
+    n = 4
+    AtA = np.eye(n)
+    AtA[2, 2] = 0.0
+    B = np.ones((n, 3))
+    with gpu.Context(0, "fp64") as c:
+        with pytest.raises(gpu.PlancGpuError) as ei:
+            c.bpp_solve(AtA, B)
+        assert ei.value.code == -9
+        X, P, it = c.bpp_solve(np.eye(n), B)
+        assert np.allclose(X, 1.0)
+
+
+def test_argument_errors(gpu):
+    X, _ = cp_tensor((8, 8, 8), 2, seed=1)
+    with gpu.Context(0, "fp64") as c:
+        with pytest.raises(gpu.PlancGpuError) as ei:
+            c.run("hals", 1)
+        assert ei.value.code == -3  # no tensor yet
+        c.set_tensor(X)
+        with pytest.raises(gpu.PlancGpuError) as ei:
+            c.set_factors(init_factors(X.shape, 65))
+        assert ei.value.code == -7
+        c.set_factors(init_factors(X.shape, 4))
+        with pytest.raises(gpu.PlancGpuError):
+            c.mttkrp(3)
+        with pytest.raises(gpu.PlancGpuError):
+            c.run(7, 1)
+        c.run("hals", 1)
+
+
+def test_synth_generator_matches_model(gpu):
+    import torch
+    dims, k = (20, 16, 12), 3
+    A = init_factors(dims, k, seed=5)
+    x = torch.empty(int(np.prod(dims)), dtype=torch.float64, device="cuda")
+    gpu.synth_cp_tensor(0, x.data_ptr(), "f64", dims, A, 0.0, 1, clip=False)
+    M = np.einsum("az,bz,cz->abc", *A).ravel(order="F")
+    assert rel(x.cpu().numpy(), M) < 1e-14
+    y = torch.empty_like(x)
+    gpu.synth_cp_tensor(0, y.data_ptr(), "f64", dims, A, 0.5, 42, clip=False)
+    z = (y - x).cpu().numpy() / 0.5
+    assert abs(z.mean()) < 0.05 and abs(z.std() - 1) < 0.05

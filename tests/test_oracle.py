@@ -1,0 +1,133 @@
+"""CPU tests of the oracle: pinned against the reference's own compiled
+dimension-tree kernels (golden fixtures, and live when oracle/_ref is built),
+an independent mt19937 computation, and known-answer identities."""
+import itertools
+import os
+
+import numpy as np
+import pytest
+
+from helpers import cp_tensor, einsum_mttkrp, init_factors, rel
+
+GOLD = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def test_tensor_randu_matches_mt19937_pin(oracle_lib):
+    # Tensor(dims) data (common/tensor.hpp:86-93, 219-235) vs an independent
+    # numpy computation of std::mt19937(103) + uniform_real_distribution.
+    gold = np.load(os.path.join(GOLD, "mt19937_103.npz"))["values"]
+    x = oracle_lib.tensor_randu((16, 16, 16), 103).ravel(order="F")
+    assert np.array_equal(x, gold)
+
+
+@pytest.mark.parametrize("case", ["n3", "n4", "n3b"])
+def test_oracle_mttkrp_matches_reference_golden(oracle_lib, case):
+    g = np.load(os.path.join(GOLD, "ref_dimtree_mttkrp.npz"))
+    dims = tuple(int(d) for d in g[case + "_dims"])
+    X = g[case + "_X"].reshape(dims, order="F")
+    F = [g["%s_F%d" % (case, i)] for i in range(len(dims))]
+    dt = oracle_lib.mttkrp_dimtree_all(X, F)
+    for n in range(len(dims)):
+        ref = g["%s_M%d" % (case, n)]
+        assert rel(oracle_lib.mttkrp_direct(X, F, n), ref) < 1e-13
+        assert rel(dt[n], ref) < 1e-13
+
+
+@pytest.mark.skipif(not __import__("oracle").ref_available(), reason="reference build absent")
+@pytest.mark.parametrize("dims,k", [((7, 6, 5), 4), ((4, 5, 6, 3), 5), ((3, 9, 2), 7)])
+def test_oracle_mttkrp_matches_reference_live(oracle_lib, dims, k):
+    X = oracle_lib.tensor_randu(dims, 103)
+    F = init_factors(dims, k, seed=5)
+    ref = oracle_lib.ref_mttkrp_dimtree_all(X, F)
+    dt = oracle_lib.mttkrp_dimtree_all(X, F)
+    for n in range(len(dims)):
+        assert rel(dt[n], ref[n]) < 1e-13
+        assert rel(oracle_lib.mttkrp_direct(X, F, n), ref[n]) < 1e-13
+
+
+@pytest.mark.parametrize("dims", [(5, 6, 7), (3, 4, 5, 6), (2, 3, 4, 2, 3)])
+def test_mttkrp_known_answer_exact_cp(oracle_lib, dims):
+    # X = [[A_0..A_{N-1}]] exactly => MTTKRP_n = A_n (*_{m!=n} A_m^T A_m)
+    k = 3
+    A = init_factors(dims, k, seed=11)
+    letters = "abcdefgh"[:len(dims)]
+    X = np.asfortranarray(np.einsum(",".join(c + "z" for c in letters) + "->" + letters, *A))
+    for n in range(len(dims)):
+        H = np.ones((k, k))
+        for m in range(len(dims)):
+            if m != n:
+                H *= A[m].T @ A[m]
+        assert rel(oracle_lib.mttkrp_direct(X, A, n), A[n] @ H) < 1e-12
+        assert rel(oracle_lib.gram_loo(A, n), H) < 1e-13
+
+
+def test_krp_order_matches_einsum(oracle_lib):
+    dims = (3, 4, 5)
+    F = init_factors(dims, 2, seed=3)
+    X = oracle_lib.tensor_randu(dims, 7)
+    for n in range(3):
+        assert rel(oracle_lib.mttkrp_direct(X, F, n), einsum_mttkrp(X, F, n)) < 1e-13
+
+
+@pytest.mark.parametrize("algo", ["hals", "mu"])
+def test_update_fixed_point_at_exact_factors(oracle_lib, algo):
+    # At the exact (normalised) factors of a noise-free CP tensor, the HALS and
+    # MU updates leave the factors unchanged (up to MU's 1e-6 regulariser).
+    dims, k = (6, 5, 7), 3
+    A = init_factors(dims, k, seed=4)
+    lam = np.ones(k)
+    An = []
+    for a in A:
+        nrm = np.linalg.norm(a, axis=0)
+        An.append(a / nrm)
+        lam *= nrm
+    An[0] = An[0] * lam  # fold lambda into mode 0 (the updated mode)
+    letters = "abc"
+    X = np.asfortranarray(np.einsum("az,bz,cz->abc", *An))
+    M = oracle_lib.mttkrp_direct(X, An, 0)
+    G = oracle_lib.gram_loo(An, 0)
+    upd = oracle_lib.hals_update(An[0], M, G) if algo == "hals" else oracle_lib.mu_update(An[0], M, G)
+    assert rel(upd, An[0]) < (1e-12 if algo == "hals" else 1e-4)
+
+
+def _nnls_exhaustive(AtA, b):
+    """min 0.5 x'AtA x - b'x s.t. x >= 0 by enumerating passive sets."""
+    n = len(b)
+    best, bestx = np.inf, None
+    for mask in itertools.product([0, 1], repeat=n):
+        idx = [i for i in range(n) if mask[i]]
+        x = np.zeros(n)
+        if idx:
+            x[idx] = np.linalg.solve(AtA[np.ix_(idx, idx)], b[idx])
+            if (x[idx] < 0).any():
+                continue
+        f = 0.5 * x @ AtA @ x - b @ x
+        if f < best - 1e-14:
+            best, bestx = f, x
+    return bestx
+
+
+@pytest.mark.parametrize("n", [2, 5, 8])
+def test_bpp_matches_exhaustive_active_set(oracle_lib, n):
+    rng = np.random.default_rng(n)
+    A = rng.random((3 * n, n))
+    AtA = A.T @ A
+    B = rng.standard_normal((n, 40)) * 2 + 0.3
+    X, mask, it = oracle_lib.bpp_update(B.T.copy(), AtA)
+    assert it >= 0
+    for c in range(B.shape[1]):
+        x_ex = _nnls_exhaustive(AtA, B[:, c])
+        assert np.allclose(X[c], x_ex, atol=1e-10, rtol=1e-9)
+        assert np.array_equal(mask[c].astype(bool), X[c] > 0)
+
+
+def test_ntf_error_decreases_and_dimtree_equals_direct(oracle_lib):
+    X, _ = cp_tensor((20, 18, 16), 4, noise=0.01, seed=2)
+    F0 = init_factors(X.shape, 4, seed=3)
+    for algo in ["hals", "mu", "anlsbpp"]:
+        F, lam, e = oracle_lib.ntf_run(X, F0, algo, 8, dimtree=True)
+        F2, lam2, e2 = oracle_lib.ntf_run(X, F0, algo, 8, dimtree=False)
+        assert e[-1] < e[0]
+        assert np.allclose(e, e2, rtol=1e-12, atol=0)
+        for a, b in zip(F, F2):
+            assert rel(a, b) < 1e-11
