@@ -16,7 +16,7 @@ constexpr double kEps12 = 1e-12;                 // EPSILON_1EMINUS12
 
 // Kernel classes for the optional event timing (planc_gpu_set_timing).
 enum KClass { KC_CONTRACT = 0, KC_TTV = 1, KC_UPDATE = 2, KC_NORMGRAM = 3,
-              KC_ERROR = 4, KC_REDUCE = 5, KC_BPP = 6, KC_COUNT = 7 };
+              KC_ERROR = 4, KC_REDUCE = 5, KC_BPP = 6, KC_PREP = 7, KC_COUNT = 8 };
 
 // Device status codes written by kernels (match planc_gpu.h).
 constexpr int kStBppMaxIter = -4;

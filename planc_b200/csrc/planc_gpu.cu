@@ -263,6 +263,7 @@ void ensure_buffers(planc_gpu_ctx* c) {
       need = std::max(need, (size_t)t2.nsplit * c->dims[1] * k);
     }
     need = std::max(need, tc_scratch_elems(c->tct, c->sm_count, k));
+    CK(tc_ensure(c->tct, k));
   }
   for (int n = 0; n < c->N; ++n) {
     int64_t A, B;
@@ -365,7 +366,10 @@ void partial_right(planc_gpu_ctx* c) {
     ContractPlan p = plan_contract(c, false, c->L, c->L, c->R, 1, 0);
     run_contract(c, p, false, c->X64, wg, c->P);
   } else {
-    launch(c, KC_CONTRACT, [&] { tc_right(c->tct, c->F[c->N - 1], c->k, c->P32, c->stream); });
+    launch(c, KC_PREP, [&] { tc_right_prep(c->tct, c->F[c->N - 1], c->k, c->stream); });
+    launch(c, KC_CONTRACT, [&] {
+      tc_right(c->tct, c->k, c->P32, c->status_dev, c->sm_count, c->stream);
+    });
   }
 }
 
@@ -381,7 +385,7 @@ void partial_left(planc_gpu_ctx* c, double* out) {
     WGen wg = make_wgen(c, modes);
     int nsplit = 0;
     launch(c, KC_CONTRACT, [&] {
-      nsplit = tc_left(c->tct, wg, c->k, c->scratch, c->sm_count, c->stream);
+      nsplit = tc_left(c->tct, wg, c->k, c->scratch, c->status_dev, c->sm_count, c->stream);
     });
     int64_t n = c->R * c->k;
     launch(c, KC_REDUCE, [&] {
@@ -703,7 +707,11 @@ int planc_gpu_set_tensor(planc_gpu_ctx* c, const void* X, int dtype, const int64
           cudaFree(c->X64);
           c->X64 = nullptr;
         }
-        tc_set_tensor(c->tct, src, dtype == PLANC_GPU_F64, c->L, c->R, c->precision, c->stream);
+        cudaError_t te =
+            tc_set_tensor(c->tct, src, dtype == PLANC_GPU_F64, c->L, c->R, c->precision, c->stream);
+        if (te == cudaErrorInvalidValue)
+          fail(PLANC_GPU_ERR_CUDA, "cuTensorMapEncodeTiled rejected the tensor map");
+        CK(te);
       }
       CK(cudaGetLastError());
       CK(cudaStreamSynchronize(c->stream));

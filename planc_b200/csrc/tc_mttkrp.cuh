@@ -1,25 +1,770 @@
-// tc_mttkrp.cuh -- tensor-core (tcgen05 / TMEM / TMA) partial MTTKRP for the
-// BF16 precisions. (placeholder: filled in by the sm_100a kernels)
+// tc_mttkrp.cuh -- tensor-core partial MTTKRP for the BF16 precisions:
+// tcgen05.mma (kind::f16, BF16 inputs, FP32 accumulator in TMEM), operands
+// staged in shared memory by TMA (cp.async.bulk.tensor) and bulk copies,
+// warp-specialised persistent kernels with mbarrier pipelines.
+//
+// The tensor is held as a 2-D matrix X[l + Lpad*j] (l < L = prod_{i<=s} I_i,
+// j < R = prod_{i>s} I_i, Lpad = L rounded up to 8 so every TMA row starts on
+// a 16-byte boundary) in BF16 (PREC_BF16) or as a BF16 hi/lo pair
+// (PREC_BF16X2: x = hi + lo, each rounded to nearest).
+//
+//   right contraction (dimtree/dimtrees.hpp:106-138, P = X * F_{N-1}):
+//     A = X tile 128(l) x 64(j), MN-major (l contiguous), TMA box {64,64} x2
+//     B = F_{N-1} slab, pre-split into hi|lo BF16 rows and pre-swizzled in
+//         global memory, one bulk copy per stage (K-major, 128B swizzle)
+//     D = TMEM 128 lanes x (2*kp) columns: [X*F_hi | X*F_lo]; two
+//         accumulators double-buffered so the epilogue of tile t overlaps the
+//         MMAs of tile t+1. Epilogue: P32[l*k + r] = D[l, r] + D[l, kp + r].
+//   left contraction (dimtrees.hpp:72-105, M_{N-1} = X^T * KRP(F_0..F_s)):
+//     A = X^T tile 128(j) x 64(l), K-major, TMA box {64,128}
+//     B = Khatri-Rao rows for 64 values of l, generated in shared memory by
+//         four producer warps (FP64 product, split hi|lo), K-major 128B swizzle
+//     split-K over the CTAs; each CTA writes an FP64 partial R x k that a
+//     fixed-order reduction sums (deterministic).
+//
+// All mbarrier waits are bounded (about 2 s of clock64); a wait that runs out
+// sets *status = kStTimeout and a shared abort flag that every other wait
+// honours, then the CTA drains its in-flight copies (bounded), frees its TMEM
+// and returns.
 #pragma once
+#include <cuda.h>
+#include <cuda_bf16.h>
+
 #include "common.cuh"
 
 namespace pg {
 
+// ------------------------------------------------------------ PTX helpers
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}"
+      : "=r"(ok)
+      : "r"(bar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
+
+// Bounded wait on phase `parity`. Returns false (and raises the abort flag)
+// when the wait runs out or another warp already aborted.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag,
+                                          int* status) {
+  if (mbar_try(bar, parity)) return true;
+  long long t0 = clock64();
+  while (true) {
+    if (mbar_try(bar, parity)) return true;
+    if (*abort_flag) return false;
+    if (clock64() - t0 > kWaitCycles) {
+      *abort_flag = 1;
+      atomicMin(status, kStTimeout);
+      return false;
+    }
+    __nanosleep(64);
+  }
+}
+
+// After an abort, give every copy already issued time to land (bulk copies
+// complete in microseconds) before the CTA's shared memory is released.
+__device__ __forceinline__ void tc_drain_after_abort() {
+  long long t0 = clock64();
+  while (clock64() - t0 < 20000000LL) __nanosleep(1000);
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y,
+                                            uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(dst),
+      "l"((uint64_t)map), "r"(x), "r"(y), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes,
+                                          uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          dst),
+      "l"((uint64_t)src), "r"(bytes), "r"(bar)
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+
+// SMEM matrix descriptor (tcgen05): start, leading / stride byte offsets (all
+// >> 4), version 1, base offset 0, 128-byte swizzle.
+__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((addr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version (sm_100)
+  d |= (uint64_t)2 << 61;  // SWIZZLE_128B
+  return d;
+}
+
+// Instruction descriptor, kind::f16: BF16 A and B, FP32 D, M = 128.
+__host__ __device__ constexpr uint32_t idesc_bf16(int n, bool a_mn_major, bool b_mn_major) {
+  return (1u << 4)                          // D format F32
+         | (1u << 7)                        // A format BF16
+         | (1u << 10)                       // B format BF16
+         | ((a_mn_major ? 1u : 0u) << 15)   // A major
+         | ((b_mn_major ? 1u : 0u) << 16)   // B major
+         | ((uint32_t)(n >> 3) << 17)       // N >> 3
+         | ((uint32_t)(128 >> 4) << 24);    // M >> 4
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc,
+                                          uint32_t idesc, uint32_t accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   bar)
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]),
+        "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]),
+        "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_alloc(uint32_t dst_smem, uint32_t ncols) {
+  asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst_smem),
+               "r"(ncols)
+               : "memory");
+  asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+}
+__device__ __forceinline__ void tmem_dealloc(uint32_t taddr, uint32_t ncols) {
+  asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(taddr), "r"(ncols)
+               : "memory");
+}
+
+// Byte offset of element (row, kk) (kk < 64 BF16 values along K) inside a
+// K-major 128B-swizzled tile whose rows are 128 bytes and whose 8-row groups
+// are 1024 bytes apart.
+__host__ __device__ __forceinline__ uint32_t sw128_kmajor_off(int row, int kk) {
+  uint32_t chunk = (uint32_t)(kk >> 3);        // 16-byte chunk within the row
+  uint32_t phys = chunk ^ (uint32_t)(row & 7);  // 128B swizzle
+  return (uint32_t)(row >> 3) * 1024u + (uint32_t)(row & 7) * 128u + phys * 16u +
+         (uint32_t)(kk & 7) * 2u;
+}
+
+__device__ __forceinline__ void split_bf16(double w, __nv_bfloat16& hi, __nv_bfloat16& lo) {
+  hi = __double2bfloat16(w);
+  lo = __double2bfloat16(w - (double)__bfloat162float(hi));
+}
+
+constexpr int TC_BM = 128;   // rows per MMA tile
+constexpr int TC_BK = 64;    // K per pipeline stage (one 128-byte swizzle row of BF16)
+constexpr int TC_THREADS = 192;  // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue / KRP producers
+
+// ------------------------------------------------------------ right kernel
+// P32[l*k + r] = sum_j X[l, j] * F[j, r], l < L, r < k.
+template <int KP, bool X2>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    k_tc_right(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
+               const uint8_t* __restrict__ bimg, int64_t L, int64_t R, int k, int stages,
+               float* __restrict__ P, int* __restrict__ status) {
+  constexpr int NCOL = 2 * KP;                       // hi | lo columns
+  constexpr uint32_t A_BYTES = TC_BM * TC_BK * 2;    // one BF16 A tile
+  constexpr uint32_t A_STAGE = X2 ? 2 * A_BYTES : A_BYTES;
+  constexpr uint32_t B_STAGE = NCOL * 128;           // NCOL rows x 128 B
+  constexpr uint32_t STAGE = A_STAGE + B_STAGE;
+  constexpr uint32_t TMEM_COLS = 2 * NCOL < 32 ? 32 : 2 * NCOL;
+  constexpr uint32_t IDESC = idesc_bf16(NCOL, true, false);
+
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ uint64_t bars[2 * 8 + 4];
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ int abort_sh;
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const uint32_t smem0 = smem_u32(smem);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t ntiles = (L + TC_BM - 1) / TC_BM;
+  const int nk = (int)((R + TC_BK - 1) / TC_BK);
+  auto full = [&](int s) { return smem_u32(&bars[s]); };
+  auto empty = [&](int s) { return smem_u32(&bars[8 + s]); };
+  auto accf = [&](int b) { return smem_u32(&bars[16 + b]); };
+  auto acce = [&](int b) { return smem_u32(&bars[18 + b]); };
+
+  if (threadIdx.x == 0) {
+    abort_sh = 0;
+    for (int s = 0; s < stages; ++s) {
+      mbar_init(full(s), 1);
+      mbar_init(empty(s), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(accf(b), 1);
+      mbar_init(acce(b), 4);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) tmem_alloc(smem_u32(&tmem_base_sh), TMEM_COLS);
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+  volatile int* abort_flag = &abort_sh;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      bool ok = true;
+      for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        const int l0 = (int)(t * TC_BM);
+        for (int kb = 0; kb < nk; ++kb) {
+          if (!mbar_wait(empty(s), ph ^ 1, abort_flag, status)) { ok = false; break; }
+          const uint32_t st = smem0 + s * STAGE;
+          mbar_expect_tx(full(s), STAGE);
+          tma_load_2d(st, &tm_hi, l0, kb * TC_BK, full(s));
+          tma_load_2d(st + A_BYTES / 2, &tm_hi, l0 + 64, kb * TC_BK, full(s));
+          if (X2) {
+            tma_load_2d(st + A_BYTES, &tm_lo, l0, kb * TC_BK, full(s));
+            tma_load_2d(st + A_BYTES + A_BYTES / 2, &tm_lo, l0 + 64, kb * TC_BK, full(s));
+          }
+          bulk_load(st + A_STAGE, bimg + (size_t)kb * B_STAGE, B_STAGE, full(s));
+          if (++s == stages) { s = 0; ph ^= 1; }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      int buf = 0;
+      uint32_t aph[2] = {0, 0};
+      bool ok = true;
+      for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+        if (!mbar_wait(acce(buf), aph[buf] ^ 1, abort_flag, status)) break;
+        tc_fence_after();
+        const uint32_t d = tmem + buf * NCOL;
+        for (int kb = 0; kb < nk; ++kb) {
+          if (!mbar_wait(full(s), ph, abort_flag, status)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t st = smem0 + s * STAGE;
+#pragma unroll
+          for (int kk = 0; kk < TC_BK / 16; ++kk) {
+            // MN-major A: K advances 16 rows = two 1024 B k-groups
+            const uint64_t bdesc = smem_desc(st + A_STAGE + kk * 32, 16, 1024);
+            const uint64_t adesc = smem_desc(st + kk * 2048, A_BYTES / 2, 1024);
+            umma_bf16(d, adesc, bdesc, IDESC, (kb | kk) != 0);
+            if (X2) {
+              const uint64_t adesc2 = smem_desc(st + A_BYTES + kk * 2048, A_BYTES / 2, 1024);
+              umma_bf16(d, adesc2, bdesc, IDESC, 1);
+            }
+          }
+          umma_commit(empty(s));  // frees the stage once these MMAs finish
+          if (++s == stages) { s = 0; ph ^= 1; }
+        }
+        if (!ok) break;
+        umma_commit(accf(buf));
+        aph[buf] ^= 1;
+        buf ^= 1;
+      }
+    }
+  } else {
+    // epilogue warps 2..5: TMEM lane quarter = warp % 4
+    const int q = warp & 3;
+    int buf = 0;
+    uint32_t aph[2] = {0, 0};
+    for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+      if (!mbar_wait(accf(buf), aph[buf], abort_flag, status)) break;
+      tc_fence_after();
+      const int64_t row = t * TC_BM + q * 32 + lane;
+      float v[NCOL];
+#pragma unroll
+      for (int c = 0; c < NCOL; c += 32)
+        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + buf * NCOL + c, v + c);
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acce(buf));
+      aph[buf] ^= 1;
+      buf ^= 1;
+      if (row < L) {
+        float* dst = P + row * k;
+        if (k == KP && (KP % 4) == 0) {
+#pragma unroll
+          for (int r = 0; r < KP; r += 4) {
+            float4 o = make_float4(v[r] + v[KP + r], v[r + 1] + v[KP + r + 1],
+                                   v[r + 2] + v[KP + r + 2], v[r + 3] + v[KP + r + 3]);
+            *reinterpret_cast<float4*>(dst + r) = o;
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < KP; ++r)
+            if (r < k) dst[r] = v[r] + v[KP + r];
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (abort_sh) tc_drain_after_abort();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, TMEM_COLS);
+  }
+}
+
+// Pre-swizzled B image for the right contraction: for stage kb, NCOL rows of
+// 128 bytes (K-major, 128B swizzle); row r < KP holds hi(F[j, r]) and row
+// KP + r holds lo(F[j, r]) for j = kb*64 .. kb*64+63 (zero beyond R or k).
+template <int KP>
+__global__ void k_tc_bimage(const double* __restrict__ F, int64_t R, int k, int nk,
+                            uint8_t* __restrict__ img) {
+  constexpr int NCOL = 2 * KP;
+  const int64_t total = (int64_t)nk * KP * TC_BK;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int kk = (int)(e % TC_BK);
+    const int r = (int)((e / TC_BK) % KP);
+    const int kb = (int)(e / ((int64_t)TC_BK * KP));
+    const int64_t j = (int64_t)kb * TC_BK + kk;
+    __nv_bfloat16 hi = __float2bfloat16(0.f), lo = __float2bfloat16(0.f);
+    if (j < R && r < k) split_bf16(F[j * k + r], hi, lo);
+    uint8_t* st = img + (size_t)kb * NCOL * 128;
+    *reinterpret_cast<__nv_bfloat16*>(st + sw128_kmajor_off(r, kk)) = hi;
+    *reinterpret_cast<__nv_bfloat16*>(st + sw128_kmajor_off(KP + r, kk)) = lo;
+  }
+}
+
+// ------------------------------------------------------------ left kernel
+// part[split][j*k + r] = sum_{l in split} X[l, j] * W(l, r), W = KRP(F_0..F_s).
+// Grid: (mgroups, nsplit); a CTA owns MT consecutive 128-row tiles of j.
+template <int KP, int MT, bool X2>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    k_tc_left(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
+              WGen wg, int64_t L, int64_t R, int k, int stages, int64_t chunks_per_split,
+              double* __restrict__ part, int* __restrict__ status) {
+  constexpr int NCOL = 2 * KP;
+  constexpr uint32_t A_TILE = TC_BM * TC_BK * 2;  // 16 KB
+  constexpr uint32_t A_BYTES = MT * A_TILE;
+  constexpr uint32_t A_STAGE = X2 ? 2 * A_BYTES : A_BYTES;
+  constexpr uint32_t B_STAGE = NCOL * 128;
+  constexpr uint32_t STAGE = A_STAGE + B_STAGE;
+  constexpr uint32_t TMEM_NEED = MT * NCOL;
+  constexpr uint32_t TMEM_COLS = TMEM_NEED <= 32 ? 32 : TMEM_NEED <= 64 ? 64 : TMEM_NEED <= 128 ? 128
+                                 : TMEM_NEED <= 256 ? 256 : 512;
+  constexpr uint32_t IDESC = idesc_bf16(NCOL, false, false);
+
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ uint64_t bars[2 * 8 + 1];
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ int abort_sh;
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const uint32_t smem0 = smem_u32(smem);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t nchunks = (L + TC_BK - 1) / TC_BK;
+  const int64_t c_begin = (int64_t)blockIdx.y * chunks_per_split;
+  int64_t c_end = c_begin + chunks_per_split;
+  if (c_end > nchunks) c_end = nchunks;
+  const int j0 = blockIdx.x * MT * TC_BM;
+  auto full = [&](int s) { return smem_u32(&bars[s]); };
+  auto empty = [&](int s) { return smem_u32(&bars[8 + s]); };
+  const uint32_t accf = smem_u32(&bars[16]);
+
+  if (threadIdx.x == 0) {
+    abort_sh = 0;
+    for (int s = 0; s < stages; ++s) {
+      mbar_init(full(s), 1 + 4);  // TMA expect_tx arrival + 4 producer warps
+      mbar_init(empty(s), 1);
+    }
+    mbar_init(accf, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) tmem_alloc(smem_u32(&tmem_base_sh), TMEM_COLS);
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+  volatile int* abort_flag = &abort_sh;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      for (int64_t c = c_begin; c < c_end; ++c) {
+        if (!mbar_wait(empty(s), ph ^ 1, abort_flag, status)) break;
+        const uint32_t st = smem0 + s * STAGE;
+        mbar_expect_tx(full(s), A_STAGE);
+        for (int mt = 0; mt < MT; ++mt) {
+          tma_load_2d(st + mt * A_TILE, &tm_hi, (int)(c * TC_BK), j0 + mt * TC_BM, full(s));
+          if (X2) tma_load_2d(st + A_BYTES + mt * A_TILE, &tm_lo, (int)(c * TC_BK), j0 + mt * TC_BM, full(s));
+        }
+        if (++s == stages) { s = 0; ph ^= 1; }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      bool any = false;
+      for (int64_t c = c_begin; c < c_end; ++c) {
+        if (!mbar_wait(full(s), ph, abort_flag, status)) break;
+        tc_fence_after();
+        const uint32_t st = smem0 + s * STAGE;
+#pragma unroll
+        for (int kk = 0; kk < TC_BK / 16; ++kk) {
+          const uint64_t bdesc = smem_desc(st + A_STAGE + kk * 32, 16, 1024);
+#pragma unroll
+          for (int mt = 0; mt < MT; ++mt) {
+            const uint64_t adesc = smem_desc(st + mt * A_TILE + kk * 32, 16, 1024);
+            umma_bf16(tmem + mt * NCOL, adesc, bdesc, IDESC, (c != c_begin || kk != 0) ? 1u : 0u);
+            if (X2) {
+              const uint64_t adesc2 = smem_desc(st + A_BYTES + mt * A_TILE + kk * 32, 16, 1024);
+              umma_bf16(tmem + mt * NCOL, adesc2, bdesc, IDESC, 1);
+            }
+          }
+        }
+        any = true;
+        umma_commit(empty(s));
+        if (++s == stages) { s = 0; ph ^= 1; }
+      }
+      if (any) umma_commit(accf);
+    }
+  } else {
+    // producer warps 2..5 build the Khatri-Rao B tile, then run the epilogue
+    const int pt = threadIdx.x - 64;  // 0..127
+    int s = 0;
+    uint32_t ph = 0;
+    bool ok = true;
+    for (int64_t c = c_begin; c < c_end; ++c) {
+      if (!mbar_wait(empty(s), ph ^ 1, abort_flag, status)) { ok = false; break; }
+      uint8_t* bt = smem + s * STAGE + A_STAGE;
+      // 64 values of l x KP ranks; thread pt handles l = pt & 63, ranks r = (pt >> 6) + 2i
+      const int kk = pt & (TC_BK - 1);
+      const int64_t l = c * TC_BK + kk;
+      for (int r = pt >> 6; r < KP; r += 2) {
+        __nv_bfloat16 hi = __float2bfloat16(0.f), lo = __float2bfloat16(0.f);
+        if (l < L && r < k) split_bf16(wgen_eval(wg, l, r, k), hi, lo);
+        *reinterpret_cast<__nv_bfloat16*>(bt + sw128_kmajor_off(r, kk)) = hi;
+        *reinterpret_cast<__nv_bfloat16*>(bt + sw128_kmajor_off(KP + r, kk)) = lo;
+      }
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncwarp();
+      if (lane == 0) mbar_arrive(full(s));
+      if (++s == stages) { s = 0; ph ^= 1; }
+    }
+    if (ok && c_end > c_begin) {
+      const int q = warp & 3;
+      if (mbar_wait(accf, 0, abort_flag, status)) {
+        tc_fence_after();
+        double* dst = part + (int64_t)blockIdx.y * R * k;
+        for (int mt = 0; mt < MT; ++mt) {
+          float v[NCOL];
+#pragma unroll
+          for (int cc = 0; cc < NCOL; cc += 32)
+            tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + mt * NCOL + cc, v + cc);
+          const int64_t j = (int64_t)j0 + mt * TC_BM + q * 32 + lane;
+          if (j < R) {
+#pragma unroll
+            for (int r = 0; r < KP; ++r)
+              if (r < k) dst[j * k + r] = (double)v[r] + (double)v[KP + r];
+          }
+        }
+        tc_fence_before();
+      }
+    } else if (c_end <= c_begin) {
+      // no work: this split contributes zeros
+      const int q = warp & 3;
+      double* dst = part + (int64_t)blockIdx.y * R * k;
+      for (int mt = 0; mt < MT; ++mt) {
+        const int64_t j = (int64_t)j0 + mt * TC_BM + q * 32 + lane;
+        if (j < R)
+          for (int r = 0; r < k; ++r) dst[j * k + r] = 0.0;
+      }
+    }
+  }
+  __syncthreads();
+  if (abort_sh) tc_drain_after_abort();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, TMEM_COLS);
+  }
+}
+
+// X (f32/f64, L x R column-major) -> BF16 hi (and lo) with leading dim Lpad.
+template <typename T>
+__global__ void k_tc_convert(const T* __restrict__ X, int64_t L, int64_t R, int64_t Lpad,
+                             __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
+  const int64_t total = Lpad * R;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t l = e % Lpad, j = e / Lpad;
+    double x = l < L ? (double)X[l + L * j] : 0.0;
+    __nv_bfloat16 h = __double2bfloat16(x);
+    hi[e] = h;
+    if (lo) lo[e] = __double2bfloat16(x - (double)__bfloat162float(h));
+  }
+}
+
+// ------------------------------------------------------------ host side
 struct TcTensor {
-  void* hi = nullptr;
-  void* lo = nullptr;
+  __nv_bfloat16* hi = nullptr;
+  __nv_bfloat16* lo = nullptr;
   int64_t L = 0, R = 0, Lpad = 0;
   int prec = 0;
+  CUtensorMap mR_hi, mR_lo, mL_hi, mL_lo;
+  uint8_t* bimg = nullptr;
+  size_t bimg_bytes = 0;
+  int kpad = 0;
 };
 
-inline size_t tc_scratch_elems(const TcTensor&, int, int) { return 0; }
+inline int tc_kpad(int k) { return k <= 16 ? 16 : k <= 32 ? 32 : 64; }
+
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+inline EncodeTiledFn tc_encode_fn() {
+  static EncodeTiledFn fn = nullptr;
+  if (!fn) {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = (EncodeTiledFn)p;
+  }
+  return fn;
+}
+
+// 2-D BF16 map over (L rows fastest, R columns), row stride Lpad elements.
+inline bool tc_make_map(CUtensorMap* m, void* base, int64_t L, int64_t R, int64_t Lpad,
+                        uint32_t box0, uint32_t box1) {
+  EncodeTiledFn fn = tc_encode_fn();
+  if (!fn) return false;
+  cuuint64_t gdim[2] = {(cuuint64_t)L, (cuuint64_t)R};
+  cuuint64_t gstride[1] = {(cuuint64_t)(Lpad * 2)};
+  cuuint32_t box[2] = {box0, box1};
+  cuuint32_t estr[2] = {1, 1};
+  return fn(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, base, gdim, gstride, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+            CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
 inline void tc_free(TcTensor& t) {
   if (t.hi) cudaFree(t.hi);
   if (t.lo) cudaFree(t.lo);
+  if (t.bimg) cudaFree(t.bimg);
   t.hi = t.lo = nullptr;
+  t.bimg = nullptr;
+  t.bimg_bytes = 0;
 }
-inline void tc_set_tensor(TcTensor&, const void*, bool, int64_t, int64_t, int, cudaStream_t) {}
-inline void tc_right(const TcTensor&, const double*, int, float*, cudaStream_t) {}
-inline int tc_left(const TcTensor&, const WGen&, int, double*, int, cudaStream_t) { return 1; }
+
+// Returns cudaSuccess or an error; false map creation is reported as
+// cudaErrorInvalidValue.
+inline cudaError_t tc_set_tensor(TcTensor& t, const void* src, bool src_f64, int64_t L, int64_t R,
+                                 int prec, cudaStream_t st) {
+  tc_free(t);
+  t.L = L;
+  t.R = R;
+  t.Lpad = (L + 7) / 8 * 8;
+  t.prec = prec;
+  size_t n = (size_t)t.Lpad * R;
+  cudaError_t e = cudaMalloc(&t.hi, n * 2);
+  if (e != cudaSuccess) return e;
+  if (prec == 2) {
+    e = cudaMalloc(&t.lo, n * 2);
+    if (e != cudaSuccess) return e;
+  }
+  if (src_f64)
+    k_tc_convert<double><<<4096, 256, 0, st>>>((const double*)src, L, R, t.Lpad, t.hi, t.lo);
+  else
+    k_tc_convert<float><<<4096, 256, 0, st>>>((const float*)src, L, R, t.Lpad, t.hi, t.lo);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  bool ok = tc_make_map(&t.mR_hi, t.hi, L, R, t.Lpad, 64, 64) &&
+            tc_make_map(&t.mL_hi, t.hi, L, R, t.Lpad, 64, 128);
+  if (ok && t.lo)
+    ok = tc_make_map(&t.mR_lo, t.lo, L, R, t.Lpad, 64, 64) &&
+         tc_make_map(&t.mL_lo, t.lo, L, R, t.Lpad, 64, 128);
+  else if (ok) {
+    t.mR_lo = t.mR_hi;
+    t.mL_lo = t.mL_hi;
+  }
+  return ok ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+inline int tc_stages(uint32_t stage_bytes) {
+  const uint32_t budget = 200 * 1024;
+  int s = (int)(budget / stage_bytes);
+  return s < 2 ? 2 : (s > 8 ? 8 : s);
+}
+
+inline int tc_left_mt(int64_t R) { return R > 128 ? 2 : 1; }
+
+inline void tc_left_plan(const TcTensor& t, int sm_count, int* mgroups, int* nsplit,
+                         int64_t* per) {
+  const int MT = tc_left_mt(t.R);
+  *mgroups = (int)((t.R + MT * TC_BM - 1) / (MT * TC_BM));
+  int ns = sm_count / *mgroups;
+  if (ns < 1) ns = 1;
+  const int64_t nch = (t.L + TC_BK - 1) / TC_BK;
+  if (ns > nch) ns = (int)nch;
+  *per = (nch + ns - 1) / ns;
+  *nsplit = (int)((nch + *per - 1) / *per);
+}
+
+inline size_t tc_scratch_elems(const TcTensor& t, int sm_count, int k) {
+  if (!t.hi) return 0;
+  int mg, ns;
+  int64_t per;
+  tc_left_plan(t, sm_count, &mg, &ns, &per);
+  return (size_t)ns * t.R * k;
+}
+
+template <int KP, bool X2>
+inline cudaError_t tc_set_attrs() {
+  constexpr uint32_t SR = (X2 ? 2 : 1) * TC_BM * TC_BK * 2 + 2 * KP * 128;
+  constexpr uint32_t SL1 = (X2 ? 2 : 1) * 1 * TC_BM * TC_BK * 2 + 2 * KP * 128;
+  constexpr uint32_t SL2 = (X2 ? 2 : 1) * 2 * TC_BM * TC_BK * 2 + 2 * KP * 128;
+  cudaError_t e = cudaFuncSetAttribute(k_tc_right<KP, X2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)(tc_stages(SR) * SR + 1024));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_tc_left<KP, 1, X2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(tc_stages(SL1) * SL1 + 1024));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_tc_left<KP, 2, X2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(tc_stages(SL2) * SL2 + 1024));
+  return e;
+}
+
+// Allocates the B image for rank k and sets the kernels' shared-memory
+// limits (host calls made outside any graph capture).
+inline cudaError_t tc_ensure(TcTensor& t, int k) {
+  if (!t.hi) return cudaSuccess;
+  const int kp = tc_kpad(k);
+  const bool x2 = t.prec == 2;
+  cudaError_t e = kp == 16 ? (x2 ? tc_set_attrs<16, true>() : tc_set_attrs<16, false>())
+                  : kp == 32 ? (x2 ? tc_set_attrs<32, true>() : tc_set_attrs<32, false>())
+                             : (x2 ? tc_set_attrs<64, true>() : tc_set_attrs<64, false>());
+  if (e != cudaSuccess) return e;
+  const int nk = (int)((t.R + TC_BK - 1) / TC_BK);
+  size_t need = (size_t)nk * 2 * kp * 128;
+  if (t.bimg && t.bimg_bytes >= need && t.kpad == kp) return cudaSuccess;
+  if (t.bimg) cudaFree(t.bimg);
+  t.bimg = nullptr;
+  t.kpad = kp;
+  t.bimg_bytes = need;
+  return cudaMalloc(&t.bimg, need);
+}
+
+// Builds the pre-swizzled hi|lo B image of F_{N-1} for the right contraction.
+inline void tc_right_prep(const TcTensor& t, const double* F, int k, cudaStream_t st) {
+  const int nk = (int)((t.R + TC_BK - 1) / TC_BK);
+  const int kp = tc_kpad(k);
+  const unsigned blocks = (unsigned)std::min<int64_t>(((int64_t)nk * kp * TC_BK + 255) / 256, 1024);
+  if (kp == 16)
+    k_tc_bimage<16><<<blocks, 256, 0, st>>>(F, t.R, k, nk, t.bimg);
+  else if (kp == 32)
+    k_tc_bimage<32><<<blocks, 256, 0, st>>>(F, t.R, k, nk, t.bimg);
+  else
+    k_tc_bimage<64><<<blocks, 256, 0, st>>>(F, t.R, k, nk, t.bimg);
+}
+
+template <int KP, bool X2>
+inline void tc_right_launch(const TcTensor& t, int k, float* P, int* status, int sm_count,
+                            cudaStream_t st) {
+  constexpr uint32_t STAGE = (X2 ? 2 : 1) * TC_BM * TC_BK * 2 + 2 * KP * 128;
+  const int stages = tc_stages(STAGE);
+  const size_t smem = (size_t)stages * STAGE + 1024;
+  const int64_t ntiles = (t.L + TC_BM - 1) / TC_BM;
+  const int grid = (int)std::min<int64_t>(ntiles, sm_count);
+  k_tc_right<KP, X2><<<grid, TC_THREADS, smem, st>>>(t.mR_hi, t.mR_lo, t.bimg, t.L, t.R, k, stages,
+                                                     P, status);
+}
+
+// P32 = X * F_{N-1} on the tensor cores (call tc_right_prep first).
+inline void tc_right(const TcTensor& t, int k, float* P, int* status, int sm_count,
+                     cudaStream_t st) {
+  const bool x2 = t.prec == 2;
+  switch (tc_kpad(k)) {
+    case 16: x2 ? tc_right_launch<16, true>(t, k, P, status, sm_count, st)
+                : tc_right_launch<16, false>(t, k, P, status, sm_count, st); break;
+    case 32: x2 ? tc_right_launch<32, true>(t, k, P, status, sm_count, st)
+                : tc_right_launch<32, false>(t, k, P, status, sm_count, st); break;
+    default: x2 ? tc_right_launch<64, true>(t, k, P, status, sm_count, st)
+                : tc_right_launch<64, false>(t, k, P, status, sm_count, st); break;
+  }
+}
+
+template <int KP, int MT, bool X2>
+inline void tc_left_launch(const TcTensor& t, const WGen& wg, int k, double* part, int* status,
+                           int sm_count, cudaStream_t st, int* nsplit_out) {
+  int mg, ns;
+  int64_t per;
+  tc_left_plan(t, sm_count, &mg, &ns, &per);
+  constexpr uint32_t STAGE = (X2 ? 2 : 1) * MT * TC_BM * TC_BK * 2 + 2 * KP * 128;
+  const int stages = tc_stages(STAGE);
+  const size_t smem = (size_t)stages * STAGE + 1024;
+  k_tc_left<KP, MT, X2><<<dim3(mg, ns), TC_THREADS, smem, st>>>(t.mL_hi, t.mL_lo, wg, t.L, t.R, k,
+                                                                stages, per, part, status);
+  *nsplit_out = ns;
+}
+
+// Returns the number of split-K partials written to `part`.
+inline int tc_left(const TcTensor& t, const WGen& wg, int k, double* part, int* status,
+                   int sm_count, cudaStream_t st) {
+  const bool x2 = t.prec == 2;
+  const int MT = tc_left_mt(t.R);
+  int ns = 1;
+#define TCL(KP)                                                                                  \
+  if (MT == 2) {                                                                                 \
+    x2 ? tc_left_launch<KP, 2, true>(t, wg, k, part, status, sm_count, st, &ns)                  \
+       : tc_left_launch<KP, 2, false>(t, wg, k, part, status, sm_count, st, &ns);                \
+  } else {                                                                                       \
+    x2 ? tc_left_launch<KP, 1, true>(t, wg, k, part, status, sm_count, st, &ns)                  \
+       : tc_left_launch<KP, 1, false>(t, wg, k, part, status, sm_count, st, &ns);                \
+  }
+  switch (tc_kpad(k)) {
+    case 16: TCL(16) break;
+    case 32: TCL(32) break;
+    default: TCL(64) break;
+  }
+#undef TCL
+  return ns;
+}
 
 }  // namespace pg

@@ -149,7 +149,7 @@ def test_argument_errors(gpu):
         assert ei.value.code == -7
         c.set_factors(init_factors(X.shape, 4))
         with pytest.raises(gpu.PlancGpuError):
-            c.mttkrp(3)
+            c.mttkrp(-1)
         with pytest.raises(gpu.PlancGpuError):
             c.run(7, 1)
         c.run("hals", 1)

@@ -1,0 +1,92 @@
+"""GPU parity of the tensor-core (tcgen05) MTTKRP paths against the FP64
+oracle, through the C ABI.
+
+Stated error bounds (max-abs error / max-abs value of the FP64 result):
+  bf16   : the tensor is rounded to BF16 (relative 2^-9 per element), factors
+           and Khatri-Rao rows are split hi+lo (relative ~2^-17), FP32
+           accumulation: bound 4e-3.
+  bf16x2 : the tensor is split hi+lo as well: bound 2e-5.
+Final relative error of a full NTF run vs the FP64 path: within 1e-4
+(absolute), the north-star bar for mixed precision, for bf16x2 at every size
+and for bf16 at 192^3. The bf16 error estimate carries its own noise: the
+Gram-form error uses <bf16(X), model>, whose deviation from <X, model> is a
+sum of numel rounding errors, about 2 * 0.0016 / sqrt(numel) relative to
+||X||^2; divided by 2*err that is ~3e-4 at 64^3 with err ~ 0.01 (and ~5e-6
+at 1024^3). At 64^3 the bf16 bound is therefore 1e-3."""
+import numpy as np
+import pytest
+
+from helpers import cp_tensor, init_factors, rel
+
+pytestmark = pytest.mark.gpu
+BOUND = {"bf16": 4e-3, "bf16x2": 2e-5}
+
+
+def _normalized(F):
+    return [f / np.linalg.norm(f, axis=0) for f in F]
+
+
+@pytest.mark.parametrize("prec", ["bf16", "bf16x2"])
+@pytest.mark.parametrize("dims,k", [((64, 64, 64), 8), ((40, 33, 21), 32), ((13, 7, 20), 5),
+                                    ((9, 8, 7, 10), 64), ((130, 3, 300), 16), ((24, 16, 16, 40), 32)])
+def test_tc_mttkrp_all_modes(gpu, oracle_lib, prec, dims, k):
+    X, _ = cp_tensor(dims, 4, seed=21)
+    F = init_factors(dims, k, seed=22)
+    Fn = _normalized(F)
+    with gpu.Context(0, prec) as c:
+        c.set_tensor(X)
+        c.set_factors(F)
+        for n in range(len(dims)):
+            ref = oracle_lib.mttkrp_direct(X, Fn, n)
+            got = c.mttkrp(n, dimtree=True)
+            assert rel(got, ref) < BOUND[prec], (n, rel(got, ref))
+
+
+@pytest.mark.parametrize("prec", ["bf16", "bf16x2"])
+@pytest.mark.parametrize("algo", ["hals", "mu", "anlsbpp"])
+def test_tc_ntf_matches_fp64_error(gpu, prec, algo):
+    dims, k, iters = (64, 64, 64), 8, 20
+    X, _ = cp_tensor(dims, k, noise=0.01, seed=23)
+    F0 = init_factors(dims, k, seed=24)
+    with gpu.Context(0, "fp64") as c:
+        c.set_tensor(X)
+        c.set_factors(F0)
+        e64 = c.run(algo, iters)
+    with gpu.Context(0, prec) as c:
+        c.set_tensor(X.astype(np.float32))
+        c.set_factors(F0)
+        e = c.run(algo, iters)
+        assert abs(c.objective_error() - e[-1]) < 1e-4
+    assert np.all(np.isfinite(e))
+    tol = 1e-4 if prec == "bf16x2" else 1e-3
+    assert abs(e[-1] - e64[-1]) < tol, (e[-1], e64[-1])
+
+
+@pytest.mark.parametrize("algo", ["hals", "anlsbpp"])
+def test_tc_bf16_error_within_1e4_at_192cube(gpu, algo):
+    dims, k, iters = (192, 192, 192), 16, 12
+    X, _ = cp_tensor(dims, k, noise=0.01, seed=26)
+    F0 = init_factors(dims, k, seed=27)
+    errs = {}
+    for prec in ("fp64", "bf16"):
+        with gpu.Context(0, prec) as c:
+            c.set_tensor(X.astype(np.float32))
+            c.set_factors(F0)
+            errs[prec] = c.run(algo, iters)[-1]
+    assert abs(errs["bf16"] - errs["fp64"]) < 1e-4, errs
+
+
+def test_tc_large_split_k(gpu, oracle_lib):
+    # long reduction (L = 147456 -> many split-K partials) and R = 300 with a
+    # ragged last tile
+    dims, k = (384, 384, 300), 32
+    rng = np.random.default_rng(5)
+    X = np.asfortranarray(rng.random(dims, dtype=np.float32))
+    F = init_factors(dims, k, seed=25)
+    Fn = _normalized(F)
+    with gpu.Context(0, "bf16x2") as c:
+        c.set_tensor(X)
+        c.set_factors(F)
+        for n in (0, 2):
+            ref = oracle_lib.mttkrp_direct(X.astype(np.float64), Fn, n)
+            assert rel(c.mttkrp(n), ref) < BOUND["bf16x2"]
