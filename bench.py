@@ -122,13 +122,13 @@ def peaks():
     return 6650.0, "fallback"
 
 
-def traffic_from_profiles(precision, dims, k):
-    """Per-launch DRAM traffic of the partial MTTKRP kernels from the
-    committed ncu summary (a line `traffic_per_launch_bytes <prec> <dims> <k>: <n>`)."""
+def traffic_from_profiles(precision, dims, k, which):
+    """Per-launch DRAM traffic of a partial MTTKRP kernel from the committed ncu
+    summary (a line `traffic_per_launch_bytes <which> <prec> <dims> <k>: <n>`)."""
     path = os.path.join(ROOT, "profiles", "mttkrp_tc_1024cube_k32.md")
     if not os.path.exists(path):
         return None
-    key = "traffic_per_launch_bytes %s %s %d:" % (precision, "x".join(map(str, dims)), k)
+    key = "traffic_per_launch_bytes %s %s %s %d:" % (which, precision, "x".join(map(str, dims)), k)
     for line in open(path):
         if line.strip().startswith(key):
             try:
@@ -278,23 +278,35 @@ def main():
     ctx.set_timing(False)
     value = world * args.steps / (ms * 1e-3)
 
-    # dominant kernel: the partial MTTKRP contraction
-    c_ms, c_n = kt["contract"]
+    # dominant kernel: the partial MTTKRP contraction (right: P = X*F_last,
+    # writes P in FP32; left: X^T*KRP, writes split-K FP64 partials)
     L = dims[0] * dims[1]
     R = numel // L
     nsplit_left = max(1, 148 // ((R + 255) // 256))
-    bytes_right = numel * EB[args.precision] + L * k * 4
-    bytes_left = numel * EB[args.precision] + nsplit_left * R * k * 8
-    avg_bytes = 0.5 * (bytes_right + bytes_left)
-    avg_launch_s = (c_ms / max(c_n, 1)) * 1e-3
+    kern = {
+        "right": (kt["contract"], numel * EB[args.precision] + L * k * 4),
+        "left": (kt["contract_left"], numel * EB[args.precision] + nsplit_left * R * k * 8),
+    }
     peak, peak_kind = peaks()
-    achieved = avg_bytes / avg_launch_s / 1e9
+    per_kernel = {}
+    for name, ((kms, kn), kbytes) in kern.items():
+        avg_s = (kms / max(kn, 1)) * 1e-3
+        per_kernel[name] = {"launches": kn, "avg_launch_ms": avg_s * 1e3,
+                            "algorithmic_bytes_per_launch": kbytes,
+                            "achieved_gbs": kbytes / avg_s / 1e9 if avg_s > 0 else None}
+    dom = max(per_kernel, key=lambda n: kern[n][0][0])
+    d = per_kernel[dom]
+    c_ms = kern["right"][0][0] + kern["left"][0][0]
+    c_n = kern["right"][0][1] + kern["left"][0][1]
     mttkrp_tflops = (2.0 * numel * k * c_n) / (c_ms * 1e-3) / 1e12 if c_ms > 0 else None
-    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": traffic_from_profiles(args.precision, dims, k),
-                "peak_source": peak_kind, "kernel": "partial MTTKRP (k_tc_right / k_tc_left)",
-                "algorithmic_bytes_per_launch": avg_bytes,
-                "avg_launch_ms": avg_launch_s * 1e3, "launches": c_n}
+    roofline = {"bound": "hbm", "achieved": d["achieved_gbs"], "peak": peak, "unit": "GB/s",
+                "frac": d["achieved_gbs"] / peak if d["achieved_gbs"] else None,
+                "traffic": traffic_from_profiles(args.precision, dims, k, dom),
+                "peak_source": peak_kind,
+                "kernel": "partial MTTKRP, %s contraction (k_tc_%s)" % (dom, dom),
+                "algorithmic_bytes_per_launch": d["algorithmic_bytes_per_launch"],
+                "avg_launch_ms": d["avg_launch_ms"], "launches": d["launches"],
+                "per_kernel": per_kernel}
     kernel_share = {c: round(v[0] / max(sum(x[0] for x in kt.values()), 1e-9), 4)
                     for c, v in kt.items() if v[1]}
 

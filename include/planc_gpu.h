@@ -143,9 +143,10 @@ int planc_gpu_bpp_solve(planc_gpu_ctx* ctx, const double* AtA, const double* AtB
 
 /* Kernel timing, for roofline measurement: while enabled, CUDA events bracket
  * every launch of each kernel class on the context's stream. Class ids:
- *   0 partial MTTKRP (tensor contraction), 1 multi-TTV, 2 factor update,
- *   3 normalise + Gram, 4 error, 5 split-K reduction, 6 BPP,
- *   7 operand preparation (tensor-core B image).
+ *   0 partial MTTKRP, right contraction (P = X * F_last) and direct mode 0,
+ *   1 multi-TTV, 2 factor update, 3 normalise + Gram, 4 error,
+ *   5 split-K reduction, 6 BPP, 7 operand preparation (tensor-core B image),
+ *   8 partial MTTKRP, left contraction (X^T * KRP) and direct modes > 0.
  * get_kernel_times fills ms[c] and launches[c] for c < n and resets them. */
 int planc_gpu_set_timing(planc_gpu_ctx* ctx, int enable);
 int planc_gpu_get_kernel_times(planc_gpu_ctx* ctx, double* ms, int64_t* launches, int n);

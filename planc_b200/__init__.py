@@ -26,7 +26,8 @@ ERR = {
 PREC = {"fp64": 0, "bf16": 1, "bf16x2": 2}
 ALGO = {"mu": 0, "hals": 1, "anlsbpp": 2}
 F64, F32 = 0, 1
-KERNEL_CLASSES = ["contract", "ttv", "update", "normgram", "error", "reduce", "bpp", "prep"]
+KERNEL_CLASSES = ["contract", "ttv", "update", "normgram", "error", "reduce", "bpp", "prep",
+                  "contract_left"]
 
 # Every symbol declared in include/planc_gpu.h.
 EXPORTS = [

@@ -214,9 +214,17 @@ __global__ void __launch_bounds__(256) k_ttv_right(const TT* __restrict__ T, int
   int64_t b0 = (int64_t)blockIdx.y * b_per_split;
   int64_t b1 = b0 + b_per_split;
   if (b1 > B) b1 = B;
+  if (b0 >= b1) {
+    out[(int64_t)blockIdx.y * split_stride + e] = 0.0;
+    return;
+  }
+  WIdx wi;
+  widx_init(wg, b0, wi);
   double s = 0.0;
-  for (int64_t b = b0; b < b1; ++b)
-    s = fma((double)T[(a + A * b) * k + r], wgen_eval(wg, b, r, k), s);
+  for (int64_t b = b0; b < b1; ++b) {
+    s = fma((double)T[(a + A * b) * k + r], wgen_row(wg, wi, r, k), s);
+    widx_advance(wg, wi, 1);
+  }
   out[(int64_t)blockIdx.y * split_stride + e] = s;
 }
 
@@ -245,10 +253,15 @@ __global__ void __launch_bounds__(128) k_hals_rows(double* __restrict__ H, const
 #pragma unroll
   for (int i = 0; i < KP; ++i) {
     if (i < k) {
-      double hg = 0.0;
+      double p0 = 0.0, p1 = 0.0, p2 = 0.0, p3 = 0.0;
 #pragma unroll
-      for (int j = 0; j < KP; ++j)
-        if (j < k) hg = fma(h[j], Gs[j * k + i], hg);
+      for (int j = 0; j < KP; j += 4) {
+        if (j < k) p0 = fma(h[j], Gs[j * k + i], p0);
+        if (j + 1 < k) p1 = fma(h[j + 1], Gs[(j + 1) * k + i], p1);
+        if (j + 2 < k) p2 = fma(h[j + 2], Gs[(j + 2) * k + i], p2);
+        if (j + 3 < k) p3 = fma(h[j + 3], Gs[(j + 3) * k + i], p3);
+      }
+      double hg = (p0 + p1) + (p2 + p3);
       double u = h[i] + (m[i] - hg);
       h[i] = (u < kEps17) ? kEps17 : u;
     }
@@ -272,11 +285,13 @@ __global__ void __launch_bounds__(128) k_mu_rows(double* __restrict__ H, const d
   for (int j = 0; j < KP; ++j) h[j] = j < k ? H[row * k + j] : 0.0;
 #pragma unroll
   for (int c = 0; c < KP; ++c) {
-    double acc = 0.0;
+    double p0 = 0.0, p1 = 0.0;
 #pragma unroll
-    for (int j = 0; j < KP; ++j)
-      if (j < k && c < k) acc = fma(h[j], Gs[j * k + c], acc);
-    t[c] = acc + kEps6;
+    for (int j = 0; j < KP; j += 2) {
+      if (j < k && c < k) p0 = fma(h[j], Gs[j * k + c], p0);
+      if (j + 1 < k && c < k) p1 = fma(h[j + 1], Gs[(j + 1) * k + c], p1);
+    }
+    t[c] = (p0 + p1) + kEps6;
   }
 #pragma unroll
   for (int c = 0; c < KP; ++c)
@@ -294,8 +309,10 @@ __global__ void __launch_bounds__(1024) k_normalize_gram(double* __restrict__ F,
                                                          double* __restrict__ lambda,
                                                          double* __restrict__ Gall, int N, int n,
                                                          int next, double* __restrict__ Gloo) {
+  constexpr int ROWS = 64;
   __shared__ double red[1024];
   __shared__ double lam[kMaxRank];
+  __shared__ double tile[ROWS * kMaxRank];
   const int tid = threadIdx.x;
   const int lanes = 1024 / k;
   const int r = tid % k, lane = tid / k;
@@ -315,24 +332,47 @@ __global__ void __launch_bounds__(1024) k_normalize_gram(double* __restrict__ F,
     if (lambda) lambda[tid] = nrm;
   }
   __syncthreads();
-  for (int64_t e = tid; e < I * k; e += 1024) {
-    double nrm = lam[e % k];
-    if (nrm > 0) F[e] = F[e] / nrm;
+  // normalise row blocks in place and accumulate F^T F from shared memory;
+  // thread tid owns Gram entries e = tid + 1024*q (q < 4 since k <= 64)
+  double acc[4] = {0.0, 0.0, 0.0, 0.0};
+  const int kk2 = k * k;
+  for (int64_t row0 = 0; row0 < I; row0 += ROWS) {
+    const int nrows = (int)((I - row0) < ROWS ? (I - row0) : ROWS);
+    for (int e = tid; e < nrows * k; e += 1024) {
+      int64_t g = row0 * k + e;
+      double nrm = lam[e % k];
+      double v = F[g];
+      if (nrm > 0) {
+        v = v / nrm;
+        F[g] = v;
+      }
+      tile[e] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      int e = tid + 1024 * q;
+      if (e < kk2) {
+        int a = e / k, b = e % k;
+        double s = acc[q];
+        for (int i = 0; i < nrows; ++i) s = fma(tile[i * k + a], tile[i * k + b], s);
+        acc[q] = s;
+      }
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  double* Gn = Gall + (int64_t)n * k * k;
-  for (int e = tid; e < k * k; e += 1024) {
-    int a = e / k, b = e % k;
-    double s = 0.0;
-    for (int64_t i = 0; i < I; ++i) s = fma(F[i * k + a], F[i * k + b], s);
-    Gn[e] = s;
+  double* Gn = Gall + (int64_t)n * kk2;
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    int e = tid + 1024 * q;
+    if (e < kk2) Gn[e] = acc[q];
   }
   if (next < 0) return;
   __syncthreads();
-  for (int e = tid; e < k * k; e += 1024) {
+  for (int e = tid; e < kk2; e += 1024) {
     double g = 1.0;
     for (int i = 0; i < N; ++i)
-      if (i != next) g = g * Gall[(int64_t)i * k * k + e];
+      if (i != next) g = g * Gall[(int64_t)i * kk2 + e];
     Gloo[e] = g;
   }
 }

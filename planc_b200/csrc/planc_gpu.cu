@@ -167,7 +167,7 @@ void launch(planc_gpu_ctx* c, int cls, Fn&& fn) {
   if (timed) {
     CK(cudaEventRecord(b, c->stream));
     c->pending.push_back({cls, a, b});
-    if (c->pending.size() > 4096) drain_timing(c);
+    if (c->pending.size() > (1u << 16)) drain_timing(c);
   }
   c->launch_count++;
 }
@@ -256,6 +256,8 @@ void ensure_buffers(planc_gpu_ctx* c) {
   if (c->N == 3 || c->N == 4) {
     ContractPlan pl = plan_contract(c, true, c->R, c->L, c->L, 1, 0);
     need = std::max(need, contract_scratch(pl));
+    ContractPlan pr = plan_contract(c, false, c->L, c->L, c->R, 1, 0);
+    need = std::max(need, contract_scratch(pr));
     TtvRightPlan tr = plan_ttv_right(c, c->dims[0], c->L / c->dims[0]);
     need = std::max(need, (size_t)tr.nsplit * c->dims[0] * k);
     if (c->N == 4) {
@@ -290,8 +292,10 @@ void ensure_buffers(planc_gpu_ctx* c) {
 void run_contract(planc_gpu_ctx* c, const ContractPlan& p, bool left, const double* X,
                   const WGen& wg, double* out) {
   const int k = c->k;
+  if (contract_scratch(p) > c->scratch_elems)
+    fail(PLANC_GPU_ERR_STATE, "internal: contraction scratch larger than planned");
   double* dst = p.nsplit > 1 ? c->scratch : out;
-  launch(c, KC_CONTRACT, [&] {
+  launch(c, left ? KC_CONTRACT_LEFT : KC_CONTRACT, [&] {
     switch (kpad(k)) {
 #define CASE(KP)                                                                      \
   case KP:                                                                            \
@@ -317,6 +321,8 @@ template <typename TT>
 void run_ttv_right(planc_gpu_ctx* c, const TT* T, int64_t A, int64_t B, const WGen& wg,
                    double* out) {
   TtvRightPlan p = plan_ttv_right(c, A, B);
+  if (p.nsplit > 1 && (size_t)p.nsplit * A * c->k > c->scratch_elems)
+    fail(PLANC_GPU_ERR_STATE, "internal: multi-TTV scratch larger than planned");
   double* dst = p.nsplit > 1 ? c->scratch : out;
   int k = c->k;
   launch(c, KC_TTV, [&] {
@@ -384,7 +390,9 @@ void partial_left(planc_gpu_ctx* c, double* out) {
   } else {
     WGen wg = make_wgen(c, modes);
     int nsplit = 0;
-    launch(c, KC_CONTRACT, [&] {
+    if (tc_scratch_elems(c->tct, c->sm_count, c->k) > c->scratch_elems)
+      fail(PLANC_GPU_ERR_STATE, "internal: split-K scratch larger than planned");
+    launch(c, KC_CONTRACT_LEFT, [&] {
       nsplit = tc_left(c->tct, wg, c->k, c->scratch, c->status_dev, c->sm_count, c->stream);
     });
     int64_t n = c->R * c->k;

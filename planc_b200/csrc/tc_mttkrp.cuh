@@ -30,6 +30,8 @@
 #include <cuda.h>
 #include <cuda_bf16.h>
 
+#include <type_traits>
+
 #include "common.cuh"
 
 namespace pg {
@@ -372,37 +374,51 @@ __global__ void k_tc_bimage(const double* __restrict__ F, int64_t R, int k, int 
 // ------------------------------------------------------------ left kernel
 // part[split][j*k + r] = sum_{l in split} X[l, j] * W(l, r), W = KRP(F_0..F_s).
 // Grid: (mgroups, nsplit); a CTA owns MT consecutive 128-row tiles of j.
+// Split y takes the 64-wide chunks of l numbered y, y + nsplit, y + 2*nsplit..
+// so the CTAs running together read neighbouring 128-byte pieces of the same
+// rows of X (DRAM page locality). The tensor-core accumulator is restarted
+// every TCL_GROUP chunks (double-buffered in TMEM) and drained by four
+// dedicated warps into register running sums, which keeps every FP32
+// accumulation chain short.
+constexpr int TCL_GROUP = 8;        // chunks per accumulator group
+constexpr int TCL_THREADS = 320;    // warp 0 TMA, 1 MMA, 2-5 KRP producers, 6-9 drain
+
 template <int KP, int MT, bool X2>
-__global__ void __launch_bounds__(TC_THREADS, 1)
+__global__ void __launch_bounds__(TCL_THREADS, 1)
     k_tc_left(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
-              WGen wg, int64_t L, int64_t R, int k, int stages, int64_t chunks_per_split,
-              double* __restrict__ part, int* __restrict__ status) {
+              WGen wg, int64_t L, int64_t R, int k, int stages, double* __restrict__ part,
+              int* __restrict__ status) {
   constexpr int NCOL = 2 * KP;
   constexpr uint32_t A_TILE = TC_BM * TC_BK * 2;  // 16 KB
   constexpr uint32_t A_BYTES = MT * A_TILE;
   constexpr uint32_t A_STAGE = X2 ? 2 * A_BYTES : A_BYTES;
   constexpr uint32_t B_STAGE = NCOL * 128;
   constexpr uint32_t STAGE = A_STAGE + B_STAGE;
-  constexpr uint32_t TMEM_NEED = MT * NCOL;
+  constexpr uint32_t ACC_COLS = MT * NCOL;  // one accumulator buffer
+  constexpr uint32_t TMEM_NEED = 2 * ACC_COLS;
   constexpr uint32_t TMEM_COLS = TMEM_NEED <= 32 ? 32 : TMEM_NEED <= 64 ? 64 : TMEM_NEED <= 128 ? 128
                                  : TMEM_NEED <= 256 ? 256 : 512;
   constexpr uint32_t IDESC = idesc_bf16(NCOL, false, false);
+  // running sums of the drain warps: FP64 when they fit in registers
+  using Acc = typename std::conditional<(MT * KP <= 64), double, float>::type;
 
   extern __shared__ uint8_t smem_raw[];
-  __shared__ uint64_t bars[2 * 8 + 1];
+  __shared__ uint64_t bars[2 * 8 + 4];
   __shared__ uint32_t tmem_base_sh;
   __shared__ int abort_sh;
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const uint32_t smem0 = smem_u32(smem);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t nchunks = (L + TC_BK - 1) / TC_BK;
-  const int64_t c_begin = (int64_t)blockIdx.y * chunks_per_split;
-  int64_t c_end = c_begin + chunks_per_split;
-  if (c_end > nchunks) c_end = nchunks;
+  const int64_t ns = gridDim.y;
+  const int64_t y = blockIdx.y;
+  const int64_t my_chunks = y < nchunks ? (nchunks - y + ns - 1) / ns : 0;
+  const int64_t ngroups = (my_chunks + TCL_GROUP - 1) / TCL_GROUP;
   const int j0 = blockIdx.x * MT * TC_BM;
   auto full = [&](int s) { return smem_u32(&bars[s]); };
   auto empty = [&](int s) { return smem_u32(&bars[8 + s]); };
-  const uint32_t accf = smem_u32(&bars[16]);
+  auto accf = [&](int b) { return smem_u32(&bars[16 + b]); };
+  auto acce = [&](int b) { return smem_u32(&bars[18 + b]); };
 
   if (threadIdx.x == 0) {
     abort_sh = 0;
@@ -410,7 +426,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       mbar_init(full(s), 1 + 4);  // TMA expect_tx arrival + 4 producer warps
       mbar_init(empty(s), 1);
     }
-    mbar_init(accf, 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(accf(b), 1);
+      mbar_init(acce(b), 4);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   if (warp == 1) tmem_alloc(smem_u32(&tmem_base_sh), TMEM_COLS);
@@ -423,7 +442,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (lane == 0) {
       int s = 0;
       uint32_t ph = 0;
-      for (int64_t c = c_begin; c < c_end; ++c) {
+      for (int64_t i = 0; i < my_chunks; ++i) {
+        const int64_t c = y + i * ns;
         if (!mbar_wait(empty(s), ph ^ 1, abort_flag, status)) break;
         const uint32_t st = smem0 + s * STAGE;
         mbar_expect_tx(full(s), A_STAGE);
@@ -438,80 +458,107 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (lane == 0) {
       int s = 0;
       uint32_t ph = 0;
-      bool any = false;
-      for (int64_t c = c_begin; c < c_end; ++c) {
-        if (!mbar_wait(full(s), ph, abort_flag, status)) break;
+      uint32_t aph[2] = {0, 0};
+      bool ok = true;
+      int64_t i = 0;
+      for (int64_t g = 0; g < ngroups && ok; ++g) {
+        const int buf = (int)(g & 1);
+        if (!mbar_wait(acce(buf), aph[buf] ^ 1, abort_flag, status)) break;
         tc_fence_after();
-        const uint32_t st = smem0 + s * STAGE;
+        const uint32_t d = tmem + buf * ACC_COLS;
+        const int64_t iend = (i + TCL_GROUP < my_chunks) ? i + TCL_GROUP : my_chunks;
+        for (int64_t i0 = i; i < iend; ++i) {
+          if (!mbar_wait(full(s), ph, abort_flag, status)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t st = smem0 + s * STAGE;
 #pragma unroll
-        for (int kk = 0; kk < TC_BK / 16; ++kk) {
-          const uint64_t bdesc = smem_desc(st + A_STAGE + kk * 32, 16, 1024);
+          for (int kk = 0; kk < TC_BK / 16; ++kk) {
+            const uint64_t bdesc = smem_desc(st + A_STAGE + kk * 32, 16, 1024);
 #pragma unroll
-          for (int mt = 0; mt < MT; ++mt) {
-            const uint64_t adesc = smem_desc(st + mt * A_TILE + kk * 32, 16, 1024);
-            umma_bf16(tmem + mt * NCOL, adesc, bdesc, IDESC, (c != c_begin || kk != 0) ? 1u : 0u);
-            if (X2) {
-              const uint64_t adesc2 = smem_desc(st + A_BYTES + mt * A_TILE + kk * 32, 16, 1024);
-              umma_bf16(tmem + mt * NCOL, adesc2, bdesc, IDESC, 1);
+            for (int mt = 0; mt < MT; ++mt) {
+              const uint64_t adesc = smem_desc(st + mt * A_TILE + kk * 32, 16, 1024);
+              umma_bf16(d + mt * NCOL, adesc, bdesc, IDESC, (i != i0 || kk != 0) ? 1u : 0u);
+              if (X2) {
+                const uint64_t adesc2 = smem_desc(st + A_BYTES + mt * A_TILE + kk * 32, 16, 1024);
+                umma_bf16(d + mt * NCOL, adesc2, bdesc, IDESC, 1);
+              }
             }
           }
+          umma_commit(empty(s));
+          if (++s == stages) { s = 0; ph ^= 1; }
         }
-        any = true;
-        umma_commit(empty(s));
-        if (++s == stages) { s = 0; ph ^= 1; }
+        if (!ok) break;
+        umma_commit(accf(buf));
+        aph[buf] ^= 1;
       }
-      if (any) umma_commit(accf);
     }
-  } else {
-    // producer warps 2..5 build the Khatri-Rao B tile, then run the epilogue
+  } else if (warp < 6) {
+    // producer warps 2..5 build the Khatri-Rao B tile of every chunk
     const int pt = threadIdx.x - 64;  // 0..127
     int s = 0;
     uint32_t ph = 0;
-    bool ok = true;
-    for (int64_t c = c_begin; c < c_end; ++c) {
-      if (!mbar_wait(empty(s), ph ^ 1, abort_flag, status)) { ok = false; break; }
+    // 64 values of l x KP ranks per stage; thread pt handles l = c*64 + (pt & 63)
+    // and ranks r = (pt >> 6) + 2i; the row's mode digits advance per chunk
+    const int kk = pt & (TC_BK - 1);
+    WIdx wi;
+    widx_init(wg, y * TC_BK + kk, wi);
+    for (int64_t i = 0; i < my_chunks; ++i) {
+      const int64_t c = y + i * ns;
+      if (!mbar_wait(empty(s), ph ^ 1, abort_flag, status)) break;
       uint8_t* bt = smem + s * STAGE + A_STAGE;
-      // 64 values of l x KP ranks; thread pt handles l = pt & 63, ranks r = (pt >> 6) + 2i
-      const int kk = pt & (TC_BK - 1);
       const int64_t l = c * TC_BK + kk;
+#pragma unroll 4
       for (int r = pt >> 6; r < KP; r += 2) {
         __nv_bfloat16 hi = __float2bfloat16(0.f), lo = __float2bfloat16(0.f);
-        if (l < L && r < k) split_bf16(wgen_eval(wg, l, r, k), hi, lo);
+        if (l < L && r < k) split_bf16(wgen_row(wg, wi, r, k), hi, lo);
         *reinterpret_cast<__nv_bfloat16*>(bt + sw128_kmajor_off(r, kk)) = hi;
         *reinterpret_cast<__nv_bfloat16*>(bt + sw128_kmajor_off(KP + r, kk)) = lo;
       }
+      widx_advance(wg, wi, TC_BK * ns);
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive(full(s));
       if (++s == stages) { s = 0; ph ^= 1; }
     }
-    if (ok && c_end > c_begin) {
-      const int q = warp & 3;
-      if (mbar_wait(accf, 0, abort_flag, status)) {
-        tc_fence_after();
-        double* dst = part + (int64_t)blockIdx.y * R * k;
-        for (int mt = 0; mt < MT; ++mt) {
-          float v[NCOL];
+  } else {
+    // drain warps 6..9: TMEM lane quarter = warp % 4
+    const int q = warp & 3;
+    Acc sum[MT][KP];
 #pragma unroll
-          for (int cc = 0; cc < NCOL; cc += 32)
-            tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + mt * NCOL + cc, v + cc);
-          const int64_t j = (int64_t)j0 + mt * TC_BM + q * 32 + lane;
-          if (j < R) {
+    for (int mt = 0; mt < MT; ++mt)
 #pragma unroll
-            for (int r = 0; r < KP; ++r)
-              if (r < k) dst[j * k + r] = (double)v[r] + (double)v[KP + r];
-          }
+      for (int r = 0; r < KP; ++r) sum[mt][r] = 0;
+    uint32_t aph[2] = {0, 0};
+    bool ok = true;
+    for (int64_t g = 0; g < ngroups; ++g) {
+      const int buf = (int)(g & 1);
+      if (!mbar_wait(accf(buf), aph[buf], abort_flag, status)) { ok = false; break; }
+      tc_fence_after();
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt) {
+#pragma unroll
+        for (int cc = 0; cc < NCOL; cc += 32) {
+          float v[32];
+          tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + buf * ACC_COLS + mt * NCOL + cc, v);
+#pragma unroll
+          for (int i = 0; i < 32; ++i) sum[mt][(cc + i) % KP] += (Acc)v[i];  // hi then lo column
         }
-        tc_fence_before();
       }
-    } else if (c_end <= c_begin) {
-      // no work: this split contributes zeros
-      const int q = warp & 3;
-      double* dst = part + (int64_t)blockIdx.y * R * k;
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acce(buf));
+      aph[buf] ^= 1;
+    }
+    if (ok) {
+      double* dst = part + y * R * k;
+#pragma unroll
       for (int mt = 0; mt < MT; ++mt) {
         const int64_t j = (int64_t)j0 + mt * TC_BM + q * 32 + lane;
-        if (j < R)
-          for (int r = 0; r < k; ++r) dst[j * k + r] = 0.0;
+        if (j < R) {
+#pragma unroll
+          for (int r = 0; r < KP; ++r)
+            if (r < k) dst[j * k + r] = (double)sum[mt][r];
+        }
       }
     }
   }
@@ -635,23 +682,20 @@ inline int tc_stages(uint32_t stage_bytes) {
 
 inline int tc_left_mt(int64_t R) { return R > 128 ? 2 : 1; }
 
-inline void tc_left_plan(const TcTensor& t, int sm_count, int* mgroups, int* nsplit,
-                         int64_t* per) {
+inline void tc_left_plan(const TcTensor& t, int sm_count, int* mgroups, int* nsplit) {
   const int MT = tc_left_mt(t.R);
   *mgroups = (int)((t.R + MT * TC_BM - 1) / (MT * TC_BM));
   int ns = sm_count / *mgroups;
   if (ns < 1) ns = 1;
   const int64_t nch = (t.L + TC_BK - 1) / TC_BK;
   if (ns > nch) ns = (int)nch;
-  *per = (nch + ns - 1) / ns;
-  *nsplit = (int)((nch + *per - 1) / *per);
+  *nsplit = ns;
 }
 
 inline size_t tc_scratch_elems(const TcTensor& t, int sm_count, int k) {
   if (!t.hi) return 0;
   int mg, ns;
-  int64_t per;
-  tc_left_plan(t, sm_count, &mg, &ns, &per);
+  tc_left_plan(t, sm_count, &mg, &ns);
   return (size_t)ns * t.R * k;
 }
 
@@ -734,13 +778,12 @@ template <int KP, int MT, bool X2>
 inline void tc_left_launch(const TcTensor& t, const WGen& wg, int k, double* part, int* status,
                            int sm_count, cudaStream_t st, int* nsplit_out) {
   int mg, ns;
-  int64_t per;
-  tc_left_plan(t, sm_count, &mg, &ns, &per);
+  tc_left_plan(t, sm_count, &mg, &ns);
   constexpr uint32_t STAGE = (X2 ? 2 : 1) * MT * TC_BM * TC_BK * 2 + 2 * KP * 128;
   const int stages = tc_stages(STAGE);
   const size_t smem = (size_t)stages * STAGE + 1024;
-  k_tc_left<KP, MT, X2><<<dim3(mg, ns), TC_THREADS, smem, st>>>(t.mL_hi, t.mL_lo, wg, t.L, t.R, k,
-                                                                stages, per, part, status);
+  k_tc_left<KP, MT, X2><<<dim3(mg, ns), TCL_THREADS, smem, st>>>(t.mL_hi, t.mL_lo, wg, t.L, t.R, k,
+                                                                 stages, part, status);
   *nsplit_out = ns;
 }
 
