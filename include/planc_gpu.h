@@ -141,6 +141,34 @@ int planc_gpu_bpp_solve(planc_gpu_ctx* ctx, const double* AtA, const double* AtB
                         int n, int64_t ncols, double* X, int32_t* passive,
                         int32_t* iters);
 
+/* MTTKRP of `mode` for caller-supplied DEVICE factors F_dev[n] (row-major
+ * I_n x k FP64, k = the rank set by planc_gpu_set_factors, on the context's
+ * device), written to the device buffer M_dev (row-major I_mode x k FP64).
+ * The context's own factors are not touched. flags: bit 0 = dimension tree
+ * (N in {3,4}); bit 1 = reuse the partial MTTKRP left by the previous call of
+ * mode 0 (and, for N = 4 mode 2, of mode 1) made with the same factors, the
+ * in-order reuse of DenseDimensionTree::in_order_reuse_MTTKRP
+ * (dimtree/ddt.hpp:134-243). Runs on the context's stream and returns without
+ * synchronising. This is the adjoint used by the differentiable CP loss. */
+int planc_gpu_mttkrp_device(planc_gpu_ctx* ctx, int mode, const double* const* F_dev,
+                            double* M_dev, int flags);
+
+/* ||X||^2 of the context's tensor in FP64 (Tensor::norm,
+ * common/tensor.hpp:350-356), written to host memory. */
+int planc_gpu_tensor_norm2(planc_gpu_ctx* ctx, double* out);
+
+/* Lowers the BPP iteration cap (0 restores the reference's 5k,
+ * nnls/bppnnls.hpp:69). Used to exercise the "BPP failed" path
+ * (PLANC_GPU_ERR_BPP_MAXITER) without a pathological input. */
+int planc_gpu_set_bpp_max_iter(planc_gpu_ctx* ctx, int max_iter);
+
+/* Self-test of the kernels' bounded waits: launches one thread that waits on
+ * a barrier nothing ever signals, with a limit of `seconds` (0 < s <= 5).
+ * The wait runs out, the kernel writes the timeout status and returns; the
+ * status the device wrote is returned in *status_out (PLANC_GPU_ERR_TIMEOUT
+ * when the bounded-wait path works) and the device stays usable. */
+int planc_gpu_selftest_wait_timeout(int device, double seconds, int* status_out);
+
 /* Kernel timing, for roofline measurement: while enabled, CUDA events bracket
  * every launch of each kernel class on the context's stream. Class ids:
  *   0 partial MTTKRP, right contraction (P = X * F_last) and direct mode 0,

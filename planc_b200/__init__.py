@@ -36,7 +36,8 @@ EXPORTS = [
     "planc_gpu_get_factors", "planc_gpu_mttkrp", "planc_gpu_gram_loo",
     "planc_gpu_objective_error", "planc_gpu_mode_begin", "planc_gpu_mode_end",
     "planc_gpu_bpp_solve", "planc_gpu_set_timing", "planc_gpu_get_kernel_times",
-    "planc_gpu_launch_count", "planc_gpu_synth_cp_tensor",
+    "planc_gpu_launch_count", "planc_gpu_synth_cp_tensor", "planc_gpu_mttkrp_device",
+    "planc_gpu_tensor_norm2", "planc_gpu_set_bpp_max_iter", "planc_gpu_selftest_wait_timeout",
 ]
 
 
@@ -82,6 +83,10 @@ def load():
     L.planc_gpu_launch_count.restype = i64
     L.planc_gpu_synth_cp_tensor.argtypes = [i32, vp, i32, pi64, i32, P(pd), i32, d, ctypes.c_uint64,
                                             i32, vp]
+    L.planc_gpu_mttkrp_device.argtypes = [vp, i32, P(vp), vp, i32]
+    L.planc_gpu_tensor_norm2.argtypes = [vp, pd]
+    L.planc_gpu_set_bpp_max_iter.argtypes = [vp, i32]
+    L.planc_gpu_selftest_wait_timeout.argtypes = [i32, d, P(i32)]
     for name in EXPORTS:
         getattr(L, name).restype = getattr(L, name).restype or i32
     L.planc_gpu_last_error.restype = ctypes.c_char_p
@@ -226,6 +231,21 @@ class Context:
             it.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))))
         return X.T.copy(), P.T.copy(), it
 
+    def mttkrp_device(self, mode, factor_ptrs, out_ptr, dimtree=True, reuse=False):
+        """MTTKRP of `mode` for device factors (pointers to row-major (I_n, k)
+        float64 buffers) into the device buffer out_ptr; stream-ordered."""
+        arr = (ctypes.c_void_p * len(factor_ptrs))(*[int(p) for p in factor_ptrs])
+        _check(load().planc_gpu_mttkrp_device(self.h, mode, arr, ctypes.c_void_p(int(out_ptr)),
+                                              int(dimtree) | (2 if reuse else 0)))
+
+    def tensor_norm2(self):
+        v = ctypes.c_double()
+        _check(load().planc_gpu_tensor_norm2(self.h, ctypes.byref(v)))
+        return v.value
+
+    def set_bpp_max_iter(self, n):
+        _check(load().planc_gpu_set_bpp_max_iter(self.h, int(n)))
+
     def set_timing(self, on):
         _check(load().planc_gpu_set_timing(self.h, int(on)))
 
@@ -239,6 +259,13 @@ class Context:
 
     def launch_count(self):
         return int(load().planc_gpu_launch_count(self.h))
+
+
+def selftest_wait_timeout(device=0, seconds=0.05):
+    """Runs the bounded-wait self-test; returns the status the kernel wrote."""
+    st = ctypes.c_int32()
+    _check(load().planc_gpu_selftest_wait_timeout(device, float(seconds), ctypes.byref(st)))
+    return st.value
 
 
 def synth_cp_tensor(device, x_dev_ptr, dtype, dims, A, sigma, seed, clip=True, stream=None):

@@ -1,0 +1,102 @@
+"""Differentiable CP reconstruction loss on the B200 kernels.
+
+    loss(F_0..F_{N-1}) = 1/2 ||X - [[F_0, ..., F_{N-1}]]||^2
+                       = 1/2 ||X||^2 - <M_0, F_0> + 1/2 sum(*_n F_n^T F_n)
+
+with M_n the mode-n MTTKRP. The gradient is the reference's NTF gradient form
+(ntf/ntfnes.hpp:138-147, G_{-n} H^T - M^T in its k x I layout):
+
+    d loss / d F_n = F_n (*_{m != n} F_m^T F_m) - M_n
+
+The forward pass runs the mode-0 MTTKRP on the tensor-core (or FP64) kernel
+of a planc_b200.Context; the hand-written backward runs the remaining modes'
+MTTKRPs on the same kernels (mode 1 reuses the dimension tree's partial
+contraction from the forward pass, the last mode is the left contraction), so
+one forward + backward reads X twice. Factors are float64 CUDA tensors of
+shape (I_n, k), contiguous (row-major, the library's factor layout).
+"""
+import torch
+
+from . import Context
+
+
+def _hadamard_grams(grams, skip=None):
+    H = None
+    for i, g in enumerate(grams):
+        if i == skip:
+            continue
+        H = g.clone() if H is None else H * g
+    return H
+
+
+class _CPLoss(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, handle, *factors):
+        factors = [f.contiguous() for f in factors]
+        dev = factors[0].device
+        stream = torch.cuda.ExternalStream(handle.stream, device=dev)
+        M0 = torch.empty_like(factors[0])
+        ptrs = [f.data_ptr() for f in factors]
+        stream.wait_stream(torch.cuda.current_stream(dev))
+        handle.mttkrp_device(0, ptrs, M0.data_ptr(), dimtree=True, reuse=False)
+        torch.cuda.current_stream(dev).wait_stream(stream)
+        grams = [f.T @ f for f in factors]
+        inner = (M0 * factors[0]).sum()
+        loss = 0.5 * handle._norm2 - inner + 0.5 * _hadamard_grams(grams).sum()
+        ctx.handle = handle
+        ctx.save_for_backward(M0, *factors)
+        return loss
+
+    @staticmethod
+    def backward(ctx, g):
+        M0, *factors = ctx.saved_tensors
+        handle = ctx.handle
+        dev = factors[0].device
+        stream = torch.cuda.ExternalStream(handle.stream, device=dev)
+        ptrs = [f.data_ptr() for f in factors]
+        N = len(factors)
+        s = N // 2
+        Ms = [M0]
+        stream.wait_stream(torch.cuda.current_stream(dev))
+        for n in range(1, N):
+            Mn = torch.empty_like(factors[n])
+            # modes 1..s reuse the partial contraction of the forward's mode 0
+            handle.mttkrp_device(n, ptrs, Mn.data_ptr(), dimtree=True, reuse=(n <= s))
+            Ms.append(Mn)
+        torch.cuda.current_stream(dev).wait_stream(stream)
+        grams = [f.T @ f for f in factors]
+        grads = [g * (factors[n] @ _hadamard_grams(grams, skip=n) - Ms[n]) for n in range(N)]
+        return (None, *grads)
+
+
+class CPLoss:
+    """Holds the tensor on the device; call with the factor leaves.
+
+        loss_fn = CPLoss(X_device_ptr_or_array, dims, rank, precision="bf16")
+        loss = loss_fn(A, B, C); loss.backward()
+    """
+
+    def __init__(self, X, dims=None, rank=None, precision="fp64", device=0, dtype="f32"):
+        import numpy as np
+        self.ctx = Context(device, precision)
+        if isinstance(X, torch.Tensor):
+            X = X.contiguous()
+            dims = tuple(dims)
+            self.ctx.set_tensor(X.data_ptr(), dims=dims, dtype="f32" if X.dtype == torch.float32 else "f64")
+        else:
+            self.ctx.set_tensor(X)
+            dims = X.shape
+        self.dims = tuple(int(d) for d in dims)
+        self.rank = rank
+        # factors of the right rank give the context its buffers; their values are unused
+        self.ctx.set_factors([np.ones((d, rank)) for d in self.dims])
+        self.ctx._norm2 = self.ctx.tensor_norm2()
+
+    def __call__(self, *factors):
+        for f, d in zip(factors, self.dims):
+            if f.dtype != torch.float64 or not f.is_cuda or tuple(f.shape) != (d, self.rank):
+                raise ValueError("factors must be float64 CUDA tensors of shape (I_n, rank)")
+        return _CPLoss.apply(self.ctx, *factors)
+
+    def close(self):
+        self.ctx.close()

@@ -121,7 +121,7 @@ __global__ void __launch_bounds__(32 * BPP_WARPS) k_bpp(const double* __restrict
                                                         int64_t ncols, double* __restrict__ Xout,
                                                         int* __restrict__ passive_out,
                                                         int* __restrict__ iters_out,
-                                                        int* __restrict__ status) {
+                                                        int* __restrict__ status, int max_iter_override) {
   __shared__ double sA[BPP_WARPS][KP * KP];
   __shared__ double sx[BPP_WARPS][KP], sy[BPP_WARPS][KP], sb[BPP_WARPS][KP];
   __shared__ double sz[BPP_WARPS][KP];
@@ -145,7 +145,8 @@ __global__ void __launch_bounds__(32 * BPP_WARPS) k_bpp(const double* __restrict
   uint64_t passive = 0;  // PassiveSet = (X > 0) = {}, bppnnls.hpp:74
   const int pbar = 3;
   int P = pbar, Ninf = n + 1;  // bppnnls.hpp:76-81
-  const unsigned max_it = 5u * (unsigned)n;  // bppnnls.hpp:69
+  // bppnnls.hpp:69 (MAX_ITERATIONS = 5n); a positive override lowers the cap
+  const unsigned max_it = max_iter_override > 0 ? (unsigned)max_iter_override : 5u * (unsigned)n;
   auto classify = [&](uint64_t& nonopt, uint64_t& infea) {
     bool lo_no = has_lo && (y[lane] < 0) && !((passive >> lane) & 1);
     bool hi_no = has_hi && (y[lane + 32] < 0) && !((passive >> (lane + 32)) & 1);

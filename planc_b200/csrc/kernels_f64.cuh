@@ -76,6 +76,8 @@ __global__ void __launch_bounds__(256) k_contract_f64(const double* __restrict__
         int64_t gj = j0 + kk;
         xr[i] = (gm < g.M && gj < g.A) ? X[gm + g.ldx * gj] : 0.0;
       }
+      WIdx base;
+      if (wg.nf > 1) widx_init(wg, j0, base);
 #pragma unroll
       for (int i = 0; i < (BK * KP + 255) / 256; ++i) {
         int e = tid + 256 * i;
@@ -83,7 +85,15 @@ __global__ void __launch_bounds__(256) k_contract_f64(const double* __restrict__
         if (e < BK * KP) {
           int kk = e / KP, r = e % KP;
           int64_t gj = j0 + kk;
-          if (r < k && gj < g.A) v = wgen_eval(wg, gj, r, k);
+          if (r < k && gj < g.A) {
+            if (wg.nf == 1) {
+              v = wg.f[0][gj * k + r];
+            } else {
+              WIdx w = base;
+              widx_advance(wg, w, kk);
+              v = wgen_row(wg, w, r, k);
+            }
+          }
         }
         wr[i] = v;
       }
@@ -98,6 +108,8 @@ __global__ void __launch_bounds__(256) k_contract_f64(const double* __restrict__
         int64_t gm = m0 + mm;
         xr[i] = (gm < g.M && ga < g.A) ? X[ga + g.ldx * gm + g.ldb * b] : 0.0;
       }
+      WIdx base;
+      widx_init(wg, a0 + g.A * b, base);
 #pragma unroll
       for (int i = 0; i < (BK * KP + 255) / 256; ++i) {
         int e = tid + 256 * i;
@@ -105,7 +117,11 @@ __global__ void __launch_bounds__(256) k_contract_f64(const double* __restrict__
         if (e < BK * KP) {
           int kk = e / KP, r = e % KP;
           int64_t gaa = a0 + kk;
-          if (r < k && gaa < g.A) v = wgen_eval(wg, gaa + g.A * b, r, k);
+          if (r < k && gaa < g.A) {
+            WIdx w = base;
+            widx_advance(wg, w, kk);
+            v = wgen_row(wg, w, r, k);
+          }
         }
         wr[i] = v;
       }
@@ -218,12 +234,28 @@ __global__ void __launch_bounds__(256) k_ttv_right(const TT* __restrict__ T, int
     out[(int64_t)blockIdx.y * split_stride + e] = 0.0;
     return;
   }
-  WIdx wi;
-  widx_init(wg, b0, wi);
   double s = 0.0;
-  for (int64_t b = b0; b < b1; ++b) {
-    s = fma((double)T[(a + A * b) * k + r], wgen_row(wg, wi, r, k), s);
-    widx_advance(wg, wi, 1);
+  const TT* Tp = T + (a + A * b0) * k + r;
+  const int64_t tstride = A * k;
+  if (wg.nf == 1) {
+    const double* W = wg.f[0] + r;
+    double s1 = 0.0;
+    int64_t b = b0;
+    for (; b + 1 < b1; b += 2) {
+      s = fma((double)Tp[0], W[b * k], s);
+      s1 = fma((double)Tp[tstride], W[(b + 1) * k], s1);
+      Tp += 2 * tstride;
+    }
+    if (b < b1) s = fma((double)Tp[0], W[b * k], s);
+    s += s1;
+  } else {
+    WIdx wi;
+    widx_init(wg, b0, wi);
+    for (int64_t b = b0; b < b1; ++b) {
+      s = fma((double)Tp[0], wgen_row(wg, wi, r, k), s);
+      Tp += tstride;
+      widx_advance(wg, wi, 1);
+    }
   }
   out[(int64_t)blockIdx.y * split_stride + e] = s;
 }

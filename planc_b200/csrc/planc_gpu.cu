@@ -110,6 +110,7 @@ struct planc_gpu_ctx {
   double kms[KC_COUNT] = {0};
   int64_t klaunch[KC_COUNT] = {0};
   int64_t launch_count = 0;
+  int bpp_max_iter = 0;  // 0: the reference's 5k cap
 };
 
 namespace {
@@ -232,9 +233,9 @@ struct TtvRightPlan {
 TtvRightPlan plan_ttv_right(planc_gpu_ctx* c, int64_t A, int64_t B) {
   TtvRightPlan p;
   int64_t gx = (A * c->k + 255) / 256;
-  int64_t target = 2 * (int64_t)c->sm_count;
-  int64_t ns = std::max<int64_t>(1, std::min<int64_t>((target + gx - 1) / gx, B));
-  ns = std::min<int64_t>(ns, 256);
+  int64_t target = 8 * (int64_t)c->sm_count;  // latency-bound loop: many warps per SM
+  int64_t ns = std::max<int64_t>(1, std::min<int64_t>((target + gx - 1) / gx, (B + 15) / 16));
+  ns = std::min<int64_t>(ns, 512);
   p.bper = (B + ns - 1) / ns;
   ns = (B + p.bper - 1) / p.bper;
   p.nsplit = (int)ns;
@@ -390,6 +391,7 @@ void partial_left(planc_gpu_ctx* c, double* out) {
   } else {
     WGen wg = make_wgen(c, modes);
     int nsplit = 0;
+    if (wg.nf < 2 || wg.nf > 3) fail(PLANC_GPU_ERR_UNSUPPORTED, "left contraction needs 2 or 3 modes");
     if (tc_scratch_elems(c->tct, c->sm_count, c->k) > c->scratch_elems)
       fail(PLANC_GPU_ERR_STATE, "internal: split-K scratch larger than planned");
     launch(c, KC_CONTRACT_LEFT, [&] {
@@ -480,7 +482,7 @@ void run_update(planc_gpu_ctx* c, int algo, int n) {
 #define CASE(KP)                                                                                   \
   case KP:                                                                                         \
     k_bpp<KP><<<blocks, 32 * BPP_WARPS, 0, c->stream>>>(c->Gloo, c->M[n], k, I, c->F[n], nullptr, \
-                                                        nullptr, c->status_dev);                   \
+                                                        nullptr, c->status_dev, c->bpp_max_iter);  \
     break;
         CASE(8) CASE(16) CASE(32) CASE(64)
 #undef CASE
@@ -704,6 +706,13 @@ int planc_gpu_set_tensor(planc_gpu_ctx* c, const void* X, int dtype, const int64
         k_sumsq_partial<float><<<nb, 256, 0, c->stream>>>((const float*)src, numel, part);
       k_reduce_splits<<<1, 32, 0, c->stream>>>(part, nb, 1, 1, c->normX2);
       CK(cudaGetLastError());
+      double nx = 0.0;
+      CK(cudaMemcpyAsync(&nx, c->normX2, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      if (!std::isfinite(nx)) {
+        cudaFree(part);
+        fail(PLANC_GPU_ERR_NONFINITE, "the tensor holds NaN or Inf values");
+      }
       if (c->precision == PLANC_GPU_PREC_FP64) {
         dalloc(&c->X64, (size_t)numel);
         if (dtype == PLANC_GPU_F64)
@@ -716,7 +725,8 @@ int planc_gpu_set_tensor(planc_gpu_ctx* c, const void* X, int dtype, const int64
           c->X64 = nullptr;
         }
         cudaError_t te =
-            tc_set_tensor(c->tct, src, dtype == PLANC_GPU_F64, c->L, c->R, c->precision, c->stream);
+            tc_set_tensor(c->tct, src, dtype == PLANC_GPU_F64, c->L, c->R, c->dims[0], c->precision,
+                          c->stream);
         if (te == cudaErrorInvalidValue)
           fail(PLANC_GPU_ERR_CUDA, "cuTensorMapEncodeTiled rejected the tensor map");
         CK(te);
@@ -980,7 +990,7 @@ int planc_gpu_bpp_solve(planc_gpu_ctx* c, const double* AtA, const double* AtB, 
 #define CASE(KP)                                                                            \
   case KP:                                                                                  \
     k_bpp<KP><<<blocks, 32 * BPP_WARPS, 0, c->stream>>>(dA, dB, n, ncols, dX, dP, dI,      \
-                                                        c->status_dev);                     \
+                                                        c->status_dev, c->bpp_max_iter);    \
     break;
           CASE(8) CASE(16) CASE(32) CASE(64)
 #undef CASE
@@ -997,6 +1007,81 @@ int planc_gpu_bpp_solve(planc_gpu_ctx* c, const double* AtA, const double* AtB, 
       throw;
     }
     cleanup();
+  });
+}
+
+int planc_gpu_mttkrp_device(planc_gpu_ctx* c, int mode, const double* const* F_dev, double* M_dev,
+                            int flags) {
+  return guarded([&] {
+    require_ready(c);
+    if (mode < 0 || mode >= c->N || !F_dev || !M_dev) fail(PLANC_GPU_ERR_ARG, "bad mode or null pointer");
+    for (int n = 0; n < c->N; ++n)
+      if (!F_dev[n]) fail(PLANC_GPU_ERR_ARG, "null factor");
+    set_device(c);
+    ensure_buffers(c);
+    const bool dt = (flags & 1) && (c->N == 3 || c->N == 4);
+    const bool reuse = (flags & 2) != 0;
+    if (c->precision != PLANC_GPU_PREC_FP64 && !dt)
+      fail(PLANC_GPU_ERR_UNSUPPORTED, "tensor-core precisions run the dimension tree only");
+    double* saved[kMaxModes];
+    for (int n = 0; n < c->N; ++n) {
+      saved[n] = c->F[n];
+      c->F[n] = const_cast<double*>(F_dev[n]);
+    }
+    try {
+      if (dt) {
+        if (mode >= 1 && mode <= c->s && !reuse) {
+          mttkrp_dimtree(c, 0, c->M[0]);
+          if (c->N == 4 && mode == 2) mttkrp_dimtree(c, 1, c->M[1]);
+        }
+        mttkrp_dimtree(c, mode, M_dev);
+      } else {
+        mttkrp_direct(c, mode, M_dev);
+      }
+    } catch (...) {
+      for (int n = 0; n < c->N; ++n) c->F[n] = saved[n];
+      throw;
+    }
+    for (int n = 0; n < c->N; ++n) c->F[n] = saved[n];
+  });
+}
+
+int planc_gpu_tensor_norm2(planc_gpu_ctx* c, double* out) {
+  return guarded([&] {
+    if (!c || !out) fail(PLANC_GPU_ERR_ARG, "null argument");
+    if (!c->have_tensor) fail(PLANC_GPU_ERR_STATE, "no tensor set");
+    set_device(c);
+    CK(cudaMemcpyAsync(out, c->normX2, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int planc_gpu_set_bpp_max_iter(planc_gpu_ctx* c, int max_iter) {
+  return guarded([&] {
+    if (!c || max_iter < 0) fail(PLANC_GPU_ERR_ARG, "bad argument");
+    c->bpp_max_iter = max_iter;
+    reset_graph(c);
+  });
+}
+
+int planc_gpu_selftest_wait_timeout(int device, double seconds, int* status_out) {
+  return guarded([&] {
+    if (!status_out || !(seconds > 0) || seconds > 5) fail(PLANC_GPU_ERR_ARG, "bad argument");
+    CK(cudaSetDevice(device));
+    int clk_khz = 0;
+    CK(cudaDeviceGetAttribute(&clk_khz, cudaDevAttrClockRate, device));
+    long long limit = (long long)(seconds * (double)clk_khz * 1e3);
+    int* st = nullptr;
+    CK(cudaMalloc(&st, sizeof(int)));
+    cudaMemset(st, 0, sizeof(int));
+    k_tc_wait_selftest<<<1, 32>>>(limit, st);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    int h = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&h, st, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(st);
+    cuda_check(e, "wait self-test");
+    *status_out = h;
   });
 }
 

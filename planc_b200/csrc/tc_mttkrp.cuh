@@ -68,13 +68,13 @@ constexpr long long kWaitCycles = 4000000000LL;  // ~2 s at 1.9 GHz
 // Bounded wait on phase `parity`. Returns false (and raises the abort flag)
 // when the wait runs out or another warp already aborted.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag,
-                                          int* status) {
+                                          int* status, long long limit = kWaitCycles) {
   if (mbar_try(bar, parity)) return true;
   long long t0 = clock64();
   while (true) {
     if (mbar_try(bar, parity)) return true;
     if (*abort_flag) return false;
-    if (clock64() - t0 > kWaitCycles) {
+    if (clock64() - t0 > limit) {
       *abort_flag = 1;
       atomicMin(status, kStTimeout);
       return false;
@@ -493,28 +493,86 @@ __global__ void __launch_bounds__(TCL_THREADS, 1)
       }
     }
   } else if (warp < 6) {
-    // producer warps 2..5 build the Khatri-Rao B tile of every chunk
-    const int pt = threadIdx.x - 64;  // 0..127
+    // producer warps 2..5 build the Khatri-Rao B tile of every chunk:
+    // thread pt owns rank r = pt % KP and octets of l (8 consecutive values,
+    // one 16-byte swizzled store per octet for hi and for lo); a warp's lanes
+    // read 32 consecutive ranks of a factor row (coalesced).
+    constexpr int OCT_LANES = 128 / KP;        // threads per rank
+    constexpr int OCT_PER = 8 / OCT_LANES;     // octets per thread per chunk
+    const int pt = threadIdx.x - 64;           // 0..127
+    const int r = pt % KP;
+    const int oct0 = pt / KP;
+    const bool rok = r < k;
+    const int nf = wg.nf;                      // 2 (N = 3) or 3 (N = 4)
+    const double* F0 = wg.f[0];
+    const double* F1 = wg.f[1];
+    const double* F2 = nf > 2 ? wg.f[2] : wg.f[1];
+    const int64_t D0 = wg.dim[0], D1 = wg.dim[1];
+    // digits of l0 = c * 64 for the first chunk of this split
+    int64_t b0, b1, b2;
+    {
+      const int64_t l0 = y * TC_BK;
+      b0 = l0 % D0;
+      b1 = (l0 / D0) % D1;
+      b2 = nf > 2 ? l0 / (D0 * D1) : 0;
+    }
+    const int64_t step = TC_BK * ns;  // l advance between this split's chunks
     int s = 0;
     uint32_t ph = 0;
-    // 64 values of l x KP ranks per stage; thread pt handles l = c*64 + (pt & 63)
-    // and ranks r = (pt >> 6) + 2i; the row's mode digits advance per chunk
-    const int kk = pt & (TC_BK - 1);
-    WIdx wi;
-    widx_init(wg, y * TC_BK + kk, wi);
     for (int64_t i = 0; i < my_chunks; ++i) {
       const int64_t c = y + i * ns;
       if (!mbar_wait(empty(s), ph ^ 1, abort_flag, status)) break;
       uint8_t* bt = smem + s * STAGE + A_STAGE;
-      const int64_t l = c * TC_BK + kk;
-#pragma unroll 4
-      for (int r = pt >> 6; r < KP; r += 2) {
-        __nv_bfloat16 hi = __float2bfloat16(0.f), lo = __float2bfloat16(0.f);
-        if (l < L && r < k) split_bf16(wgen_row(wg, wi, r, k), hi, lo);
-        *reinterpret_cast<__nv_bfloat16*>(bt + sw128_kmajor_off(r, kk)) = hi;
-        *reinterpret_cast<__nv_bfloat16*>(bt + sw128_kmajor_off(KP + r, kk)) = lo;
+#pragma unroll
+      for (int t = 0; t < OCT_PER; ++t) {
+        const int j = oct0 + OCT_LANES * t;  // octet 0..7
+        int64_t d0 = b0 + 8 * j, d1 = b1, d2 = b2;
+        while (d0 >= D0) { d0 -= D0; ++d1; }
+        if (nf > 2) while (d1 >= D1) { d1 -= D1; ++d2; }
+        const int64_t lbase = c * TC_BK + 8 * j;
+        // product of the slower modes' factor entries, constant along a run of l
+        auto tail_of = [&](int64_t e1, int64_t e2) -> float {
+          double tl = F1[e1 * k + r];
+          if (nf > 2) tl = tl * F2[e2 * k + r];
+          return (float)tl;
+        };
+        float tail = (rok && lbase < L) ? tail_of(d1, d2) : 0.f;
+        uint32_t hw[4], lw[4];
+#pragma unroll
+        for (int e = 0; e < 8; e += 2) {
+          float w[2];
+#pragma unroll
+          for (int u = 0; u < 2; ++u) {
+            w[u] = 0.f;
+            if (rok && lbase + e + u < L) w[u] = (float)F0[d0 * k + r] * tail;
+            if (++d0 == D0) {
+              d0 = 0;
+              if (++d1 == D1 && nf > 2) { d1 = 0; ++d2; }
+              if (rok && lbase + e + u + 1 < L) tail = tail_of(d1, d2);
+            }
+          }
+          // FP32 product split into BF16 hi + lo (w - hi is exact in FP32)
+          __nv_bfloat162 h2 = __floats2bfloat162_rn(w[0], w[1]);
+          float2 hf = __bfloat1622float2(h2);
+          __nv_bfloat162 l2 = __floats2bfloat162_rn(w[0] - hf.x, w[1] - hf.y);
+          hw[e >> 1] = *reinterpret_cast<uint32_t*>(&h2);
+          lw[e >> 1] = *reinterpret_cast<uint32_t*>(&l2);
+        }
+        *reinterpret_cast<uint4*>(bt + sw128_kmajor_off(r, 8 * j)) = make_uint4(hw[0], hw[1], hw[2], hw[3]);
+        *reinterpret_cast<uint4*>(bt + sw128_kmajor_off(KP + r, 8 * j)) = make_uint4(lw[0], lw[1], lw[2], lw[3]);
       }
-      widx_advance(wg, wi, TC_BK * ns);
+      // advance the chunk base digits by `step`
+      b0 += step;
+      if (b0 >= D0) {
+        int64_t q = b0 / D0;
+        b0 -= q * D0;
+        b1 += q;
+        if (nf > 2 && b1 >= D1) {
+          int64_t q2 = b1 / D1;
+          b1 -= q2 * D1;
+          b2 += q2;
+        }
+      }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncwarp();
       if (lane == 0) mbar_arrive(full(s));
@@ -571,6 +629,195 @@ __global__ void __launch_bounds__(TCL_THREADS, 1)
   }
 }
 
+// ------------------------------------------------------------ left kernel, factored form
+// When I_0 is a multiple of 64, every 64-wide chunk of l lies inside one run
+// of I_0 consecutive values of l that share the slower modes' digits, so the
+// Khatri-Rao row factors as W(l, r) = F_0[i_0, r] * tail(g, r) with
+// g = l / I_0 and tail = F_1[i_1, r] (* F_2[i_2, r]) (the reference's
+// product F_0 * (F_1 * F_2) up to rounding). Then
+//     M[j, r] = sum_g tail(g, r) * sum_{i_0} X[i_0 + I_0 g, j] * F_0[i_0, r]
+// The inner sums are tensor-core MMAs against a static operand, F_0 split into
+// BF16 hi|lo rows and pre-swizzled in global memory (one bulk copy per stage,
+// as in the right contraction); the accumulator of each run g is drained and
+// scaled by tail(g, .) in FP64 by four drain warps. No producer warps, and the
+// tensor-core accumulation chain is one run (I_0/64 chunks) long.
+// Split y takes runs y, y + nsplit, ..., so concurrent CTAs read adjacent
+// I_0-element pieces of the same rows of X.
+constexpr int TCF_THREADS = 192;  // warp 0 TMA, 1 MMA, 2-5 drain
+
+template <int KP, int MT, bool X2>
+__global__ void __launch_bounds__(TCF_THREADS, 1)
+    k_tc_left_fac(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
+                  const uint8_t* __restrict__ img0, const double* __restrict__ F1,
+                  const double* __restrict__ F2, int64_t D1, int64_t I0, int64_t L, int64_t R, int k,
+                  int stages, double* __restrict__ part, int* __restrict__ status) {
+  constexpr int NCOL = 2 * KP;
+  constexpr uint32_t A_TILE = TC_BM * TC_BK * 2;  // 16 KB
+  constexpr uint32_t A_BYTES = MT * A_TILE;
+  constexpr uint32_t A_STAGE = X2 ? 2 * A_BYTES : A_BYTES;
+  constexpr uint32_t B_STAGE = NCOL * 128;
+  constexpr uint32_t STAGE = A_STAGE + B_STAGE;
+  constexpr uint32_t ACC_COLS = MT * NCOL;
+  constexpr uint32_t TMEM_NEED = 2 * ACC_COLS;
+  constexpr uint32_t TMEM_COLS = TMEM_NEED <= 32 ? 32 : TMEM_NEED <= 64 ? 64 : TMEM_NEED <= 128 ? 128
+                                 : TMEM_NEED <= 256 ? 256 : 512;
+  constexpr uint32_t IDESC = idesc_bf16(NCOL, false, false);
+  using Acc = typename std::conditional<(MT * KP <= 64), double, float>::type;
+
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ uint64_t bars[2 * 8 + 4];
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ int abort_sh;
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const uint32_t smem0 = smem_u32(smem);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t G = I0 / TC_BK;          // chunks per run
+  const int64_t nruns = L / I0;
+  const int64_t ns = gridDim.y;
+  const int64_t y = blockIdx.y;
+  const int64_t my_runs = y < nruns ? (nruns - y + ns - 1) / ns : 0;
+  const int j0 = blockIdx.x * MT * TC_BM;
+  auto full = [&](int s) { return smem_u32(&bars[s]); };
+  auto empty = [&](int s) { return smem_u32(&bars[8 + s]); };
+  auto accf = [&](int b) { return smem_u32(&bars[16 + b]); };
+  auto acce = [&](int b) { return smem_u32(&bars[18 + b]); };
+
+  if (threadIdx.x == 0) {
+    abort_sh = 0;
+    for (int s = 0; s < stages; ++s) {
+      mbar_init(full(s), 1);
+      mbar_init(empty(s), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(accf(b), 1);
+      mbar_init(acce(b), 4);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) tmem_alloc(smem_u32(&tmem_base_sh), TMEM_COLS);
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+  volatile int* abort_flag = &abort_sh;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      bool ok = true;
+      for (int64_t i = 0; i < my_runs && ok; ++i) {
+        const int64_t g = y + i * ns;
+        for (int64_t q = 0; q < G; ++q) {
+          const int64_t c = g * G + q;
+          if (!mbar_wait(empty(s), ph ^ 1, abort_flag, status)) { ok = false; break; }
+          const uint32_t st = smem0 + s * STAGE;
+          mbar_expect_tx(full(s), STAGE);
+          for (int mt = 0; mt < MT; ++mt) {
+            tma_load_2d(st + mt * A_TILE, &tm_hi, (int)(c * TC_BK), j0 + mt * TC_BM, full(s));
+            if (X2) tma_load_2d(st + A_BYTES + mt * A_TILE, &tm_lo, (int)(c * TC_BK), j0 + mt * TC_BM, full(s));
+          }
+          bulk_load(st + A_STAGE, img0 + (size_t)q * B_STAGE, B_STAGE, full(s));
+          if (++s == stages) { s = 0; ph ^= 1; }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      uint32_t aph[2] = {0, 0};
+      bool ok = true;
+      for (int64_t i = 0; i < my_runs && ok; ++i) {
+        const int buf = (int)(i & 1);
+        if (!mbar_wait(acce(buf), aph[buf] ^ 1, abort_flag, status)) break;
+        tc_fence_after();
+        const uint32_t d = tmem + buf * ACC_COLS;
+        for (int64_t q = 0; q < G; ++q) {
+          if (!mbar_wait(full(s), ph, abort_flag, status)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t st = smem0 + s * STAGE;
+#pragma unroll
+          for (int kk = 0; kk < TC_BK / 16; ++kk) {
+            const uint64_t bdesc = smem_desc(st + A_STAGE + kk * 32, 16, 1024);
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt) {
+              const uint64_t adesc = smem_desc(st + mt * A_TILE + kk * 32, 16, 1024);
+              umma_bf16(d + mt * NCOL, adesc, bdesc, IDESC, (q != 0 || kk != 0) ? 1u : 0u);
+              if (X2) {
+                const uint64_t adesc2 = smem_desc(st + A_BYTES + mt * A_TILE + kk * 32, 16, 1024);
+                umma_bf16(d + mt * NCOL, adesc2, bdesc, IDESC, 1);
+              }
+            }
+          }
+          umma_commit(empty(s));
+          if (++s == stages) { s = 0; ph ^= 1; }
+        }
+        if (!ok) break;
+        umma_commit(accf(buf));
+        aph[buf] ^= 1;
+      }
+    }
+  } else {
+    // drain warps 2..5: TMEM lane quarter = warp % 4
+    const int q4 = warp & 3;
+    Acc sum[MT][KP];
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+      for (int r = 0; r < KP; ++r) sum[mt][r] = 0;
+    uint32_t aph[2] = {0, 0};
+    bool ok = true;
+    for (int64_t i = 0; i < my_runs; ++i) {
+      const int buf = (int)(i & 1);
+      const int64_t g = y + i * ns;
+      const int64_t i1 = F2 ? g % D1 : g;
+      const int64_t i2 = F2 ? g / D1 : 0;
+      if (!mbar_wait(accf(buf), aph[buf], abort_flag, status)) { ok = false; break; }
+      tc_fence_after();
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt) {
+#pragma unroll
+        for (int cc = 0; cc < NCOL; cc += 32) {
+          float v[32];
+          tmem_ld32(tmem + ((uint32_t)(q4 * 32) << 16) + buf * ACC_COLS + mt * NCOL + cc, v);
+#pragma unroll
+          for (int e = 0; e < 32; ++e) {
+            const int r = (cc + e) % KP;  // hi column, then lo column
+            if (r < k) {
+              double t = F1[i1 * k + r];
+              if (F2) t = t * F2[i2 * k + r];
+              sum[mt][r] += (Acc)(t * (double)v[e]);
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acce(buf));
+      aph[buf] ^= 1;
+    }
+    if (ok) {
+      double* dst = part + y * R * k;
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt) {
+        const int64_t j = (int64_t)j0 + mt * TC_BM + q4 * 32 + lane;
+        if (j < R) {
+#pragma unroll
+          for (int r = 0; r < KP; ++r)
+            if (r < k) dst[j * k + r] = (double)sum[mt][r];
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (abort_sh) tc_drain_after_abort();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, TMEM_COLS);
+  }
+}
+
 // X (f32/f64, L x R column-major) -> BF16 hi (and lo) with leading dim Lpad.
 template <typename T>
 __global__ void k_tc_convert(const T* __restrict__ X, int64_t L, int64_t R, int64_t Lpad,
@@ -586,6 +833,25 @@ __global__ void k_tc_convert(const T* __restrict__ X, int64_t L, int64_t R, int6
   }
 }
 
+// Self-test of the bounded-wait path: one thread waits on an mbarrier that no
+// one ever arrives on, with a limit of `limit` cycles; the wait runs out, sets
+// *status = kStTimeout and the kernel returns normally.
+__global__ void k_tc_wait_selftest(long long limit, int* status) {
+  __shared__ uint64_t bar;
+  __shared__ int abort_sh;
+  if (threadIdx.x == 0) {
+    abort_sh = 0;
+    mbar_init(smem_u32(&bar), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    bool ok = mbar_wait(smem_u32(&bar), 0, &abort_sh, status, limit);
+    if (ok) atomicExch(status, 1);  // cannot happen: nothing arrives
+  }
+  __syncthreads();
+}
+
 // ------------------------------------------------------------ host side
 struct TcTensor {
   __nv_bfloat16* hi = nullptr;
@@ -593,9 +859,12 @@ struct TcTensor {
   int64_t L = 0, R = 0, Lpad = 0;
   int prec = 0;
   CUtensorMap mR_hi, mR_lo, mL_hi, mL_lo;
-  uint8_t* bimg = nullptr;
+  uint8_t* bimg = nullptr;   // B image of F_{N-1} (right contraction)
   size_t bimg_bytes = 0;
+  uint8_t* bimg0 = nullptr;  // B image of F_0 (factored left contraction)
+  size_t bimg0_bytes = 0;
   int kpad = 0;
+  int64_t I0 = 0;            // mode-0 size (factored left contraction when I0 % 64 == 0)
 };
 
 inline int tc_kpad(int k) { return k <= 16 ? 16 : k <= 32 ? 32 : 64; }
@@ -635,16 +904,20 @@ inline void tc_free(TcTensor& t) {
   if (t.hi) cudaFree(t.hi);
   if (t.lo) cudaFree(t.lo);
   if (t.bimg) cudaFree(t.bimg);
+  if (t.bimg0) cudaFree(t.bimg0);
   t.hi = t.lo = nullptr;
-  t.bimg = nullptr;
-  t.bimg_bytes = 0;
+  t.bimg = t.bimg0 = nullptr;
+  t.bimg_bytes = t.bimg0_bytes = 0;
 }
+
+inline bool tc_left_factored(const TcTensor& t) { return t.I0 > 0 && t.I0 % TC_BK == 0; }
 
 // Returns cudaSuccess or an error; false map creation is reported as
 // cudaErrorInvalidValue.
 inline cudaError_t tc_set_tensor(TcTensor& t, const void* src, bool src_f64, int64_t L, int64_t R,
-                                 int prec, cudaStream_t st) {
+                                 int64_t I0, int prec, cudaStream_t st) {
   tc_free(t);
+  t.I0 = I0;
   t.L = L;
   t.R = R;
   t.Lpad = (L + 7) / 8 * 8;
@@ -680,22 +953,24 @@ inline int tc_stages(uint32_t stage_bytes) {
   return s < 2 ? 2 : (s > 8 ? 8 : s);
 }
 
-inline int tc_left_mt(int64_t R) { return R > 128 ? 2 : 1; }
+// j-tiles per CTA of the left contraction: 2 when R > 128, except at the
+// 64-wide rank (keeps the drain warps' running sums in registers)
+inline int tc_left_mt(int64_t R, int k) { return (R > 128 && k <= 32) ? 2 : 1; }
 
-inline void tc_left_plan(const TcTensor& t, int sm_count, int* mgroups, int* nsplit) {
-  const int MT = tc_left_mt(t.R);
+inline void tc_left_plan(const TcTensor& t, int k, int sm_count, int* mgroups, int* nsplit) {
+  const int MT = tc_left_mt(t.R, k);
   *mgroups = (int)((t.R + MT * TC_BM - 1) / (MT * TC_BM));
   int ns = sm_count / *mgroups;
   if (ns < 1) ns = 1;
-  const int64_t nch = (t.L + TC_BK - 1) / TC_BK;
-  if (ns > nch) ns = (int)nch;
+  const int64_t units = tc_left_factored(t) ? t.L / t.I0 : (t.L + TC_BK - 1) / TC_BK;
+  if (ns > units) ns = (int)units;
   *nsplit = ns;
 }
 
 inline size_t tc_scratch_elems(const TcTensor& t, int sm_count, int k) {
   if (!t.hi) return 0;
   int mg, ns;
-  tc_left_plan(t, sm_count, &mg, &ns);
+  tc_left_plan(t, k, sm_count, &mg, &ns);
   return (size_t)ns * t.R * k;
 }
 
@@ -712,6 +987,12 @@ inline cudaError_t tc_set_attrs() {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_tc_left<KP, 2, X2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(tc_stages(SL2) * SL2 + 1024));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_tc_left_fac<KP, 1, X2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(tc_stages(SL1) * SL1 + 1024));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_tc_left_fac<KP, 2, X2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(tc_stages(SL2) * SL2 + 1024));
   return e;
 }
 
@@ -727,12 +1008,17 @@ inline cudaError_t tc_ensure(TcTensor& t, int k) {
   if (e != cudaSuccess) return e;
   const int nk = (int)((t.R + TC_BK - 1) / TC_BK);
   size_t need = (size_t)nk * 2 * kp * 128;
-  if (t.bimg && t.bimg_bytes >= need && t.kpad == kp) return cudaSuccess;
+  size_t need0 = tc_left_factored(t) ? (size_t)(t.I0 / TC_BK) * 2 * kp * 128 : 0;
+  if (t.bimg && t.bimg_bytes >= need && t.kpad == kp && t.bimg0_bytes >= need0) return cudaSuccess;
   if (t.bimg) cudaFree(t.bimg);
-  t.bimg = nullptr;
+  if (t.bimg0) cudaFree(t.bimg0);
+  t.bimg = t.bimg0 = nullptr;
   t.kpad = kp;
   t.bimg_bytes = need;
-  return cudaMalloc(&t.bimg, need);
+  t.bimg0_bytes = need0;
+  e = cudaMalloc(&t.bimg, need);
+  if (e == cudaSuccess && need0) e = cudaMalloc(&t.bimg0, need0);
+  return e;
 }
 
 // Builds the pre-swizzled hi|lo B image of F_{N-1} for the right contraction.
@@ -778,12 +1064,22 @@ template <int KP, int MT, bool X2>
 inline void tc_left_launch(const TcTensor& t, const WGen& wg, int k, double* part, int* status,
                            int sm_count, cudaStream_t st, int* nsplit_out) {
   int mg, ns;
-  tc_left_plan(t, sm_count, &mg, &ns);
+  tc_left_plan(t, k, sm_count, &mg, &ns);
   constexpr uint32_t STAGE = (X2 ? 2 : 1) * MT * TC_BM * TC_BK * 2 + 2 * KP * 128;
   const int stages = tc_stages(STAGE);
   const size_t smem = (size_t)stages * STAGE + 1024;
-  k_tc_left<KP, MT, X2><<<dim3(mg, ns), TCL_THREADS, smem, st>>>(t.mL_hi, t.mL_lo, wg, t.L, t.R, k,
-                                                                 stages, part, status);
+  if (tc_left_factored(t)) {
+    // F_0 image (hi|lo rows, swizzled), then the factored kernel over runs of I_0
+    const int nslab = (int)(t.I0 / TC_BK);
+    k_tc_bimage<KP><<<(unsigned)std::min<int64_t>(((int64_t)nslab * KP * TC_BK + 255) / 256, 1024),
+                      256, 0, st>>>(wg.f[0], t.I0, k, nslab, t.bimg0);
+    const double* F2 = wg.nf > 2 ? wg.f[2] : nullptr;
+    k_tc_left_fac<KP, MT, X2><<<dim3(mg, ns), TCF_THREADS, smem, st>>>(
+        t.mL_hi, t.mL_lo, t.bimg0, wg.f[1], F2, wg.dim[1], t.I0, t.L, t.R, k, stages, part, status);
+  } else {
+    k_tc_left<KP, MT, X2><<<dim3(mg, ns), TCL_THREADS, smem, st>>>(t.mL_hi, t.mL_lo, wg, t.L, t.R, k,
+                                                                   stages, part, status);
+  }
   *nsplit_out = ns;
 }
 
@@ -791,7 +1087,7 @@ inline void tc_left_launch(const TcTensor& t, const WGen& wg, int k, double* par
 inline int tc_left(const TcTensor& t, const WGen& wg, int k, double* part, int* status,
                    int sm_count, cudaStream_t st) {
   const bool x2 = t.prec == 2;
-  const int MT = tc_left_mt(t.R);
+  const int MT = tc_left_mt(t.R, k);
   int ns = 1;
 #define TCL(KP)                                                                                  \
   if (MT == 2) {                                                                                 \

@@ -1,0 +1,95 @@
+"""Differentiable CP loss (torch.autograd.Function over the MTTKRP kernels):
+value vs the explicit reconstruction, gradient vs FP64 central finite
+differences and vs the reference's gradient form F_n G_{-n} - M_n
+(ntf/ntfnes.hpp:138-147) evaluated with the CPU oracle's MTTKRP."""
+import numpy as np
+import pytest
+
+from helpers import cp_tensor, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(prec, dims=(64, 64, 64), k=8, seed=31):
+    import torch
+    from planc_b200.autograd import CPLoss
+    X, _ = cp_tensor(dims, k, noise=0.05, seed=seed)
+    rng = np.random.default_rng(seed + 1)
+    F = [rng.random((d, k)) for d in dims]
+    lossf = CPLoss(X if prec == "fp64" else X.astype(np.float32), rank=k, precision=prec)
+    Ft = [torch.tensor(f, device="cuda", dtype=torch.float64, requires_grad=True) for f in F]
+    return X, F, lossf, Ft
+
+
+def test_cp_loss_value_and_reference_gradient(gpu, oracle_lib):
+    X, F, lossf, Ft = _setup("fp64")
+    loss = lossf(*Ft)
+    loss.backward()
+    model = np.einsum("az,bz,cz->abc", *F)
+    ref_loss = 0.5 * np.sum((X - model) ** 2)
+    assert abs(loss.item() - ref_loss) / ref_loss < 1e-10
+    for n in range(3):
+        M = oracle_lib.mttkrp_direct(X, F, n)
+        G = oracle_lib.gram_loo(F, n)
+        ref_grad = F[n] @ G - M
+        assert rel(Ft[n].grad.cpu().numpy(), ref_grad) < 1e-10
+    lossf.close()
+
+
+def test_cp_loss_gradient_finite_differences(gpu):
+    import torch
+    X, F, lossf, Ft = _setup("fp64", seed=33)
+    loss = lossf(*Ft)
+    loss.backward()
+    rng = np.random.default_rng(7)
+    h = 1e-5
+    for n in range(3):
+        E = torch.tensor(rng.standard_normal(F[n].shape), device="cuda", dtype=torch.float64)
+        with torch.no_grad():
+            plus = [f.detach().clone() for f in Ft]
+            minus = [f.detach().clone() for f in Ft]
+            plus[n] += h * E
+            minus[n] -= h * E
+            fd = (lossf(*plus).item() - lossf(*minus).item()) / (2 * h)
+        an = float((Ft[n].grad * E).sum())
+        assert abs(fd - an) / abs(an) < 1e-6, (n, fd, an)
+    lossf.close()
+
+
+@pytest.mark.parametrize("prec", ["bf16", "bf16x2"])
+def test_cp_loss_mixed_precision_gradient(gpu, prec):
+    X, F, lossf, Ft = _setup("fp64", seed=35)
+    loss64 = lossf(*Ft)
+    loss64.backward()
+    g64 = [f.grad.clone() for f in Ft]
+    lossf.close()
+    _, _, lossf2, Ft2 = _setup(prec, seed=35)
+    loss = lossf2(*Ft2)
+    loss.backward()
+    bound = 4e-3 if prec == "bf16" else 2e-5
+    for a, b in zip(Ft2, g64):
+        assert rel(a.grad.cpu().numpy(), b.cpu().numpy()) < bound
+    lossf2.close()
+
+
+def test_projected_gradient_descent_decreases_loss(gpu):
+    # block-coordinate projected gradient steps, step 1/L_n with L_n the
+    # largest eigenvalue of the leave-one-out Gram product: every step is a
+    # descent step for the block it moves
+    import torch
+    X, F, lossf, Ft = _setup("fp64", dims=(48, 40, 32), k=6, seed=37)
+    losses = []
+    for it in range(10):
+        for n in range(3):
+            for f in Ft:
+                f.grad = None
+            loss = lossf(*Ft)
+            loss.backward()
+            losses.append(loss.item())
+            with torch.no_grad():
+                others = [g for m, g in enumerate(Ft) if m != n]
+                Lc = float(torch.linalg.matrix_norm((others[0].T @ others[0]) * (others[1].T @ others[1]), 2))
+                Ft[n].sub_(Ft[n].grad / Lc).clamp_(min=0.0)
+    assert all(b <= a * (1 + 1e-6) for a, b in zip(losses, losses[1:]))
+    assert losses[-1] < 0.5 * losses[0]
+    lossf.close()
