@@ -157,6 +157,29 @@ int planc_gpu_mttkrp_device(planc_gpu_ctx* ctx, int mode, const double* const* F
  * common/tensor.hpp:350-356), written to host memory. */
 int planc_gpu_tensor_norm2(planc_gpu_ctx* ctx, double* out);
 
+/* MTTKRP of the last mode, allocation-free. No counterpart in the reference:
+ * this entry point exists for callers that cannot allocate device memory when
+ * they call the library -- applications whose GPU memory is reserved up front
+ * by a pool allocator (a cudaMalloc would fail or escape the pool), and
+ * latency-critical loops that must not pay the device-wide synchronisation a
+ * cudaMalloc/cudaFree can imply. It makes no allocation of any kind: the
+ * split-K partials go to a fixed 8 MiB device array (2^20 doubles) that every
+ * GPU loading the library holds until exit.
+ *   out[j, r] = sum_l X[l + L*j] * KRP(F_0..F_{N-2})[l, r],  j < I_{N-1}
+ * (the direct last-mode MTTKRP, common/tensor.hpp:246-327, FP64). X_dev:
+ * device tensor, FP64, mode 0 fastest; F_dev[n] (n < N-1): device factors,
+ * row-major I_n x k FP64; out_dev: device I_{N-1} x k FP64, row-major. The
+ * caller passes all of them; I_{N-1} * k above 2^20 is rejected with
+ * PLANC_GPU_ERR_UNSUPPORTED. Runs on `cuda_stream` on the current device and
+ * returns without synchronising. All calls share the one array: calls that
+ * overlap on the GPU (different streams or threads at once) race and must be
+ * serialised by the caller. The first call on a device resolves the array's
+ * device address (cudaGetSymbolAddress); make that first call before any
+ * stream capture. */
+int planc_gpu_mttkrp_last_mode_noalloc(const double* X_dev, const int64_t* dims, int nmodes,
+                                       const double* const* F_dev, int k, double* out_dev,
+                                       void* cuda_stream);
+
 /* Lowers the BPP iteration cap (0 restores the reference's 5k,
  * nnls/bppnnls.hpp:69). Used to exercise the "BPP failed" path
  * (PLANC_GPU_ERR_BPP_MAXITER) without a pathological input. */

@@ -12,6 +12,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1155,3 +1156,109 @@ int planc_gpu_synth_cp_tensor(int device, void* X_dev, int dtype, const int64_t*
 }
 
 }  // extern "C"
+
+// ============================================================ allocation-free MTTKRP
+// A variant of the split-K FP64 contraction whose split-K partials live in a
+// fixed, file-scope device array instead of memory obtained from cudaMalloc.
+// It serves callers that cannot allocate device memory at the time they call
+// this library: applications whose device memory is reserved up front by a
+// pool allocator (a cudaMalloc would fail or bypass the pool's accounting),
+// and latency-critical loops that must not pay the implicit device-wide
+// synchronisation a cudaMalloc or cudaFree can cause. Every GPU that loads the
+// library holds the array (kNoAllocScratchDoubles doubles = 8 MiB) until exit.
+namespace {
+
+constexpr size_t kNoAllocScratchDoubles = size_t(1) << 20;
+constexpr int kNoAllocMaxDevices = 64;
+__device__ __align__(256) double g_noalloc_scratch[kNoAllocScratchDoubles];
+std::mutex g_noalloc_mutex;
+double* g_noalloc_addr[kNoAllocMaxDevices] = {nullptr};
+
+// Device address of g_noalloc_scratch on the current device. The host-side
+// name of the array is only a stand-in, so the address is resolved once per
+// device with cudaGetSymbolAddress (with that device current) and cached.
+double* noalloc_scratch(int dev) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    CK(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    g_noalloc_addr[dev] = static_cast<double*>(p);
+  }
+  return g_noalloc_addr[dev];
+}
+
+}  // namespace
+
+extern "C" int planc_gpu_mttkrp_last_mode_noalloc(const double* X_dev, const int64_t* dims,
+                                                  int nmodes, const double* const* F_dev, int k,
+                                                  double* out_dev, void* cuda_stream) {
+  return guarded([&] {
+    if (!X_dev || !dims || !F_dev || !out_dev) fail(PLANC_GPU_ERR_ARG, "null argument");
+    if (nmodes < 2 || nmodes > kMaxModes)
+      fail(PLANC_GPU_ERR_ARG, "nmodes must be in [2, " + std::to_string(kMaxModes) + "]");
+    if (k < 1 || k > kMaxRank) fail(PLANC_GPU_ERR_UNSUPPORTED, "rank must be in [1, 64]");
+    for (int n = 0; n < nmodes; ++n) {
+      if (dims[n] < 1) fail(PLANC_GPU_ERR_ARG, "every mode size must be >= 1");
+      if (n < nmodes - 1 && !F_dev[n]) fail(PLANC_GPU_ERR_ARG, "null factor");
+    }
+    const int64_t R = dims[nmodes - 1];
+    int64_t A = 1;
+    for (int n = 0; n < nmodes - 1; ++n) A *= dims[n];
+    if ((size_t)R * (size_t)k > kNoAllocScratchDoubles)
+      fail(PLANC_GPU_ERR_UNSUPPORTED,
+           "last mode size x rank = " + std::to_string(R * k) +
+               " exceeds the allocation-free scratch of " +
+               std::to_string(kNoAllocScratchDoubles) + " doubles");
+    int dev = 0;
+    CK(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= kNoAllocMaxDevices) fail(PLANC_GPU_ERR_UNSUPPORTED, "device index too large");
+    double* scratch = noalloc_scratch(dev);
+    int sms = 148;
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    // Khatri-Rao operand over modes 0..N-2, lowest mode fastest
+    WGen wg;
+    memset(&wg, 0, sizeof(wg));
+    wg.nf = nmodes - 1;
+    int64_t stride = 1;
+    for (int t = 0; t < wg.nf; ++t) {
+      wg.f[t] = F_dev[t];
+      wg.dim[t] = dims[t];
+      wg.stride[t] = stride;
+      stride *= dims[t];
+    }
+    // split-K plan of the left contraction out[j, r] = sum_a X[a + A*j] W(a, r),
+    // capped so that every split's partial fits in the fixed scratch
+    ContractGeom g;
+    memset(&g, 0, sizeof(g));
+    g.M = R;
+    g.ldx = A;
+    g.A = A;
+    g.B = 1;
+    g.ldb = 0;
+    const int bk = k > 32 ? ct_bk<64>() : ct_bk<32>();
+    g.ktiles = (A + bk - 1) / bk;
+    const int64_t mtiles = (R + CT_BM - 1) / CT_BM;
+    int64_t ns = (2 * (int64_t)sms + mtiles - 1) / mtiles;
+    ns = std::max<int64_t>(1, std::min<int64_t>(ns, g.ktiles));
+    ns = std::min<int64_t>(ns, (int64_t)(kNoAllocScratchDoubles / ((size_t)R * k)));
+    g.tiles_per_split = (g.ktiles + ns - 1) / ns;
+    ns = (g.ktiles + g.tiles_per_split - 1) / g.tiles_per_split;
+    g.split_stride = R * k;
+    const dim3 grid((unsigned)mtiles, (unsigned)ns, 1);
+    cudaStream_t st = (cudaStream_t)cuda_stream;
+    // every split writes its whole R x k partial (zeros when it has no tiles),
+    // so nothing left in the scratch by an earlier call is read
+    switch (kpad(k)) {
+      case 8: k_contract_f64<8, true><<<grid, 256, 0, st>>>(X_dev, g, wg, k, scratch); break;
+      case 16: k_contract_f64<16, true><<<grid, 256, 0, st>>>(X_dev, g, wg, k, scratch); break;
+      case 32: k_contract_f64<32, true><<<grid, 256, 0, st>>>(X_dev, g, wg, k, scratch); break;
+      default: k_contract_f64<64, true><<<grid, 256, 0, st>>>(X_dev, g, wg, k, scratch); break;
+    }
+    CK(cudaGetLastError());
+    const int64_t n = R * k;
+    k_reduce_splits<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, st>>>(
+        scratch, (int)ns, n, n, out_dev);
+    CK(cudaGetLastError());
+  });
+}
+
