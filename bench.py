@@ -114,6 +114,24 @@ class ClockSampler:
                 "samples": len(sm), "reasons": sorted(reasons)}
 
 
+def max_over_ranks(x, dist=None, device="cpu"):
+    """Max of a per-rank scalar over all ranks (the job's time is the slowest
+    rank's); identity without a process group."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_value(local_ms, steps, world, dist=None, device="cpu"):
+    """Whole-job iterations/s of `world` independent replicas that each ran
+    `steps` iterations: all ranks' iterations / the slowest rank's time."""
+    ms = max_over_ranks(local_ms, dist, device)
+    return world * steps / (ms * 1e-3), ms
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -246,12 +264,7 @@ def main():
         if dist is not None:
             dist.barrier()
 
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda:%d" % dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    devname = "cuda:%d" % dev
 
     # ---------------- mixed precision, tensor resident in HBM
     ctx = gpu.Context(dev, args.precision)
@@ -272,11 +285,10 @@ def main():
     e1.record(stream)
     barrier()
     clocks = sampler.stop()
-    ms = max_over_ranks(e0.elapsed_time(e1))
+    value, ms = replica_value(e0.elapsed_time(e1), args.steps, world, dist, devname)
     launches = ctx.launch_count() - n0
     kt = ctx.kernel_times()
     ctx.set_timing(False)
-    value = world * args.steps / (ms * 1e-3)
 
     # dominant kernel: the partial MTTKRP contraction (right: P = X*F_last,
     # writes P in FP32; left: X^T*KRP, writes split-K FP64 partials)
@@ -326,7 +338,7 @@ def main():
         ctx64.run(args.algo, k64, compute_error=True)
         f1.record(s64)
         barrier()
-        ms64 = max_over_ranks(f0.elapsed_time(f1))
+        ms64 = max_over_ranks(f0.elapsed_time(f1), dist, devname)
         fp64 = {"value": world * k64 / (ms64 * 1e-3), "unit": "iters/s",
                 "ms_per_step": ms64 / k64, "steps": k64, "dtype": "f64"}
         # equal-iteration-count relative error, HALS and MU, both paths
@@ -360,7 +372,7 @@ def main():
             ctx.get_factors()
         g1.record(stream)
         barrier()
-        ms_e2e = max_over_ranks(g0.elapsed_time(g1))
+        ms_e2e = max_over_ranks(g0.elapsed_time(g1), dist, devname)
         fbytes = sum(d * k * 8 for d in dims)
         e2e = {"value": world * steps_e2e * T / (ms_e2e * 1e-3), "unit": "iters/s",
                "h2d_bytes_per_step": numel * 4 + fbytes,

@@ -157,6 +157,31 @@ int planc_gpu_mttkrp_device(planc_gpu_ctx* ctx, int mode, const double* const* F
  * common/tensor.hpp:350-356), written to host memory. */
 int planc_gpu_tensor_norm2(planc_gpu_ctx* ctx, double* out);
 
+/* ---- Batched factorisation of many independent tensors (uneven shapes and
+ * ranks). Each member is a context bound to one of `nstreams` worker streams;
+ * one outer iteration of every member is captured into a single CUDA graph,
+ * launched once per iteration, so the members' kernels overlap. Members use
+ * the dimension tree (N in {3,4}). The reference factorises tensors one at a
+ * time with AUNTF::computeNTF (ntf/auntf.hpp:128-177); the batch runs the same
+ * iteration for each member. */
+typedef struct planc_gpu_batch planc_gpu_batch;
+int planc_gpu_batch_create(planc_gpu_batch** out, int device, int precision, int nstreams);
+/* Adds a member: tensor as planc_gpu_set_tensor, factors as
+ * planc_gpu_set_factors (lambda = ones); *index receives its position. */
+int planc_gpu_batch_add(planc_gpu_batch* b, const void* X, int dtype, const int64_t* dims,
+                        int nmodes, int x_on_device, const double* const* F, int k, int* index);
+int planc_gpu_batch_count(planc_gpu_batch* b);
+int planc_gpu_batch_set_factors(planc_gpu_batch* b, int index, const double* const* F, int k);
+/* `iters` iterations of every member; errs (may be NULL) receives
+ * count x iters relative errors, member-major. */
+int planc_gpu_batch_run(planc_gpu_batch* b, int algo, int iters, int compute_error, double* errs);
+int planc_gpu_batch_get_factors(planc_gpu_batch* b, int index, double* const* F, double* lambda);
+/* Times the batch graph under candidate per-launch parallelism settings per
+ * member size class and keeps the fastest; members' factors are unchanged.
+ * best_ms (may be NULL) receives the tuned time of one batched iteration. */
+int planc_gpu_batch_autotune(planc_gpu_batch* b, int algo, int trials, double* best_ms);
+int planc_gpu_batch_destroy(planc_gpu_batch* b);
+
 /* MTTKRP of the last mode, allocation-free. No counterpart in the reference:
  * this entry point exists for callers that cannot allocate device memory when
  * they call the library -- applications whose GPU memory is reserved up front

@@ -38,6 +38,9 @@ EXPORTS = [
     "planc_gpu_bpp_solve", "planc_gpu_set_timing", "planc_gpu_get_kernel_times",
     "planc_gpu_launch_count", "planc_gpu_synth_cp_tensor", "planc_gpu_mttkrp_device",
     "planc_gpu_tensor_norm2", "planc_gpu_set_bpp_max_iter", "planc_gpu_selftest_wait_timeout",
+    "planc_gpu_batch_create", "planc_gpu_batch_add", "planc_gpu_batch_count",
+    "planc_gpu_batch_set_factors", "planc_gpu_batch_run", "planc_gpu_batch_get_factors",
+    "planc_gpu_batch_autotune", "planc_gpu_batch_destroy", "planc_gpu_mttkrp_last_mode_noalloc",
 ]
 
 
@@ -86,6 +89,15 @@ def load():
     L.planc_gpu_mttkrp_device.argtypes = [vp, i32, P(vp), vp, i32]
     L.planc_gpu_tensor_norm2.argtypes = [vp, pd]
     L.planc_gpu_set_bpp_max_iter.argtypes = [vp, i32]
+    L.planc_gpu_batch_create.argtypes = [P(vp), i32, i32, i32]
+    L.planc_gpu_batch_add.argtypes = [vp, vp, i32, pi64, i32, i32, P(pd), i32, P(i32)]
+    L.planc_gpu_batch_count.argtypes = [vp]
+    L.planc_gpu_batch_set_factors.argtypes = [vp, i32, P(pd), i32]
+    L.planc_gpu_batch_run.argtypes = [vp, i32, i32, i32, pd]
+    L.planc_gpu_batch_get_factors.argtypes = [vp, i32, P(pd), pd]
+    L.planc_gpu_batch_autotune.argtypes = [vp, i32, i32, pd]
+    L.planc_gpu_batch_destroy.argtypes = [vp]
+    L.planc_gpu_mttkrp_last_mode_noalloc.argtypes = [vp, pi64, i32, P(vp), i32, vp, vp]
     L.planc_gpu_selftest_wait_timeout.argtypes = [i32, d, P(i32)]
     for name in EXPORTS:
         getattr(L, name).restype = getattr(L, name).restype or i32
@@ -259,6 +271,64 @@ class Context:
 
     def launch_count(self):
         return int(load().planc_gpu_launch_count(self.h))
+
+
+class Batch:
+    """Many independent tensors factorised together (planc_gpu_batch)."""
+
+    def __init__(self, device=0, precision="fp64", nstreams=16):
+        h = ctypes.c_void_p()
+        _check(load().planc_gpu_batch_create(ctypes.byref(h), device, PREC[precision], nstreams))
+        self.h = h
+        self.members = []  # (dims, k)
+
+    def add(self, X, F, dims=None, dtype=None):
+        F = [_c64(f) for f in F]
+        k = F[0].shape[1]
+        if isinstance(X, np.ndarray):
+            dims = X.shape
+            arr = np.asfortranarray(X) if X.dtype == np.float32 else np.asfortranarray(X, dtype=np.float64)
+            dt, ptr, on_dev = (F32 if arr.dtype == np.float32 else F64), arr.ctypes.data_as(ctypes.c_void_p), 0
+        else:
+            dt, ptr, on_dev = (F32 if dtype == "f32" else F64), ctypes.c_void_p(int(X)), 1
+        d = (ctypes.c_int64 * len(dims))(*dims)
+        idx = ctypes.c_int()
+        _check(load().planc_gpu_batch_add(self.h, ptr, dt, d, len(dims), on_dev, _fptrs(F), k,
+                                          ctypes.byref(idx)))
+        self.members.append((tuple(int(x) for x in dims), k))
+        return idx.value
+
+    def set_factors(self, index, F):
+        F = [_c64(f) for f in F]
+        _check(load().planc_gpu_batch_set_factors(self.h, index, _fptrs(F), F[0].shape[1]))
+
+    def run(self, algo, iters, compute_error=True):
+        errs = np.zeros((len(self.members), max(iters, 1)))
+        _check(load().planc_gpu_batch_run(self.h, ALGO[algo], iters, int(compute_error), _pd(errs)))
+        return errs[:, :iters]
+
+    def get_factors(self, index):
+        dims, k = self.members[index]
+        F = [np.zeros((d, k)) for d in dims]
+        lam = np.zeros(k)
+        _check(load().planc_gpu_batch_get_factors(self.h, index, _fptrs(F), _pd(lam)))
+        return F, lam
+
+    def autotune(self, algo, trials=3):
+        ms = ctypes.c_double()
+        _check(load().planc_gpu_batch_autotune(self.h, ALGO[algo], trials, ctypes.byref(ms)))
+        return ms.value
+
+    def close(self):
+        if self.h:
+            load().planc_gpu_batch_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
 
 
 def selftest_wait_timeout(device=0, seconds=0.05):

@@ -204,8 +204,20 @@ __global__ void __launch_bounds__(256) k_ttv_left(const TT* __restrict__ T, int6
   for (int64_t b = blockIdx.x; b < B; b += gridDim.x) {
     double s = 0.0;
     if (lane < lanes) {
-      const TT* Tb = T + (A * b) * k;
-      for (int64_t a = lane; a < A; a += lanes) s = fma((double)Tb[a * k + r], F[a * k + r], s);
+      const TT* Tb = T + (A * b) * k + r;
+      const double* Fr = F + r;
+      double s1 = 0.0, s2 = 0.0, s3 = 0.0;
+      const int64_t step = (int64_t)lanes * k;
+      int64_t a = lane;
+      for (; a + 3 * lanes < A; a += 4 * lanes) {
+        const int64_t o = a * k;
+        s = fma((double)Tb[o], Fr[o], s);
+        s1 = fma((double)Tb[o + step], Fr[o + step], s1);
+        s2 = fma((double)Tb[o + 2 * step], Fr[o + 2 * step], s2);
+        s3 = fma((double)Tb[o + 3 * step], Fr[o + 3 * step], s3);
+      }
+      for (; a < A; a += lanes) s = fma((double)Tb[a * k], Fr[a * k], s);
+      s = (s + s1) + (s2 + s3);
     }
     red[tid] = s;
     __syncthreads();
@@ -330,6 +342,170 @@ __global__ void __launch_bounds__(128) k_mu_rows(double* __restrict__ H, const d
     if (c < k) H[row * k + c] = (h[c] * M[row * k + c]) / t[c];
 }
 
+// Warp-per-row forms of the same updates (lane c owns columns c and c + 32).
+// HALS keeps g = H(row,:) * G up to date incrementally: after column i moves
+// by delta, g += delta * G(i,:), so g(i) always equals the reference's
+// H(row,:) * G(:,i) with columns < i already replaced (ntf/ntfhals.hpp:17-18).
+template <int KP>
+__global__ void __launch_bounds__(256) k_hals_warp(double* __restrict__ H, const double* __restrict__ M,
+                                                   const double* __restrict__ G, int64_t I, int k) {
+  constexpr int PER = KP / 32;
+  __shared__ double Gs[KP * KP];
+  for (int e = threadIdx.x; e < k * k; e += blockDim.x) Gs[e] = G[e];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int64_t row = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (row >= I) return;
+  double h[PER], m[PER], g[PER];
+#pragma unroll
+  for (int p = 0; p < PER; ++p) {
+    const int c = lane + 32 * p;
+    h[p] = c < k ? H[row * k + c] : 0.0;
+    m[p] = c < k ? M[row * k + c] : 0.0;
+    g[p] = 0.0;
+  }
+  for (int j = 0; j < k; ++j) {
+    const double hj = (PER == 1 || j < 32) ? __shfl_sync(0xffffffffu, h[0], j & 31)
+                                           : __shfl_sync(0xffffffffu, h[PER - 1], j & 31);
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+      const int c = lane + 32 * p;
+      if (c < k) g[p] = fma(hj, Gs[j * k + c], g[p]);
+    }
+  }
+  for (int i = 0; i < k; ++i) {
+    const int owner = i & 31, pi = i >> 5;
+    double delta = 0.0;
+    if (lane == owner) {
+#pragma unroll
+      for (int p = 0; p < PER; ++p)
+        if (p == pi) {
+          double u = h[p] + (m[p] - g[p]);
+          u = (u < kEps17) ? kEps17 : u;
+          delta = u - h[p];
+          h[p] = u;
+        }
+    }
+    delta = __shfl_sync(0xffffffffu, delta, owner);
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+      const int c = lane + 32 * p;
+      if (c < k) g[p] = fma(delta, Gs[i * k + c], g[p]);
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < PER; ++p) {
+    const int c = lane + 32 * p;
+    if (c < k) H[row * k + c] = h[p];
+  }
+}
+
+template <int KP>
+__global__ void __launch_bounds__(256) k_mu_warp(double* __restrict__ H, const double* __restrict__ M,
+                                                 const double* __restrict__ G, int64_t I, int k) {
+  constexpr int PER = KP / 32;
+  __shared__ double Gs[KP * KP];
+  for (int e = threadIdx.x; e < k * k; e += blockDim.x) Gs[e] = G[e];
+  __syncthreads();
+  const int lane = threadIdx.x & 31;
+  const int64_t row = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (row >= I) return;
+  double h[PER], t[PER];
+#pragma unroll
+  for (int p = 0; p < PER; ++p) {
+    const int c = lane + 32 * p;
+    h[p] = c < k ? H[row * k + c] : 0.0;
+    t[p] = 0.0;
+  }
+  for (int j = 0; j < k; ++j) {
+    const double hj = (PER == 1 || j < 32) ? __shfl_sync(0xffffffffu, h[0], j & 31)
+                                           : __shfl_sync(0xffffffffu, h[PER - 1], j & 31);
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+      const int c = lane + 32 * p;
+      if (c < k) t[p] = fma(hj, Gs[j * k + c], t[p]);
+    }
+  }
+#pragma unroll
+  for (int p = 0; p < PER; ++p) {
+    const int c = lane + 32 * p;
+    if (c < k) H[row * k + c] = (h[p] * M[row * k + c]) / (t[p] + kEps6);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Normalisation + Gram over many CTAs: each CTA adds U^T U of a block of rows
+// of the new (unnormalised) factor U; k_gram_finalize sums the blocks in a
+// fixed order, takes lambda_r = sqrt((U^T U)_rr) = ||U(:,r)||, writes the Gram
+// of the normalised factor G_n = (U^T U)_ab / (lambda_a lambda_b), normalises
+// U in place (ncpfactors.hpp:346-351) and forms the next leave-one-out product.
+// ---------------------------------------------------------------------------
+constexpr int GP_ROWS = 64;
+
+__global__ void __launch_bounds__(256) k_gram_partial(const double* __restrict__ U, int64_t I, int k,
+                                                      double* __restrict__ part) {
+  __shared__ double tile[GP_ROWS * kMaxRank];
+  const int64_t row0 = (int64_t)blockIdx.x * GP_ROWS;
+  const int nrows = (int)((I - row0) < GP_ROWS ? (I - row0) : GP_ROWS);
+  for (int e = threadIdx.x; e < nrows * k; e += 256) tile[e] = U[row0 * k + e];
+  __syncthreads();
+  const int kk2 = k * k;
+  for (int e = threadIdx.x; e < kk2; e += 256) {
+    const int a = e / k, b = e % k;
+    double s0 = 0.0, s1 = 0.0;
+    int i = 0;
+    for (; i + 1 < nrows; i += 2) {
+      s0 = fma(tile[i * k + a], tile[i * k + b], s0);
+      s1 = fma(tile[(i + 1) * k + a], tile[(i + 1) * k + b], s1);
+    }
+    if (i < nrows) s0 = fma(tile[i * k + a], tile[i * k + b], s0);
+    part[(int64_t)blockIdx.x * kk2 + e] = s0 + s1;
+  }
+}
+
+__global__ void __launch_bounds__(1024) k_gram_finalize(double* __restrict__ F, int64_t I, int k,
+                                                        const double* __restrict__ part, int nblk,
+                                                        double* __restrict__ lambda,
+                                                        double* __restrict__ Gall, int N, int n,
+                                                        int next, double* __restrict__ Gloo) {
+  __shared__ double lam[kMaxRank];
+  __shared__ double gs[kMaxRank * kMaxRank];
+  const int tid = threadIdx.x;
+  const int kk2 = k * k;
+  for (int e = tid; e < kk2; e += 1024) {
+    double s = 0.0;
+    for (int b = 0; b < nblk; ++b) s += part[(int64_t)b * kk2 + e];
+    gs[e] = s;
+  }
+  __syncthreads();
+  if (tid < k) {
+    const double nrm = sqrt(gs[tid * k + tid]);
+    lam[tid] = nrm;
+    if (lambda) lambda[tid] = nrm;
+  }
+  __syncthreads();
+  double* Gn = Gall + (int64_t)n * kk2;
+  for (int e = tid; e < kk2; e += 1024) {
+    const int a = e / k, b = e % k;
+    const double la = lam[a], lb = lam[b];
+    Gn[e] = (la > 0 && lb > 0) ? gs[e] / (la * lb) : gs[e];
+  }
+  const int r = tid % k, lane = tid / k, lanes = 1024 / k;
+  if (lane < lanes) {
+    const double nrm = lam[r];
+    if (nrm > 0)
+      for (int64_t i = lane; i < I; i += lanes) F[i * k + r] = F[i * k + r] / nrm;
+  }
+  if (next < 0) return;
+  __syncthreads();
+  for (int e = tid; e < kk2; e += 1024) {
+    double g = 1.0;
+    for (int i = 0; i < N; ++i)
+      if (i != next) g = g * Gall[(int64_t)i * kk2 + e];
+    Gloo[e] = g;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Normalise mode n (NCPFactors::normalize(int), common/ncpfactors.hpp:346-351:
 // lambda_r = ||F(:,r)||, F(:,r) /= lambda_r when > 0), then G_n = F^T F of the
@@ -429,19 +605,29 @@ __global__ void k_gram_loo(const double* __restrict__ Gall, int N, int k, int n,
 // Writes errs[*counter] and increments *counter (so one captured graph can be
 // replayed across iterations). One CTA of 256 threads.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_error(const double* __restrict__ Mlast,
-                                               const double* __restrict__ Flast, int64_t I,
-                                               const double* __restrict__ lambda,
-                                               const double* __restrict__ Gall, int N, int k,
-                                               const double* __restrict__ normX2,
-                                               double* __restrict__ errs, int* __restrict__ counter) {
-  __shared__ double red[256];
-  __shared__ double red2[256];
+__global__ void __launch_bounds__(1024) k_error(const double* __restrict__ Mlast,
+                                                const double* __restrict__ Flast, int64_t I,
+                                                const double* __restrict__ lambda,
+                                                const double* __restrict__ Gall, int N, int k,
+                                                const double* __restrict__ normX2,
+                                                double* __restrict__ errs, int* __restrict__ counter) {
+  __shared__ double red[1024];
+  __shared__ double red2[1024];
   const int tid = threadIdx.x;
+  const int r = tid % k, lane = tid / k, lanes = 1024 / k;
   double inner = 0.0;
-  for (int64_t e = tid; e < I * k; e += 256) inner = fma(Mlast[e] * Flast[e], lambda[e % k], inner);
+  if (lane < lanes) {
+    double s0 = 0.0, s1 = 0.0;
+    int64_t i = lane;
+    for (; i + lanes < I; i += 2 * lanes) {
+      s0 = fma(Mlast[i * k + r], Flast[i * k + r], s0);
+      s1 = fma(Mlast[(i + lanes) * k + r], Flast[(i + lanes) * k + r], s1);
+    }
+    if (i < I) s0 = fma(Mlast[i * k + r], Flast[i * k + r], s0);
+    inner = (s0 + s1) * lambda[r];
+  }
   double mn = 0.0;
-  for (int e = tid; e < k * k; e += 256) {
+  for (int e = tid; e < k * k; e += 1024) {
     double g = 1.0;
     for (int i = 0; i < N; ++i) g = g * Gall[(int64_t)i * k * k + e];
     mn = fma(lambda[e / k] * lambda[e % k], g, mn);
@@ -449,7 +635,7 @@ __global__ void __launch_bounds__(256) k_error(const double* __restrict__ Mlast,
   red[tid] = inner;
   red2[tid] = mn;
   __syncthreads();
-  for (int s = 128; s > 0; s >>= 1) {
+  for (int s = 512; s > 0; s >>= 1) {
     if (tid < s) {
       red[tid] += red[tid + s];
       red2[tid] += red2[tid + s];

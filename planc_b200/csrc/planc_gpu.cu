@@ -91,6 +91,8 @@ struct planc_gpu_ctx {
   double* Q = nullptr;           // N = 4: P contracted with F_0, row-major (I1*I2) x k
   double* scratch = nullptr;
   size_t scratch_elems = 0;
+  double* gram_part = nullptr;  // per-row-block partial Grams
+  size_t gram_part_elems = 0;
   double* errs_dev = nullptr;
   int errs_cap = 0;
   int* counter_dev = nullptr;
@@ -112,11 +114,25 @@ struct planc_gpu_ctx {
   int64_t klaunch[KC_COUNT] = {0};
   int64_t launch_count = 0;
   int bpp_max_iter = 0;  // 0: the reference's 5k cap
+  // Fraction of the GPU one launch of this context aims to fill (split-K and
+  // grid sizing). 1 for a context alone on the GPU; the batch autotuner lowers
+  // it when many contexts run concurrently.
+  double par_scale = 1.0;
+  // Incremented whenever a device buffer that a captured graph may reference
+  // is (re)allocated; cached graphs are rebuilt when it changes.
+  int64_t buf_epoch = 0;
+  int64_t g_epoch = -1;
 };
 
 namespace {
 
 void set_device(planc_gpu_ctx* c) { CK(cudaSetDevice(c->device)); }
+
+// SMs one launch of this context is sized for
+int eff_sm(const planc_gpu_ctx* c) {
+  int v = (int)(c->sm_count * c->par_scale);
+  return v < 1 ? 1 : v;
+}
 
 template <typename T>
 void dalloc(T** p, size_t n) {
@@ -208,7 +224,7 @@ ContractPlan plan_contract(planc_gpu_ctx* c, bool left, int64_t M, int64_t ldx, 
   int64_t tilesA = (A + bk - 1) / bk;
   p.g.ktiles = left ? tilesA * B : tilesA;
   int64_t mtiles = (M + CT_BM - 1) / CT_BM;
-  int64_t target = 2 * (int64_t)c->sm_count;
+  int64_t target = 2 * (int64_t)eff_sm(c);
   int64_t ns = (target + mtiles - 1) / mtiles;
   ns = std::max<int64_t>(1, std::min<int64_t>(ns, p.g.ktiles));
   ns = std::min<int64_t>(ns, 1024);
@@ -234,7 +250,7 @@ struct TtvRightPlan {
 TtvRightPlan plan_ttv_right(planc_gpu_ctx* c, int64_t A, int64_t B) {
   TtvRightPlan p;
   int64_t gx = (A * c->k + 255) / 256;
-  int64_t target = 8 * (int64_t)c->sm_count;  // latency-bound loop: many warps per SM
+  int64_t target = 8 * (int64_t)eff_sm(c);  // latency-bound loop: many warps per SM
   int64_t ns = std::max<int64_t>(1, std::min<int64_t>((target + gx - 1) / gx, (B + 15) / 16));
   ns = std::min<int64_t>(ns, 512);
   p.bper = (B + ns - 1) / ns;
@@ -251,8 +267,32 @@ void direct_geom(planc_gpu_ctx* c, int n, int64_t* A, int64_t* B) {
   for (int m = n + 1; m < c->N; ++m) *B *= c->dims[m];
 }
 
-// Computes the largest scratch any MTTKRP path needs and (re)allocates.
+void ensure_buffers_impl(planc_gpu_ctx* c);
+
+// Computes the largest scratch any MTTKRP path needs and (re)allocates; any
+// reallocation invalidates the cached graph (it holds the old pointers).
 void ensure_buffers(planc_gpu_ctx* c) {
+  const void* before[6] = {c->scratch, c->P, c->P32, c->Q, c->tct.bimg, c->tct.bimg0};
+  ensure_buffers_impl(c);
+  const void* after[6] = {c->scratch, c->P, c->P32, c->Q, c->tct.bimg, c->tct.bimg0};
+  for (int i = 0; i < 6; ++i)
+    if (before[i] != after[i]) {
+      c->buf_epoch++;
+      break;
+    }
+}
+
+// Error-history buffer of at least `n` entries (reallocation bumps the epoch).
+void ensure_errs(planc_gpu_ctx* c, int n) {
+  if (n < 1) n = 1;
+  if (!c->errs_dev || n > c->errs_cap) {
+    dalloc(&c->errs_dev, (size_t)n);
+    c->errs_cap = n;
+    c->buf_epoch++;
+  }
+}
+
+void ensure_buffers_impl(planc_gpu_ctx* c) {
   const int k = c->k;
   size_t need = 0;
   if (c->N == 3 || c->N == 4) {
@@ -266,7 +306,7 @@ void ensure_buffers(planc_gpu_ctx* c) {
       TtvRightPlan t2 = plan_ttv_right(c, c->dims[1], c->dims[2]);
       need = std::max(need, (size_t)t2.nsplit * c->dims[1] * k);
     }
-    need = std::max(need, tc_scratch_elems(c->tct, c->sm_count, k));
+    need = std::max(need, tc_scratch_elems(c->tct, eff_sm(c), k));
     CK(tc_ensure(c->tct, k));
   }
   for (int n = 0; n < c->N; ++n) {
@@ -376,7 +416,7 @@ void partial_right(planc_gpu_ctx* c) {
   } else {
     launch(c, KC_PREP, [&] { tc_right_prep(c->tct, c->F[c->N - 1], c->k, c->stream); });
     launch(c, KC_CONTRACT, [&] {
-      tc_right(c->tct, c->k, c->P32, c->status_dev, c->sm_count, c->stream);
+      tc_right(c->tct, c->k, c->P32, c->status_dev, eff_sm(c), c->stream);
     });
   }
 }
@@ -393,10 +433,10 @@ void partial_left(planc_gpu_ctx* c, double* out) {
     WGen wg = make_wgen(c, modes);
     int nsplit = 0;
     if (wg.nf < 2 || wg.nf > 3) fail(PLANC_GPU_ERR_UNSUPPORTED, "left contraction needs 2 or 3 modes");
-    if (tc_scratch_elems(c->tct, c->sm_count, c->k) > c->scratch_elems)
+    if (tc_scratch_elems(c->tct, eff_sm(c), c->k) > c->scratch_elems)
       fail(PLANC_GPU_ERR_STATE, "internal: split-K scratch larger than planned");
     launch(c, KC_CONTRACT_LEFT, [&] {
-      nsplit = tc_left(c->tct, wg, c->k, c->scratch, c->status_dev, c->sm_count, c->stream);
+      nsplit = tc_left(c->tct, wg, c->k, c->scratch, c->status_dev, eff_sm(c), c->stream);
     });
     int64_t n = c->R * c->k;
     launch(c, KC_REDUCE, [&] {
@@ -460,18 +500,19 @@ void run_update(planc_gpu_ctx* c, int algo, int n) {
   const int k = c->k;
   const int64_t I = c->dims[n];
   if (algo == PLANC_GPU_HALS || algo == PLANC_GPU_MU) {
-    unsigned blocks = (unsigned)((I + 127) / 128);
+    // one warp per factor row, 8 rows per CTA
+    unsigned blocks = (unsigned)((I + 7) / 8);
     launch(c, KC_UPDATE, [&] {
-      switch (kpad(k)) {
-#define CASE(KP)                                                                              \
-  case KP:                                                                                    \
-    if (algo == PLANC_GPU_HALS)                                                               \
-      k_hals_rows<KP><<<blocks, 128, 0, c->stream>>>(c->F[n], c->M[n], c->Gloo, I, k);        \
-    else                                                                                      \
-      k_mu_rows<KP><<<blocks, 128, 0, c->stream>>>(c->F[n], c->M[n], c->Gloo, I, k);          \
-    break;
-        CASE(8) CASE(16) CASE(32) CASE(64)
-#undef CASE
+      if (k <= 32) {
+        if (algo == PLANC_GPU_HALS)
+          k_hals_warp<32><<<blocks, 256, 0, c->stream>>>(c->F[n], c->M[n], c->Gloo, I, k);
+        else
+          k_mu_warp<32><<<blocks, 256, 0, c->stream>>>(c->F[n], c->M[n], c->Gloo, I, k);
+      } else {
+        if (algo == PLANC_GPU_HALS)
+          k_hals_warp<64><<<blocks, 256, 0, c->stream>>>(c->F[n], c->M[n], c->Gloo, I, k);
+        else
+          k_mu_warp<64><<<blocks, 256, 0, c->stream>>>(c->F[n], c->M[n], c->Gloo, I, k);
       }
     });
   } else if (algo == PLANC_GPU_ANLSBPP) {
@@ -495,9 +536,16 @@ void run_update(planc_gpu_ctx* c, int algo, int n) {
 }
 
 void normalize_gram(planc_gpu_ctx* c, int n, int next, double* lambda) {
+  const int64_t I = c->dims[n];
+  const int nblk = (int)((I + GP_ROWS - 1) / GP_ROWS);
+  if ((size_t)nblk * c->k * c->k > c->gram_part_elems)
+    fail(PLANC_GPU_ERR_STATE, "internal: Gram partial buffer too small");
   launch(c, KC_NORMGRAM, [&] {
-    k_normalize_gram<<<1, 1024, 0, c->stream>>>(c->F[n], c->dims[n], c->k, lambda, c->Gall, c->N,
-                                                n, next, c->Gloo);
+    k_gram_partial<<<nblk, 256, 0, c->stream>>>(c->F[n], I, c->k, c->gram_part);
+  });
+  launch(c, KC_NORMGRAM, [&] {
+    k_gram_finalize<<<1, 1024, 0, c->stream>>>(c->F[n], I, c->k, c->gram_part, nblk, lambda,
+                                               c->Gall, c->N, n, next, c->Gloo);
   });
 }
 
@@ -508,7 +556,7 @@ void gram_loo(planc_gpu_ctx* c, int n) {
 void error_kernel(planc_gpu_ctx* c) {
   const int last = c->N - 1;
   launch(c, KC_ERROR, [&] {
-    k_error<<<1, 256, 0, c->stream>>>(c->M[last], c->F[last], c->dims[last], c->lambda, c->Gall,
+    k_error<<<1, 1024, 0, c->stream>>>(c->M[last], c->F[last], c->dims[last], c->lambda, c->Gall,
                                       c->N, c->k, c->normX2, c->errs_dev, c->counter_dev);
   });
 }
@@ -567,6 +615,8 @@ void free_all(planc_gpu_ctx* c) {
     c->factor_cap[n] = 0;
   }
   f(c->Gall);
+  f(c->gram_part);
+  c->gram_part_elems = 0;
   f(c->Gloo);
   f(c->lambda);
   f(c->P);
@@ -776,6 +826,12 @@ int planc_gpu_set_factors(planc_gpu_ctx* c, const double* const* F, const double
       CK(cudaMemcpyAsync(c->F[n], F[n], need * 8, cudaMemcpyHostToDevice, c->stream));
     }
     dalloc(&c->Gall, (size_t)c->N * k * k);
+    {
+      int64_t maxI = 1;
+      for (int n = 0; n < c->N; ++n) maxI = std::max(maxI, c->dims[n]);
+      c->gram_part_elems = (size_t)((maxI + GP_ROWS - 1) / GP_ROWS) * k * k;
+      dalloc(&c->gram_part, c->gram_part_elems);
+    }
     dalloc(&c->Gloo, (size_t)k * k);
     dalloc(&c->lambda, (size_t)k);
     // AUNTF::reset: update_factor_mode on every mode (normalise, Gram), then
@@ -803,14 +859,8 @@ int planc_gpu_run(planc_gpu_ctx* c, int algo, int iters, int dimtree, int comput
     if (iters == 0) return;
     set_device(c);
     ensure_buffers(c);
-    if (compute_error && iters > c->errs_cap) {
-      dalloc(&c->errs_dev, (size_t)iters);
-      c->errs_cap = iters;
-    }
-    if (!c->errs_dev) {
-      dalloc(&c->errs_dev, 1);
-      c->errs_cap = 1;
-    }
+    ensure_errs(c, compute_error ? iters : 1);
+    if (c->g_epoch != c->buf_epoch) reset_graph(c);
     CK(cudaMemsetAsync(c->counter_dev, 0, sizeof(int), c->stream));
     gram_loo(c, 0);
     bool use_graph = !c->timing;
@@ -836,6 +886,7 @@ int planc_gpu_run(planc_gpu_ctx* c, int algo, int iters, int dimtree, int comput
         c->g_algo = algo;
         c->g_dimtree = (int)dt;
         c->g_err = compute_error;
+        c->g_epoch = c->buf_epoch;
       }
       for (int it = 0; it < iters; ++it) CK(cudaGraphLaunch(c->gexec, c->stream));
     } else {
@@ -905,10 +956,7 @@ int planc_gpu_objective_error(planc_gpu_ctx* c, double* err) {
     if (!err) fail(PLANC_GPU_ERR_ARG, "null output");
     set_device(c);
     ensure_buffers(c);
-    if (!c->errs_dev) {
-      dalloc(&c->errs_dev, 1);
-      c->errs_cap = 1;
-    }
+    ensure_errs(c, 1);
     const int last = c->N - 1;
     // <X, model> needs the MTTKRP of the last mode from the current factors
     if (c->precision == PLANC_GPU_PREC_FP64 || c->N == 3 || c->N == 4) {
@@ -1152,6 +1200,301 @@ int planc_gpu_synth_cp_tensor(int device, void* X_dev, int dtype, const int64_t*
       throw;
     }
     for (auto p : bufs) cudaFree(p);
+  });
+}
+
+}  // extern "C"
+
+// ============================================================ batched factorisation
+// Many independent tensors (uneven shapes and ranks) factorised together: one
+// context per tensor, each bound to one of S worker streams; one outer
+// iteration of every tensor is captured into ONE CUDA graph (fork from a
+// master stream to the workers, join back) and that graph is launched once
+// per iteration, so the tensors' kernels overlap on the GPU. The per-context
+// parallelism (split-K / grid sizing) is chosen by an autotuner that times
+// the whole batch graph for a few candidate settings per size class.
+struct planc_gpu_batch {
+  int device = 0;
+  int precision = PLANC_GPU_PREC_FP64;
+  cudaStream_t master = nullptr;
+  std::vector<cudaStream_t> workers;
+  std::vector<planc_gpu_ctx*> members;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> joins;
+  cudaGraphExec_t gexec = nullptr;
+  int g_algo = -1, g_err = -1;
+  int64_t g_epoch = -1;  // sum of the members' buffer epochs at capture
+};
+
+namespace {
+
+void batch_reset_graph(planc_gpu_batch* b);
+
+int64_t batch_epoch(const planc_gpu_batch* b) {
+  int64_t e = (int64_t)b->members.size();
+  for (auto* m : b->members) e += m->buf_epoch;
+  return e;
+}
+
+// every buffer the batch graph will reference, allocated before capture
+void batch_ensure(planc_gpu_batch* b, int iters, bool err) {
+  for (auto* m : b->members) {
+    ensure_buffers(m);
+    ensure_errs(m, err ? iters : 1);
+  }
+  if (b->g_epoch != batch_epoch(b)) batch_reset_graph(b);
+}
+
+void batch_reset_graph(planc_gpu_batch* b) {
+  if (b->gexec) cudaGraphExecDestroy(b->gexec);
+  b->gexec = nullptr;
+  b->g_algo = b->g_err = -1;
+}
+
+// size class of a member for the autotuner: by element count
+int batch_class(const planc_gpu_ctx* c) {
+  return c->numel < (1 << 20) ? 0 : c->numel < (1 << 23) ? 1 : 2;
+}
+
+void batch_capture(planc_gpu_batch* b, int algo, bool err) {
+  batch_reset_graph(b);
+  cudaGraph_t graph = nullptr;
+  CK(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal));
+  try {
+    CK(cudaEventRecord(b->fork, b->master));
+    for (auto w : b->workers) CK(cudaStreamWaitEvent(w, b->fork, 0));
+    for (auto* m : b->members) {
+      m->capturing = true;
+      one_iteration(m, algo, true, err);
+      m->capturing = false;
+    }
+    for (size_t i = 0; i < b->workers.size(); ++i) {
+      CK(cudaEventRecord(b->joins[i], b->workers[i]));
+      CK(cudaStreamWaitEvent(b->master, b->joins[i], 0));
+    }
+  } catch (...) {
+    for (auto* m : b->members) m->capturing = false;
+    cudaStreamEndCapture(b->master, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  CK(cudaStreamEndCapture(b->master, &graph));
+  cudaError_t e = cudaGraphInstantiate(&b->gexec, graph, 0);
+  cudaGraphDestroy(graph);
+  cuda_check(e, "cudaGraphInstantiate (batch)");
+  b->g_algo = algo;
+  b->g_err = err ? 1 : 0;
+  b->g_epoch = batch_epoch(b);
+}
+
+// per-run set-up of every member (error counters, first leave-one-out Gram),
+// ordered before the graph launches on the master stream
+void batch_prepare(planc_gpu_batch* b) {
+  for (auto* m : b->members) {
+    CK(cudaMemsetAsync(m->counter_dev, 0, sizeof(int), m->stream));
+    gram_loo(m, 0);
+  }
+  for (size_t i = 0; i < b->workers.size(); ++i) {
+    CK(cudaEventRecord(b->joins[i], b->workers[i]));
+    CK(cudaStreamWaitEvent(b->master, b->joins[i], 0));
+  }
+}
+
+void batch_finish(planc_gpu_batch* b) {
+  CK(cudaStreamSynchronize(b->master));
+  for (auto* m : b->members) check_status(m);
+}
+
+}  // namespace
+
+extern "C" {
+
+int planc_gpu_batch_create(planc_gpu_batch** out, int device, int precision, int nstreams) {
+  return guarded([&] {
+    if (!out) fail(PLANC_GPU_ERR_ARG, "out is null");
+    *out = nullptr;
+    if (nstreams < 1 || nstreams > 64) fail(PLANC_GPU_ERR_ARG, "nstreams must be in [1, 64]");
+    if (precision < PLANC_GPU_PREC_FP64 || precision > PLANC_GPU_PREC_BF16X2)
+      fail(PLANC_GPU_ERR_ARG, "unknown precision");
+    CK(cudaSetDevice(device));
+    planc_gpu_batch* b = new planc_gpu_batch();
+    b->device = device;
+    b->precision = precision;
+    try {
+      CK(cudaStreamCreateWithFlags(&b->master, cudaStreamNonBlocking));
+      CK(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+      for (int i = 0; i < nstreams; ++i) {
+        cudaStream_t w;
+        CK(cudaStreamCreateWithFlags(&w, cudaStreamNonBlocking));
+        b->workers.push_back(w);
+        cudaEvent_t e;
+        CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        b->joins.push_back(e);
+      }
+    } catch (...) {
+      for (auto w : b->workers) cudaStreamDestroy(w);
+      for (auto e : b->joins) cudaEventDestroy(e);
+      if (b->fork) cudaEventDestroy(b->fork);
+      if (b->master) cudaStreamDestroy(b->master);
+      delete b;
+      throw;
+    }
+    *out = b;
+  });
+}
+
+int planc_gpu_batch_add(planc_gpu_batch* b, const void* X, int dtype, const int64_t* dims,
+                        int nmodes, int x_on_device, const double* const* F, int k, int* index) {
+  return guarded([&] {
+    if (!b) fail(PLANC_GPU_ERR_ARG, "null batch");
+    if (nmodes != 3 && nmodes != 4)
+      fail(PLANC_GPU_ERR_UNSUPPORTED, "batched members run the dimension tree (N in {3,4})");
+    batch_reset_graph(b);
+    planc_gpu_ctx* m = nullptr;
+    cudaStream_t w = b->workers[b->members.size() % b->workers.size()];
+    int rc = planc_gpu_create(&m, b->device, b->precision, (void*)w);
+    if (rc != PLANC_GPU_OK) throw Fail{rc};
+    rc = planc_gpu_set_tensor(m, X, dtype, dims, nmodes, x_on_device);
+    if (rc == PLANC_GPU_OK) rc = planc_gpu_set_factors(m, F, nullptr, k);
+    if (rc != PLANC_GPU_OK) {
+      std::string msg = g_last_error;
+      planc_gpu_destroy(m);
+      g_last_error = msg;
+      throw Fail{rc};
+    }
+    b->members.push_back(m);
+    if (index) *index = (int)b->members.size() - 1;
+  });
+}
+
+int planc_gpu_batch_count(planc_gpu_batch* b) { return b ? (int)b->members.size() : -1; }
+
+int planc_gpu_batch_set_factors(planc_gpu_batch* b, int index, const double* const* F, int k) {
+  return guarded([&] {
+    if (!b || index < 0 || index >= (int)b->members.size()) fail(PLANC_GPU_ERR_ARG, "bad index");
+    int rc = planc_gpu_set_factors(b->members[index], F, nullptr, k);
+    if (rc != PLANC_GPU_OK) throw Fail{rc};
+    batch_reset_graph(b);
+  });
+}
+
+int planc_gpu_batch_run(planc_gpu_batch* b, int algo, int iters, int compute_error, double* errs) {
+  return guarded([&] {
+    if (!b) fail(PLANC_GPU_ERR_ARG, "null batch");
+    if (b->members.empty()) fail(PLANC_GPU_ERR_STATE, "empty batch");
+    if (algo != PLANC_GPU_MU && algo != PLANC_GPU_HALS && algo != PLANC_GPU_ANLSBPP)
+      fail(PLANC_GPU_ERR_ARG, "unknown algorithm");
+    if (iters <= 0) return;
+    CK(cudaSetDevice(b->device));
+    const bool err = compute_error != 0;
+    batch_ensure(b, iters, err);
+    if (!b->gexec || b->g_algo != algo || b->g_err != (int)err) batch_capture(b, algo, err);
+    batch_prepare(b);
+    for (int it = 0; it < iters; ++it) CK(cudaGraphLaunch(b->gexec, b->master));
+    batch_finish(b);
+    if (err && errs) {
+      for (size_t i = 0; i < b->members.size(); ++i)
+        CK(cudaMemcpy(errs + i * iters, b->members[i]->errs_dev, iters * sizeof(double),
+                      cudaMemcpyDeviceToHost));
+    }
+  });
+}
+
+int planc_gpu_batch_get_factors(planc_gpu_batch* b, int index, double* const* F, double* lambda) {
+  return guarded([&] {
+    if (!b || index < 0 || index >= (int)b->members.size()) fail(PLANC_GPU_ERR_ARG, "bad index");
+    int rc = planc_gpu_get_factors(b->members[index], F, lambda);
+    if (rc != PLANC_GPU_OK) throw Fail{rc};
+  });
+}
+
+// Autotuner: for each member size class (by element count), tries the
+// parallelism settings {1, 1/2, 1/4, 1/8, 1/16, 1/32} of the GPU per launch,
+// timing `trials` graph launches of the whole batch for each, coordinate by
+// coordinate, and keeps the fastest. Factors are restored afterwards.
+int planc_gpu_batch_autotune(planc_gpu_batch* b, int algo, int trials, double* best_ms) {
+  return guarded([&] {
+    if (!b || b->members.empty()) fail(PLANC_GPU_ERR_STATE, "empty batch");
+    if (trials < 1) trials = 1;
+    CK(cudaSetDevice(b->device));
+    // save factors so the tuning iterations leave no trace
+    std::vector<std::vector<std::vector<double>>> saved(b->members.size());
+    std::vector<std::vector<double>> saved_lam(b->members.size());
+    for (size_t i = 0; i < b->members.size(); ++i) {
+      planc_gpu_ctx* m = b->members[i];
+      saved[i].resize(m->N);
+      std::vector<double*> ptr(m->N);
+      for (int n = 0; n < m->N; ++n) {
+        saved[i][n].resize((size_t)m->dims[n] * m->k);
+        ptr[n] = saved[i][n].data();
+      }
+      saved_lam[i].resize(m->k);
+      int rc = planc_gpu_get_factors(m, ptr.data(), saved_lam[i].data());
+      if (rc != PLANC_GPU_OK) throw Fail{rc};
+    }
+    const double cand[] = {1.0, 0.5, 0.25, 0.125, 0.0625, 0.03125};
+    double scale[3] = {1.0, 1.0, 1.0};
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    auto time_cfg = [&]() -> float {
+      for (auto* m : b->members) m->par_scale = scale[batch_class(m)];
+      batch_ensure(b, 1, false);
+      batch_capture(b, algo, false);
+      batch_prepare(b);
+      CK(cudaGraphLaunch(b->gexec, b->master));  // warm-up
+      CK(cudaEventRecord(e0, b->master));
+      for (int t = 0; t < trials; ++t) CK(cudaGraphLaunch(b->gexec, b->master));
+      CK(cudaEventRecord(e1, b->master));
+      batch_finish(b);
+      float ms = 0.f;
+      CK(cudaEventElapsedTime(&ms, e0, e1));
+      return ms / trials;
+    };
+    float best = time_cfg();
+    for (int cls = 0; cls < 3; ++cls) {
+      bool present = false;
+      for (auto* m : b->members) present |= batch_class(m) == cls;
+      if (!present) continue;
+      double keep = scale[cls];
+      for (double cv : cand) {
+        if (cv == keep) continue;
+        scale[cls] = cv;
+        float t = time_cfg();
+        if (t < best) {
+          best = t;
+          keep = cv;
+        }
+      }
+      scale[cls] = keep;
+    }
+    for (auto* m : b->members) m->par_scale = scale[batch_class(m)];
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    batch_reset_graph(b);
+    for (size_t i = 0; i < b->members.size(); ++i) {
+      planc_gpu_ctx* m = b->members[i];
+      std::vector<const double*> ptr(m->N);
+      for (int n = 0; n < m->N; ++n) ptr[n] = saved[i][n].data();
+      int rc = planc_gpu_set_factors(m, ptr.data(), saved_lam[i].data(), m->k);
+      if (rc != PLANC_GPU_OK) throw Fail{rc};
+    }
+    if (best_ms) *best_ms = best;
+  });
+}
+
+int planc_gpu_batch_destroy(planc_gpu_batch* b) {
+  if (!b) return PLANC_GPU_OK;
+  return guarded([&] {
+    cudaSetDevice(b->device);
+    cudaStreamSynchronize(b->master);
+    batch_reset_graph(b);
+    for (auto* m : b->members) planc_gpu_destroy(m);
+    for (auto w : b->workers) cudaStreamDestroy(w);
+    for (auto e : b->joins) cudaEventDestroy(e);
+    cudaEventDestroy(b->fork);
+    cudaStreamDestroy(b->master);
+    delete b;
   });
 }
 
