@@ -51,6 +51,9 @@ def parse():
     ap.add_argument("--no-fp64", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--workload", default="cfg2", choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5"],
+                    help="cfg2 (default) is the metric's workload; the others are the remaining "
+                         "synthetic configurations, measured with the same JSON contract")
     return ap.parse_args()
 
 
@@ -240,6 +243,10 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         reference_arm(args, rank, world)
+        return
+    if args.workload != "cfg2":
+        import bench_configs
+        bench_configs.run(args, rank, world, local)
         return
     import torch
     import planc_b200 as gpu

@@ -1,0 +1,236 @@
+"""The synthetic configurations other than the headline one, measured with
+the bench.py JSON contract (python bench.py --workload cfgN ...):
+
+  cfg1  64x64x64 FP64 tensor, rank-8 CP + 1 % noise, HALS k=8, 20 iterations,
+        FP64 plain path (latency-bound: one CUDA graph per iteration); parity
+        against the CPU oracle on the same inputs is reported.
+  cfg3  192x192x192x192 FP32 tensor from a rank-64 CP model with half of the
+        factor entries zeroed, + 1 % noise; ANLS/BPP k=64, 30 iterations,
+        BF16 tensor-core MTTKRP, one batched BPP launch per mode; FP64 plain
+        path alongside.
+  cfg4  256 independent 3-way FP32 tensors, mode sizes U{32..256}, ranks
+        U{4,8,16,32}, CP + 1 % noise; HALS, one CUDA-graph launch per
+        iteration for all 256 tensors, autotuned per-launch parallelism.
+  cfg5  512^3 BF16 CP loss 1/2||X - [[A,B,C]]||^2 (rank 32, 5 % noise),
+        torch.autograd with the MTTKRP kernels as backward, projected
+        accelerated gradient steps on the factor leaves.
+
+A step is one outer iteration (cfg1, cfg3), one batched iteration of all
+256 tensors (cfg4) or one forward+backward+update (cfg5). Inputs are
+generated on the device and stay resident; the timed region is bracketed by
+synchronisation and timed with CUDA events on the launching stream.
+"""
+import json
+import time
+
+import numpy as np
+
+METRIC = "NTF iters/s + MTTKRP TFLOP/s, mixed vs FP64 plain on same GPU, equal rel-error"
+
+
+def _synth(gpu, torch, dev, dims, A, sigma, seed, dtype="f32"):
+    n = int(np.prod(dims))
+    X = torch.empty(n, dtype=torch.float32 if dtype == "f32" else torch.float64,
+                    device="cuda:%d" % dev)
+    gpu.synth_cp_tensor(dev, X.data_ptr(), dtype, dims, A, sigma, seed, clip=True)
+    return X
+
+
+def _sigma(A, rho):
+    k = A[0].shape[1]
+    G = np.ones((k, k))
+    for a in A:
+        G *= a.T @ a
+    return rho * np.sqrt(G.sum() / float(np.prod([a.shape[0] for a in A])))
+
+
+def _time_run(torch, ctx, algo, steps, err=True):
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n0 = ctx.launch_count()
+    e0.record(stream)
+    errs = ctx.run(algo, steps, compute_error=err)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1), errs, ctx.launch_count() - n0
+
+
+def _line(args, world, value, unit, ms_per_step, dtype, config, **extra):
+    line = {"metric": METRIC, "value": value, "unit": unit, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": dtype, "data": "synthetic",
+            "config": config}
+    line.update(extra)
+    return line
+
+
+def cfg1(args, gpu, torch, dev):
+    import oracle
+    dims, k, T = (64, 64, 64), 8, 20
+    rng = np.random.default_rng(101)
+    A = [rng.random((d, k)) for d in dims]
+    Xd = _synth(gpu, torch, dev, dims, A, _sigma(A, 0.01), 11, dtype="f64")
+    X = Xd.cpu().numpy().reshape(dims, order="F")
+    F0 = [np.random.default_rng(102).random((d, k)) for d in dims]
+    with gpu.Context(dev, "fp64") as c:
+        c.set_tensor(X)
+        c.set_factors(F0)
+        c.run("hals", args.warmup)
+        c.set_factors(F0)
+        ms, errs, launches = _time_run(torch, c, "hals", T)
+        Fg, lg = c.get_factors()
+    t0 = time.perf_counter()
+    Fo, lo, eo = oracle.ntf_run(X, F0, "hals", T)
+    cpu_s = time.perf_counter() - t0
+    par_err = float(np.max(np.abs(errs - eo) / eo))
+    par_f = max(float(np.abs(a - b).max() / np.abs(b).max()) for a, b in zip(Fg, Fo))
+    return _line(args, 1, T / (ms * 1e-3), "iters/s", ms / T, "f64",
+                 {"workload": "64x64x64 FP64, rank-8 CP + 1% noise, HALS k=8, 20 iterations, "
+                              "dimension tree, FP64 plain path", "dims": list(dims), "rank": k},
+                 us_per_iter=1e3 * ms / T, gpu_launches=launches, launches_per_iter=launches / T,
+                 parity_vs_oracle={"max_rel_err_diff": par_err, "max_rel_factor_diff": par_f,
+                                   "bar": 1e-10},
+                 cpu_baseline={"value": T / cpu_s, "unit": "iters/s", "cores": 1, "kind": "port",
+                               "sample": "the whole 20-iteration run, oracle restatement"})
+
+
+def cfg3(args, gpu, torch, dev):
+    dims, k, T = (192, 192, 192, 192), 64, 30
+    rng = np.random.default_rng(301)
+    A = []
+    for d in dims:
+        a = rng.random((d, k))
+        a[rng.random(a.shape) < 0.5] = 0.0
+        A.append(a)
+    X = _synth(gpu, torch, dev, dims, A, _sigma(A, 0.01), 31)
+    F0 = [np.random.default_rng(302).random((d, k)) for d in dims]
+    out = {}
+    for prec in ("bf16", "fp64"):
+        with gpu.Context(dev, prec) as c:
+            c.set_tensor(X.data_ptr(), dims=dims, dtype="f32")
+            c.set_factors(F0)
+            c.run("anlsbpp", max(args.warmup, 1), compute_error=False)
+            c.set_factors(F0)
+            c.set_timing(True)
+            c.kernel_times()
+            ms, errs, launches = _time_run(torch, c, "anlsbpp", T)
+            kt = c.kernel_times()
+            out[prec] = (ms, errs, launches, kt)
+    ms, errs, launches, kt = out["bf16"]
+    ms64, errs64, _, kt64 = out["fp64"]
+    return _line(args, 1, T / (ms * 1e-3), "iters/s", ms / T, "bf16",
+                 {"workload": "192^4 FP32 tensor, rank-64 sparse-factor CP + 1% noise, ANLS/BPP "
+                              "k=64, 30 iterations, dimension tree, BF16 tensor-core MTTKRP",
+                  "dims": list(dims), "rank": k},
+                 fp64_plain={"value": T / (ms64 * 1e-3), "unit": "iters/s", "ms_per_step": ms64 / T},
+                 speedup_vs_fp64=ms64 / ms,
+                 rel_error={"mixed": float(errs[-1]), "fp64": float(errs64[-1]),
+                            "abs_diff": float(abs(errs[-1] - errs64[-1]))},
+                 kernel_ms_per_iter={kk: round(v[0] / T, 4) for kk, v in kt.items() if v[1]},
+                 kernel_ms_per_iter_fp64={kk: round(v[0] / T, 4) for kk, v in kt64.items() if v[1]},
+                 gpu_launches=launches)
+
+
+def cfg4(args, gpu, torch, dev):
+    T = 100
+    rng = np.random.default_rng(401)
+    specs = [(tuple(int(d) for d in rng.integers(32, 257, size=3)), int(rng.choice([4, 8, 16, 32])))
+             for _ in range(256)]
+    b = gpu.Batch(dev, "bf16", nstreams=64)
+    total = 0
+    for i, (dims, k) in enumerate(specs):
+        r = np.random.default_rng(1000 + i)
+        A = [r.random((d, k)) for d in dims]
+        X = _synth(gpu, torch, dev, dims, A, _sigma(A, 0.01), 2000 + i)
+        b.add(X.data_ptr(), [r.random((d, k)) for d in dims], dims=dims, dtype="f32")
+        total += int(np.prod(dims))
+        del X
+    t0 = time.perf_counter()
+    tuned_ms = b.autotune("hals", trials=2)
+    tune_s = time.perf_counter() - t0
+    b.run("hals", args.warmup, compute_error=False)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    errs = b.run("hals", T, compute_error=True)
+    wall = time.perf_counter() - t0
+    b.close()
+    return _line(args, 1, T / wall, "batched iters/s (256 tensors)", 1e3 * wall / T, "bf16",
+                 {"workload": "256 independent 3-way FP32 tensors, dims U{32..256}, ranks "
+                              "U{4,8,16,32}, HALS, one CUDA-graph launch per batched iteration",
+                  "tensors": 256, "total_elements": total},
+                 timing="host wall clock around batch_run (its graph launches and the final "
+                        "synchronisation), 100 iterations",
+                 autotune={"best_ms_per_iter": tuned_ms, "tuning_seconds": tune_s},
+                 final_rel_error={"median": float(np.median(errs[:, -1])),
+                                  "max": float(np.max(errs[:, -1]))},
+                 tensors_per_s=256 * T / wall)
+
+
+def cfg5(args, gpu, torch, dev):
+    from planc_b200.autograd import CPLoss
+    dims, k, T = (512, 512, 512), 32, 200
+    rng = np.random.default_rng(501)
+    A = [rng.random((d, k)) for d in dims]
+    X = _synth(gpu, torch, dev, dims, A, _sigma(A, 0.05), 51)
+    lossf = CPLoss(X, dims=dims, rank=k, precision="bf16", device=dev)
+    F = [torch.tensor(np.random.default_rng(502 + i).random((d, k)), device="cuda:%d" % dev,
+                      dtype=torch.float64, requires_grad=True) for i, d in enumerate(dims)]
+    Y = [f.detach().clone() for f in F]
+
+    def step(F, Y, Fprev, t, eta):
+        # projected accelerated gradient on all factors from one forward+backward
+        for y in Y:
+            y.requires_grad_(True)
+            y.grad = None
+        loss = lossf(*Y)
+        loss.backward()
+        with torch.no_grad():
+            newF = [(y - eta * y.grad).clamp_(min=0.0) for y in Y]
+            t_next = 0.5 * (1 + (1 + 4 * t * t) ** 0.5)
+            mom = (t - 1) / t_next
+            newY = [nf + mom * (nf - fp) for nf, fp in zip(newF, Fprev)]
+        return newF, [y.detach() for y in newY], t_next, loss.detach()
+
+    with torch.no_grad():
+        Lmax = max(float(torch.linalg.matrix_norm((F[1].T @ F[1]) * (F[2].T @ F[2]), 2)),
+                   float(torch.linalg.matrix_norm((F[0].T @ F[0]) * (F[2].T @ F[2]), 2)),
+                   float(torch.linalg.matrix_norm((F[0].T @ F[0]) * (F[1].T @ F[1]), 2)))
+    eta = 1.0 / (3.0 * Lmax)
+    Fc = [f.detach() for f in F]
+    t = 1.0
+    for _ in range(args.warmup):
+        Fc, Y, t, l0 = step(Fc, Y, Fc, t, eta)
+    Fc = [f.detach() for f in F]
+    Y = [f.clone() for f in Fc]
+    t = 1.0
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    losses = []
+    for _ in range(T):
+        Fn, Y, t, loss = step(Fc, Y, Fc, t, eta)
+        Fc = Fn
+        losses.append(loss)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    lv = [float(x) for x in losses]
+    lossf.close()
+    return _line(args, 1, T / (ms * 1e-3), "steps/s", ms / T, "bf16",
+                 {"workload": "512^3 BF16 CP loss (rank 32, 5% noise), autograd with MTTKRP "
+                              "backward, 200 projected accelerated gradient steps",
+                  "dims": list(dims), "rank": k},
+                 loss_first=lv[0], loss_last=lv[-1],
+                 x_passes_per_step=2)
+
+
+def run(args, rank, world, local):
+    import torch
+    import planc_b200 as gpu
+    dev = local
+    torch.cuda.set_device(dev)
+    fn = {"cfg1": cfg1, "cfg3": cfg3, "cfg4": cfg4, "cfg5": cfg5}[args.workload]
+    line = fn(args, gpu, torch, dev)
+    if rank == 0:
+        print(json.dumps(line))

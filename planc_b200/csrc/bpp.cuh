@@ -16,7 +16,7 @@
 
 namespace pg {
 
-constexpr int BPP_WARPS = 1;  // columns per CTA (static shared memory <= 48 KB at k = 64)
+constexpr int BPP_WARPS = 2;  // right-hand sides per CTA (they share the AtA copy)
 
 __device__ __forceinline__ uint64_t warp_mask64(bool pred_lo, bool pred_hi) {
   uint64_t lo = __ballot_sync(0xffffffffu, pred_lo);
@@ -25,18 +25,24 @@ __device__ __forceinline__ uint64_t warp_mask64(bool pred_lo, bool pred_hi) {
 }
 
 // Cholesky solve of A z = rhs for the m x m matrix in A (column-major,
-// leading dimension ld, overwritten by L), rhs in/out in z. Warp-cooperative;
-// at step j lane l owns rows j+1+l, j+33+l. Returns false (A, z clobbered)
-// when a pivot is not positive and finite.
-__device__ bool warp_chol_solve(double* A, int ld, int m, double* z) {
+// leading dimension ld, overwritten by L), rhs in/out in z; dinv receives
+// 1/L(j,j), so the column scaling and both triangular solves multiply instead
+// of dividing (one division and one square root per column on the critical
+// path). Warp-cooperative; at step j lane l owns rows j+1+l, j+33+l.
+// Returns false (A, z clobbered) when a pivot is not positive and finite.
+__device__ bool warp_chol_solve(double* A, int ld, int m, double* z, double* dinv) {
   const int lane = threadIdx.x & 31;
   for (int j = 0; j < m; ++j) {
     double ajj = A[j + ld * j];
     if (!(ajj > 0.0) || !isfinite(ajj)) return false;  // uniform across the warp
-    double ljj = sqrt(ajj);
+    const double ljj = sqrt(ajj);
+    const double inv = 1.0 / ljj;
     __syncwarp();
-    for (int i = j + 1 + lane; i < m; i += 32) A[i + ld * j] = A[i + ld * j] / ljj;
-    if (lane == 0) A[j + ld * j] = ljj;
+    for (int i = j + 1 + lane; i < m; i += 32) A[i + ld * j] = A[i + ld * j] * inv;
+    if (lane == 0) {
+      A[j + ld * j] = ljj;
+      dinv[j] = inv;
+    }
     __syncwarp();
     for (int i = j + 1 + lane; i < m; i += 32) {
       double lij = A[i + ld * j];
@@ -45,14 +51,14 @@ __device__ bool warp_chol_solve(double* A, int ld, int m, double* z) {
     __syncwarp();
   }
   for (int j = 0; j < m; ++j) {  // L y = z
-    double yj = z[j] / A[j + ld * j];
+    double yj = z[j] * dinv[j];
     __syncwarp();
     if (lane == 0) z[j] = yj;
     for (int i = j + 1 + lane; i < m; i += 32) z[i] = fma(-A[i + ld * j], yj, z[i]);
     __syncwarp();
   }
   for (int j = m - 1; j >= 0; --j) {  // L^T x = y
-    double xj = z[j] / A[j + ld * j];
+    double xj = z[j] * dinv[j];
     __syncwarp();
     if (lane == 0) z[j] = xj;
     for (int i = lane; i < j; i += 32) z[i] = fma(-A[j + ld * i], xj, z[i]);
@@ -111,30 +117,37 @@ __device__ int warp_lu_solve(double* A, int ld, int m, double* z) {
   return 0;
 }
 
-// One warp per right-hand side c: AtA (n x n), rhs b_c = B[c*n .. c*n+n-1]
-// (row-major ncols x n == column-major n x ncols), X_c written the same way.
-// passive/iters (optional) receive the final passive set and the iteration
-// count. *status receives the most negative failure code (0 if none).
+// One warp per right-hand side c, BPP_WARPS right-hand sides per CTA: AtA
+// (n x n) is staged once in shared memory for all warps of the CTA; rhs
+// b_c = B[c*n .. c*n+n-1] (row-major ncols x n == column-major n x ncols),
+// X_c written the same way. passive/iters (optional) receive the final
+// passive set and the iteration count. *status receives the most negative
+// failure code (0 if none). Dynamic shared memory: bpp_smem_bytes(KP).
+__host__ __device__ constexpr size_t bpp_smem_bytes(int KP) {
+  return (size_t)KP * KP * 8 * (1 + BPP_WARPS) + (size_t)BPP_WARPS * (5 * KP * 8 + KP * 4);
+}
+
 template <int KP>
-__global__ void __launch_bounds__(32 * BPP_WARPS) k_bpp(const double* __restrict__ AtA,
+__global__ void __launch_bounds__(32 * BPP_WARPS) k_bpp(const double* __restrict__ AtA_g,
                                                         const double* __restrict__ Bm, int n,
                                                         int64_t ncols, double* __restrict__ Xout,
                                                         int* __restrict__ passive_out,
                                                         int* __restrict__ iters_out,
                                                         int* __restrict__ status, int max_iter_override) {
-  __shared__ double sA[BPP_WARPS][KP * KP];
-  __shared__ double sx[BPP_WARPS][KP], sy[BPP_WARPS][KP], sb[BPP_WARPS][KP];
-  __shared__ double sz[BPP_WARPS][KP];
-  __shared__ int sidx[BPP_WARPS][KP];
+  extern __shared__ __align__(16) unsigned char bpp_smem[];
+  double* AtA = reinterpret_cast<double*>(bpp_smem);  // n x n, leading dimension n
+  for (int e = threadIdx.x; e < n * n; e += blockDim.x) AtA[e] = AtA_g[e];
+  __syncthreads();
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* A = AtA + KP * KP + (size_t)w * (KP * KP + 5 * KP);
+  double* x = A + KP * KP;
+  double* y = x + KP;
+  double* b = y + KP;
+  double* z = b + KP;
+  double* dinv = z + KP;
+  int* idx = reinterpret_cast<int*>(AtA + KP * KP + (size_t)BPP_WARPS * (KP * KP + 5 * KP)) + w * KP;
   const int64_t c = (int64_t)blockIdx.x * BPP_WARPS + w;
-  if (c >= ncols) return;  // whole warp leaves together
-  double* A = sA[w];
-  double* x = sx[w];
-  double* y = sy[w];
-  double* b = sb[w];
-  double* z = sz[w];
-  int* idx = sidx[w];
+  if (c >= ncols) return;  // whole warp leaves together (no CTA barrier follows)
   const bool has_lo = lane < n, has_hi = lane + 32 < n;
   for (int i = lane; i < n; i += 32) {
     b[i] = Bm[c * n + i];
@@ -175,23 +188,22 @@ __global__ void __launch_bounds__(32 * BPP_WARPS) k_bpp(const double* __restrict
       passive ^= (1ull << rowidx);
     }
     // gather the passive submatrix, bppnnls.hpp:163-166 / 204-259
-    int m = __popcll(passive);
-    if (lane == 0) {
-      int q = 0;
-      for (int i = 0; i < n; ++i)
-        if ((passive >> i) & 1) idx[q++] = i;
-    }
+    const int m = __popcll(passive);
+    // idx[q] = position of the q-th passive index (warp-parallel compaction)
+    if ((passive >> lane) & 1) idx[__popcll(passive & ((1ull << lane) - 1ull))] = lane;
+    if ((passive >> (lane + 32)) & 1)
+      idx[__popcll(passive & ((1ull << (lane + 32)) - 1ull))] = lane + 32;
     __syncwarp();
     auto gather = [&]() {
       for (int e = lane; e < m * m; e += 32) {
         int ii = e % m, jj = e / m;
-        A[ii + KP * jj] = AtA[idx[ii] + (int64_t)n * idx[jj]];
+        A[ii + KP * jj] = AtA[idx[ii] + n * idx[jj]];
       }
       for (int i = lane; i < m; i += 32) z[i] = b[idx[i]];
       __syncwarp();
     };
     gather();
-    if (m > 0 && !warp_chol_solve(A, KP, m, z)) {
+    if (m > 0 && !warp_chol_solve(A, KP, m, z, dinv)) {
       gather();
       int rc = warp_lu_solve(A, KP, m, z);
       if (rc != 0) { st = rc; break; }
@@ -203,7 +215,7 @@ __global__ void __launch_bounds__(32 * BPP_WARPS) k_bpp(const double* __restrict
     // Y = AtA*X - AtB (bppnnls.hpp:167-168), then the 1e-12 zeroing (170-172)
     for (int i = lane; i < n; i += 32) {
       double acc = 0.0;
-      for (int j = 0; j < n; ++j) acc = fma(AtA[i + (int64_t)n * j], x[j], acc);
+      for (int j = 0; j < n; ++j) acc = fma(AtA[i + n * j], x[j], acc);
       double yi = acc - b[i];
       y[i] = (fabs(yi) < kEps12) ? 0.0 : yi;
       double xi = x[i];

@@ -182,7 +182,16 @@ __global__ void k_reduce_splits(const double* __restrict__ part, int nsplit, int
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     double s = 0.0;
-    for (int p = 0; p < nsplit; ++p) s += part[p * stride + i];
+    int p = 0;
+    for (; p + 4 <= nsplit; p += 4) {  // loads issued together, summed in order
+      const double v0 = part[p * stride + i], v1 = part[(p + 1) * stride + i];
+      const double v2 = part[(p + 2) * stride + i], v3 = part[(p + 3) * stride + i];
+      s += v0;
+      s += v1;
+      s += v2;
+      s += v3;
+    }
+    for (; p < nsplit; ++p) s += part[p * stride + i];
     out[i] = s;
   }
 }
@@ -270,6 +279,77 @@ __global__ void __launch_bounds__(256) k_ttv_right(const TT* __restrict__ T, int
     }
   }
   out[(int64_t)blockIdx.y * split_stride + e] = s;
+}
+
+// Tiled right multi-TTV: a CTA owns AT = 4096/KP consecutive a values (all
+// ranks) and a range of b; per b it reads the AT*k contiguous entries of
+// T[(a0..a0+AT-1) + A*b, :] (coalesced), each thread owning rank r = tid % KP
+// and 16 rows. W(b, r) comes from the row digits of b, advanced per step.
+// Writes one partial (A x k) per b-range; k_reduce_splits sums them.
+template <typename TT, int KP>
+__global__ void __launch_bounds__(256) k_ttv_right_tiled(const TT* __restrict__ T, int64_t A,
+                                                         int64_t B, int k, WGen wg,
+                                                         int64_t b_per_split,
+                                                         double* __restrict__ out) {
+  constexpr int J = 16;
+  constexpr int AT = J * 256 / KP;
+  constexpr int BC = 32;  // b values per shared-memory W chunk
+  __shared__ double Ws[BC][KP];
+  const int tid = threadIdx.x;
+  const int r = tid % KP;
+  const int arow = tid / KP;  // 0 .. 256/KP - 1
+  const int64_t a0 = (int64_t)blockIdx.x * AT;
+  const int64_t b0 = (int64_t)blockIdx.y * b_per_split;
+  int64_t b1 = b0 + b_per_split;
+  if (b1 > B) b1 = B;
+  double acc[J];
+#pragma unroll
+  for (int j = 0; j < J; ++j) acc[j] = 0.0;
+  const bool rok = r < k;
+  for (int64_t bc = b0; bc < b1; bc += BC) {
+    const int nb = (int)((b1 - bc) < BC ? (b1 - bc) : BC);
+    __syncthreads();
+    // W(b, r) for this chunk: thread tid < nb*KP computes one entry
+    for (int e = tid; e < nb * KP; e += 256) {
+      const int bb = e / KP, rr = e % KP;
+      Ws[bb][rr] = rr < k ? wgen_eval(wg, bc + bb, rr, k) : 0.0;
+    }
+    __syncthreads();
+    if (rok) {
+      const TT* Tb = T + (A * bc) * k + r;
+      const int64_t tstride = A * k;
+      int bb = 0;
+      for (; bb + 1 < nb; bb += 2) {
+        const double w0 = Ws[bb][r], w1 = Ws[bb + 1][r];
+        const TT* T0 = Tb + bb * tstride;
+        const TT* T1 = T0 + tstride;
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+          const int64_t a = a0 + arow + (int64_t)(256 / KP) * j;
+          if (a < A) {
+            const double x0 = (double)T0[a * k], x1 = (double)T1[a * k];
+            acc[j] = fma(x1, w1, fma(x0, w0, acc[j]));
+          }
+        }
+      }
+      if (bb < nb) {
+        const double w0 = Ws[bb][r];
+        const TT* T0 = Tb + bb * tstride;
+#pragma unroll
+        for (int j = 0; j < J; ++j) {
+          const int64_t a = a0 + arow + (int64_t)(256 / KP) * j;
+          if (a < A) acc[j] = fma((double)T0[a * k], w0, acc[j]);
+        }
+      }
+    }
+  }
+  if (!rok) return;
+  double* o = out + (int64_t)blockIdx.y * A * k;
+#pragma unroll
+  for (int j = 0; j < J; ++j) {
+    const int64_t a = a0 + arow + (int64_t)(256 / KP) * j;
+    if (a < A) o[a * k + r] = acc[j];
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -490,12 +570,6 @@ __global__ void __launch_bounds__(1024) k_gram_finalize(double* __restrict__ F, 
     const double la = lam[a], lb = lam[b];
     Gn[e] = (la > 0 && lb > 0) ? gs[e] / (la * lb) : gs[e];
   }
-  const int r = tid % k, lane = tid / k, lanes = 1024 / k;
-  if (lane < lanes) {
-    const double nrm = lam[r];
-    if (nrm > 0)
-      for (int64_t i = lane; i < I; i += lanes) F[i * k + r] = F[i * k + r] / nrm;
-  }
   if (next < 0) return;
   __syncthreads();
   for (int e = tid; e < kk2; e += 1024) {
@@ -503,6 +577,16 @@ __global__ void __launch_bounds__(1024) k_gram_finalize(double* __restrict__ F, 
     for (int i = 0; i < N; ++i)
       if (i != next) g = g * Gall[(int64_t)i * kk2 + e];
     Gloo[e] = g;
+  }
+}
+
+// F(:, r) /= lambda_r where lambda_r > 0 (ncpfactors.hpp:346-351), many CTAs.
+__global__ void __launch_bounds__(256) k_scale_cols(double* __restrict__ F, int64_t I, int k,
+                                                    const double* __restrict__ lambda) {
+  const int64_t n = I * k;
+  for (int64_t e = (int64_t)blockIdx.x * 256 + threadIdx.x; e < n; e += (int64_t)gridDim.x * 256) {
+    const double nrm = lambda[e % k];
+    if (nrm > 0) F[e] = F[e] / nrm;
   }
 }
 

@@ -91,6 +91,7 @@ struct planc_gpu_ctx {
   double* Q = nullptr;           // N = 4: P contracted with F_0, row-major (I1*I2) x k
   double* scratch = nullptr;
   size_t scratch_elems = 0;
+  double* lam_tmp = nullptr;    // lambda of a normalisation whose lambda is not kept
   double* gram_part = nullptr;  // per-row-block partial Grams
   size_t gram_part_elems = 0;
   double* errs_dev = nullptr;
@@ -247,11 +248,16 @@ struct TtvRightPlan {
   dim3 grid;
 };
 
+// Tiled right multi-TTV: a-tiles of 4096/KP rows; enough b-splits for about
+// two CTAs per SM, capped so the partials stay a small fraction of T.
 TtvRightPlan plan_ttv_right(planc_gpu_ctx* c, int64_t A, int64_t B) {
   TtvRightPlan p;
-  int64_t gx = (A * c->k + 255) / 256;
-  int64_t target = 8 * (int64_t)eff_sm(c);  // latency-bound loop: many warps per SM
-  int64_t ns = std::max<int64_t>(1, std::min<int64_t>((target + gx - 1) / gx, (B + 15) / 16));
+  const int KP = kpad(c->k);
+  const int64_t AT = 16 * 256 / KP;
+  const int64_t gx = (A + AT - 1) / AT;
+  const int64_t target = 2 * (int64_t)eff_sm(c);
+  int64_t ns = std::max<int64_t>(1, (target + gx - 1) / gx);
+  ns = std::min<int64_t>(ns, std::max<int64_t>(1, B / 8));  // >= 8 b per split
   ns = std::min<int64_t>(ns, 512);
   p.bper = (B + ns - 1) / ns;
   ns = (B + p.bper - 1) / p.bper;
@@ -368,7 +374,12 @@ void run_ttv_right(planc_gpu_ctx* c, const TT* T, int64_t A, int64_t B, const WG
   double* dst = p.nsplit > 1 ? c->scratch : out;
   int k = c->k;
   launch(c, KC_TTV, [&] {
-    k_ttv_right<TT><<<p.grid, 256, 0, c->stream>>>(T, A, B, k, wg, p.bper, A * k, dst);
+    switch (kpad(k)) {
+      case 8: k_ttv_right_tiled<TT, 8><<<p.grid, 256, 0, c->stream>>>(T, A, B, k, wg, p.bper, dst); break;
+      case 16: k_ttv_right_tiled<TT, 16><<<p.grid, 256, 0, c->stream>>>(T, A, B, k, wg, p.bper, dst); break;
+      case 32: k_ttv_right_tiled<TT, 32><<<p.grid, 256, 0, c->stream>>>(T, A, B, k, wg, p.bper, dst); break;
+      default: k_ttv_right_tiled<TT, 64><<<p.grid, 256, 0, c->stream>>>(T, A, B, k, wg, p.bper, dst); break;
+    }
   });
   if (p.nsplit > 1) {
     int64_t n = A * k;
@@ -523,8 +534,8 @@ void run_update(planc_gpu_ctx* c, int algo, int n) {
       switch (kpad(k)) {
 #define CASE(KP)                                                                                   \
   case KP:                                                                                         \
-    k_bpp<KP><<<blocks, 32 * BPP_WARPS, 0, c->stream>>>(c->Gloo, c->M[n], k, I, c->F[n], nullptr, \
-                                                        nullptr, c->status_dev, c->bpp_max_iter);  \
+    k_bpp<KP><<<blocks, 32 * BPP_WARPS, bpp_smem_bytes(KP), c->stream>>>(                      \
+        c->Gloo, c->M[n], k, I, c->F[n], nullptr, nullptr, c->status_dev, c->bpp_max_iter);        \
     break;
         CASE(8) CASE(16) CASE(32) CASE(64)
 #undef CASE
@@ -543,9 +554,15 @@ void normalize_gram(planc_gpu_ctx* c, int n, int next, double* lambda) {
   launch(c, KC_NORMGRAM, [&] {
     k_gram_partial<<<nblk, 256, 0, c->stream>>>(c->F[n], I, c->k, c->gram_part);
   });
+  double* lam = lambda ? lambda : c->lam_tmp;
   launch(c, KC_NORMGRAM, [&] {
-    k_gram_finalize<<<1, 1024, 0, c->stream>>>(c->F[n], I, c->k, c->gram_part, nblk, lambda,
+    k_gram_finalize<<<1, 1024, 0, c->stream>>>(c->F[n], I, c->k, c->gram_part, nblk, lam,
                                                c->Gall, c->N, n, next, c->Gloo);
+  });
+  launch(c, KC_NORMGRAM, [&] {
+    const int64_t ne = I * c->k;
+    k_scale_cols<<<(unsigned)std::min<int64_t>((ne + 255) / 256, 2048), 256, 0, c->stream>>>(
+        c->F[n], I, c->k, lam);
   });
 }
 
@@ -616,6 +633,7 @@ void free_all(planc_gpu_ctx* c) {
   }
   f(c->Gall);
   f(c->gram_part);
+  f(c->lam_tmp);
   c->gram_part_elems = 0;
   f(c->Gloo);
   f(c->lambda);
@@ -653,6 +671,17 @@ int planc_gpu_create(planc_gpu_ctx** out, int device, int precision, void* cuda_
     CK(cudaGetDeviceProperties(&prop, device));
     if (precision != PLANC_GPU_PREC_FP64 && prop.major < 10)
       fail(PLANC_GPU_ERR_UNSUPPORTED, "tensor-core precisions need an sm_100 device");
+    {
+      // k_bpp<64> needs more than the default 48 KB of dynamic shared memory
+      static bool attrs_set[64] = {false};
+      if (device < 64 && !attrs_set[device]) {
+        CK(cudaFuncSetAttribute(k_bpp<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)bpp_smem_bytes(64)));
+        CK(cudaFuncSetAttribute(k_bpp<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)bpp_smem_bytes(32)));
+        attrs_set[device] = true;
+      }
+    }
     planc_gpu_ctx* c = new planc_gpu_ctx();
     c->device = device;
     c->precision = precision;
@@ -834,6 +863,7 @@ int planc_gpu_set_factors(planc_gpu_ctx* c, const double* const* F, const double
     }
     dalloc(&c->Gloo, (size_t)k * k);
     dalloc(&c->lambda, (size_t)k);
+    dalloc(&c->lam_tmp, (size_t)k);
     // AUNTF::reset: update_factor_mode on every mode (normalise, Gram), then
     // set_lambda(new lambda)
     for (int n = 0; n < c->N; ++n) normalize_gram(c, n, n == c->N - 1 ? 0 : -1, c->lambda);
@@ -1038,8 +1068,8 @@ int planc_gpu_bpp_solve(planc_gpu_ctx* c, const double* AtA, const double* AtB, 
         switch (kpad(n)) {
 #define CASE(KP)                                                                            \
   case KP:                                                                                  \
-    k_bpp<KP><<<blocks, 32 * BPP_WARPS, 0, c->stream>>>(dA, dB, n, ncols, dX, dP, dI,      \
-                                                        c->status_dev, c->bpp_max_iter);    \
+    k_bpp<KP><<<blocks, 32 * BPP_WARPS, bpp_smem_bytes(KP), c->stream>>>(                    \
+        dA, dB, n, ncols, dX, dP, dI, c->status_dev, c->bpp_max_iter);                           \
     break;
           CASE(8) CASE(16) CASE(32) CASE(64)
 #undef CASE

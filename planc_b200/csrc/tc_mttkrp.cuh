@@ -171,6 +171,20 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float* v) {
   for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
 __device__ __forceinline__ void tmem_alloc(uint32_t dst_smem, uint32_t ncols) {
   asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst_smem),
                "r"(ncols)
@@ -668,6 +682,7 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
   __shared__ uint64_t bars[2 * 8 + 4];
   __shared__ uint32_t tmem_base_sh;
   __shared__ int abort_sh;
+  __shared__ double tail_w[4][KP];
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
   const uint32_t smem0 = smem_u32(smem);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -758,8 +773,10 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
       }
     }
   } else {
-    // drain warps 2..5: TMEM lane quarter = warp % 4
+    // drain warps 2..5: TMEM lane quarter = warp % 4. Each warp stages the
+    // run's tail(g, .) in its own shared-memory slice (no cross-warp wait).
     const int q4 = warp & 3;
+    double* tail = tail_w[warp - 2];
     Acc sum[MT][KP];
 #pragma unroll
     for (int mt = 0; mt < MT; ++mt)
@@ -772,22 +789,36 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
       const int64_t g = y + i * ns;
       const int64_t i1 = F2 ? g % D1 : g;
       const int64_t i2 = F2 ? g / D1 : 0;
+      __syncwarp();
+      for (int r = lane; r < KP; r += 32) {
+        double t = 0.0;
+        if (r < k) {
+          t = F1[i1 * k + r];
+          if (F2) t = t * F2[i2 * k + r];
+        }
+        tail[r] = t;
+      }
+      __syncwarp();
       if (!mbar_wait(accf(buf), aph[buf], abort_flag, status)) { ok = false; break; }
       tc_fence_after();
 #pragma unroll
       for (int mt = 0; mt < MT; ++mt) {
-#pragma unroll
-        for (int cc = 0; cc < NCOL; cc += 32) {
+        const uint32_t base = tmem + ((uint32_t)(q4 * 32) << 16) + buf * ACC_COLS + mt * NCOL;
+        if (KP == 16) {
           float v[32];
-          tmem_ld32(tmem + ((uint32_t)(q4 * 32) << 16) + buf * ACC_COLS + mt * NCOL + cc, v);
+          tmem_ld32(base, v);  // columns 0..15 hi, 16..31 lo
 #pragma unroll
-          for (int e = 0; e < 32; ++e) {
-            const int r = (cc + e) % KP;  // hi column, then lo column
-            if (r < k) {
-              double t = F1[i1 * k + r];
-              if (F2) t = t * F2[i2 * k + r];
-              sum[mt][r] += (Acc)(t * (double)v[e]);
-            }
+          for (int r = 0; r < 16; ++r)
+            sum[mt][r] += (Acc)(tail[r] * ((double)v[r] + (double)v[16 + r]));
+        } else {
+#pragma unroll
+          for (int cc = 0; cc < KP; cc += 16) {
+            float vh[16], vl[16];
+            tmem_ld16(base + cc, vh);
+            tmem_ld16(base + KP + cc, vl);
+#pragma unroll
+            for (int e = 0; e < 16; ++e)
+              sum[mt][cc + e] += (Acc)(tail[cc + e] * ((double)vh[e] + (double)vl[e]));
           }
         }
       }

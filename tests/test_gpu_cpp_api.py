@@ -1,0 +1,70 @@
+"""The C++ drop-in layer on the GPU: the dense_ntf driver (Tensor(dims) data,
+--init injection through AUNTF::reset, the reference's printed error lines)
+and a user AUNTF subclass with a host update(), both against the oracle."""
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+from helpers import init_factors, rel
+
+pytestmark = pytest.mark.gpu
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+PKG = os.path.join(ROOT, "planc_b200")
+
+
+def _compile(src, out):
+    cmd = ["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"),
+           "-I" + os.path.join(PKG, "cpp"), src, "-L" + PKG, "-lplanc_gpu",
+           "-Wl,-rpath," + PKG, "-o", out]
+    subprocess.run(cmd, check=True)
+
+
+def _write_init(prefix, F):
+    for n, f in enumerate(F):
+        np.savetxt("%s_%d.txt" % (prefix, n), f, fmt="%.17g")
+
+
+def _read_factors(prefix, N):
+    return [np.loadtxt("%s_%d.txt" % (prefix, n), ndmin=2) for n in range(N)]
+
+
+@pytest.mark.parametrize("algo,code", [("hals", 1), ("mu", 0), ("anlsbpp", 2)])
+def test_dense_ntf_driver_matches_oracle(gpu, oracle_lib, tmp_path, algo, code):
+    exe = str(tmp_path / "dense_ntf")
+    _compile(os.path.join(PKG, "cpp", "ntf.cpp"), exe)
+    dims, k, iters = (24, 20, 16), 4, 6
+    F0 = init_factors(dims, k, seed=60)
+    init = str(tmp_path / "init")
+    _write_init(init, F0)
+    out = str(tmp_path / "out")
+    res = subprocess.run([exe, "-a", str(code), "-d", " ".join(map(str, dims)), "-k", str(k),
+                          "-t", str(iters), "-e", "1", "--init", init, "-o", out],
+                         capture_output=True, text=True, check=True)
+    errs = [float(m) for m in re.findall(r"relative_error at it::\d+::([0-9.eE+-]+)", res.stdout)]
+    assert len(errs) == iters
+    X = oracle_lib.tensor_randu(dims, 103)  # Tensor(dims) data
+    Fo, lo, eo = oracle_lib.ntf_run(X, F0, algo, iters)
+    assert rel(np.array(errs), eo) < 1e-5  # printed with 6 significant digits
+    Fg = _read_factors(out, 3)
+    # the driver writes NCPFactors::factor(n) (I_n x k)
+    assert all(rel(a, b) < 1e-10 for a, b in zip(Fg, Fo))
+
+
+def test_custom_host_update_subclass(gpu, oracle_lib, tmp_path):
+    exe = str(tmp_path / "custom_update")
+    _compile(os.path.join(ROOT, "tests", "cpp", "custom_update.cpp"), exe)
+    dims, k, iters = (18, 15, 12), 3, 4
+    F0 = init_factors(dims, k, seed=61)
+    init, out = str(tmp_path / "init"), str(tmp_path / "out")
+    _write_init(init, F0)
+    res = subprocess.run([exe] + [str(d) for d in dims] + [str(k), str(iters), init, out],
+                         capture_output=True, text=True, check=True)
+    X = oracle_lib.tensor_randu(dims, 103)
+    Fo, lo, eo = oracle_lib.ntf_run(X, F0, "hals", iters)
+    Fg = _read_factors(out, 3)
+    assert all(rel(a, b) < 1e-10 for a, b in zip(Fg, Fo))
+    final = float(re.search(r"final_error ([0-9.eE+-]+)", res.stdout).group(1))
+    assert abs(final - eo[-1]) / eo[-1] < 1e-5
