@@ -24,52 +24,129 @@ __device__ __forceinline__ uint64_t warp_mask64(bool pred_lo, bool pred_hi) {
   return lo | (hi << 32);
 }
 
-// Cholesky solve of A z = rhs for the m x m matrix in A (column-major,
-// leading dimension ld, overwritten by L), rhs in/out in z; dinv receives
-// 1/L(j,j), so the column scaling and both triangular solves multiply instead
-// of dividing (one division and one square root per column on the critical
-// path). Warp-cooperative; at step j lane l owns rows j+1+l, j+33+l.
-// Returns false (A, z clobbered) when a pivot is not positive and finite.
-__device__ bool warp_chol_solve(double* A, int ld, int m, double* z, double* dinv) {
+// Blocked left-looking (Crout) Cholesky of the passive principal submatrix
+// A(i,j) = AtA[idx[i] + n*idx[j]], i,j < m, into Ls (column-major, leading
+// dimension KP+1: odd, so that walking a row and walking a column are both
+// free of shared-memory bank conflicts). Lane l owns rows l and l+32 of the
+// factor; inv[q] receives 1/L(row,row) for its rows. Columns go in panels of
+// NB: first every owned row at or below the panel takes the contribution of
+// all finished columns to the NB panel columns (NB independent accumulators
+// per row, one load of L(row,c) shared by NB fused multiply-adds), then the
+// panel is factored column by column in registers, the panel rows' entries
+// travelling by shuffle. Only the strict lower triangle is stored.
+// Returns false when a pivot is not positive and finite (uniform across the
+// warp), where the reference's Cholesky solve fails too.
+template <int KP>
+__device__ __forceinline__ bool warp_chol_crout(const double* __restrict__ AtA, int n, const int* idx,
+                                                int m, double* Ls, double (&inv)[KP > 32 ? 2 : 1]) {
+  constexpr int LD = KP + 1, R = KP > 32 ? 2 : 1, NB = 8;
   const int lane = threadIdx.x & 31;
-  for (int j = 0; j < m; ++j) {
-    double ajj = A[j + ld * j];
-    if (!(ajj > 0.0) || !isfinite(ajj)) return false;  // uniform across the warp
-    const double ljj = sqrt(ajj);
-    const double inv = 1.0 / ljj;
-    __syncwarp();
-    for (int i = j + 1 + lane; i < m; i += 32) A[i + ld * j] = A[i + ld * j] * inv;
-    if (lane == 0) {
-      A[j + ld * j] = ljj;
-      dinv[j] = inv;
-    }
-    __syncwarp();
-    for (int i = j + 1 + lane; i < m; i += 32) {
-      double lij = A[i + ld * j];
-      for (int c = j + 1; c <= i; ++c) A[i + ld * c] = fma(-lij, A[c + ld * j], A[i + ld * c]);
-    }
-    __syncwarp();
+  int gi[R];
+#pragma unroll
+  for (int q = 0; q < R; ++q) {
+    const int row = lane + 32 * q;
+    gi[q] = row < m ? idx[row] : 0;
+    inv[q] = 0.0;
   }
-  for (int j = 0; j < m; ++j) {  // L y = z
-    double yj = z[j] * dinv[j];
-    __syncwarp();
-    if (lane == 0) z[j] = yj;
-    for (int i = j + 1 + lane; i < m; i += 32) z[i] = fma(-A[i + ld * j], yj, z[i]);
-    __syncwarp();
-  }
-  for (int j = m - 1; j >= 0; --j) {  // L^T x = y
-    double xj = z[j] * dinv[j];
-    __syncwarp();
-    if (lane == 0) z[j] = xj;
-    for (int i = lane; i < j; i += 32) z[i] = fma(-A[j + ld * i], xj, z[i]);
+  for (int j0 = 0; j0 < m; j0 += NB) {
+    const int pw = min(NB, m - j0);
+    double acc[R][NB];
+#pragma unroll
+    for (int q = 0; q < R; ++q)
+#pragma unroll
+      for (int t = 0; t < NB; ++t) acc[q][t] = 0.0;
+    // contribution of the finished columns c < j0
+    for (int c = 0; c < j0; ++c) {
+      double lj[NB];
+#pragma unroll
+      for (int t = 0; t < NB; ++t) lj[t] = t < pw ? Ls[j0 + t + LD * c] : 0.0;
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int row = lane + 32 * q;
+        if (32 * q + 31 >= j0) {  // warp-uniform: some owned row of this slot is in play
+          const double li = (row >= j0 && row < m) ? Ls[row + LD * c] : 0.0;
+#pragma unroll
+          for (int t = 0; t < NB; ++t) acc[q][t] = fma(li, lj[t], acc[q][t]);
+        }
+      }
+    }
+#pragma unroll
+    for (int t = 0; t < NB; ++t) {
+      if (t < pw) {
+        const double* colA = AtA + (size_t)n * idx[j0 + t];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const int row = lane + 32 * q;
+          acc[q][t] = (row >= j0 && row < m) ? colA[gi[q]] - acc[q][t] : 0.0;
+        }
+      }
+    }
+    // factor the panel
+#pragma unroll
+    for (int t = 0; t < NB; ++t) {
+      if (t < pw) {
+        const int jj = j0 + t;
+        const double sjj = __shfl_sync(0xffffffffu, jj < 32 ? acc[0][t] : acc[R - 1][t], jj & 31);
+        if (!(sjj > 0.0) || !isfinite(sjj)) return false;
+        const double ij = rsqrt(sjj);
+        double lcol[R];
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const int row = lane + 32 * q;
+          lcol[q] = acc[q][t] * ij;
+          if (row > jj && row < m) Ls[row + LD * jj] = lcol[q];
+          if (row == jj) inv[q] = ij;
+        }
+#pragma unroll
+        for (int t2 = t + 1; t2 < NB; ++t2) {
+          if (t2 < pw) {
+            const int r2 = j0 + t2;
+            const double l2 = __shfl_sync(0xffffffffu, r2 < 32 ? lcol[0] : lcol[R - 1], r2 & 31);
+#pragma unroll
+            for (int q = 0; q < R; ++q) acc[q][t2] = fma(-lcol[q], l2, acc[q][t2]);
+          }
+        }
+      }
+    }
     __syncwarp();
   }
   return true;
 }
 
+// Forward and back substitution with the factor of warp_chol_crout: z (the
+// owned rows' right-hand side) becomes the solution in place. Each step is
+// one shuffle of the finished entry plus one fused multiply-add per owned
+// row; the factor entries are independent loads that the compiler hoists.
+template <int KP>
+__device__ __forceinline__ void warp_chol_subst(const double* Ls, int m, const double (&inv)[KP > 32 ? 2 : 1],
+                                double (&z)[KP > 32 ? 2 : 1]) {
+  constexpr int LD = KP + 1, R = KP > 32 ? 2 : 1;
+  const int lane = threadIdx.x & 31;
+  for (int j = 0; j < m; ++j) {  // L y = z
+    const double t = j < 32 ? z[0] * inv[0] : z[R - 1] * inv[R - 1];
+    const double yj = __shfl_sync(0xffffffffu, t, j & 31);
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int row = lane + 32 * q;
+      if (row == j) z[q] = yj;
+      else if (row > j && row < m) z[q] = fma(-Ls[row + LD * j], yj, z[q]);
+    }
+  }
+  for (int j = m - 1; j >= 0; --j) {  // L^T x = y
+    const double t = j < 32 ? z[0] * inv[0] : z[R - 1] * inv[R - 1];
+    const double xj = __shfl_sync(0xffffffffu, t, j & 31);
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int row = lane + 32 * q;
+      if (row == j) z[q] = xj;
+      else if (row < j) z[q] = fma(-Ls[j + LD * row], xj, z[q]);
+    }
+  }
+}
+
 // Gaussian elimination with partial pivoting (the general-solver fallback of
 // a failed Cholesky). Returns 0 or kStSingular.
-__device__ int warp_lu_solve(double* A, int ld, int m, double* z) {
+__device__ __forceinline__ int warp_lu_solve(double* A, int ld, int m, double* z) {
   const int lane = threadIdx.x & 31;
   for (int j = 0; j < m; ++j) {
     double best = -1.0;
@@ -123,29 +200,46 @@ __device__ int warp_lu_solve(double* A, int ld, int m, double* z) {
 // X_c written the same way. passive/iters (optional) receive the final
 // passive set and the iteration count. *status receives the most negative
 // failure code (0 if none). Dynamic shared memory: bpp_smem_bytes(KP).
+// Per warp: the factor (KP x (KP+1)), x, y, b and the compacted solution zs
+// (KP each), and the passive index list idx (KP ints).
 __host__ __device__ constexpr size_t bpp_smem_bytes(int KP) {
-  return (size_t)KP * KP * 8 * (1 + BPP_WARPS) + (size_t)BPP_WARPS * (5 * KP * 8 + KP * 4);
+  return (size_t)KP * KP * 8 + (size_t)BPP_WARPS * ((size_t)KP * (KP + 1) * 8 + 4 * KP * 8 + KP * 4);
 }
 
 template <int KP>
-__global__ void __launch_bounds__(32 * BPP_WARPS) k_bpp(const double* __restrict__ AtA_g,
+__global__ void __launch_bounds__(32 * BPP_WARPS, 1) k_bpp(const double* __restrict__ AtA_g,
                                                         const double* __restrict__ Bm, int n,
                                                         int64_t ncols, double* __restrict__ Xout,
                                                         int* __restrict__ passive_out,
                                                         int* __restrict__ iters_out,
                                                         int* __restrict__ status, int max_iter_override) {
+  constexpr int LD = KP + 1, R = KP > 32 ? 2 : 1;
   extern __shared__ __align__(16) unsigned char bpp_smem[];
   double* AtA = reinterpret_cast<double*>(bpp_smem);  // n x n, leading dimension n
-  for (int e = threadIdx.x; e < n * n; e += blockDim.x) AtA[e] = AtA_g[e];
+  {
+    const int nn = n * n;
+    for (int e0 = threadIdx.x; e0 < nn; e0 += 8 * blockDim.x) {
+      double v[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int e = e0 + u * blockDim.x;
+        v[u] = e < nn ? __ldg(AtA_g + e) : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int e = e0 + u * blockDim.x;
+        if (e < nn) AtA[e] = v[u];
+      }
+    }
+  }
   __syncthreads();
   const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  double* A = AtA + KP * KP + (size_t)w * (KP * KP + 5 * KP);
-  double* x = A + KP * KP;
+  double* Ls = AtA + KP * KP + (size_t)w * (KP * LD + 4 * KP);
+  double* x = Ls + KP * LD;
   double* y = x + KP;
   double* b = y + KP;
-  double* z = b + KP;
-  double* dinv = z + KP;
-  int* idx = reinterpret_cast<int*>(AtA + KP * KP + (size_t)BPP_WARPS * (KP * KP + 5 * KP)) + w * KP;
+  double* zs = b + KP;
+  int* idx = reinterpret_cast<int*>(AtA + KP * KP + (size_t)BPP_WARPS * (KP * LD + 4 * KP)) + w * KP;
   const int64_t c = (int64_t)blockIdx.x * BPP_WARPS + w;
   if (c >= ncols) return;  // whole warp leaves together (no CTA barrier follows)
   const bool has_lo = lane < n, has_hi = lane + 32 < n;
@@ -187,38 +281,65 @@ __global__ void __launch_bounds__(32 * BPP_WARPS) k_bpp(const double* __restrict
       int rowidx = 63 - __clzll(nonopt | infea);
       passive ^= (1ull << rowidx);
     }
-    // gather the passive submatrix, bppnnls.hpp:163-166 / 204-259
+    // solve the passive system AtA(P,P) x_P = AtB(P), bppnnls.hpp:163-166 / 204-259
     const int m = __popcll(passive);
     // idx[q] = position of the q-th passive index (warp-parallel compaction)
     if ((passive >> lane) & 1) idx[__popcll(passive & ((1ull << lane) - 1ull))] = lane;
     if ((passive >> (lane + 32)) & 1)
       idx[__popcll(passive & ((1ull << (lane + 32)) - 1ull))] = lane + 32;
     __syncwarp();
-    auto gather = [&]() {
-      for (int e = lane; e < m * m; e += 32) {
-        int ii = e % m, jj = e / m;
-        A[ii + KP * jj] = AtA[idx[ii] + n * idx[jj]];
-      }
-      for (int i = lane; i < m; i += 32) z[i] = b[idx[i]];
-      __syncwarp();
-    };
-    gather();
-    if (m > 0 && !warp_chol_solve(A, KP, m, z, dinv)) {
-      gather();
-      int rc = warp_lu_solve(A, KP, m, z);
-      if (rc != 0) { st = rc; break; }
+    double z[R];
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int row = lane + 32 * q;
+      z[q] = row < m ? b[idx[row]] : 0.0;
     }
+    double inv[R];
+    if (m > 0) {
+      if (warp_chol_crout<KP>(AtA, n, idx, m, Ls, inv)) {
+        warp_chol_subst<KP>(Ls, m, inv, z);
+      } else {  // not positive definite: the general solver, as arma::solve falls back
+        for (int e = lane; e < m * m; e += 32) {
+          const int ii = e % m, jj = e / m;
+          Ls[ii + LD * jj] = AtA[idx[ii] + n * idx[jj]];
+        }
+        for (int i = lane; i < m; i += 32) zs[i] = b[idx[i]];
+        __syncwarp();
+        const int rc = warp_lu_solve(Ls, LD, m, zs);
+        if (rc != 0) { st = rc; break; }
+        __syncwarp();
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const int row = lane + 32 * q;
+          z[q] = row < m ? zs[row] : 0.0;
+        }
+      }
+    }
+    // scatter: X(P) = x_P, X(~P) = 0
     for (int i = lane; i < n; i += 32) x[i] = 0.0;
     __syncwarp();
-    for (int i = lane; i < m; i += 32) x[idx[i]] = z[i];
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int row = lane + 32 * q;
+      if (row < m) {
+        x[idx[row]] = z[q];
+        zs[row] = z[q];
+      }
+    }
     __syncwarp();
-    // Y = AtA*X - AtB (bppnnls.hpp:167-168), then the 1e-12 zeroing (170-172)
+    // Y = AtA*X - AtB over the passive columns (bppnnls.hpp:167-168), then the
+    // 1e-12 zeroing of X and Y (bppnnls.hpp:170-172)
     for (int i = lane; i < n; i += 32) {
-      double acc = 0.0;
-      for (int j = 0; j < n; ++j) acc = fma(AtA[i + n * j], x[j], acc);
-      double yi = acc - b[i];
+      double a0 = 0.0, a1 = 0.0;
+      int q = 0;
+      for (; q + 2 <= m; q += 2) {
+        a0 = fma(AtA[i + n * idx[q]], zs[q], a0);
+        a1 = fma(AtA[i + n * idx[q + 1]], zs[q + 1], a1);
+      }
+      if (q < m) a0 = fma(AtA[i + n * idx[q]], zs[q], a0);
+      const double yi = (a0 + a1) - b[i];
       y[i] = (fabs(yi) < kEps12) ? 0.0 : yi;
-      double xi = x[i];
+      const double xi = x[i];
       if (!isfinite(xi) || !isfinite(yi)) st = kStNonFinite;
       x[i] = (fabs(xi) < kEps12) ? 0.0 : xi;
     }
