@@ -6,8 +6,9 @@ the bench.py JSON contract (python bench.py --workload cfgN ...):
         against the CPU oracle on the same inputs is reported.
   cfg3  192x192x192x192 FP32 tensor from a rank-64 CP model with half of the
         factor entries zeroed, + 1 % noise; ANLS/BPP k=64, 30 iterations,
-        BF16 tensor-core MTTKRP, one batched BPP launch per mode; FP64 plain
-        path alongside.
+        BF16 tensor-core MTTKRP on the balanced 4-way tree, one batched BPP
+        launch per mode; split-BF16 (bf16x2) and the FP64 plain path
+        alongside.
   cfg4  256 independent 3-way FP32 tensors, mode sizes U{32..256}, ranks
         U{4,8,16,32}, CP + 1 % noise; HALS, one CUDA-graph launch per
         iteration for all 256 tensors, autotuned per-launch parallelism.
@@ -106,7 +107,7 @@ def cfg3(args, gpu, torch, dev):
     X = _synth(gpu, torch, dev, dims, A, _sigma(A, 0.01), 31)
     F0 = [np.random.default_rng(302).random((d, k)) for d in dims]
     out = {}
-    for prec in ("bf16", "fp64"):
+    for prec in ("bf16x2", "bf16", "fp64"):
         with gpu.Context(dev, prec) as c:
             c.set_tensor(X.data_ptr(), dims=dims, dtype="f32")
             c.set_factors(F0)
@@ -117,16 +118,23 @@ def cfg3(args, gpu, torch, dev):
             ms, errs, launches = _time_run(torch, c, "anlsbpp", T)
             kt = c.kernel_times()
             out[prec] = (ms, errs, launches, kt)
+    # headline: single BF16 (stochastically rounded tensor); the split-BF16
+    # run is reported beside it
     ms, errs, launches, kt = out["bf16"]
+    ms1, errs1, _, kt1 = out["bf16x2"]
     ms64, errs64, _, kt64 = out["fp64"]
     return _line(args, 1, T / (ms * 1e-3), "iters/s", ms / T, "bf16",
                  {"workload": "192^4 FP32 tensor, rank-64 sparse-factor CP + 1% noise, ANLS/BPP "
-                              "k=64, 30 iterations, dimension tree, BF16 tensor-core MTTKRP",
-                  "dims": list(dims), "rank": k},
+                              "k=64, 30 iterations, balanced dimension tree, BF16 tensor-core "
+                              "MTTKRP", "dims": list(dims), "rank": k},
                  fp64_plain={"value": T / (ms64 * 1e-3), "unit": "iters/s", "ms_per_step": ms64 / T},
                  speedup_vs_fp64=ms64 / ms,
                  rel_error={"mixed": float(errs[-1]), "fp64": float(errs64[-1]),
                             "abs_diff": float(abs(errs[-1] - errs64[-1]))},
+                 bf16x2={"value": T / (ms1 * 1e-3), "unit": "iters/s",
+                              "speedup_vs_fp64": ms64 / ms1, "rel_error": float(errs1[-1]),
+                              "abs_diff_vs_fp64": float(abs(errs1[-1] - errs64[-1])),
+                              "kernel_ms_per_iter": {kk: round(v[0] / T, 4) for kk, v in kt1.items() if v[1]}},
                  kernel_ms_per_iter={kk: round(v[0] / T, 4) for kk, v in kt.items() if v[1]},
                  kernel_ms_per_iter_fp64={kk: round(v[0] / T, 4) for kk, v in kt64.items() if v[1]},
                  gpu_launches=launches)

@@ -145,10 +145,11 @@ int planc_gpu_bpp_solve(planc_gpu_ctx* ctx, const double* AtA, const double* AtB
  * I_n x k FP64, k = the rank set by planc_gpu_set_factors, on the context's
  * device), written to the device buffer M_dev (row-major I_mode x k FP64).
  * The context's own factors are not touched. flags: bit 0 = dimension tree
- * (N in {3,4}); bit 1 = reuse the partial MTTKRP left by the previous call of
- * mode 0 (and, for N = 4 mode 2, of mode 1) made with the same factors, the
- * in-order reuse of DenseDimensionTree::in_order_reuse_MTTKRP
- * (dimtree/ddt.hpp:134-243). Runs on the context's stream and returns without
+ * (N in {3,4}); bit 1 = reuse the partial MTTKRPs left by the previous calls
+ * of the modes before `mode` in its branch of the tree, made in order with the
+ * same factors (the in-order reuse of
+ * DenseDimensionTree::in_order_reuse_MTTKRP, dimtree/ddt.hpp:134-243); without
+ * it those modes' partial contractions are recomputed first. Runs on the context's stream and returns without
  * synchronising. This is the adjoint used by the differentiable CP loss. */
 int planc_gpu_mttkrp_device(planc_gpu_ctx* ctx, int mode, const double* const* F_dev,
                             double* M_dev, int flags);

@@ -10,8 +10,8 @@ with M_n the mode-n MTTKRP. The gradient is the reference's NTF gradient form
 
 The forward pass runs the mode-0 MTTKRP on the tensor-core (or FP64) kernel
 of a planc_b200.Context; the hand-written backward runs the remaining modes'
-MTTKRPs on the same kernels (mode 1 reuses the dimension tree's partial
-contraction from the forward pass, the last mode is the left contraction), so
+MTTKRPs on the same kernels (the modes after 0 reuse the dimension tree's
+partial contractions in order, starting from the forward pass's mode 0), so
 one forward + backward reads X twice. Factors are float64 CUDA tensors of
 shape (I_n, k), contiguous (row-major, the library's factor layout).
 """
@@ -55,13 +55,13 @@ class _CPLoss(torch.autograd.Function):
         stream = torch.cuda.ExternalStream(handle.stream, device=dev)
         ptrs = [f.data_ptr() for f in factors]
         N = len(factors)
-        s = N // 2
         Ms = [M0]
         stream.wait_stream(torch.cuda.current_stream(dev))
         for n in range(1, N):
             Mn = torch.empty_like(factors[n])
-            # modes 1..s reuse the partial contraction of the forward's mode 0
-            handle.mttkrp_device(n, ptrs, Mn.data_ptr(), dimtree=True, reuse=(n <= s))
+            # in-order sweep with unchanged factors: every mode reuses the tree
+            # state left by the previous ones (the forward's mode 0 included)
+            handle.mttkrp_device(n, ptrs, Mn.data_ptr(), dimtree=True, reuse=True)
             Ms.append(Mn)
         torch.cuda.current_stream(dev).wait_stream(stream)
         grams = [f.T @ f for f in factors]

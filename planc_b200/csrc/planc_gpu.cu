@@ -61,6 +61,11 @@ int guarded(F&& f) {
 
 int kpad(int k) { return k <= 8 ? 8 : k <= 16 ? 16 : k <= 32 ? 32 : 64; }
 
+// Longest Khatri-Rao operand (rows) of the balanced 4-way tree: at rank 64
+// its hi|lo image is 256 B a row, 32 MiB at this bound, small enough to stay
+// in L2 while every CTA of the long-K contraction streams it.
+constexpr int64_t kBal4MaxK = int64_t(1) << 17;
+
 }  // namespace
 
 struct planc_gpu_ctx {
@@ -75,6 +80,9 @@ struct planc_gpu_ctx {
   int64_t numel = 0;
   int s = 0;
   int64_t L = 0, R = 0;
+  // 4-way tensor on the tensor-core paths: balanced tree {0,1} | {2,3} (see
+  // mttkrp_bal4) instead of the reference's {0,1,2} | {3}.
+  bool bal4 = false;
   int k = 0;
   bool have_tensor = false, have_factors = false;
 
@@ -88,7 +96,8 @@ struct planc_gpu_ctx {
   double* lambda = nullptr;
   double* P = nullptr;           // right-contracted partial MTTKRP, row-major L x k
   float* P32 = nullptr;          // same, FP32, for the tensor-core paths
-  double* Q = nullptr;           // N = 4: P contracted with F_0, row-major (I1*I2) x k
+  double* Q = nullptr;           // N = 4: P contracted with F_0, row-major (I1*I2) x k;
+                                 // balanced 4-way tree: X^T KRP(F_0, F_1), (I2*I3) x k
   double* scratch = nullptr;
   size_t scratch_elems = 0;
   double* lam_tmp = nullptr;    // lambda of a normalisation whose lambda is not kept
@@ -278,10 +287,10 @@ void ensure_buffers_impl(planc_gpu_ctx* c);
 // Computes the largest scratch any MTTKRP path needs and (re)allocates; any
 // reallocation invalidates the cached graph (it holds the old pointers).
 void ensure_buffers(planc_gpu_ctx* c) {
-  const void* before[6] = {c->scratch, c->P, c->P32, c->Q, c->tct.bimg, c->tct.bimg0};
+  const void* before[7] = {c->scratch, c->P, c->P32, c->Q, c->tct.bimg, c->tct.bimg0, c->tct.wimg};
   ensure_buffers_impl(c);
-  const void* after[6] = {c->scratch, c->P, c->P32, c->Q, c->tct.bimg, c->tct.bimg0};
-  for (int i = 0; i < 6; ++i)
+  const void* after[7] = {c->scratch, c->P, c->P32, c->Q, c->tct.bimg, c->tct.bimg0, c->tct.wimg};
+  for (int i = 0; i < 7; ++i)
     if (before[i] != after[i]) {
       c->buf_epoch++;
       break;
@@ -313,6 +322,13 @@ void ensure_buffers_impl(planc_gpu_ctx* c) {
       need = std::max(need, (size_t)t2.nsplit * c->dims[1] * k);
     }
     need = std::max(need, tc_scratch_elems(c->tct, eff_sm(c), k));
+    if (c->bal4) {
+      TtvRightPlan t3 = plan_ttv_right(c, c->dims[2], c->dims[3]);
+      need = std::max(need, (size_t)t3.nsplit * c->dims[2] * k);
+      need = std::max(need, tc_long_scratch_elems(c->tct, true, k, eff_sm(c)));
+      need = std::max(need, tc_long_scratch_elems(c->tct, false, k, eff_sm(c)));
+      c->tct.wimg_K = std::max(c->L, c->R);
+    }
     CK(tc_ensure(c->tct, k));
   }
   for (int n = 0; n < c->N; ++n) {
@@ -327,7 +343,10 @@ void ensure_buffers_impl(planc_gpu_ctx* c) {
     dalloc(&c->scratch, need);
     c->scratch_elems = need;
   }
-  if ((c->N == 3 || c->N == 4)) {
+  if (c->bal4) {
+    if (!c->P) dalloc(&c->P, (size_t)c->L * k);
+    if (!c->Q) dalloc(&c->Q, (size_t)c->R * k);
+  } else if ((c->N == 3 || c->N == 4)) {
     if (c->precision == PLANC_GPU_PREC_FP64) {
       if (!c->P) dalloc(&c->P, (size_t)c->L * k);
     } else {
@@ -457,10 +476,59 @@ void partial_left(planc_gpu_ctx* c, double* out) {
   }
 }
 
+// Long-K tensor-core contraction of the balanced 4-way tree: the Khatri-Rao
+// image of `modes`, then out = X W (right, L x k) or X^T W (left, R x k).
+void long_contract(planc_gpu_ctx* c, bool left, const std::vector<int>& modes, double* out) {
+  WGen wg = make_wgen(c, modes);
+  launch(c, KC_PREP, [&] { tc_long_prep(c->tct, left, wg, c->k, c->stream); });
+  if (tc_long_scratch_elems(c->tct, left, c->k, eff_sm(c)) > c->scratch_elems)
+    fail(PLANC_GPU_ERR_STATE, "internal: split-K scratch larger than planned");
+  int nsplit = 1;
+  launch(c, left ? KC_CONTRACT_LEFT : KC_CONTRACT, [&] {
+    nsplit = tc_long(c->tct, left, c->k, out, c->scratch, c->status_dev, eff_sm(c), c->stream);
+  });
+  if (nsplit > 1) {
+    const int64_t n = (left ? c->R : c->L) * c->k;
+    launch(c, KC_REDUCE, [&] {
+      k_reduce_splits<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, c->stream>>>(
+          c->scratch, nsplit, n, n, out);
+    });
+  }
+}
+
+// MTTKRP of mode n on the balanced 4-way tree {0,1} | {2,3} (tensor-core
+// paths). Same in-order reuse as DenseDimensionTree::in_order_reuse_MTTKRP
+// (dimtree/ddt.hpp:134-243) with split mode 1 instead of N/2:
+//   mode 0: P = X KRP(F_2, F_3) (L = I0 I1 rows), M_0 = multi-TTV of P with F_1
+//   mode 1: M_1 = TTV of P with the updated F_0
+//   mode 2: Q = X^T KRP(F_0, F_1) (R = I2 I3 rows), M_2 = multi-TTV of Q with F_3
+//   mode 3: M_3 = TTV of Q with the updated F_2
+// Both intermediates are (I0 I1 or I2 I3) x k, so an iteration streams X
+// twice and nothing else of its size; the reference's split would write and
+// re-read an (I0 I1 I2) x k intermediate.
+void mttkrp_bal4(planc_gpu_ctx* c, int n, double* out) {
+  const int64_t* d = c->dims;
+  if (n == 0) {
+    long_contract(c, false, {2, 3}, c->P);
+    run_ttv_right<double>(c, c->P, d[0], d[1], make_wgen(c, {1}), out);
+  } else if (n == 1) {
+    run_ttv_left<double>(c, c->P, d[0], d[1], c->F[0], out);
+  } else if (n == 2) {
+    long_contract(c, true, {0, 1}, c->Q);
+    run_ttv_right<double>(c, c->Q, d[2], d[3], make_wgen(c, {3}), out);
+  } else {
+    run_ttv_left<double>(c, c->Q, d[2], d[3], c->F[2], out);
+  }
+}
+
 // Dimension-tree MTTKRP of mode n (DenseDimensionTree::in_order_reuse_MTTKRP,
 // dimtree/ddt.hpp:134-243). Mode 0 recomputes P from the current F_{N-1};
 // modes 1..s reuse it with the freshly updated F_0 (.. F_{n-1}).
 void mttkrp_dimtree(planc_gpu_ctx* c, int n, double* out) {
+  if (c->bal4) {
+    mttkrp_bal4(c, n, out);
+    return;
+  }
   const int N = c->N;
   const bool f64 = c->precision == PLANC_GPU_PREC_FP64;
   if (n == 0) {
@@ -497,6 +565,14 @@ void mttkrp_dimtree(planc_gpu_ctx* c, int n, double* out) {
   }
   // n == 2
   run_ttv_left<double>(c, c->Q, c->dims[1], c->dims[2], c->F[1], out);
+}
+
+// Runs the tree modes that `mode` reuses (from the root of its branch, 0 or
+// s + 1, up to mode - 1) so that a single call sees the state an in-order
+// sweep would leave.
+void dimtree_prereq(planc_gpu_ctx* c, int mode) {
+  const int root = mode <= c->s ? 0 : c->s + 1;
+  for (int m = root; m < mode; ++m) mttkrp_dimtree(c, m, c->M[m]);
 }
 
 void mttkrp_any(planc_gpu_ctx* c, int n, bool dimtree, double* out) {
@@ -760,6 +836,12 @@ int planc_gpu_set_tensor(planc_gpu_ctx* c, const void* X, int dtype, const int64
     for (int i = 0; i < nmodes; ++i) c->dims[i] = dims[i];
     c->numel = numel;
     c->s = nmodes / 2;  // ntf/auntf.hpp:122-123
+    // PLANC_GPU_DIMTREE_SPLIT=reference keeps the reference's split everywhere
+    const char* split_env = getenv("PLANC_GPU_DIMTREE_SPLIT");
+    const bool ref_split = split_env && strcmp(split_env, "reference") == 0;
+    c->bal4 = !ref_split && nmodes == 4 && c->precision != PLANC_GPU_PREC_FP64 &&
+              std::max(dims[0] * dims[1], dims[2] * dims[3]) <= kBal4MaxK;
+    if (c->bal4) c->s = 1;
     c->L = 1;
     c->R = 1;
     for (int i = 0; i < nmodes; ++i) (i <= c->s ? c->L : c->R) *= dims[i];
@@ -956,8 +1038,7 @@ int planc_gpu_mttkrp(planc_gpu_ctx* c, int mode, int dimtree, double* out) {
       fail(PLANC_GPU_ERR_UNSUPPORTED, "tensor-core precisions run the dimension tree only");
     if (dt) {
       // the tree state for `mode` comes from the current factors
-      if (mode >= 1) mttkrp_dimtree(c, 0, c->M[0]);
-      if (c->N == 4 && mode == 2) mttkrp_dimtree(c, 1, c->M[1]);
+      dimtree_prereq(c, mode);
       mttkrp_dimtree(c, mode, c->M[mode]);
     } else {
       mttkrp_direct(c, mode, c->M[mode]);
@@ -1109,10 +1190,7 @@ int planc_gpu_mttkrp_device(planc_gpu_ctx* c, int mode, const double* const* F_d
     }
     try {
       if (dt) {
-        if (mode >= 1 && mode <= c->s && !reuse) {
-          mttkrp_dimtree(c, 0, c->M[0]);
-          if (c->N == 4 && mode == 2) mttkrp_dimtree(c, 1, c->M[1]);
-        }
+        if (!reuse) dimtree_prereq(c, mode);
         mttkrp_dimtree(c, mode, M_dev);
       } else {
         mttkrp_direct(c, mode, M_dev);

@@ -30,6 +30,7 @@
 #include <cuda.h>
 #include <cuda_bf16.h>
 
+#include <cstdlib>
 #include <type_traits>
 
 #include "common.cuh"
@@ -183,6 +184,36 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
   asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Two 32-column loads (lane quarter of the calling warp) and one wait.
+__device__ __forceinline__ void tmem_ld32x2(uint32_t ta, uint32_t tb, float* va, float* vb) {
+  uint32_t a[32], b[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%64];\n\t"
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+      "{%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,"
+      "%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%65];\n\t"
+      "tcgen05.wait::ld.sync.aligned;"
+      : "=r"(a[0]), "=r"(a[1]), "=r"(a[2]), "=r"(a[3]), "=r"(a[4]), "=r"(a[5]), "=r"(a[6]),
+        "=r"(a[7]), "=r"(a[8]), "=r"(a[9]), "=r"(a[10]), "=r"(a[11]), "=r"(a[12]), "=r"(a[13]),
+        "=r"(a[14]), "=r"(a[15]), "=r"(a[16]), "=r"(a[17]), "=r"(a[18]), "=r"(a[19]), "=r"(a[20]),
+        "=r"(a[21]), "=r"(a[22]), "=r"(a[23]), "=r"(a[24]), "=r"(a[25]), "=r"(a[26]), "=r"(a[27]),
+        "=r"(a[28]), "=r"(a[29]), "=r"(a[30]), "=r"(a[31]),
+        "=r"(b[0]), "=r"(b[1]), "=r"(b[2]), "=r"(b[3]), "=r"(b[4]), "=r"(b[5]), "=r"(b[6]),
+        "=r"(b[7]), "=r"(b[8]), "=r"(b[9]), "=r"(b[10]), "=r"(b[11]), "=r"(b[12]), "=r"(b[13]),
+        "=r"(b[14]), "=r"(b[15]), "=r"(b[16]), "=r"(b[17]), "=r"(b[18]), "=r"(b[19]), "=r"(b[20]),
+        "=r"(b[21]), "=r"(b[22]), "=r"(b[23]), "=r"(b[24]), "=r"(b[25]), "=r"(b[26]), "=r"(b[27]),
+        "=r"(b[28]), "=r"(b[29]), "=r"(b[30]), "=r"(b[31])
+      : "r"(ta), "r"(tb)
+      : "memory");
+#pragma unroll
+  for (int i = 0; i < 32; ++i) {
+    va[i] = __uint_as_float(a[i]);
+    vb[i] = __uint_as_float(b[i]);
+  }
 }
 
 __device__ __forceinline__ void tmem_alloc(uint32_t dst_smem, uint32_t ncols) {
@@ -849,7 +880,256 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
   }
 }
 
+// ------------------------------------------------------------ long-K kernel
+// part[y][row*k + r] = sum over the K blocks of split y of A(row, K) W(K, r)
+// with W a pre-swizzled hi|lo image (k_tc_wimage):
+//   KMAJ  (left contraction)  rows = j < R, K = l < L: A = X^T, K-major tiles
+//          (one 64 x 128 box, the same tiles as the factored left kernel);
+//   !KMAJ (right contraction) rows = l < L, K = j < R: A = X, MN-major tiles
+//          (two 64 x 64 boxes, the same tiles as k_tc_right).
+// K blocks go in groups of `group` (tc_long_group); a group is one
+// tensor-core accumulation chain in a double-buffered TMEM accumulator,
+// drained by four warps into register running sums, so K of any length keeps
+// every FP32 chain short.
+// Grid (mgroups, nsplit): a CTA owns MT consecutive 128-row tiles; split y
+// takes groups y, y + nsplit, ...
+constexpr int TCG_GROUP = 2;  // default K blocks per accumulation chain
+
+template <int KP, int MT, bool X2, bool KMAJ>
+__global__ void __launch_bounds__(TCF_THREADS, 1)
+    k_tc_long(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
+              const uint8_t* __restrict__ wimg, int64_t rows, int64_t K, int k, int stages,
+              int group, double* __restrict__ part, int* __restrict__ status) {
+  constexpr int NCOL = 2 * KP;
+  constexpr uint32_t A_TILE = TC_BM * TC_BK * 2;  // 16 KB
+  constexpr uint32_t A_BYTES = MT * A_TILE;
+  constexpr uint32_t A_STAGE = X2 ? 2 * A_BYTES : A_BYTES;
+  constexpr uint32_t B_STAGE = NCOL * 128;
+  constexpr uint32_t STAGE = A_STAGE + B_STAGE;
+  constexpr uint32_t ACC_COLS = MT * NCOL;
+  constexpr uint32_t TMEM_NEED = 2 * ACC_COLS;
+  constexpr uint32_t TMEM_COLS = TMEM_NEED <= 32 ? 32 : TMEM_NEED <= 64 ? 64 : TMEM_NEED <= 128 ? 128
+                                 : TMEM_NEED <= 256 ? 256 : 512;
+  constexpr uint32_t IDESC = idesc_bf16(NCOL, !KMAJ, false);
+  using Acc = float;  // register adds round to nearest: no drift from the many drains
+
+  extern __shared__ uint8_t smem_raw[];
+  __shared__ uint64_t bars[2 * 8 + 4];
+  __shared__ uint32_t tmem_base_sh;
+  __shared__ int abort_sh;
+  uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
+  const uint32_t smem0 = smem_u32(smem);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int64_t nk = (K + TC_BK - 1) / TC_BK;
+  const int64_t ngroups = (nk + group - 1) / group;
+  const int64_t ns = gridDim.y;
+  const int64_t y = blockIdx.y;
+  const int64_t my_groups = y < ngroups ? (ngroups - y + ns - 1) / ns : 0;
+  const int row0 = blockIdx.x * MT * TC_BM;
+  auto full = [&](int s) { return smem_u32(&bars[s]); };
+  auto empty = [&](int s) { return smem_u32(&bars[8 + s]); };
+  auto accf = [&](int b) { return smem_u32(&bars[16 + b]); };
+  auto acce = [&](int b) { return smem_u32(&bars[18 + b]); };
+
+  if (threadIdx.x == 0) {
+    abort_sh = 0;
+    for (int s = 0; s < stages; ++s) {
+      mbar_init(full(s), 1);
+      mbar_init(empty(s), 1);
+    }
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(accf(b), 1);
+      mbar_init(acce(b), 4);
+    }
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  if (warp == 1) tmem_alloc(smem_u32(&tmem_base_sh), TMEM_COLS);
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_sh;
+  volatile int* abort_flag = &abort_sh;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      bool ok = true;
+      for (int64_t i = 0; i < my_groups && ok; ++i) {
+        const int64_t g = y + i * ns;
+        const int64_t kb1 = min((g + 1) * group, nk);
+        for (int64_t kb = g * group; kb < kb1; ++kb) {
+          if (!mbar_wait(empty(s), ph ^ 1, abort_flag, status)) { ok = false; break; }
+          const uint32_t st = smem0 + s * STAGE;
+          const int kx = (int)(kb * TC_BK);
+          mbar_expect_tx(full(s), STAGE);
+#pragma unroll
+          for (int mt = 0; mt < MT; ++mt) {
+            const int r0 = row0 + mt * TC_BM;
+            if (KMAJ) {
+              tma_load_2d(st + mt * A_TILE, &tm_hi, kx, r0, full(s));
+              if (X2) tma_load_2d(st + A_BYTES + mt * A_TILE, &tm_lo, kx, r0, full(s));
+            } else {
+              tma_load_2d(st + mt * A_TILE, &tm_hi, r0, kx, full(s));
+              tma_load_2d(st + mt * A_TILE + A_TILE / 2, &tm_hi, r0 + 64, kx, full(s));
+              if (X2) {
+                tma_load_2d(st + A_BYTES + mt * A_TILE, &tm_lo, r0, kx, full(s));
+                tma_load_2d(st + A_BYTES + mt * A_TILE + A_TILE / 2, &tm_lo, r0 + 64, kx, full(s));
+              }
+            }
+          }
+          bulk_load(st + A_STAGE, wimg + (size_t)kb * B_STAGE, B_STAGE, full(s));
+          if (++s == stages) { s = 0; ph ^= 1; }
+        }
+      }
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      int s = 0;
+      uint32_t ph = 0;
+      uint32_t aph[2] = {0, 0};
+      bool ok = true;
+      for (int64_t i = 0; i < my_groups && ok; ++i) {
+        const int buf = (int)(i & 1);
+        const int64_t g = y + i * ns;
+        const int64_t kb0 = g * group, kb1 = min((g + 1) * group, nk);
+        if (!mbar_wait(acce(buf), aph[buf] ^ 1, abort_flag, status)) break;
+        tc_fence_after();
+        const uint32_t d = tmem + buf * ACC_COLS;
+        for (int64_t kb = kb0; kb < kb1; ++kb) {
+          if (!mbar_wait(full(s), ph, abort_flag, status)) { ok = false; break; }
+          tc_fence_after();
+          const uint32_t st = smem0 + s * STAGE;
+#pragma unroll
+          for (int kk = 0; kk < TC_BK / 16; ++kk) {
+            const uint64_t bdesc = smem_desc(st + A_STAGE + kk * 32, 16, 1024);
+#pragma unroll
+            for (int mt = 0; mt < MT; ++mt) {
+              // K-major A: +32 B per K = 16; MN-major A: K advances 16 rows =
+              // two 1024 B groups, the two 64-row halves 8 KB apart
+              const uint32_t a0 = st + mt * A_TILE + (KMAJ ? kk * 32 : kk * 2048);
+              const uint64_t adesc = KMAJ ? smem_desc(a0, 16, 1024) : smem_desc(a0, A_TILE / 2, 1024);
+              umma_bf16(d + mt * NCOL, adesc, bdesc, IDESC, (kb != kb0 || kk != 0) ? 1u : 0u);
+              if (X2) {
+                const uint64_t adesc2 = KMAJ ? smem_desc(a0 + A_BYTES, 16, 1024)
+                                             : smem_desc(a0 + A_BYTES, A_TILE / 2, 1024);
+                umma_bf16(d + mt * NCOL, adesc2, bdesc, IDESC, 1);
+              }
+            }
+          }
+          umma_commit(empty(s));
+          if (++s == stages) { s = 0; ph ^= 1; }
+        }
+        if (!ok) break;
+        umma_commit(accf(buf));
+        aph[buf] ^= 1;
+      }
+    }
+  } else {
+    // drain warps 2..5: TMEM lane quarter = warp % 4
+    const int q4 = warp & 3;
+    Acc sum[MT][KP];
+#pragma unroll
+    for (int mt = 0; mt < MT; ++mt)
+#pragma unroll
+      for (int r = 0; r < KP; ++r) sum[mt][r] = 0;
+    uint32_t aph[2] = {0, 0};
+    bool ok = true;
+    for (int64_t i = 0; i < my_groups; ++i) {
+      const int buf = (int)(i & 1);
+      if (!mbar_wait(accf(buf), aph[buf], abort_flag, status)) { ok = false; break; }
+      tc_fence_after();
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt) {
+        const uint32_t base = tmem + ((uint32_t)(q4 * 32) << 16) + buf * ACC_COLS + mt * NCOL;
+        if (KP == 16) {
+          float v[32];
+          tmem_ld32(base, v);  // columns 0..15 hi, 16..31 lo
+#pragma unroll
+          for (int r = 0; r < 16; ++r) sum[mt][r] += v[r] + v[16 + r];
+        } else {
+#pragma unroll
+          for (int cc = 0; cc < KP; cc += 32) {  // hi and lo 32-column slices, one wait
+            float vh[32], vl[32];
+            tmem_ld32x2(base + cc, base + KP + cc, vh, vl);
+#pragma unroll
+            for (int e = 0; e < 32; ++e) sum[mt][cc + e] += vh[e] + vl[e];
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive(acce(buf));
+      aph[buf] ^= 1;
+    }
+    if (ok) {
+      double* dst = part + y * rows * k;
+#pragma unroll
+      for (int mt = 0; mt < MT; ++mt) {
+        const int64_t row = (int64_t)row0 + mt * TC_BM + q4 * 32 + lane;
+        if (row < rows) {
+#pragma unroll
+          for (int r = 0; r < KP; ++r)
+            if (r < k) dst[row * k + r] = (double)sum[mt][r];
+        }
+      }
+    }
+  }
+  __syncthreads();
+  if (abort_sh) tc_drain_after_abort();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    tmem_dealloc(tmem, TMEM_COLS);
+  }
+}
+
+// Pre-swizzled hi|lo image of a Khatri-Rao product W(kk, r) = prod_t
+// F_t[digit_t(kk), r] (the B operand of k_tc_long), laid out as k_tc_bimage.
+template <int KP>
+__global__ void k_tc_wimage(const WGen wg, int64_t K, int k, int64_t nk, uint8_t* __restrict__ img) {
+  constexpr int NCOL = 2 * KP;
+  const int64_t total = nk * KP * TC_BK;
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int kk = (int)(e % TC_BK);
+    const int r = (int)((e / TC_BK) % KP);
+    const int64_t kb = e / ((int64_t)TC_BK * KP);
+    const int64_t j = kb * TC_BK + kk;
+    __nv_bfloat16 hi = __float2bfloat16(0.f), lo = __float2bfloat16(0.f);
+    if (j < K && r < k) split_bf16(wgen_eval(wg, j, r, k), hi, lo);
+    uint8_t* st = img + (size_t)kb * NCOL * 128;
+    *reinterpret_cast<__nv_bfloat16*>(st + sw128_kmajor_off(r, kk)) = hi;
+    *reinterpret_cast<__nv_bfloat16*>(st + sw128_kmajor_off(KP + r, kk)) = lo;
+  }
+}
+
+// 32-bit mix of a 64-bit counter (the finaliser of the splitmix64 generator,
+// Steele, Lea & Flood 2014), the random source of the stochastic rounding.
+__device__ __forceinline__ uint32_t sr_hash(uint64_t z) {
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return (uint32_t)((z ^ (z >> 31)) >> 32);
+}
+
+// BF16 of a finite float by stochastic rounding: up with probability equal
+// to the discarded fraction of an ulp, so E[result] = x. Round-to-nearest is
+// biased on data whose density falls across each binade (nonnegative CP
+// tensors: about -3e-6 relative in every MTTKRP entry); the stochastic
+// errors have mean zero and average out in the long MTTKRP sums. `r` supplies
+// the 16 random bits.
+__device__ __forceinline__ __nv_bfloat16 bf16_stochastic(float x, uint32_t r) {
+  const uint32_t u = __float_as_uint(x);
+  if ((u & 0x7f800000u) == 0x7f800000u) return __float2bfloat16(x);  // Inf / NaN
+  const uint32_t v = u + (r & 0xffffu);
+  if ((v & 0x7f800000u) == 0x7f800000u) return __float2bfloat16(x);  // would overflow
+  return __ushort_as_bfloat16((unsigned short)(v >> 16));
+}
+
 // X (f32/f64, L x R column-major) -> BF16 hi (and lo) with leading dim Lpad.
+// Split-BF16 (lo != null): hi = RN(x), lo = RN(x - hi), residual ~2^-17 |x|.
+// Single BF16: stochastic rounding of RN_f32(x), seeded by the element index
+// (deterministic).
 template <typename T>
 __global__ void k_tc_convert(const T* __restrict__ X, int64_t L, int64_t R, int64_t Lpad,
                              __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
@@ -858,9 +1138,13 @@ __global__ void k_tc_convert(const T* __restrict__ X, int64_t L, int64_t R, int6
        e += (int64_t)gridDim.x * blockDim.x) {
     const int64_t l = e % Lpad, j = e / Lpad;
     double x = l < L ? (double)X[l + L * j] : 0.0;
-    __nv_bfloat16 h = __double2bfloat16(x);
-    hi[e] = h;
-    if (lo) lo[e] = __double2bfloat16(x - (double)__bfloat162float(h));
+    if (lo) {
+      __nv_bfloat16 h = __double2bfloat16(x);
+      hi[e] = h;
+      lo[e] = __double2bfloat16(x - (double)__bfloat162float(h));
+    } else {
+      hi[e] = bf16_stochastic((float)x, sr_hash((uint64_t)e));
+    }
   }
 }
 
@@ -896,6 +1180,9 @@ struct TcTensor {
   size_t bimg0_bytes = 0;
   int kpad = 0;
   int64_t I0 = 0;            // mode-0 size (factored left contraction when I0 % 64 == 0)
+  uint8_t* wimg = nullptr;   // Khatri-Rao image of the long-K kernel (k_tc_long)
+  size_t wimg_bytes = 0;
+  int64_t wimg_K = 0;        // longest K it must hold (0: long-K kernel unused)
 };
 
 inline int tc_kpad(int k) { return k <= 16 ? 16 : k <= 32 ? 32 : 64; }
@@ -936,9 +1223,10 @@ inline void tc_free(TcTensor& t) {
   if (t.lo) cudaFree(t.lo);
   if (t.bimg) cudaFree(t.bimg);
   if (t.bimg0) cudaFree(t.bimg0);
+  if (t.wimg) cudaFree(t.wimg);
   t.hi = t.lo = nullptr;
-  t.bimg = t.bimg0 = nullptr;
-  t.bimg_bytes = t.bimg0_bytes = 0;
+  t.bimg = t.bimg0 = t.wimg = nullptr;
+  t.bimg_bytes = t.bimg0_bytes = t.wimg_bytes = 0;
 }
 
 inline bool tc_left_factored(const TcTensor& t) { return t.I0 > 0 && t.I0 % TC_BK == 0; }
@@ -1024,6 +1312,20 @@ inline cudaError_t tc_set_attrs() {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_tc_left_fac<KP, 2, X2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(tc_stages(SL2) * SL2 + 1024));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_tc_long<KP, 1, X2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(tc_stages(SL1) * SL1 + 1024));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(k_tc_long<KP, 1, X2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(tc_stages(SL1) * SL1 + 1024));
+  if constexpr (KP <= 32) {  // two tiles per CTA (tc_long_mt)
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_tc_long<KP, 2, X2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)(tc_stages(SL2) * SL2 + 1024));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_tc_long<KP, 2, X2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)(tc_stages(SL2) * SL2 + 1024));
+  }
   return e;
 }
 
@@ -1040,15 +1342,21 @@ inline cudaError_t tc_ensure(TcTensor& t, int k) {
   const int nk = (int)((t.R + TC_BK - 1) / TC_BK);
   size_t need = (size_t)nk * 2 * kp * 128;
   size_t need0 = tc_left_factored(t) ? (size_t)(t.I0 / TC_BK) * 2 * kp * 128 : 0;
-  if (t.bimg && t.bimg_bytes >= need && t.kpad == kp && t.bimg0_bytes >= need0) return cudaSuccess;
+  size_t needw = (size_t)((t.wimg_K + TC_BK - 1) / TC_BK) * 2 * kp * 128;
+  if (t.bimg && t.bimg_bytes >= need && t.kpad == kp && t.bimg0_bytes >= need0 &&
+      t.wimg_bytes >= needw)
+    return cudaSuccess;
   if (t.bimg) cudaFree(t.bimg);
   if (t.bimg0) cudaFree(t.bimg0);
-  t.bimg = t.bimg0 = nullptr;
+  if (t.wimg) cudaFree(t.wimg);
+  t.bimg = t.bimg0 = t.wimg = nullptr;
   t.kpad = kp;
   t.bimg_bytes = need;
   t.bimg0_bytes = need0;
+  t.wimg_bytes = needw;
   e = cudaMalloc(&t.bimg, need);
   if (e == cudaSuccess && need0) e = cudaMalloc(&t.bimg0, need0);
+  if (e == cudaSuccess && needw) e = cudaMalloc(&t.wimg, needw);
   return e;
 }
 
@@ -1134,6 +1442,95 @@ inline int tc_left(const TcTensor& t, const WGen& wg, int k, double* part, int* 
     default: TCL(64) break;
   }
 #undef TCL
+  return ns;
+}
+
+// ---- long-K kernel (k_tc_long): plan, image, launch
+// 128-row tiles per CTA: 2 when there are more than one (halves the image's
+// share of the shared-memory traffic), except at the 64-wide rank, whose two
+// tiles' running sums would not fit the drain warps' registers.
+inline int tc_long_mt(int64_t rows, int k) { return (rows > TC_BM && tc_kpad(k) <= 32) ? 2 : 1; }
+
+// K blocks per tensor-core accumulation chain of k_tc_long (environment
+// PLANC_GPU_TC_GROUP overrides the default).
+inline int tc_long_group() {
+  static int g = [] {
+    const char* e = getenv("PLANC_GPU_TC_GROUP");
+    int v = e ? atoi(e) : TCG_GROUP;
+    return v < 1 ? 1 : (v > 1024 ? 1024 : v);
+  }();
+  return g;
+}
+
+inline void tc_long_plan(int64_t rows, int64_t K, int k, int sm_count, int* mgroups, int* nsplit) {
+  const int MT = tc_long_mt(rows, k);
+  *mgroups = (int)((rows + MT * TC_BM - 1) / (MT * TC_BM));
+  int ns = sm_count / *mgroups;
+  if (ns < 1) ns = 1;
+  const int64_t ngroups = ((K + TC_BK - 1) / TC_BK + tc_long_group() - 1) / tc_long_group();
+  if (ns > ngroups) ns = (int)ngroups;
+  *nsplit = ns;
+}
+
+// Split-K partials the long-K kernel writes for `left` (0 when it writes the
+// output directly).
+inline size_t tc_long_scratch_elems(const TcTensor& t, bool left, int k, int sm_count) {
+  const int64_t rows = left ? t.R : t.L, K = left ? t.L : t.R;
+  int mg, ns;
+  tc_long_plan(rows, K, k, sm_count, &mg, &ns);
+  return ns > 1 ? (size_t)ns * rows * k : 0;
+}
+
+// Image of W = KRP over the K index of the left (K = l, rows j) or right
+// (K = j, rows l) contraction.
+inline void tc_long_prep(const TcTensor& t, bool left, const WGen& wg, int k, cudaStream_t st) {
+  const int64_t K = left ? t.L : t.R;
+  const int64_t nk = (K + TC_BK - 1) / TC_BK;
+  const int kp = tc_kpad(k);
+  const unsigned blocks = (unsigned)std::min<int64_t>((nk * kp * TC_BK + 255) / 256, 2048);
+  if (kp == 16)
+    k_tc_wimage<16><<<blocks, 256, 0, st>>>(wg, K, k, nk, t.wimg);
+  else if (kp == 32)
+    k_tc_wimage<32><<<blocks, 256, 0, st>>>(wg, K, k, nk, t.wimg);
+  else
+    k_tc_wimage<64><<<blocks, 256, 0, st>>>(wg, K, k, nk, t.wimg);
+}
+
+template <int KP, int MT, bool X2, bool KMAJ>
+inline void tc_long_launch(const TcTensor& t, int k, int mg, int ns, double* part, int* status,
+                           cudaStream_t st) {
+  constexpr uint32_t STAGE = (X2 ? 2 : 1) * MT * TC_BM * TC_BK * 2 + 2 * KP * 128;
+  const int stages = tc_stages(STAGE);
+  const size_t smem = (size_t)stages * STAGE + 1024;
+  k_tc_long<KP, MT, X2, KMAJ><<<dim3(mg, ns), TCF_THREADS, smem, st>>>(
+      KMAJ ? t.mL_hi : t.mR_hi, KMAJ ? t.mL_lo : t.mR_lo, t.wimg, KMAJ ? t.R : t.L,
+      KMAJ ? t.L : t.R, k, stages, tc_long_group(), part, status);
+}
+
+// Left (out = X^T W, R x k) or right (out = X W, L x k) contraction against
+// the image built by tc_long_prep. Writes `out` directly and returns 1, or
+// writes that many split-K partials to `part` (R or L x k each).
+inline int tc_long(const TcTensor& t, bool left, int k, double* out, double* part, int* status,
+                   int sm_count, cudaStream_t st) {
+  const int64_t rows = left ? t.R : t.L, K = left ? t.L : t.R;
+  int mg, ns;
+  tc_long_plan(rows, K, k, sm_count, &mg, &ns);
+  double* dst = ns > 1 ? part : out;
+  const bool x2 = t.prec == 2;
+  const int MT = tc_long_mt(rows, k);
+#define TCG(KP, M)                                                                           \
+  if (left)                                                                                  \
+    x2 ? tc_long_launch<KP, M, true, true>(t, k, mg, ns, dst, status, st)                    \
+       : tc_long_launch<KP, M, false, true>(t, k, mg, ns, dst, status, st);                  \
+  else                                                                                       \
+    x2 ? tc_long_launch<KP, M, true, false>(t, k, mg, ns, dst, status, st)                   \
+       : tc_long_launch<KP, M, false, false>(t, k, mg, ns, dst, status, st);
+  switch (tc_kpad(k)) {
+    case 16: if (MT == 2) { TCG(16, 2) } else { TCG(16, 1) } break;
+    case 32: if (MT == 2) { TCG(32, 2) } else { TCG(32, 1) } break;
+    default: TCG(64, 1) break;
+  }
+#undef TCG
   return ns;
 }
 

@@ -93,3 +93,25 @@ def test_projected_gradient_descent_decreases_loss(gpu):
     assert all(b <= a * (1 + 1e-6) for a, b in zip(losses, losses[1:]))
     assert losses[-1] < 0.5 * losses[0]
     lossf.close()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "bf16x2"])
+def test_cp_loss_4way_reference_gradient(gpu, oracle_lib, prec):
+    # 4-way: the backward's in-order reuse walks both branches of the tree
+    import torch
+    from planc_b200.autograd import CPLoss
+    dims, k = (20, 16, 24, 12), 5
+    X, _ = cp_tensor(dims, k, noise=0.05, seed=51)
+    rng = np.random.default_rng(52)
+    F = [rng.random((d, k)) for d in dims]
+    lossf = CPLoss(X if prec == "fp64" else X.astype(np.float32), rank=k, precision=prec)
+    Ft = [torch.tensor(f, device="cuda", dtype=torch.float64, requires_grad=True) for f in F]
+    loss = lossf(*Ft)
+    loss.backward()
+    bound = 1e-10 if prec == "fp64" else 2e-5
+    for n in range(4):
+        M = oracle_lib.mttkrp_direct(X, F, n)
+        G = oracle_lib.gram_loo(F, n)
+        ref_grad = F[n] @ G - M
+        assert rel(Ft[n].grad.cpu().numpy(), ref_grad) < bound, (n, rel(Ft[n].grad.cpu().numpy(), ref_grad))
+    lossf.close()

@@ -28,7 +28,11 @@ def _normalized(F):
 
 @pytest.mark.parametrize("prec", ["bf16", "bf16x2"])
 @pytest.mark.parametrize("dims,k", [((64, 64, 64), 8), ((40, 33, 21), 32), ((13, 7, 20), 5),
-                                    ((9, 8, 7, 10), 64), ((130, 3, 300), 16), ((24, 16, 16, 40), 32)])
+                                    ((9, 8, 7, 10), 64), ((130, 3, 300), 16), ((24, 16, 16, 40), 32),
+                                    # 4-way, balanced tree: split-K of the long right
+                                    # contraction (128 rows, K = 4096), ragged K
+                                    ((8, 16, 64, 64), 16), ((7, 9, 33, 65), 20),
+                                    ((16, 12, 40, 40), 64)])
 def test_tc_mttkrp_all_modes(gpu, oracle_lib, prec, dims, k):
     X, _ = cp_tensor(dims, 4, seed=21)
     F = init_factors(dims, k, seed=22)
@@ -90,3 +94,19 @@ def test_tc_large_split_k(gpu, oracle_lib):
         for n in (0, 2):
             ref = oracle_lib.mttkrp_direct(X.astype(np.float64), Fn, n)
             assert rel(c.mttkrp(n), ref) < BOUND["bf16x2"]
+
+
+@pytest.mark.parametrize("prec", ["bf16x2"])
+def test_tc_4way_ntf_matches_fp64_error(gpu, prec):
+    # the 4-way tensor-core path runs the balanced {0,1}|{2,3} tree, the FP64
+    # path the reference's {0,1,2}|{3}: same iterates within the bf16x2 bound
+    dims, k, iters = (24, 20, 32, 28), 6, 15
+    X, _ = cp_tensor(dims, k, noise=0.01, seed=41)
+    F0 = init_factors(dims, k, seed=42)
+    errs = {}
+    for p in ("fp64", prec):
+        with gpu.Context(0, p) as c:
+            c.set_tensor(X if p == "fp64" else X.astype(np.float32))
+            c.set_factors(F0)
+            errs[p] = c.run("hals", iters)
+    assert abs(errs[prec][-1] - errs["fp64"][-1]) < 1e-4, (errs[prec][-1], errs["fp64"][-1])
