@@ -279,12 +279,11 @@ def main():
     ctx.set_factors(F0)
     stream = torch.cuda.ExternalStream(ctx.stream, device="cuda:%d" % dev)
     ctx.run(args.algo, args.warmup)
-    ctx.set_timing(True)
-    ctx.kernel_times()
     sampler = ClockSampler(dev)
     sampler.start()
     time.sleep(0.2)
     barrier()
+    # timed region: one CUDA graph per outer iteration, as a user's run executes
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     n0 = ctx.launch_count()
     e0.record(stream)
@@ -294,8 +293,19 @@ def main():
     clocks = sampler.stop()
     value, ms = replica_value(e0.elapsed_time(e1), args.steps, world, dist, devname)
     launches = ctx.launch_count() - n0
+    # per-kernel durations: a second region of the same steps with CUDA events
+    # around every launch on the library's stream (graphs off while timing)
+    ctx.set_timing(True)
+    ctx.kernel_times()
+    barrier()
+    ek0, ek1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ek0.record(stream)
+    ctx.run(args.algo, args.steps, compute_error=True)
+    ek1.record(stream)
+    barrier()
     kt = ctx.kernel_times()
     ctx.set_timing(False)
+    ms_event_timed = ek0.elapsed_time(ek1) / args.steps
 
     # dominant kernel: the partial MTTKRP contraction (right: P = X*F_last,
     # writes P in FP32; left: X^T*KRP, writes split-K FP64 partials)
@@ -417,6 +427,8 @@ def main():
             "rel_error": quality,
             "roofline": roofline,
             "kernel_time_share": kernel_share,
+            "kernel_ms_per_iter": {c: round(v[0] / args.steps, 4) for c, v in kt.items() if v[1]},
+            "ms_per_step_event_timed": ms_event_timed,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": launches,

@@ -113,10 +113,14 @@ def cfg3(args, gpu, torch, dev):
             c.set_factors(F0)
             c.run("anlsbpp", max(args.warmup, 1), compute_error=False)
             c.set_factors(F0)
+            ms, errs, launches = _time_run(torch, c, "anlsbpp", T)  # one CUDA graph per iteration
+            # per-kernel breakdown from a separate run with event timing (no graphs)
+            c.set_factors(F0)
             c.set_timing(True)
             c.kernel_times()
-            ms, errs, launches = _time_run(torch, c, "anlsbpp", T)
+            c.run("anlsbpp", T, compute_error=True)
             kt = c.kernel_times()
+            c.set_timing(False)
             out[prec] = (ms, errs, launches, kt)
     # headline: single BF16 (stochastically rounded tensor); the split-BF16
     # run is reported beside it

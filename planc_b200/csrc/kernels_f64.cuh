@@ -176,24 +176,42 @@ __global__ void __launch_bounds__(256) k_contract_f64(const double* __restrict__
   }
 }
 
-// out[i] = sum_{s < nsplit} part[s * stride + i], fixed order.
+// out[i] = sum_{s < nsplit} part[s * stride + i] in a fixed order: eight
+// lanes per output each sum the splits s = lane8, lane8 + 8, ... and a fixed
+// shuffle tree adds the eight (deterministic run to run; eight times the
+// loads in flight of a thread-per-output loop).
 __global__ void k_reduce_splits(const double* __restrict__ part, int nsplit, int64_t stride,
                                 int64_t n, double* __restrict__ out) {
-  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
+  const int sub = threadIdx.x & 7;
+  const int64_t step = ((int64_t)gridDim.x * blockDim.x) >> 3;
+  // every lane of a warp runs the same number of iterations (shuffles below)
+  const int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) << 2;
+  for (int64_t i0 = base; i0 < n; i0 += step) {
+    const int64_t i = i0 + ((threadIdx.x >> 3) & 3);
     double s = 0.0;
-    int p = 0;
-    for (; p + 4 <= nsplit; p += 4) {  // loads issued together, summed in order
-      const double v0 = part[p * stride + i], v1 = part[(p + 1) * stride + i];
-      const double v2 = part[(p + 2) * stride + i], v3 = part[(p + 3) * stride + i];
-      s += v0;
-      s += v1;
-      s += v2;
-      s += v3;
+    if (i < n) {
+      int p = sub;
+      for (; p + 24 < nsplit; p += 32) {
+        const double v0 = part[p * stride + i], v1 = part[(p + 8) * stride + i];
+        const double v2 = part[(p + 16) * stride + i], v3 = part[(p + 24) * stride + i];
+        s += v0;
+        s += v1;
+        s += v2;
+        s += v3;
+      }
+      for (; p < nsplit; p += 8) s += part[p * stride + i];
     }
-    for (; p < nsplit; ++p) s += part[p * stride + i];
-    out[i] = s;
+    s += __shfl_xor_sync(0xffffffffu, s, 1);
+    s += __shfl_xor_sync(0xffffffffu, s, 2);
+    s += __shfl_xor_sync(0xffffffffu, s, 4);
+    if (sub == 0 && i < n) out[i] = s;
   }
+}
+
+// Grid of k_reduce_splits for n outputs (256-thread blocks, 8 lanes each).
+inline unsigned reduce_grid(int64_t n) {
+  const int64_t b = (8 * n + 255) / 256;
+  return (unsigned)(b < 1 ? 1 : (b > 8192 ? 8192 : b));
 }
 
 // ---------------------------------------------------------------------------
@@ -520,8 +538,14 @@ __global__ void __launch_bounds__(256) k_mu_warp(double* __restrict__ H, const d
 // of the normalised factor G_n = (U^T U)_ab / (lambda_a lambda_b), normalises
 // U in place (ncpfactors.hpp:346-351) and forms the next leave-one-out product.
 // ---------------------------------------------------------------------------
-constexpr int GP_ROWS = 64;
+constexpr int GP_ROWS = 16;
+// Largest I*k that k_gram_finalize normalises itself (one CTA); above it the
+// many-CTA k_scale_cols does.
+constexpr int64_t kFinalizeScaleMax = 65536;
 
+// 256 threads; thread (ta, tb) owns the 4 x 4 outputs a = ta + kt*u,
+// b = tb + kt*v (kt = ceil(k/4)), so a warp's loads of the b-values are
+// consecutive in shared memory.
 __global__ void __launch_bounds__(256) k_gram_partial(const double* __restrict__ U, int64_t I, int k,
                                                       double* __restrict__ part) {
   __shared__ double tile[GP_ROWS * kMaxRank];
@@ -529,20 +553,43 @@ __global__ void __launch_bounds__(256) k_gram_partial(const double* __restrict__
   const int nrows = (int)((I - row0) < GP_ROWS ? (I - row0) : GP_ROWS);
   for (int e = threadIdx.x; e < nrows * k; e += 256) tile[e] = U[row0 * k + e];
   __syncthreads();
-  const int kk2 = k * k;
-  for (int e = threadIdx.x; e < kk2; e += 256) {
-    const int a = e / k, b = e % k;
-    double s0 = 0.0, s1 = 0.0;
-    int i = 0;
-    for (; i + 1 < nrows; i += 2) {
-      s0 = fma(tile[i * k + a], tile[i * k + b], s0);
-      s1 = fma(tile[(i + 1) * k + a], tile[(i + 1) * k + b], s1);
+  const int kt = (k + 3) / 4;
+  const int t = threadIdx.x;
+  if (t >= kt * kt) return;
+  const int ta = t / kt, tb = t % kt;
+  double acc[4][4];
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) acc[u][v] = 0.0;
+  for (int i = 0; i < nrows; ++i) {
+    const double* r = tile + i * k;
+    double av[4], bv[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int a = ta + kt * u, b = tb + kt * u;
+      av[u] = a < k ? r[a] : 0.0;
+      bv[u] = b < k ? r[b] : 0.0;
     }
-    if (i < nrows) s0 = fma(tile[i * k + a], tile[i * k + b], s0);
-    part[(int64_t)blockIdx.x * kk2 + e] = s0 + s1;
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) acc[u][v] = fma(av[u], bv[v], acc[u][v]);
   }
+  double* dst = part + (int64_t)blockIdx.x * k * k;
+#pragma unroll
+  for (int u = 0; u < 4; ++u)
+#pragma unroll
+    for (int v = 0; v < 4; ++v) {
+      const int a = ta + kt * u, b = tb + kt * v;
+      if (a < k && b < k) dst[a * k + b] = acc[u][v];
+    }
 }
 
+// One CTA: sums the row-block partials in a fixed order (eight independent
+// running sums per element), lambda_r = sqrt((U^T U)_rr), G_n = (U^T U)_ab /
+// (lambda_a lambda_b), the next leave-one-out product and, when
+// I*k <= kFinalizeScaleMax, the normalisation U(:, r) /= lambda_r itself.
 __global__ void __launch_bounds__(1024) k_gram_finalize(double* __restrict__ F, int64_t I, int k,
                                                         const double* __restrict__ part, int nblk,
                                                         double* __restrict__ lambda,
@@ -553,9 +600,14 @@ __global__ void __launch_bounds__(1024) k_gram_finalize(double* __restrict__ F, 
   const int tid = threadIdx.x;
   const int kk2 = k * k;
   for (int e = tid; e < kk2; e += 1024) {
-    double s = 0.0;
-    for (int b = 0; b < nblk; ++b) s += part[(int64_t)b * kk2 + e];
-    gs[e] = s;
+    double s[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    int b = 0;
+    for (; b + 8 <= nblk; b += 8) {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) s[u] += part[(int64_t)(b + u) * kk2 + e];
+    }
+    for (; b < nblk; ++b) s[0] += part[(int64_t)b * kk2 + e];
+    gs[e] = ((s[0] + s[1]) + (s[2] + s[3])) + ((s[4] + s[5]) + (s[6] + s[7]));
   }
   __syncthreads();
   if (tid < k) {
@@ -564,6 +616,12 @@ __global__ void __launch_bounds__(1024) k_gram_finalize(double* __restrict__ F, 
     if (lambda) lambda[tid] = nrm;
   }
   __syncthreads();
+  if (I * k <= kFinalizeScaleMax) {
+    for (int64_t e = tid; e < I * k; e += 1024) {
+      const double nrm = lam[e % k];
+      if (nrm > 0) F[e] = F[e] / nrm;
+    }
+  }
   double* Gn = Gall + (int64_t)n * kk2;
   for (int e = tid; e < kk2; e += 1024) {
     const int a = e / k, b = e % k;

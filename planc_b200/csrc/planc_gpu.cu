@@ -378,7 +378,7 @@ void run_contract(planc_gpu_ctx* c, const ContractPlan& p, bool left, const doub
   if (p.nsplit > 1) {
     int64_t n = p.g.M * k;
     launch(c, KC_REDUCE, [&] {
-      k_reduce_splits<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, c->stream>>>(
+      k_reduce_splits<<<reduce_grid(n), 256, 0, c->stream>>>(
           c->scratch, p.nsplit, p.g.split_stride, n, out);
     });
   }
@@ -403,7 +403,7 @@ void run_ttv_right(planc_gpu_ctx* c, const TT* T, int64_t A, int64_t B, const WG
   if (p.nsplit > 1) {
     int64_t n = A * k;
     launch(c, KC_REDUCE, [&] {
-      k_reduce_splits<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, c->stream>>>(
+      k_reduce_splits<<<reduce_grid(n), 256, 0, c->stream>>>(
           c->scratch, p.nsplit, n, n, out);
     });
   }
@@ -470,7 +470,7 @@ void partial_left(planc_gpu_ctx* c, double* out) {
     });
     int64_t n = c->R * c->k;
     launch(c, KC_REDUCE, [&] {
-      k_reduce_splits<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, c->stream>>>(
+      k_reduce_splits<<<reduce_grid(n), 256, 0, c->stream>>>(
           c->scratch, nsplit, n, n, out);
     });
   }
@@ -490,7 +490,7 @@ void long_contract(planc_gpu_ctx* c, bool left, const std::vector<int>& modes, d
   if (nsplit > 1) {
     const int64_t n = (left ? c->R : c->L) * c->k;
     launch(c, KC_REDUCE, [&] {
-      k_reduce_splits<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, c->stream>>>(
+      k_reduce_splits<<<reduce_grid(n), 256, 0, c->stream>>>(
           c->scratch, nsplit, n, n, out);
     });
   }
@@ -635,11 +635,13 @@ void normalize_gram(planc_gpu_ctx* c, int n, int next, double* lambda) {
     k_gram_finalize<<<1, 1024, 0, c->stream>>>(c->F[n], I, c->k, c->gram_part, nblk, lam,
                                                c->Gall, c->N, n, next, c->Gloo);
   });
-  launch(c, KC_NORMGRAM, [&] {
-    const int64_t ne = I * c->k;
-    k_scale_cols<<<(unsigned)std::min<int64_t>((ne + 255) / 256, 2048), 256, 0, c->stream>>>(
-        c->F[n], I, c->k, lam);
-  });
+  const int64_t ne = I * c->k;
+  if (ne > kFinalizeScaleMax) {
+    launch(c, KC_NORMGRAM, [&] {
+      k_scale_cols<<<(unsigned)std::min<int64_t>((ne + 255) / 256, 2048), 256, 0, c->stream>>>(
+          c->F[n], I, c->k, lam);
+    });
+  }
 }
 
 void gram_loo(planc_gpu_ctx* c, int n) {
@@ -1707,7 +1709,7 @@ extern "C" int planc_gpu_mttkrp_last_mode_noalloc(const double* X_dev, const int
     }
     CK(cudaGetLastError());
     const int64_t n = R * k;
-    k_reduce_splits<<<(unsigned)std::min<int64_t>((n + 255) / 256, 4096), 256, 0, st>>>(
+    k_reduce_splits<<<reduce_grid(n), 256, 0, st>>>(
         scratch, (int)ns, n, n, out_dev);
     CK(cudaGetLastError());
   });
