@@ -211,6 +211,14 @@ int planc_gpu_mttkrp_last_mode_noalloc(const double* X_dev, const int64_t* dims,
  * (PLANC_GPU_ERR_BPP_MAXITER) without a pathological input. */
 int planc_gpu_set_bpp_max_iter(planc_gpu_ctx* ctx, int max_iter);
 
+/* ANLS/BPP row solves of planc_gpu_run start from the passive set of the
+ * factor being replaced (enable = 1, the default) or from the empty set as
+ * NTFANLSBPP::update does (enable = 0, nnls/bppnnls.hpp:73-74). G is
+ * positive definite, so the NNLS optimum is unique and BPP reaches it from
+ * any start: the factors are the same, only the number of exchange steps
+ * drops. planc_gpu_bpp_solve always starts from the empty set. */
+int planc_gpu_set_bpp_warm_start(planc_gpu_ctx* ctx, int enable);
+
 /* Self-test of the kernels' bounded waits: launches one thread that waits on
  * a barrier nothing ever signals, with a limit of `seconds` (0 < s <= 5).
  * The wait runs out, the kernel writes the timeout status and returns; the

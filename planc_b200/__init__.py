@@ -37,7 +37,8 @@ EXPORTS = [
     "planc_gpu_objective_error", "planc_gpu_mode_begin", "planc_gpu_mode_end",
     "planc_gpu_bpp_solve", "planc_gpu_set_timing", "planc_gpu_get_kernel_times",
     "planc_gpu_launch_count", "planc_gpu_synth_cp_tensor", "planc_gpu_mttkrp_device",
-    "planc_gpu_tensor_norm2", "planc_gpu_set_bpp_max_iter", "planc_gpu_selftest_wait_timeout",
+    "planc_gpu_tensor_norm2", "planc_gpu_set_bpp_max_iter", "planc_gpu_set_bpp_warm_start",
+    "planc_gpu_selftest_wait_timeout",
     "planc_gpu_batch_create", "planc_gpu_batch_add", "planc_gpu_batch_count",
     "planc_gpu_batch_set_factors", "planc_gpu_batch_run", "planc_gpu_batch_get_factors",
     "planc_gpu_batch_autotune", "planc_gpu_batch_destroy", "planc_gpu_mttkrp_last_mode_noalloc",
@@ -89,6 +90,7 @@ def load():
     L.planc_gpu_mttkrp_device.argtypes = [vp, i32, P(vp), vp, i32]
     L.planc_gpu_tensor_norm2.argtypes = [vp, pd]
     L.planc_gpu_set_bpp_max_iter.argtypes = [vp, i32]
+    L.planc_gpu_set_bpp_warm_start.argtypes = [vp, i32]
     L.planc_gpu_batch_create.argtypes = [P(vp), i32, i32, i32]
     L.planc_gpu_batch_add.argtypes = [vp, vp, i32, pi64, i32, i32, P(pd), i32, P(i32)]
     L.planc_gpu_batch_count.argtypes = [vp]
@@ -257,6 +259,9 @@ class Context:
 
     def set_bpp_max_iter(self, n):
         _check(load().planc_gpu_set_bpp_max_iter(self.h, int(n)))
+
+    def set_bpp_warm_start(self, on):
+        _check(load().planc_gpu_set_bpp_warm_start(self.h, int(bool(on))))
 
     def set_timing(self, on):
         _check(load().planc_gpu_set_timing(self.h, int(on)))

@@ -212,7 +212,8 @@ __global__ void __launch_bounds__(32 * BPP_WARPS, 1) k_bpp(const double* __restr
                                                         int64_t ncols, double* __restrict__ Xout,
                                                         int* __restrict__ passive_out,
                                                         int* __restrict__ iters_out,
-                                                        int* __restrict__ status, int max_iter_override) {
+                                                        int* __restrict__ status, int max_iter_override,
+                                                        const double* __restrict__ Pinit) {
   constexpr int LD = KP + 1, R = KP > 32 ? 2 : 1;
   extern __shared__ __align__(16) unsigned char bpp_smem[];
   double* AtA = reinterpret_cast<double*>(bpp_smem);  // n x n, leading dimension n
@@ -262,25 +263,10 @@ __global__ void __launch_bounds__(32 * BPP_WARPS, 1) k_bpp(const double* __restr
     nonopt = warp_mask64(lo_no, hi_no);
     infea = warp_mask64(lo_in, hi_in);
   };
-  uint64_t nonopt, infea;
-  classify(nonopt, infea);
-  int notgood = __popcll(nonopt) + __popcll(infea);
-  unsigned iter = 0;
-  int st = 0;
-  while (notgood > 0) {
-    ++iter;
-    if (iter > max_it) { st = kStBppMaxIter; break; }
-    if (notgood < Ninf) {  // Cols1, bppnnls.hpp:109, 115-129
-      P = pbar;
-      Ninf = notgood;
-      passive = (passive | nonopt) & ~infea;
-    } else if (P >= 1) {  // Cols2, bppnnls.hpp:110, 133-146
-      P -= 1;
-      passive = (passive | nonopt) & ~infea;
-    } else {  // backup rule: flip the largest offending index, bppnnls.hpp:149-160
-      int rowidx = 63 - __clzll(nonopt | infea);
-      passive ^= (1ull << rowidx);
-    }
+  // X(P) = solve(AtA(P,P), AtB(P)), X(~P) = 0, Y = AtA X - AtB and the 1e-12
+  // zeroing for the current passive set; returns 0 or a failure status
+  auto solve_passive = [&]() -> int {
+    int bad = 0;
     // solve the passive system AtA(P,P) x_P = AtB(P), bppnnls.hpp:163-166 / 204-259
     const int m = __popcll(passive);
     // idx[q] = position of the q-th passive index (warp-parallel compaction)
@@ -306,7 +292,7 @@ __global__ void __launch_bounds__(32 * BPP_WARPS, 1) k_bpp(const double* __restr
         for (int i = lane; i < m; i += 32) zs[i] = b[idx[i]];
         __syncwarp();
         const int rc = warp_lu_solve(Ls, LD, m, zs);
-        if (rc != 0) { st = rc; break; }
+        if (rc != 0) return rc;
         __syncwarp();
 #pragma unroll
         for (int q = 0; q < R; ++q) {
@@ -340,11 +326,49 @@ __global__ void __launch_bounds__(32 * BPP_WARPS, 1) k_bpp(const double* __restr
       const double yi = (a0 + a1) - b[i];
       y[i] = (fabs(yi) < kEps12) ? 0.0 : yi;
       const double xi = x[i];
-      if (!isfinite(xi) || !isfinite(yi)) st = kStNonFinite;
+      if (!isfinite(xi) || !isfinite(yi)) bad = kStNonFinite;
       x[i] = (fabs(xi) < kEps12) ? 0.0 : xi;
     }
     __syncwarp();
-    st = __reduce_min_sync(0xffffffffu, st);
+    __syncwarp();
+    return __reduce_min_sync(0xffffffffu, bad);
+  };
+  unsigned iter = 0;
+  int st = 0;
+  if (Pinit) {
+    // warm start from the previous solution's passive set: BPP reaches the
+    // unique NNLS optimum from any starting set (Kim & Park), so the result
+    // is the reference's; only the number of exchange steps changes
+    const bool lo = has_lo && Pinit[c * n + lane] > 0.0;
+    const bool hi = has_hi && Pinit[c * n + lane + 32] > 0.0;
+    passive = warp_mask64(lo, hi);
+    __syncwarp();  // every lane has read its Pinit before any store below
+    if (passive) {
+      ++iter;
+      st = solve_passive();
+    }
+  }
+  uint64_t nonopt = 0, infea = 0;
+  int notgood = 0;
+  if (st == 0) {
+    classify(nonopt, infea);
+    notgood = __popcll(nonopt) + __popcll(infea);
+  }
+  while (st == 0 && notgood > 0) {
+    ++iter;
+    if (iter > max_it) { st = kStBppMaxIter; break; }
+    if (notgood < Ninf) {  // Cols1, bppnnls.hpp:109, 115-129
+      P = pbar;
+      Ninf = notgood;
+      passive = (passive | nonopt) & ~infea;
+    } else if (P >= 1) {  // Cols2, bppnnls.hpp:110, 133-146
+      P -= 1;
+      passive = (passive | nonopt) & ~infea;
+    } else {  // backup rule: flip the largest offending index, bppnnls.hpp:149-160
+      int rowidx = 63 - __clzll(nonopt | infea);
+      passive ^= (1ull << rowidx);
+    }
+    st = solve_passive();
     if (st != 0) break;
     classify(nonopt, infea);
     notgood = __popcll(nonopt) + __popcll(infea);

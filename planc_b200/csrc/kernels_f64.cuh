@@ -538,19 +538,25 @@ __global__ void __launch_bounds__(256) k_mu_warp(double* __restrict__ H, const d
 // of the normalised factor G_n = (U^T U)_ab / (lambda_a lambda_b), normalises
 // U in place (ncpfactors.hpp:346-351) and forms the next leave-one-out product.
 // ---------------------------------------------------------------------------
-constexpr int GP_ROWS = 16;
-// Largest I*k that k_gram_finalize normalises itself (one CTA); above it the
-// many-CTA k_scale_cols does.
-constexpr int64_t kFinalizeScaleMax = 65536;
+constexpr int GP_ROWS = 16;      // fewest rows per block (partial buffers are sized for it)
+constexpr int GP_ROWS_MAX = 64;  // most rows per block (shared-memory tile)
+
+// Rows per block: about 32 blocks per factor (more blocks than that only
+// lengthen k_gram_finalize's fixed-order sum), between GP_ROWS and GP_ROWS_MAX.
+inline int gram_rows_per_block(int64_t I) {
+  int64_t r = (I + 31) / 32;
+  r = (r + GP_ROWS - 1) / GP_ROWS * GP_ROWS;
+  return (int)(r < GP_ROWS ? GP_ROWS : (r > GP_ROWS_MAX ? GP_ROWS_MAX : r));
+}
 
 // 256 threads; thread (ta, tb) owns the 4 x 4 outputs a = ta + kt*u,
 // b = tb + kt*v (kt = ceil(k/4)), so a warp's loads of the b-values are
 // consecutive in shared memory.
 __global__ void __launch_bounds__(256) k_gram_partial(const double* __restrict__ U, int64_t I, int k,
-                                                      double* __restrict__ part) {
-  __shared__ double tile[GP_ROWS * kMaxRank];
-  const int64_t row0 = (int64_t)blockIdx.x * GP_ROWS;
-  const int nrows = (int)((I - row0) < GP_ROWS ? (I - row0) : GP_ROWS);
+                                                      int rows_per_block, double* __restrict__ part) {
+  __shared__ double tile[GP_ROWS_MAX * kMaxRank];
+  const int64_t row0 = (int64_t)blockIdx.x * rows_per_block;
+  const int nrows = (int)((I - row0) < rows_per_block ? (I - row0) : rows_per_block);
   for (int e = threadIdx.x; e < nrows * k; e += 256) tile[e] = U[row0 * k + e];
   __syncthreads();
   const int kt = (k + 3) / 4;
@@ -588,8 +594,8 @@ __global__ void __launch_bounds__(256) k_gram_partial(const double* __restrict__
 
 // One CTA: sums the row-block partials in a fixed order (eight independent
 // running sums per element), lambda_r = sqrt((U^T U)_rr), G_n = (U^T U)_ab /
-// (lambda_a lambda_b), the next leave-one-out product and, when
-// I*k <= kFinalizeScaleMax, the normalisation U(:, r) /= lambda_r itself.
+// (lambda_a lambda_b) and the next leave-one-out product; k_scale_cols then
+// normalises U.
 __global__ void __launch_bounds__(1024) k_gram_finalize(double* __restrict__ F, int64_t I, int k,
                                                         const double* __restrict__ part, int nblk,
                                                         double* __restrict__ lambda,
@@ -616,12 +622,6 @@ __global__ void __launch_bounds__(1024) k_gram_finalize(double* __restrict__ F, 
     if (lambda) lambda[tid] = nrm;
   }
   __syncthreads();
-  if (I * k <= kFinalizeScaleMax) {
-    for (int64_t e = tid; e < I * k; e += 1024) {
-      const double nrm = lam[e % k];
-      if (nrm > 0) F[e] = F[e] / nrm;
-    }
-  }
   double* Gn = Gall + (int64_t)n * kk2;
   for (int e = tid; e < kk2; e += 1024) {
     const int a = e / k, b = e % k;

@@ -124,6 +124,7 @@ struct planc_gpu_ctx {
   int64_t klaunch[KC_COUNT] = {0};
   int64_t launch_count = 0;
   int bpp_max_iter = 0;  // 0: the reference's 5k cap
+  bool bpp_warm = true;  // ANLS/BPP rows start from the replaced factor's passive set
   // Fraction of the GPU one launch of this context aims to fill (split-K and
   // grid sizing). 1 for a context alone on the GPU; the batch autotuner lowers
   // it when many contexts run concurrently.
@@ -611,7 +612,8 @@ void run_update(planc_gpu_ctx* c, int algo, int n) {
 #define CASE(KP)                                                                                   \
   case KP:                                                                                         \
     k_bpp<KP><<<blocks, 32 * BPP_WARPS, bpp_smem_bytes(KP), c->stream>>>(                      \
-        c->Gloo, c->M[n], k, I, c->F[n], nullptr, nullptr, c->status_dev, c->bpp_max_iter);        \
+        c->Gloo, c->M[n], k, I, c->F[n], nullptr, nullptr, c->status_dev, c->bpp_max_iter,         \
+        c->bpp_warm ? c->F[n] : nullptr);                                                          \
     break;
         CASE(8) CASE(16) CASE(32) CASE(64)
 #undef CASE
@@ -624,24 +626,23 @@ void run_update(planc_gpu_ctx* c, int algo, int n) {
 
 void normalize_gram(planc_gpu_ctx* c, int n, int next, double* lambda) {
   const int64_t I = c->dims[n];
-  const int nblk = (int)((I + GP_ROWS - 1) / GP_ROWS);
+  const int rpb = gram_rows_per_block(I);
+  const int nblk = (int)((I + rpb - 1) / rpb);
   if ((size_t)nblk * c->k * c->k > c->gram_part_elems)
     fail(PLANC_GPU_ERR_STATE, "internal: Gram partial buffer too small");
   launch(c, KC_NORMGRAM, [&] {
-    k_gram_partial<<<nblk, 256, 0, c->stream>>>(c->F[n], I, c->k, c->gram_part);
+    k_gram_partial<<<nblk, 256, 0, c->stream>>>(c->F[n], I, c->k, rpb, c->gram_part);
   });
   double* lam = lambda ? lambda : c->lam_tmp;
   launch(c, KC_NORMGRAM, [&] {
     k_gram_finalize<<<1, 1024, 0, c->stream>>>(c->F[n], I, c->k, c->gram_part, nblk, lam,
                                                c->Gall, c->N, n, next, c->Gloo);
   });
-  const int64_t ne = I * c->k;
-  if (ne > kFinalizeScaleMax) {
-    launch(c, KC_NORMGRAM, [&] {
-      k_scale_cols<<<(unsigned)std::min<int64_t>((ne + 255) / 256, 2048), 256, 0, c->stream>>>(
-          c->F[n], I, c->k, lam);
-    });
-  }
+  launch(c, KC_NORMGRAM, [&] {
+    const int64_t ne = I * c->k;
+    k_scale_cols<<<(unsigned)std::min<int64_t>((ne + 255) / 256, 2048), 256, 0, c->stream>>>(
+        c->F[n], I, c->k, lam);
+  });
 }
 
 void gram_loo(planc_gpu_ctx* c, int n) {
@@ -1152,7 +1153,7 @@ int planc_gpu_bpp_solve(planc_gpu_ctx* c, const double* AtA, const double* AtB, 
 #define CASE(KP)                                                                            \
   case KP:                                                                                  \
     k_bpp<KP><<<blocks, 32 * BPP_WARPS, bpp_smem_bytes(KP), c->stream>>>(                    \
-        dA, dB, n, ncols, dX, dP, dI, c->status_dev, c->bpp_max_iter);                           \
+        dA, dB, n, ncols, dX, dP, dI, c->status_dev, c->bpp_max_iter, nullptr);                  \
     break;
           CASE(8) CASE(16) CASE(32) CASE(64)
 #undef CASE
@@ -1220,6 +1221,16 @@ int planc_gpu_set_bpp_max_iter(planc_gpu_ctx* c, int max_iter) {
     if (!c || max_iter < 0) fail(PLANC_GPU_ERR_ARG, "bad argument");
     c->bpp_max_iter = max_iter;
     reset_graph(c);
+  });
+}
+
+int planc_gpu_set_bpp_warm_start(planc_gpu_ctx* c, int enable) {
+  return guarded([&] {
+    if (!c) fail(PLANC_GPU_ERR_ARG, "null context");
+    if (c->bpp_warm != (enable != 0)) {
+      c->bpp_warm = enable != 0;
+      reset_graph(c);  // captured graphs hold the launch arguments
+    }
   });
 }
 

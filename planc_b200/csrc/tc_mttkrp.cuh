@@ -1085,21 +1085,38 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
 
 // Pre-swizzled hi|lo image of a Khatri-Rao product W(kk, r) = prod_t
 // F_t[digit_t(kk), r] (the B operand of k_tc_long), laid out as k_tc_bimage.
+// One thread per (k block, r, 16-byte chunk): eight consecutive kk, written
+// as one 16-byte store each for hi and lo. Two-mode products with K < 2^31
+// (the balanced 4-way tree) take their digits with 32-bit arithmetic.
 template <int KP>
 __global__ void k_tc_wimage(const WGen wg, int64_t K, int k, int64_t nk, uint8_t* __restrict__ img) {
   constexpr int NCOL = 2 * KP;
-  const int64_t total = nk * KP * TC_BK;
+  const int64_t total = nk * KP * (TC_BK / 8);
+  const bool two32 = wg.nf == 2 && K < ((int64_t)1 << 31);
   for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
        e += (int64_t)gridDim.x * blockDim.x) {
-    const int kk = (int)(e % TC_BK);
-    const int r = (int)((e / TC_BK) % KP);
-    const int64_t kb = e / ((int64_t)TC_BK * KP);
-    const int64_t j = kb * TC_BK + kk;
-    __nv_bfloat16 hi = __float2bfloat16(0.f), lo = __float2bfloat16(0.f);
-    if (j < K && r < k) split_bf16(wgen_eval(wg, j, r, k), hi, lo);
+    const int ch = (int)(e % (TC_BK / 8));
+    const int r = (int)((e / (TC_BK / 8)) % KP);
+    const int64_t kb = e / ((int64_t)(TC_BK / 8) * KP);
+    alignas(16) __nv_bfloat16 hi[8], lo[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int64_t j = kb * TC_BK + ch * 8 + u;
+      double w = 0.0;
+      if (j < K && r < k) {
+        if (two32) {
+          const int jj = (int)j, d0 = (int)wg.dim[0];
+          const int i1 = jj / d0, i0 = jj - i1 * d0;
+          w = wg.f[0][(int64_t)i0 * k + r] * wg.f[1][(int64_t)i1 * k + r];
+        } else {
+          w = wgen_eval(wg, j, r, k);
+        }
+      }
+      split_bf16(w, hi[u], lo[u]);
+    }
     uint8_t* st = img + (size_t)kb * NCOL * 128;
-    *reinterpret_cast<__nv_bfloat16*>(st + sw128_kmajor_off(r, kk)) = hi;
-    *reinterpret_cast<__nv_bfloat16*>(st + sw128_kmajor_off(KP + r, kk)) = lo;
+    *reinterpret_cast<uint4*>(st + sw128_kmajor_off(r, ch * 8)) = *reinterpret_cast<const uint4*>(hi);
+    *reinterpret_cast<uint4*>(st + sw128_kmajor_off(KP + r, ch * 8)) = *reinterpret_cast<const uint4*>(lo);
   }
 }
 
@@ -1487,7 +1504,7 @@ inline void tc_long_prep(const TcTensor& t, bool left, const WGen& wg, int k, cu
   const int64_t K = left ? t.L : t.R;
   const int64_t nk = (K + TC_BK - 1) / TC_BK;
   const int kp = tc_kpad(k);
-  const unsigned blocks = (unsigned)std::min<int64_t>((nk * kp * TC_BK + 255) / 256, 2048);
+  const unsigned blocks = (unsigned)std::min<int64_t>((nk * kp * (TC_BK / 8) + 255) / 256, 2048);
   if (kp == 16)
     k_tc_wimage<16><<<blocks, 256, 0, st>>>(wg, K, k, nk, t.wimg);
   else if (kp == 32)

@@ -1,0 +1,119 @@
+"""Small, fixed workloads for profiling single kernels of the library.
+
+    python -m planc_b200.profile_cases <case>
+
+Each case builds its input on the device, runs the path a few times and
+prints one line of timings. The cases are sized so that a profiler capture of
+one launch holds a few GB of device memory at most while the tensors stay
+larger than the 126 MB L2 (DRAM counters stay meaningful):
+
+  bpp     k_bpp: ANLS/BPP normal equations of a 192-row mode at rank 64 taken
+          from a 192 x 96 x 96 x 96 sparse-factor CP tensor after 10
+          iterations (passive sets of ~45, ~3 BPP steps per row)
+  tc3     k_tc_right / k_tc_left_fac: 512^3 FP32 tensor (BF16 copy), rank 32,
+          HALS iterations
+  tc4     k_tc_long (both sides) + the multi-TTVs of the balanced 4-way tree:
+          128^4 FP32 tensor (BF16 copy), rank 64, HALS iterations
+  cfg3it  three ANLS/BPP iterations of the 192^4 rank-64 workload (BF16), for
+          a one-pass launch list at full size
+"""
+import sys
+
+import numpy as np
+
+
+def _synth(gpu, torch, dims, k, seed, sparse=False):
+    rng = np.random.default_rng(seed)
+    A = []
+    for d in dims:
+        a = rng.random((d, k))
+        if sparse:
+            a[rng.random(a.shape) < 0.5] = 0.0
+        A.append(a)
+    G = np.ones((k, k))
+    for a in A:
+        G *= a.T @ a
+    sigma = 0.01 * np.sqrt(G.sum() / float(np.prod(dims)))
+    X = torch.empty(int(np.prod(dims)), dtype=torch.float32, device="cuda:0")
+    gpu.synth_cp_tensor(0, X.data_ptr(), "f32", dims, A, sigma, seed + 1, clip=True)
+    F0 = [np.random.default_rng(seed + 2).random((d, k)) for d in dims]
+    return X, F0
+
+
+def _timed(torch, ctx, fn, reps):
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(reps):
+        fn()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / reps
+
+
+def case_bpp(gpu, torch):
+    dims, k = (192, 96, 96, 96), 64
+    X, F0 = _synth(gpu, torch, dims, k, 11, sparse=True)
+    with gpu.Context(0, "bf16") as c:
+        c.set_tensor(X.data_ptr(), dims=dims, dtype="f32")
+        c.set_factors(F0)
+        c.run("anlsbpp", 10, compute_error=False)
+        G, M = c.mode_begin(0)
+    with gpu.Context(0, "fp64") as c:
+        for _ in range(3):
+            c.set_timing(True)
+            c.kernel_times()
+            _, P, its = c.bpp_solve(G, M.T)
+            ms = c.kernel_times()["bpp"][0]
+            c.set_timing(False)
+    print("bpp: 192 rows, k=64: kernel %.1f us, BPP steps mean %.2f max %d, passive mean %.1f"
+          % (ms * 1e3, its.mean(), its.max(), P.sum(axis=0).mean()))
+
+
+def case_tc3(gpu, torch):
+    dims, k = (512, 512, 512), 32
+    X, F0 = _synth(gpu, torch, dims, k, 21)
+    with gpu.Context(0, "bf16") as c:
+        c.set_tensor(X.data_ptr(), dims=dims, dtype="f32")
+        c.set_factors(F0)
+        ms = _timed(torch, c, lambda: c.run("hals", 1, compute_error=False), 3)
+    print("tc3: 512^3 k=32 HALS: %.3f ms per iteration" % ms)
+
+
+def case_tc4(gpu, torch):
+    dims, k = (128, 128, 128, 128), 64
+    X, F0 = _synth(gpu, torch, dims, k, 31)
+    with gpu.Context(0, "bf16") as c:
+        c.set_tensor(X.data_ptr(), dims=dims, dtype="f32")
+        c.set_factors(F0)
+        ms = _timed(torch, c, lambda: c.run("hals", 1, compute_error=False), 3)
+    print("tc4: 128^4 k=64 HALS: %.3f ms per iteration" % ms)
+
+
+def case_cfg3it(gpu, torch):
+    dims, k = (192, 192, 192, 192), 64
+    X, F0 = _synth(gpu, torch, dims, k, 301, sparse=True)
+    with gpu.Context(0, "bf16") as c:
+        c.set_tensor(X.data_ptr(), dims=dims, dtype="f32")
+        c.set_factors(F0)
+        ms = _timed(torch, c, lambda: c.run("anlsbpp", 1, compute_error=True), 3)
+    print("cfg3it: 192^4 k=64 ANLS/BPP: %.3f ms per iteration" % ms)
+
+
+CASES = {"bpp": case_bpp, "tc3": case_tc3, "tc4": case_tc4, "cfg3it": case_cfg3it}
+
+
+def main(argv):
+    if len(argv) != 1 or argv[0] not in CASES:
+        print("usage: python -m planc_b200.profile_cases {%s}" % "|".join(CASES))
+        return 2
+    import torch
+
+    import planc_b200 as gpu
+    CASES[argv[0]](gpu, torch)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main(sys.argv[1:]))

@@ -123,6 +123,32 @@ def test_bpp_solve_masks_and_values(gpu, oracle_lib, n):
     assert itg.max() <= 5 * n
 
 
+def test_bpp_warm_start_reaches_the_same_factors(gpu, oracle_lib):
+    # the ANLS/BPP rows start from the replaced factor's passive set by
+    # default; the unique NNLS optima, hence the factors, equal the cold-start
+    # (reference, bppnnls.hpp:73-74) run and the oracle's
+    dims, k, iters = (40, 36, 28, 24), 10, 12
+    rng = np.random.default_rng(71)
+    A = [rng.random((d, k)) * (rng.random((d, k)) < 0.5) for d in dims]
+    X = np.einsum("az,bz,cz,dz->abcd", *A)
+    X = np.asfortranarray(np.maximum(X + 0.01 * X.std() * rng.standard_normal(dims), 0.0))
+    F0 = init_factors(dims, k, seed=72)
+    res = {}
+    for warm in (True, False):
+        with gpu.Context(0, "fp64") as c:
+            c.set_tensor(X)
+            c.set_factors(F0)
+            c.set_bpp_warm_start(warm)
+            e = c.run("anlsbpp", iters)
+            F, lam = c.get_factors()
+            res[warm] = (F, lam, e)
+    Fo, lo, eo = oracle_lib.ntf_run(X, F0, "anlsbpp", iters)
+    for warm in (True, False):
+        F, lam, e = res[warm]
+        assert all(rel(a, b) < 1e-10 for a, b in zip(F, Fo)), warm
+        assert np.max(np.abs(e - eo) / eo) < 1e-10, warm
+
+
 def test_bpp_singular_normal_equations_reports_status(gpu):
     # AtA with a zero row/column at an index that enters the passive set:
     # the solve has no pivot; the call returns ERR_SINGULAR and the context
