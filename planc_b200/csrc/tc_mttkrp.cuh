@@ -880,6 +880,17 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
   }
 }
 
+// (s0, s1) += (a0 + b0, a1 + b1) with two packed FP32x2 adds (each lane
+// rounded to nearest, as two scalar adds would be).
+__device__ __forceinline__ void add2_acc(float& s0, float& s1, float a0, float a1, float b0, float b1) {
+  asm("{\n\t.reg .b64 s, a, b;\n\t"
+      "mov.b64 s, {%0, %1};\n\tmov.b64 a, {%2, %3};\n\tmov.b64 b, {%4, %5};\n\t"
+      "add.rn.f32x2 a, a, b;\n\tadd.rn.f32x2 s, s, a;\n\t"
+      "mov.b64 {%0, %1}, s;\n\t}"
+      : "+f"(s0), "+f"(s1)
+      : "f"(a0), "f"(a1), "f"(b0), "f"(b1));
+}
+
 // ------------------------------------------------------------ long-K kernel
 // part[y][row*k + r] = sum over the K blocks of split y of A(row, K) W(K, r)
 // with W a pre-swizzled hi|lo image (k_tc_wimage):
@@ -907,14 +918,15 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
   constexpr uint32_t B_STAGE = NCOL * 128;
   constexpr uint32_t STAGE = A_STAGE + B_STAGE;
   constexpr uint32_t ACC_COLS = MT * NCOL;
-  constexpr uint32_t TMEM_NEED = 2 * ACC_COLS;
+  constexpr int NBUF = 4;  // accumulators in flight (4 * ACC_COLS <= 512 columns)
+  constexpr uint32_t TMEM_NEED = NBUF * ACC_COLS;
   constexpr uint32_t TMEM_COLS = TMEM_NEED <= 32 ? 32 : TMEM_NEED <= 64 ? 64 : TMEM_NEED <= 128 ? 128
                                  : TMEM_NEED <= 256 ? 256 : 512;
   constexpr uint32_t IDESC = idesc_bf16(NCOL, !KMAJ, false);
   using Acc = float;  // register adds round to nearest: no drift from the many drains
 
   extern __shared__ uint8_t smem_raw[];
-  __shared__ uint64_t bars[2 * 8 + 4];
+  __shared__ uint64_t bars[2 * 8 + 2 * NBUF];
   __shared__ uint32_t tmem_base_sh;
   __shared__ int abort_sh;
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -929,7 +941,7 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
   auto full = [&](int s) { return smem_u32(&bars[s]); };
   auto empty = [&](int s) { return smem_u32(&bars[8 + s]); };
   auto accf = [&](int b) { return smem_u32(&bars[16 + b]); };
-  auto acce = [&](int b) { return smem_u32(&bars[18 + b]); };
+  auto acce = [&](int b) { return smem_u32(&bars[16 + NBUF + b]); };
 
   if (threadIdx.x == 0) {
     abort_sh = 0;
@@ -937,7 +949,7 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
       mbar_init(full(s), 1);
       mbar_init(empty(s), 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < NBUF; ++b) {
       mbar_init(accf(b), 1);
       mbar_init(acce(b), 4);
     }
@@ -986,13 +998,13 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
     if (lane == 0) {
       int s = 0;
       uint32_t ph = 0;
-      uint32_t aph[2] = {0, 0};
+      uint32_t aph = 0;  // bit b: phase of accumulator b
       bool ok = true;
       for (int64_t i = 0; i < my_groups && ok; ++i) {
-        const int buf = (int)(i & 1);
+        const int buf = (int)(i % NBUF);
         const int64_t g = y + i * ns;
         const int64_t kb0 = g * group, kb1 = min((g + 1) * group, nk);
-        if (!mbar_wait(acce(buf), aph[buf] ^ 1, abort_flag, status)) break;
+        if (!mbar_wait(acce(buf), ((aph >> buf) & 1) ^ 1, abort_flag, status)) break;
         tc_fence_after();
         const uint32_t d = tmem + buf * ACC_COLS;
         for (int64_t kb = kb0; kb < kb1; ++kb) {
@@ -1021,7 +1033,7 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
         }
         if (!ok) break;
         umma_commit(accf(buf));
-        aph[buf] ^= 1;
+        aph ^= 1u << buf;
       }
     }
   } else {
@@ -1032,11 +1044,11 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
     for (int mt = 0; mt < MT; ++mt)
 #pragma unroll
       for (int r = 0; r < KP; ++r) sum[mt][r] = 0;
-    uint32_t aph[2] = {0, 0};
+    uint32_t aph = 0;
     bool ok = true;
     for (int64_t i = 0; i < my_groups; ++i) {
-      const int buf = (int)(i & 1);
-      if (!mbar_wait(accf(buf), aph[buf], abort_flag, status)) { ok = false; break; }
+      const int buf = (int)(i % NBUF);
+      if (!mbar_wait(accf(buf), (aph >> buf) & 1, abort_flag, status)) { ok = false; break; }
       tc_fence_after();
 #pragma unroll
       for (int mt = 0; mt < MT; ++mt) {
@@ -1052,14 +1064,15 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
             float vh[32], vl[32];
             tmem_ld32x2(base + cc, base + KP + cc, vh, vl);
 #pragma unroll
-            for (int e = 0; e < 32; ++e) sum[mt][cc + e] += vh[e] + vl[e];
+            for (int e = 0; e < 32; e += 2)
+              add2_acc(sum[mt][cc + e], sum[mt][cc + e + 1], vh[e], vh[e + 1], vl[e], vl[e + 1]);
           }
         }
       }
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(acce(buf));
-      aph[buf] ^= 1;
+      aph ^= 1u << buf;
     }
     if (ok) {
       double* dst = part + y * rows * k;
