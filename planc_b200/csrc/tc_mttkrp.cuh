@@ -258,11 +258,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   constexpr uint32_t A_STAGE = X2 ? 2 * A_BYTES : A_BYTES;
   constexpr uint32_t B_STAGE = NCOL * 128;           // NCOL rows x 128 B
   constexpr uint32_t STAGE = A_STAGE + B_STAGE;
-  constexpr uint32_t TMEM_COLS = 2 * NCOL < 32 ? 32 : 2 * NCOL;
+  constexpr int NBUF = 4;  // accumulators in flight
+  constexpr uint32_t TMEM_COLS = NBUF * NCOL < 32 ? 32 : NBUF * NCOL;
   constexpr uint32_t IDESC = idesc_bf16(NCOL, true, false);
 
   extern __shared__ uint8_t smem_raw[];
-  __shared__ uint64_t bars[2 * 8 + 4];
+  __shared__ uint64_t bars[2 * 8 + 2 * NBUF];
   __shared__ uint32_t tmem_base_sh;
   __shared__ int abort_sh;
   uint8_t* smem = (uint8_t*)(((uintptr_t)smem_raw + 1023) & ~(uintptr_t)1023);
@@ -273,7 +274,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   auto full = [&](int s) { return smem_u32(&bars[s]); };
   auto empty = [&](int s) { return smem_u32(&bars[8 + s]); };
   auto accf = [&](int b) { return smem_u32(&bars[16 + b]); };
-  auto acce = [&](int b) { return smem_u32(&bars[18 + b]); };
+  auto acce = [&](int b) { return smem_u32(&bars[16 + NBUF + b]); };
 
   if (threadIdx.x == 0) {
     abort_sh = 0;
@@ -281,7 +282,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       mbar_init(full(s), 1);
       mbar_init(empty(s), 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < NBUF; ++b) {
       mbar_init(accf(b), 1);
       mbar_init(acce(b), 4);
     }
@@ -320,10 +321,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       int s = 0;
       uint32_t ph = 0;
       int buf = 0;
-      uint32_t aph[2] = {0, 0};
+      uint32_t aph = 0;  // bit b: phase of accumulator b
       bool ok = true;
       for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
-        if (!mbar_wait(acce(buf), aph[buf] ^ 1, abort_flag, status)) break;
+        if (!mbar_wait(acce(buf), ((aph >> buf) & 1) ^ 1, abort_flag, status)) break;
         tc_fence_after();
         const uint32_t d = tmem + buf * NCOL;
         for (int kb = 0; kb < nk; ++kb) {
@@ -346,17 +347,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         }
         if (!ok) break;
         umma_commit(accf(buf));
-        aph[buf] ^= 1;
-        buf ^= 1;
+        aph ^= 1u << buf;
+        buf = (buf + 1) % NBUF;
       }
     }
   } else {
     // epilogue warps 2..5: TMEM lane quarter = warp % 4
     const int q = warp & 3;
     int buf = 0;
-    uint32_t aph[2] = {0, 0};
+    uint32_t aph = 0;
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-      if (!mbar_wait(accf(buf), aph[buf], abort_flag, status)) break;
+      if (!mbar_wait(accf(buf), (aph >> buf) & 1, abort_flag, status)) break;
       tc_fence_after();
       const int64_t row = t * TC_BM + q * 32 + lane;
       float v[NCOL];
@@ -366,8 +367,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(acce(buf));
-      aph[buf] ^= 1;
-      buf ^= 1;
+      aph ^= 1u << buf;
+      buf = (buf + 1) % NBUF;
       if (row < L) {
         float* dst = P + row * k;
         if (k == KP && (KP % 4) == 0) {
@@ -703,14 +704,15 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
   constexpr uint32_t B_STAGE = NCOL * 128;
   constexpr uint32_t STAGE = A_STAGE + B_STAGE;
   constexpr uint32_t ACC_COLS = MT * NCOL;
-  constexpr uint32_t TMEM_NEED = 2 * ACC_COLS;
+  constexpr int NBUF = 4 * ACC_COLS <= 512 ? 4 : 2;  // accumulators in flight
+  constexpr uint32_t TMEM_NEED = NBUF * ACC_COLS;
   constexpr uint32_t TMEM_COLS = TMEM_NEED <= 32 ? 32 : TMEM_NEED <= 64 ? 64 : TMEM_NEED <= 128 ? 128
                                  : TMEM_NEED <= 256 ? 256 : 512;
   constexpr uint32_t IDESC = idesc_bf16(NCOL, false, false);
   using Acc = typename std::conditional<(MT * KP <= 64), double, float>::type;
 
   extern __shared__ uint8_t smem_raw[];
-  __shared__ uint64_t bars[2 * 8 + 4];
+  __shared__ uint64_t bars[2 * 8 + 2 * NBUF];
   __shared__ uint32_t tmem_base_sh;
   __shared__ int abort_sh;
   __shared__ double tail_w[4][KP];
@@ -726,7 +728,7 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
   auto full = [&](int s) { return smem_u32(&bars[s]); };
   auto empty = [&](int s) { return smem_u32(&bars[8 + s]); };
   auto accf = [&](int b) { return smem_u32(&bars[16 + b]); };
-  auto acce = [&](int b) { return smem_u32(&bars[18 + b]); };
+  auto acce = [&](int b) { return smem_u32(&bars[16 + NBUF + b]); };
 
   if (threadIdx.x == 0) {
     abort_sh = 0;
@@ -734,7 +736,7 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
       mbar_init(full(s), 1);
       mbar_init(empty(s), 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < NBUF; ++b) {
       mbar_init(accf(b), 1);
       mbar_init(acce(b), 4);
     }
@@ -771,11 +773,11 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
     if (lane == 0) {
       int s = 0;
       uint32_t ph = 0;
-      uint32_t aph[2] = {0, 0};
+      uint32_t aph = 0;  // bit b: phase of accumulator b
       bool ok = true;
       for (int64_t i = 0; i < my_runs && ok; ++i) {
-        const int buf = (int)(i & 1);
-        if (!mbar_wait(acce(buf), aph[buf] ^ 1, abort_flag, status)) break;
+        const int buf = (int)(i % NBUF);
+        if (!mbar_wait(acce(buf), ((aph >> buf) & 1) ^ 1, abort_flag, status)) break;
         tc_fence_after();
         const uint32_t d = tmem + buf * ACC_COLS;
         for (int64_t q = 0; q < G; ++q) {
@@ -800,7 +802,7 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
         }
         if (!ok) break;
         umma_commit(accf(buf));
-        aph[buf] ^= 1;
+        aph ^= 1u << buf;
       }
     }
   } else {
@@ -813,10 +815,10 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
     for (int mt = 0; mt < MT; ++mt)
 #pragma unroll
       for (int r = 0; r < KP; ++r) sum[mt][r] = 0;
-    uint32_t aph[2] = {0, 0};
+    uint32_t aph = 0;
     bool ok = true;
     for (int64_t i = 0; i < my_runs; ++i) {
-      const int buf = (int)(i & 1);
+      const int buf = (int)(i % NBUF);
       const int64_t g = y + i * ns;
       const int64_t i1 = F2 ? g % D1 : g;
       const int64_t i2 = F2 ? g / D1 : 0;
@@ -830,7 +832,7 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
         tail[r] = t;
       }
       __syncwarp();
-      if (!mbar_wait(accf(buf), aph[buf], abort_flag, status)) { ok = false; break; }
+      if (!mbar_wait(accf(buf), (aph >> buf) & 1, abort_flag, status)) { ok = false; break; }
       tc_fence_after();
 #pragma unroll
       for (int mt = 0; mt < MT; ++mt) {
@@ -856,7 +858,7 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(acce(buf));
-      aph[buf] ^= 1;
+      aph ^= 1u << buf;
     }
     if (ok) {
       double* dst = part + y * R * k;
