@@ -43,6 +43,7 @@ extern "C" {
 #define PLANC_GPU_ERR_UNSUPPORTED (-7) /* shape/rank outside what the kernels take */
 #define PLANC_GPU_ERR_OOM (-8)         /* device allocation failed */
 #define PLANC_GPU_ERR_SINGULAR (-9)    /* a normal-equation solve found no pivot */
+#define PLANC_GPU_ERR_MAXITER (-10)    /* a Nesterov update reached its inner step cap */
 
 /* MTTKRP precision. The Gram matrices, the factor updates, the BPP solves and
  * the error are FP64 in every mode. */
@@ -54,6 +55,8 @@ extern "C" {
 #define PLANC_GPU_MU 0
 #define PLANC_GPU_HALS 1
 #define PLANC_GPU_ANLSBPP 2
+#define PLANC_GPU_AOADMM 4    /* NTFAOADMM, ntf/ntfaoadmm.hpp:23-77 */
+#define PLANC_GPU_NESTEROV 5  /* NTFNES, ntf/ntfnes.hpp:11-166 */
 
 /* element types of a tensor handed to planc_gpu_set_tensor */
 #define PLANC_GPU_F64 0
@@ -94,11 +97,17 @@ int planc_gpu_set_factors(planc_gpu_ctx* ctx, const double* const* F,
                           const double* lambda, int k);
 
 /* Runs `iters` outer iterations of AUNTF::computeNTF (ntf/auntf.hpp:128-177)
- * with update `algo` (PLANC_GPU_MU / HALS / ANLSBPP). `dimtree` != 0 uses
- * the dimension tree (N in {3,4}; ddt.hpp:134-243), else the direct MTTKRP
- * (common/tensor.hpp:246-327). With `compute_error` != 0, errs_out[it]
- * receives the relative error after iteration it (auntf.hpp:165-170), in the
- * FP64 Gram form ||X||^2 - 2<X,M> + ||M||^2. errs_out may be NULL. */
+ * with update `algo` (PLANC_GPU_MU / HALS / ANLSBPP / AOADMM / NESTEROV).
+ * `dimtree` != 0 uses the dimension tree (N in {3,4}; ddt.hpp:134-243), else
+ * the direct MTTKRP (common/tensor.hpp:246-327). With `compute_error` != 0,
+ * errs_out[it] receives the relative error after iteration it
+ * (auntf.hpp:165-170), in the FP64 Gram form ||X||^2 - 2<X,M> + ||M||^2.
+ * errs_out may be NULL. NESTEROV evaluates the error every iteration in any
+ * case and, from iteration 6 of the call on, extrapolates the factors and
+ * keeps the extrapolation when it lowers the error (NTFNES::accelerate,
+ * ntf/ntfnes.hpp:64-98). AOADMM and NESTEROV keep per-mode state in the
+ * context between calls, as the reference's solver objects do
+ * (planc_gpu_reset_update_state clears it). */
 int planc_gpu_run(planc_gpu_ctx* ctx, int algo, int iters, int dimtree,
                   int compute_error, double* errs_out);
 
@@ -218,6 +227,13 @@ int planc_gpu_set_bpp_max_iter(planc_gpu_ctx* ctx, int max_iter);
  * any start: the factors are the same, only the number of exchange steps
  * drops. planc_gpu_bpp_solve always starts from the empty set. */
 int planc_gpu_set_bpp_warm_start(planc_gpu_ctx* ctx, int enable);
+
+/* Returns the AO-ADMM dual variables and the Nesterov proximal / previous
+ * iterates, lambdas and acceleration counters to their initial state (zeros,
+ * ones, acc_exp = 3), i.e. the state of a newly constructed NTFAOADMM / NTFNES
+ * object (ntf/ntfaoadmm.hpp:79-89, ntf/ntfnes.hpp:169-194). A new tensor shape
+ * or rank does the same. */
+int planc_gpu_reset_update_state(planc_gpu_ctx* ctx);
 
 /* Self-test of the kernels' bounded waits: launches one thread that waits on
  * a barrier nothing ever signals, with a limit of `seconds` (0 < s <= 5).

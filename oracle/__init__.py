@@ -23,7 +23,7 @@ import subprocess
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-ALGO = {"mu": 0, "hals": 1, "anlsbpp": 2}
+ALGO = {"mu": 0, "hals": 1, "anlsbpp": 2, "aoadmm": 4, "nesterov": 5}
 
 _lib = None
 _ref = None
@@ -76,6 +76,11 @@ def lib():
         L.orc_ntf_run.argtypes = [pd, pi64, i32, i32, ppd, pd, i32, i32, i32, i32, pd]
         L.orc_ntf_run.restype = i32
         L.orc_tensor_randu.argtypes = [i64, ctypes.c_uint, pd]
+        L.orc_admm_update.argtypes = [pd, pd, i64, i32, pd, pd, i32, d]
+        L.orc_admm_update.restype = i32
+        L.orc_nes_update.argtypes = [pd, pd, i64, i32, pd, pd, d, d, i32]
+        L.orc_nes_update.restype = i32
+        L.orc_sym_eig_minmax.argtypes = [pd, i32, pd, pd]
         _lib = L
     return _lib
 
@@ -212,6 +217,41 @@ def bpp_update(M, G):
     it = lib().orc_bpp_update(_pd(H), I, k, _pd(M), _pd(G),
                               mask.ctypes.data_as(ctypes.POINTER(ctypes.c_int)))
     return H, mask, it
+
+
+def admm_update(H, U, M, G, admm_iter=5, tol=0.01):
+    """One AO-ADMM mode update (ntf/ntfaoadmm.hpp:23-77). Returns
+    (H_new unnormalised, U_new column-normalised, iterations)."""
+    H = np.ascontiguousarray(H, dtype=np.float64).copy()
+    U = np.ascontiguousarray(U, dtype=np.float64).copy()
+    M = np.ascontiguousarray(M, dtype=np.float64)
+    G = np.ascontiguousarray(G, dtype=np.float64)
+    it = lib().orc_admm_update(_pd(H), _pd(U), H.shape[0], H.shape[1], _pd(M), _pd(G),
+                               int(admm_iter), float(tol))
+    if it < 0:
+        raise RuntimeError("chol() failed")
+    return H, U, it
+
+
+def nes_update(H0, M, G, delta1=1e-2, delta2=1e-2, max_inner=20000):
+    """One Nesterov mode update from the proximal point H0
+    (ntf/ntfnes.hpp:100-151). Returns (H_new unnormalised, inner steps)."""
+    H0 = np.ascontiguousarray(H0, dtype=np.float64)
+    M = np.ascontiguousarray(M, dtype=np.float64)
+    G = np.ascontiguousarray(G, dtype=np.float64)
+    H = np.zeros_like(H0)
+    it = lib().orc_nes_update(_pd(H0), _pd(H), H0.shape[0], H0.shape[1], _pd(M), _pd(G),
+                              float(delta1), float(delta2), int(max_inner))
+    if it < 0:
+        raise RuntimeError("inner step cap reached")
+    return H, it
+
+
+def sym_eig_minmax(G):
+    G = np.ascontiguousarray(G, dtype=np.float64)
+    lo, hi = ctypes.c_double(), ctypes.c_double()
+    lib().orc_sym_eig_minmax(_pd(G), G.shape[0], ctypes.byref(lo), ctypes.byref(hi))
+    return lo.value, hi.value
 
 
 def explicit_error(X, F, lam):

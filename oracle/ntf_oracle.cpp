@@ -40,6 +40,9 @@ void dposv_(const char* uplo, const int* n, const int* nrhs, double* a,
             const int* lda, double* b, const int* ldb, int* info);
 void dgesv_(const int* n, const int* nrhs, double* a, const int* lda,
             int* ipiv, double* b, const int* ldb, int* info);
+void dpotrf_(const char* uplo, const int* n, double* a, const int* lda, int* info);
+void dsyev_(const char* jobz, const char* uplo, const int* n, double* a,
+            const int* lda, double* w, double* work, const int* lwork, int* info);
 }
 
 namespace {
@@ -51,7 +54,7 @@ constexpr double kEps12 = 1e-12;                 // EPSILON_1EMINUS12
 // ntf/ntfanlsbpp.hpp:11
 constexpr int64_t kChunk = 2000;                 // ONE_THREAD_MATRIX_SIZE
 
-enum Algo { MU = 0, HALS = 1, ANLSBPP = 2 };  // common/utils.h:10
+enum Algo { MU = 0, HALS = 1, ANLSBPP = 2, AOADMM = 4, NESTEROV = 5 };  // common/utils.h:10
 
 int64_t prod(const int64_t* d, int a, int b) {
   int64_t p = 1;
@@ -469,6 +472,258 @@ double explicit_error(const double* X, const int64_t* dims, int N,
   return std::sqrt(err / normA);
 }
 
+
+// ---------------------------------------------------------------------------
+// AO-ADMM update, ntf/ntfaoadmm.hpp:23-77 (NTFAOADMM::update). H (in) is the
+// current normalised factor, (out) the new unnormalised one; U is the ADMM
+// auxiliary (dual) variable m_ncp_aux of this mode, I x k, kept between calls
+// and column-normalised after the loop (ntfaoadmm.hpp:74). All row-major
+// I x k, which is the memory of the reference's k x I transposed matrices.
+// Returns the number of ADMM iterations run, or -2 if chol() fails.
+int admm_update(double* H, double* U, int64_t I, int k, const double* M,
+                const double* G, int admm_iter, double tol) {
+  // alpha = trace(G) / k, 0.01 if not positive (ntfaoadmm.hpp:30-32)
+  double tr = 0.0;
+  for (int i = 0; i < k; ++i) tr += G[i * k + i];
+  double alpha = tr / k;
+  alpha = (alpha > 0) ? alpha : 0.01;
+  // L = chol(G + alpha I, "lower") (ntfaoadmm.hpp:33-35), LAPACK dpotrf
+  std::vector<double> A((size_t)k * k);
+  for (int e = 0; e < k * k; ++e) A[e] = G[e];
+  for (int i = 0; i < k; ++i) A[i * k + i] += alpha;
+  int n = k, info = 0;
+  dpotrf_("L", &n, A.data(), &n, &info);  // column-major lower = row-major upper
+  if (info != 0) return -2;
+  std::vector<double> L((size_t)k * k, 0.0);  // row-major lower: L[i*k+j], i >= j
+  for (int i = 0; i < k; ++i)
+    for (int j = 0; j <= i; ++j) L[i * k + j] = A[i + (size_t)j * k];
+  std::vector<double> prev((size_t)I * k), b(k);
+  bool stop = false;
+  int it = 0;
+  for (int i = 0; i < admm_iter && !stop; i++, it++) {
+    std::copy(H, H + (size_t)I * k, prev.begin());
+    double fac = 0.0, dual = 0.0, rr = 0.0, ss = 0.0;
+    for (int64_t row = 0; row < I; ++row) {
+      double* h = H + row * k;
+      double* u = U + row * k;
+      const double* m = M + row * k;
+      // rhs = M^T + alpha (H^T + U^T) (ntfaoadmm.hpp:44-47)
+      for (int c = 0; c < k; ++c) b[c] = m[c] + alpha * (h[c] + u[c]);
+      // solve(trimatl(L), .) then solve(trimatu(L^T), .): the column
+      // substitutions of BLAS dtrsm (Left, Lower / Upper, NoTrans)
+      for (int j = 0; j < k; ++j) {
+        b[j] = b[j] / L[j * k + j];
+        for (int c = j + 1; c < k; ++c) b[c] -= b[j] * L[c * k + j];
+      }
+      for (int j = k - 1; j >= 0; --j) {
+        b[j] = b[j] / L[j * k + j];
+        for (int c = 0; c < j; ++c) b[c] -= b[j] * L[j * k + c];
+      }
+      for (int c = 0; c < k; ++c) {
+        // H = max(aux_t^T - U, 0); U = U + H - aux_t^T (ntfaoadmm.hpp:52-61)
+        double hn = b[c] - u[c];
+        hn = hn > 0.0 ? hn : 0.0;
+        double un = (u[c] + hn) - b[c];
+        fac += hn * hn;
+        dual += un * un;
+        double d = hn - b[c];
+        rr += d * d;
+        double e = hn - prev[row * k + c];
+        ss += e * e;
+        h[c] = hn;
+        u[c] = un;
+      }
+    }
+    // stopping test (ntfaoadmm.hpp:63-71)
+    double facnorm = std::sqrt(fac), dualnorm = std::sqrt(dual);
+    double r = std::sqrt(rr), sres = std::sqrt(ss);
+    if (r < (tol * facnorm) && sres < (tol * dualnorm)) stop = true;
+  }
+  std::vector<double> lam(k);
+  normalize_mode(U, I, k, lam.data());  // m_ncp_aux.normalize(mode)
+  return it;
+}
+
+// ---------------------------------------------------------------------------
+// Nesterov-accelerated NTF, ntf/ntfnes.hpp:11-166 (NTFNES). Every NCPFactors
+// of the class is "trans" (k x I_n), i.e. row-major I_n x k here; their
+// lambdas are k-vectors. State of one solver object:
+struct NesState {
+  int N = 0, k = 0;
+  std::vector<std::vector<double>> prox, prev, acc;  // m_prox_t, m_prev_t, m_acc_t
+  std::vector<double> prox_lam, prev_lam, acc_lam;
+  // ntfnes.hpp:184-191
+  double delta1 = 1e-2, delta2 = 1e-2;
+  int acc_start = 5, acc_exp = 3, acc_fails = 0, fail_limit = 5;
+  int max_inner = 20000;  // the reference loops without a bound (ntfnes.hpp:121)
+};
+
+void nes_init(NesState& st, const int64_t* dims, int N, int k) {
+  st.N = N;
+  st.k = k;
+  st.prox.assign(N, {});
+  st.prev.assign(N, {});
+  st.acc.assign(N, {});
+  for (int n = 0; n < N; ++n) {
+    st.prox[n].assign((size_t)dims[n] * k, 0.0);  // zeros() (ntfnes.hpp:179-182)
+    st.prev[n].assign((size_t)dims[n] * k, 0.0);
+    st.acc[n].assign((size_t)dims[n] * k, 0.0);
+  }
+  st.prox_lam.assign(k, 1.0);  // NCPFactors ctor: lambda = ones
+  st.prev_lam.assign(k, 1.0);
+  st.acc_lam.assign(k, 1.0);
+}
+
+// NCPFactors::normalize_rows of a trans factor (ncpfactors.hpp:358-363):
+// rank component r is column r of the row-major I x k array.
+void normalize_rows_t(double* F, int64_t I, int k, double* lambda) {
+  normalize_mode(F, I, k, lambda);
+}
+
+// ntfnes.hpp:25-37
+double nes_get_lambda(double L, double mu) {
+  double q = L / mu;
+  double lambda = 0.0;
+  if (q > 1e6)
+    lambda = 10 * mu;
+  else if (q > 1e3)
+    lambda = mu;
+  else
+    lambda = mu / 10;
+  return lambda;
+}
+
+// ntfnes.hpp:39-50
+double nes_get_alpha(double alpha, double q) {
+  double a, b, c, D, x;
+  a = 1.0;
+  b = alpha * alpha - q;
+  c = -alpha * alpha;
+  D = b * b - 4 * a * c;
+  x = (-b + std::sqrt(D)) / 2;
+  return x;
+}
+
+// Extreme eigenvalues of a symmetric k x k matrix: arma::eig_sym (LAPACK
+// dsyev, eigenvalues only, ascending).
+void sym_eig_minmax(const double* G, int k, double* lmin, double* lmax) {
+  std::vector<double> A(G, G + (size_t)k * k), w(k);
+  int n = k, lwork = -1, info = 0;
+  double wq = 0.0;
+  dsyev_("N", "L", &n, A.data(), &n, w.data(), &wq, &lwork, &info);
+  lwork = (int)wq;
+  std::vector<double> work(lwork > 1 ? lwork : 1);
+  dsyev_("N", "L", &n, A.data(), &n, w.data(), work.data(), &lwork, &info);
+  *lmin = w[0];
+  *lmax = w[k - 1];
+}
+
+// NTFNES::update (ntfnes.hpp:100-151). Writes the unnormalised Ht to H.
+// Returns the number of inner gradient steps, or -1 at the step cap.
+int nes_update(NesState& st, int mode, double* H, int64_t I, const double* M,
+               const double* G) {
+  const int k = st.k;
+  const size_t n = (size_t)I * k;
+  if (mode == 0) st.prev_lam = st.prox_lam;
+  st.prev[mode] = st.prox[mode];
+  std::vector<double> Ht(st.prox[mode]), Htprev(Ht);
+  std::vector<double>& acc = st.acc[mode];
+  acc = Ht;
+  double L, mu;
+  sym_eig_minmax(G, k, &mu, &L);
+  double lambda = nes_get_lambda(L, mu);
+  std::vector<double> modG(G, G + (size_t)k * k);
+  for (int i = 0; i < k; ++i) modG[i * k + i] += lambda;
+  double q = (mu + lambda) / (L + lambda);
+  std::vector<double> modM(n), grad(n);
+  for (size_t e = 0; e < n; ++e) modM[e] = (-1 * lambda) * acc[e] - M[e];
+  double alpha = 1, alpha_prev = 1, beta = 1;
+  const double inv = 1 / (L + lambda);
+  int steps = 0;
+  while (true) {
+    // grad = modM + modG * acc
+    for (int64_t row = 0; row < I; ++row)
+      for (int c = 0; c < k; ++c) {
+        double s = 0.0;
+        for (int j = 0; j < k; ++j) s += modG[c * k + j] * acc[row * k + j];
+        grad[row * k + c] = modM[row * k + c] + s;
+      }
+    // stop_iter (ntfnes.hpp:52-62)
+    double absmax = 0.0, amin = grad.empty() ? 0.0 : grad[0];
+    for (size_t e = 0; e < n; ++e) {
+      absmax = std::max(absmax, std::fabs(grad[e] * acc[e]));
+      amin = std::min(amin, grad[e]);
+    }
+    if (absmax <= st.delta1 && amin >= -st.delta2) break;
+    if (steps >= st.max_inner) return -1;
+    ++steps;
+    Htprev = Ht;
+    for (size_t e = 0; e < n; ++e) {
+      double v = acc[e] - (inv * grad[e]);
+      Ht[e] = v > 0.0 ? v : 0.0;
+    }
+    alpha_prev = alpha;
+    alpha = nes_get_alpha(alpha_prev, q);
+    beta = (alpha_prev * (1 - alpha_prev)) / (alpha + alpha_prev * alpha_prev);
+    for (size_t e = 0; e < n; ++e) acc[e] = Ht[e] + beta * (Ht[e] - Htprev[e]);
+  }
+  st.prox[mode] = Ht;
+  normalize_rows_t(st.prox[mode].data(), I, k, st.prox_lam.data());
+  std::copy(Ht.begin(), Ht.end(), H);
+  return steps;
+}
+
+
+// NTFNES::accelerate (ntfnes.hpp:64-98), after the error of iteration `iter`
+// (cur_err). The extrapolated factors are installed and evaluated through
+// computeObjectiveError(m_acc_t) = reset(acc, true) + the explicit error
+// (auntf.hpp:186-198, 200-249); on failure reset(m_prox_t, true) restores the
+// proximal iterate.
+void nes_accelerate(NesState& st, int iter, double cur_err, const double* X,
+                    const int64_t* dims, int N, int k, double* const* F,
+                    double* lambda, double normA) {
+  if (iter <= st.acc_start) return;
+  double acc_step = std::pow(iter + 1, (1.0 / st.acc_exp));
+  for (int mode = 0; mode < N; mode++) {
+    const bool last = mode == N - 1;  // only the last mode is unnormalised
+    const size_t n = (size_t)dims[mode] * k;
+    std::vector<double>& acc = st.acc[mode];
+    for (size_t e = 0; e < n; ++e) {
+      const int r = (int)(e % k);
+      double cur = last ? lambda[r] * F[mode][e] : F[mode][e];
+      double prv = last ? st.prev_lam[r] * st.prev[mode][e] : st.prev[mode][e];
+      double a = cur - prv;
+      a *= acc_step;
+      a += cur;
+      acc[e] = a;
+    }
+    normalize_rows_t(acc.data(), dims[mode], k, st.acc_lam.data());
+  }
+  for (int i = 0; i < N; ++i) {
+    std::copy(st.acc[i].begin(), st.acc[i].end(), F[i]);
+    normalize_mode(F[i], dims[i], k, lambda);
+  }
+  std::copy(st.acc_lam.begin(), st.acc_lam.end(), lambda);
+  double acc_err = explicit_error(X, dims, N, F, lambda, k, normA);
+  if (acc_err < cur_err) {
+    for (int mode = 0; mode < N; mode++) {
+      st.prox[mode] = st.acc[mode];
+      normalize_rows_t(st.prox[mode].data(), dims[mode], k, st.prox_lam.data());
+    }
+  } else {
+    for (int i = 0; i < N; ++i) {
+      std::copy(st.prox[i].begin(), st.prox[i].end(), F[i]);
+      normalize_mode(F[i], dims[i], k, lambda);
+    }
+    std::copy(st.prox_lam.begin(), st.prox_lam.end(), lambda);
+    st.acc_fails++;
+    if (st.acc_fails > st.fail_limit) {
+      st.acc_fails = 0;
+      st.acc_exp++;
+    }
+  }
+}
+
 }  // namespace
 
 extern "C" {
@@ -581,6 +836,13 @@ int orc_ntf_run(const double* X, const int64_t* dims, int N, int k,
   for (int n = 0; n < N; ++n) maxI = std::max(maxI, dims[n]);
   std::vector<double> M((size_t)maxI * k);
   const double* const* Fc = F;
+  // solver-object state of NTFAOADMM (m_ncp_aux, zeros, ntfaoadmm.hpp:86) and
+  // NTFNES (ntfnes.hpp:173-191)
+  std::vector<std::vector<double>> aux;
+  if (algo == AOADMM)
+    for (int n = 0; n < N; ++n) aux.emplace_back((size_t)dims[n] * k, 0.0);
+  NesState nes;
+  if (algo == NESTEROV) nes_init(nes, dims, N, k);
   for (int it = 0; it < iters; ++it) {
     for (int n = 0; n < N; ++n) {
       gram_loo(Fc, dims, N, k, n, G.data());
@@ -595,15 +857,55 @@ int orc_ntf_run(const double* X, const int64_t* dims, int N, int k,
       } else if (algo == ANLSBPP) {
         int rc = bpp_update(F[n], dims[n], k, M.data(), G.data(), nullptr);
         if (rc < 0) return rc;
+      } else if (algo == AOADMM) {
+        int rc = admm_update(F[n], aux[n].data(), dims[n], k, M.data(), G.data(), 5, 0.01);
+        if (rc < 0) return rc;
+      } else if (algo == NESTEROV) {
+        int rc = nes_update(nes, n, F[n], dims[n], M.data(), G.data());
+        if (rc < 0) return -4;
       } else {
         return -3;
       }
       normalize_mode(F[n], dims[n], k, lambda);
     }
-    if (compute_error)
-      errs[it] = explicit_error(X, dims, N, Fc, lambda, k, normA);
+    // NTFNES switches the error on (accelerated(true), ntfnes.hpp:193) and
+    // its acceleration reads it
+    if (compute_error || algo == NESTEROV) {
+      double e = explicit_error(X, dims, N, Fc, lambda, k, normA);
+      if (compute_error) errs[it] = e;
+      if (algo == NESTEROV) nes_accelerate(nes, it, e, X, dims, N, k, F, lambda, normA);
+    }
   }
   return 0;
+}
+
+// One AO-ADMM mode update (NTFAOADMM::update, ntf/ntfaoadmm.hpp:23-77) with
+// the ADMM iteration count and tolerance as parameters (the reference fixes
+// 5 and 0.01, ntfaoadmm.hpp:87-88). H, U in/out. Returns iterations run.
+int orc_admm_update(double* H, double* U, int64_t I, int k, const double* M,
+                    const double* G, int admm_iter, double tol) {
+  return admm_update(H, U, I, k, M, G, admm_iter, tol);
+}
+
+// One Nesterov mode update from a given proximal point H0 (NTFNES::update,
+// ntf/ntfnes.hpp:100-151) with the stopping thresholds as parameters (the
+// reference uses delta1 = delta2 = 1e-2, ntfnes.hpp:184-185). Writes the
+// unnormalised update to H; returns the inner step count (-1 at the cap).
+int orc_nes_update(const double* H0, double* H, int64_t I, int k, const double* M,
+                   const double* G, double delta1, double delta2, int max_inner) {
+  NesState st;
+  int64_t dims[1] = {I};
+  nes_init(st, dims, 1, k);
+  std::copy(H0, H0 + (size_t)I * k, st.prox[0].begin());
+  st.delta1 = delta1;
+  st.delta2 = delta2;
+  st.max_inner = max_inner;
+  return nes_update(st, 0, H, I, M, G);
+}
+
+// Extreme eigenvalues of a symmetric k x k matrix (arma::eig_sym, LAPACK dsyev).
+void orc_sym_eig_minmax(const double* G, int k, double* lmin, double* lmax) {
+  sym_eig_minmax(G, k, lmin, lmax);
 }
 
 }  // extern "C"

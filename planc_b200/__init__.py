@@ -21,10 +21,10 @@ OK = 0
 ERR = {
     -1: "ERR_ARG", -2: "ERR_CUDA", -3: "ERR_STATE", -4: "ERR_BPP_MAXITER",
     -5: "ERR_NONFINITE", -6: "ERR_TIMEOUT", -7: "ERR_UNSUPPORTED", -8: "ERR_OOM",
-    -9: "ERR_SINGULAR",
+    -9: "ERR_SINGULAR", -10: "ERR_MAXITER",
 }
 PREC = {"fp64": 0, "bf16": 1, "bf16x2": 2}
-ALGO = {"mu": 0, "hals": 1, "anlsbpp": 2}
+ALGO = {"mu": 0, "hals": 1, "anlsbpp": 2, "aoadmm": 4, "nesterov": 5}
 F64, F32 = 0, 1
 KERNEL_CLASSES = ["contract", "ttv", "update", "normgram", "error", "reduce", "bpp", "prep",
                   "contract_left"]
@@ -38,7 +38,7 @@ EXPORTS = [
     "planc_gpu_bpp_solve", "planc_gpu_set_timing", "planc_gpu_get_kernel_times",
     "planc_gpu_launch_count", "planc_gpu_synth_cp_tensor", "planc_gpu_mttkrp_device",
     "planc_gpu_tensor_norm2", "planc_gpu_set_bpp_max_iter", "planc_gpu_set_bpp_warm_start",
-    "planc_gpu_selftest_wait_timeout",
+    "planc_gpu_reset_update_state", "planc_gpu_selftest_wait_timeout",
     "planc_gpu_batch_create", "planc_gpu_batch_add", "planc_gpu_batch_count",
     "planc_gpu_batch_set_factors", "planc_gpu_batch_run", "planc_gpu_batch_get_factors",
     "planc_gpu_batch_autotune", "planc_gpu_batch_destroy", "planc_gpu_mttkrp_last_mode_noalloc",
@@ -91,6 +91,7 @@ def load():
     L.planc_gpu_tensor_norm2.argtypes = [vp, pd]
     L.planc_gpu_set_bpp_max_iter.argtypes = [vp, i32]
     L.planc_gpu_set_bpp_warm_start.argtypes = [vp, i32]
+    L.planc_gpu_reset_update_state.argtypes = [vp]
     L.planc_gpu_batch_create.argtypes = [P(vp), i32, i32, i32]
     L.planc_gpu_batch_add.argtypes = [vp, vp, i32, pi64, i32, i32, P(pd), i32, P(i32)]
     L.planc_gpu_batch_count.argtypes = [vp]
@@ -262,6 +263,10 @@ class Context:
 
     def set_bpp_warm_start(self, on):
         _check(load().planc_gpu_set_bpp_warm_start(self.h, int(bool(on))))
+
+    def reset_update_state(self):
+        """Fresh AO-ADMM / Nesterov solver state (as a new solver object)."""
+        _check(load().planc_gpu_reset_update_state(self.h))
 
     def set_timing(self, on):
         _check(load().planc_gpu_set_timing(self.h, int(on)))

@@ -1,6 +1,7 @@
 """Build recipe of the native library: nvcc for sm_100a, in-tree output.
 
     python -m planc_b200.build          # builds planc_b200/libplanc_gpu.so
+                                        # and the dense_ntf driver (g++)
 """
 import os
 import shutil
@@ -11,6 +12,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 SRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libplanc_gpu.so")
+DRIVER = os.path.join(HERE, "dense_ntf")
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -42,6 +44,7 @@ def needs_build():
 
 def build(force=False, verbose=False):
     if not force and not needs_build():
+        build_driver()
         return LIB
     cmd = [nvcc()] + NVCC_FLAGS + ["-o", LIB + ".tmp", os.path.join(SRC, "planc_gpu.cu"), "-lcuda"]
     cmd[cmd.index("-lcuda"):] = ["-L/usr/local/cuda/lib64/stubs", "-lcuda"]
@@ -55,7 +58,26 @@ def build(force=False, verbose=False):
     if verbose:
         sys.stderr.write(res.stderr)
     os.replace(LIB + ".tmp", LIB)
+    build_driver()
     return LIB
+
+
+def driver_sources():
+    cpp = os.path.join(HERE, "cpp")
+    return [os.path.join(cpp, "ntf.cpp")] + [
+        os.path.join(cpp, "planc", f) for f in sorted(os.listdir(os.path.join(cpp, "planc")))]
+
+
+def build_driver(force=False):
+    """The dense_ntf command-line driver over the C++ API, linked to the library."""
+    if (not force and os.path.exists(DRIVER) and
+            all(os.path.getmtime(s) <= os.path.getmtime(DRIVER) for s in driver_sources() + [LIB])):
+        return DRIVER
+    cmd = ["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"),
+           "-I" + os.path.join(HERE, "cpp"), os.path.join(HERE, "cpp", "ntf.cpp"),
+           "-L" + HERE, "-lplanc_gpu", "-Wl,-rpath,$ORIGIN", "-o", DRIVER]
+    subprocess.run(cmd, check=True)
+    return DRIVER
 
 
 if __name__ == "__main__":

@@ -6,7 +6,8 @@
 //             [-i <file>] [--dimtree <0|1>] [--precision fp64|bf16|bf16x2]
 //             [--seed <n>] [--init <file prefix>] [-o <output prefix>]
 //
-// -a takes the reference's algotype integers (0 MU, 1 HALS, 2 ANLSBPP).
+// -a takes the reference's algotype integers (0 MU, 1 HALS, 2 ANLSBPP,
+// 4 AOADMM, 5 NESTEROV).
 // Without -i (or with an -i starting with "rand_") the tensor is
 // Tensor(dims): std::mt19937(103) uniform values, as in the reference.
 // --init reads initial factors written by -o (<prefix>_<n>.txt, I_n rows of k
@@ -23,8 +24,10 @@
 
 #include "planc/auntf.hpp"
 #include "planc/ntfanlsbpp.hpp"
+#include "planc/ntfaoadmm.hpp"
 #include "planc/ntfhals.hpp"
 #include "planc/ntfmu.hpp"
+#include "planc/ntfnes.hpp"
 #include "planc/tensor.hpp"
 
 namespace {
@@ -40,7 +43,8 @@ struct Opts {
 };
 
 void usage() {
-  std::cout << "usage: dense_ntf -a <0 MU|1 HALS|2 ANLSBPP> -d \"I0 I1 ...\" -k <rank> -t <iters>\n"
+  std::cout << "usage: dense_ntf -a <0 MU|1 HALS|2 ANLSBPP|4 AOADMM|5 NESTEROV> -d \"I0 I1 ...\"\n"
+               "                 -k <rank> -t <iters>\n"
                "                 -e <0|1> [-i <file>] [--dimtree <0|1>]\n"
                "                 [--precision fp64|bf16|bf16x2] [--init <prefix>] [-o <prefix>]\n";
 }
@@ -140,6 +144,8 @@ int main(int argc, char* argv[]) {
     case MU: return callNTF<planc::NTFMU>(o);
     case HALS: return callNTF<planc::NTFHALS>(o);
     case ANLSBPP: return callNTF<planc::NTFANLSBPP>(o);
+    case AOADMM: return callNTF<planc::NTFAOADMM>(o);
+    case NESTEROV: return callNTF<planc::NTFNES>(o);
     default:
       ERR << "Wrong algorithm choice. Quitting.." << o.algo << std::endl;
       return 1;

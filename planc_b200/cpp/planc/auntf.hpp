@@ -9,10 +9,13 @@
 // subclasses implement `MAT update(int mode)` and see m_ncp_factors,
 // ncp_mttkrp_t[mode] (k x I_mode) and gram_without_one (k x k).
 //
-// The built-in subclasses (NTFMU, NTFHALS, NTFANLSBPP) also report
-// device_algo(), which lets computeNTF run the whole iteration on the GPU
-// (one CUDA graph per iteration); any other subclass runs its update() on
-// the host between the device's Gram / MTTKRP and normalisation steps.
+// The built-in subclasses (NTFMU, NTFHALS, NTFANLSBPP, NTFAOADMM, NTFNES)
+// also report device_algo(), which lets computeNTF run the whole iteration on
+// the GPU (one CUDA graph per iteration; NTFNES's acceleration included); any
+// other subclass runs its update() on the host between the device's Gram /
+// MTTKRP and normalisation steps. With accelerated(true) on a built-in update
+// other than NTFNES, the device runs one iteration at a time and the host
+// calls accelerate() after each, as the reference's loop does.
 //
 // Differences from the reference, all documented behaviour of this build:
 //  * the relative error is computed in the FP64 Gram form
@@ -49,8 +52,8 @@ class AUNTF {
   MAT* ncp_mttkrp_t;
   MAT gram_without_one;
   virtual MAT update(const int mode) = 0;
-  // PLANC_GPU_MU / _HALS / _ANLSBPP when update() is one of the device
-  // updates; -1 runs update() on the host.
+  // PLANC_GPU_MU / _HALS / _ANLSBPP / _AOADMM / _NESTEROV when update() is
+  // one of the device updates; -1 runs update() on the host.
   virtual int device_algo() const { return -1; }
 
  private:
@@ -211,7 +214,7 @@ class AUNTF {
     upload_factors_if_needed();
     const int algo = device_algo();
     const bool want_err = m_compute_error || m_accelerated;
-    if (algo >= 0 && !m_accelerated) {
+    if (algo >= 0 && (!m_accelerated || algo == PLANC_GPU_NESTEROV)) {
       std::vector<double> errs(m_num_it > 0 ? m_num_it : 1, 0.0);
       check(planc_gpu_run(m_ctx, algo, m_num_it, m_enable_dim_tree ? 1 : 0, want_err ? 1 : 0,
                           errs.data()));
@@ -220,6 +223,16 @@ class AUNTF {
       if (want_err && m_num_it > 0) m_rel_error = errs[m_num_it - 1];
       for (auto&& s : m_stale_mttkrp) s = false;
       download_factors();
+      return;
+    }
+    if (algo >= 0) {  // built-in device update, host acceleration hook
+      for (m_current_it = 0; m_current_it < m_num_it; m_current_it++) {
+        check(planc_gpu_run(m_ctx, algo, 1, m_enable_dim_tree ? 1 : 0, 1, &m_rel_error));
+        print_iteration(m_current_it, true, m_rel_error);
+        for (auto&& s : m_stale_mttkrp) s = false;
+        download_factors();
+        accelerate();
+      }
       return;
     }
     const int N = m_input_tensor.modes();

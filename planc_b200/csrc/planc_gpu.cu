@@ -21,6 +21,7 @@
 #include "common.cuh"
 #include "kernels_f64.cuh"
 #include "tc_mttkrp.cuh"
+#include "updates_iter.cuh"
 
 using namespace pg;
 
@@ -109,8 +110,32 @@ struct planc_gpu_ctx {
   int* status_dev = nullptr;
   int64_t factor_cap[kMaxModes] = {0};
 
-  cudaGraphExec_t gexec = nullptr;
-  int g_algo = -1, g_dimtree = -1, g_err = -1;
+  // Per-mode state of the iterative updates, kept between runs like the
+  // members of the reference's solver objects; allocated zeroed on the first
+  // run of the algorithm (planc_gpu_reset_update_state zeroes it again).
+  //   AO-ADMM (NTFAOADMM, ntf/ntfaoadmm.hpp:13-21): the dual variable aux[n].
+  //   Nesterov (NTFNES, ntf/ntfnes.hpp:11-24): proximal and previous iterates
+  //   prox[n] / prev[n] and their lambdas, the acceleration counters (NesDev).
+  bool admm_ready = false, nes_ready = false;
+  double* aux[kMaxModes] = {nullptr};
+  double* admm_L = nullptr;     // k x k Cholesky factor of G + alpha I
+  double* admm_scal = nullptr;  // alpha
+  int* admm_flag = nullptr;     // [0] stop flag, [1] CTA counter
+  double* admm_part = nullptr;  // partial norms (ADMM_MAX_BLOCKS x 4) / column sums
+  size_t admm_part_elems = 0;
+  double* prox[kMaxModes] = {nullptr};
+  double* prev[kMaxModes] = {nullptr};
+  double* nes_acc = nullptr;    // maxI x k scratch of the inner loop
+  double* nes_grad = nullptr;
+  double* nes_modM = nullptr;
+  double* nes_lam = nullptr;    // [0,k) proximal, [k,2k) previous, [2k,3k) backup lambda
+  double* nes_gbak = nullptr;   // N x k x k backup Grams
+  NesDev* nes = nullptr;
+
+  // cached iteration graphs: [0] the plain iteration, [1] iteration +
+  // Nesterov acceleration
+  cudaGraphExec_t gexec[2] = {nullptr, nullptr};
+  int g_algo[2] = {-1, -1}, g_dimtree[2] = {-1, -1}, g_err[2] = {-1, -1};
 
   bool timing = false;
   bool capturing = false;
@@ -619,9 +644,69 @@ void run_update(planc_gpu_ctx* c, int algo, int n) {
 #undef CASE
       }
     });
+  } else if (algo == PLANC_GPU_AOADMM) {
+    // NTFAOADMM::update (ntf/ntfaoadmm.hpp:23-77): Cholesky of G + alpha I,
+    // at most admm_iter = 5 ADMM iterations (each launch returns at once once
+    // the stopping test has passed), then the dual variable is normalised.
+    launch(c, KC_UPDATE, [&] {
+      k_admm_prep<<<1, 256, 0, c->stream>>>(c->Gloo, k, c->admm_L, c->admm_scal, c->admm_flag,
+                                            c->admm_flag + 1, c->status_dev);
+    });
+    const unsigned nb =
+        (unsigned)std::min<int64_t>((I + ADMM_WARPS - 1) / ADMM_WARPS, ADMM_MAX_BLOCKS);
+    for (int it = 0; it < 5; ++it)
+      launch(c, KC_UPDATE, [&] {
+        if (k <= 32)
+          k_admm_step<32><<<nb, 32 * ADMM_WARPS, 0, c->stream>>>(
+              c->F[n], c->aux[n], c->M[n], c->admm_L, c->admm_scal, I, k, 0.01, c->admm_flag,
+              c->admm_part, c->admm_flag + 1);
+        else
+          k_admm_step<64><<<nb, 32 * ADMM_WARPS, 0, c->stream>>>(
+              c->F[n], c->aux[n], c->M[n], c->admm_L, c->admm_scal, I, k, 0.01, c->admm_flag,
+              c->admm_part, c->admm_flag + 1);
+      });
+    const unsigned nc = (unsigned)((I + CN_ROWS - 1) / CN_ROWS);
+    if ((size_t)nc * k > c->admm_part_elems)
+      fail(PLANC_GPU_ERR_STATE, "internal: column-norm partial buffer too small");
+    launch(c, KC_UPDATE, [&] {
+      k_colsumsq_partial<<<nc, 256, 0, c->stream>>>(c->aux[n], I, k, c->admm_part);
+    });
+    launch(c, KC_UPDATE, [&] {
+      k_colnorm_apply<<<nc, 256, 0, c->stream>>>(c->aux[n], I, k, c->admm_part, (int)nc);
+    });
+  } else if (algo == PLANC_GPU_NESTEROV) {
+    // NTFNES::update (ntf/ntfnes.hpp:100-151): eigenvalue bounds of G, then
+    // the accelerated proximal-gradient loop from the proximal point, in one
+    // cluster launch.
+    launch(c, KC_UPDATE, [&] {
+      k_nes_prep<<<1, 256, 0, c->stream>>>(c->Gloo, k, c->nes, n, c->nes_lam, c->nes_lam + k);
+    });
+    launch(c, KC_UPDATE, [&] {
+      if (k <= 32)
+        k_nes_inner<32><<<NES_CTAS, NES_THREADS, 0, c->stream>>>(
+            c->F[n], c->prox[n], c->prev[n], c->M[n], c->Gloo, c->nes, c->nes_acc, c->nes_grad,
+            c->nes_modM, I, k, NES_MAX_STEPS, c->status_dev);
+      else
+        k_nes_inner<64><<<NES_CTAS, NES_THREADS, 0, c->stream>>>(
+            c->F[n], c->prox[n], c->prev[n], c->M[n], c->Gloo, c->nes, c->nes_acc, c->nes_grad,
+            c->nes_modM, I, k, NES_MAX_STEPS, c->status_dev);
+    });
   } else {
     fail(PLANC_GPU_ERR_ARG, "unknown algorithm " + std::to_string(algo));
   }
+}
+
+unsigned elem_grid(int64_t n) { return (unsigned)std::min<int64_t>((n + 255) / 256, 1184); }
+
+// NTFNES bookkeeping after mode n's update and normalisation: m_prox_t[n] is
+// the normalised update, and after the last mode its lambda is the factor's
+// (normalize_rows, ntf/ntfnes.hpp:148-149).
+void nes_post(planc_gpu_ctx* c, int n) {
+  const int64_t ne = c->dims[n] * c->k;
+  launch(c, KC_UPDATE, [&] {
+    k_nes_post<<<elem_grid(ne), 256, 0, c->stream>>>(c->F[n], c->prox[n], ne, c->lambda,
+                                                     n == c->N - 1 ? c->nes_lam : nullptr, c->k);
+  });
 }
 
 void normalize_gram(planc_gpu_ctx* c, int n, int next, double* lambda) {
@@ -649,6 +734,19 @@ void gram_loo(planc_gpu_ctx* c, int n) {
   launch(c, KC_NORMGRAM, [&] { k_gram_loo<<<1, 1024, 0, c->stream>>>(c->Gall, c->N, c->k, n, c->Gloo); });
 }
 
+// MTTKRP of the last mode from the current factors (the <X, model> term of
+// the Gram-form error): through the tree from its second root (the state an
+// in-order sweep leaves), or directly.
+void last_mode_mttkrp(planc_gpu_ctx* c, bool dimtree) {
+  const int last = c->N - 1;
+  if (dimtree && (c->N == 3 || c->N == 4)) {
+    dimtree_prereq(c, last);
+    mttkrp_dimtree(c, last, c->M[last]);
+  } else {
+    mttkrp_direct(c, last, c->M[last]);
+  }
+}
+
 void error_kernel(planc_gpu_ctx* c) {
   const int last = c->N - 1;
   launch(c, KC_ERROR, [&] {
@@ -657,14 +755,58 @@ void error_kernel(planc_gpu_ctx* c) {
   });
 }
 
-// One AUNTF outer iteration (ntf/auntf.hpp:131-170).
-void one_iteration(planc_gpu_ctx* c, int algo, bool dimtree, bool err) {
+// NTFNES::accelerate (ntf/ntfnes.hpp:64-98) on the device, after the error
+// of the iteration: extrapolate every mode from the previous iterate,
+// normalise (the reference's reset(m_acc_t, true)), evaluate the error of the
+// extrapolated model, then keep it (prox := it) or return to the proximal
+// iterate (factors, Grams and lambda). The decision is made on the device.
+void nes_accelerate(planc_gpu_ctx* c, bool dimtree) {
+  const int N = c->N, k = c->k;
+  double* lam_bak = c->nes_lam + 2 * k;
+  launch(c, KC_UPDATE, [&] {
+    k_nes_acc_begin<<<1, 256, 0, c->stream>>>(c->counter_dev, c->errs_dev, c->nes, c->lambda,
+                                              lam_bak, c->Gall, c->nes_gbak, N * k * k, k);
+  });
+  for (int i = 0; i < N; ++i) {
+    const bool last = i == N - 1;
+    const int64_t ne = c->dims[i] * k;
+    launch(c, KC_UPDATE, [&] {
+      k_nes_extrap<<<elem_grid(ne), 256, 0, c->stream>>>(c->F[i], c->prev[i], ne, k,
+                                                         last ? lam_bak : nullptr,
+                                                         last ? c->nes_lam + k : nullptr, c->nes);
+    });
+    normalize_gram(c, i, (i + 1) % N, c->lambda);
+  }
+  last_mode_mttkrp(c, dimtree);
+  launch(c, KC_ERROR, [&] {
+    k_error<<<1, 1024, 0, c->stream>>>(c->M[N - 1], c->F[N - 1], c->dims[N - 1], c->lambda,
+                                      c->Gall, N, k, c->normX2, &c->nes->acc_err,
+                                      &c->nes->err_ctr);
+  });
+  launch(c, KC_UPDATE, [&] {
+    k_nes_decide<<<1, 256, 0, c->stream>>>(c->nes, c->lambda, c->nes_lam, c->Gall, c->nes_gbak,
+                                           N * k * k, c->Gall + (size_t)(N - 1) * k * k, k);
+  });
+  for (int i = 0; i < N; ++i) {
+    const int64_t ne = c->dims[i] * k;
+    launch(c, KC_UPDATE, [&] {
+      k_nes_commit<<<elem_grid(ne), 256, 0, c->stream>>>(c->F[i], c->prox[i], ne, c->nes);
+    });
+  }
+  gram_loo(c, 0);
+}
+
+// One AUNTF outer iteration (ntf/auntf.hpp:131-170); `accel` appends the
+// Nesterov acceleration step (auntf.hpp:171).
+void one_iteration(planc_gpu_ctx* c, int algo, bool dimtree, bool err, bool accel = false) {
   for (int n = 0; n < c->N; ++n) {
     mttkrp_any(c, n, dimtree, c->M[n]);
     run_update(c, algo, n);
     normalize_gram(c, n, (n + 1) % c->N, c->lambda);
+    if (algo == PLANC_GPU_NESTEROV) nes_post(c, n);
   }
   if (err) error_kernel(c);
+  if (accel) nes_accelerate(c, dimtree);
 }
 
 void require_ready(planc_gpu_ctx* c) {
@@ -683,21 +825,97 @@ void check_status(planc_gpu_ctx* c) {
                        : st == kStNonFinite ? "non-finite value in a BPP solve"
                        : st == kStSingular  ? "singular normal-equation matrix"
                        : st == kStTimeout   ? "bounded device wait timed out"
+                       : st == kStMaxIter   ? "an iterative update reached its step cap"
                                             : "device status error";
     fail(st, what);
   }
 }
 
 void reset_graph(planc_gpu_ctx* c) {
-  if (c->gexec) {
-    cudaGraphExecDestroy(c->gexec);
-    c->gexec = nullptr;
+  for (int v = 0; v < 2; ++v) {
+    if (c->gexec[v]) {
+      cudaGraphExecDestroy(c->gexec[v]);
+      c->gexec[v] = nullptr;
+    }
+    c->g_algo[v] = c->g_dimtree[v] = c->g_err[v] = -1;
   }
-  c->g_algo = c->g_dimtree = c->g_err = -1;
+}
+
+void free_update_state(planc_gpu_ctx* c) {
+  reset_graph(c);
+  auto f = [](auto*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+  };
+  for (int n = 0; n < kMaxModes; ++n) {
+    f(c->aux[n]);
+    f(c->prox[n]);
+    f(c->prev[n]);
+  }
+  f(c->admm_L);
+  f(c->admm_scal);
+  f(c->admm_flag);
+  f(c->admm_part);
+  c->admm_part_elems = 0;
+  f(c->nes_acc);
+  f(c->nes_grad);
+  f(c->nes_modM);
+  f(c->nes_lam);
+  f(c->nes_gbak);
+  f(c->nes);
+  c->admm_ready = c->nes_ready = false;
+}
+
+// Allocates (zeroed) the solver-object state of `algo` if it is not there:
+// the reference's constructors zero m_ncp_aux (ntfaoadmm.hpp:86) and
+// m_prox_t / m_prev_t / m_acc_t / m_grad_t (ntfnes.hpp:179-182), set the
+// NCPFactors lambdas to ones and acc_exp = 3, acc_fails = 0
+// (ntfnes.hpp:186-189). Called outside stream capture.
+void ensure_update_state(planc_gpu_ctx* c, int algo) {
+  const int k = c->k;
+  int64_t maxI = 1;
+  for (int n = 0; n < c->N; ++n) maxI = std::max(maxI, c->dims[n]);
+  if (algo == PLANC_GPU_AOADMM && !c->admm_ready) {
+    for (int n = 0; n < c->N; ++n) {
+      dalloc(&c->aux[n], (size_t)c->dims[n] * k);
+      CK(cudaMemsetAsync(c->aux[n], 0, (size_t)c->dims[n] * k * 8, c->stream));
+    }
+    dalloc(&c->admm_L, (size_t)k * k);
+    dalloc(&c->admm_scal, 4);
+    dalloc(&c->admm_flag, 2);
+    CK(cudaMemsetAsync(c->admm_flag, 0, 2 * sizeof(int), c->stream));
+    c->admm_part_elems =
+        std::max<size_t>((size_t)ADMM_MAX_BLOCKS * 4, (size_t)((maxI + CN_ROWS - 1) / CN_ROWS) * k);
+    dalloc(&c->admm_part, c->admm_part_elems);
+    c->admm_ready = true;
+    c->buf_epoch++;
+  }
+  if (algo == PLANC_GPU_NESTEROV && !c->nes_ready) {
+    for (int n = 0; n < c->N; ++n) {
+      dalloc(&c->prox[n], (size_t)c->dims[n] * k);
+      dalloc(&c->prev[n], (size_t)c->dims[n] * k);
+      CK(cudaMemsetAsync(c->prox[n], 0, (size_t)c->dims[n] * k * 8, c->stream));
+      CK(cudaMemsetAsync(c->prev[n], 0, (size_t)c->dims[n] * k * 8, c->stream));
+    }
+    dalloc(&c->nes_acc, (size_t)maxI * k);
+    dalloc(&c->nes_grad, (size_t)maxI * k);
+    dalloc(&c->nes_modM, (size_t)maxI * k);
+    dalloc(&c->nes_lam, (size_t)3 * k);
+    std::vector<double> ones((size_t)3 * k, 1.0);
+    CK(cudaMemcpyAsync(c->nes_lam, ones.data(), ones.size() * 8, cudaMemcpyHostToDevice, c->stream));
+    dalloc(&c->nes_gbak, (size_t)c->N * k * k);
+    dalloc(&c->nes, 1);
+    NesDev init{};
+    init.acc_exp = 3;
+    CK(cudaMemcpyAsync(c->nes, &init, sizeof(NesDev), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->nes_ready = true;
+    c->buf_epoch++;
+  }
 }
 
 void free_all(planc_gpu_ctx* c) {
-  reset_graph(c);
+  free_update_state(c);
   auto f = [](auto*& p) {
     if (p) cudaFree(p);
     p = nullptr;
@@ -827,6 +1045,7 @@ int planc_gpu_set_tensor(planc_gpu_ctx* c, const void* X, int dtype, const int64
     for (int i = 0; same && i < nmodes; ++i) same = c->dims[i] == dims[i];
     if (!same) {
       c->have_factors = false;
+      free_update_state(c);
       auto f = [](auto*& p) {
         if (p) cudaFree(p);
         p = nullptr;
@@ -919,6 +1138,7 @@ int planc_gpu_set_factors(planc_gpu_ctx* c, const double* const* F, const double
     set_device(c);
     reset_graph(c);
     if (k != c->k) {
+      free_update_state(c);
       auto f = [](auto*& p) {
         if (p) cudaFree(p);
         p = nullptr;
@@ -961,51 +1181,83 @@ int planc_gpu_set_factors(planc_gpu_ctx* c, const double* const* F, const double
   });
 }
 
+}  // extern "C"
+
+namespace {
+
+bool known_algo(int algo) {
+  return algo == PLANC_GPU_MU || algo == PLANC_GPU_HALS || algo == PLANC_GPU_ANLSBPP ||
+         algo == PLANC_GPU_AOADMM || algo == PLANC_GPU_NESTEROV;
+}
+
+// Captures (once) and returns the graph of one iteration; variant 1 appends
+// the Nesterov acceleration.
+cudaGraphExec_t iteration_graph(planc_gpu_ctx* c, int algo, bool dt, bool err, int variant) {
+  if (c->gexec[variant] && c->g_algo[variant] == algo && c->g_dimtree[variant] == (int)dt &&
+      c->g_err[variant] == (int)err)
+    return c->gexec[variant];
+  if (c->gexec[variant]) {
+    cudaGraphExecDestroy(c->gexec[variant]);
+    c->gexec[variant] = nullptr;
+  }
+  cudaGraph_t graph;
+  CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+  c->capturing = true;
+  try {
+    one_iteration(c, algo, dt, err, variant == 1);
+  } catch (...) {
+    c->capturing = false;
+    cudaStreamEndCapture(c->stream, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  c->capturing = false;
+  CK(cudaStreamEndCapture(c->stream, &graph));
+  cudaError_t e = cudaGraphInstantiate(&c->gexec[variant], graph, 0);
+  cudaGraphDestroy(graph);
+  cuda_check(e, "cudaGraphInstantiate");
+  c->g_algo[variant] = algo;
+  c->g_dimtree[variant] = (int)dt;
+  c->g_err[variant] = (int)err;
+  return c->gexec[variant];
+}
+
+}  // namespace
+
+extern "C" {
+
 int planc_gpu_run(planc_gpu_ctx* c, int algo, int iters, int dimtree, int compute_error,
                   double* errs_out) {
   return guarded([&] {
     require_ready(c);
     if (iters < 0) fail(PLANC_GPU_ERR_ARG, "iters < 0");
-    if (algo != PLANC_GPU_MU && algo != PLANC_GPU_HALS && algo != PLANC_GPU_ANLSBPP)
-      fail(PLANC_GPU_ERR_ARG, "unknown algorithm " + std::to_string(algo));
+    if (!known_algo(algo)) fail(PLANC_GPU_ERR_ARG, "unknown algorithm " + std::to_string(algo));
     bool dt = dimtree && (c->N == 3 || c->N == 4);
     if (c->precision != PLANC_GPU_PREC_FP64 && !dt)
       fail(PLANC_GPU_ERR_UNSUPPORTED, "tensor-core precisions run the dimension tree only");
     if (iters == 0) return;
     set_device(c);
     ensure_buffers(c);
-    ensure_errs(c, compute_error ? iters : 1);
+    // NTFNES evaluates the error every iteration (accelerated(true),
+    // ntf/ntfnes.hpp:193): its acceleration compares against it
+    const bool nes = algo == PLANC_GPU_NESTEROV;
+    const bool err = compute_error != 0 || nes;
+    ensure_errs(c, err ? iters : 1);
+    ensure_update_state(c, algo);
     if (c->g_epoch != c->buf_epoch) reset_graph(c);
     CK(cudaMemsetAsync(c->counter_dev, 0, sizeof(int), c->stream));
     gram_loo(c, 0);
     bool use_graph = !c->timing;
+    // AUNTF::computeNTF restarts its iteration count at 0 on every call and
+    // NTFNES accelerates from iteration acc_start + 1 = 6 on
+    // (ntf/auntf.hpp:129, ntf/ntfnes.hpp:65)
+    auto accel_at = [&](int it) { return nes && it > 5; };
     if (use_graph) {
-      if (!c->gexec || c->g_algo != algo || c->g_dimtree != (int)dt || c->g_err != compute_error) {
-        reset_graph(c);
-        cudaGraph_t graph;
-        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-        c->capturing = true;
-        try {
-          one_iteration(c, algo, dt, compute_error != 0);
-        } catch (...) {
-          c->capturing = false;
-          cudaStreamEndCapture(c->stream, &graph);
-          if (graph) cudaGraphDestroy(graph);
-          throw;
-        }
-        c->capturing = false;
-        CK(cudaStreamEndCapture(c->stream, &graph));
-        cudaError_t e = cudaGraphInstantiate(&c->gexec, graph, 0);
-        cudaGraphDestroy(graph);
-        cuda_check(e, "cudaGraphInstantiate");
-        c->g_algo = algo;
-        c->g_dimtree = (int)dt;
-        c->g_err = compute_error;
-        c->g_epoch = c->buf_epoch;
-      }
-      for (int it = 0; it < iters; ++it) CK(cudaGraphLaunch(c->gexec, c->stream));
+      for (int it = 0; it < iters; ++it)
+        CK(cudaGraphLaunch(iteration_graph(c, algo, dt, err, accel_at(it) ? 1 : 0), c->stream));
+      c->g_epoch = c->buf_epoch;
     } else {
-      for (int it = 0; it < iters; ++it) one_iteration(c, algo, dt, compute_error != 0);
+      for (int it = 0; it < iters; ++it) one_iteration(c, algo, dt, err, accel_at(it));
     }
     if (compute_error && errs_out)
       CK(cudaMemcpyAsync(errs_out, c->errs_dev, iters * sizeof(double), cudaMemcpyDeviceToHost,
@@ -1071,14 +1323,10 @@ int planc_gpu_objective_error(planc_gpu_ctx* c, double* err) {
     set_device(c);
     ensure_buffers(c);
     ensure_errs(c, 1);
-    const int last = c->N - 1;
-    // <X, model> needs the MTTKRP of the last mode from the current factors
-    if (c->precision == PLANC_GPU_PREC_FP64 || c->N == 3 || c->N == 4) {
-      if (c->precision == PLANC_GPU_PREC_FP64)
-        mttkrp_direct(c, last, c->M[last]);
-      else
-        partial_left(c, c->M[last]);
-    }
+    // <X, model> needs the MTTKRP of the last mode from the current factors:
+    // directly on the FP64 tensor, through the tree on the tensor-core copy
+    // (whose 4-way form is the balanced tree)
+    last_mode_mttkrp(c, c->precision != PLANC_GPU_PREC_FP64);
     CK(cudaMemsetAsync(c->counter_dev, 0, sizeof(int), c->stream));
     error_kernel(c);
     CK(cudaMemcpyAsync(err, c->errs_dev, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -1231,6 +1479,15 @@ int planc_gpu_set_bpp_warm_start(planc_gpu_ctx* c, int enable) {
       c->bpp_warm = enable != 0;
       reset_graph(c);  // captured graphs hold the launch arguments
     }
+  });
+}
+
+int planc_gpu_reset_update_state(planc_gpu_ctx* c) {
+  return guarded([&] {
+    if (!c) fail(PLANC_GPU_ERR_ARG, "null context");
+    set_device(c);
+    CK(cudaStreamSynchronize(c->stream));
+    free_update_state(c);
   });
 }
 
@@ -1503,6 +1760,8 @@ int planc_gpu_batch_run(planc_gpu_batch* b, int algo, int iters, int compute_err
   return guarded([&] {
     if (!b) fail(PLANC_GPU_ERR_ARG, "null batch");
     if (b->members.empty()) fail(PLANC_GPU_ERR_STATE, "empty batch");
+    if (algo == PLANC_GPU_AOADMM || algo == PLANC_GPU_NESTEROV)
+      fail(PLANC_GPU_ERR_UNSUPPORTED, "batched runs take MU, HALS or ANLS/BPP");
     if (algo != PLANC_GPU_MU && algo != PLANC_GPU_HALS && algo != PLANC_GPU_ANLSBPP)
       fail(PLANC_GPU_ERR_ARG, "unknown algorithm");
     if (iters <= 0) return;

@@ -1,0 +1,646 @@
+// updates_iter.cuh -- the iterative factor updates of the planc NTF solver
+// family on the device: AO-ADMM (reference ntf/ntfaoadmm.hpp:23-77) and the
+// Nesterov-accelerated proximal gradient with its outer extrapolation
+// (ntf/ntfnes.hpp:11-166).
+//
+// Both updates are row-separable: every row of the I_n x k factor solves its
+// own small problem with the shared k x k matrix (G + alpha I, or G + lambda I),
+// and the rows only meet in global stopping tests (Frobenius norms for ADMM,
+// max / min for Nesterov). A warp owns a row (lane c holds columns c and
+// c + 32), the k x k matrix sits in shared memory.
+//  * AO-ADMM runs its fixed maximum of 5 iterations as 5 launches; the last
+//    CTA of each launch sums the per-CTA partial norms in a fixed order and
+//    writes the stop flag that makes the remaining launches return at once.
+//  * The Nesterov inner loop has a data-dependent length, so it runs inside
+//    one thread-block cluster (8 CTAs): each step ends with a cluster barrier
+//    and the max / min of the stopping test are combined over distributed
+//    shared memory. Max and min are exact, so every CTA takes the same
+//    decision. No CTA spins on memory; the barrier is the hardware one.
+#pragma once
+#include <cooperative_groups.h>
+
+#include "common.cuh"
+
+namespace pg {
+
+namespace cg = cooperative_groups;
+
+constexpr int kStMaxIter = -10;  // an iterative update reached its step cap
+
+// ---------------------------------------------------------------------------
+// AO-ADMM
+// ---------------------------------------------------------------------------
+constexpr int ADMM_WARPS = 8;        // rows in flight per CTA
+constexpr int ADMM_MAX_BLOCKS = 296; // 2 CTAs per SM; partial-norm buffer size
+
+// alpha = trace(G) / k (0.01 if not positive) and L = chol(G + alpha I),
+// lower (ntfaoadmm.hpp:29-35); resets the stop flag and the CTA counter.
+// One CTA. A non-positive pivot (chol() failure in the reference) sets
+// kStSingular.
+__global__ void __launch_bounds__(256) k_admm_prep(const double* __restrict__ G, int k,
+                                                   double* __restrict__ Lg,
+                                                   double* __restrict__ scal, int* __restrict__ flag,
+                                                   int* __restrict__ counter, int* __restrict__ status) {
+  __shared__ double T[kMaxRank * (kMaxRank + 1)];
+  __shared__ double s_alpha;
+  __shared__ int s_bad;
+  constexpr int LD = kMaxRank + 1;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    double tr = 0.0;
+    for (int i = 0; i < k; ++i) tr += G[i * k + i];
+    double a = tr / k;
+    s_alpha = (a > 0) ? a : 0.01;
+    s_bad = 0;
+  }
+  __syncthreads();
+  for (int e = tid; e < k * k; e += blockDim.x) {
+    const int i = e / k, j = e % k;
+    T[i * LD + j] = G[e] + (i == j ? s_alpha : 0.0);
+  }
+  __syncthreads();
+  // left-looking (dot-product) Cholesky, column j after columns < j
+  for (int j = 0; j < k; ++j) {
+    if (tid == 0) {
+      double d = T[j * LD + j];
+      for (int p = 0; p < j; ++p) d -= T[j * LD + p] * T[j * LD + p];
+      if (!(d > 0.0)) s_bad = 1;
+      T[j * LD + j] = d > 0.0 ? sqrt(d) : 1.0;
+    }
+    __syncthreads();
+    const double ljj = T[j * LD + j];
+    for (int i = j + 1 + tid; i < k; i += blockDim.x) {
+      double v = T[i * LD + j];
+      for (int p = 0; p < j; ++p) v -= T[i * LD + p] * T[j * LD + p];
+      T[i * LD + j] = v / ljj;
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < k * k; e += blockDim.x) {
+    const int i = e / k, j = e % k;
+    Lg[e] = j <= i ? T[i * LD + j] : 0.0;
+  }
+  if (tid == 0) {
+    scal[0] = s_alpha;
+    *flag = 0;
+    *counter = 0;
+    if (s_bad) atomicCAS(status, 0, kStSingular);
+  }
+}
+
+// Selects register slot `p` of a lane's row slice with a compile-time index.
+template <int PER>
+__device__ __forceinline__ double slot_get(const double (&v)[PER], int p) {
+  double r = v[0];
+#pragma unroll
+  for (int q = 1; q < PER; ++q)
+    if (p == q) r = v[q];
+  return r;
+}
+
+// One ADMM iteration over all rows (ntfaoadmm.hpp:40-72):
+//   x   = (G + alpha I)^{-1} (m + alpha (h + u))  [two triangular solves]
+//   h'  = max(x - u, 0),  u' = (u + h') - x
+// plus the four squared norms of the stopping test. Returns at once when the
+// previous launch set the stop flag; the last CTA to finish combines the
+// per-CTA partials in CTA order and writes the flag for the next launch.
+template <int KP>
+__global__ void __launch_bounds__(32 * ADMM_WARPS) k_admm_step(
+    double* __restrict__ H, double* __restrict__ U, const double* __restrict__ M,
+    const double* __restrict__ Lg, const double* __restrict__ scal, int64_t I, int k, double tol,
+    int* __restrict__ flag, double* __restrict__ part, int* __restrict__ counter) {
+  if (*flag) return;  // written by the previous launch; uniform over the grid
+  constexpr int PER = KP / 32;
+  constexpr int LD = KP + 1;  // odd stride: row and column walks are conflict-free
+  __shared__ double Ls[KP * LD];
+  __shared__ double wred[ADMM_WARPS][4];
+  __shared__ int s_last;
+  for (int e = threadIdx.x; e < k * k; e += blockDim.x) Ls[(e / k) * LD + e % k] = Lg[e];
+  __syncthreads();
+  const double alpha = scal[0];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  double s_fac = 0.0, s_dual = 0.0, s_r = 0.0, s_s = 0.0;
+  for (int64_t row = (int64_t)blockIdx.x * ADMM_WARPS + warp; row < I;
+       row += (int64_t)gridDim.x * ADMM_WARPS) {
+    double h[PER], u[PER], y[PER];
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+      const int c = lane + 32 * p;
+      h[p] = c < k ? H[row * k + c] : 0.0;
+      u[p] = c < k ? U[row * k + c] : 0.0;
+      const double m = c < k ? M[row * k + c] : 0.0;
+      y[p] = m + alpha * (h[p] + u[p]);
+    }
+    // forward substitution with L (column-oriented, the order of dtrsm)
+    for (int j = 0; j < k; ++j) {
+      const double yj = __shfl_sync(0xffffffffu, slot_get<PER>(y, j >> 5), j & 31) / Ls[j * LD + j];
+#pragma unroll
+      for (int p = 0; p < PER; ++p) {
+        const int c = lane + 32 * p;
+        if (c == j)
+          y[p] = yj;
+        else if (c > j && c < k)
+          y[p] -= yj * Ls[c * LD + j];
+      }
+    }
+    // back substitution with L^T
+    for (int j = k - 1; j >= 0; --j) {
+      const double xj = __shfl_sync(0xffffffffu, slot_get<PER>(y, j >> 5), j & 31) / Ls[j * LD + j];
+#pragma unroll
+      for (int p = 0; p < PER; ++p) {
+        const int c = lane + 32 * p;
+        if (c == j)
+          y[p] = xj;
+        else if (c < j)
+          y[p] -= xj * Ls[j * LD + c];
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+      const int c = lane + 32 * p;
+      if (c < k) {
+        double hn = y[p] - u[p];
+        hn = hn > 0.0 ? hn : 0.0;
+        const double un = (u[p] + hn) - y[p];
+        s_fac = fma(hn, hn, s_fac);
+        s_dual = fma(un, un, s_dual);
+        const double d = hn - y[p];
+        s_r = fma(d, d, s_r);
+        const double e = hn - h[p];
+        s_s = fma(e, e, s_s);
+        H[row * k + c] = hn;
+        U[row * k + c] = un;
+      }
+    }
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    s_fac += __shfl_xor_sync(0xffffffffu, s_fac, o);
+    s_dual += __shfl_xor_sync(0xffffffffu, s_dual, o);
+    s_r += __shfl_xor_sync(0xffffffffu, s_r, o);
+    s_s += __shfl_xor_sync(0xffffffffu, s_s, o);
+  }
+  if (lane == 0) {
+    wred[warp][0] = s_fac;
+    wred[warp][1] = s_dual;
+    wred[warp][2] = s_r;
+    wred[warp][3] = s_s;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int w = 0; w < ADMM_WARPS; ++w)
+      for (int q = 0; q < 4; ++q) t[q] += wred[w][q];
+    for (int q = 0; q < 4; ++q) part[blockIdx.x * 4 + q] = t[q];
+    __threadfence();
+    s_last = atomicAdd(counter, 1) == (int)gridDim.x - 1;
+  }
+  __syncthreads();
+  if (s_last && threadIdx.x == 0) {
+    __threadfence();
+    double t[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int b = 0; b < (int)gridDim.x; ++b)
+      for (int q = 0; q < 4; ++q) t[q] += part[b * 4 + q];
+    const double facnorm = sqrt(t[0]), dualnorm = sqrt(t[1]);
+    const double r = sqrt(t[2]), s = sqrt(t[3]);
+    *flag = (r < tol * facnorm && s < tol * dualnorm) ? 1 : 0;
+    *counter = 0;
+  }
+}
+
+// Column 2-norms of an I x k row-major matrix in two launches (per-CTA
+// partial sums of squares, then every CTA sums the partials in CTA order and
+// scales its own rows): NCPFactors::normalize(int) (ncpfactors.hpp:346-351)
+// without keeping lambda.
+constexpr int CN_ROWS = 64;
+__global__ void __launch_bounds__(256) k_colsumsq_partial(const double* __restrict__ U, int64_t I,
+                                                          int k, double* __restrict__ part) {
+  __shared__ double red[256];
+  const int tid = threadIdx.x;
+  const int lanes = 256 / k;  // threads per column
+  const int c = tid % k, l = tid / k;
+  const int64_t row0 = (int64_t)blockIdx.x * CN_ROWS;
+  double s = 0.0;
+  if (l < lanes)
+    for (int64_t i = row0 + l; i < I && i < row0 + CN_ROWS; i += lanes) s = fma(U[i * k + c], U[i * k + c], s);
+  red[tid] = s;
+  __syncthreads();
+  if (tid < k) {
+    double t = 0.0;
+    for (int q = 0; q < lanes; ++q) t += red[q * k + tid];
+    part[(int64_t)blockIdx.x * k + tid] = t;
+  }
+}
+
+__global__ void __launch_bounds__(256) k_colnorm_apply(double* __restrict__ U, int64_t I, int k,
+                                                       const double* __restrict__ part, int nblk) {
+  __shared__ double nrm[kMaxRank];
+  if (threadIdx.x < k) {
+    double t = 0.0;
+    for (int b = 0; b < nblk; ++b) t += part[(int64_t)b * k + threadIdx.x];
+    nrm[threadIdx.x] = sqrt(t);
+  }
+  __syncthreads();
+  const int64_t row0 = (int64_t)blockIdx.x * CN_ROWS;
+  const int64_t rows = (I - row0) < CN_ROWS ? (I - row0) : CN_ROWS;
+  for (int64_t e = threadIdx.x; e < rows * k; e += blockDim.x) {
+    const double n = nrm[e % k];
+    if (n > 0) U[row0 * k + e] = U[row0 * k + e] / n;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Nesterov (NTFNES)
+// ---------------------------------------------------------------------------
+constexpr int NES_CTAS = 8;       // one portable cluster
+constexpr int NES_THREADS = 512;  // 16 warps per CTA, 128 rows in flight
+constexpr int NES_MAX_STEPS = 20000;
+
+// Device state of the Nesterov solver object beyond its factor-sized arrays.
+struct NesDev {
+  double L, mu, lambda, q, inv;  // of the current mode's update
+  double step;                   // acceleration step of this iteration
+  double cur_err, acc_err;       // error after the sweep / of the extrapolation
+  int acc_exp, acc_fails;        // ntfnes.hpp:186-189 (acc_exp starts at 3)
+  int accepted;                  // last acceleration kept
+  int err_ctr;                   // index slot for the error kernel
+  int steps;                     // inner steps of the last update
+};
+
+// ntfnes.hpp:25-37
+__device__ __forceinline__ double nes_lambda_of(double L, double mu) {
+  const double q = L / mu;
+  if (q > 1e6) return 10 * mu;
+  if (q > 1e3) return mu;
+  return mu / 10;
+}
+
+// ntfnes.hpp:39-50: root of x^2 + (alpha^2 - q) x - alpha^2 = 0
+__device__ __forceinline__ double nes_alpha_of(double alpha, double q) {
+  const double a = 1.0, b = alpha * alpha - q, c = -alpha * alpha;
+  const double D = b * b - 4 * a * c;
+  return (-b + sqrt(D)) / 2;
+}
+
+// Extreme eigenvalues of the symmetric G (arma::eig_sym, ntfnes.hpp:111-113)
+// by cyclic Jacobi rotations, k/2 disjoint rotations per round in the
+// round-robin order, until the off-diagonal mass is below 1e-32 of the total.
+// Then lambda, q and 1/(L + lambda) of the update (ntfnes.hpp:114-117). For
+// mode 0 it also copies the proximal lambda to the previous one
+// (ntfnes.hpp:102-104). One CTA of 256 threads.
+__global__ void __launch_bounds__(256) k_nes_prep(const double* __restrict__ G, int k,
+                                                  NesDev* __restrict__ st, int mode,
+                                                  const double* __restrict__ prox_lam,
+                                                  double* __restrict__ prev_lam) {
+  constexpr int LD = kMaxRank + 1;
+  __shared__ double A[kMaxRank * LD];
+  __shared__ double rc[kMaxRank / 2], rs[kMaxRank / 2];
+  __shared__ int rp[kMaxRank / 2], rq[kMaxRank / 2];
+  __shared__ double red[256];
+  __shared__ int s_done;
+  const int tid = threadIdx.x;
+  if (mode == 0 && tid < k) prev_lam[tid] = prox_lam[tid];
+  for (int e = tid; e < k * k; e += 256) A[(e / k) * LD + e % k] = G[e];
+  __syncthreads();
+  double tot = 0.0;
+  for (int e = tid; e < k * k; e += 256) {
+    const double v = A[(e / k) * LD + e % k];
+    tot = fma(v, v, tot);
+  }
+  red[tid] = tot;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (tid < s) red[tid] += red[tid + s];
+    __syncthreads();
+  }
+  const double total = red[0];
+  __syncthreads();
+  const int n2 = (k + 1) & ~1;  // even player count of the round-robin
+  const int np = n2 / 2;
+  for (int sweep = 0; sweep < 60; ++sweep) {
+    double off = 0.0;
+    for (int e = tid; e < k * k; e += 256) {
+      const int i = e / k, j = e % k;
+      if (i != j) off = fma(A[i * LD + j], A[i * LD + j], off);
+    }
+    red[tid] = off;
+    __syncthreads();
+    for (int s = 128; s > 0; s >>= 1) {
+      if (tid < s) red[tid] += red[tid + s];
+      __syncthreads();
+    }
+    if (tid == 0) s_done = !(red[0] > 1e-32 * total);
+    __syncthreads();
+    if (s_done) break;
+    for (int round = 0; round < n2 - 1; ++round) {
+      if (tid < np) {
+        // circle method: player 0 fixed, x_j = ((j + round) mod m) + 1 rotate;
+        // pairs (0, x_0) and (x_j, x_{m-j}) for 0 < j < np
+        const int m = n2 - 1;
+        const int a = tid == 0 ? 0 : ((tid + round) % m) + 1;
+        const int b = tid == 0 ? (round % m) + 1 : ((m - tid + round) % m) + 1;
+        const int p = a < b ? a : b, q = a < b ? b : a;
+        double c = 1.0, s = 0.0;
+        if (q < k) {
+          const double apq = A[p * LD + q];
+          if (apq != 0.0) {
+            const double theta = (A[q * LD + q] - A[p * LD + p]) / (2.0 * apq);
+            double t;
+            if (fabs(theta) > 1e150)
+              t = 0.5 / theta;
+            else
+              t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(1.0 + theta * theta));
+            c = 1.0 / sqrt(1.0 + t * t);
+            s = t * c;
+          }
+        }
+        rp[tid] = p;
+        rq[tid] = q;
+        rc[tid] = c;
+        rs[tid] = s;
+      }
+      __syncthreads();
+      // rows: A <- J^T A
+      for (int e = tid; e < np * k; e += 256) {
+        const int pr = e / k, j = e % k;
+        const int p = rp[pr], q = rq[pr];
+        const double s = rs[pr];
+        if (q < k && s != 0.0) {
+          const double c = rc[pr];
+          const double ap = A[p * LD + j], aq = A[q * LD + j];
+          A[p * LD + j] = c * ap - s * aq;
+          A[q * LD + j] = s * ap + c * aq;
+        }
+      }
+      __syncthreads();
+      // columns: A <- A J
+      for (int e = tid; e < np * k; e += 256) {
+        const int pr = e / k, j = e % k;
+        const int p = rp[pr], q = rq[pr];
+        const double s = rs[pr];
+        if (q < k && s != 0.0) {
+          const double c = rc[pr];
+          const double ap = A[j * LD + p], aq = A[j * LD + q];
+          A[j * LD + p] = c * ap - s * aq;
+          A[j * LD + q] = s * ap + c * aq;
+        }
+      }
+      __syncthreads();
+    }
+  }
+  if (tid == 0) {
+    double lo = A[0], hi = A[0];
+    for (int i = 1; i < k; ++i) {
+      const double d = A[i * LD + i];
+      lo = d < lo ? d : lo;
+      hi = d > hi ? d : hi;
+    }
+    const double lam = nes_lambda_of(hi, lo);
+    st->L = hi;
+    st->mu = lo;
+    st->lambda = lam;
+    st->q = (lo + lam) / (hi + lam);
+    st->inv = 1 / (hi + lam);
+  }
+}
+
+// NTFNES::update inner loop (ntfnes.hpp:100-151) for all rows of one mode,
+// in one cluster of NES_CTAS CTAs:
+//   prev = H0 = prox;  Ht = acc = H0;  modM = (-lambda) H0 - M
+//   loop: grad = modM + (G + lambda I) acc
+//         stop if max|grad .* acc| <= 1e-2 and min(grad) >= -1e-2
+//         Ht' = max(acc - grad / (L + lambda), 0)
+//         alpha, beta (ntfnes.hpp:143-145); acc = Ht' + beta (Ht' - Ht)
+// Ht is the mode's factor buffer (the update's output, unnormalised); acc,
+// grad and modM are I x k scratch arrays. A step cap (the reference loops
+// without one) sets kStMaxIter.
+template <int KP>
+__global__ void __cluster_dims__(NES_CTAS, 1, 1) __launch_bounds__(NES_THREADS, 1)
+    k_nes_inner(double* __restrict__ Ht, const double* __restrict__ prox, double* __restrict__ prev,
+                const double* __restrict__ M, const double* __restrict__ G, NesDev* __restrict__ st,
+                double* __restrict__ acc, double* __restrict__ grad, double* __restrict__ modM,
+                int64_t I, int k, int max_steps, int* __restrict__ status) {
+  constexpr int PER = KP / 32;
+  constexpr int NW = NES_THREADS / 32;
+  cg::cluster_group cluster = cg::this_cluster();
+  __shared__ double Gs[KP * KP];
+  __shared__ double wmax[NW], wmin[NW];
+  __shared__ double slot[2][2];
+  const double lam = st->lambda, q = st->q, inv = st->inv;
+  for (int e = threadIdx.x; e < k * k; e += NES_THREADS)
+    Gs[e] = G[e] + ((e / k) == (e % k) ? lam : 0.0);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t stride = (int64_t)gridDim.x * NW;
+  const int64_t row0 = (int64_t)blockIdx.x * NW + warp;
+  double vmax = 0.0, vmin = INFINITY;
+
+  // grad = modM + Gs acc for one row (acc in registers), with the row's
+  // contribution to the stopping test
+  auto row_grad = [&](int64_t row, const double (&a)[PER], const double (&mm)[PER]) {
+    double g[PER];
+#pragma unroll
+    for (int p = 0; p < PER; ++p) g[p] = 0.0;
+    for (int j = 0; j < k; ++j) {
+      const double aj = __shfl_sync(0xffffffffu, slot_get<PER>(a, j >> 5), j & 31);
+#pragma unroll
+      for (int p = 0; p < PER; ++p) {
+        const int c = lane + 32 * p;
+        if (c < k) g[p] = fma(aj, Gs[j * k + c], g[p]);
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+      const int c = lane + 32 * p;
+      if (c < k) {
+        const double gr = mm[p] + g[p];
+        grad[row * k + c] = gr;
+        vmax = fmax(vmax, fabs(gr * a[p]));
+        vmin = fmin(vmin, gr);
+      }
+    }
+  };
+
+  for (int64_t row = row0; row < I; row += stride) {
+    double a[PER], mm[PER];
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+      const int c = lane + 32 * p;
+      const double h0 = c < k ? prox[row * k + c] : 0.0;
+      a[p] = h0;
+      mm[p] = c < k ? (-1 * lam) * h0 - M[row * k + c] : 0.0;
+      if (c < k) {
+        prev[row * k + c] = h0;
+        Ht[row * k + c] = h0;
+        acc[row * k + c] = h0;
+        modM[row * k + c] = mm[p];
+      }
+    }
+    row_grad(row, a, mm);
+  }
+
+  double alpha = 1.0, beta = 1.0;
+  int t = 0;
+  for (;;) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+      vmin = fmin(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
+    }
+    if (lane == 0) {
+      wmax[warp] = vmax;
+      wmin[warp] = vmin;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double m = 0.0, n = INFINITY;
+      for (int w = 0; w < NW; ++w) {
+        m = fmax(m, wmax[w]);
+        n = fmin(n, wmin[w]);
+      }
+      slot[t & 1][0] = m;
+      slot[t & 1][1] = n;
+    }
+    cluster.sync();
+    double gmax = 0.0, gmin = INFINITY;
+    for (unsigned r = 0; r < cluster.num_blocks(); ++r) {
+      const double* rs = cluster.map_shared_rank(&slot[t & 1][0], r);
+      gmax = fmax(gmax, rs[0]);
+      gmin = fmin(gmin, rs[1]);
+    }
+    if (gmax <= 1e-2 && gmin >= -1e-2) break;  // stop_iter, ntfnes.hpp:52-62
+    if (t >= max_steps) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(status, 0, kStMaxIter);
+      break;
+    }
+    ++t;
+    const double alpha_prev = alpha;
+    alpha = nes_alpha_of(alpha_prev, q);
+    beta = (alpha_prev * (1 - alpha_prev)) / (alpha + alpha_prev * alpha_prev);
+    vmax = 0.0;
+    vmin = INFINITY;
+    for (int64_t row = row0; row < I; row += stride) {
+      double a[PER], mm[PER];
+#pragma unroll
+      for (int p = 0; p < PER; ++p) {
+        const int c = lane + 32 * p;
+        a[p] = 0.0;
+        mm[p] = 0.0;
+        if (c < k) {
+          const double hprev = Ht[row * k + c];
+          const double v = acc[row * k + c] - (inv * grad[row * k + c]);
+          const double hn = v > 0.0 ? v : 0.0;
+          a[p] = hn + beta * (hn - hprev);
+          mm[p] = modM[row * k + c];
+          Ht[row * k + c] = hn;
+          acc[row * k + c] = a[p];
+        }
+      }
+      row_grad(row, a, mm);
+    }
+  }
+  cluster.sync();  // no CTA leaves while another may still read its slots
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->steps = t;
+}
+
+// After the mode's normalisation: prox = the normalised factor, and for the
+// last mode the proximal lambda = the factor's lambda (normalize_rows of
+// m_prox_t, ntfnes.hpp:148-149).
+__global__ void __launch_bounds__(256) k_nes_post(const double* __restrict__ F,
+                                                  double* __restrict__ prox, int64_t n,
+                                                  const double* __restrict__ lambda,
+                                                  double* __restrict__ prox_lam, int k) {
+  for (int64_t e = (int64_t)blockIdx.x * 256 + threadIdx.x; e < n; e += (int64_t)gridDim.x * 256)
+    prox[e] = F[e];
+  if (prox_lam && blockIdx.x == 0 && threadIdx.x < k) prox_lam[threadIdx.x] = lambda[threadIdx.x];
+}
+
+// Start of NTFNES::accelerate (ntfnes.hpp:64-75) for the iteration whose
+// error was just written: acc_step = (iter + 1)^(1 / acc_exp); keeps the
+// current error, lambda and Grams (the state a failed extrapolation returns
+// to) and resets the error slot index of the extrapolation's error.
+__global__ void __launch_bounds__(256) k_nes_acc_begin(const int* __restrict__ counter,
+                                                       const double* __restrict__ errs,
+                                                       NesDev* __restrict__ st,
+                                                       const double* __restrict__ lambda,
+                                                       double* __restrict__ lam_bak,
+                                                       const double* __restrict__ Gall,
+                                                       double* __restrict__ gall_bak, int nG, int k) {
+  if (threadIdx.x == 0) {
+    const int iter = *counter - 1;
+    st->cur_err = errs[iter];
+    st->step = pow((double)(iter + 1), 1.0 / st->acc_exp);
+    st->err_ctr = 0;
+  }
+  if (threadIdx.x < k) lam_bak[threadIdx.x] = lambda[threadIdx.x];
+  for (int e = threadIdx.x; e < nG; e += 256) gall_bak[e] = Gall[e];
+}
+
+// Extrapolated factor of one mode (ntfnes.hpp:76-88), written over the
+// factor: a = cur + step (cur - prv), cur = diag(sc) F, prv = diag(sp) prev,
+// with sc / sp the current / previous lambda for the last mode (the only
+// unnormalised one) and the identity otherwise.
+__global__ void __launch_bounds__(256) k_nes_extrap(double* __restrict__ F,
+                                                    const double* __restrict__ prev, int64_t n, int k,
+                                                    const double* __restrict__ sc,
+                                                    const double* __restrict__ sp,
+                                                    const NesDev* __restrict__ st) {
+  const double step = st->step;
+  for (int64_t e = (int64_t)blockIdx.x * 256 + threadIdx.x; e < n; e += (int64_t)gridDim.x * 256) {
+    const int r = (int)(e % k);
+    const double cur = sc ? sc[r] * F[e] : F[e];
+    const double prv = sp ? sp[r] * prev[e] : prev[e];
+    double a = cur - prv;
+    a *= step;
+    a += cur;
+    F[e] = a;
+  }
+}
+
+// Acceptance test of the extrapolation (ntfnes.hpp:89-98). Rejected: the
+// Grams and lambda of the proximal iterate come back (its factors by
+// k_nes_commit), the failure count rises and every fail_limit + 1 failures
+// the step exponent grows. Accepted: the proximal lambda becomes the norms
+// of the (normalised) extrapolated last factor, sqrt(diag G_{N-1}).
+__global__ void __launch_bounds__(256) k_nes_decide(NesDev* __restrict__ st,
+                                                    double* __restrict__ lambda,
+                                                    double* __restrict__ prox_lam,
+                                                    double* __restrict__ Gall,
+                                                    const double* __restrict__ gall_bak, int nG,
+                                                    const double* __restrict__ Glast, int k) {
+  __shared__ int s_acc;
+  if (threadIdx.x == 0) s_acc = st->acc_err < st->cur_err;
+  __syncthreads();
+  const int accepted = s_acc;
+  if (accepted) {
+    if (threadIdx.x < k) prox_lam[threadIdx.x] = sqrt(Glast[threadIdx.x * k + threadIdx.x]);
+  } else {
+    if (threadIdx.x < k) lambda[threadIdx.x] = prox_lam[threadIdx.x];
+    for (int e = threadIdx.x; e < nG; e += 256) Gall[e] = gall_bak[e];
+  }
+  if (threadIdx.x == 0) {
+    st->accepted = accepted;
+    if (!accepted) {
+      st->acc_fails++;
+      if (st->acc_fails > 5) {  // fail_limit, ntfnes.hpp:190
+        st->acc_fails = 0;
+        st->acc_exp++;
+      }
+    }
+  }
+}
+
+// Factor side of the decision for one mode: accepted -> prox = F (the
+// extrapolated, normalised factor); rejected -> F = prox.
+__global__ void __launch_bounds__(256) k_nes_commit(double* __restrict__ F, double* __restrict__ prox,
+                                                    int64_t n, const NesDev* __restrict__ st) {
+  const int accepted = st->accepted;
+  for (int64_t e = (int64_t)blockIdx.x * 256 + threadIdx.x; e < n; e += (int64_t)gridDim.x * 256) {
+    if (accepted)
+      prox[e] = F[e];
+    else
+      F[e] = prox[e];
+  }
+}
+
+}  // namespace pg

@@ -31,11 +31,13 @@ def _read_factors(prefix, N):
     return [np.loadtxt("%s_%d.txt" % (prefix, n), ndmin=2) for n in range(N)]
 
 
-@pytest.mark.parametrize("algo,code", [("hals", 1), ("mu", 0), ("anlsbpp", 2)])
+@pytest.mark.parametrize("algo,code", [("hals", 1), ("mu", 0), ("anlsbpp", 2), ("aoadmm", 4),
+                                       ("nesterov", 5)])
 def test_dense_ntf_driver_matches_oracle(gpu, oracle_lib, tmp_path, algo, code):
     exe = str(tmp_path / "dense_ntf")
     _compile(os.path.join(PKG, "cpp", "ntf.cpp"), exe)
-    dims, k, iters = (24, 20, 16), 4, 6
+    # 8 iterations: the Nesterov acceleration runs from iteration 6 on
+    dims, k, iters = (24, 20, 16), 4, 8
     F0 = init_factors(dims, k, seed=60)
     init = str(tmp_path / "init")
     _write_init(init, F0)

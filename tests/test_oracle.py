@@ -131,3 +131,74 @@ def test_ntf_error_decreases_and_dimtree_equals_direct(oracle_lib):
         assert np.allclose(e, e2, rtol=1e-12, atol=0)
         for a, b in zip(F, F2):
             assert rel(a, b) < 1e-11
+
+
+# ---- AO-ADMM and Nesterov updates (ntf/ntfaoadmm.hpp, ntf/ntfnes.hpp) ----
+
+def _spd_problem(I, k, seed):
+    rng = np.random.default_rng(seed)
+    A = rng.random((3 * k, k))
+    G = A.T @ A
+    M = rng.random((I, k)) @ G  # right-hand sides with a mix of active and inactive bounds
+    M -= 0.4 * M.mean()
+    return np.ascontiguousarray(M), G
+
+
+def test_oracle_sym_eig_matches_numpy(oracle_lib):
+    _, G = _spd_problem(5, 12, 3)
+    lo, hi = oracle_lib.sym_eig_minmax(G)
+    w = np.linalg.eigvalsh(G)
+    assert abs(lo - w[0]) < 1e-12 * w[-1] and abs(hi - w[-1]) < 1e-12 * w[-1]
+
+
+def test_oracle_admm_reaches_nnls_optimum(oracle_lib):
+    # with the iteration cap and tolerance opened up, the ADMM of
+    # NTFAOADMM::update converges to the unique NNLS optimum that BPP finds
+    M, G = _spd_problem(40, 8, 4)
+    H0 = np.random.default_rng(5).random(M.shape)
+    H, U, it = oracle_lib.admm_update(H0, np.zeros_like(H0), M, G, admm_iter=5000, tol=1e-13)
+    ref, _, _ = oracle_lib.bpp_update(M, G)
+    assert rel(H, ref) < 1e-8, rel(H, ref)
+    # the dual variable leaves the call column-normalised (ntfaoadmm.hpp:74)
+    nrm = np.linalg.norm(U, axis=0)
+    assert np.allclose(nrm[nrm > 0], 1.0)
+
+
+def test_oracle_admm_reference_defaults_stop_within_five(oracle_lib):
+    M, G = _spd_problem(30, 6, 6)
+    H0 = np.random.default_rng(7).random(M.shape)
+    _, _, it = oracle_lib.admm_update(H0, np.zeros_like(H0), M, G)
+    assert 1 <= it <= 5
+
+
+def test_oracle_nes_reaches_proximal_nnls_optimum(oracle_lib):
+    # from H0 = 0 the Nesterov inner loop minimises
+    # 1/2 h^T (G + lambda I) h - m^T h over h >= 0 (ntfnes.hpp:113-145), whose
+    # optimum BPP computes with AtA = G + lambda I
+    M, G = _spd_problem(25, 6, 8)
+    H, steps = oracle_lib.nes_update(np.zeros_like(M), M, G, delta1=1e-13, delta2=1e-13)
+    w = np.linalg.eigvalsh(G)
+    L, mu = w[-1], w[0]
+    q = L / mu
+    lam = 10 * mu if q > 1e6 else (mu if q > 1e3 else mu / 10)
+    ref, _, _ = oracle_lib.bpp_update(M, G + lam * np.eye(G.shape[0]))
+    assert steps > 0
+    assert rel(H, ref) < 1e-6, rel(H, ref)
+
+
+@pytest.mark.parametrize("algo", ["aoadmm", "nesterov"])
+def test_oracle_ntf_run_new_algorithms_descend(oracle_lib, algo):
+    dims, k = (14, 12, 10), 4
+    X, _ = cp_tensor(dims, k, noise=0.01, seed=31)
+    F0 = init_factors(dims, k, seed=32)
+    F, lam, errs = oracle_lib.ntf_run(X, F0, algo, 15)
+    assert np.all(np.isfinite(errs))
+    assert errs[-1] < 0.7 * errs[0], errs
+    # lambda and the factors describe the model whose error is reported; the
+    # Nesterov acceleration that follows the last error keeps its extrapolated
+    # factors only if they lower it (ntfnes.hpp:80-96)
+    e = oracle_lib.explicit_error(X, F, lam)
+    if algo == "nesterov":
+        assert e < errs[-1] + 1e-12
+    else:
+        assert abs(e - errs[-1]) < 1e-12
