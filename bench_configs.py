@@ -15,6 +15,10 @@ the bench.py JSON contract (python bench.py --workload cfgN ...):
   cfg5  512^3 BF16 CP loss 1/2||X - [[A,B,C]]||^2 (rank 32, 5 % noise),
         torch.autograd with the MTTKRP kernels as backward, projected
         accelerated gradient steps on the factor leaves.
+  updates  the headline tensor (1024^3 FP32, rank-32 CP + 1 % noise) under
+        every update of the solver family -- MU, HALS, ANLS/BPP, AO-ADMM and
+        Nesterov (with its extrapolation step) -- 20 iterations each, BF16
+        tensor-core MTTKRP and the FP64 plain path, from the same start.
 
 A step is one outer iteration (cfg1, cfg3), one batched iteration of all
 256 tensors (cfg4) or one forward+backward+update (cfg5). Inputs are
@@ -43,6 +47,18 @@ def _sigma(A, rho):
     for a in A:
         G *= a.T @ a
     return rho * np.sqrt(G.sum() / float(np.prod([a.shape[0] for a in A])))
+
+
+def _launches_per_run(ctx, algo, steps, err=True):
+    """Kernel launches of one `steps`-iteration run, counted on an eager
+    (graphs off) pass; a graph replay launches the same kernels."""
+    ctx.set_timing(True)
+    n0 = ctx.launch_count()
+    ctx.run(algo, steps, compute_error=err)
+    n = ctx.launch_count() - n0
+    kt = ctx.kernel_times()
+    ctx.set_timing(False)
+    return n, kt
 
 
 def _time_run(torch, ctx, algo, steps, err=True):
@@ -79,8 +95,9 @@ def cfg1(args, gpu, torch, dev):
         c.set_factors(F0)
         c.run("hals", args.warmup)
         c.set_factors(F0)
-        ms, errs, launches = _time_run(torch, c, "hals", T)
+        ms, errs, _ = _time_run(torch, c, "hals", T)
         Fg, lg = c.get_factors()
+        launches, _ = _launches_per_run(c, "hals", T)
     t0 = time.perf_counter()
     Fo, lo, eo = oracle.ntf_run(X, F0, "hals", T)
     cpu_s = time.perf_counter() - t0
@@ -113,14 +130,12 @@ def cfg3(args, gpu, torch, dev):
             c.set_factors(F0)
             c.run("anlsbpp", max(args.warmup, 1), compute_error=False)
             c.set_factors(F0)
-            ms, errs, launches = _time_run(torch, c, "anlsbpp", T)  # one CUDA graph per iteration
-            # per-kernel breakdown from a separate run with event timing (no graphs)
+            ms, errs, _ = _time_run(torch, c, "anlsbpp", T)  # one CUDA graph per iteration
+            # per-kernel breakdown and launch count from a separate run with
+            # event timing (no graphs)
             c.set_factors(F0)
-            c.set_timing(True)
             c.kernel_times()
-            c.run("anlsbpp", T, compute_error=True)
-            kt = c.kernel_times()
-            c.set_timing(False)
+            launches, kt = _launches_per_run(c, "anlsbpp", T)
             out[prec] = (ms, errs, launches, kt)
     # headline: single BF16 (stochastically rounded tensor); the split-BF16
     # run is reported beside it
@@ -237,12 +252,54 @@ def cfg5(args, gpu, torch, dev):
                  x_passes_per_step=2)
 
 
+def updates(args, gpu, torch, dev):
+    from bench import workload
+    dims, k, T = (1024, 1024, 1024), 32, 20
+    A, sigma, F0 = workload(dims, k)
+    X = _synth(gpu, torch, dev, dims, A, sigma, 7)
+    algos = {}
+    for algo in ("mu", "hals", "anlsbpp", "aoadmm", "nesterov"):
+        row = {}
+        for prec in ("bf16", "fp64"):
+            with gpu.Context(dev, prec) as c:
+                c.set_tensor(X.data_ptr(), dims=dims, dtype="f32")
+                c.set_factors(F0)
+                c.run(algo, max(args.warmup, 1), compute_error=True)
+                c.reset_update_state()
+                c.set_factors(F0)
+                ms, errs, _ = _time_run(torch, c, algo, T)
+                r = {"iters_per_s": T / (ms * 1e-3), "ms_per_iter": ms / T,
+                     "final_rel_error": float(errs[-1])}
+                if prec == "bf16":
+                    c.reset_update_state()
+                    c.set_factors(F0)
+                    c.kernel_times()
+                    n, kt = _launches_per_run(c, algo, T)
+                    r["launches_per_iter"] = n / T
+                    r["kernel_ms_per_iter"] = {kk: round(v[0] / T, 4) for kk, v in kt.items()
+                                               if v[1]}
+                row[prec] = r
+        row["speedup_vs_fp64"] = row["fp64"]["ms_per_iter"] / row["bf16"]["ms_per_iter"]
+        row["final_error_abs_diff"] = abs(row["bf16"]["final_rel_error"] -
+                                          row["fp64"]["final_rel_error"])
+        algos[algo] = row
+    slowest = min(algos, key=lambda a: algos[a]["bf16"]["iters_per_s"])
+    v = algos[slowest]["bf16"]["iters_per_s"]
+    return _line(args, 1, v, "iters/s", 1e3 / v, "bf16",
+                 {"workload": "1024x1024x1024 FP32 tensor, rank-32 CP + 1% noise, 20 iterations "
+                              "of each update (MU, HALS, ANLS/BPP, AO-ADMM, Nesterov), dimension "
+                              "tree, BF16 tensor-core MTTKRP vs the FP64 plain path",
+                  "dims": list(dims), "rank": k},
+                 value_is="iters/s of the slowest update (%s), BF16" % slowest,
+                 algorithms=algos)
+
+
 def run(args, rank, world, local):
     import torch
     import planc_b200 as gpu
     dev = local
     torch.cuda.set_device(dev)
-    fn = {"cfg1": cfg1, "cfg3": cfg3, "cfg4": cfg4, "cfg5": cfg5}[args.workload]
+    fn = {"cfg1": cfg1, "cfg3": cfg3, "cfg4": cfg4, "cfg5": cfg5, "updates": updates}[args.workload]
     line = fn(args, gpu, torch, dev)
     if rank == 0:
         print(json.dumps(line))

@@ -131,6 +131,7 @@ struct planc_gpu_ctx {
   double* nes_lam = nullptr;    // [0,k) proximal, [k,2k) previous, [2k,3k) backup lambda
   double* nes_gbak = nullptr;   // N x k x k backup Grams
   NesDev* nes = nullptr;
+  int cl_ctas = NES_CTAS;       // CTAs of the register-resident update clusters
 
   // cached iteration graphs: [0] the plain iteration, [1] iteration +
   // Nesterov acceleration
@@ -224,6 +225,52 @@ void launch(planc_gpu_ctx* c, int cls, Fn&& fn) {
     if (c->pending.size() > (1u << 16)) drain_timing(c);
   }
   c->launch_count++;
+}
+
+// Launches `kern` as one thread-block cluster of `ncta` CTAs of NES_THREADS
+// threads (cluster sizes above 8 need the kernel's non-portable attribute,
+// set by enable_cluster16).
+template <typename... KArgs, typename... Args>
+void launch_cluster(void (*kern)(KArgs...), int ncta, cudaStream_t s, Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3((unsigned)ncta, 1, 1);
+  cfg.blockDim = dim3(NES_THREADS, 1, 1);
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = (unsigned)ncta;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  CK(cudaLaunchKernelEx(&cfg, kern, args...));
+}
+
+// Allows clusters of 16 for `kern` and reports whether one fits on the device.
+template <typename... KArgs>
+bool enable_cluster16(void (*kern)(KArgs...)) {
+  if (cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(NES_CTAS_MAX, 1, 1);
+  cfg.blockDim = dim3(NES_THREADS, 1, 1);
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeClusterDimension;
+  at[0].val.clusterDim.x = NES_CTAS_MAX;
+  at[0].val.clusterDim.y = 1;
+  at[0].val.clusterDim.z = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  int n = 0;
+  if (cudaOccupancyMaxActiveClusters(&n, (const void*)kern, &cfg) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return n >= 1;
 }
 
 WGen make_wgen(planc_gpu_ctx* c, const std::vector<int>& modes) {
@@ -645,9 +692,31 @@ void run_update(planc_gpu_ctx* c, int algo, int n) {
       }
     });
   } else if (algo == PLANC_GPU_AOADMM) {
+    if (!c->admm_ready) fail(PLANC_GPU_ERR_STATE, "internal: AO-ADMM state not allocated");
     // NTFAOADMM::update (ntf/ntfaoadmm.hpp:23-77): Cholesky of G + alpha I,
-    // at most admm_iter = 5 ADMM iterations (each launch returns at once once
-    // the stopping test has passed), then the dual variable is normalised.
+    // at most admm_iter = 5 ADMM iterations, then the dual variable is
+    // normalised. Up to 1024 rows (rank <= 32) or 512 rows (rank <= 64): one
+    // cluster launch with the rows in registers.
+    const int64_t warps = (int64_t)c->cl_ctas * (NES_THREADS / 32);
+    const int64_t rpw = (I + warps - 1) / warps;
+    if ((k <= 32 && rpw <= 8) || rpw <= 4) {
+      launch(c, KC_UPDATE, [&] {
+#define ADMM_CL(KP, R)                                                                       \
+  launch_cluster(k_admm_cluster<KP, R>, c->cl_ctas, c->stream, c->F[n], c->aux[n],           \
+                 (const double*)c->M[n], (const double*)c->Gloo, I, k, 0.01, c->status_dev)
+        if (k <= 32 && rpw <= 1) ADMM_CL(32, 1);
+        else if (k <= 32 && rpw <= 2) ADMM_CL(32, 2);
+        else if (k <= 32 && rpw <= 4) ADMM_CL(32, 4);
+        else if (k <= 32) ADMM_CL(32, 8);
+        else if (rpw <= 1) ADMM_CL(64, 1);
+        else if (rpw <= 2) ADMM_CL(64, 2);
+        else ADMM_CL(64, 4);
+#undef ADMM_CL
+      });
+      return;
+    }
+    // larger modes: one launch per ADMM iteration (each returns at once once
+    // the stopping test has passed)
     launch(c, KC_UPDATE, [&] {
       k_admm_prep<<<1, 256, 0, c->stream>>>(c->Gloo, k, c->admm_L, c->admm_scal, c->admm_flag,
                                             c->admm_flag + 1, c->status_dev);
@@ -675,14 +744,30 @@ void run_update(planc_gpu_ctx* c, int algo, int n) {
       k_colnorm_apply<<<nc, 256, 0, c->stream>>>(c->aux[n], I, k, c->admm_part, (int)nc);
     });
   } else if (algo == PLANC_GPU_NESTEROV) {
+    if (!c->nes_ready) fail(PLANC_GPU_ERR_STATE, "internal: Nesterov state not allocated");
     // NTFNES::update (ntf/ntfnes.hpp:100-151): eigenvalue bounds of G, then
     // the accelerated proximal-gradient loop from the proximal point, in one
     // cluster launch.
     launch(c, KC_UPDATE, [&] {
       k_nes_prep<<<1, 256, 0, c->stream>>>(c->Gloo, k, c->nes, n, c->nes_lam, c->nes_lam + k);
     });
+    // rows per warp of the cluster; up to 8 (rank <= 32) or 4 (rank <= 64)
+    // rows stay in registers, beyond that the state lives in global scratch
+    const int64_t warps = (int64_t)c->cl_ctas * (NES_THREADS / 32);
+    const int64_t rpw = (I + warps - 1) / warps;
     launch(c, KC_UPDATE, [&] {
-      if (k <= 32)
+#define NES_REG(KP, R)                                                                       \
+  launch_cluster(k_nes_inner_reg<KP, R>, c->cl_ctas, c->stream, c->F[n],                      \
+                 (const double*)c->prox[n], c->prev[n], (const double*)c->M[n],               \
+                 (const double*)c->Gloo, c->nes, I, k, (int)NES_MAX_STEPS, c->status_dev)
+      if (k <= 32 && rpw <= 1) NES_REG(32, 1);
+      else if (k <= 32 && rpw <= 2) NES_REG(32, 2);
+      else if (k <= 32 && rpw <= 4) NES_REG(32, 4);
+      else if (k <= 32 && rpw <= 8) NES_REG(32, 8);
+      else if (k > 32 && rpw <= 1) NES_REG(64, 1);
+      else if (k > 32 && rpw <= 2) NES_REG(64, 2);
+      else if (k > 32 && rpw <= 4) NES_REG(64, 4);
+      else if (k <= 32)
         k_nes_inner<32><<<NES_CTAS, NES_THREADS, 0, c->stream>>>(
             c->F[n], c->prox[n], c->prev[n], c->M[n], c->Gloo, c->nes, c->nes_acc, c->nes_grad,
             c->nes_modM, I, k, NES_MAX_STEPS, c->status_dev);
@@ -690,6 +775,7 @@ void run_update(planc_gpu_ctx* c, int algo, int n) {
         k_nes_inner<64><<<NES_CTAS, NES_THREADS, 0, c->stream>>>(
             c->F[n], c->prox[n], c->prev[n], c->M[n], c->Gloo, c->nes, c->nes_acc, c->nes_grad,
             c->nes_modM, I, k, NES_MAX_STEPS, c->status_dev);
+#undef NES_REG
     });
   } else {
     fail(PLANC_GPU_ERR_ARG, "unknown algorithm " + std::to_string(algo));
@@ -702,6 +788,7 @@ unsigned elem_grid(int64_t n) { return (unsigned)std::min<int64_t>((n + 255) / 2
 // the normalised update, and after the last mode its lambda is the factor's
 // (normalize_rows, ntf/ntfnes.hpp:148-149).
 void nes_post(planc_gpu_ctx* c, int n) {
+  if (!c->nes_ready) fail(PLANC_GPU_ERR_STATE, "internal: Nesterov state not allocated");
   const int64_t ne = c->dims[n] * c->k;
   launch(c, KC_UPDATE, [&] {
     k_nes_post<<<elem_grid(ne), 256, 0, c->stream>>>(c->F[n], c->prox[n], ne, c->lambda,
@@ -761,6 +848,7 @@ void error_kernel(planc_gpu_ctx* c) {
 // extrapolated model, then keep it (prox := it) or return to the proximal
 // iterate (factors, Grams and lambda). The decision is made on the device.
 void nes_accelerate(planc_gpu_ctx* c, bool dimtree) {
+  if (!c->nes_ready) fail(PLANC_GPU_ERR_STATE, "internal: Nesterov state not allocated");
   const int N = c->N, k = c->k;
   double* lam_bak = c->nes_lam + 2 * k;
   launch(c, KC_UPDATE, [&] {
@@ -872,6 +960,20 @@ void free_update_state(planc_gpu_ctx* c) {
 // NCPFactors lambdas to ones and acc_exp = 3, acc_fails = 0
 // (ntfnes.hpp:186-189). Called outside stream capture.
 void ensure_update_state(planc_gpu_ctx* c, int algo) {
+  if ((algo == PLANC_GPU_AOADMM || algo == PLANC_GPU_NESTEROV) && !c->admm_ready &&
+      !c->nes_ready) {
+    // clusters of 16 where every register-resident kernel accepts them
+    bool ok = true;
+    ok = ok && enable_cluster16(k_admm_cluster<32, 1>) && enable_cluster16(k_admm_cluster<32, 2>);
+    ok = ok && enable_cluster16(k_admm_cluster<32, 4>) && enable_cluster16(k_admm_cluster<32, 8>);
+    ok = ok && enable_cluster16(k_admm_cluster<64, 1>) && enable_cluster16(k_admm_cluster<64, 2>);
+    ok = ok && enable_cluster16(k_admm_cluster<64, 4>);
+    ok = ok && enable_cluster16(k_nes_inner_reg<32, 1>) && enable_cluster16(k_nes_inner_reg<32, 2>);
+    ok = ok && enable_cluster16(k_nes_inner_reg<32, 4>) && enable_cluster16(k_nes_inner_reg<32, 8>);
+    ok = ok && enable_cluster16(k_nes_inner_reg<64, 1>) && enable_cluster16(k_nes_inner_reg<64, 2>);
+    ok = ok && enable_cluster16(k_nes_inner_reg<64, 4>);
+    c->cl_ctas = ok ? NES_CTAS_MAX : NES_CTAS;
+  }
   const int k = c->k;
   int64_t maxI = 1;
   for (int n = 0; n < c->N; ++n) maxI = std::max(maxI, c->dims[n]);

@@ -12,10 +12,15 @@
 //    CTA of each launch sums the per-CTA partial norms in a fixed order and
 //    writes the stop flag that makes the remaining launches return at once.
 //  * The Nesterov inner loop has a data-dependent length, so it runs inside
-//    one thread-block cluster (8 CTAs): each step ends with a cluster barrier
-//    and the max / min of the stopping test are combined over distributed
-//    shared memory. Max and min are exact, so every CTA takes the same
-//    decision. No CTA spins on memory; the barrier is the hardware one.
+//    one thread-block cluster: each step ends with a cluster barrier, before
+//    which every CTA stores its partial max / min into the shared memory of
+//    every CTA of the cluster (distributed shared memory); after it each CTA
+//    combines the partials from its own shared memory. Max and min are exact,
+//    so every CTA takes the same decision. No CTA spins on memory; the
+//    barrier is the hardware one. A partial slot is double-buffered by step
+//    parity: a CTA can be at most one barrier ahead of another, so it never
+//    overwrites a slot another CTA has still to read, and no CTA stores into
+//    another after the last barrier, so CTAs may leave in any order.
 #pragma once
 #include <cooperative_groups.h>
 
@@ -26,6 +31,13 @@ namespace pg {
 namespace cg = cooperative_groups;
 
 constexpr int kStMaxIter = -10;  // an iterative update reached its step cap
+
+// Shape of the cluster launches: 16 warps per CTA; 8 CTAs (a portable
+// cluster) for the global-memory Nesterov loop, and 16 CTAs where the device
+// runs clusters of 16 (8 otherwise) for the register-resident kernels.
+constexpr int NES_CTAS = 8;
+constexpr int NES_CTAS_MAX = 16;
+constexpr int NES_THREADS = 512;
 
 // ---------------------------------------------------------------------------
 // AO-ADMM
@@ -113,9 +125,11 @@ __global__ void __launch_bounds__(32 * ADMM_WARPS) k_admm_step(
   constexpr int PER = KP / 32;
   constexpr int LD = KP + 1;  // odd stride: row and column walks are conflict-free
   __shared__ double Ls[KP * LD];
+  __shared__ double rinv[KP];
   __shared__ double wred[ADMM_WARPS][4];
   __shared__ int s_last;
   for (int e = threadIdx.x; e < k * k; e += blockDim.x) Ls[(e / k) * LD + e % k] = Lg[e];
+  if (threadIdx.x < k) rinv[threadIdx.x] = 1.0 / Lg[threadIdx.x * k + threadIdx.x];
   __syncthreads();
   const double alpha = scal[0];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -131,9 +145,10 @@ __global__ void __launch_bounds__(32 * ADMM_WARPS) k_admm_step(
       const double m = c < k ? M[row * k + c] : 0.0;
       y[p] = m + alpha * (h[p] + u[p]);
     }
-    // forward substitution with L (column-oriented, the order of dtrsm)
+    // forward substitution with L (column-oriented, the order of dtrsm; the
+    // diagonal enters as its reciprocal)
     for (int j = 0; j < k; ++j) {
-      const double yj = __shfl_sync(0xffffffffu, slot_get<PER>(y, j >> 5), j & 31) / Ls[j * LD + j];
+      const double yj = __shfl_sync(0xffffffffu, slot_get<PER>(y, j >> 5), j & 31) * rinv[j];
 #pragma unroll
       for (int p = 0; p < PER; ++p) {
         const int c = lane + 32 * p;
@@ -145,7 +160,7 @@ __global__ void __launch_bounds__(32 * ADMM_WARPS) k_admm_step(
     }
     // back substitution with L^T
     for (int j = k - 1; j >= 0; --j) {
-      const double xj = __shfl_sync(0xffffffffu, slot_get<PER>(y, j >> 5), j & 31) / Ls[j * LD + j];
+      const double xj = __shfl_sync(0xffffffffu, slot_get<PER>(y, j >> 5), j & 31) * rinv[j];
 #pragma unroll
       for (int p = 0; p < PER; ++p) {
         const int c = lane + 32 * p;
@@ -208,6 +223,211 @@ __global__ void __launch_bounds__(32 * ADMM_WARPS) k_admm_step(
   }
 }
 
+// The whole AO-ADMM update of one mode in one cluster of NES_CTAS CTAs, for
+// modes of at most R * 128 rows (every row's h, u and m in registers):
+// alpha and the Cholesky factor (each CTA computes the same one), at most 5
+// ADMM iterations whose stopping norms are summed per warp, per CTA (warp
+// order) and over the cluster (CTA order) -- the same sums in every CTA, so
+// every CTA takes the same decision -- then the column normalisation of the
+// dual variable with column sums formed the same way. Writes the new factor
+// (unnormalised) and the dual variable.
+template <int KP, int R>
+__global__ void __launch_bounds__(NES_THREADS, 1)
+    k_admm_cluster(double* __restrict__ H, double* __restrict__ U, const double* __restrict__ M,
+                   const double* __restrict__ G, int64_t I, int k, double tol,
+                   int* __restrict__ status) {
+  constexpr int PER = KP / 32;
+  constexpr int NW = NES_THREADS / 32;
+  constexpr int LD = KP + 1;
+  cg::cluster_group cluster = cg::this_cluster();
+  __shared__ double Ls[KP * LD];
+  __shared__ double wred[NW][4];
+  // per-CTA partials pushed into every CTA of the cluster (remote shared-
+  // memory stores before the cluster barrier), read back locally after it
+  __shared__ double slot[2][NES_CTAS_MAX][4];
+  static_assert((NW + NES_CTAS_MAX) * KP <= KP * LD, "column partials must fit in Ls");
+  __shared__ double rinv[KP];
+  __shared__ double s_alpha;
+  __shared__ int s_bad;
+  const int tid = threadIdx.x;
+  // alpha = trace(G) / k (0.01 if not positive), L = chol(G + alpha I)
+  // (ntfaoadmm.hpp:29-35), left-looking
+  if (tid == 0) {
+    double tr = 0.0;
+    for (int i = 0; i < k; ++i) tr += G[i * k + i];
+    const double a = tr / k;
+    s_alpha = (a > 0) ? a : 0.01;
+    s_bad = 0;
+  }
+  __syncthreads();
+  const double alpha = s_alpha;
+  for (int e = tid; e < k * k; e += NES_THREADS) {
+    const int i = e / k, j = e % k;
+    Ls[i * LD + j] = G[e] + (i == j ? alpha : 0.0);
+  }
+  __syncthreads();
+  for (int j = 0; j < k; ++j) {
+    if (tid == 0) {
+      double d = Ls[j * LD + j];
+      for (int p = 0; p < j; ++p) d -= Ls[j * LD + p] * Ls[j * LD + p];
+      if (!(d > 0.0)) s_bad = 1;
+      Ls[j * LD + j] = d > 0.0 ? sqrt(d) : 1.0;
+    }
+    __syncthreads();
+    const double ljj = Ls[j * LD + j];
+    for (int i = j + 1 + tid; i < k; i += NES_THREADS) {
+      double v = Ls[i * LD + j];
+      for (int p = 0; p < j; ++p) v -= Ls[i * LD + p] * Ls[j * LD + p];
+      Ls[i * LD + j] = v / ljj;
+    }
+    __syncthreads();
+  }
+  if (s_bad && blockIdx.x == 0 && tid == 0) atomicCAS(status, 0, kStSingular);
+  // reciprocal diagonal: the substitutions multiply by it (as OpenBLAS's
+  // triangular-solve kernels do) instead of dividing on the dependency chain
+  if (tid < k) rinv[tid] = 1.0 / Ls[tid * LD + tid];
+  __syncthreads();
+
+  const int lane = tid & 31, warp = tid >> 5;
+  const int64_t stride = (int64_t)gridDim.x * NW;
+  const int64_t row0 = (int64_t)blockIdx.x * NW + warp;
+  double h[R][PER], u[R][PER], m[R][PER];
+  bool live[R][PER];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int64_t row = row0 + r * stride;
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+      const int c = lane + 32 * p;
+      live[r][p] = row < I && c < k;
+      h[r][p] = live[r][p] ? H[row * k + c] : 0.0;
+      u[r][p] = live[r][p] ? U[row * k + c] : 0.0;
+      m[r][p] = live[r][p] ? M[row * k + c] : 0.0;
+    }
+  }
+  for (int it = 0; it < 5; ++it) {  // admm_iter, ntfaoadmm.hpp:87
+    double y[R][PER];
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int p = 0; p < PER; ++p) y[r][p] = m[r][p] + alpha * (h[r][p] + u[r][p]);
+    // forward substitution with L, then back substitution with L^T (the
+    // column orders of dtrsm), all held rows interleaved
+    for (int j = 0; j < k; ++j) {
+      const double d = rinv[j];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const double yj = __shfl_sync(0xffffffffu, slot_get<PER>(y[r], j >> 5), j & 31) * d;
+#pragma unroll
+        for (int p = 0; p < PER; ++p) {
+          const int c = lane + 32 * p;
+          if (c == j)
+            y[r][p] = yj;
+          else if (c > j && c < k)
+            y[r][p] -= yj * Ls[c * LD + j];
+        }
+      }
+    }
+    for (int j = k - 1; j >= 0; --j) {
+      const double d = rinv[j];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const double xj = __shfl_sync(0xffffffffu, slot_get<PER>(y[r], j >> 5), j & 31) * d;
+#pragma unroll
+        for (int p = 0; p < PER; ++p) {
+          const int c = lane + 32 * p;
+          if (c == j)
+            y[r][p] = xj;
+          else if (c < j)
+            y[r][p] -= xj * Ls[j * LD + c];
+        }
+      }
+    }
+    double s4[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int p = 0; p < PER; ++p)
+        if (live[r][p]) {
+          double hn = y[r][p] - u[r][p];
+          hn = hn > 0.0 ? hn : 0.0;
+          const double un = (u[r][p] + hn) - y[r][p];
+          s4[0] = fma(hn, hn, s4[0]);
+          s4[1] = fma(un, un, s4[1]);
+          const double dr = hn - y[r][p];
+          s4[2] = fma(dr, dr, s4[2]);
+          const double ds = hn - h[r][p];
+          s4[3] = fma(ds, ds, s4[3]);
+          h[r][p] = hn;
+          u[r][p] = un;
+        }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+      for (int qd = 0; qd < 4; ++qd) s4[qd] += __shfl_xor_sync(0xffffffffu, s4[qd], o);
+    if (lane == 0)
+#pragma unroll
+      for (int qd = 0; qd < 4; ++qd) wred[warp][qd] = s4[qd];
+    __syncthreads();
+    if (tid < (int)cluster.num_blocks()) {
+      double t4[4] = {0.0, 0.0, 0.0, 0.0};
+      for (int w = 0; w < NW; ++w)
+        for (int qd = 0; qd < 4; ++qd) t4[qd] += wred[w][qd];
+      double* dst = cluster.map_shared_rank(&slot[it & 1][cluster.block_rank()][0], tid);
+      for (int qd = 0; qd < 4; ++qd) dst[qd] = t4[qd];
+    }
+    cluster.sync();
+    double tot[4] = {0.0, 0.0, 0.0, 0.0};
+    for (unsigned b = 0; b < cluster.num_blocks(); ++b)
+      for (int qd = 0; qd < 4; ++qd) tot[qd] += slot[it & 1][b][qd];
+    const double facnorm = sqrt(tot[0]), dualnorm = sqrt(tot[1]);
+    const double rn = sqrt(tot[2]), sn = sqrt(tot[3]);
+    if (rn < tol * facnorm && sn < tol * dualnorm) break;  // ntfaoadmm.hpp:63-71
+  }
+  // dual variable column norms (m_ncp_aux.normalize(mode), ntfaoadmm.hpp:74).
+  // Ls is dead in every CTA once all have passed the loop's last cluster
+  // barrier, so its space holds the per-warp column sums and the per-CTA
+  // partials the other CTAs push.
+  double(*colw)[KP] = reinterpret_cast<double(*)[KP]>(Ls);
+  double(*colpart)[KP] = reinterpret_cast<double(*)[KP]>(Ls + NW * KP);
+#pragma unroll
+  for (int p = 0; p < PER; ++p) {
+    double cs = 0.0;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+      if (live[r][p]) cs = fma(u[r][p], u[r][p], cs);
+    colw[warp][lane + 32 * p] = cs;
+  }
+  __syncthreads();
+  if (tid < k) {
+    double t = 0.0;
+    for (int w = 0; w < NW; ++w) t += colw[w][tid];
+    for (unsigned b = 0; b < cluster.num_blocks(); ++b)
+      *cluster.map_shared_rank(&colpart[cluster.block_rank()][tid], b) = t;
+  }
+  cluster.sync();
+  double nrm[PER];
+#pragma unroll
+  for (int p = 0; p < PER; ++p) {
+    const int c = lane + 32 * p;
+    double t = 0.0;
+    if (c < k)
+      for (unsigned b = 0; b < cluster.num_blocks(); ++b) t += colpart[b][c];
+    nrm[p] = sqrt(t);
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int64_t row = row0 + r * stride;
+#pragma unroll
+    for (int p = 0; p < PER; ++p)
+      if (live[r][p]) {
+        const int c = lane + 32 * p;
+        H[row * k + c] = h[r][p];
+        U[row * k + c] = nrm[p] > 0 ? u[r][p] / nrm[p] : u[r][p];
+      }
+  }
+}
+
 // Column 2-norms of an I x k row-major matrix in two launches (per-CTA
 // partial sums of squares, then every CTA sums the partials in CTA order and
 // scales its own rows): NCPFactors::normalize(int) (ncpfactors.hpp:346-351)
@@ -252,8 +472,6 @@ __global__ void __launch_bounds__(256) k_colnorm_apply(double* __restrict__ U, i
 // ---------------------------------------------------------------------------
 // Nesterov (NTFNES)
 // ---------------------------------------------------------------------------
-constexpr int NES_CTAS = 8;       // one portable cluster
-constexpr int NES_THREADS = 512;  // 16 warps per CTA, 128 rows in flight
 constexpr int NES_MAX_STEPS = 20000;
 
 // Device state of the Nesterov solver object beyond its factor-sized arrays.
@@ -284,7 +502,8 @@ __device__ __forceinline__ double nes_alpha_of(double alpha, double q) {
 
 // Extreme eigenvalues of the symmetric G (arma::eig_sym, ntfnes.hpp:111-113)
 // by cyclic Jacobi rotations, k/2 disjoint rotations per round in the
-// round-robin order, until the off-diagonal mass is below 1e-32 of the total.
+// round-robin order, until a sweep finds every off-diagonal entry below the
+// rounding level of its two diagonal entries.
 // Then lambda, q and 1/(L + lambda) of the update (ntfnes.hpp:114-117). For
 // mode 0 it also copies the proximal lambda to the previous one
 // (ntfnes.hpp:102-104). One CTA of 256 threads.
@@ -296,42 +515,16 @@ __global__ void __launch_bounds__(256) k_nes_prep(const double* __restrict__ G, 
   __shared__ double A[kMaxRank * LD];
   __shared__ double rc[kMaxRank / 2], rs[kMaxRank / 2];
   __shared__ int rp[kMaxRank / 2], rq[kMaxRank / 2];
-  __shared__ double red[256];
-  __shared__ int s_done;
+  __shared__ int s_rot;
   const int tid = threadIdx.x;
   if (mode == 0 && tid < k) prev_lam[tid] = prox_lam[tid];
   for (int e = tid; e < k * k; e += 256) A[(e / k) * LD + e % k] = G[e];
   __syncthreads();
-  double tot = 0.0;
-  for (int e = tid; e < k * k; e += 256) {
-    const double v = A[(e / k) * LD + e % k];
-    tot = fma(v, v, tot);
-  }
-  red[tid] = tot;
-  __syncthreads();
-  for (int s = 128; s > 0; s >>= 1) {
-    if (tid < s) red[tid] += red[tid + s];
-    __syncthreads();
-  }
-  const double total = red[0];
-  __syncthreads();
   const int n2 = (k + 1) & ~1;  // even player count of the round-robin
   const int np = n2 / 2;
+  if (tid == 0) s_rot = 0;
+  __syncthreads();
   for (int sweep = 0; sweep < 60; ++sweep) {
-    double off = 0.0;
-    for (int e = tid; e < k * k; e += 256) {
-      const int i = e / k, j = e % k;
-      if (i != j) off = fma(A[i * LD + j], A[i * LD + j], off);
-    }
-    red[tid] = off;
-    __syncthreads();
-    for (int s = 128; s > 0; s >>= 1) {
-      if (tid < s) red[tid] += red[tid + s];
-      __syncthreads();
-    }
-    if (tid == 0) s_done = !(red[0] > 1e-32 * total);
-    __syncthreads();
-    if (s_done) break;
     for (int round = 0; round < n2 - 1; ++round) {
       if (tid < np) {
         // circle method: player 0 fixed, x_j = ((j + round) mod m) + 1 rotate;
@@ -343,8 +536,11 @@ __global__ void __launch_bounds__(256) k_nes_prep(const double* __restrict__ G, 
         double c = 1.0, s = 0.0;
         if (q < k) {
           const double apq = A[p * LD + q];
-          if (apq != 0.0) {
-            const double theta = (A[q * LD + q] - A[p * LD + p]) / (2.0 * apq);
+          const double app = A[p * LD + p], aqq = A[q * LD + q];
+          // a pair whose coupling is below the rounding level of its diagonal
+          // is converged (the classical threshold of cyclic Jacobi)
+          if (fabs(apq) > 1e-17 * sqrt(fabs(app * aqq)) && apq != 0.0) {
+            const double theta = (aqq - app) / (2.0 * apq);
             double t;
             if (fabs(theta) > 1e150)
               t = 0.5 / theta;
@@ -352,6 +548,7 @@ __global__ void __launch_bounds__(256) k_nes_prep(const double* __restrict__ G, 
               t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(1.0 + theta * theta));
             c = 1.0 / sqrt(1.0 + t * t);
             s = t * c;
+            s_rot = 1;
           }
         }
         rp[tid] = p;
@@ -387,6 +584,11 @@ __global__ void __launch_bounds__(256) k_nes_prep(const double* __restrict__ G, 
       }
       __syncthreads();
     }
+    const int rotated = s_rot;  // read by every thread before it is reset
+    __syncthreads();
+    if (!rotated) break;  // a sweep without a rotation: converged
+    if (tid == 0) s_rot = 0;
+    __syncthreads();
   }
   if (tid == 0) {
     double lo = A[0], hi = A[0];
@@ -425,7 +627,7 @@ __global__ void __cluster_dims__(NES_CTAS, 1, 1) __launch_bounds__(NES_THREADS, 
   cg::cluster_group cluster = cg::this_cluster();
   __shared__ double Gs[KP * KP];
   __shared__ double wmax[NW], wmin[NW];
-  __shared__ double slot[2][2];
+  __shared__ double slot[2][NES_CTAS_MAX][2];  // pushed by every CTA, read locally
   const double lam = st->lambda, q = st->q, inv = st->inv;
   for (int e = threadIdx.x; e < k * k; e += NES_THREADS)
     Gs[e] = G[e] + ((e / k) == (e % k) ? lam : 0.0);
@@ -492,21 +694,24 @@ __global__ void __cluster_dims__(NES_CTAS, 1, 1) __launch_bounds__(NES_THREADS, 
       wmin[warp] = vmin;
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      double m = 0.0, n = INFINITY;
-      for (int w = 0; w < NW; ++w) {
-        m = fmax(m, wmax[w]);
-        n = fmin(n, wmin[w]);
+    if (warp == 0) {  // CTA max / min over the warps, pushed to every CTA
+      double m = lane < NW ? wmax[lane] : 0.0, n = lane < NW ? wmin[lane] : INFINITY;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        n = fmin(n, __shfl_xor_sync(0xffffffffu, n, o));
       }
-      slot[t & 1][0] = m;
-      slot[t & 1][1] = n;
+      if (lane < (int)cluster.num_blocks()) {
+        double* dst = cluster.map_shared_rank(&slot[t & 1][cluster.block_rank()][0], lane);
+        dst[0] = m;
+        dst[1] = n;
+      }
     }
     cluster.sync();
     double gmax = 0.0, gmin = INFINITY;
     for (unsigned r = 0; r < cluster.num_blocks(); ++r) {
-      const double* rs = cluster.map_shared_rank(&slot[t & 1][0], r);
-      gmax = fmax(gmax, rs[0]);
-      gmin = fmin(gmin, rs[1]);
+      gmax = fmax(gmax, slot[t & 1][r][0]);
+      gmin = fmin(gmin, slot[t & 1][r][1]);
     }
     if (gmax <= 1e-2 && gmin >= -1e-2) break;  // stop_iter, ntfnes.hpp:52-62
     if (t >= max_steps) {
@@ -539,7 +744,147 @@ __global__ void __cluster_dims__(NES_CTAS, 1, 1) __launch_bounds__(NES_THREADS, 
       row_grad(row, a, mm);
     }
   }
-  cluster.sync();  // no CTA leaves while another may still read its slots
+  if (blockIdx.x == 0 && threadIdx.x == 0) st->steps = t;
+}
+
+// The same loop with every row's state in registers: each warp holds up to
+// R rows (row0 + r * 128); no global traffic inside the loop, and the R
+// matrix-vector products of a step are interleaved. Used when the mode has at
+// most R * 128 rows.
+template <int KP, int R>
+__global__ void __launch_bounds__(NES_THREADS, 1)
+    k_nes_inner_reg(double* __restrict__ Ht_out, const double* __restrict__ prox,
+                    double* __restrict__ prev, const double* __restrict__ M,
+                    const double* __restrict__ G, NesDev* __restrict__ st, int64_t I, int k,
+                    int max_steps, int* __restrict__ status) {
+  constexpr int PER = KP / 32;
+  constexpr int NW = NES_THREADS / 32;
+  cg::cluster_group cluster = cg::this_cluster();
+  __shared__ double Gs[KP * KP];
+  __shared__ double wmax[NW], wmin[NW];
+  __shared__ double slot[2][NES_CTAS_MAX][2];  // pushed by every CTA, read locally
+  const double lam = st->lambda, q = st->q, inv = st->inv;
+  for (int e = threadIdx.x; e < k * k; e += NES_THREADS)
+    Gs[e] = G[e] + ((e / k) == (e % k) ? lam : 0.0);
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int64_t stride = (int64_t)gridDim.x * NW;
+  const int64_t row0 = (int64_t)blockIdx.x * NW + warp;
+  double ht[R][PER], acc[R][PER], gr[R][PER], mm[R][PER];
+  bool live[R][PER];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int64_t row = row0 + r * stride;
+#pragma unroll
+    for (int p = 0; p < PER; ++p) {
+      const int c = lane + 32 * p;
+      live[r][p] = row < I && c < k;
+      const double h0 = live[r][p] ? prox[row * k + c] : 0.0;
+      ht[r][p] = h0;
+      acc[r][p] = h0;
+      mm[r][p] = live[r][p] ? (-1 * lam) * h0 - M[row * k + c] : 0.0;
+      if (live[r][p]) prev[row * k + c] = h0;
+    }
+  }
+  double vmax, vmin;
+  // grad = modM + (G + lambda I) acc for every held row, and the stopping
+  // test's max |grad .* acc| and min grad over them
+  auto all_grads = [&]() {
+    double g[R][PER];
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int p = 0; p < PER; ++p) g[r][p] = 0.0;
+    for (int j = 0; j < k; ++j) {
+      double gv[PER];
+#pragma unroll
+      for (int p = 0; p < PER; ++p) {
+        const int c = lane + 32 * p;
+        gv[p] = c < k ? Gs[j * k + c] : 0.0;
+      }
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const double aj = __shfl_sync(0xffffffffu, slot_get<PER>(acc[r], j >> 5), j & 31);
+#pragma unroll
+        for (int p = 0; p < PER; ++p) g[r][p] = fma(aj, gv[p], g[r][p]);
+      }
+    }
+    vmax = 0.0;
+    vmin = INFINITY;
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int p = 0; p < PER; ++p) {
+        gr[r][p] = mm[r][p] + g[r][p];
+        if (live[r][p]) {
+          vmax = fmax(vmax, fabs(gr[r][p] * acc[r][p]));
+          vmin = fmin(vmin, gr[r][p]);
+        }
+      }
+  };
+  all_grads();
+
+  double alpha = 1.0, beta = 1.0;
+  int t = 0;
+  for (;;) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      vmax = fmax(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+      vmin = fmin(vmin, __shfl_xor_sync(0xffffffffu, vmin, o));
+    }
+    if (lane == 0) {
+      wmax[warp] = vmax;
+      wmin[warp] = vmin;
+    }
+    __syncthreads();
+    if (warp == 0) {  // CTA max / min over the warps, pushed to every CTA
+      double m = lane < NW ? wmax[lane] : 0.0, n = lane < NW ? wmin[lane] : INFINITY;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+        n = fmin(n, __shfl_xor_sync(0xffffffffu, n, o));
+      }
+      if (lane < (int)cluster.num_blocks()) {
+        double* dst = cluster.map_shared_rank(&slot[t & 1][cluster.block_rank()][0], lane);
+        dst[0] = m;
+        dst[1] = n;
+      }
+    }
+    cluster.sync();
+    double gmax = 0.0, gmin = INFINITY;
+    for (unsigned r = 0; r < cluster.num_blocks(); ++r) {
+      gmax = fmax(gmax, slot[t & 1][r][0]);
+      gmin = fmin(gmin, slot[t & 1][r][1]);
+    }
+    if (gmax <= 1e-2 && gmin >= -1e-2) break;  // stop_iter, ntfnes.hpp:52-62
+    if (t >= max_steps) {
+      if (blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(status, 0, kStMaxIter);
+      break;
+    }
+    ++t;
+    const double alpha_prev = alpha;
+    alpha = nes_alpha_of(alpha_prev, q);
+    beta = (alpha_prev * (1 - alpha_prev)) / (alpha + alpha_prev * alpha_prev);
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int p = 0; p < PER; ++p)
+        if (live[r][p]) {
+          const double hprev = ht[r][p];
+          const double v = acc[r][p] - (inv * gr[r][p]);
+          const double hn = v > 0.0 ? v : 0.0;
+          acc[r][p] = hn + beta * (hn - hprev);
+          ht[r][p] = hn;
+        }
+    all_grads();
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int64_t row = row0 + r * stride;
+#pragma unroll
+    for (int p = 0; p < PER; ++p)
+      if (live[r][p]) Ht_out[row * k + lane + 32 * p] = ht[r][p];
+  }
   if (blockIdx.x == 0 && threadIdx.x == 0) st->steps = t;
 }
 

@@ -37,8 +37,13 @@ def _run(gpu, X, F0, algo, iters, prec="fp64", dimtree=True):
 
 
 @pytest.mark.parametrize("algo", ["aoadmm", "nesterov"])
+# the cases cover the row-per-warp forms of the cluster kernels (1, 4 and 8
+# rows at rank <= 32; 1 and 4 at rank <= 64) and their global-memory forms
+# beyond them (1100 rows)
 @pytest.mark.parametrize("dims,k,rank", [((20, 18, 16), 5, 5), ((300, 40, 33), 8, 6),
-                                         ((9, 8, 7, 10), 4, 4), ((50, 45, 40), 40, 40)])
+                                         ((9, 8, 7, 10), 4, 4), ((50, 45, 40), 40, 40),
+                                         ((800, 12, 10), 6, 6), ((1100, 12, 10), 6, 6),
+                                         ((260, 48, 44), 40, 40)])
 def test_iterative_update_matches_oracle(gpu, oracle_lib, algo, dims, k, rank):
     iters = 20
     X, _ = cp_tensor(dims, rank, noise=0.01, seed=51)
