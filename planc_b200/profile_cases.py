@@ -16,6 +16,9 @@ larger than the 126 MB L2 (DRAM counters stay meaningful):
           128^4 FP32 tensor (BF16 copy), rank 64, HALS iterations
   cfg3it  three ANLS/BPP iterations of the 192^4 rank-64 workload (BF16), for
           a one-pass launch list at full size
+  ttv     the multi-TTVs of the 3-way tensor-core path with the headline's
+          intermediate: 1024 x 1024 x 64 FP32 tensor (BF16 copy), rank 32, so
+          the FP32 partial MTTKRP P is 1024*1024 x 32 (134 MB > L2)
 """
 import sys
 
@@ -101,7 +104,24 @@ def case_cfg3it(gpu, torch):
     print("cfg3it: 192^4 k=64 ANLS/BPP: %.3f ms per iteration" % ms)
 
 
-CASES = {"bpp": case_bpp, "tc3": case_tc3, "tc4": case_tc4, "cfg3it": case_cfg3it}
+def case_ttv(gpu, torch):
+    dims, k = (1024, 1024, 64), 32
+    X, F0 = _synth(gpu, torch, dims, k, 41)
+    with gpu.Context(0, "bf16") as c:
+        c.set_tensor(X.data_ptr(), dims=dims, dtype="f32")
+        c.set_factors(F0)
+        c.run("hals", 2, compute_error=False)
+        c.set_timing(True)
+        c.kernel_times()
+        c.run("hals", 3, compute_error=False)
+        kt = c.kernel_times()
+        c.set_timing(False)
+    print("ttv: 1024x1024x64 k=32 HALS, per iteration: " +
+          ", ".join("%s %.1f us" % (n, 1e3 * v[0] / 3) for n, v in kt.items() if v[1]))
+
+
+CASES = {"bpp": case_bpp, "tc3": case_tc3, "tc4": case_tc4, "cfg3it": case_cfg3it,
+         "ttv": case_ttv}
 
 
 def main(argv):
