@@ -7,7 +7,10 @@
 //             [--seed <n>] [--init <file prefix>] [-o <output prefix>]
 //
 // -a takes the reference's algotype integers (0 MU, 1 HALS, 2 ANLSBPP,
-// 4 AOADMM, 5 NESTEROV).
+// 4 AOADMM, 5 NESTEROV). -i reads raw FP64 with a .info sidecar
+// (Tensor::read) or, for a name ending in .npy, a NumPy array
+// (NumPyArray::load, common/npyio.hpp); with .npy the shape comes from the
+// file and -d may be left out.
 // Without -i (or with an -i starting with "rand_") the tensor is
 // Tensor(dims): std::mt19937(103) uniform values, as in the reference.
 // --init reads initial factors written by -o (<prefix>_<n>.txt, I_n rows of k
@@ -23,6 +26,7 @@
 #include <vector>
 
 #include "planc/auntf.hpp"
+#include "planc/npyio.hpp"
 #include "planc/ntfanlsbpp.hpp"
 #include "planc/ntfaoadmm.hpp"
 #include "planc/ntfhals.hpp"
@@ -90,11 +94,19 @@ bool parse(int argc, char** argv, Opts& o) {
 
 template <class NTFTYPE>
 int callNTF(const Opts& o) {
-  UVEC dims(o.dims);
-  planc::Tensor my_tensor(dims);
   const std::string rand_prefix("rand_");
-  if (!o.input.empty() && o.input.compare(0, rand_prefix.size(), rand_prefix) != 0)
-    my_tensor.read(o.input);
+  const bool npy = o.input.size() > 4 && o.input.compare(o.input.size() - 4, 4, ".npy") == 0;
+  planc::Tensor my_tensor;
+  if (npy) {
+    planc::NumPyArray npyreader;
+    npyreader.load(o.input);
+    npyreader.printInfo();
+    my_tensor = *npyreader.m_input_tensor;
+  } else {
+    my_tensor = planc::Tensor(UVEC(o.dims));
+    if (!o.input.empty() && o.input.compare(0, rand_prefix.size(), rand_prefix) != 0)
+      my_tensor.read(o.input);
+  }
   NTFTYPE ntfsolver(my_tensor, o.k, static_cast<algotype>(o.algo));
   ntfsolver.num_it(o.iters);
   ntfsolver.compute_error(o.err != 0);
@@ -135,7 +147,8 @@ int callNTF(const Opts& o) {
 int main(int argc, char* argv[]) {
   Opts o;
   if (!parse(argc, argv, o)) return 0;
-  if (o.dims.size() < 2) {
+  const bool npy = o.input.size() > 4 && o.input.compare(o.input.size() - 4, 4, ".npy") == 0;
+  if (o.dims.size() < 2 && !npy) {
     usage();
     return 1;
   }

@@ -70,3 +70,24 @@ def test_custom_host_update_subclass(gpu, oracle_lib, tmp_path):
     assert all(rel(a, b) < 1e-10 for a, b in zip(Fg, Fo))
     final = float(re.search(r"final_error ([0-9.eE+-]+)", res.stdout).group(1))
     assert abs(final - eo[-1]) / eo[-1] < 1e-5
+
+
+def test_dense_ntf_reads_npy(gpu, oracle_lib, tmp_path):
+    # -i <file>.npy goes through NumPyArray::load (common/npyio.hpp); the shape
+    # comes from the file, so -d is left out
+    exe = str(tmp_path / "dense_ntf")
+    _compile(os.path.join(PKG, "cpp", "ntf.cpp"), exe)
+    dims, k, iters = (20, 16, 12), 4, 6
+    rng = np.random.default_rng(62)
+    X = np.asfortranarray(rng.random(dims))
+    src = str(tmp_path / "x.npy")
+    np.save(src, X)
+    F0 = init_factors(dims, k, seed=63)
+    init, out = str(tmp_path / "init"), str(tmp_path / "out")
+    _write_init(init, F0)
+    res = subprocess.run([exe, "-a", "1", "-i", src, "-k", str(k), "-t", str(iters), "-e", "1",
+                          "--init", init, "-o", out], capture_output=True, text=True, check=True)
+    errs = [float(m) for m in re.findall(r"relative_error at it::\d+::([0-9.eE+-]+)", res.stdout)]
+    Fo, lo, eo = oracle_lib.ntf_run(X, F0, "hals", iters)
+    assert rel(np.array(errs), eo) < 1e-5
+    assert all(rel(a, b) < 1e-10 for a, b in zip(_read_factors(out, 3), Fo))
