@@ -215,6 +215,42 @@ int planc_gpu_mttkrp_last_mode_noalloc(const double* X_dev, const int64_t* dims,
                                        const double* const* F_dev, int k, double* out_dev,
                                        void* cuda_stream);
 
+/* ---- Shared-memory NMF of a dense matrix, A ~ W H^T (reference
+ * common/nmf.hpp, nmf/hals.hpp, nmf/mu.hpp, nmf/bppnmf.hpp). A is the
+ * context's tensor with two modes: planc_gpu_set_tensor(ctx, A, dtype,
+ * {m, n}, 2, ...) with A column-major m x n (an Armadillo MAT). W is m x k
+ * and H is n x k, both row-major here (the memory of the reference's W^T and
+ * H^T). A H and A^T W are the tensor's mode-0 / mode-1 MTTKRPs (FP64, or the
+ * tensor-core contraction at BF16 / split-BF16); Grams, updates and the
+ * objective are FP64. */
+
+/* Sets W and H as given, unnormalised: the NMF(A, W, H) constructor
+ * (common/nmf.hpp:193-210). 1 <= k <= 64. */
+int planc_gpu_nmf_set_factors(planc_gpu_ctx* ctx, const double* W, const double* H, int k);
+
+/* Regularisation of the next runs (NMF::regW / regH / symm_reg,
+ * common/nmf.hpp:467-480): regW = {L2, L1} and regH = {L2, L1} (NULL: none),
+ * symm_reg > 0 (square A only) adds symm_reg I to the Grams and symm_reg *
+ * the other factor to the right-hand sides of BPP (common/nmf.hpp:118-124)
+ * and symm_reg ||W - H||^2 to the objective. All >= 0. */
+int planc_gpu_nmf_set_regularization(planc_gpu_ctx* ctx, const double* regW, const double* regH,
+                                     double symm_reg);
+
+/* `iters` iterations of HALSNMF / MUNMF / BPPNMF::computeNMF
+ * (nmf/hals.hpp:50-110, nmf/mu.hpp:55-92, nmf/bppnmf.hpp:190-240) with algo
+ * PLANC_GPU_HALS / MU / ANLSBPP. HALS normalises by W first, as its
+ * constructor does; MU and ANLS/BPP normalise by W after the last iteration.
+ * objective[it] and rel_error[it] (either may be NULL) receive
+ * NMF::computeObjectiveError's objective and sqrt(fit) / ||A|| after
+ * iteration it (common/nmf.hpp:386-431). */
+int planc_gpu_nmf_run(planc_gpu_ctx* ctx, int algo, int iters, double* objective,
+                      double* rel_error);
+
+/* Copies W (m x k) and H (n x k), row-major, to host memory
+ * (getLeftLowRankFactor / getRightLowRankFactor, common/nmf.hpp:214-215);
+ * either may be NULL. */
+int planc_gpu_nmf_get_factors(planc_gpu_ctx* ctx, double* W, double* H);
+
 /* Lowers the BPP iteration cap (0 restores the reference's 5k,
  * nnls/bppnnls.hpp:69). Used to exercise the "BPP failed" path
  * (PLANC_GPU_ERR_BPP_MAXITER) without a pathological input. */

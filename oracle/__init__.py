@@ -81,6 +81,8 @@ def lib():
         L.orc_nes_update.argtypes = [pd, pd, i64, i32, pd, pd, d, d, i32]
         L.orc_nes_update.restype = i32
         L.orc_sym_eig_minmax.argtypes = [pd, i32, pd, pd]
+        L.orc_nmf_run.argtypes = [pd, i64, i64, i32, pd, pd, i32, i32, pd, pd, pd]
+        L.orc_nmf_run.restype = i32
         _lib = L
     return _lib
 
@@ -274,3 +276,24 @@ def ntf_run(X, F_init, algo, iters, dimtree=True, compute_error=True, lam=None):
     if rc != 0:
         raise RuntimeError("oracle ntf_run failed with code %d" % rc)
     return F, lam, errs[:iters]
+
+
+def nmf_run(A, W0, H0, algo, iters, reg=None):
+    """Shared-memory NMF A ~ W H^T (nmf/hals.hpp, nmf/mu.hpp, nmf/bppnmf.hpp)
+    from W0 (m x k) and H0 (n x k). reg = (regW L2, regW L1, regH L2, regH L1,
+    symm_reg) or None. Returns (W, H, objective per iteration, relative error
+    per iteration)."""
+    A = np.asfortranarray(np.asarray(A, dtype=np.float64))
+    m, n = A.shape
+    W = np.ascontiguousarray(W0, dtype=np.float64).copy()
+    H = np.ascontiguousarray(H0, dtype=np.float64).copy()
+    k = W.shape[1]
+    obj = np.zeros(max(iters, 1))
+    rel = np.zeros(max(iters, 1))
+    r = None if reg is None else np.ascontiguousarray(reg, dtype=np.float64)
+    rc = lib().orc_nmf_run(_pd(A), m, n, k, _pd(W), _pd(H),
+                           ALGO[algo] if isinstance(algo, str) else int(algo), iters,
+                           _pd(r) if r is not None else None, _pd(obj), _pd(rel))
+    if rc != 0:
+        raise RuntimeError("oracle nmf_run failed with code %d" % rc)
+    return W, H, obj[:iters], rel[:iters]

@@ -724,6 +724,137 @@ void nes_accelerate(NesState& st, int iter, double cur_err, const double* X,
   }
 }
 
+
+// ===========================================================================
+// Shared-memory NMF of a dense matrix, A ~ W H^T (common/nmf.hpp,
+// nmf/hals.hpp, nmf/mu.hpp, nmf/bppnmf.hpp). A is column-major m x n
+// (Armadillo MAT); W (m x k) and H (n x k) are row-major here, the memory of
+// the reference's W^T and H^T.
+// ===========================================================================
+struct NmfReg {
+  double w2 = 0, w1 = 0, h2 = 0, h1 = 0, sym = 0;  // regW(0..1), regH(0..1), symm_reg
+};
+
+// out (row-major m x k) = A H (nmf/hals.hpp:86 "AH = A * H")
+void nmf_AH(const double* A, int64_t m, int64_t n, int k, const double* H, double* out) {
+  cblas_dgemm(CblasColMajor, CblasNoTrans, CblasTrans, k, (int)m, (int)n, 1.0, H, k, A, (int)m,
+              0.0, out, k);
+}
+// out (row-major n x k) = A^T W (nmf/mu.hpp:60 "AtW = At * W")
+void nmf_AtW(const double* A, int64_t m, int64_t n, int k, const double* W, double* out) {
+  cblas_dgemm(CblasColMajor, CblasNoTrans, CblasNoTrans, k, (int)n, (int)m, 1.0, W, k, A, (int)m,
+              0.0, out, k);
+}
+
+// NMF::applyReg (common/nmf.hpp:76-92): L2 adds l2 I, L1 adds l1 ones.
+void nmf_apply_reg(double* G, int k, double l2, double l1) {
+  if (l2 > 0)
+    for (int i = 0; i < k; ++i) G[i * k + i] += l2;
+  if (l1 > 0)
+    for (int e = 0; e < k * k; ++e) G[e] += l1;
+}
+
+// NMF::normalize_by_W (common/nmf.hpp:150-160)
+void nmf_normalize_by_W(double* W, int64_t m, double* H, int64_t n, int k) {
+  for (int i = 0; i < k; ++i) {
+    double ss = 0.0;
+    for (int64_t r = 0; r < m; ++r) ss += W[r * k + i] * W[r * k + i];
+    const double nrm = std::sqrt(ss);
+    if (nrm > 0) {
+      for (int64_t r = 0; r < m; ++r) W[r * k + i] = W[r * k + i] / nrm;
+      for (int64_t r = 0; r < n; ++r) H[r * k + i] = H[r * k + i] * nrm;
+    }
+  }
+}
+
+// HALSNMF W sweep (nmf/hals.hpp:92-105): column by column,
+// Wx = W(:,x) HtH(x,x) + (AH(:,x) - W HtH(:,x)), entries < 1e-17 set to
+// 1e-17, then W(:,x) = Wx / ||Wx|| when ||Wx|| != 0.
+void nmf_hals_w(double* W, int64_t m, int k, const double* AH, const double* G) {
+  std::vector<double> wx((size_t)m);
+  for (int x = 0; x < k; ++x) {
+    for (int64_t r = 0; r < m; ++r) {
+      double s = 0.0;
+      for (int j = 0; j < k; ++j) s += W[r * k + j] * G[j * k + x];
+      double v = (W[r * k + x] * G[x * k + x]) + (AH[r * k + x] - s);
+      wx[r] = (v < kEps17) ? kEps17 : v;
+    }
+    double ss = 0.0;
+    for (int64_t r = 0; r < m; ++r) ss += wx[r] * wx[r];
+    const double nrm = std::sqrt(ss);
+    if (nrm != 0)
+      for (int64_t r = 0; r < m; ++r) W[r * k + x] = wx[r] / nrm;
+  }
+}
+
+// MUNMF update of one factor (nmf/mu.hpp:68, 80): U = (U % M) / (U G + 1e-17)
+void nmf_mu(double* U, int64_t I, int k, const double* M, const double* G) {
+  std::vector<double> t((size_t)k);
+  for (int64_t r = 0; r < I; ++r) {
+    for (int c = 0; c < k; ++c) {
+      double acc = 0.0;
+      for (int j = 0; j < k; ++j) acc += U[r * k + j] * G[j * k + c];
+      t[c] = acc + kEps17;
+    }
+    for (int c = 0; c < k; ++c) U[r * k + c] = (U[r * k + c] * M[r * k + c]) / t[c];
+  }
+}
+
+// NMF::computeObjectiveError (common/nmf.hpp:386-425) from AtW = A^T W of the
+// current W. Writes the objective and the relative error sqrt(fit)/||A||.
+void nmf_error(const double* W, int64_t m, const double* H, int64_t n, int k, const double* AtW,
+               double normA, const NmfReg& reg, double* objective, double* relerr) {
+  std::vector<double> WtW((size_t)k * k), HtH((size_t)k * k);
+  gram(W, m, k, WtW.data());
+  gram(H, n, k, HtH.data());
+  const double sqnormA = normA * normA;
+  double tr_htatw = 0.0;
+  for (int64_t e = 0; e < n * k; ++e) tr_htatw += H[e] * AtW[e];
+  double tr_ww_hh = 0.0;
+  for (int a = 0; a < k; ++a)
+    for (int b = 0; b < k; ++b) tr_ww_hh += WtW[a * k + b] * HtH[b * k + a];
+  double fro_w = 0.0, fro_h = 0.0;
+  for (int i = 0; i < k; ++i) {
+    fro_w += WtW[i * k + i];
+    fro_h += HtH[i * k + i];
+  }
+  auto l1sq = [k](const double* U, int64_t I) {
+    double s = 0.0;
+    for (int64_t r = 0; r < I; ++r) {
+      double rs = 0.0;
+      for (int c = 0; c < k; ++c) rs += U[r * k + c];
+      s += rs * rs;
+    }
+    return s;  // ||sum(U, 1)||_2^2
+  };
+  const double fit = sqnormA - (2 * tr_htatw) + tr_ww_hh;
+  double sym_obj = 0.0;
+  if (reg.sym > 0) {
+    double d = 0.0;
+    for (int64_t e = 0; e < m * k; ++e) d += (W[e] - H[e]) * (W[e] - H[e]);
+    sym_obj = reg.sym * d;
+  }
+  *objective = fit + reg.w2 * fro_w + reg.h2 * fro_h + reg.w1 * l1sq(W, m) +
+               reg.h1 * l1sq(H, n) + sym_obj;
+  const double err = fit > 0 ? std::sqrt(fit) : normA;
+  *relerr = err / normA;
+}
+
+// BPPNMF::updateOtherGivenOneMultipleRHS (nmf/bppnmf.hpp:24-80): solves the
+// rows of `out` (I x k) from G = given^T given + reg (+ symm_reg I) and the
+// right-hand sides M (+ symm_reg given). Returns -1 on a BPP failure.
+int nmf_bpp(double* out, int64_t I, int k, const double* M, const double* given,
+            int64_t gI, double l2, double l1, double sym) {
+  std::vector<double> G((size_t)k * k), R(M, M + (size_t)I * k);
+  gram(given, gI, k, G.data());
+  nmf_apply_reg(G.data(), k, l2, l1);
+  if (sym > 0) {
+    for (int i = 0; i < k; ++i) G[i * k + i] += sym;
+    for (int64_t e = 0; e < I * k; ++e) R[e] += sym * given[e];
+  }
+  return bpp_solve(G.data(), R.data(), k, I, out, nullptr) < 0 ? -1 : 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -906,6 +1037,62 @@ int orc_nes_update(const double* H0, double* H, int64_t I, int k, const double* 
 // Extreme eigenvalues of a symmetric k x k matrix (arma::eig_sym, LAPACK dsyev).
 void orc_sym_eig_minmax(const double* G, int k, double* lmin, double* lmax) {
   sym_eig_minmax(G, k, lmin, lmax);
+}
+
+
+// The NMF loop of HALSNMF / MUNMF / BPPNMF::computeNMF (nmf/hals.hpp:50-110,
+// nmf/mu.hpp:55-92, nmf/bppnmf.hpp:190-240) from injected W0, H0 (the
+// NMF(A, W, H) constructor, common/nmf.hpp:193-210; HALSNMF normalises by W
+// first, nmf/hals.hpp:44-48). A column-major m x n; W, H row-major (in/out).
+// reg = {regW L2, regW L1, regH L2, regH L1, symm_reg} (may be NULL). The
+// objective and relative error of every iteration go to obj / relerr.
+int orc_nmf_run(const double* A, int64_t m, int64_t n, int k, double* W, double* H, int algo,
+                int iters, const double* reg5, double* obj, double* relerr) {
+  NmfReg reg;
+  if (reg5) {
+    reg.w2 = reg5[0];
+    reg.w1 = reg5[1];
+    reg.h2 = reg5[2];
+    reg.h1 = reg5[3];
+    reg.sym = reg5[4];
+  }
+  if (reg.sym > 0 && m != n) return -2;
+  double normA = 0.0;
+  for (int64_t e = 0; e < m * n; ++e) normA += A[e] * A[e];
+  normA = std::sqrt(normA);  // arma::norm(A, "fro")
+  std::vector<double> AH((size_t)m * k), AtW((size_t)n * k), G((size_t)k * k);
+  if (algo == HALS) nmf_normalize_by_W(W, m, H, n, k);
+  for (int it = 0; it < iters; ++it) {
+    if (algo == HALS || algo == MU) {
+      nmf_AtW(A, m, n, k, W, AtW.data());
+      gram(W, m, k, G.data());
+      nmf_apply_reg(G.data(), k, reg.h2, reg.h1);
+      if (algo == HALS)
+        hals_update(H, n, k, AtW.data(), G.data());
+      else
+        nmf_mu(H, n, k, AtW.data(), G.data());
+      nmf_AH(A, m, n, k, H, AH.data());
+      gram(H, n, k, G.data());
+      nmf_apply_reg(G.data(), k, reg.w2, reg.w1);
+      if (algo == HALS) {
+        nmf_hals_w(W, m, k, AH.data(), G.data());
+        nmf_normalize_by_W(W, m, H, n, k);
+      } else {
+        nmf_mu(W, m, k, AH.data(), G.data());
+      }
+    } else if (algo == ANLSBPP) {
+      nmf_AH(A, m, n, k, H, AH.data());
+      if (nmf_bpp(W, m, k, AH.data(), H, n, reg.w2, reg.w1, reg.sym) < 0) return -1;
+      nmf_AtW(A, m, n, k, W, AtW.data());
+      if (nmf_bpp(H, n, k, AtW.data(), W, m, reg.h2, reg.h1, reg.sym) < 0) return -1;
+    } else {
+      return -3;
+    }
+    nmf_AtW(A, m, n, k, W, AtW.data());
+    nmf_error(W, m, H, n, k, AtW.data(), normA, reg, &obj[it], &relerr[it]);
+  }
+  if (algo == MU || algo == ANLSBPP) nmf_normalize_by_W(W, m, H, n, k);
+  return 0;
 }
 
 }  // extern "C"

@@ -39,6 +39,8 @@ EXPORTS = [
     "planc_gpu_launch_count", "planc_gpu_synth_cp_tensor", "planc_gpu_mttkrp_device",
     "planc_gpu_tensor_norm2", "planc_gpu_set_bpp_max_iter", "planc_gpu_set_bpp_warm_start",
     "planc_gpu_reset_update_state", "planc_gpu_selftest_wait_timeout",
+    "planc_gpu_nmf_set_factors", "planc_gpu_nmf_set_regularization", "planc_gpu_nmf_run",
+    "planc_gpu_nmf_get_factors",
     "planc_gpu_batch_create", "planc_gpu_batch_add", "planc_gpu_batch_count",
     "planc_gpu_batch_set_factors", "planc_gpu_batch_run", "planc_gpu_batch_get_factors",
     "planc_gpu_batch_autotune", "planc_gpu_batch_destroy", "planc_gpu_mttkrp_last_mode_noalloc",
@@ -92,6 +94,10 @@ def load():
     L.planc_gpu_set_bpp_max_iter.argtypes = [vp, i32]
     L.planc_gpu_set_bpp_warm_start.argtypes = [vp, i32]
     L.planc_gpu_reset_update_state.argtypes = [vp]
+    L.planc_gpu_nmf_set_factors.argtypes = [vp, pd, pd, i32]
+    L.planc_gpu_nmf_set_regularization.argtypes = [vp, pd, pd, ctypes.c_double]
+    L.planc_gpu_nmf_run.argtypes = [vp, i32, i32, pd, pd]
+    L.planc_gpu_nmf_get_factors.argtypes = [vp, pd, pd]
     L.planc_gpu_batch_create.argtypes = [P(vp), i32, i32, i32]
     L.planc_gpu_batch_add.argtypes = [vp, vp, i32, pi64, i32, i32, P(pd), i32, P(i32)]
     L.planc_gpu_batch_count.argtypes = [vp]
@@ -206,6 +212,29 @@ class Context:
         lam = np.zeros(self.k)
         _check(load().planc_gpu_get_factors(self.h, _fptrs(F), _pd(lam)))
         return F, lam
+
+    # ---- shared-memory NMF of a matrix A ~ W H^T (set_tensor(A) with a 2-D
+    # Fortran-order array; W: (m, k), H: (n, k))
+    def nmf_set_factors(self, W, H):
+        W, H = _c64(W), _c64(H)
+        _check(load().planc_gpu_nmf_set_factors(self.h, _pd(W), _pd(H), W.shape[1]))
+        self.k = W.shape[1]
+
+    def nmf_set_regularization(self, regW=(0.0, 0.0), regH=(0.0, 0.0), symm_reg=0.0):
+        rw, rh = _c64(np.asarray(regW, dtype=np.float64)), _c64(np.asarray(regH, dtype=np.float64))
+        _check(load().planc_gpu_nmf_set_regularization(self.h, _pd(rw), _pd(rh), float(symm_reg)))
+
+    def nmf_run(self, algo, iters):
+        """Returns (objective, relative error) per iteration."""
+        obj, rel = np.zeros(max(iters, 1)), np.zeros(max(iters, 1))
+        _check(load().planc_gpu_nmf_run(self.h, ALGO[algo] if isinstance(algo, str) else int(algo),
+                                        iters, _pd(obj), _pd(rel)))
+        return obj[:iters], rel[:iters]
+
+    def nmf_get_factors(self):
+        W, H = np.zeros((self.dims[0], self.k)), np.zeros((self.dims[1], self.k))
+        _check(load().planc_gpu_nmf_get_factors(self.h, _pd(W), _pd(H)))
+        return W, H
 
     def mttkrp(self, mode, dimtree=True):
         out = np.zeros((self.dims[mode], self.k))

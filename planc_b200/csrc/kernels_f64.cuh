@@ -498,9 +498,12 @@ __global__ void __launch_bounds__(256) k_hals_warp(double* __restrict__ H, const
   }
 }
 
+// MU: H = (H .* M) ./ (H G + eps); eps is 1e-6 for NTF (ntf/ntfmu.hpp:14) and
+// 1e-17 for NMF (nmf/mu.hpp:68, 80).
 template <int KP>
 __global__ void __launch_bounds__(256) k_mu_warp(double* __restrict__ H, const double* __restrict__ M,
-                                                 const double* __restrict__ G, int64_t I, int k) {
+                                                 const double* __restrict__ G, int64_t I, int k,
+                                                 double eps) {
   constexpr int PER = KP / 32;
   __shared__ double Gs[KP * KP];
   for (int e = threadIdx.x; e < k * k; e += blockDim.x) Gs[e] = G[e];
@@ -527,7 +530,7 @@ __global__ void __launch_bounds__(256) k_mu_warp(double* __restrict__ H, const d
 #pragma unroll
   for (int p = 0; p < PER; ++p) {
     const int c = lane + 32 * p;
-    if (c < k) H[row * k + c] = (h[p] * M[row * k + c]) / (t[p] + kEps6);
+    if (c < k) H[row * k + c] = (h[p] * M[row * k + c]) / (t[p] + eps);
   }
 }
 

@@ -21,6 +21,7 @@
 #include "common.cuh"
 #include "kernels_f64.cuh"
 #include "tc_mttkrp.cuh"
+#include "nmf.cuh"
 #include "updates_iter.cuh"
 
 using namespace pg;
@@ -132,6 +133,25 @@ struct planc_gpu_ctx {
   double* nes_gbak = nullptr;   // N x k x k backup Grams
   NesDev* nes = nullptr;
   int cl_ctas = NES_CTAS;       // CTAs of the register-resident update clusters
+
+  // Shared-memory NMF of the context's 2-way tensor A ~ W H^T (W = F[0],
+  // H = F[1], A H -> M[0], A^T W -> M[1]); buffers allocated on the first run.
+  bool nmf_have = false;        // W and H set by planc_gpu_nmf_set_factors
+  bool nmf_ready = false;
+  double* nmf_G = nullptr;      // regularised Gram of the fixed factor, k x k
+  double* nmf_GW = nullptr;     // W^T W and H^T H of the objective, k x k each
+  double* nmf_GH = nullptr;
+  double* nmf_norms = nullptr;  // column norms of the HALS W sweep, k
+  double* nmf_part = nullptr;   // Gram / column-sum / norm partials
+  size_t nmf_part_elems = 0;
+  int* nmf_ctr = nullptr;       // [0] objective index, [1] CTA ticket of the W sweep
+  double* nmf_obj = nullptr;    // objective and relative error per iteration
+  double* nmf_rel = nullptr;
+  int nmf_cap = 0;
+  double nmf_reg[5] = {0, 0, 0, 0, 0};  // regW L2, L1, regH L2, L1, symm_reg
+  cudaGraphExec_t nmf_gexec = nullptr;
+  int nmf_galgo = -1;
+  int64_t nmf_gepoch = -1;
 
   // cached iteration graphs: [0] the plain iteration, [1] iteration +
   // Nesterov acceleration
@@ -667,12 +687,12 @@ void run_update(planc_gpu_ctx* c, int algo, int n) {
         if (algo == PLANC_GPU_HALS)
           k_hals_warp<32><<<blocks, 256, 0, c->stream>>>(c->F[n], c->M[n], c->Gloo, I, k);
         else
-          k_mu_warp<32><<<blocks, 256, 0, c->stream>>>(c->F[n], c->M[n], c->Gloo, I, k);
+          k_mu_warp<32><<<blocks, 256, 0, c->stream>>>(c->F[n], c->M[n], c->Gloo, I, k, kEps6);
       } else {
         if (algo == PLANC_GPU_HALS)
           k_hals_warp<64><<<blocks, 256, 0, c->stream>>>(c->F[n], c->M[n], c->Gloo, I, k);
         else
-          k_mu_warp<64><<<blocks, 256, 0, c->stream>>>(c->F[n], c->M[n], c->Gloo, I, k);
+          k_mu_warp<64><<<blocks, 256, 0, c->stream>>>(c->F[n], c->M[n], c->Gloo, I, k, kEps6);
       }
     });
   } else if (algo == PLANC_GPU_ANLSBPP) {
@@ -952,6 +972,20 @@ void free_update_state(planc_gpu_ctx* c) {
   f(c->nes_gbak);
   f(c->nes);
   c->admm_ready = c->nes_ready = false;
+  if (c->nmf_gexec) cudaGraphExecDestroy(c->nmf_gexec);
+  c->nmf_gexec = nullptr;
+  c->nmf_galgo = -1;
+  f(c->nmf_G);
+  f(c->nmf_GW);
+  f(c->nmf_GH);
+  f(c->nmf_norms);
+  f(c->nmf_part);
+  c->nmf_part_elems = 0;
+  f(c->nmf_ctr);
+  f(c->nmf_obj);
+  f(c->nmf_rel);
+  c->nmf_cap = 0;
+  c->nmf_ready = false;
 }
 
 // Allocates (zeroed) the solver-object state of `algo` if it is not there:
@@ -1147,6 +1181,7 @@ int planc_gpu_set_tensor(planc_gpu_ctx* c, const void* X, int dtype, const int64
     for (int i = 0; same && i < nmodes; ++i) same = c->dims[i] == dims[i];
     if (!same) {
       c->have_factors = false;
+      c->nmf_have = false;
       free_update_state(c);
       auto f = [](auto*& p) {
         if (p) cudaFree(p);
@@ -1160,6 +1195,8 @@ int planc_gpu_set_tensor(planc_gpu_ctx* c, const void* X, int dtype, const int64
     for (int i = 0; i < nmodes; ++i) c->dims[i] = dims[i];
     c->numel = numel;
     c->s = nmodes / 2;  // ntf/auntf.hpp:122-123
+    // a matrix (NMF): rows = mode 0 (L), columns = mode 1 (R)
+    if (nmodes == 2) c->s = 0;
     // PLANC_GPU_DIMTREE_SPLIT=reference keeps the reference's split everywhere
     const char* split_env = getenv("PLANC_GPU_DIMTREE_SPLIT");
     const bool ref_split = split_env && strcmp(split_env, "reference") == 0;
@@ -1280,6 +1317,7 @@ int planc_gpu_set_factors(planc_gpu_ctx* c, const double* const* F, const double
     ensure_buffers(c);
     CK(cudaStreamSynchronize(c->stream));
     c->have_factors = true;
+    c->nmf_have = false;
   });
 }
 
@@ -2087,3 +2125,340 @@ extern "C" int planc_gpu_mttkrp_last_mode_noalloc(const double* X_dev, const int
   });
 }
 
+
+// ===================================================================== NMF
+// Shared-memory NMF of a dense matrix A ~ W H^T (reference common/nmf.hpp,
+// nmf/hals.hpp, nmf/mu.hpp, nmf/bppnmf.hpp) on a context holding A as its
+// 2-way tensor (mode 0 = rows). A H and A^T W are the mode-0 and mode-1
+// MTTKRPs: the FP64 contraction kernels, or the long-K tensor-core
+// contraction against a hi|lo image of H or W. One CUDA graph per iteration.
+namespace {
+
+bool nmf_tc(const planc_gpu_ctx* c) { return c->precision != PLANC_GPU_PREC_FP64; }
+
+void ensure_nmf(planc_gpu_ctx* c, int iters) {
+  ensure_buffers(c);
+  const int k = c->k;
+  const int64_t m = c->dims[0], n = c->dims[1], maxI = std::max(m, n);
+  if (nmf_tc(c)) {
+    const void* before = c->tct.wimg;
+    c->tct.wimg_K = std::max(c->L, c->R);
+    CK(tc_ensure(c->tct, k));
+    size_t need = std::max(tc_long_scratch_elems(c->tct, true, k, eff_sm(c)),
+                           tc_long_scratch_elems(c->tct, false, k, eff_sm(c)));
+    if (need > c->scratch_elems) {
+      dalloc(&c->scratch, need);
+      c->scratch_elems = need;
+      c->buf_epoch++;
+    }
+    if (before != c->tct.wimg) c->buf_epoch++;
+  }
+  if (!c->nmf_ready) {
+    dalloc(&c->nmf_G, (size_t)k * k);
+    dalloc(&c->nmf_GW, (size_t)k * k);
+    dalloc(&c->nmf_GH, (size_t)k * k);
+    dalloc(&c->nmf_norms, (size_t)k);
+    c->nmf_part_elems = std::max<size_t>(
+        std::max<size_t>((size_t)((maxI + GP_ROWS - 1) / GP_ROWS) * k * k,
+                         (size_t)((maxI + CN_ROWS - 1) / CN_ROWS) * k),
+        NMFW_MAX_BLOCKS);
+    dalloc(&c->nmf_part, c->nmf_part_elems);
+    dalloc(&c->nmf_ctr, 2);
+    CK(cudaMemset(c->nmf_ctr, 0, 2 * sizeof(int)));
+    c->nmf_ready = true;
+    c->buf_epoch++;
+  }
+  if (iters > c->nmf_cap) {
+    dalloc(&c->nmf_obj, (size_t)iters);
+    dalloc(&c->nmf_rel, (size_t)iters);
+    c->nmf_cap = iters;
+    c->buf_epoch++;
+  }
+}
+
+// out = U^T U (+ l2 I + l1 ones + diag I)
+void nmf_gram(planc_gpu_ctx* c, const double* U, int64_t I, double l2, double l1, double diag,
+              double* out) {
+  const int k = c->k;
+  const int rpb = gram_rows_per_block(I);
+  const int nblk = (int)((I + rpb - 1) / rpb);
+  if ((size_t)nblk * k * k > c->nmf_part_elems) fail(PLANC_GPU_ERR_STATE, "internal: NMF partials");
+  launch(c, KC_NORMGRAM, [&] {
+    k_gram_partial<<<nblk, 256, 0, c->stream>>>(U, I, k, rpb, c->nmf_part);
+  });
+  launch(c, KC_NORMGRAM, [&] {
+    k_nmf_gram<<<1, 1024, 0, c->stream>>>(c->nmf_part, nblk, k, l2, l1, diag, out);
+  });
+}
+
+// M[0] = A H
+void nmf_AH(planc_gpu_ctx* c) {
+  if (nmf_tc(c))
+    long_contract(c, false, {1}, c->M[0]);
+  else
+    mttkrp_direct(c, 0, c->M[0]);
+}
+
+// M[1] = A^T W
+void nmf_AtW(planc_gpu_ctx* c) {
+  if (nmf_tc(c))
+    long_contract(c, true, {0}, c->M[1]);
+  else
+    mttkrp_direct(c, 1, c->M[1]);
+}
+
+// NMF::normalize_by_W (common/nmf.hpp:150-160)
+void nmf_normalize(planc_gpu_ctx* c) {
+  const int64_t m = c->dims[0], n = c->dims[1];
+  const unsigned nb = (unsigned)((m + CN_ROWS - 1) / CN_ROWS);
+  const unsigned nr = (unsigned)((std::max(m, n) + NRM_ROWS - 1) / NRM_ROWS);
+  launch(c, KC_NORMGRAM, [&] {
+    k_colsumsq_partial<<<nb, 256, 0, c->stream>>>(c->F[0], m, c->k, c->nmf_part);
+  });
+  launch(c, KC_NORMGRAM, [&] {
+    k_nmf_rescale<<<nr, 256, 0, c->stream>>>(c->F[0], m, c->F[1], n, c->k, c->nmf_part, (int)nb);
+  });
+}
+
+// rows of U (I x k) from the Gram nmf_G and right-hand sides M: HALS
+// (H only), MU or BPP
+void nmf_row_update(planc_gpu_ctx* c, int algo, double* U, const double* M, int64_t I) {
+  const int k = c->k;
+  if (algo == PLANC_GPU_HALS || algo == PLANC_GPU_MU) {
+    const unsigned blocks = (unsigned)((I + 7) / 8);
+    launch(c, KC_UPDATE, [&] {
+      if (algo == PLANC_GPU_HALS) {
+        if (k <= 32)
+          k_hals_warp<32><<<blocks, 256, 0, c->stream>>>(U, M, c->nmf_G, I, k);
+        else
+          k_hals_warp<64><<<blocks, 256, 0, c->stream>>>(U, M, c->nmf_G, I, k);
+      } else {
+        if (k <= 32)
+          k_mu_warp<32><<<blocks, 256, 0, c->stream>>>(U, M, c->nmf_G, I, k, kEps17);
+        else
+          k_mu_warp<64><<<blocks, 256, 0, c->stream>>>(U, M, c->nmf_G, I, k, kEps17);
+      }
+    });
+  } else {
+    const unsigned blocks = (unsigned)((I + BPP_WARPS - 1) / BPP_WARPS);
+    launch(c, KC_BPP, [&] {
+      switch (kpad(k)) {
+#define CASE(KP)                                                                               \
+  case KP:                                                                                     \
+    k_bpp<KP><<<blocks, 32 * BPP_WARPS, bpp_smem_bytes(KP), c->stream>>>(                      \
+        c->nmf_G, M, k, I, U, nullptr, nullptr, c->status_dev, c->bpp_max_iter,                \
+        c->bpp_warm ? U : nullptr);                                                            \
+    break;
+        CASE(8) CASE(16) CASE(32) CASE(64)
+#undef CASE
+      }
+    });
+  }
+}
+
+// HALSNMF's W sweep (nmf/hals.hpp:92-105): k + 1 launches, one per column
+// plus the finishing normalisation of the last
+void nmf_hals_w(planc_gpu_ctx* c) {
+  const int k = c->k;
+  const int64_t m = c->dims[0];
+  const unsigned nb = (unsigned)std::min<int64_t>((m + NMFW_WARPS - 1) / NMFW_WARPS, NMFW_MAX_BLOCKS);
+  for (int x = 0; x <= k; ++x)
+    launch(c, KC_UPDATE, [&] {
+      if (k <= 32)
+        k_nmf_hals_w<32><<<nb, 32 * NMFW_WARPS, 0, c->stream>>>(
+            c->F[0], c->M[0], c->nmf_G, m, k, x, c->nmf_norms, c->nmf_part, c->nmf_ctr + 1);
+      else
+        k_nmf_hals_w<64><<<nb, 32 * NMFW_WARPS, 0, c->stream>>>(
+            c->F[0], c->M[0], c->nmf_G, m, k, x, c->nmf_norms, c->nmf_part, c->nmf_ctr + 1);
+    });
+}
+
+void nmf_error(planc_gpu_ctx* c) {
+  const int64_t m = c->dims[0], n = c->dims[1];
+  nmf_gram(c, c->F[0], m, 0, 0, 0, c->nmf_GW);
+  nmf_gram(c, c->F[1], n, 0, 0, 0, c->nmf_GH);
+  NmfReg reg{c->nmf_reg[0], c->nmf_reg[1], c->nmf_reg[2], c->nmf_reg[3], c->nmf_reg[4]};
+  launch(c, KC_ERROR, [&] {
+    k_nmf_error<<<1, 1024, 0, c->stream>>>(c->F[0], m, c->F[1], n, c->k, c->M[1], c->nmf_GW,
+                                          c->nmf_GH, c->normX2, reg, c->nmf_obj, c->nmf_rel,
+                                          c->nmf_ctr);
+  });
+}
+
+// One iteration of HALSNMF / MUNMF / BPPNMF::computeNMF. HALS and MU find
+// A^T W of the current W in M[1] (left there by the previous iteration's
+// objective, or computed before the first).
+void nmf_iteration(planc_gpu_ctx* c, int algo) {
+  const int64_t m = c->dims[0], n = c->dims[1];
+  const double* r = c->nmf_reg;
+  const double sym = r[4];
+  if (algo == PLANC_GPU_HALS || algo == PLANC_GPU_MU) {
+    // H <- f(H, A^T W, W^T W + regH)   (nmf/hals.hpp:60-76, nmf/mu.hpp:60-68)
+    nmf_gram(c, c->F[0], m, r[2], r[3], 0, c->nmf_G);
+    nmf_row_update(c, algo, c->F[1], c->M[1], n);
+    // W <- f(W, A H, H^T H + regW)     (nmf/hals.hpp:82-106, nmf/mu.hpp:72-80)
+    nmf_AH(c);
+    nmf_gram(c, c->F[1], n, r[0], r[1], 0, c->nmf_G);
+    if (algo == PLANC_GPU_HALS) {
+      nmf_hals_w(c);
+      nmf_normalize(c);
+    } else {
+      nmf_row_update(c, algo, c->F[0], c->M[0], m);
+    }
+    nmf_AtW(c);
+  } else {
+    // ANLS: W from (H^T H + regW, H^T A^T), then H from (W^T W + regH, W^T A),
+    // each with the symmetric regularisation when set (nmf/bppnmf.hpp:24-80,
+    // 208-214)
+    nmf_AH(c);
+    nmf_gram(c, c->F[1], n, r[0], r[1], sym, c->nmf_G);
+    if (sym > 0)
+      launch(c, KC_UPDATE, [&] {
+        k_nmf_axpy<<<elem_grid(m * c->k), 256, 0, c->stream>>>(c->M[0], c->F[1], m * c->k, sym);
+      });
+    nmf_row_update(c, algo, c->F[0], c->M[0], m);
+    nmf_AtW(c);
+    nmf_gram(c, c->F[0], m, r[2], r[3], sym, c->nmf_G);
+    if (sym > 0)
+      launch(c, KC_UPDATE, [&] {
+        k_nmf_axpy<<<elem_grid(n * c->k), 256, 0, c->stream>>>(c->M[1], c->F[0], n * c->k, sym);
+      });
+    nmf_row_update(c, algo, c->F[1], c->M[1], n);
+    if (sym > 0) nmf_AtW(c);  // the objective takes A^T W without the shift
+  }
+  nmf_error(c);
+}
+
+void require_nmf(planc_gpu_ctx* c) {
+  if (!c) fail(PLANC_GPU_ERR_ARG, "null context");
+  if (!c->have_tensor || c->N != 2) fail(PLANC_GPU_ERR_STATE, "NMF needs a matrix (2-way tensor)");
+  if (!c->nmf_have) fail(PLANC_GPU_ERR_STATE, "no NMF factors set");
+}
+
+}  // namespace
+
+extern "C" {
+
+int planc_gpu_nmf_set_factors(planc_gpu_ctx* c, const double* W, const double* H, int k) {
+  return guarded([&] {
+    if (!c || !W || !H) fail(PLANC_GPU_ERR_ARG, "null argument");
+    if (!c->have_tensor || c->N != 2) fail(PLANC_GPU_ERR_STATE, "set a matrix (2-way tensor) first");
+    if (k < 1 || k > kMaxRank)
+      fail(PLANC_GPU_ERR_UNSUPPORTED, "rank must be in [1, " + std::to_string(kMaxRank) + "]");
+    set_device(c);
+    reset_graph(c);
+    if (k != c->k) {
+      free_update_state(c);
+      for (int i = 0; i < kMaxModes; ++i) c->factor_cap[i] = 0;
+    }
+    c->k = k;
+    const double* src[2] = {W, H};
+    for (int i = 0; i < 2; ++i) {
+      const size_t need = (size_t)c->dims[i] * k;
+      if (c->factor_cap[i] != (int64_t)need) {
+        dalloc(&c->F[i], need);
+        dalloc(&c->M[i], need);
+        c->factor_cap[i] = (int64_t)need;
+        c->buf_epoch++;
+      }
+      CK(cudaMemcpyAsync(c->F[i], src[i], need * 8, cudaMemcpyHostToDevice, c->stream));
+    }
+    CK(cudaStreamSynchronize(c->stream));
+    c->have_factors = false;  // the NTF factors (normalised, with Grams) are not these
+    c->nmf_have = true;
+  });
+}
+
+int planc_gpu_nmf_set_regularization(planc_gpu_ctx* c, const double* regW, const double* regH,
+                                     double symm_reg) {
+  return guarded([&] {
+    if (!c) fail(PLANC_GPU_ERR_ARG, "null context");
+    double r[5] = {regW ? regW[0] : 0.0, regW ? regW[1] : 0.0, regH ? regH[0] : 0.0,
+                   regH ? regH[1] : 0.0, symm_reg};
+    for (double v : r)
+      if (!(v >= 0) || !std::isfinite(v)) fail(PLANC_GPU_ERR_ARG, "regularisation must be >= 0");
+    if (std::memcmp(r, c->nmf_reg, sizeof(r)) != 0) {
+      std::memcpy(c->nmf_reg, r, sizeof(r));
+      if (c->nmf_gexec) cudaGraphExecDestroy(c->nmf_gexec);  // the weights are launch arguments
+      c->nmf_gexec = nullptr;
+      c->nmf_galgo = -1;
+    }
+  });
+}
+
+int planc_gpu_nmf_run(planc_gpu_ctx* c, int algo, int iters, double* objective,
+                      double* rel_error) {
+  return guarded([&] {
+    require_nmf(c);
+    if (iters < 0) fail(PLANC_GPU_ERR_ARG, "iters < 0");
+    if (algo != PLANC_GPU_MU && algo != PLANC_GPU_HALS && algo != PLANC_GPU_ANLSBPP)
+      fail(PLANC_GPU_ERR_ARG, "NMF takes MU, HALS or ANLS/BPP");
+    if (c->nmf_reg[4] > 0 && c->dims[0] != c->dims[1])
+      fail(PLANC_GPU_ERR_ARG, "symmetric regularisation needs a square matrix");
+    if (iters == 0) return;
+    set_device(c);
+    ensure_nmf(c, iters);
+    if (c->nmf_gepoch != c->buf_epoch && c->nmf_gexec) {
+      cudaGraphExecDestroy(c->nmf_gexec);
+      c->nmf_gexec = nullptr;
+      c->nmf_galgo = -1;
+    }
+    CK(cudaMemsetAsync(c->nmf_ctr, 0, sizeof(int), c->stream));
+    if (algo == PLANC_GPU_HALS) nmf_normalize(c);  // HALSNMF's constructor, nmf/hals.hpp:44-48
+    if (algo != PLANC_GPU_ANLSBPP) nmf_AtW(c);
+    if (!c->timing) {
+      if (!c->nmf_gexec || c->nmf_galgo != algo) {
+        if (c->nmf_gexec) cudaGraphExecDestroy(c->nmf_gexec);
+        c->nmf_gexec = nullptr;
+        cudaGraph_t graph;
+        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+        c->capturing = true;
+        try {
+          nmf_iteration(c, algo);
+        } catch (...) {
+          c->capturing = false;
+          cudaStreamEndCapture(c->stream, &graph);
+          if (graph) cudaGraphDestroy(graph);
+          throw;
+        }
+        c->capturing = false;
+        CK(cudaStreamEndCapture(c->stream, &graph));
+        cudaError_t e = cudaGraphInstantiate(&c->nmf_gexec, graph, 0);
+        cudaGraphDestroy(graph);
+        cuda_check(e, "cudaGraphInstantiate (NMF)");
+        c->nmf_galgo = algo;
+        c->nmf_gepoch = c->buf_epoch;
+      }
+      for (int it = 0; it < iters; ++it) CK(cudaGraphLaunch(c->nmf_gexec, c->stream));
+    } else {
+      for (int it = 0; it < iters; ++it) nmf_iteration(c, algo);
+    }
+    // MUNMF / BPPNMF normalise by W after the loop (nmf/mu.hpp:90,
+    // nmf/bppnmf.hpp:240)
+    if (algo != PLANC_GPU_HALS) nmf_normalize(c);
+    if (objective)
+      CK(cudaMemcpyAsync(objective, c->nmf_obj, iters * sizeof(double), cudaMemcpyDeviceToHost,
+                         c->stream));
+    if (rel_error)
+      CK(cudaMemcpyAsync(rel_error, c->nmf_rel, iters * sizeof(double), cudaMemcpyDeviceToHost,
+                         c->stream));
+    check_status(c);
+    drain_timing(c);
+  });
+}
+
+int planc_gpu_nmf_get_factors(planc_gpu_ctx* c, double* W, double* H) {
+  return guarded([&] {
+    require_nmf(c);
+    set_device(c);
+    if (W)
+      CK(cudaMemcpyAsync(W, c->F[0], (size_t)c->dims[0] * c->k * 8, cudaMemcpyDeviceToHost,
+                         c->stream));
+    if (H)
+      CK(cudaMemcpyAsync(H, c->F[1], (size_t)c->dims[1] * c->k * 8, cudaMemcpyDeviceToHost,
+                         c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+  });
+}
+
+}  // extern "C"

@@ -202,3 +202,52 @@ def test_oracle_ntf_run_new_algorithms_descend(oracle_lib, algo):
         assert e < errs[-1] + 1e-12
     else:
         assert abs(e - errs[-1]) < 1e-12
+
+
+# ---- shared-memory NMF (nmf/hals.hpp, nmf/mu.hpp, nmf/bppnmf.hpp) ----
+
+def _nmf_problem(m, n, k, seed, noise=0.01):
+    rng = np.random.default_rng(seed)
+    A = rng.random((m, k)) @ rng.random((k, n))
+    A = np.maximum(A + noise * A.std() * rng.standard_normal(A.shape), 0.0)
+    return np.asfortranarray(A), rng.random((m, k)), rng.random((n, k))
+
+
+@pytest.mark.parametrize("algo", ["hals", "mu", "anlsbpp"])
+def test_oracle_nmf_error_is_the_fit(oracle_lib, algo):
+    # the reported relative error is ||A - W H^T|| / ||A|| of the factors the
+    # run returns (normalize_by_W rescales W and H without changing W H^T)
+    A, W0, H0 = _nmf_problem(40, 30, 5, 71)
+    W, H, obj, rel = oracle_lib.nmf_run(A, W0, H0, algo, 12)
+    direct = np.linalg.norm(A - W @ H.T) / np.linalg.norm(A)
+    assert abs(direct - rel[-1]) < 1e-10
+    assert abs(obj[-1] - (rel[-1] * np.linalg.norm(A)) ** 2) < 1e-8 * obj[-1]
+    assert rel[-1] < rel[0]
+    # W leaves the run with unit columns
+    assert np.allclose(np.linalg.norm(W, axis=0), 1.0)
+
+
+def test_oracle_nmf_bpp_is_monotone_and_solves_nnls(oracle_lib):
+    # ANLS: each half step is an exact NNLS solve, so the objective never
+    # rises, and H is the NNLS optimum for the W it was solved with (the final
+    # normalize_by_W scales W's columns by 1/s and H's by s, which maps one
+    # NNLS optimum onto the other)
+    from scipy.optimize import nnls
+    A, W0, H0 = _nmf_problem(50, 35, 6, 72)
+    W, H, obj, rel = oracle_lib.nmf_run(A, W0, H0, "anlsbpp", 10)
+    assert np.all(np.diff(obj) <= 1e-9 * obj[0])
+    for j in range(0, 35, 7):
+        x, _ = nnls(W, A[:, j])
+        assert np.allclose(x, H[j], atol=1e-8 * np.abs(H).max())
+
+
+def test_oracle_nmf_regularized_objective(oracle_lib):
+    # HALS normalises by W before each error, so the returned factors are the
+    # ones the last objective was computed from (common/nmf.hpp:386-425)
+    A, W0, H0 = _nmf_problem(30, 30, 4, 73)
+    w2, w1, h2, h1 = 0.5, 0.1, 0.3, 0.2
+    W, H, obj, rel = oracle_lib.nmf_run(A, W0, H0, "hals", 3, reg=(w2, w1, h2, h1, 0.0))
+    fit = np.linalg.norm(A - W @ H.T) ** 2
+    ref = (fit + w2 * np.sum(W * W) + h2 * np.sum(H * H) + w1 * np.sum(W.sum(1) ** 2)
+           + h1 * np.sum(H.sum(1) ** 2))
+    assert abs(obj[-1] - ref) < 1e-9 * ref
