@@ -13,6 +13,7 @@ ROOT = os.path.dirname(HERE)
 SRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libplanc_gpu.so")
 DRIVER = os.path.join(HERE, "dense_ntf")
+DRIVERS = {"dense_ntf": "ntf.cpp", "dense_nmf": "nmf.cpp"}
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -64,19 +65,22 @@ def build(force=False, verbose=False):
 
 def driver_sources():
     cpp = os.path.join(HERE, "cpp")
-    return [os.path.join(cpp, "ntf.cpp")] + [
+    return [os.path.join(cpp, f) for f in DRIVERS.values()] + [
         os.path.join(cpp, "planc", f) for f in sorted(os.listdir(os.path.join(cpp, "planc")))]
 
 
 def build_driver(force=False):
-    """The dense_ntf command-line driver over the C++ API, linked to the library."""
-    if (not force and os.path.exists(DRIVER) and
-            all(os.path.getmtime(s) <= os.path.getmtime(DRIVER) for s in driver_sources() + [LIB])):
-        return DRIVER
-    cmd = ["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"),
-           "-I" + os.path.join(HERE, "cpp"), os.path.join(HERE, "cpp", "ntf.cpp"),
-           "-L" + HERE, "-lplanc_gpu", "-Wl,-rpath,$ORIGIN", "-o", DRIVER]
-    subprocess.run(cmd, check=True)
+    """The dense_ntf and dense_nmf command-line drivers over the C++ API,
+    linked to the library."""
+    for exe, src in DRIVERS.items():
+        out = os.path.join(HERE, exe)
+        if (not force and os.path.exists(out) and
+                all(os.path.getmtime(s) <= os.path.getmtime(out) for s in driver_sources() + [LIB])):
+            continue
+        cmd = ["g++", "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "include"),
+               "-I" + os.path.join(HERE, "cpp"), os.path.join(HERE, "cpp", src),
+               "-L" + HERE, "-lplanc_gpu", "-Wl,-rpath,$ORIGIN", "-o", out]
+        subprocess.run(cmd, check=True)
     return DRIVER
 
 

@@ -12,6 +12,7 @@
 #include <armadillo>
 #define MAT arma::mat
 #define VEC arma::vec
+#define FVEC arma::fvec
 #define UVEC arma::uvec
 #define UWORD arma::uword
 #else
@@ -120,6 +121,7 @@ T prod(const DenseMat<T>& v) {
 
 #define MAT planc::DenseMat<double>
 #define VEC planc::DenseMat<double>
+#define FVEC planc::DenseMat<float>
 #define UVEC planc::DenseMat<uint64_t>
 #define UWORD planc::uword
 #endif

@@ -21,6 +21,8 @@ enum algotype { MU, HALS, ANLSBPP, NAIVEANLSBPP, AOADMM, NESTEROV, CPALS, GNSYM,
 #define OUTPUT std::cout
 #endif
 
+typedef unsigned int UINT;  // common/utils.h:76
+
 // common/utils.h:46-49
 #define EPSILON_1EMINUS16 0.00000000000000001
 #define EPSILON_1EMINUS8 0.00000001

@@ -91,3 +91,34 @@ def test_dense_ntf_reads_npy(gpu, oracle_lib, tmp_path):
     Fo, lo, eo = oracle_lib.ntf_run(X, F0, "hals", iters)
     assert rel(np.array(errs), eo) < 1e-5
     assert all(rel(a, b) < 1e-10 for a, b in zip(_read_factors(out, 3), Fo))
+
+
+@pytest.mark.parametrize("algo,code", [("mu", 0), ("hals", 1), ("anlsbpp", 2)])
+def test_dense_nmf_driver_matches_oracle(gpu, oracle_lib, tmp_path, algo, code):
+    # the NMF classes of the C++ API (HALSNMF / MUNMF / BPPNMF) through the
+    # dense_nmf driver: A from a .npy file, W and H injected, L1/L2
+    # regularisation on both factors
+    exe = str(tmp_path / "dense_nmf")
+    _compile(os.path.join(PKG, "cpp", "nmf.cpp"), exe)
+    m, n, k, iters = 48, 36, 5, 7
+    rng = np.random.default_rng(64)
+    A = np.asfortranarray(rng.random((m, k)) @ rng.random((k, n)) + 0.01 * rng.random((m, n)))
+    src = str(tmp_path / "a.npy")
+    np.save(src, A)
+    W0, H0 = rng.random((m, k)), rng.random((n, k))
+    init, out = str(tmp_path / "init"), str(tmp_path / "out")
+    np.savetxt(init + "_W.txt", W0, fmt="%.17g")
+    np.savetxt(init + "_H.txt", H0, fmt="%.17g")
+    res = subprocess.run([exe, "-a", str(code), "-i", src, "-k", str(k), "-t", str(iters),
+                          "--init", init, "-o", out, "-r", "0.1 0.05 0.2 0.01"],
+                         capture_output=True, text=True, check=True)
+    rels = [float(x) for x in re.findall(r"relative error::([0-9.eE+-]+)", res.stdout)]
+    assert len(rels) == iters
+    # the regularisers are FVEC (float) in the API, as in the reference
+    # (common/nmf.hpp:49-50, 82, 88): the oracle gets the float values
+    regf = tuple(float(np.float32(x)) for x in (0.1, 0.05, 0.2, 0.01)) + (0.0,)
+    Wo, Ho, oo, ro = oracle_lib.nmf_run(A, W0, H0, algo, iters, reg=regf)
+    assert rel(np.array(rels), ro) < 1e-5  # printed with 6 significant digits
+    W = np.loadtxt(out + "_W", ndmin=2)
+    H = np.loadtxt(out + "_H", ndmin=2)
+    assert rel(W, Wo) < 1e-10 and rel(H, Ho) < 1e-10
