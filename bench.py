@@ -52,7 +52,7 @@ def parse():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--workload", default="cfg2",
-                    choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5", "updates"],
+                    choices=["cfg1", "cfg2", "cfg3", "cfg4", "cfg5", "updates", "nmf"],
                     help="cfg2 (default) is the metric's workload; the others are the remaining "
                          "synthetic configurations, measured with the same JSON contract")
     return ap.parse_args()

@@ -15,6 +15,10 @@ the bench.py JSON contract (python bench.py --workload cfgN ...):
   cfg5  512^3 BF16 CP loss 1/2||X - [[A,B,C]]||^2 (rank 32, 5 % noise),
         torch.autograd with the MTTKRP kernels as backward, projected
         accelerated gradient steps on the factor leaves.
+  nmf   shared-memory NMF of a dense 16384 x 16384 FP32 matrix (1.07 GB, rank-32
+        nonnegative model + 1 % noise): MU, HALS and ANLS/BPP, 20 iterations
+        each, A H and A^T W on tensor cores (BF16 copy of A) and on the FP64
+        plain path, from the same start.
   updates  the headline tensor (1024^3 FP32, rank-32 CP + 1 % noise) under
         every update of the solver family -- MU, HALS, ANLS/BPP, AO-ADMM and
         Nesterov (with its extrapolation step) -- 20 iterations each, BF16
@@ -294,12 +298,70 @@ def updates(args, gpu, torch, dev):
                  algorithms=algos)
 
 
+def nmf(args, gpu, torch, dev):
+    m, n, k, T = 16384, 16384, 32, 20
+    rng = np.random.default_rng(601)
+    A = [rng.random((m, k)), rng.random((n, k))]
+    X = _synth(gpu, torch, dev, (m, n), A, _sigma(A, 0.01), 61)
+    W0 = np.random.default_rng(602).random((m, k))
+    H0 = np.random.default_rng(603).random((n, k))
+    algos = {}
+    for algo in ("mu", "hals", "anlsbpp"):
+        row = {}
+        for prec in ("bf16", "fp64"):
+            with gpu.Context(dev, prec) as c:
+                c.set_tensor(X.data_ptr(), dims=(m, n), dtype="f32")
+                c.nmf_set_factors(W0, H0)
+                c.nmf_run(algo, max(args.warmup, 1))
+                c.nmf_set_factors(W0, H0)
+                stream = torch.cuda.ExternalStream(c.stream)
+                torch.cuda.synchronize()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                _, rel = c.nmf_run(algo, T)
+                e1.record(stream)
+                torch.cuda.synchronize()
+                ms = e0.elapsed_time(e1)
+                r = {"iters_per_s": T / (ms * 1e-3), "ms_per_iter": ms / T,
+                     "final_rel_error": float(rel[-1])}
+                if prec == "bf16":
+                    c.nmf_set_factors(W0, H0)
+                    c.set_timing(True)
+                    c.kernel_times()
+                    n0 = c.launch_count()
+                    c.nmf_run(algo, T)
+                    r["launches_per_iter"] = (c.launch_count() - n0) / T
+                    kt = c.kernel_times()
+                    c.set_timing(False)
+                    r["kernel_ms_per_iter"] = {kk: round(v[0] / T, 4) for kk, v in kt.items()
+                                               if v[1]}
+                    # A H (right, "contract") and A^T W (left, "contract_left"):
+                    # one pass over the BF16 copy of A each
+                    for cls in ("contract", "contract_left"):
+                        if kt[cls][1]:
+                            avg = kt[cls][0] / kt[cls][1] * 1e-3
+                            r["%s_gbs" % cls] = (m * n * 2 + max(m, n) * k * 8) / avg / 1e9
+                row[prec] = r
+        row["speedup_vs_fp64"] = row["fp64"]["ms_per_iter"] / row["bf16"]["ms_per_iter"]
+        row["final_error_abs_diff"] = abs(row["bf16"]["final_rel_error"] -
+                                          row["fp64"]["final_rel_error"])
+        algos[algo] = row
+    v = algos["hals"]["bf16"]["iters_per_s"]
+    return _line(args, 1, v, "iters/s", 1e3 / v, "bf16",
+                 {"workload": "NMF of a dense 16384x16384 FP32 matrix (rank-32 nonnegative model "
+                              "+ 1% noise), rank 32, 20 iterations of MU, HALS and ANLS/BPP, BF16 "
+                              "tensor-core A H / A^T W vs the FP64 plain path",
+                  "dims": [m, n], "rank": k},
+                 value_is="HALS iters/s, BF16", algorithms=algos)
+
+
 def run(args, rank, world, local):
     import torch
     import planc_b200 as gpu
     dev = local
     torch.cuda.set_device(dev)
-    fn = {"cfg1": cfg1, "cfg3": cfg3, "cfg4": cfg4, "cfg5": cfg5, "updates": updates}[args.workload]
+    fn = {"cfg1": cfg1, "cfg3": cfg3, "cfg4": cfg4, "cfg5": cfg5, "updates": updates,
+          "nmf": nmf}[args.workload]
     line = fn(args, gpu, torch, dev)
     if rank == 0:
         print(json.dumps(line))

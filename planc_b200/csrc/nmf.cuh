@@ -12,17 +12,42 @@
 
 namespace pg {
 
-// Gram U^T U from k_gram_partial's row-block partials, summed in block order,
-// plus NMF::applyReg (common/nmf.hpp:76-92: l2 I, then l1 ones) and an extra
-// diagonal shift (the symmetric regularisation of BPPNMF, common/nmf.hpp:
-// 118-124). One CTA.
-__global__ void __launch_bounds__(1024) k_nmf_gram(const double* __restrict__ part, int nblk, int k,
-                                                   double l2, double l1, double diag,
-                                                   double* __restrict__ out) {
+// Sum of v[i * stride] for i < n by a whole CTA in a fixed order: thread t
+// adds entries t, t + blockDim.x, ... and a fixed tree over the threads adds
+// the rest (sh: blockDim.x doubles, blockDim.x a power of two). Every thread
+// returns the total.
+__device__ __forceinline__ double cta_sum_fixed(const double* __restrict__ v, int n, int stride,
+                                                double* sh) {
+  double s = 0.0;
+  for (int i = threadIdx.x; i < n; i += blockDim.x) s += v[(int64_t)i * stride];
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x >> 1; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  const double t = sh[0];
+  __syncthreads();
+  return t;
+}
+
+// Gram U^T U from k_gram_partial's row-block partials plus NMF::applyReg
+// (common/nmf.hpp:76-92: l2 I, then l1 ones) and an extra diagonal shift (the
+// symmetric regularisation of BPPNMF, common/nmf.hpp:118-124). A warp per
+// entry: lane l adds partials l, l + 32, ... in order, then a fixed shuffle
+// tree adds the lanes. 8 entries per CTA.
+__global__ void __launch_bounds__(256) k_nmf_gram(const double* __restrict__ part, int nblk, int k,
+                                                  double l2, double l1, double diag,
+                                                  double* __restrict__ out) {
   const int kk2 = k * k;
-  for (int e = threadIdx.x; e < kk2; e += 1024) {
-    double s = 0.0;
-    for (int b = 0; b < nblk; ++b) s += part[(int64_t)b * kk2 + e];
+  const int lane = threadIdx.x & 31;
+  const int e = blockIdx.x * 8 + (threadIdx.x >> 5);
+  if (e >= kk2) return;
+  double s = 0.0;
+  for (int b = lane; b < nblk; b += 32) s += part[(int64_t)b * kk2 + e];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) {
     const bool d = (e / k) == (e % k);
     if (l2 > 0 && d) s = s + l2;
     if (l1 > 0) s = s + l1;
@@ -49,46 +74,68 @@ constexpr int NMFW_MAX_BLOCKS = 296;
 // is stored unnormalised and its squared norm summed (per CTA in warp order,
 // over CTAs in CTA order by the last CTA to finish, which writes norms[x]).
 // The sweep is launches x = 0 .. k; the last only finishes column k-1.
+constexpr int NMFW_ROWS = 4;  // rows of a warp whose loads are in flight together
+
 template <int KP>
 __global__ void __launch_bounds__(32 * NMFW_WARPS) k_nmf_hals_w(
     double* __restrict__ W, const double* __restrict__ AH, const double* __restrict__ G, int64_t m,
     int k, int x, double* __restrict__ norms, double* __restrict__ part, int* __restrict__ counter) {
   constexpr int PER = KP / 32;
   __shared__ double wred[NMFW_WARPS];
+  __shared__ double sh[32 * NMFW_WARPS];
   __shared__ int s_last;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const double nprev = x > 0 ? norms[x - 1] : 0.0;
+  double gx[PER];  // G(:, x) for this lane's columns
+#pragma unroll
+  for (int p = 0; p < PER; ++p) {
+    const int c = lane + 32 * p;
+    gx[p] = (x < k && c < k) ? G[c * k + x] : 0.0;
+  }
+  const double gxx = x < k ? G[x * k + x] : 0.0;
   double ss = 0.0;
-  for (int64_t row = (int64_t)blockIdx.x * NMFW_WARPS + warp; row < m;
-       row += (int64_t)gridDim.x * NMFW_WARPS) {
-    double w[PER];
+  const int64_t wstride = (int64_t)gridDim.x * NMFW_WARPS;
+  for (int64_t row0 = (int64_t)blockIdx.x * NMFW_WARPS + warp; row0 < m;
+       row0 += wstride * NMFW_ROWS) {
+    double w[NMFW_ROWS][PER], ah[NMFW_ROWS];
 #pragma unroll
-    for (int p = 0; p < PER; ++p) {
-      const int c = lane + 32 * p;
-      w[p] = c < k ? W[row * k + c] : 0.0;
-      if (c == x - 1 && nprev != 0) {
-        w[p] = w[p] / nprev;
-        W[row * k + c] = w[p];
+    for (int u = 0; u < NMFW_ROWS; ++u) {
+      const int64_t row = row0 + wstride * u;
+#pragma unroll
+      for (int p = 0; p < PER; ++p) {
+        const int c = lane + 32 * p;
+        w[u][p] = (row < m && c < k) ? W[row * k + c] : 0.0;
       }
+      ah[u] = (row < m && x < k) ? AH[row * k + x] : 0.0;
     }
-    if (x < k) {
-      // s = sum_j W(row, j) G(j, x), reduced across the warp in a fixed order
-      double s = 0.0;
+#pragma unroll
+    for (int u = 0; u < NMFW_ROWS; ++u) {
+      const int64_t row = row0 + wstride * u;
+      if (row >= m) continue;  // warp-uniform
 #pragma unroll
       for (int p = 0; p < PER; ++p) {
         const int c = lane + 32 * p;
-        if (c < k) s = fma(w[p], G[c * k + x], s);
+        if (c == x - 1 && nprev != 0) {
+          w[u][p] = w[u][p] / nprev;
+          W[row * k + c] = w[u][p];
+        }
       }
+      if (x < k) {
+        // s = sum_j W(row, j) G(j, x), reduced across the warp in a fixed order
+        double s = 0.0;
 #pragma unroll
-      for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        for (int p = 0; p < PER; ++p) s = fma(w[u][p], gx[p], s);
 #pragma unroll
-      for (int p = 0; p < PER; ++p) {
-        const int c = lane + 32 * p;
-        if (c == x) {
-          double v = (w[p] * G[x * k + x]) + (AH[row * k + x] - s);
-          v = (v < kEps17) ? kEps17 : v;
-          W[row * k + x] = v;
-          ss = fma(v, v, ss);
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+#pragma unroll
+        for (int p = 0; p < PER; ++p) {
+          const int c = lane + 32 * p;
+          if (c == x) {
+            double v = (w[u][p] * gxx) + (ah[u] - s);
+            v = (v < kEps17) ? kEps17 : v;
+            W[row * k + x] = v;
+            ss = fma(v, v, ss);
+          }
         }
       }
     }
@@ -106,10 +153,10 @@ __global__ void __launch_bounds__(32 * NMFW_WARPS) k_nmf_hals_w(
     s_last = atomicAdd(counter, 1) == (int)gridDim.x - 1;
   }
   __syncthreads();
-  if (s_last && threadIdx.x == 0) {
-    __threadfence();
-    double t = 0.0;
-    for (int b = 0; b < (int)gridDim.x; ++b) t += part[b];
+  if (!s_last) return;
+  __threadfence();
+  const double t = cta_sum_fixed(part, gridDim.x, 1, sh);
+  if (threadIdx.x == 0) {
     norms[x] = sqrt(t);
     *counter = 0;
   }
@@ -123,10 +170,17 @@ __global__ void __launch_bounds__(256) k_nmf_rescale(double* __restrict__ W, int
                                                      double* __restrict__ H, int64_t n, int k,
                                                      const double* __restrict__ part, int nblk) {
   __shared__ double nrm[kMaxRank];
-  if (threadIdx.x < k) {
-    double t = 0.0;
-    for (int b = 0; b < nblk; ++b) t += part[(int64_t)b * k + threadIdx.x];
-    nrm[threadIdx.x] = sqrt(t);
+  {
+    // a warp per column: lane l adds partials l, l + 32, ..., then a fixed
+    // shuffle tree
+    const int lane = threadIdx.x & 31;
+    for (int c = threadIdx.x >> 5; c < k; c += blockDim.x >> 5) {
+      double t = 0.0;
+      for (int b = lane; b < nblk; b += 32) t += part[(int64_t)b * k + c];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+      if (lane == 0) nrm[c] = sqrt(t);
+    }
   }
   __syncthreads();
   const int64_t row0 = (int64_t)blockIdx.x * NRM_ROWS;
@@ -152,65 +206,80 @@ struct NmfReg {
 //   objective = fit + regW(0) ||W||^2 + regH(0) ||H||^2
 //             + regW(1) ||W 1||^2 + regH(1) ||H 1||^2 + symm_reg ||W - H||^2
 // and the relative error sqrt(fit) / ||A|| (||A|| when fit <= 0,
-// common/nmf.hpp:428-431). Writes obj[*ctr], rel[*ctr] and increments *ctr.
-// One CTA of 1024 threads; every sum is in a fixed order.
-__global__ void __launch_bounds__(1024) k_nmf_error(const double* __restrict__ W, int64_t m,
-                                                    const double* __restrict__ H, int64_t n, int k,
-                                                    const double* __restrict__ AtW,
-                                                    const double* __restrict__ GW,
-                                                    const double* __restrict__ GH,
-                                                    const double* __restrict__ normA2, NmfReg reg,
-                                                    double* __restrict__ obj, double* __restrict__ rel,
-                                                    int* __restrict__ ctr) {
-  __shared__ double red[5][1024];
-  const int tid = threadIdx.x;
-  double tr = 0.0, l1w = 0.0, l1h = 0.0, sym = 0.0, ww = 0.0;
-  for (int64_t e = tid; e < n * k; e += 1024) tr = fma(H[e], AtW[e], tr);
-  // row sums: thread per row
-  for (int64_t r = tid; r < m; r += 1024) {
-    double s = 0.0;
-    for (int c = 0; c < k; ++c) s += W[r * k + c];
-    l1w = fma(s, s, l1w);
-  }
-  for (int64_t r = tid; r < n; r += 1024) {
-    double s = 0.0;
-    for (int c = 0; c < k; ++c) s += H[r * k + c];
-    l1h = fma(s, s, l1h);
-  }
-  if (reg.sym > 0)
-    for (int64_t e = tid; e < m * k; e += 1024) {
-      const double d = W[e] - H[e];
-      sym = fma(d, d, sym);
+// common/nmf.hpp:428-431). Each CTA sums its share of the row terms (a warp
+// per row, fixed order) into part[cta][4]; the last CTA to finish adds the
+// CTAs in order, writes obj[*ctr], rel[*ctr] and increments *ctr.
+constexpr int NMFE_WARPS = 8;
+__global__ void __launch_bounds__(32 * NMFE_WARPS) k_nmf_error(
+    const double* __restrict__ W, int64_t m, const double* __restrict__ H, int64_t n, int k,
+    const double* __restrict__ AtW, const double* __restrict__ GW, const double* __restrict__ GH,
+    const double* __restrict__ normA2, NmfReg reg, double* __restrict__ part,
+    int* __restrict__ ticket, double* __restrict__ obj, double* __restrict__ rel,
+    int* __restrict__ ctr) {
+  __shared__ double wred[NMFE_WARPS][4];
+  __shared__ double sh[32 * NMFE_WARPS];
+  __shared__ int s_last;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // q0: tr(H^T AtW), q1: ||W 1||^2, q2: ||H 1||^2, q3: ||W - H||^2
+  double q[4] = {0.0, 0.0, 0.0, 0.0};
+  const int64_t rows = m > n ? m : n;
+  for (int64_t r = (int64_t)blockIdx.x * NMFE_WARPS + warp; r < rows;
+       r += (int64_t)gridDim.x * NMFE_WARPS) {
+    double hw = 0.0, ws = 0.0, hs = 0.0, dd = 0.0;
+    for (int c = lane; c < k; c += 32) {
+      const double w = r < m ? W[r * k + c] : 0.0;
+      const double h = r < n ? H[r * k + c] : 0.0;
+      if (r < n) hw = fma(h, AtW[r * k + c], hw);
+      ws += w;
+      hs += h;
+      if (reg.sym > 0 && r < m && r < n) dd = fma(w - h, w - h, dd);
     }
-  for (int e = tid; e < k * k; e += 1024) ww = fma(GW[e], GH[(e % k) * k + e / k], ww);
-  red[0][tid] = tr;
-  red[1][tid] = l1w;
-  red[2][tid] = l1h;
-  red[3][tid] = sym;
-  red[4][tid] = ww;
-  __syncthreads();
-  for (int s = 512; s > 0; s >>= 1) {
-    if (tid < s)
 #pragma unroll
-      for (int q = 0; q < 5; ++q) red[q][tid] += red[q][tid + s];
-    __syncthreads();
-  }
-  if (tid == 0) {
-    double fro_w = 0.0, fro_h = 0.0;
-    for (int i = 0; i < k; ++i) {
-      fro_w += GW[i * k + i];
-      fro_h += GH[i * k + i];
+    for (int o = 16; o > 0; o >>= 1) {
+      hw += __shfl_xor_sync(0xffffffffu, hw, o);
+      ws += __shfl_xor_sync(0xffffffffu, ws, o);
+      hs += __shfl_xor_sync(0xffffffffu, hs, o);
+      dd += __shfl_xor_sync(0xffffffffu, dd, o);
     }
-    const double a2 = *normA2;
-    const double fit = a2 - (2 * red[0][0]) + red[4][0];
-    const double o = fit + reg.w2 * fro_w + reg.h2 * fro_h + reg.w1 * red[1][0] +
-                     reg.h1 * red[2][0] + (reg.sym > 0 ? reg.sym * red[3][0] : 0.0);
-    const double na = sqrt(a2);
-    const int c = *ctr;
-    obj[c] = o;
-    rel[c] = (fit > 0 ? sqrt(fit) : na) / na;
-    *ctr = c + 1;
+    q[0] += hw;
+    q[1] = fma(ws, ws, q[1]);
+    q[2] = fma(hs, hs, q[2]);
+    q[3] += dd;
   }
+  if (lane == 0)
+#pragma unroll
+    for (int i = 0; i < 4; ++i) wred[warp][i] = q[i];
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int w = 0; w < NMFE_WARPS; ++w)
+      for (int i = 0; i < 4; ++i) t[i] += wred[w][i];
+    for (int i = 0; i < 4; ++i) part[blockIdx.x * 4 + i] = t[i];
+    __threadfence();
+    s_last = atomicAdd(ticket, 1) == (int)gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  double t[4];
+  for (int i = 0; i < 4; ++i) t[i] = cta_sum_fixed(part + i, gridDim.x, 4, sh);
+  if (threadIdx.x != 0) return;
+  double ww = 0.0, fro_w = 0.0, fro_h = 0.0;
+  for (int a = 0; a < k; ++a) {
+    fro_w += GW[a * k + a];
+    fro_h += GH[a * k + a];
+    for (int b = 0; b < k; ++b) ww = fma(GW[a * k + b], GH[b * k + a], ww);
+  }
+  const double a2 = *normA2;
+  const double fit = a2 - (2 * t[0]) + ww;
+  const double o = fit + reg.w2 * fro_w + reg.h2 * fro_h + reg.w1 * t[1] + reg.h1 * t[2] +
+                   (reg.sym > 0 ? reg.sym * t[3] : 0.0);
+  const double na = sqrt(a2);
+  const int c = *ctr;
+  obj[c] = o;
+  rel[c] = (fit > 0 ? sqrt(fit) : na) / na;
+  *ctr = c + 1;
+  *ticket = 0;
 }
 
 }  // namespace pg

@@ -2161,7 +2161,7 @@ void ensure_nmf(planc_gpu_ctx* c, int iters) {
     c->nmf_part_elems = std::max<size_t>(
         std::max<size_t>((size_t)((maxI + GP_ROWS - 1) / GP_ROWS) * k * k,
                          (size_t)((maxI + CN_ROWS - 1) / CN_ROWS) * k),
-        NMFW_MAX_BLOCKS);
+        (size_t)NMFW_MAX_BLOCKS * 4);
     dalloc(&c->nmf_part, c->nmf_part_elems);
     dalloc(&c->nmf_ctr, 2);
     CK(cudaMemset(c->nmf_ctr, 0, 2 * sizeof(int)));
@@ -2187,7 +2187,8 @@ void nmf_gram(planc_gpu_ctx* c, const double* U, int64_t I, double l2, double l1
     k_gram_partial<<<nblk, 256, 0, c->stream>>>(U, I, k, rpb, c->nmf_part);
   });
   launch(c, KC_NORMGRAM, [&] {
-    k_nmf_gram<<<1, 1024, 0, c->stream>>>(c->nmf_part, nblk, k, l2, l1, diag, out);
+    k_nmf_gram<<<(unsigned)((k * k + 7) / 8), 256, 0, c->stream>>>(c->nmf_part, nblk, k, l2, l1,
+                                                                  diag, out);
   });
 }
 
@@ -2278,10 +2279,12 @@ void nmf_error(planc_gpu_ctx* c) {
   nmf_gram(c, c->F[0], m, 0, 0, 0, c->nmf_GW);
   nmf_gram(c, c->F[1], n, 0, 0, 0, c->nmf_GH);
   NmfReg reg{c->nmf_reg[0], c->nmf_reg[1], c->nmf_reg[2], c->nmf_reg[3], c->nmf_reg[4]};
+  const unsigned nb =
+      (unsigned)std::min<int64_t>((std::max(m, n) + NMFE_WARPS - 1) / NMFE_WARPS, NMFW_MAX_BLOCKS);
   launch(c, KC_ERROR, [&] {
-    k_nmf_error<<<1, 1024, 0, c->stream>>>(c->F[0], m, c->F[1], n, c->k, c->M[1], c->nmf_GW,
-                                          c->nmf_GH, c->normX2, reg, c->nmf_obj, c->nmf_rel,
-                                          c->nmf_ctr);
+    k_nmf_error<<<nb, 32 * NMFE_WARPS, 0, c->stream>>>(
+        c->F[0], m, c->F[1], n, c->k, c->M[1], c->nmf_GW, c->nmf_GH, c->normX2, reg,
+        c->nmf_part, c->nmf_ctr + 1, c->nmf_obj, c->nmf_rel, c->nmf_ctr);
   });
 }
 

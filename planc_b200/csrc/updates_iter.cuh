@@ -211,11 +211,24 @@ __global__ void __launch_bounds__(32 * ADMM_WARPS) k_admm_step(
     s_last = atomicAdd(counter, 1) == (int)gridDim.x - 1;
   }
   __syncthreads();
-  if (s_last && threadIdx.x == 0) {
-    __threadfence();
-    double t[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int b = 0; b < (int)gridDim.x; ++b)
-      for (int q = 0; q < 4; ++q) t[q] += part[b * 4 + q];
+  if (!s_last) return;
+  __threadfence();
+  // the last CTA adds the CTAs' partials, in parallel and in a fixed order
+  __shared__ double sh[32 * ADMM_WARPS];
+  double t[4];
+  for (int q = 0; q < 4; ++q) {
+    double v = 0.0;
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) v += part[b * 4 + q];
+    sh[threadIdx.x] = v;
+    __syncthreads();
+    for (int o = blockDim.x >> 1; o > 0; o >>= 1) {
+      if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+      __syncthreads();
+    }
+    t[q] = sh[0];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
     const double facnorm = sqrt(t[0]), dualnorm = sqrt(t[1]);
     const double r = sqrt(t[2]), s = sqrt(t[3]);
     *flag = (r < tol * facnorm && s < tol * dualnorm) ? 1 : 0;
