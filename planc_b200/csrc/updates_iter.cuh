@@ -531,7 +531,7 @@ __global__ void __launch_bounds__(256) k_nes_prep(const double* __restrict__ G, 
   __shared__ int s_rot;
   const int tid = threadIdx.x;
   if (mode == 0 && tid < k) prev_lam[tid] = prox_lam[tid];
-  for (int e = tid; e < k * k; e += 256) A[(e / k) * LD + e % k] = G[e];
+  for (int e = tid; e < k * k; e += blockDim.x) A[(e / k) * LD + e % k] = G[e];
   __syncthreads();
   const int n2 = (k + 1) & ~1;  // even player count of the round-robin
   const int np = n2 / 2;
@@ -570,30 +570,39 @@ __global__ void __launch_bounds__(256) k_nes_prep(const double* __restrict__ G, 
         rs[tid] = s;
       }
       __syncthreads();
-      // rows: A <- J^T A
-      for (int e = tid; e < np * k; e += 256) {
-        const int pr = e / k, j = e % k;
-        const int p = rp[pr], q = rq[pr];
-        const double s = rs[pr];
-        if (q < k && s != 0.0) {
-          const double c = rc[pr];
-          const double ap = A[p * LD + j], aq = A[q * LD + j];
-          A[p * LD + j] = c * ap - s * aq;
-          A[q * LD + j] = s * ap + c * aq;
+      // A <- J^T A J in one pass: the rotations are disjoint, so every 2 x 2
+      // block (pair pi's rows, pair pj's columns) changes only through its own
+      // four entries; a thread rotates its block's rows, then its columns (the
+      // same operations as a row pass followed by a column pass)
+      for (int blk = tid; blk < np * np; blk += blockDim.x) {
+        const int pi = blk / np, pj = blk % np;
+        const int p1 = rp[pi], q1 = rq[pi], p2 = rp[pj], q2 = rq[pj];
+        const double s1 = rs[pi], s2 = rs[pj];
+        if (s1 == 0.0 && s2 == 0.0) continue;
+        const double c1 = rc[pi], c2 = rc[pj];
+        const bool q1ok = q1 < k, q2ok = q2 < k;
+        const double a11 = A[p1 * LD + p2];
+        const double a12 = q2ok ? A[p1 * LD + q2] : 0.0;
+        const double a21 = q1ok ? A[q1 * LD + p2] : 0.0;
+        const double a22 = (q1ok && q2ok) ? A[q1 * LD + q2] : 0.0;
+        double r11 = a11, r12 = a12, r21 = a21, r22 = a22;
+        if (s1 != 0.0) {
+          r11 = c1 * a11 - s1 * a21;
+          r21 = s1 * a11 + c1 * a21;
+          r12 = c1 * a12 - s1 * a22;
+          r22 = s1 * a12 + c1 * a22;
         }
-      }
-      __syncthreads();
-      // columns: A <- A J
-      for (int e = tid; e < np * k; e += 256) {
-        const int pr = e / k, j = e % k;
-        const int p = rp[pr], q = rq[pr];
-        const double s = rs[pr];
-        if (q < k && s != 0.0) {
-          const double c = rc[pr];
-          const double ap = A[j * LD + p], aq = A[j * LD + q];
-          A[j * LD + p] = c * ap - s * aq;
-          A[j * LD + q] = s * ap + c * aq;
+        double o11 = r11, o12 = r12, o21 = r21, o22 = r22;
+        if (s2 != 0.0) {
+          o11 = c2 * r11 - s2 * r12;
+          o12 = s2 * r11 + c2 * r12;
+          o21 = c2 * r21 - s2 * r22;
+          o22 = s2 * r21 + c2 * r22;
         }
+        A[p1 * LD + p2] = o11;
+        if (q2ok) A[p1 * LD + q2] = o12;
+        if (q1ok) A[q1 * LD + p2] = o21;
+        if (q1ok && q2ok) A[q1 * LD + q2] = o22;
       }
       __syncthreads();
     }

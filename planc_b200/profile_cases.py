@@ -16,6 +16,11 @@ larger than the 126 MB L2 (DRAM counters stay meaningful):
           128^4 FP32 tensor (BF16 copy), rank 64, HALS iterations
   cfg3it  three ANLS/BPP iterations of the 192^4 rank-64 workload (BF16), for
           a one-pass launch list at full size
+  nmf     shared-memory NMF of a dense 16384 x 16384 FP32 matrix (BF16 copy),
+          rank 32: three iterations each of MU, HALS and ANLS/BPP
+  upd     AO-ADMM and Nesterov NTF updates on the 1024^3 rank-32 headline
+          tensor (BF16 copy): three iterations each (Nesterov's extrapolation
+          runs from the sixth iteration of a call, so it is off here)
   ttv     the multi-TTVs of the 3-way tensor-core path with the headline's
           intermediate: 1024 x 1024 x 64 FP32 tensor (BF16 copy), rank 32, so
           the FP32 partial MTTKRP P is 1024*1024 x 32 (134 MB > L2)
@@ -120,8 +125,42 @@ def case_ttv(gpu, torch):
           ", ".join("%s %.1f us" % (n, 1e3 * v[0] / 3) for n, v in kt.items() if v[1]))
 
 
+def case_nmf(gpu, torch):
+    m, n, k = 16384, 16384, 32
+    rng = np.random.default_rng(601)
+    A = [rng.random((m, k)), rng.random((n, k))]
+    G = (A[0].T @ A[0]) * (A[1].T @ A[1])
+    sigma = 0.01 * np.sqrt(G.sum() / float(m * n))
+    X = torch.empty(m * n, dtype=torch.float32, device="cuda:0")
+    gpu.synth_cp_tensor(0, X.data_ptr(), "f32", (m, n), A, sigma, 61, clip=True)
+    W0 = np.random.default_rng(602).random((m, k))
+    H0 = np.random.default_rng(603).random((n, k))
+    out = []
+    with gpu.Context(0, "bf16") as c:
+        c.set_tensor(X.data_ptr(), dims=(m, n), dtype="f32")
+        for algo in ("mu", "hals", "anlsbpp"):
+            c.nmf_set_factors(W0, H0)
+            ms = _timed(torch, c, lambda: c.nmf_run(algo, 1), 3)
+            out.append("%s %.3f ms" % (algo, ms))
+    print("nmf: 16384^2 k=32 per iteration: " + ", ".join(out))
+
+
+def case_upd(gpu, torch):
+    dims, k = (1024, 1024, 1024), 32
+    X, F0 = _synth(gpu, torch, dims, k, 51)
+    out = []
+    with gpu.Context(0, "bf16") as c:
+        c.set_tensor(X.data_ptr(), dims=dims, dtype="f32")
+        for algo in ("aoadmm", "nesterov"):
+            c.set_factors(F0)
+            c.reset_update_state()
+            ms = _timed(torch, c, lambda: c.run(algo, 1), 3)
+            out.append("%s %.3f ms" % (algo, ms))
+    print("upd: 1024^3 k=32 per iteration: " + ", ".join(out))
+
+
 CASES = {"bpp": case_bpp, "tc3": case_tc3, "tc4": case_tc4, "cfg3it": case_cfg3it,
-         "ttv": case_ttv}
+         "ttv": case_ttv, "nmf": case_nmf, "upd": case_upd}
 
 
 def main(argv):
