@@ -410,6 +410,8 @@ void ensure_buffers_impl(planc_gpu_ctx* c) {
     need = std::max(need, contract_scratch(pr));
     TtvRightPlan tr = plan_ttv_right(c, c->dims[0], c->L / c->dims[0]);
     need = std::max(need, (size_t)tr.nsplit * c->dims[0] * k);
+    if (c->N == 3 && c->precision != PLANC_GPU_PREC_FP64)
+      need = std::max(need, (size_t)tc_right_ttv_nsplit(c->tct, k, eff_sm(c)) * c->dims[0] * k);
     if (c->N == 4) {
       TtvRightPlan t2 = plan_ttv_right(c, c->dims[1], c->dims[2]);
       need = std::max(need, (size_t)t2.nsplit * c->dims[1] * k);
@@ -625,6 +627,22 @@ void mttkrp_dimtree(planc_gpu_ctx* c, int n, double* out) {
   const int N = c->N;
   const bool f64 = c->precision == PLANC_GPU_PREC_FP64;
   if (n == 0) {
+    if (!f64 && N == 3) {
+      const int ns = tc_right_ttv_nsplit(c->tct, c->k, eff_sm(c));
+      if (ns > 0 && (size_t)ns * c->dims[0] * c->k <= c->scratch_elems) {
+        // P = X F_2 with M_0 = TTV(P, F_1) formed in the same pass
+        launch(c, KC_PREP, [&] { tc_right_prep(c->tct, c->F[2], c->k, c->stream); });
+        launch(c, KC_CONTRACT, [&] {
+          tc_right_ttv(c->tct, c->k, c->P32, c->F[1], c->scratch, c->status_dev, eff_sm(c),
+                       c->stream);
+        });
+        const int64_t nn = c->dims[0] * c->k;
+        launch(c, KC_REDUCE, [&] {
+          k_reduce_splits<<<reduce_grid(nn), 256, 0, c->stream>>>(c->scratch, ns, nn, nn, out);
+        });
+        return;
+      }
+    }
     partial_right(c);
     std::vector<int> modes;
     for (int m = 1; m <= c->s; ++m) modes.push_back(m);

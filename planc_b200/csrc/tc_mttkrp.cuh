@@ -248,11 +248,20 @@ constexpr int TC_THREADS = 192;  // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue /
 
 // ------------------------------------------------------------ right kernel
 // P32[l*k + r] = sum_j X[l, j] * F[j, r], l < L, r < k.
-template <int KP, bool X2>
+// With TTV (3-way tree, I0 a multiple of 128, gridDim a multiple of
+// tpb = I0 / 128) the epilogue also forms the mode-0 multi-TTV of the tiles
+// it drains: tile t covers rows l = i0 + I0 * i1 with i1 = t / tpb and
+// i0 = (t % tpb) * 128 + row, and t % tpb = blockIdx % tpb for every tile of
+// a CTA, so each epilogue thread keeps one i0's sums
+//   sum_{i1 of its tiles} P[i0 + I0 i1, r] * F1[i1, r]   (FP64)
+// and writes them to part[blockIdx / tpb][i0][r]; k_reduce_splits adds the
+// gridDim / tpb partials into M_0 (the sum k_ttv_right_tiled forms from P).
+template <int KP, bool X2, bool TTV = false>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_tc_right(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
                const uint8_t* __restrict__ bimg, int64_t L, int64_t R, int k, int stages,
-               float* __restrict__ P, int* __restrict__ status) {
+               float* __restrict__ P, int* __restrict__ status, const double* __restrict__ F1 = nullptr,
+               int tpb = 1, int64_t I0 = 0, double* __restrict__ part = nullptr) {
   constexpr int NCOL = 2 * KP;                       // hi | lo columns
   constexpr uint32_t A_BYTES = TC_BM * TC_BK * 2;    // one BF16 A tile
   constexpr uint32_t A_STAGE = X2 ? 2 * A_BYTES : A_BYTES;
@@ -356,6 +365,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const int q = warp & 3;
     int buf = 0;
     uint32_t aph = 0;
+    double tacc[TTV ? KP : 1];
+#pragma unroll
+    for (int r = 0; r < (TTV ? KP : 1); ++r) tacc[r] = 0.0;
     for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
       if (!mbar_wait(accf(buf), (aph >> buf) & 1, abort_flag, status)) break;
       tc_fence_after();
@@ -383,7 +395,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
           for (int r = 0; r < KP; ++r)
             if (r < k) dst[r] = v[r] + v[KP + r];
         }
+        if constexpr (TTV) {
+          const double* f = F1 + (t / tpb) * k;
+#pragma unroll
+          for (int r = 0; r < KP; ++r)
+            if (r < k) tacc[r] = fma((double)(v[r] + v[KP + r]), f[r], tacc[r]);
+        }
       }
+    }
+    if constexpr (TTV) {
+      const int64_t i0 = (int64_t)(blockIdx.x % tpb) * TC_BM + q * 32 + lane;
+      double* dst = part + (int64_t)(blockIdx.x / tpb) * I0 * k + i0 * k;
+#pragma unroll
+      for (int r = 0; r < KP; ++r)
+        if (r < k) dst[r] = tacc[r];
     }
   }
   __syncthreads();
@@ -1332,6 +1357,9 @@ inline cudaError_t tc_set_attrs() {
   constexpr uint32_t SL2 = (X2 ? 2 : 1) * 2 * TC_BM * TC_BK * 2 + 2 * KP * 128;
   cudaError_t e = cudaFuncSetAttribute(k_tc_right<KP, X2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)(tc_stages(SR) * SR + 1024));
+  if (e == cudaSuccess && KP <= 32)
+    e = cudaFuncSetAttribute(k_tc_right<KP, X2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(tc_stages(SR) * SR + 1024));
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_tc_left<KP, 1, X2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(tc_stages(SL1) * SL1 + 1024));
@@ -1415,6 +1443,50 @@ inline void tc_right_launch(const TcTensor& t, int k, float* P, int* status, int
   const int grid = (int)std::min<int64_t>(ntiles, sm_count);
   k_tc_right<KP, X2><<<grid, TC_THREADS, smem, st>>>(t.mR_hi, t.mR_lo, t.bimg, t.L, t.R, k, stages,
                                                      P, status);
+}
+
+// Whether the mode-0 multi-TTV can ride on the right contraction: 3-way
+// tree with I0 a multiple of 128 (tiles never straddle an i1), rank <= 32,
+// and at least one CTA per i0 block.
+inline int tc_right_ttv_tpb(const TcTensor& t, int k, int sm_count) {
+  if (k > 32 || t.I0 <= 0 || t.I0 % TC_BM != 0) return 0;
+  const int64_t tpb = t.I0 / TC_BM;
+  if (tpb > sm_count || t.L % t.I0 != 0) return 0;
+  return (int)tpb;
+}
+// Partials it writes (nsplit x I0 x k), and nsplit.
+inline int tc_right_ttv_nsplit(const TcTensor& t, int k, int sm_count) {
+  const int tpb = tc_right_ttv_tpb(t, k, sm_count);
+  if (!tpb) return 0;
+  const int64_t ntiles = (t.L + TC_BM - 1) / TC_BM;
+  const int64_t grid = std::min<int64_t>(ntiles, sm_count) / tpb * tpb;
+  return (int)(grid / tpb);
+}
+
+template <int KP, bool X2>
+inline void tc_right_ttv_launch(const TcTensor& t, int k, float* P, const double* F1, double* part,
+                                int* status, int sm_count, cudaStream_t st) {
+  constexpr uint32_t STAGE = (X2 ? 2 : 1) * TC_BM * TC_BK * 2 + 2 * KP * 128;
+  const int stages = tc_stages(STAGE);
+  const size_t smem = (size_t)stages * STAGE + 1024;
+  const int tpb = tc_right_ttv_tpb(t, k, sm_count);
+  const int grid = tc_right_ttv_nsplit(t, k, sm_count) * tpb;
+  k_tc_right<KP, X2, true><<<grid, TC_THREADS, smem, st>>>(t.mR_hi, t.mR_lo, t.bimg, t.L, t.R, k,
+                                                           stages, P, status, F1, tpb, t.I0, part);
+}
+
+// P32 = X * F_{N-1} and the mode-0 multi-TTV partials against F1
+// (tc_right_ttv_tpb(...) != 0; call tc_right_prep first). Returns nsplit.
+inline int tc_right_ttv(const TcTensor& t, int k, float* P, const double* F1, double* part,
+                        int* status, int sm_count, cudaStream_t st) {
+  const bool x2 = t.prec == 2;
+  if (tc_kpad(k) == 16)
+    x2 ? tc_right_ttv_launch<16, true>(t, k, P, F1, part, status, sm_count, st)
+       : tc_right_ttv_launch<16, false>(t, k, P, F1, part, status, sm_count, st);
+  else
+    x2 ? tc_right_ttv_launch<32, true>(t, k, P, F1, part, status, sm_count, st)
+       : tc_right_ttv_launch<32, false>(t, k, P, F1, part, status, sm_count, st);
+  return tc_right_ttv_nsplit(t, k, sm_count);
 }
 
 // P32 = X * F_{N-1} on the tensor cores (call tc_right_prep first).

@@ -110,3 +110,34 @@ def test_tc_4way_ntf_matches_fp64_error(gpu, prec):
             c.set_factors(F0)
             errs[p] = c.run("hals", iters)
     assert abs(errs[prec][-1] - errs["fp64"][-1]) < 1e-4, (errs[prec][-1], errs["fp64"][-1])
+
+
+@pytest.mark.parametrize("prec", ["bf16", "bf16x2"])
+@pytest.mark.parametrize("dims,k", [((256, 40, 50), 16), ((512, 30, 20), 32), ((384, 17, 23), 24),
+                                    ((128, 9, 31), 5)])
+def test_tc_mode0_ttv_in_right_contraction(gpu, oracle_lib, prec, dims, k):
+    # 3-way tensors whose mode 0 is a multiple of 128 form the mode-0
+    # multi-TTV inside the right contraction's epilogue (per-CTA partials
+    # reduced in order) instead of re-reading P
+    X, _ = cp_tensor(dims, 4, seed=28)
+    F = init_factors(dims, k, seed=29)
+    Fn = _normalized(F)
+    with gpu.Context(0, prec) as c:
+        c.set_tensor(X)
+        c.set_factors(F)
+        for n in range(3):
+            ref = oracle_lib.mttkrp_direct(X, Fn, n)
+            assert rel(c.mttkrp(n, dimtree=True), ref) < BOUND[prec], n
+
+
+def test_tc_ntf_fused_ttv_matches_fp64_error(gpu):
+    dims, k, iters = (256, 64, 48), 8, 15
+    X, _ = cp_tensor(dims, k, noise=0.01, seed=30)
+    F0 = init_factors(dims, k, seed=31)
+    errs = {}
+    for p in ("fp64", "bf16x2"):
+        with gpu.Context(0, p) as c:
+            c.set_tensor(X if p == "fp64" else X.astype(np.float32))
+            c.set_factors(F0)
+            errs[p] = c.run("hals", iters)
+    assert abs(errs["bf16x2"][-1] - errs["fp64"][-1]) < 1e-4
