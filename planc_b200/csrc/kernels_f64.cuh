@@ -214,6 +214,33 @@ inline unsigned reduce_grid(int64_t n) {
   return (unsigned)(b < 1 ? 1 : (b > 8192 ? 8192 : b));
 }
 
+// k_reduce_splits for nsplit <= 8: a thread per output, coalesced across the
+// warp, adding the partials with the same pairwise tree the eight lanes of
+// k_reduce_splits form ((p0 + p1) + (p2 + p3)) + ((p4 + p5) + (p6 + p7)),
+// absent partials reading as 0, so both kernels give the same bits.
+__global__ void __launch_bounds__(256) k_reduce_splits_few(const double* __restrict__ part,
+                                                           int nsplit, int64_t stride, int64_t n,
+                                                           double* __restrict__ out) {
+  for (int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256) {
+    double v[8];
+#pragma unroll
+    for (int p = 0; p < 8; ++p) v[p] = p < nsplit ? part[p * stride + i] : 0.0;
+    out[i] = ((v[0] + v[1]) + (v[2] + v[3])) + ((v[4] + v[5]) + (v[6] + v[7]));
+  }
+}
+
+// out[i] = sum over the nsplit partials part[p * stride + i], i < n.
+inline void reduce_splits(cudaStream_t st, const double* part, int nsplit, int64_t stride,
+                          int64_t n, double* out) {
+  if (nsplit <= 8) {
+    const int64_t b = (n + 255) / 256;
+    k_reduce_splits_few<<<(unsigned)(b < 1 ? 1 : (b > 4096 ? 4096 : b)), 256, 0, st>>>(
+        part, nsplit, stride, n, out);
+  } else {
+    k_reduce_splits<<<reduce_grid(n), 256, 0, st>>>(part, nsplit, stride, n, out);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Multi-TTV on a row-major (A*B) x k intermediate T (rank index fastest),
 // dimtree/dimtrees.hpp:315-410:

@@ -16,6 +16,20 @@ namespace pg {
 // adds entries t, t + blockDim.x, ... and a fixed tree over the threads adds
 // the rest (sh: blockDim.x doubles, blockDim.x a power of two). Every thread
 // returns the total.
+// Sum of one value per thread over the CTA by a fixed tree (sh: blockDim.x
+// doubles, blockDim.x a power of two). Every thread returns the total.
+__device__ __forceinline__ double cta_tree_fixed(double s, double* sh) {
+  sh[threadIdx.x] = s;
+  __syncthreads();
+  for (int o = blockDim.x >> 1; o > 0; o >>= 1) {
+    if (threadIdx.x < o) sh[threadIdx.x] += sh[threadIdx.x + o];
+    __syncthreads();
+  }
+  const double t = sh[0];
+  __syncthreads();
+  return t;
+}
+
 __device__ __forceinline__ double cta_sum_fixed(const double* __restrict__ v, int n, int stride,
                                                 double* sh) {
   double s = 0.0;
@@ -162,26 +176,56 @@ __global__ void __launch_bounds__(32 * NMFW_WARPS) k_nmf_hals_w(
   }
 }
 
-// NMF::normalize_by_W (common/nmf.hpp:150-160) from k_colsumsq_partial's
-// per-CTA column sums of W^2: every CTA adds the partials in CTA order, then
-// W(:, c) /= norm_c and H(:, c) *= norm_c (norm_c > 0) over its rows.
+// NMF::normalize_by_W (common/nmf.hpp:150-160), first launch: per-CTA column
+// sums of W^2 over NRM_ROWS rows; the last CTA to finish adds the CTAs'
+// partials in CTA order (a warp per column: lane l adds partials l, l + 32,
+// ..., then a fixed shuffle tree) and writes norms[c] = ||W(:, c)||.
 constexpr int NRM_ROWS = 64;
+__global__ void __launch_bounds__(256) k_nmf_colnorms(const double* __restrict__ W, int64_t m,
+                                                      int k, double* __restrict__ part,
+                                                      int* __restrict__ ticket,
+                                                      double* __restrict__ norms) {
+  __shared__ double red[256];
+  __shared__ int s_last;
+  const int tid = threadIdx.x;
+  const int lanes = 256 / k;  // threads per column
+  const int c = tid % k, l = tid / k;
+  const int64_t row0 = (int64_t)blockIdx.x * NRM_ROWS;
+  double s = 0.0;
+  if (l < lanes)
+    for (int64_t i = row0 + l; i < m && i < row0 + NRM_ROWS; i += lanes)
+      s = fma(W[i * k + c], W[i * k + c], s);
+  red[tid] = s;
+  __syncthreads();
+  if (tid < k) {
+    double t = 0.0;
+    for (int q = 0; q < lanes; ++q) t += red[q * k + tid];
+    part[(int64_t)blockIdx.x * k + tid] = t;
+  }
+  __threadfence();
+  __syncthreads();
+  if (tid == 0) s_last = atomicAdd(ticket, 1) == (int)gridDim.x - 1;
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  const int lane = tid & 31;
+  for (int cc = tid >> 5; cc < k; cc += 8) {
+    double t = 0.0;
+    for (int b = lane; b < (int)gridDim.x; b += 32) t += __ldcg(part + (int64_t)b * k + cc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0) norms[cc] = sqrt(t);
+  }
+  if (tid == 0) *ticket = 0;
+}
+
+// Second launch: W(:, c) /= norm_c and H(:, c) *= norm_c (norm_c > 0) over
+// NRM_ROWS rows of each.
 __global__ void __launch_bounds__(256) k_nmf_rescale(double* __restrict__ W, int64_t m,
                                                      double* __restrict__ H, int64_t n, int k,
-                                                     const double* __restrict__ part, int nblk) {
+                                                     const double* __restrict__ norms) {
   __shared__ double nrm[kMaxRank];
-  {
-    // a warp per column: lane l adds partials l, l + 32, ..., then a fixed
-    // shuffle tree
-    const int lane = threadIdx.x & 31;
-    for (int c = threadIdx.x >> 5; c < k; c += blockDim.x >> 5) {
-      double t = 0.0;
-      for (int b = lane; b < nblk; b += 32) t += part[(int64_t)b * k + c];
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
-      if (lane == 0) nrm[c] = sqrt(t);
-    }
-  }
+  if (threadIdx.x < k) nrm[threadIdx.x] = norms[threadIdx.x];
   __syncthreads();
   const int64_t row0 = (int64_t)blockIdx.x * NRM_ROWS;
   for (int64_t e = threadIdx.x; e < (int64_t)NRM_ROWS * k; e += 256) {
@@ -193,6 +237,167 @@ __global__ void __launch_bounds__(256) k_nmf_rescale(double* __restrict__ W, int
       if (row < n) H[row * k + c] = H[row * k + c] * v;
     }
   }
+}
+
+// ---------------------------------------------------------------------------
+// HALSNMF's W sweep in one cooperative launch (nmf/hals.hpp:92-105)
+// ---------------------------------------------------------------------------
+// Each CTA keeps its block of W's rows in shared memory for the whole sweep
+// (a thread per row, up to NMFC_RPT rows a thread). For column x every thread
+// forms, for its rows,
+//   Wx = W(:,x) HtH(x,x) + (AH(:,x) - W HtH(:,x)),  entries < 1e-17 -> 1e-17
+// the CTA adds its squares in a fixed order and stores the sum in
+// part[x][cta]; every CTA then waits until all CTAs' sums of column x are
+// there, adds them in the same fixed order and divides column x by ||Wx||, so
+// all CTAs see the same normalised column before column x + 1 reads it.
+//
+// part[x][*] is filled with the bit pattern NMFC_EMPTY (all ones, a NaN no
+// arithmetic here produces; a sum with those bits is stored as another NaN)
+// before the launch; a slot holds a CTA's sum once it reads otherwise. While
+// warp 0 waits, every thread forms W HtH(:, x+1) of its rows without the
+// term of column x, which it adds once ||Wx|| is known. The waits are
+// bounded: after NMFC_SPINS polls a CTA sets an error flag (flag[0]) and
+// kStTimeout and returns, and waiting CTAs leave when they see the flag, so
+// the launch always ends. The launch is cooperative (all CTAs resident).
+constexpr int NMFC_THREADS = 256;
+constexpr int NMFC_RPT = 4;
+constexpr unsigned NMFC_SPINS = 1u << 21;
+constexpr long long NMFC_EMPTY = -1LL;
+
+// Dynamic shared memory k_nmf_hals_w_coop may take on a device whose opt-in
+// limit per CTA is `optin` (1 KB stays for its static variables).
+inline size_t nmfc_smem_limit(size_t optin) { return optin > 1024 ? optin - 1024 : 0; }
+
+// Shared memory of k_nmf_hals_w_coop for `rows` rows a CTA.
+inline size_t nmfc_smem_bytes(int KP, int rows) {
+  return ((size_t)rows * (KP + 1) + (size_t)KP * KP + NMFC_THREADS) * sizeof(double);
+}
+
+template <int KP>
+__global__ void __launch_bounds__(NMFC_THREADS) k_nmf_hals_w_coop(
+    double* __restrict__ W, const double* __restrict__ AH, const double* __restrict__ G, int64_t m,
+    int k, int rows_per_cta, double* __restrict__ norms, double* __restrict__ part,
+    unsigned* __restrict__ flag, int* __restrict__ status) {
+  constexpr int LD = KP + 1;  // odd row stride: a warp's rows fall in distinct banks
+  extern __shared__ double nmfc_sm[];
+  double* Ws = nmfc_sm;                          // rows_per_cta x LD
+  double* Gs = Ws + (size_t)rows_per_cta * LD;   // Gs[x * KP + j] = G(j, x)
+  double* red = Gs + KP * KP;                    // NMFC_THREADS
+  __shared__ double s_norm;
+  __shared__ int s_ok;
+  const int tid = threadIdx.x;
+  const int64_t row0 = (int64_t)blockIdx.x * rows_per_cta;
+  const int nrows = (int)((m - row0) < rows_per_cta ? (m - row0) : rows_per_cta);
+  for (int e = tid; e < nrows * k; e += NMFC_THREADS)
+    Ws[(e / k) * LD + (e % k)] = W[row0 * k + e];
+  for (int e = tid; e < k * k; e += NMFC_THREADS) Gs[(e % k) * KP + (e / k)] = G[e];
+  double ah[NMFC_RPT], s[NMFC_RPT];
+#pragma unroll
+  for (int u = 0; u < NMFC_RPT; ++u) {
+    const int r = tid + u * NMFC_THREADS;
+    ah[u] = r < nrows ? AH[(row0 + r) * k] : 0.0;
+    s[u] = 0.0;
+  }
+  __syncthreads();
+  // W HtH(:, 0)
+  for (int j = 0; j < k; ++j) {
+    const double g = Gs[j];
+#pragma unroll
+    for (int u = 0; u < NMFC_RPT; ++u) {
+      const int r = tid + u * NMFC_THREADS;
+      if (r < nrows) s[u] = fma(Ws[r * LD + j], g, s[u]);
+    }
+  }
+  for (int x = 0; x < k; ++x) {
+    const double gxx = Gs[x * KP + x];
+    double ss = 0.0;
+#pragma unroll
+    for (int u = 0; u < NMFC_RPT; ++u) {
+      const int r = tid + u * NMFC_THREADS;
+      if (r < nrows) {
+        double v = (Ws[r * LD + x] * gxx) + (ah[u] - s[u]);
+        v = (v < kEps17) ? kEps17 : v;
+        Ws[r * LD + x] = v;
+        ss = fma(v, v, ss);
+        // next column's right-hand side, in flight across the wait
+        if (x + 1 < k) ah[u] = AH[(row0 + r) * k + x + 1];
+      }
+    }
+    double t = cta_tree_fixed(ss, red);
+    double* slot = part + (int64_t)x * gridDim.x;
+    if (tid == 0) {
+      if (__double_as_longlong(t) == NMFC_EMPTY) t = __longlong_as_double(0x7ff8000000000000LL);
+      __stcg(slot + blockIdx.x, t);
+    }
+    // W HtH(:, x+1) without column x's term
+    const double* gn = Gs + (x + 1 < k ? x + 1 : 0) * KP;
+#pragma unroll
+    for (int u = 0; u < NMFC_RPT; ++u) s[u] = 0.0;
+    if (x + 1 < k)
+      for (int j = 0; j < k; ++j) {
+        if (j == x) continue;
+        const double g = gn[j];
+#pragma unroll
+        for (int u = 0; u < NMFC_RPT; ++u) {
+          const int r = tid + u * NMFC_THREADS;
+          if (r < nrows) s[u] = fma(Ws[r * LD + j], g, s[u]);
+        }
+      }
+    // ||Wx||: warp 0 waits for every CTA's slot, adds them (lane l: CTAs l,
+    // l + 32, ...; then a fixed shuffle tree), the same sum in every CTA
+    if (tid < 32) {
+      int ok = 1;
+      double q = 0.0;
+      for (unsigned spins = 0;; ++spins) {
+        bool have = true;
+        q = 0.0;
+        for (int b = tid; b < (int)gridDim.x; b += 32) {
+          const double v = __ldcv(slot + b);
+          have = have && (__double_as_longlong(v) != NMFC_EMPTY);
+          q += v;
+        }
+        if (__all_sync(0xffffffffu, have)) break;
+        if (*(volatile unsigned*)flag) {
+          ok = 0;
+          break;
+        }
+        if (spins > NMFC_SPINS) {
+          if (tid == 0) {
+            atomicExch(flag, 1u);
+            atomicCAS(status, 0, kStTimeout);
+          }
+          ok = 0;
+          break;
+        }
+        __nanosleep(20);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+      if (tid == 0) {
+        s_ok = ok;
+        s_norm = sqrt(q);
+        if (blockIdx.x == 0 && ok) norms[x] = s_norm;
+      }
+    }
+    __syncthreads();
+    if (!s_ok) return;
+    const double nrm = s_norm;
+    const double gx1 = x + 1 < k ? gn[x] : 0.0;
+#pragma unroll
+    for (int u = 0; u < NMFC_RPT; ++u) {
+      const int r = tid + u * NMFC_THREADS;
+      if (r < nrows) {
+        double w = Ws[r * LD + x];
+        if (nrm != 0) {
+          w = w / nrm;
+          Ws[r * LD + x] = w;
+        }
+        s[u] = fma(w, gx1, s[u]);
+      }
+    }
+  }
+  __syncthreads();
+  for (int e = tid; e < nrows * k; e += NMFC_THREADS) W[row0 * k + e] = Ws[(e / k) * LD + (e % k)];
 }
 
 // Regularisation weights of the objective.
@@ -263,13 +468,21 @@ __global__ void __launch_bounds__(32 * NMFE_WARPS) k_nmf_error(
   __threadfence();
   double t[4];
   for (int i = 0; i < 4; ++i) t[i] = cta_sum_fixed(part + i, gridDim.x, 4, sh);
-  if (threadIdx.x != 0) return;
-  double ww = 0.0, fro_w = 0.0, fro_h = 0.0;
-  for (int a = 0; a < k; ++a) {
-    fro_w += GW[a * k + a];
-    fro_h += GH[a * k + a];
-    for (int b = 0; b < k; ++b) ww = fma(GW[a * k + b], GH[b * k + a], ww);
+  // tr(WtW HtH) and the Gram traces: thread j takes entries j, j + blockDim.x,
+  // ... of the k x k products, a fixed tree adds the threads
+  double pw = 0.0, pfw = 0.0, pfh = 0.0;
+  for (int e = threadIdx.x; e < k * k; e += blockDim.x) {
+    const int a = e / k, b = e % k;
+    pw = fma(GW[e], GH[b * k + a], pw);
+    if (a == b) {
+      pfw += GW[e];
+      pfh += GH[e];
+    }
   }
+  const double ww = cta_tree_fixed(pw, sh);
+  const double fro_w = cta_tree_fixed(pfw, sh);
+  const double fro_h = cta_tree_fixed(pfh, sh);
+  if (threadIdx.x != 0) return;
   const double a2 = *normA2;
   const double fit = a2 - (2 * t[0]) + ww;
   const double o = fit + reg.w2 * fro_w + reg.h2 * fro_h + reg.w1 * t[1] + reg.h1 * t[2] +

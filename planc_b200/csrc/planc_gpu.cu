@@ -76,6 +76,8 @@ struct planc_gpu_ctx {
   cudaStream_t stream = nullptr;
   bool own_stream = false;
   int sm_count = 148;
+  size_t smem_optin = 0;     // dynamic shared memory the cooperative W sweep may use
+  bool coop_launch = false;  // device takes cooperative launches
 
   int N = 0;
   int64_t dims[kMaxModes] = {0};
@@ -144,7 +146,7 @@ struct planc_gpu_ctx {
   double* nmf_norms = nullptr;  // column norms of the HALS W sweep, k
   double* nmf_part = nullptr;   // Gram / column-sum / norm partials
   size_t nmf_part_elems = 0;
-  int* nmf_ctr = nullptr;       // [0] objective index, [1] CTA ticket of the W sweep
+  int* nmf_ctr = nullptr;       // [0] objective index, [1] CTA ticket, [4] W sweep error flag
   double* nmf_obj = nullptr;    // objective and relative error per iteration
   double* nmf_rel = nullptr;
   int nmf_cap = 0;
@@ -473,8 +475,7 @@ void run_contract(planc_gpu_ctx* c, const ContractPlan& p, bool left, const doub
   if (p.nsplit > 1) {
     int64_t n = p.g.M * k;
     launch(c, KC_REDUCE, [&] {
-      k_reduce_splits<<<reduce_grid(n), 256, 0, c->stream>>>(
-          c->scratch, p.nsplit, p.g.split_stride, n, out);
+      reduce_splits(c->stream, c->scratch, p.nsplit, p.g.split_stride, n, out);
     });
   }
 }
@@ -498,8 +499,7 @@ void run_ttv_right(planc_gpu_ctx* c, const TT* T, int64_t A, int64_t B, const WG
   if (p.nsplit > 1) {
     int64_t n = A * k;
     launch(c, KC_REDUCE, [&] {
-      k_reduce_splits<<<reduce_grid(n), 256, 0, c->stream>>>(
-          c->scratch, p.nsplit, n, n, out);
+      reduce_splits(c->stream, c->scratch, p.nsplit, n, n, out);
     });
   }
 }
@@ -565,8 +565,7 @@ void partial_left(planc_gpu_ctx* c, double* out) {
     });
     int64_t n = c->R * c->k;
     launch(c, KC_REDUCE, [&] {
-      k_reduce_splits<<<reduce_grid(n), 256, 0, c->stream>>>(
-          c->scratch, nsplit, n, n, out);
+      reduce_splits(c->stream, c->scratch, nsplit, n, n, out);
     });
   }
 }
@@ -585,8 +584,7 @@ void long_contract(planc_gpu_ctx* c, bool left, const std::vector<int>& modes, d
   if (nsplit > 1) {
     const int64_t n = (left ? c->R : c->L) * c->k;
     launch(c, KC_REDUCE, [&] {
-      k_reduce_splits<<<reduce_grid(n), 256, 0, c->stream>>>(
-          c->scratch, nsplit, n, n, out);
+      reduce_splits(c->stream, c->scratch, nsplit, n, n, out);
     });
   }
 }
@@ -638,7 +636,7 @@ void mttkrp_dimtree(planc_gpu_ctx* c, int n, double* out) {
         });
         const int64_t nn = c->dims[0] * c->k;
         launch(c, KC_REDUCE, [&] {
-          k_reduce_splits<<<reduce_grid(nn), 256, 0, c->stream>>>(c->scratch, ns, nn, nn, out);
+          reduce_splits(c->stream, c->scratch, ns, nn, nn, out);
         });
         return;
       }
@@ -1130,6 +1128,11 @@ int planc_gpu_create(planc_gpu_ctx** out, int device, int precision, void* cuda_
                                 (int)bpp_smem_bytes(64)));
         CK(cudaFuncSetAttribute(k_bpp<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)bpp_smem_bytes(32)));
+        // the opt-in limit covers static and dynamic shared memory together
+        CK(cudaFuncSetAttribute(k_nmf_hals_w_coop<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)nmfc_smem_limit(prop.sharedMemPerBlockOptin)));
+        CK(cudaFuncSetAttribute(k_nmf_hals_w_coop<64>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)nmfc_smem_limit(prop.sharedMemPerBlockOptin)));
         attrs_set[device] = true;
       }
     }
@@ -1137,6 +1140,8 @@ int planc_gpu_create(planc_gpu_ctx** out, int device, int precision, void* cuda_
     c->device = device;
     c->precision = precision;
     c->sm_count = prop.multiProcessorCount;
+    c->smem_optin = nmfc_smem_limit(prop.sharedMemPerBlockOptin);
+    c->coop_launch = prop.cooperativeLaunch != 0;
     if (cuda_stream) {
       c->stream = (cudaStream_t)cuda_stream;
     } else {
@@ -2137,8 +2142,7 @@ extern "C" int planc_gpu_mttkrp_last_mode_noalloc(const double* X_dev, const int
     }
     CK(cudaGetLastError());
     const int64_t n = R * k;
-    k_reduce_splits<<<reduce_grid(n), 256, 0, st>>>(
-        scratch, (int)ns, n, n, out_dev);
+    reduce_splits(st, scratch, (int)ns, n, n, out_dev);
     CK(cudaGetLastError());
   });
 }
@@ -2181,8 +2185,8 @@ void ensure_nmf(planc_gpu_ctx* c, int iters) {
                          (size_t)((maxI + CN_ROWS - 1) / CN_ROWS) * k),
         (size_t)NMFW_MAX_BLOCKS * 4);
     dalloc(&c->nmf_part, c->nmf_part_elems);
-    dalloc(&c->nmf_ctr, 2);
-    CK(cudaMemset(c->nmf_ctr, 0, 2 * sizeof(int)));
+    dalloc(&c->nmf_ctr, 8);
+    CK(cudaMemset(c->nmf_ctr, 0, 8 * sizeof(int)));
     c->nmf_ready = true;
     c->buf_epoch++;
   }
@@ -2229,13 +2233,15 @@ void nmf_AtW(planc_gpu_ctx* c) {
 // NMF::normalize_by_W (common/nmf.hpp:150-160)
 void nmf_normalize(planc_gpu_ctx* c) {
   const int64_t m = c->dims[0], n = c->dims[1];
-  const unsigned nb = (unsigned)((m + CN_ROWS - 1) / CN_ROWS);
+  const unsigned nb = (unsigned)((m + NRM_ROWS - 1) / NRM_ROWS);
   const unsigned nr = (unsigned)((std::max(m, n) + NRM_ROWS - 1) / NRM_ROWS);
+  if ((size_t)nb * c->k > c->nmf_part_elems) fail(PLANC_GPU_ERR_STATE, "internal: NMF partials");
   launch(c, KC_NORMGRAM, [&] {
-    k_colsumsq_partial<<<nb, 256, 0, c->stream>>>(c->F[0], m, c->k, c->nmf_part);
+    k_nmf_colnorms<<<nb, 256, 0, c->stream>>>(c->F[0], m, c->k, c->nmf_part, c->nmf_ctr + 1,
+                                               c->nmf_norms);
   });
   launch(c, KC_NORMGRAM, [&] {
-    k_nmf_rescale<<<nr, 256, 0, c->stream>>>(c->F[0], m, c->F[1], n, c->k, c->nmf_part, (int)nb);
+    k_nmf_rescale<<<nr, 256, 0, c->stream>>>(c->F[0], m, c->F[1], n, c->k, c->nmf_norms);
   });
 }
 
@@ -2275,11 +2281,68 @@ void nmf_row_update(planc_gpu_ctx* c, int algo, double* U, const double* M, int6
   }
 }
 
-// HALSNMF's W sweep (nmf/hals.hpp:92-105): k + 1 launches, one per column
-// plus the finishing normalisation of the last
+// Plan of the cooperative W sweep: CTAs and rows per CTA (a thread per row up
+// to NMFC_RPT rows a thread, all CTAs resident, W's rows in shared memory).
+// False when W does not fit.
+bool nmfc_plan(planc_gpu_ctx* c, int64_t m, int KP, int* grid, int* rows) {
+  if (!c->coop_launch || m < 1) return false;
+  int occ = 0;
+  const int cap_rows = NMFC_THREADS * NMFC_RPT;
+  // fewest CTAs first: a CTA of up to NMFC_THREADS rows takes as long as one
+  // row, and fewer CTAs make the barriers cheaper
+  int64_t g = (m + NMFC_THREADS - 1) / NMFC_THREADS;
+  if (g > c->sm_count) g = c->sm_count;
+  int64_t r = (m + g - 1) / g;
+  if (r > cap_rows) return false;
+  const size_t smem = nmfc_smem_bytes(KP, (int)r);
+  if (smem > c->smem_optin) return false;
+  if (KP == 32)
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_nmf_hals_w_coop<32>, NMFC_THREADS, smem));
+  else
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_nmf_hals_w_coop<64>, NMFC_THREADS, smem));
+  if ((int64_t)occ * c->sm_count < g) return false;
+  if ((size_t)g * c->k > c->nmf_part_elems) return false;
+  *grid = (int)g;
+  *rows = (int)r;
+  return true;
+}
+
+// HALSNMF's W sweep (nmf/hals.hpp:92-105): one cooperative launch when W fits
+// in the CTAs' shared memory, else k + 1 launches, one per column plus the
+// finishing normalisation of the last
 void nmf_hals_w(planc_gpu_ctx* c) {
   const int k = c->k;
   const int64_t m = c->dims[0];
+  const int KP = k <= 32 ? 32 : 64;
+  int grid = 0, rows = 0;
+  if (nmfc_plan(c, m, KP, &grid, &rows)) {
+    // error flag clear, every column's partial-sum slots empty (all ones)
+    unsigned* flag = reinterpret_cast<unsigned*>(c->nmf_ctr + 4);
+    CK(cudaMemsetAsync(flag, 0, sizeof(unsigned), c->stream));
+    CK(cudaMemsetAsync(c->nmf_part, 0xFF, (size_t)grid * k * sizeof(double), c->stream));
+    launch(c, KC_UPDATE, [&] {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3((unsigned)grid, 1, 1);
+      cfg.blockDim = dim3(NMFC_THREADS, 1, 1);
+      cfg.dynamicSmemBytes = nmfc_smem_bytes(KP, rows);
+      cfg.stream = c->stream;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeCooperative;
+      at[0].val.cooperative = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      double* W = c->F[0];
+      const double* AH = c->M[0];
+      const double* G = c->nmf_G;
+      if (KP == 32)
+        CK(cudaLaunchKernelEx(&cfg, k_nmf_hals_w_coop<32>, W, AH, G, m, k, rows, c->nmf_norms,
+                              c->nmf_part, flag, c->status_dev));
+      else
+        CK(cudaLaunchKernelEx(&cfg, k_nmf_hals_w_coop<64>, W, AH, G, m, k, rows, c->nmf_norms,
+                              c->nmf_part, flag, c->status_dev));
+    });
+    return;
+  }
   const unsigned nb = (unsigned)std::min<int64_t>((m + NMFW_WARPS - 1) / NMFW_WARPS, NMFW_MAX_BLOCKS);
   for (int x = 0; x <= k; ++x)
     launch(c, KC_UPDATE, [&] {

@@ -46,6 +46,18 @@ def test_nmf_matches_oracle(gpu, oracle_lib, algo, m, n, k):
     assert rel(W, Wo) < TOL and rel(H, Ho) < TOL
 
 
+# HALS's W sweep runs as one cooperative launch with W's rows in shared
+# memory: one row a thread (40 x 3000 rows: 12 CTAs), two rows a thread (40000
+# rows over all SMs), and as k + 1 launches when W does not fit (130000 rows)
+@pytest.mark.parametrize("m,n,k", [(3000, 70, 40), (40000, 12, 8), (130000, 6, 3)])
+def test_nmf_hals_w_sweep_forms(gpu, oracle_lib, m, n, k):
+    A, W0, H0 = _problem(m, n, k, 86)
+    Wo, Ho, oo, ro = oracle_lib.nmf_run(A, W0, H0, "hals", 6)
+    W, H, obj, re = _gpu_nmf(gpu, A, W0, H0, "hals", 6)
+    assert rel(obj, oo) < TOL and rel(re, ro) < TOL
+    assert rel(W, Wo) < TOL and rel(H, Ho) < TOL
+
+
 @pytest.mark.parametrize("algo", ["hals", "mu", "anlsbpp"])
 def test_nmf_regularized_matches_oracle(gpu, oracle_lib, algo):
     A, W0, H0 = _problem(70, 50, 5, 82)
