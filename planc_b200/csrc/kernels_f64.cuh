@@ -284,6 +284,64 @@ __global__ void __launch_bounds__(256) k_ttv_left(const TT* __restrict__ T, int6
   }
 }
 
+// k_ttv_left for an FP32 T with k a multiple of 4: a CTA takes TTVL_NB
+// consecutive b at once, so each F row it loads serves TTVL_NB rows of T. A
+// thread owns 4 ranks (one float4 of T and two double2 of F per row a) and
+// the rows a = l, l + RL, ... of its row lane l, four rows' loads in flight;
+// the CTA adds its RL row lanes in order through shared memory. Four CTAs
+// an SM (64 registers a thread): the loop is bound by loads in flight.
+constexpr int TTVL_NB = 2;
+__global__ void __launch_bounds__(256, 4) k_ttv_left_f4(const float* __restrict__ T, int64_t A,
+                                                        int64_t B, int k,
+                                                        const double* __restrict__ F,
+                                                        double* __restrict__ out) {
+  __shared__ double red[256 * TTVL_NB * 4];
+  const int q = k >> 2;                  // float4 per row
+  const int tpr = q <= 8 ? 8 : 16;       // threads per row
+  const int RL = 256 / tpr;              // row lanes
+  const int tid = threadIdx.x;
+  const int r4 = tid % tpr, rl = tid / tpr;
+  const bool active = r4 < q;
+  const int64_t b0 = (int64_t)blockIdx.x * TTVL_NB;
+  const int nb = (int)((B - b0) < TTVL_NB ? (B - b0) : TTVL_NB);
+  double acc[TTVL_NB][4];
+#pragma unroll
+  for (int j = 0; j < TTVL_NB; ++j)
+#pragma unroll
+    for (int c = 0; c < 4; ++c) acc[j][c] = 0.0;
+  if (active) {
+#pragma unroll 4
+    for (int64_t a = rl; a < A; a += RL) {
+      const double2 f01 = *reinterpret_cast<const double2*>(F + a * k + 4 * r4);
+      const double2 f23 = *reinterpret_cast<const double2*>(F + a * k + 4 * r4 + 2);
+      float4 t[TTVL_NB];
+#pragma unroll
+      for (int j = 0; j < TTVL_NB; ++j)
+        t[j] = j < nb ? *reinterpret_cast<const float4*>(T + (a + A * (b0 + j)) * k + 4 * r4)
+                      : make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll
+      for (int j = 0; j < TTVL_NB; ++j) {
+        acc[j][0] = fma((double)t[j].x, f01.x, acc[j][0]);
+        acc[j][1] = fma((double)t[j].y, f01.y, acc[j][1]);
+        acc[j][2] = fma((double)t[j].z, f23.x, acc[j][2]);
+        acc[j][3] = fma((double)t[j].w, f23.y, acc[j][3]);
+      }
+    }
+  }
+  // red[l][j * k + r]
+  if (active)
+#pragma unroll
+    for (int j = 0; j < TTVL_NB; ++j)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) red[rl * (TTVL_NB * k) + j * k + 4 * r4 + c] = acc[j][c];
+  __syncthreads();
+  for (int e = tid; e < nb * k; e += 256) {
+    double t = 0.0;
+    for (int l = 0; l < RL; ++l) t += red[l * (TTVL_NB * k) + e];
+    out[b0 * k + e] = t;
+  }
+}
+
 template <typename TT>
 __global__ void __launch_bounds__(256) k_ttv_right(const TT* __restrict__ T, int64_t A, int64_t B,
                                                    int k, WGen wg, int64_t b_per_split,

@@ -14,6 +14,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/planc_gpu.h"
@@ -77,6 +78,7 @@ struct planc_gpu_ctx {
   bool own_stream = false;
   int sm_count = 148;
   size_t smem_optin = 0;     // dynamic shared memory the cooperative W sweep may use
+  int ngc_ctas = 0;          // cluster size of k_normgram_cluster (0: not used)
   bool coop_launch = false;  // device takes cooperative launches
 
   int N = 0;
@@ -295,6 +297,49 @@ bool enable_cluster16(void (*kern)(KArgs...)) {
   return n >= 1;
 }
 
+template <int BE>
+int ngc_cluster_size_of() {
+  auto kern = k_normgram_cluster<BE>;
+  for (int cl : {16, 8}) {
+    if (cl == 16 &&
+        cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+            cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    if (cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)ngc_smem_bytes(64)) != cudaSuccess) {
+      cudaGetLastError();
+      return 0;
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)cl, 1, 1);
+    cfg.blockDim = dim3(NGC_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = ngc_smem_bytes(64);
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cl;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    int nc = 0;
+    if (cudaOccupancyMaxActiveClusters(&nc, (const void*)kern, &cfg) != cudaSuccess) {
+      cudaGetLastError();
+      continue;
+    }
+    if (nc >= 1) return cl;
+  }
+  return 0;
+}
+
+// Cluster size of k_normgram_cluster on the current device: 16 where clusters
+// of 16 fit, else 8 where 8 fit, else 0 (the three-launch form).
+int ngc_cluster_size() {
+  const int a = ngc_cluster_size_of<2>(), b = ngc_cluster_size_of<4>();
+  return a < b ? a : b;
+}
+
 WGen make_wgen(planc_gpu_ctx* c, const std::vector<int>& modes) {
   WGen g;
   memset(&g, 0, sizeof(g));
@@ -508,6 +553,13 @@ template <typename TT>
 void run_ttv_left(planc_gpu_ctx* c, const TT* T, int64_t A, int64_t B, const double* Fa,
                   double* out) {
   int k = c->k;
+  const int64_t g2 = (B + TTVL_NB - 1) / TTVL_NB;
+  if (std::is_same<TT, float>::value && k % 4 == 0 && g2 >= c->sm_count && g2 <= 65535) {
+    launch(c, KC_TTV, [&] {
+      k_ttv_left_f4<<<(unsigned)g2, 256, 0, c->stream>>>((const float*)T, A, B, k, Fa, out);
+    });
+    return;
+  }
   launch(c, KC_TTV, [&] {
     k_ttv_left<TT><<<(unsigned)std::min<int64_t>(B, 65535), 256, 0, c->stream>>>(T, A, B, k, Fa, out);
   });
@@ -834,6 +886,30 @@ void nes_post(planc_gpu_ctx* c, int n) {
 
 void normalize_gram(planc_gpu_ctx* c, int n, int next, double* lambda) {
   const int64_t I = c->dims[n];
+  if (I <= NGC_MAX_ROWS && c->ngc_ctas > 0) {
+    double* lam = lambda ? lambda : c->lam_tmp;
+    launch(c, KC_NORMGRAM, [&] {
+      cudaLaunchConfig_t cfg = {};
+      cfg.gridDim = dim3((unsigned)c->ngc_ctas, 1, 1);
+      cfg.blockDim = dim3(NGC_THREADS, 1, 1);
+      cfg.dynamicSmemBytes = ngc_smem_bytes(c->k);
+      cfg.stream = c->stream;
+      cudaLaunchAttribute at[1];
+      at[0].id = cudaLaunchAttributeClusterDimension;
+      at[0].val.clusterDim.x = (unsigned)c->ngc_ctas;
+      at[0].val.clusterDim.y = 1;
+      at[0].val.clusterDim.z = 1;
+      cfg.attrs = at;
+      cfg.numAttrs = 1;
+      if (c->k <= 32)
+        CK(cudaLaunchKernelEx(&cfg, k_normgram_cluster<2>, c->F[n], I, c->k, lam, c->Gall, c->N,
+                              n, next, c->Gloo));
+      else
+        CK(cudaLaunchKernelEx(&cfg, k_normgram_cluster<4>, c->F[n], I, c->k, lam, c->Gall, c->N,
+                              n, next, c->Gloo));
+    });
+    return;
+  }
   const int rpb = gram_rows_per_block(I);
   const int nblk = (int)((I + rpb - 1) / rpb);
   if ((size_t)nblk * c->k * c->k > c->gram_part_elems)
@@ -1141,6 +1217,7 @@ int planc_gpu_create(planc_gpu_ctx** out, int device, int precision, void* cuda_
     c->precision = precision;
     c->sm_count = prop.multiProcessorCount;
     c->smem_optin = nmfc_smem_limit(prop.sharedMemPerBlockOptin);
+    c->ngc_ctas = ngc_cluster_size();
     c->coop_launch = prop.cooperativeLaunch != 0;
     if (cuda_stream) {
       c->stream = (cudaStream_t)cuda_stream;

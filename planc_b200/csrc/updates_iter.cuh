@@ -483,6 +483,132 @@ __global__ void __launch_bounds__(256) k_colnorm_apply(double* __restrict__ U, i
 }
 
 // ---------------------------------------------------------------------------
+// Normalisation + Gram of one factor in one cluster launch
+// ---------------------------------------------------------------------------
+// The outputs of k_gram_partial + k_gram_finalize + k_scale_cols
+// (NCPFactors::normalize(int), ncpfactors.hpp:346-351; the Gram of the
+// normalised factor, ncpfactors.hpp:144; the leave-one-out product for mode
+// `next`, ncpfactors.hpp:139-148) from one cluster of CTAs that split U's rows
+// evenly. Each CTA forms U^T U of its rows (64-row tiles in shared memory,
+// rows in increasing order, a thread per 2 x 2 (k <= 32) or 4 x 4 block of
+// outputs) in its own shared memory; after a cluster barrier CTA c adds slice
+// c of the entries over the cluster's CTAs in rank order and stores the sums
+// into every CTA's copy of the Gram (distributed shared memory); after a
+// second barrier every CTA holds the same Gram, takes lambda_r =
+// sqrt((U^T U)_rr) and divides its own rows by lambda, and CTA 0 writes
+// lambda, G_n = (U^T U)_ab / (lambda_a lambda_b) and the leave-one-out
+// product. Meant for factors of up to NGC_MAX_ROWS rows, where three launches
+// cost more than the work.
+constexpr int NGC_THREADS = 256;
+constexpr int NGC_TILE = 64;          // rows of a shared-memory tile
+constexpr int64_t NGC_MAX_ROWS = 4096;
+constexpr int NGC_MAX_CL = 16;        // largest cluster
+
+inline size_t ngc_smem_bytes(int k) {
+  const int kp = k <= 32 ? 32 : 64;
+  return ((size_t)NGC_TILE * kp + (size_t)kp * kp) * sizeof(double);
+}
+
+template <int BE>  // edge of a thread's block of outputs: 2 (k <= 32) or 4
+__global__ void __launch_bounds__(NGC_THREADS, 1)
+    k_normgram_cluster(double* __restrict__ F, int64_t I, int k, double* __restrict__ lambda,
+                       double* __restrict__ Gall, int N, int n, int next,
+                       double* __restrict__ Gloo) {
+  cg::cluster_group cluster = cg::this_cluster();
+  const int CL = (int)cluster.num_blocks(), me = (int)cluster.block_rank();
+  extern __shared__ double ngc_sm[];
+  const int kp = k <= 32 ? 32 : 64;
+  double* tile = ngc_sm;                   // NGC_TILE x k; later this CTA's copy of the Gram
+  double* gpart = ngc_sm + NGC_TILE * kp;  // k x k: U^T U of this CTA's rows
+  __shared__ double lam[kMaxRank];
+  const int tid = threadIdx.x;
+  const int kk2 = k * k;
+  const int64_t per = (I + CL - 1) / CL;
+  const int64_t r0 = (int64_t)me * per;
+  const int64_t r1 = (r0 + per) < I ? (r0 + per) : I;
+  const int kt = (k + BE - 1) / BE;
+  const bool owner = tid < kt * kt;
+  const int ta = tid / kt, tb = tid % kt;
+  double acc[BE][BE];
+#pragma unroll
+  for (int u = 0; u < BE; ++u)
+#pragma unroll
+    for (int v = 0; v < BE; ++v) acc[u][v] = 0.0;
+  for (int64_t c0 = r0; c0 < r1; c0 += NGC_TILE) {
+    const int nrows = (int)((r1 - c0) < NGC_TILE ? (r1 - c0) : NGC_TILE);
+    __syncthreads();
+    for (int e = tid; e < nrows * k; e += NGC_THREADS) tile[e] = F[c0 * k + e];
+    __syncthreads();
+    if (owner)
+      for (int i = 0; i < nrows; ++i) {
+        const double* r = tile + i * k;
+        double av[BE], bv[BE];
+#pragma unroll
+        for (int u = 0; u < BE; ++u) {
+          const int a = ta + kt * u, b = tb + kt * u;
+          av[u] = a < k ? r[a] : 0.0;
+          bv[u] = b < k ? r[b] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < BE; ++u)
+#pragma unroll
+          for (int v = 0; v < BE; ++v) acc[u][v] = fma(av[u], bv[v], acc[u][v]);
+      }
+  }
+  if (owner)
+#pragma unroll
+    for (int u = 0; u < BE; ++u)
+#pragma unroll
+      for (int v = 0; v < BE; ++v) {
+        const int a = ta + kt * u, b = tb + kt * v;
+        if (a < k && b < k) gpart[a * k + b] = acc[u][v];
+      }
+  __syncthreads();  // the tile is free for the Gram copy
+  cluster.sync();
+  {
+    const int sl = (kk2 + CL - 1) / CL;
+    const int e0 = me * sl, e1 = (e0 + sl) < kk2 ? (e0 + sl) : kk2;
+    for (int e = e0 + tid; e < e1; e += NGC_THREADS) {
+      // all remote loads in flight before the in-order sum
+      double v[NGC_MAX_CL];
+#pragma unroll
+      for (int b = 0; b < NGC_MAX_CL; ++b) v[b] = b < CL ? *cluster.map_shared_rank(gpart + e, b) : 0.0;
+      double t = 0.0;
+#pragma unroll
+      for (int b = 0; b < NGC_MAX_CL; ++b)
+        if (b < CL) t += v[b];
+#pragma unroll
+      for (int b = 0; b < NGC_MAX_CL; ++b)
+        if (b < CL) *cluster.map_shared_rank(tile + e, b) = t;
+    }
+  }
+  cluster.sync();
+  const double* gs = tile;
+  if (tid < k) lam[tid] = sqrt(gs[tid * k + tid]);
+  __syncthreads();
+  for (int64_t e = r0 * k + tid; e < r1 * k; e += NGC_THREADS) {
+    const double nrm = lam[e % k];
+    if (nrm > 0) F[e] = F[e] / nrm;
+  }
+  if (me != 0) return;
+  if (tid < k && lambda) lambda[tid] = lam[tid];
+  double* Gn = Gall + (int64_t)n * kk2;
+  for (int e = tid; e < kk2; e += NGC_THREADS) {
+    const int a = e / k, b = e % k;
+    const double la = lam[a], lb = lam[b];
+    Gn[e] = (la > 0 && lb > 0) ? gs[e] / (la * lb) : gs[e];
+  }
+  if (next < 0) return;
+  __syncthreads();
+  for (int e = tid; e < kk2; e += NGC_THREADS) {
+    double g = 1.0;
+    for (int i = 0; i < N; ++i)
+      if (i != next) g = g * Gall[(int64_t)i * kk2 + e];
+    Gloo[e] = g;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Nesterov (NTFNES)
 // ---------------------------------------------------------------------------
 constexpr int NES_MAX_STEPS = 20000;
