@@ -972,8 +972,15 @@ __global__ void __launch_bounds__(NES_THREADS, 1)
   };
   all_grads();
 
+  // Each step's cluster barrier is split: after a CTA has pushed its max /
+  // min it arrives, forms the next step speculatively (the same arithmetic
+  // the loop would do next), and only then waits; when the test says stop,
+  // the step's iterate saved before the speculation is the result. The
+  // barrier's latency overlaps a step's math; the values are unchanged.
   double alpha = 1.0, beta = 1.0;
   int t = 0;
+  double hsave[R][PER];
+  cluster.sync();  // every CTA of the cluster running before remote stores
   for (;;) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -998,34 +1005,44 @@ __global__ void __launch_bounds__(NES_THREADS, 1)
         dst[1] = n;
       }
     }
-    cluster.sync();
+    asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+    // speculative step t + 1
+    const double alpha_n = nes_alpha_of(alpha, q);
+    const double beta_n = (alpha * (1 - alpha)) / (alpha_n + alpha * alpha);
+#pragma unroll
+    for (int r = 0; r < R; ++r)
+#pragma unroll
+      for (int p = 0; p < PER; ++p) {
+        hsave[r][p] = ht[r][p];
+        if (live[r][p]) {
+          const double hprev = ht[r][p];
+          const double v = acc[r][p] - (inv * gr[r][p]);
+          const double hn = v > 0.0 ? v : 0.0;
+          acc[r][p] = hn + beta_n * (hn - hprev);
+          ht[r][p] = hn;
+        }
+      }
+    all_grads();
+    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
     double gmax = 0.0, gmin = INFINITY;
     for (unsigned r = 0; r < cluster.num_blocks(); ++r) {
       gmax = fmax(gmax, slot[t & 1][r][0]);
       gmin = fmin(gmin, slot[t & 1][r][1]);
     }
-    if (gmax <= 1e-2 && gmin >= -1e-2) break;  // stop_iter, ntfnes.hpp:52-62
-    if (t >= max_steps) {
-      if (blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(status, 0, kStMaxIter);
+    const bool stop = gmax <= 1e-2 && gmin >= -1e-2;  // stop_iter, ntfnes.hpp:52-62
+    if (stop || t >= max_steps) {
+      if (!stop && blockIdx.x == 0 && threadIdx.x == 0) atomicCAS(status, 0, kStMaxIter);
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+#pragma unroll
+        for (int p = 0; p < PER; ++p) ht[r][p] = hsave[r][p];
       break;
     }
     ++t;
-    const double alpha_prev = alpha;
-    alpha = nes_alpha_of(alpha_prev, q);
-    beta = (alpha_prev * (1 - alpha_prev)) / (alpha + alpha_prev * alpha_prev);
-#pragma unroll
-    for (int r = 0; r < R; ++r)
-#pragma unroll
-      for (int p = 0; p < PER; ++p)
-        if (live[r][p]) {
-          const double hprev = ht[r][p];
-          const double v = acc[r][p] - (inv * gr[r][p]);
-          const double hn = v > 0.0 ? v : 0.0;
-          acc[r][p] = hn + beta * (hn - hprev);
-          ht[r][p] = hn;
-        }
-    all_grads();
+    alpha = alpha_n;
+    beta = beta_n;
   }
+  (void)beta;
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const int64_t row = row0 + r * stride;
