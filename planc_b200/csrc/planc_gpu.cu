@@ -78,7 +78,7 @@ struct planc_gpu_ctx {
   bool own_stream = false;
   int sm_count = 148;
   size_t smem_optin = 0;     // dynamic shared memory the cooperative W sweep may use
-  int ngc_ctas = 0;          // cluster size of k_normgram_cluster (0: not used)
+  int ngc_ctas = 0;          // largest cluster of k_normgram_cluster (0: not used)
   bool coop_launch = false;  // device takes cooperative launches
 
   int N = 0;
@@ -886,17 +886,22 @@ void nes_post(planc_gpu_ctx* c, int n) {
 
 void normalize_gram(planc_gpu_ctx* c, int n, int next, double* lambda) {
   const int64_t I = c->dims[n];
+  // one cluster launch per factor, a CTA per 64 rows up to the largest
+  // cluster: the size depends on I alone, so every context (a batch member
+  // too) sums a factor's Gram in the same order, and small factors take small
+  // clusters that run beside other contexts' kernels
   if (I <= NGC_MAX_ROWS && c->ngc_ctas > 0) {
     double* lam = lambda ? lambda : c->lam_tmp;
+    const int cl = (int)std::min<int64_t>(c->ngc_ctas, std::max<int64_t>(1, (I + NGC_TILE - 1) / NGC_TILE));
     launch(c, KC_NORMGRAM, [&] {
       cudaLaunchConfig_t cfg = {};
-      cfg.gridDim = dim3((unsigned)c->ngc_ctas, 1, 1);
+      cfg.gridDim = dim3((unsigned)cl, 1, 1);
       cfg.blockDim = dim3(NGC_THREADS, 1, 1);
       cfg.dynamicSmemBytes = ngc_smem_bytes(c->k);
       cfg.stream = c->stream;
       cudaLaunchAttribute at[1];
       at[0].id = cudaLaunchAttributeClusterDimension;
-      at[0].val.clusterDim.x = (unsigned)c->ngc_ctas;
+      at[0].val.clusterDim.x = (unsigned)cl;
       at[0].val.clusterDim.y = 1;
       at[0].val.clusterDim.z = 1;
       cfg.attrs = at;

@@ -21,6 +21,9 @@ larger than the 126 MB L2 (DRAM counters stay meaningful):
   upd     AO-ADMM and Nesterov NTF updates on the 1024^3 rank-32 headline
           tensor (BF16 copy): three iterations each (Nesterov's extrapolation
           runs from the sixth iteration of a call, so it is off here)
+  nes     Nesterov NTF update on a 512^3 rank-32 tensor (BF16 copy): eight
+          iterations in one call (the extrapolation runs from the sixth), for a
+          capture of the register-resident inner kernel
   ttv     the multi-TTVs of the 3-way tensor-core path with the headline's
           intermediate: 1024 x 1024 x 64 FP32 tensor (BF16 copy), rank 32, so
           the FP32 partial MTTKRP P is 1024*1024 x 32 (134 MB > L2)
@@ -159,7 +162,17 @@ def case_upd(gpu, torch):
     print("upd: 1024^3 k=32 per iteration: " + ", ".join(out))
 
 
-CASES = {"bpp": case_bpp, "tc3": case_tc3, "tc4": case_tc4, "cfg3it": case_cfg3it,
+def case_nes(gpu, torch):
+    dims, k = (512, 512, 512), 32
+    X, F0 = _synth(gpu, torch, dims, k, 71)
+    with gpu.Context(0, "bf16") as c:
+        c.set_tensor(X.data_ptr(), dims=dims, dtype="f32")
+        c.set_factors(F0)
+        ms = _timed(torch, c, lambda: c.run("nesterov", 8), 1) / 8
+    print("nes: 512^3 k=32 Nesterov: %.3f ms per iteration (8 in one call)" % ms)
+
+
+CASES = {"bpp": case_bpp, "nes": case_nes, "tc3": case_tc3, "tc4": case_tc4, "cfg3it": case_cfg3it,
          "ttv": case_ttv, "nmf": case_nmf, "upd": case_upd}
 
 
