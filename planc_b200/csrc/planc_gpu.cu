@@ -886,13 +886,15 @@ void nes_post(planc_gpu_ctx* c, int n) {
 
 void normalize_gram(planc_gpu_ctx* c, int n, int next, double* lambda) {
   const int64_t I = c->dims[n];
-  // one cluster launch per factor, a CTA per 64 rows up to the largest
-  // cluster: the size depends on I alone, so every context (a batch member
-  // too) sums a factor's Gram in the same order, and small factors take small
-  // clusters that run beside other contexts' kernels
+  // one cluster launch per factor, a CTA per 64 rows (16 rows above rank 32,
+  // where a row's outer product is four times the work) up to the largest
+  // cluster: the size depends on I and k alone, so every context (a batch
+  // member too) sums a factor's Gram in the same order, and small factors
+  // take small clusters that run beside other contexts' kernels
   if (I <= NGC_MAX_ROWS && c->ngc_ctas > 0) {
     double* lam = lambda ? lambda : c->lam_tmp;
-    const int cl = (int)std::min<int64_t>(c->ngc_ctas, std::max<int64_t>(1, (I + NGC_TILE - 1) / NGC_TILE));
+    const int64_t rpc = c->k > 32 ? 16 : NGC_TILE;
+    const int cl = (int)std::min<int64_t>(c->ngc_ctas, std::max<int64_t>(1, (I + rpc - 1) / rpc));
     launch(c, KC_NORMGRAM, [&] {
       cudaLaunchConfig_t cfg = {};
       cfg.gridDim = dim3((unsigned)cl, 1, 1);
