@@ -48,7 +48,10 @@ def test_direct_mttkrp_five_modes(gpu, oracle_lib):
 
 
 @pytest.mark.parametrize("algo", ["hals", "mu", "anlsbpp"])
-@pytest.mark.parametrize("dims,k,iters", [((64, 64, 64), 8, 20), ((20, 31, 17, 9), 6, 6)])
+# (5000, 7, 6): a factor above the one-cluster normalisation's 4096 rows
+# (multi-CTA Gram partials, fixed-order finish, column scaling)
+@pytest.mark.parametrize("dims,k,iters", [((64, 64, 64), 8, 20), ((20, 31, 17, 9), 6, 6),
+                                          ((5000, 7, 6), 5, 6)])
 def test_ntf_run_matches_oracle(gpu, oracle_lib, algo, dims, k, iters):
     X, _ = cp_tensor(dims, k, noise=0.01, seed=7)
     F0 = init_factors(dims, k, seed=8)

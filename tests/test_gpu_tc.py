@@ -80,6 +80,24 @@ def test_tc_bf16_error_within_1e4_at_192cube(gpu, algo):
     assert abs(errs["bf16"] - errs["fp64"]) < 1e-4, errs
 
 
+@pytest.mark.parametrize("prec", ["bf16", "bf16x2"])
+# mode 1 of the 3-way tree reads the FP32 P with k_ttv_left_f4 (two i1 per
+# CTA, float4 loads) once I1 / 2 gives a CTA per SM: 8 and 16 threads a row,
+# and an odd I1 whose last CTA has a single i1
+@pytest.mark.parametrize("dims,k", [((64, 320, 24), 12), ((40, 297, 20), 32), ((32, 300, 16), 64)])
+def test_tc_mode1_ttv_two_rows_per_cta(gpu, oracle_lib, prec, dims, k):
+    X, _ = cp_tensor(dims, 4, seed=33)
+    F = init_factors(dims, k, seed=34)
+    Fn = _normalized(F)
+    with gpu.Context(0, prec) as c:
+        c.set_tensor(X)
+        c.set_factors(F)
+        for n in range(3):
+            ref = oracle_lib.mttkrp_direct(X, Fn, n)
+            got = c.mttkrp(n, dimtree=True)
+            assert rel(got, ref) < BOUND[prec], (n, rel(got, ref))
+
+
 def test_tc_large_split_k(gpu, oracle_lib):
     # long reduction (L = 147456 -> many split-K partials) and R = 300 with a
     # ragged last tile
