@@ -2439,10 +2439,23 @@ void nmf_hals_w(planc_gpu_ctx* c) {
     });
 }
 
-void nmf_error(planc_gpu_ctx* c) {
+// out = G + l2 I + l1 ones + diag I from an unregularised Gram G that
+// nmf_gram wrote (the same bits nmf_gram would give with the terms: the one
+// partial is added to zero, then the terms in the same order)
+void nmf_gram_reg(planc_gpu_ctx* c, const double* G, double l2, double l1, double diag,
+                  double* out) {
+  const int k = c->k;
+  launch(c, KC_NORMGRAM, [&] {
+    k_nmf_gram<<<(unsigned)((k * k + 7) / 8), 256, 0, c->stream>>>(G, 1, k, l2, l1, diag, out);
+  });
+}
+
+// The objective from the Grams of the final W and H: `gw` / `gh` form them
+// here, otherwise nmf_GW / nmf_GH already hold them.
+void nmf_error(planc_gpu_ctx* c, bool gw, bool gh) {
   const int64_t m = c->dims[0], n = c->dims[1];
-  nmf_gram(c, c->F[0], m, 0, 0, 0, c->nmf_GW);
-  nmf_gram(c, c->F[1], n, 0, 0, 0, c->nmf_GH);
+  if (gw) nmf_gram(c, c->F[0], m, 0, 0, 0, c->nmf_GW);
+  if (gh) nmf_gram(c, c->F[1], n, 0, 0, 0, c->nmf_GH);
   NmfReg reg{c->nmf_reg[0], c->nmf_reg[1], c->nmf_reg[2], c->nmf_reg[3], c->nmf_reg[4]};
   const unsigned nb =
       (unsigned)std::min<int64_t>((std::max(m, n) + NMFE_WARPS - 1) / NMFE_WARPS, NMFW_MAX_BLOCKS);
@@ -2455,46 +2468,62 @@ void nmf_error(planc_gpu_ctx* c) {
 
 // One iteration of HALSNMF / MUNMF / BPPNMF::computeNMF. HALS and MU find
 // A^T W of the current W in M[1] (left there by the previous iteration's
-// objective, or computed before the first).
+// objective, or computed before the first). A factor's Gram is formed once
+// per change of the factor: the unregularised W^T W / H^T H in nmf_GW /
+// nmf_GH serve both the next update (regularised by nmf_gram_reg) and the
+// objective; before the first iteration nmf_prereq_gram forms the one the
+// first update needs.
 void nmf_iteration(planc_gpu_ctx* c, int algo) {
   const int64_t m = c->dims[0], n = c->dims[1];
   const double* r = c->nmf_reg;
   const double sym = r[4];
   if (algo == PLANC_GPU_HALS || algo == PLANC_GPU_MU) {
     // H <- f(H, A^T W, W^T W + regH)   (nmf/hals.hpp:60-76, nmf/mu.hpp:60-68)
-    nmf_gram(c, c->F[0], m, r[2], r[3], 0, c->nmf_G);
+    nmf_gram_reg(c, c->nmf_GW, r[2], r[3], 0, c->nmf_G);
     nmf_row_update(c, algo, c->F[1], c->M[1], n);
     // W <- f(W, A H, H^T H + regW)     (nmf/hals.hpp:82-106, nmf/mu.hpp:72-80)
     nmf_AH(c);
-    nmf_gram(c, c->F[1], n, r[0], r[1], 0, c->nmf_G);
+    nmf_gram(c, c->F[1], n, 0, 0, 0, c->nmf_GH);
+    nmf_gram_reg(c, c->nmf_GH, r[0], r[1], 0, c->nmf_G);
     if (algo == PLANC_GPU_HALS) {
       nmf_hals_w(c);
-      nmf_normalize(c);
+      nmf_normalize(c);  // rescales H too: both Grams are formed again
     } else {
       nmf_row_update(c, algo, c->F[0], c->M[0], m);
     }
     nmf_AtW(c);
+    nmf_error(c, true, algo == PLANC_GPU_HALS);
   } else {
     // ANLS: W from (H^T H + regW, H^T A^T), then H from (W^T W + regH, W^T A),
     // each with the symmetric regularisation when set (nmf/bppnmf.hpp:24-80,
     // 208-214)
     nmf_AH(c);
-    nmf_gram(c, c->F[1], n, r[0], r[1], sym, c->nmf_G);
+    nmf_gram_reg(c, c->nmf_GH, r[0], r[1], sym, c->nmf_G);
     if (sym > 0)
       launch(c, KC_UPDATE, [&] {
         k_nmf_axpy<<<elem_grid(m * c->k), 256, 0, c->stream>>>(c->M[0], c->F[1], m * c->k, sym);
       });
     nmf_row_update(c, algo, c->F[0], c->M[0], m);
     nmf_AtW(c);
-    nmf_gram(c, c->F[0], m, r[2], r[3], sym, c->nmf_G);
+    nmf_gram(c, c->F[0], m, 0, 0, 0, c->nmf_GW);
+    nmf_gram_reg(c, c->nmf_GW, r[2], r[3], sym, c->nmf_G);
     if (sym > 0)
       launch(c, KC_UPDATE, [&] {
         k_nmf_axpy<<<elem_grid(n * c->k), 256, 0, c->stream>>>(c->M[1], c->F[0], n * c->k, sym);
       });
     nmf_row_update(c, algo, c->F[1], c->M[1], n);
     if (sym > 0) nmf_AtW(c);  // the objective takes A^T W without the shift
+    nmf_error(c, false, true);
   }
-  nmf_error(c);
+}
+
+// Before a run's first iteration: the Gram the first update reads (W^T W
+// for HALS / MU, H^T H for ANLS/BPP), unregularised.
+void nmf_prereq_gram(planc_gpu_ctx* c, int algo) {
+  if (algo == PLANC_GPU_ANLSBPP)
+    nmf_gram(c, c->F[1], c->dims[1], 0, 0, 0, c->nmf_GH);
+  else
+    nmf_gram(c, c->F[0], c->dims[0], 0, 0, 0, c->nmf_GW);
 }
 
 void require_nmf(planc_gpu_ctx* c) {
@@ -2574,6 +2603,7 @@ int planc_gpu_nmf_run(planc_gpu_ctx* c, int algo, int iters, double* objective,
     CK(cudaMemsetAsync(c->nmf_ctr, 0, sizeof(int), c->stream));
     if (algo == PLANC_GPU_HALS) nmf_normalize(c);  // HALSNMF's constructor, nmf/hals.hpp:44-48
     if (algo != PLANC_GPU_ANLSBPP) nmf_AtW(c);
+    nmf_prereq_gram(c, algo);
     if (!c->timing) {
       if (!c->nmf_gexec || c->nmf_galgo != algo) {
         if (c->nmf_gexec) cudaGraphExecDestroy(c->nmf_gexec);
