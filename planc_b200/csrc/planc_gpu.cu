@@ -79,6 +79,7 @@ struct planc_gpu_ctx {
   int sm_count = 148;
   size_t smem_optin = 0;     // dynamic shared memory the cooperative W sweep may use
   int ngc_ctas = 0;          // largest cluster of k_normgram_cluster (0: not used)
+  int nes_max_steps = NES_MAX_STEPS;  // step cap of the Nesterov inner loop
   bool coop_launch = false;  // device takes cooperative launches
 
   int N = 0;
@@ -847,7 +848,7 @@ void run_update(planc_gpu_ctx* c, int algo, int n) {
 #define NES_REG(KP, R)                                                                       \
   launch_cluster(k_nes_inner_reg<KP, R>, c->cl_ctas, c->stream, c->F[n],                      \
                  (const double*)c->prox[n], c->prev[n], (const double*)c->M[n],               \
-                 (const double*)c->Gloo, c->nes, I, k, (int)NES_MAX_STEPS, c->status_dev)
+                 (const double*)c->Gloo, c->nes, I, k, c->nes_max_steps, c->status_dev)
       if (k <= 32 && rpw <= 1) NES_REG(32, 1);
       else if (k <= 32 && rpw <= 2) NES_REG(32, 2);
       else if (k <= 32 && rpw <= 4) NES_REG(32, 4);
@@ -858,11 +859,11 @@ void run_update(planc_gpu_ctx* c, int algo, int n) {
       else if (k <= 32)
         k_nes_inner<32><<<NES_CTAS, NES_THREADS, 0, c->stream>>>(
             c->F[n], c->prox[n], c->prev[n], c->M[n], c->Gloo, c->nes, c->nes_acc, c->nes_grad,
-            c->nes_modM, I, k, NES_MAX_STEPS, c->status_dev);
+            c->nes_modM, I, k, c->nes_max_steps, c->status_dev);
       else
         k_nes_inner<64><<<NES_CTAS, NES_THREADS, 0, c->stream>>>(
             c->F[n], c->prox[n], c->prev[n], c->M[n], c->Gloo, c->nes, c->nes_acc, c->nes_grad,
-            c->nes_modM, I, k, NES_MAX_STEPS, c->status_dev);
+            c->nes_modM, I, k, c->nes_max_steps, c->status_dev);
 #undef NES_REG
     });
   } else {
@@ -1225,6 +1226,12 @@ int planc_gpu_create(planc_gpu_ctx** out, int device, int precision, void* cuda_
     c->sm_count = prop.multiProcessorCount;
     c->smem_optin = nmfc_smem_limit(prop.sharedMemPerBlockOptin);
     c->ngc_ctas = ngc_cluster_size();
+    // PLANC_GPU_NES_MAX_STEPS lowers the Nesterov inner loop's step cap for
+    // contexts created while it is set (1 .. NES_MAX_STEPS)
+    if (const char* e = getenv("PLANC_GPU_NES_MAX_STEPS")) {
+      const int v = atoi(e);
+      if (v >= 1 && v <= NES_MAX_STEPS) c->nes_max_steps = v;
+    }
     c->coop_launch = prop.cooperativeLaunch != 0;
     if (cuda_stream) {
       c->stream = (cudaStream_t)cuda_stream;

@@ -124,3 +124,27 @@ def test_objective_error_balanced_4way(gpu, oracle_lib):
         c.set_tensor(X.astype(np.float32))
         c.set_factors(F0)
         assert abs(c.objective_error() - ref) < 1e-4
+
+
+@pytest.mark.parametrize("dims", [(20, 18, 16), (1100, 12, 10)])
+def test_nesterov_step_cap_reports_maxiter(gpu, monkeypatch, dims):
+    # an inner loop that the step cap stops (here 2 steps, set for the
+    # context through PLANC_GPU_NES_MAX_STEPS) ends with PLANC_GPU_ERR_MAXITER,
+    # in the register-resident form and in the global-memory form (1100 rows);
+    # a context created without the setting then runs normally
+    k = 5
+    X, _ = cp_tensor(dims, k, noise=0.01, seed=63)
+    F0 = init_factors(dims, k, seed=64)
+    monkeypatch.setenv("PLANC_GPU_NES_MAX_STEPS", "2")
+    with gpu.Context(0, "fp64") as c:
+        c.set_tensor(X)
+        c.set_factors(F0)
+        with pytest.raises(gpu.PlancGpuError) as ei:
+            c.run("nesterov", 3)
+        assert ei.value.code == -10
+    monkeypatch.delenv("PLANC_GPU_NES_MAX_STEPS")
+    with gpu.Context(0, "fp64") as c:
+        c.set_tensor(X)
+        c.set_factors(F0)
+        e = c.run("nesterov", 3)
+    assert np.all(np.isfinite(e))
