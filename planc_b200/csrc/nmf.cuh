@@ -323,9 +323,16 @@ __global__ void __launch_bounds__(NMFC_THREADS) k_nmf_hals_w_coop(
         if (x + 1 < k) ah[u] = AH[(row0 + r) * k + x + 1];
       }
     }
-    double t = cta_tree_fixed(ss, red);
+    // the CTA's sum: a fixed shuffle tree per warp, then thread 0 adds the
+    // warps in order (one barrier)
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) ss += __shfl_xor_sync(0xffffffffu, ss, o);
+    if ((tid & 31) == 0) red[tid >> 5] = ss;
+    __syncthreads();
     double* slot = part + (int64_t)x * gridDim.x;
     if (tid == 0) {
+      double t = 0.0;
+      for (int w = 0; w < NMFC_THREADS / 32; ++w) t += red[w];
       if (__double_as_longlong(t) == NMFC_EMPTY) t = __longlong_as_double(0x7ff8000000000000LL);
       __stcg(slot + blockIdx.x, t);
     }
