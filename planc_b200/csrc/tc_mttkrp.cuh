@@ -1139,21 +1139,39 @@ __global__ void k_tc_wimage(const WGen wg, int64_t K, int k, int64_t nk, uint8_t
     const int r = (int)((e / (TC_BK / 8)) % KP);
     const int64_t kb = e / ((int64_t)(TC_BK / 8) * KP);
     alignas(16) __nv_bfloat16 hi[8], lo[8];
+    // the eight rows' factor values are all loaded before any is converted
+    // (one memory latency per thread, not eight)
+    double w[8];
+    if (wg.nf == 1) {
+      const double* f0 = wg.f[0];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int64_t j = kb * TC_BK + ch * 8 + u;
-      double w = 0.0;
-      if (j < K && r < k) {
-        if (two32) {
-          const int jj = (int)j, d0 = (int)wg.dim[0];
-          const int i1 = jj / d0, i0 = jj - i1 * d0;
-          w = wg.f[0][(int64_t)i0 * k + r] * wg.f[1][(int64_t)i1 * k + r];
-        } else {
-          w = wgen_eval(wg, j, r, k);
-        }
+      for (int u = 0; u < 8; ++u) {
+        const int64_t j = kb * TC_BK + ch * 8 + u;
+        w[u] = (j < K && r < k) ? f0[j * k + r] : 0.0;
       }
-      split_bf16(w, hi[u], lo[u]);
+    } else if (two32) {
+      const int d0 = (int)wg.dim[0];
+      double a[8], b[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int64_t j = kb * TC_BK + ch * 8 + u;
+        const bool in = j < K && r < k;
+        const int jj = in ? (int)j : 0;
+        const int i1 = jj / d0, i0 = jj - i1 * d0;
+        a[u] = in ? wg.f[0][(int64_t)i0 * k + r] : 0.0;
+        b[u] = in ? wg.f[1][(int64_t)i1 * k + r] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) w[u] = a[u] * b[u];
+    } else {
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int64_t j = kb * TC_BK + ch * 8 + u;
+        w[u] = (j < K && r < k) ? wgen_eval(wg, j, r, k) : 0.0;
+      }
     }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) split_bf16(w[u], hi[u], lo[u]);
     uint8_t* st = img + (size_t)kb * NCOL * 128;
     *reinterpret_cast<uint4*>(st + sw128_kmajor_off(r, ch * 8)) = *reinterpret_cast<const uint4*>(hi);
     *reinterpret_cast<uint4*>(st + sw128_kmajor_off(KP + r, ch * 8)) = *reinterpret_cast<const uint4*>(lo);
