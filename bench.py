@@ -160,6 +160,17 @@ def traffic_from_profiles(precision, dims, k, which):
     return None
 
 
+def left_splits(L, R, I0, k, sm_count):
+    """Split-K count of the 3-way left contraction, as the library plans it
+    (tc_left_plan: 128-row tiles, two per CTA when R > 128 and k <= 32, the
+    SMs shared among the row groups, at most one split per run of I_0 rows)."""
+    mt = 2 if (R > 128 and k <= 32) else 1
+    groups = -(-R // (mt * 128))
+    ns = max(1, sm_count // groups)
+    units = L // I0 if I0 % 64 == 0 else -(-L // 64)
+    return min(ns, units)
+
+
 def cpu_sample(gpu, torch, dev, dims, A, sigma, F0, algo, iters=3):
     """The reference algorithm on the host cores over a bounded slice of the
     workload: dims[0] x dims[1] x 128 (1/8 of the tensor for 1024^3), same rank
@@ -314,7 +325,7 @@ def main():
     # writes P in FP32; left: X^T*KRP, writes split-K FP64 partials)
     L = dims[0] * dims[1]
     R = numel // L
-    nsplit_left = max(1, 148 // ((R + 255) // 256))
+    nsplit_left = left_splits(L, R, dims[0], k, torch.cuda.get_device_properties(dev).multi_processor_count)
     kern = {
         "right": (kt["contract"], numel * EB[args.precision] + L * k * 4),
         "left": (kt["contract_left"], numel * EB[args.precision] + nsplit_left * R * k * 8),

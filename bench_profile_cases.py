@@ -1,6 +1,6 @@
 """Small, fixed workloads for profiling single kernels of the library.
 
-    python -m planc_b200.profile_cases <case>
+    python bench_profile_cases.py <case>
 
 Each case builds its input on the device, runs the path a few times and
 prints one line of timings. The cases are sized so that a profiler capture of
@@ -178,7 +178,7 @@ CASES = {"bpp": case_bpp, "nes": case_nes, "tc3": case_tc3, "tc4": case_tc4, "cf
 
 def main(argv):
     if len(argv) != 1 or argv[0] not in CASES:
-        print("usage: python -m planc_b200.profile_cases {%s}" % "|".join(CASES))
+        print("usage: python bench_profile_cases.py {%s}" % "|".join(CASES))
         return 2
     import torch
 

@@ -201,7 +201,7 @@ int planc_gpu_batch_destroy(planc_gpu_batch* b);
  * split-K partials go to a fixed 8 MiB device array (2^20 doubles) that every
  * GPU loading the library holds until exit.
  *   out[j, r] = sum_l X[l + L*j] * KRP(F_0..F_{N-2})[l, r],  j < I_{N-1}
- * (the direct last-mode MTTKRP, common/tensor.hpp:246-327, FP64). X_dev:
+ * with L = I_0 * ... * I_{N-2}, in FP64. X_dev:
  * device tensor, FP64, mode 0 fastest; F_dev[n] (n < N-1): device factors,
  * row-major I_n x k FP64; out_dev: device I_{N-1} x k FP64, row-major. The
  * caller passes all of them; I_{N-1} * k above 2^20 is rejected with
@@ -209,8 +209,11 @@ int planc_gpu_batch_destroy(planc_gpu_batch* b);
  * returns without synchronising. All calls share the one array: calls that
  * overlap on the GPU (different streams or threads at once) race and must be
  * serialised by the caller. The first call on a device resolves the array's
- * device address (cudaGetSymbolAddress); make that first call before any
- * stream capture. */
+ * device address (cudaGetSymbolAddress) and keeps it for the life of the
+ * process; make that first call before any stream capture. A device reset
+ * (cudaDeviceReset, or the primary context released and created again)
+ * reloads the module and invalidates the kept address: do not call this entry
+ * point on a device after resetting it. */
 int planc_gpu_mttkrp_last_mode_noalloc(const double* X_dev, const int64_t* dims, int nmodes,
                                        const double* const* F_dev, int k, double* out_dev,
                                        void* cuda_stream);

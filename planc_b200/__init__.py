@@ -149,6 +149,9 @@ class Context:
         self.device = device
         self.dims = None
         self.k = None
+        # bumped by every call that may leave new dimension-tree intermediates
+        # in the context (a caller that wants to reuse them checks it)
+        self.tree_epoch = 0
 
     def close(self):
         if self.h:
@@ -174,6 +177,7 @@ class Context:
     def set_tensor(self, X, dims=None, dtype=None):
         """X: numpy array (any shape; Fortran order = mode 0 fastest), or a
         device pointer (int) with explicit dims and dtype ('f32'/'f64')."""
+        self.tree_epoch += 1
         L = load()
         if isinstance(X, np.ndarray):
             dims = X.shape
@@ -192,6 +196,7 @@ class Context:
         self.dims = tuple(int(x) for x in dims)
 
     def set_factors(self, F, lam=None):
+        self.tree_epoch += 1
         F = [_c64(f) for f in F]
         k = F[0].shape[1]
         lamp = _pd(_c64(lam)) if lam is not None else None
@@ -202,6 +207,7 @@ class Context:
         self.k = k
 
     def run(self, algo, iters, dimtree=True, compute_error=True):
+        self.tree_epoch += 1
         errs = np.zeros(max(iters, 1))
         _check(load().planc_gpu_run(self.h, ALGO[algo] if isinstance(algo, str) else int(algo),
                                     iters, int(dimtree), int(compute_error), _pd(errs)))
@@ -226,6 +232,7 @@ class Context:
 
     def nmf_run(self, algo, iters):
         """Returns (objective, relative error) per iteration."""
+        self.tree_epoch += 1
         obj, rel = np.zeros(max(iters, 1)), np.zeros(max(iters, 1))
         _check(load().planc_gpu_nmf_run(self.h, ALGO[algo] if isinstance(algo, str) else int(algo),
                                         iters, _pd(obj), _pd(rel)))
@@ -237,6 +244,7 @@ class Context:
         return W, H
 
     def mttkrp(self, mode, dimtree=True):
+        self.tree_epoch += 1
         out = np.zeros((self.dims[mode], self.k))
         _check(load().planc_gpu_mttkrp(self.h, mode, int(dimtree), _pd(out)))
         return out
@@ -247,17 +255,20 @@ class Context:
         return out
 
     def objective_error(self):
+        self.tree_epoch += 1
         e = ctypes.c_double()
         _check(load().planc_gpu_objective_error(self.h, ctypes.byref(e)))
         return e.value
 
     def mode_begin(self, mode, dimtree=True):
+        self.tree_epoch += 1
         G = np.zeros((self.k, self.k))
         M = np.zeros((self.dims[mode], self.k))
         _check(load().planc_gpu_mode_begin(self.h, mode, int(dimtree), _pd(G), _pd(M)))
         return G, M
 
     def mode_end(self, mode, factor):
+        self.tree_epoch += 1
         f = _c64(factor)
         _check(load().planc_gpu_mode_end(self.h, mode, _pd(f)))
 
@@ -279,6 +290,7 @@ class Context:
         """MTTKRP of `mode` for device factors (pointers to row-major (I_n, k)
         float64 buffers) into the device buffer out_ptr; stream-ordered."""
         arr = (ctypes.c_void_p * len(factor_ptrs))(*[int(p) for p in factor_ptrs])
+        self.tree_epoch += 1
         _check(load().planc_gpu_mttkrp_device(self.h, mode, arr, ctypes.c_void_p(int(out_ptr)),
                                               int(dimtree) | (2 if reuse else 0)))
 

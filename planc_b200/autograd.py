@@ -12,7 +12,10 @@ The forward pass runs the mode-0 MTTKRP on the tensor-core (or FP64) kernel
 of a planc_b200.Context; the hand-written backward runs the remaining modes'
 MTTKRPs on the same kernels (the modes after 0 reuse the dimension tree's
 partial contractions in order, starting from the forward pass's mode 0), so
-one forward + backward reads X twice. Factors are float64 CUDA tensors of
+one forward + backward reads X twice. The context's tree epoch is recorded by
+the forward; when anything else has run an MTTKRP on the context since (a
+second forward before this backward, a direct call), the backward recomputes
+mode 1 from the tensor instead of reusing another call's intermediates. Factors are float64 CUDA tensors of
 shape (I_n, k), contiguous (row-major, the library's factor layout).
 """
 import torch
@@ -39,6 +42,7 @@ class _CPLoss(torch.autograd.Function):
         ptrs = [f.data_ptr() for f in factors]
         stream.wait_stream(torch.cuda.current_stream(dev))
         handle.mttkrp_device(0, ptrs, M0.data_ptr(), dimtree=True, reuse=False)
+        ctx.tree_epoch = handle.tree_epoch
         torch.cuda.current_stream(dev).wait_stream(stream)
         grams = [f.T @ f for f in factors]
         inner = (M0 * factors[0]).sum()
@@ -57,11 +61,15 @@ class _CPLoss(torch.autograd.Function):
         N = len(factors)
         Ms = [M0]
         stream.wait_stream(torch.cuda.current_stream(dev))
+        # the tree holds this forward's mode-0 intermediates only if no other
+        # MTTKRP ran on the context since
+        fresh = handle.tree_epoch == ctx.tree_epoch
         for n in range(1, N):
             Mn = torch.empty_like(factors[n])
             # in-order sweep with unchanged factors: every mode reuses the tree
-            # state left by the previous ones (the forward's mode 0 included)
-            handle.mttkrp_device(n, ptrs, Mn.data_ptr(), dimtree=True, reuse=True)
+            # state left by the previous one
+            handle.mttkrp_device(n, ptrs, Mn.data_ptr(), dimtree=True,
+                                 reuse=(n > 1) or fresh)
             Ms.append(Mn)
         torch.cuda.current_stream(dev).wait_stream(stream)
         grams = [f.T @ f for f in factors]

@@ -115,3 +115,35 @@ def test_cp_loss_4way_reference_gradient(gpu, oracle_lib, prec):
         ref_grad = F[n] @ G - M
         assert rel(Ft[n].grad.cpu().numpy(), ref_grad) < bound, (n, rel(Ft[n].grad.cpu().numpy(), ref_grad))
     lossf.close()
+
+
+@pytest.mark.parametrize("dims", [(40, 36, 28), (20, 16, 24, 12)])
+def test_cp_loss_backward_after_second_forward(gpu, dims):
+    # two forwards on one CPLoss, then the FIRST loss's backward: its gradient
+    # must be built from its own factors, not from the tree state the second
+    # forward left in the context (checked against torch autograd of the
+    # dense FP64 reconstruction)
+    import torch
+    from planc_b200.autograd import CPLoss
+    k = 5
+    X, _ = cp_tensor(dims, k, noise=0.05, seed=61)
+    rng = np.random.default_rng(62)
+    F1 = [rng.random((d, k)) for d in dims]
+    F2 = [rng.random((d, k)) for d in dims]
+    lossf = CPLoss(X, rank=k, precision="fp64")
+    A = [torch.tensor(f, device="cuda", dtype=torch.float64, requires_grad=True) for f in F1]
+    B = [torch.tensor(f, device="cuda", dtype=torch.float64, requires_grad=True) for f in F2]
+    loss_a = lossf(*A)
+    loss_b = lossf(*B)
+    loss_a.backward()
+    loss_b.backward()
+    Xt = torch.tensor(X, device="cuda", dtype=torch.float64)
+    letters = "abcd"[:len(dims)]
+    spec = ",".join(c + "z" for c in letters) + "->" + letters
+    for got, F in ((A, F1), (B, F2)):
+        R = [torch.tensor(f, device="cuda", dtype=torch.float64, requires_grad=True) for f in F]
+        ref = 0.5 * ((Xt - torch.einsum(spec, *R)) ** 2).sum()
+        ref.backward()
+        for g, r in zip(got, R):
+            assert rel(g.grad.cpu().numpy(), r.grad.cpu().numpy()) < 1e-10
+    lossf.close()
