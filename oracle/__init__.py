@@ -6,9 +6,11 @@ Only tests/, ``__graft_entry__.smoke()`` and the CPU-baseline legs of
 Two libraries are loaded:
   * ``liboracle.so``: the CPU restatement of the reference NTF path
     (``ntf_oracle.cpp``; every function cites the reference lines it follows);
-  * ``_ref/libref_dimtree.so``: the reference's own dimension-tree MTTKRP
-    kernels (``dimtree/dimtrees.hpp``, ``dimtree/ddttensor.hpp``) compiled
-    unmodified by ``oracle/Makefile``, driven by ``ref_dimtree_driver.cpp``.
+  * ``_ref/libref_planc.so``: the reference's own shared-memory NTF code
+    (``AUNTF`` and its updates, ``BPPNNLS``, ``NCPFactors``, ``Tensor``,
+    ``DenseDimensionTree``) compiled unmodified by ``oracle/Makefile`` against
+    the Armadillo-subset shim in ``ref_shim/``, driven by
+    ``ref_planc_driver.cpp``.
 
 Array conventions: tensors are numpy arrays in Fortran order (mode 0
 fastest, ``common/tensor.hpp:22-28``); factors are C-order ``(I_n, k)``
@@ -40,7 +42,7 @@ def find_openblas():
 
 
 def build(reference_dir=None):
-    """Compile liboracle.so (and _ref/libref_dimtree.so when the reference
+    """Compile liboracle.so (and _ref/libref_planc.so when the reference
     tree is present)."""
     cmd = ["make", "-s", "-C", HERE, "OPENBLAS=" + find_openblas()]
     if reference_dir and os.path.isdir(reference_dir):
@@ -87,25 +89,208 @@ def lib():
     return _lib
 
 
+REF_LIB = os.path.join(HERE, "_ref", "libref_planc.so")
+
+
 def ref_available():
-    return os.path.exists(os.path.join(HERE, "_ref", "libref_dimtree.so"))
+    """True when the reference's own code (oracle/_ref/libref_planc.so, built
+    from the reference tree by oracle/Makefile) is present."""
+    return os.path.exists(REF_LIB)
 
 
 def ref():
+    """ctypes handle of oracle/_ref/libref_planc.so: the reference's AUNTF,
+    its updates, BPPNNLS, NCPFactors, Tensor and DenseDimensionTree compiled
+    unmodified against the Armadillo-subset shim (ref_planc_driver.cpp)."""
     global _ref
     if _ref is None:
-        path = os.path.join(HERE, "_ref", "libref_dimtree.so")
-        R = ctypes.CDLL(path)
+        R = ctypes.CDLL(REF_LIB)
         P = ctypes.POINTER
-        pd = P(ctypes.c_double)
-        li = ctypes.c_long
-        R.ref_dimtree_create.argtypes = [pd, P(li), li, li, P(pd), li]
-        R.ref_dimtree_create.restype = ctypes.c_void_p
-        R.ref_dimtree_set_factor.argtypes = [ctypes.c_void_p, li, pd]
-        R.ref_dimtree_mttkrp.argtypes = [ctypes.c_void_p, li, pd]
-        R.ref_dimtree_destroy.argtypes = [ctypes.c_void_p]
+        d, vp, i32, li = ctypes.c_double, ctypes.c_void_p, ctypes.c_int, ctypes.c_long
+        pd = P(d)
+        ppd = P(pd)
+        R.ref_tensor_new.argtypes = [P(li), i32, i32]
+        R.ref_tensor_new.restype = vp
+        R.ref_tensor_from.argtypes = [P(li), i32, pd]
+        R.ref_tensor_from.restype = vp
+        R.ref_tensor_data.argtypes = [vp]
+        R.ref_tensor_data.restype = pd
+        R.ref_tensor_norm.argtypes = [vp]
+        R.ref_tensor_norm.restype = d
+        R.ref_tensor_free.argtypes = [vp]
+        R.ref_tensor_mttkrp.argtypes = [vp, ppd, i32, i32, pd]
+        R.ref_gram_leave_out_one.argtypes = [P(li), i32, i32, ppd, i32, pd]
+        R.ref_normalize_mode.argtypes = [pd, li, i32, pd]
+        R.ref_update.argtypes = [i32, pd, pd, pd, li, i32, pd]
+        R.ref_update.restype = i32
+        R.ref_bpp_solve.argtypes = [pd, pd, i32, li, pd]
+        R.ref_bpp_solve.restype = i32
+        R.ref_ntf_create.argtypes = [vp, i32, i32, i32, ppd, i32]
+        R.ref_ntf_create.restype = vp
+        R.ref_ntf_run.argtypes = [vp, i32]
+        R.ref_ntf_run.restype = d
+        R.ref_ntf_factors.argtypes = [vp, ppd, pd]
+        R.ref_ntf_objective_error.argtypes = [vp]
+        R.ref_ntf_objective_error.restype = d
+        R.ref_ntf_destroy.argtypes = [vp]
+        R.ref_dimtree_create.argtypes = [pd, P(li), i32, i32, ppd]
+        R.ref_dimtree_create.restype = vp
+        R.ref_dimtree_set_factor.argtypes = [vp, li, pd]
+        R.ref_dimtree_mttkrp.argtypes = [vp, li, pd]
+        R.ref_dimtree_destroy.argtypes = [vp]
         _ref = R
     return _ref
+
+
+def _ldims(shape):
+    return (ctypes.c_long * len(shape))(*shape)
+
+
+class RefTensor:
+    """planc::Tensor of the reference (common/tensor.hpp), owning its data."""
+
+    def __init__(self, X=None, dims=None, serial=True):
+        """From an array X (copied, Tensor(dims, data)), or Tensor(dims) with
+        the reference's mt19937(103) fill (one OpenMP thread when serial)."""
+        R = ref()
+        if X is not None:
+            X = _xf(X)
+            self.dims = tuple(X.shape)
+            self.h = R.ref_tensor_from(_ldims(X.shape), X.ndim, _pd(X))
+        else:
+            self.dims = tuple(int(x) for x in dims)
+            self.h = R.ref_tensor_new(_ldims(self.dims), len(self.dims), int(serial))
+
+    def data(self):
+        """The tensor's m_data as a Fortran-order view (no copy)."""
+        n = int(np.prod(self.dims))
+        p = ref().ref_tensor_data(self.h)
+        return np.ctypeslib.as_array(p, shape=(n,)).reshape(self.dims, order="F")
+
+    def norm(self):
+        """Tensor::norm(): the squared Frobenius norm (common/tensor.hpp:350-356)."""
+        return ref().ref_tensor_norm(self.h)
+
+    def mttkrp(self, F, n):
+        """Tensor::mttkrp(n, krp_leave_out_one(n)) as row-major I_n x k."""
+        F = [_c(f) for f in F]
+        out = np.zeros((self.dims[n], F[0].shape[1]))
+        ref().ref_tensor_mttkrp(self.h, _fptrs(F), F[0].shape[1], n, _pd(out))
+        return out
+
+    def close(self):
+        if self.h:
+            ref().ref_tensor_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class RefNTF:
+    """The reference's AUNTF subclass for `algo` on a RefTensor, driven as a
+    library user drives it: dim_tree() before reset(initial factors),
+    compute_error(), then computeNTF() for a number of iterations."""
+
+    def __init__(self, tensor, F0, algo, dimtree=True, compute_error=True):
+        F0 = [_c(f) for f in F0]
+        self.tensor = tensor
+        self.k = F0[0].shape[1]
+        self.h = ref().ref_ntf_create(tensor.h, self.k, ALGO[algo], int(dimtree), _fptrs(F0),
+                                      int(compute_error))
+        if not self.h:
+            raise ValueError("unknown algorithm")
+
+    def run(self, iters):
+        """computeNTF() with num_it(iters); returns current_error()."""
+        return ref().ref_ntf_run(self.h, iters)
+
+    def factors(self):
+        F = [np.zeros((d, self.k)) for d in self.tensor.dims]
+        lam = np.zeros(self.k)
+        ref().ref_ntf_factors(self.h, _fptrs(F), _pd(lam))
+        return F, lam
+
+    def objective_error(self):
+        return ref().ref_ntf_objective_error(self.h)
+
+    def close(self):
+        if self.h:
+            ref().ref_ntf_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def ref_ntf_run(X, F0, algo, iters, dimtree=True, compute_error=True):
+    """The reference's own AUNTF run from injected factors. Returns (factors,
+    lambda, per-iteration relative errors). Nesterov runs its iterations in
+    one computeNTF() call (its acceleration counts iterations within a call)
+    and reports the final error only; the other updates run one iteration per
+    call so that every iteration's error is seen (the loop state carries over
+    between calls)."""
+    t = RefTensor(X)
+    s = RefNTF(t, F0, algo, dimtree, compute_error)
+    try:
+        if algo == "nesterov":
+            errs = np.array([s.run(iters)])
+        else:
+            errs = np.array([s.run(1) for _ in range(iters)])
+        F, lam = s.factors()
+    finally:
+        s.close()
+        t.close()
+    return F, lam, errs
+
+
+def ref_update(algo, H, M, G):
+    """update(mode) of the reference's NTF class for `algo` with the given
+    factor H (I x k), MTTKRP M (I x k) and leave-one-out Gram G; returns the
+    new factor (I x k)."""
+    H, M, G = _c(H), _c(M), _c(G)
+    out = np.zeros_like(H)
+    rc = ref().ref_update(ALGO[algo], _pd(H), _pd(M), _pd(G), H.shape[0], H.shape[1], _pd(out))
+    if rc != 0:
+        raise ValueError("unsupported algorithm for an isolated update")
+    return out
+
+
+def ref_bpp_solve(AtA, AtB):
+    """BPPNNLS(AtA, AtB, true).solveNNLS(); returns (X, iterations)."""
+    A = np.asfortranarray(AtA, dtype=np.float64)
+    B = np.asfortranarray(AtB, dtype=np.float64)
+    X = np.zeros(B.shape, order="F")
+    it = ref().ref_bpp_solve(_pd(A), _pd(B), A.shape[0], B.shape[1], _pd(X))
+    return X, it
+
+
+def ref_normalize(H):
+    """NCPFactors::normalize(mode) of H; returns (normalised H, lambda)."""
+    H = _c(H).copy()
+    lam = np.zeros(H.shape[1])
+    ref().ref_normalize_mode(_pd(H), H.shape[0], H.shape[1], _pd(lam))
+    return H, lam
+
+
+def ref_gram_loo(F, n):
+    """NCPFactors::gram_leave_out_one(n)."""
+    F = [_c(f) for f in F]
+    k = F[0].shape[1]
+    G = np.zeros((k, k))
+    ref().ref_gram_leave_out_one(_ldims([f.shape[0] for f in F]), len(F), k, _fptrs(F), n,
+                                 _pd(G))
+    return G.T.copy()
+
+
+def _c(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
 
 
 # ---------------------------------------------------------------- helpers
@@ -165,15 +350,15 @@ def mttkrp_dimtree_all(X, F):
     return outs
 
 
-def ref_mttkrp_dimtree_all(X, F, nthreads=1):
-    """All-mode MTTKRP through the reference's compiled dimension-tree kernels,
-    with fixed factors (the factor slot overwritten by each MTTKRP is restored
-    as AUNTF's set_factor would, ntf/auntf.hpp:70-73)."""
+def ref_mttkrp_dimtree_all(X, F):
+    """All-mode MTTKRP through the reference's DenseDimensionTree, with fixed
+    factors (the factor slot overwritten by each MTTKRP is restored as AUNTF's
+    set_factor would, ntf/auntf.hpp:70-73)."""
     X = _xf(X)
     k = F[0].shape[1]
     R = ref()
     dims = (ctypes.c_long * X.ndim)(*X.shape)
-    h = R.ref_dimtree_create(_pd(X), dims, X.ndim, k, _fptrs(F), nthreads)
+    h = R.ref_dimtree_create(_pd(X), dims, X.ndim, k, _fptrs(F))
     outs = []
     try:
         for n in range(X.ndim):

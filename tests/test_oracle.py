@@ -251,3 +251,129 @@ def test_oracle_nmf_regularized_objective(oracle_lib):
     ref = (fit + w2 * np.sum(W * W) + h2 * np.sum(H * H) + w1 * np.sum(W.sum(1) ** 2)
            + h1 * np.sum(H.sum(1) ** 2))
     assert abs(obj[-1] - ref) < 1e-9 * ref
+
+
+# ---------------------------------------------------------------------------
+# The update, normalisation, BPP and AUNTF-loop steps of the oracle pinned to
+# the reference's OWN code (ntf/auntf.hpp, ntf/ntf*.hpp, nnls/bppnnls.hpp,
+# common/ncpfactors.hpp compiled unmodified against the Armadillo-subset shim
+# in oracle/ref_shim/): committed fixtures made by tests/golden/make_golden.py,
+# and the live library when oracle/_ref is built.
+
+def _golden_runs():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(GOLD, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    return mg
+
+
+_MG = _golden_runs()
+_RUN_CASES = [(name, a) for name, _, _, _, _, algos, _, _ in _MG.RUNS for a in algos]
+
+
+@pytest.mark.parametrize("name,algo", _RUN_CASES)
+def test_oracle_ntf_runs_match_reference_golden(oracle_lib, name, algo):
+    g = np.load(os.path.join(GOLD, "ref_ntf_runs.npz"))
+    dims = tuple(int(d) for d in g[name + "_dims"])
+    k, iters, dt, seed = (int(v) for v in g[name + "_meta"])
+    X, F0 = _MG.run_inputs(dims, k, float(g[name + "_noise"][0]), seed)
+    xs = g[name + "_xsum"]
+    assert abs(X.sum() - xs[0]) <= 1e-12 * xs[0] and X.ravel(order="F")[7] == xs[2]
+    F, lam, errs = oracle_lib.ntf_run(X, F0, algo, iters, dimtree=bool(dt))
+    pre = "%s_%s_" % (name, algo)
+    for i in range(len(dims)):
+        assert rel(F[i], g[pre + "F%d" % i]) < 1e-10, i
+    assert rel(lam, g[pre + "lam"]) < 1e-10
+    ref_err = g[pre + "err"]
+    if algo == "nesterov":  # the reference run reports its final error only
+        assert abs(errs[-1] - ref_err[-1]) <= 1e-10 * ref_err[-1]
+    else:
+        assert np.max(np.abs(errs - ref_err) / ref_err) < 1e-10
+
+
+@pytest.mark.parametrize("case", [0, 1, 2])
+def test_oracle_updates_match_reference_golden(oracle_lib, case):
+    g = np.load(os.path.join(GOLD, "ref_updates.npz"))
+    H, M, G = g["u%d_H" % case], g["u%d_M" % case], g["u%d_G" % case]
+    assert rel(oracle_lib.hals_update(H, M, G), g["u%d_hals" % case]) < 1e-13
+    assert rel(oracle_lib.mu_update(H, M, G), g["u%d_mu" % case]) < 1e-13
+    Hb, mask, _ = oracle_lib.bpp_update(M, G)
+    ref_b = g["u%d_anlsbpp" % case]
+    assert rel(Hb, ref_b) < 1e-12
+    assert np.array_equal(mask != 0, ref_b > 0)
+    Ha, _, _ = oracle_lib.admm_update(H, np.zeros_like(H), M, G)
+    assert rel(Ha, g["u%d_aoadmm" % case]) < 1e-12
+
+
+@pytest.mark.parametrize("case", [0, 1, 2])
+def test_oracle_bpp_matches_reference_golden(oracle_lib, case):
+    # BPPNNLS (nnls/bppnnls.hpp:67-191) on normal equations; case 2 is one
+    # mode of the 192^4 rank-64 workload in size (k = 64, 192 right-hand sides)
+    g = np.load(os.path.join(GOLD, "ref_updates.npz"))
+    AtA, AtB, Xr = g["b%d_AtA" % case], g["b%d_AtB" % case], g["b%d_X" % case]
+    H, mask, it = oracle_lib.bpp_update(AtB.T, AtA)
+    assert rel(H.T, Xr) < 1e-11
+    assert np.array_equal(mask.T != 0, Xr > 0)
+    assert it == int(g["b%d_iters" % case][0])
+
+
+_live = pytest.mark.skipif(not __import__("oracle").ref_available(), reason="reference build absent")
+
+
+@_live
+@pytest.mark.parametrize("algo", ["mu", "hals", "anlsbpp", "aoadmm", "nesterov"])
+@pytest.mark.parametrize("dims,k,dimtree", [((11, 9, 13), 4, True), ((6, 5, 7, 4), 3, True),
+                                            ((10, 8, 7), 6, False), ((5, 6, 4, 3), 2, False)])
+def test_oracle_ntf_run_matches_reference_live(oracle_lib, algo, dims, k, dimtree):
+    X, _ = cp_tensor(dims, k, noise=0.05, seed=sum(dims) + k)
+    F0 = init_factors(dims, k, seed=k + 40)
+    iters = 7
+    Fr, lr, er = oracle_lib.ref_ntf_run(X, F0, algo, iters, dimtree=dimtree)
+    F, lam, errs = oracle_lib.ntf_run(X, F0, algo, iters, dimtree=dimtree)
+    for a, b in zip(F, Fr):
+        assert rel(a, b) < 1e-10
+    assert rel(lam, lr) < 1e-10
+    if algo == "nesterov":
+        assert abs(errs[-1] - er[-1]) <= 1e-10 * er[-1]
+    else:
+        assert np.max(np.abs(errs - er) / er) < 1e-10
+
+
+@_live
+@pytest.mark.parametrize("seed", range(6))
+def test_oracle_bpp_matches_reference_live(oracle_lib, seed):
+    # random normal equations, rank-deficient data, single and many columns
+    rng = np.random.default_rng(900 + seed)
+    n = int(rng.integers(2, 40))
+    ncols = [1, 3, 17, 120, 2, 64][seed]
+    B = rng.random((2 * n, n))
+    B[rng.random(B.shape) < 0.4] = 0.0
+    AtA = B.T @ B + 1e-6 * np.eye(n)
+    AtB = rng.standard_normal((n, ncols)) * np.abs(AtA).mean() * n
+    Xr, it_r = oracle_lib.ref_bpp_solve(AtA, AtB)
+    H, mask, it = oracle_lib.bpp_update(AtB.T, AtA)
+    assert rel(H.T, Xr) < 1e-9
+    assert np.array_equal(mask.T != 0, Xr > 0)
+    assert it == it_r
+
+
+@_live
+def test_oracle_normalize_and_gram_match_reference_live(oracle_lib):
+    rng = np.random.default_rng(5)
+    F = [rng.random((d, 6)) for d in (9, 4, 7, 5)]
+    F[1][:, 2] = 0.0  # a zero column keeps lambda 0 and the column unscaled
+    for n in range(4):
+        assert rel(oracle_lib.gram_loo(F, n), oracle_lib.ref_gram_loo(F, n)) < 1e-14
+    Hn, lam = oracle_lib.normalize(F[1])
+    Hr, lr = oracle_lib.ref_normalize(F[1])
+    assert rel(Hn, Hr) < 1e-14 and rel(lam, lr) < 1e-14 and lr[2] == 0.0
+
+
+@_live
+def test_reference_tensor_fill_matches_mt19937_pin(oracle_lib):
+    # the reference's own Tensor(dims) constructor fill (single-threaded)
+    gold = np.load(os.path.join(GOLD, "mt19937_103.npz"))["values"]
+    t = oracle_lib.RefTensor(dims=(16, 16, 16))
+    assert np.array_equal(t.data().ravel(order="F"), gold)
+    t.close()
