@@ -171,78 +171,90 @@ def left_splits(L, R, I0, k, sm_count):
     return min(ns, units)
 
 
-def cpu_sample(gpu, torch, dev, dims, A, sigma, F0, algo, iters=3):
-    """The reference algorithm on the host cores over a bounded slice of the
-    workload: dims[0] x dims[1] x 128 (1/8 of the tensor for 1024^3), same rank
-    and noise model; iters/s scaled to the full tensor by the element ratio
-    (the per-iteration cost is linear in the element count)."""
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def workload_name(dims, k, algo):
+    """The workload both arms run, named without implementation details."""
+    return ("%s FP32 tensor, rank-%d CP + 1%% noise, %s, rank %d, dimension-tree MTTKRP, "
+            "relative error every iteration" % ("x".join(map(str, dims)), k, algo.upper(), k))
+
+
+def reference_cpu(dims, k, algo, warmup, steps):
+    """The reference's own NTF code on the host cores (oracle/_ref; the
+    oracle's restatement when that build is absent) over the full workload:
+    the same factors, noise and seed as the GPU arm, generated on the host.
+    Returns (iters/s, details)."""
     import oracle
     from oracle import cpu_ntf
-    sdims = (dims[0], dims[1], min(dims[2], 128))
-    As = [A[0], A[1], A[2][:sdims[2]]]
-    n = int(np.prod(sdims))
-    x = torch.empty(n, dtype=torch.float64, device="cuda:%d" % dev)
-    gpu.synth_cp_tensor(dev, x.data_ptr(), "f64", sdims, As, sigma, 7, clip=True)
-    X = x.cpu().numpy().reshape(sdims, order="F")
-    del x
-    Fs = [F0[0], F0[1], F0[2][:sdims[2]]]
+    A, sigma, F0 = workload(dims, k)
     oracle.lib()
-    sec, _ = cpu_ntf.run_timed(X, Fs, algo, iters, _CORES, use_ref=True)
-    scale = n / float(np.prod(dims))
-    return {"value": (1.0 / sec) * scale, "unit": "iters/s", "cores": _CORES,
-            "kind": "port",
-            "sample": "%d outer %s iterations on a %dx%dx%d slice (same rank/noise), "
-                      "iters/s scaled by the element ratio %.4f; MTTKRP through the reference's "
-                      "own dimension-tree sources (oracle/_ref, OpenBLAS dgemm, %d threads) when "
-                      "built, updates by the oracle restatement" % (iters, algo, *sdims, scale,
-                                                                     _CORES)}
+    r = cpu_ntf.run(dims, A, sigma, 7, F0, algo, warmup, steps, compute_error=True)
+    total = sum(r["step_s"])
+    value = steps / total if total > 0 else None
+    return value, r
+
+
+def cpu_sample(dims, k, algo, warmup=1, steps=3):
+    """cpu_baseline of the GPU arm: a bounded sample of the same workload,
+    `steps` timed outer iterations (after `warmup`) of the reference's own
+    code on the full tensor, all host cores."""
+    value, r = reference_cpu(dims, k, algo, warmup, steps)
+    return {"value": value, "unit": "iters/s", "cores": _CORES, "kind": r["kind"],
+            "cpu": cpu_model(),
+            "sample": "%d timed outer %s iterations (after %d untimed) of the full %s workload, "
+                      "relative error every iteration; %s on %d host threads (OpenBLAS, "
+                      "OpenMP)" % (steps, algo.upper(), warmup, "x".join(map(str, dims)),
+                                   "the reference's own AUNTF + DenseDimensionTree compiled "
+                                   "from its sources (oracle/_ref)" if r["kind"] == "reference"
+                                   else "the oracle's restatement", _CORES),
+            "final_rel_error": r["error"]}
 
 
 def reference_arm(args, rank, world):
+    """--impl reference: the reference's CPU implementation of the path on the
+    host cores (no GPU, no library of this repository), on this bench's
+    workload, metric and unit. Rank 0 alone runs; other ranks exit."""
     if rank != 0:
         return
-    import oracle
-    from oracle import cpu_ntf
-    import torch
-    import planc_b200 as gpu
     dims = tuple(int(x) for x in args.dims.split(","))
     k = args.rank
-    A, sigma, F0 = workload(dims, k)
-    sdims = (dims[0], dims[1], min(dims[2], 128))
-    As = [A[0], A[1], A[2][:sdims[2]]]
-    n = int(np.prod(sdims))
-    dev = 0
-    if torch.cuda.is_available():
-        x = torch.empty(n, dtype=torch.float64, device="cuda:0")
-        gpu.synth_cp_tensor(dev, x.data_ptr(), "f64", sdims, As, sigma, 7, clip=True)
-        X = x.cpu().numpy().reshape(sdims, order="F")
-        del x
-    else:
-        rng = np.random.default_rng(7)
-        M = np.einsum("az,bz,cz->abc", *As)
-        X = np.asfortranarray(np.maximum(M + sigma * rng.standard_normal(M.shape), 0))
-    Fs = [F0[0], F0[1], F0[2][:sdims[2]]]
-    oracle.lib()
-    cpu_ntf.run_timed(X, Fs, args.algo, max(args.warmup, 0), _CORES, use_ref=True)
     t0 = time.perf_counter()
-    sec, _ = cpu_ntf.run_timed(X, Fs, args.algo, args.steps, _CORES, use_ref=True)
+    value, r = reference_cpu(dims, k, args.algo, max(args.warmup, 0), args.steps)
     wall = time.perf_counter() - t0
-    scale = n / float(np.prod(dims))
-    value = (1.0 / sec) * scale
+    steps_ms = [1e3 * x for x in r["step_s"]]
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "iters/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": "%s FP32 tensor, rank %d, %s, dimension tree (CPU sample %s)"
-                   % ("x".join(map(str, dims)), k, args.algo.upper(), "x".join(map(str, sdims))),
-                   "dims": list(dims), "rank": k, "algo": args.algo},
-        "cpu_baseline": {"value": value, "unit": "iters/s", "cores": _CORES, "kind": "port",
-                         "sample": "each step one outer iteration on a %s slice, iters/s scaled by "
-                                   "%.4f; MTTKRP via the reference's dimension-tree sources "
-                                   "(oracle/_ref) when built" % ("x".join(map(str, sdims)), scale)},
+        "ms_per_step": sum(steps_ms) / max(len(steps_ms), 1), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic: rank-%d CP model, U[0,1) factors, 1%% Gaussian noise, clipped >= 0, "
+                "values rounded to FP32, generated on the host (Philox, the GPU arm's "
+                "generator)" % k,
+        "config": {"workload": workload_name(dims, k, args.algo), "dims": list(dims), "rank": k,
+                   "algo": args.algo, "parallelism": "host cores x%d" % _CORES,
+                   "l2": "inputs larger than L2 (%.1f GB FP64 tensor)" % (np.prod(dims) * 8 / 1e9)},
+        "cpu_baseline": {"value": value, "unit": "iters/s", "cores": _CORES, "kind": r["kind"],
+                         "cpu": cpu_model(),
+                         "sample": "each step one outer iteration of the full workload through "
+                                   "%s" % ("the reference's own AUNTF (NTF%s) with its "
+                                           "DenseDimensionTree, compiled unmodified from its "
+                                           "sources (oracle/_ref)" % args.algo.upper()
+                                           if r["kind"] == "reference" else
+                                           "the oracle's restatement")},
         "e2e": {"value": value, "unit": "iters/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
+        "step_ms": {"min": min(steps_ms) if steps_ms else None,
+                    "max": max(steps_ms) if steps_ms else None},
+        "final_rel_error": r["error"],
+        "setup_s": r["setup_s"],
         "wall_s": wall,
     }
     print(json.dumps(line))
@@ -411,14 +423,15 @@ def main():
                "step": "set_tensor(host) + set_factors + %d iterations + get_factors" % T}
         del xh
 
+    ctx.close()
+    del X
+    torch.cuda.empty_cache()
     cpu = None
     if not args.no_cpu and world == 1 and rank == 0:
         try:
-            cpu = cpu_sample(gpu, torch, dev, dims, A, sigma, F0, args.algo)
+            cpu = cpu_sample(dims, k, args.algo)
         except Exception as ex:  # the baseline is reported, not required
             cpu = {"value": None, "error": str(ex)[:200]}
-    ctx.close()
-    del X
 
     if rank == 0:
         line = {
@@ -428,10 +441,9 @@ def main():
             "dtype": args.precision,
             "data": "synthetic: rank-%d CP model, U[0,1) factors, 1%% Gaussian noise, clipped >= 0, "
                     "generated on the device (Philox)" % k,
-            "config": {"workload": "%s FP32 tensor, rank %d, %s, dimension-tree MTTKRP on tensor "
-                                   "cores (%s), FP64 Gram/update/error"
-                                   % ("x".join(map(str, dims)), k, args.algo.upper(),
-                                      args.precision),
+            "config": {"workload": workload_name(dims, k, args.algo),
+                       "mttkrp": "tcgen05 tensor cores (%s operands, FP32 accumulate); FP64 "
+                                 "Grams, updates and error" % args.precision,
                        "dims": list(dims), "rank": k, "algo": args.algo,
                        "precision": args.precision, "parallelism": "replicas x%d" % world,
                        "l2": "inputs larger than L2 (%.1f GB tensor)" % (numel * 4 / 1e9)},

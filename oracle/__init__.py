@@ -78,6 +78,7 @@ def lib():
         L.orc_ntf_run.argtypes = [pd, pi64, i32, i32, ppd, pd, i32, i32, i32, i32, pd]
         L.orc_ntf_run.restype = i32
         L.orc_tensor_randu.argtypes = [i64, ctypes.c_uint, pd]
+        L.orc_synth_cp.argtypes = [pi64, i32, ppd, i32, d, ctypes.c_uint64, i32, i32, pd]
         L.orc_admm_update.argtypes = [pd, pd, i64, i32, pd, pd, i32, d]
         L.orc_admm_update.restype = i32
         L.orc_nes_update.argtypes = [pd, pd, i64, i32, pd, pd, d, d, i32]
@@ -125,7 +126,7 @@ def ref():
         R.ref_update.restype = i32
         R.ref_bpp_solve.argtypes = [pd, pd, i32, li, pd]
         R.ref_bpp_solve.restype = i32
-        R.ref_ntf_create.argtypes = [vp, i32, i32, i32, ppd, i32]
+        R.ref_ntf_create.argtypes = [vp, i32, i32, i32, ppd, i32, i32]
         R.ref_ntf_create.restype = vp
         R.ref_ntf_run.argtypes = [vp, i32]
         R.ref_ntf_run.restype = d
@@ -195,12 +196,12 @@ class RefNTF:
     library user drives it: dim_tree() before reset(initial factors),
     compute_error(), then computeNTF() for a number of iterations."""
 
-    def __init__(self, tensor, F0, algo, dimtree=True, compute_error=True):
+    def __init__(self, tensor, F0, algo, dimtree=True, compute_error=True, serial_setup=True):
         F0 = [_c(f) for f in F0]
         self.tensor = tensor
         self.k = F0[0].shape[1]
         self.h = ref().ref_ntf_create(tensor.h, self.k, ALGO[algo], int(dimtree), _fptrs(F0),
-                                      int(compute_error))
+                                      int(compute_error), int(serial_setup))
         if not self.h:
             raise ValueError("unknown algorithm")
 
@@ -322,6 +323,25 @@ def tensor_randu(dims, seed=103):
     flat = np.empty(n, dtype=np.float64)
     lib().orc_tensor_randu(n, seed, _pd(flat))
     return flat.reshape(tuple(dims), order="F")
+
+
+def synth_cp(dims, A, sigma, seed, clip=True, round_f32=False, out=None):
+    """Synthetic CP tensor [[A]] + sigma N(0,1) (clipped at 0) on the host,
+    the same function of (factors, sigma, seed) as the library's device
+    generator; round_f32 rounds every value to FP32 (the device generator's
+    FP32 output), stored as float64. `out`: a ctypes double pointer or a
+    float64 array of numel elements to fill; returns the Fortran-order array
+    when out is None."""
+    A = [_c(a) for a in A]
+    d = (ctypes.c_int64 * len(dims))(*dims)
+    X = None
+    if out is None:
+        X = np.empty(int(np.prod(dims)), dtype=np.float64)
+        out = X
+    p = _pd(out) if isinstance(out, np.ndarray) else out
+    lib().orc_synth_cp(d, len(dims), _fptrs(A), A[0].shape[1], float(sigma), int(seed),
+                       int(clip), int(round_f32), p)
+    return None if X is None else X.reshape(tuple(dims), order="F")
 
 
 def gram_loo(F, n):

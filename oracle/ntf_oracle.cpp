@@ -871,6 +871,62 @@ void orc_tensor_randu(int64_t numel, unsigned seed, double* out) {
   for (int64_t i = 0; i < numel; ++i) out[i] = dis(gen);
 }
 
+// Synthetic CP tensor on the host: X = [[A_0..A_{N-1}]] + sigma * N(0,1),
+// clipped at 0 when `clip`; the same pure function of (factors, sigma, seed)
+// as the library's device generator (planc_gpu_synth_cp_tensor): normals from
+// Philox-4x32-10 (Salmon et al., SC'11) keyed by the seed and counted by the
+// element index, through the Box-Muller transform. The noise model is the
+// reference's (dimtree/ddttensor.hpp:951-952, sigma = rho ||M|| / sqrt(numel)).
+// A[m]: row-major I_m x k. X: column-major, mode 0 fastest. With round_f32
+// every value is rounded to FP32 (and stored widened), as the device
+// generator's FP32 output is. OpenMP-parallel.
+static inline void philox4x32_10(uint32_t c[4], uint32_t key[2]) {
+  const uint32_t M0 = 0xD2511F53u, M1 = 0xCD9E8D57u;
+  const uint32_t W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
+  for (int round = 0; round < 10; ++round) {
+    const uint64_t p0 = (uint64_t)M0 * c[0], p1 = (uint64_t)M1 * c[2];
+    const uint32_t n0 = (uint32_t)(p1 >> 32) ^ c[1] ^ key[0];
+    const uint32_t n1 = (uint32_t)p1;
+    const uint32_t n2 = (uint32_t)(p0 >> 32) ^ c[3] ^ key[1];
+    const uint32_t n3 = (uint32_t)p0;
+    c[0] = n0, c[1] = n1, c[2] = n2, c[3] = n3;
+    key[0] += W0;
+    key[1] += W1;
+  }
+}
+
+void orc_synth_cp(const int64_t* dims, int N, const double* const* A, int k, double sigma,
+                  uint64_t seed, int clip, int round_f32, double* X) {
+  int64_t numel = 1;
+  for (int m = 0; m < N; ++m) numel *= dims[m];
+  const double pi = 3.14159265358979323846;
+#pragma omp parallel for schedule(static)
+  for (int64_t idx = 0; idx < numel; ++idx) {
+    int64_t rem = idx, sub[16];
+    for (int m = 0; m < N; ++m) {
+      sub[m] = rem % dims[m];
+      rem /= dims[m];
+    }
+    double v = 0.0;
+    for (int r = 0; r < k; ++r) {
+      double p = 1.0;
+      for (int m = N - 1; m >= 1; --m) p = A[m][sub[m] * k + r] * p;
+      v = std::fma(A[0][sub[0] * k + r], p, v);
+    }
+    if (sigma > 0) {
+      uint32_t c[4] = {(uint32_t)idx, (uint32_t)(idx >> 32), 0x5eedu, 0u};
+      uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+      philox4x32_10(c, key);
+      const double u1 = ((double)c[0] + 1.0) * (1.0 / 4294967296.0);  // (0, 1]
+      const double u2 = (double)c[1] * (1.0 / 4294967296.0);          // [0, 1)
+      const double z = std::sqrt(-2.0 * std::log(u1)) * std::cos(pi * (2.0 * u2));
+      v = std::fma(sigma, z, v);
+    }
+    if (clip && v < 0) v = 0;
+    X[idx] = round_f32 ? (double)(float)v : v;
+  }
+}
+
 void orc_gram_loo(const double* const* F, const int64_t* dims, int N, int k,
                   int n, double* G) {
   gram_loo(F, dims, N, k, n, G);

@@ -203,11 +203,17 @@ int ref_bpp_solve(const double* AtA, const double* AtB, int n, long ncols, doubl
 // tensor: from ref_tensor_new / ref_tensor_from (must outlive the handle).
 // F: initial factors, row-major I_n x k; they are set unnormalised through
 // NCPFactors::set and handed to reset() (which normalises each mode).
+// serial_setup != 0 runs the constructor with one OpenMP thread: AUNTF's
+// constructor builds its reconstruction buffer with Tensor(dims), whose fill
+// loop shares one random generator among the OpenMP threads.
 void* ref_ntf_create(void* tensor, int k, int algo, int dimtree, const double* const* F,
-                     int compute_error) {
+                     int compute_error, int serial_setup) {
   Quiet q;
   planc::Tensor* T = (planc::Tensor*)tensor;
+  const int nt = omp_get_max_threads();
+  if (serial_setup) omp_set_num_threads(1);
   planc::AUNTF* s = make_solver(*T, k, algo);
+  if (serial_setup) omp_set_num_threads(nt);
   if (!s) return nullptr;
   if (dimtree) s->dim_tree(true);
   planc::NCPFactors init(T->dimensions(), k, false);

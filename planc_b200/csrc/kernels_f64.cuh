@@ -7,7 +7,7 @@
 namespace pg {
 
 // ---------------------------------------------------------------------------
-// Tensor contraction with a generated Khatri-Rao operand (FP64 DFMA).
+// Tensor contraction with a generated Khatri-Rao operand (FP64, DMMA).
 //
 //   RIGHT  (partial MTTKRP right contraction, dimtree/dimtrees.hpp:106-138,
 //           and the direct mode-0 MTTKRP, common/tensor.hpp:279-281):
@@ -20,13 +20,25 @@ namespace pg {
 // out is row-major (m, r) with row stride k; with a split-K grid
 // (gridDim.y > 1) each y-slice writes its partial to out + y*split_stride and
 // k_reduce_splits sums them in a fixed order (deterministic).
-// CTA tile: 128 rows x KP ranks x 32 reduction steps, 256 threads, each
-// thread owns 4 rows x KP/8 ranks.
+//
+// CTA tile: 128 rows x KP ranks x BK reduction steps, 256 threads (8 warps).
+// The products run on the FP64 tensor cores: warp-level
+// mma.sync.m8n8k4.f64 (the only FP64 MMA of sm_100a), each warp owning a
+// (128 / WARPS_M) x (KP / WARPS_N) block of the output as 8 x 8 accumulator
+// tiles. The next reduction tile is loaded into registers while the current
+// one is multiplied out of shared memory. Shared-memory layouts are chosen so
+// that every fragment load is two 128-byte wavefronts (no bank conflicts):
+//   RIGHT: Xs[kk][m], row stride 128 + 8 doubles (X is m-contiguous);
+//   LEFT : Xs[m][kk], row stride BK + 4 doubles (X is kk-contiguous);
+//   both : Ws[kk][r], row stride KP + 8 (KP + 16 at KP = 8).
+// Fragment layouts of m8n8k4 (f64): A element (row g, col t), B element
+// (row t, col g), C elements (row g, cols 2t, 2t+1), g = lane / 4, t = lane % 4.
 // ---------------------------------------------------------------------------
 constexpr int CT_BM = 128;
-constexpr int CT_BK = 32;  // reduction tile (16 at KP = 64 to stay within 48 KB of shared memory)
 template <int KP>
 constexpr int ct_bk() { return KP == 64 ? 16 : 32; }
+template <int KP>
+constexpr int ct_ws() { return KP % 16 == 0 ? KP + 8 : KP + 16; }
 
 struct ContractGeom {
   int64_t M;        // output rows
@@ -39,31 +51,46 @@ struct ContractGeom {
   int64_t split_stride;
 };
 
+__device__ __forceinline__ void dmma_m8n8k4(double (&c)[2], double a, double b) {
+  asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+               : "+d"(c[0]), "+d"(c[1])
+               : "d"(a), "d"(b));
+}
+
 template <int KP, bool LEFT>
-__global__ void __launch_bounds__(256) k_contract_f64(const double* __restrict__ X,
-                                                      ContractGeom g, WGen wg, int k,
-                                                      double* __restrict__ out) {
-  constexpr int TN = KP / 8;
+__global__ void __launch_bounds__(256, 2) k_contract_f64(const double* __restrict__ X,
+                                                         ContractGeom g, WGen wg, int k,
+                                                         double* __restrict__ out) {
   constexpr int BK = ct_bk<KP>();
   constexpr int XPT = BK * CT_BM / 256;  // X elements per thread per tile
-  __shared__ double Xs[BK][CT_BM + 1];
-  __shared__ double Ws[BK][KP];
+  constexpr int WPT = (BK * KP + 255) / 256;
+  constexpr int WARPS_M = KP >= 32 ? 4 : 8;
+  constexpr int WARPS_N = 8 / WARPS_M;
+  constexpr int MT = CT_BM / WARPS_M / 8;  // 8-row MMA tiles per warp
+  constexpr int NT = KP / WARPS_N / 8;     // 8-rank MMA tiles per warp
+  constexpr int SX = LEFT ? BK + 4 : CT_BM + 8;
+  constexpr int SW = ct_ws<KP>();
+  __shared__ __align__(16) double Xs[LEFT ? CT_BM * SX : BK * SX];
+  __shared__ __align__(16) double Ws[BK * SW];
   const int tid = threadIdx.x;
-  const int tr = tid & 7, tm = tid >> 3;
+  const int lane = tid & 31, warp = tid >> 5;
+  const int fg = lane >> 2, ft = lane & 3;
+  const int wm0 = (warp % WARPS_M) * (MT * 8);
+  const int wn0 = (warp / WARPS_M) * (NT * 8);
   const int64_t m0 = (int64_t)blockIdx.x * CT_BM;
   const int64_t t_begin = (int64_t)blockIdx.y * g.tiles_per_split;
   int64_t t_end = t_begin + g.tiles_per_split;
   if (t_end > g.ktiles) t_end = g.ktiles;
   const int64_t tilesA = (g.A + BK - 1) / BK;
 
-  double acc[4][TN];
+  double acc[MT][NT][2];
 #pragma unroll
-  for (int i = 0; i < 4; ++i)
+  for (int i = 0; i < MT; ++i)
 #pragma unroll
-    for (int j = 0; j < TN; ++j) acc[i][j] = 0.0;
+    for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
   double xr[XPT];
-  double wr[(BK * KP + 255) / 256];
+  double wr[WPT];
 
   auto load_tile = [&](int64_t t) {
     if constexpr (!LEFT) {
@@ -79,7 +106,7 @@ __global__ void __launch_bounds__(256) k_contract_f64(const double* __restrict__
       WIdx base;
       if (wg.nf > 1) widx_init(wg, j0, base);
 #pragma unroll
-      for (int i = 0; i < (BK * KP + 255) / 256; ++i) {
+      for (int i = 0; i < WPT; ++i) {
         int e = tid + 256 * i;
         double v = 0.0;
         if (e < BK * KP) {
@@ -111,7 +138,7 @@ __global__ void __launch_bounds__(256) k_contract_f64(const double* __restrict__
       WIdx base;
       widx_init(wg, a0 + g.A * b, base);
 #pragma unroll
-      for (int i = 0; i < (BK * KP + 255) / 256; ++i) {
+      for (int i = 0; i < WPT; ++i) {
         int e = tid + 256 * i;
         double v = 0.0;
         if (e < BK * KP) {
@@ -131,16 +158,16 @@ __global__ void __launch_bounds__(256) k_contract_f64(const double* __restrict__
     if constexpr (!LEFT) {
       const int mm = tid & 127;
 #pragma unroll
-      for (int i = 0; i < XPT; ++i) Xs[(tid >> 7) + 2 * i][mm] = xr[i];
+      for (int i = 0; i < XPT; ++i) Xs[((tid >> 7) + 2 * i) * SX + mm] = xr[i];
     } else {
       const int aa = tid % BK;
 #pragma unroll
-      for (int i = 0; i < XPT; ++i) Xs[aa][tid / BK + (256 / BK) * i] = xr[i];
+      for (int i = 0; i < XPT; ++i) Xs[(tid / BK + (256 / BK) * i) * SX + aa] = xr[i];
     }
 #pragma unroll
-    for (int i = 0; i < (BK * KP + 255) / 256; ++i) {
+    for (int i = 0; i < WPT; ++i) {
       int e = tid + 256 * i;
-      if (e < BK * KP) Ws[e / KP][e % KP] = wr[i];
+      if (e < BK * KP) Ws[(e / KP) * SW + (e % KP)] = wr[i];
     }
   };
 
@@ -150,28 +177,33 @@ __global__ void __launch_bounds__(256) k_contract_f64(const double* __restrict__
     store_tile();
     __syncthreads();
     if (t + 1 < t_end) load_tile(t + 1);
-#pragma unroll 8
-    for (int kk = 0; kk < BK; ++kk) {
-      double xv[4], wv[TN];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) xv[i] = Xs[kk][tm + 32 * i];
+    for (int s4 = 0; s4 < BK / 4; ++s4) {
+      const int kk = s4 * 4 + ft;
+      double af[MT], bf[NT];
 #pragma unroll
-      for (int j = 0; j < TN; ++j) wv[j] = Ws[kk][tr + 8 * j];
+      for (int i = 0; i < MT; ++i) {
+        const int m = wm0 + i * 8 + fg;
+        af[i] = LEFT ? Xs[m * SX + kk] : Xs[kk * SX + m];
+      }
 #pragma unroll
-      for (int i = 0; i < 4; ++i)
+      for (int j = 0; j < NT; ++j) bf[j] = Ws[kk * SW + wn0 + j * 8 + fg];
 #pragma unroll
-        for (int j = 0; j < TN; ++j) acc[i][j] = fma(xv[i], wv[j], acc[i][j]);
+      for (int i = 0; i < MT; ++i)
+#pragma unroll
+        for (int j = 0; j < NT; ++j) dmma_m8n8k4(acc[i][j], af[i], bf[j]);
     }
   }
   double* o = out + (int64_t)blockIdx.y * g.split_stride;
 #pragma unroll
-  for (int i = 0; i < 4; ++i) {
-    int64_t gm = m0 + tm + 32 * i;
+  for (int i = 0; i < MT; ++i) {
+    const int64_t gm = m0 + wm0 + i * 8 + fg;
     if (gm >= g.M) continue;
 #pragma unroll
-    for (int j = 0; j < TN; ++j) {
-      int r = tr + 8 * j;
-      if (r < k) o[gm * k + r] = acc[i][j];
+    for (int j = 0; j < NT; ++j) {
+      const int r = wn0 + j * 8 + 2 * ft;
+      if (r < k) o[gm * k + r] = acc[i][j][0];
+      if (r + 1 < k) o[gm * k + r + 1] = acc[i][j][1];
     }
   }
 }

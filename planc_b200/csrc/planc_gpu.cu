@@ -95,6 +95,10 @@ struct planc_gpu_ctx {
 
   double* X64 = nullptr;         // FP64 tensor (plain path)
   TcTensor tct;                  // tensor-core operand copy (BF16 paths)
+  // copies with mode n moved last for the direct (non-tree) MTTKRP on the
+  // tensor cores, made on first use; the last mode uses tct when its view
+  // already splits before the last mode
+  TcTensor tcd[kMaxModes];
   double* normX2 = nullptr;      // device scalar ||X||^2
   double* F[kMaxModes] = {nullptr};
   double* M[kMaxModes] = {nullptr};
@@ -567,9 +571,72 @@ void run_ttv_left(planc_gpu_ctx* c, const TT* T, int64_t A, int64_t B, const dou
 }
 
 // ---------------------------------------------------------------- MTTKRP
-// Direct MTTKRP of mode n (common/tensor.hpp:246-327), FP64.
+// The tensor-core view whose left contraction is mode n's direct MTTKRP:
+// the tree's copy for the last mode when its view splits before it, else the
+// mode's own copy (ensure_direct makes them before any graph capture).
+const TcTensor& direct_view(planc_gpu_ctx* c, int n) {
+  if (n == c->N - 1 && !c->bal4 && c->s == c->N - 2) return c->tct;
+  if (!c->tcd[n].hi) fail(PLANC_GPU_ERR_STATE, "internal: direct tensor-core copy missing");
+  return c->tcd[n];
+}
+
+// Makes the direct-MTTKRP copies of a tensor-core context and sizes their
+// images and split-K scratch (outside graph capture; any allocation bumps
+// the buffer epoch so cached graphs are rebuilt).
+void ensure_direct(planc_gpu_ctx* c) {
+  if (c->precision == PLANC_GPU_PREC_FP64) return;
+  bool grew = false;
+  size_t need = 0;
+  CK(tc_ensure(c->tct, c->k));
+  for (int n = 0; n < c->N; ++n) {
+    if (!(n == c->N - 1 && !c->bal4 && c->s == c->N - 2) && !c->tcd[n].hi) {
+      cudaError_t e = tc_direct_copy(c->tcd[n], c->tct, c->dims, c->N, n, c->s, c->stream);
+      if (e == cudaErrorInvalidValue)
+        fail(PLANC_GPU_ERR_CUDA, "cuTensorMapEncodeTiled rejected a direct-MTTKRP view");
+      CK(e);
+      grew = true;
+    }
+    TcTensor& t = const_cast<TcTensor&>(direct_view(c, n));
+    uint8_t* before[3] = {t.bimg, t.bimg0, t.wimg};
+    CK(tc_ensure(t, c->k));
+    if (before[0] != t.bimg || before[1] != t.bimg0 || before[2] != t.wimg) grew = true;
+    need = std::max(need, tc_scratch_elems(t, eff_sm(c), c->k));
+  }
+  if (need > c->scratch_elems) {
+    dalloc(&c->scratch, need);
+    c->scratch_elems = need;
+    grew = true;
+  }
+  if (grew) c->buf_epoch++;
+}
+
+// Direct MTTKRP of mode n on the tensor cores: the left contraction of the
+// (prod_{i != n} I_i) x I_n view against the Khatri-Rao rows of the other
+// modes, split-K partials summed in a fixed order.
+void mttkrp_direct_tc(planc_gpu_ctx* c, int n, double* out) {
+  std::vector<int> modes;
+  for (int m = 0; m < c->N; ++m)
+    if (m != n) modes.push_back(m);
+  WGen wg = make_wgen(c, modes);
+  const TcTensor& t = direct_view(c, n);
+  if (tc_scratch_elems(t, eff_sm(c), c->k) > c->scratch_elems)
+    fail(PLANC_GPU_ERR_STATE, "internal: split-K scratch larger than planned");
+  int nsplit = 0;
+  launch(c, KC_CONTRACT_LEFT, [&] {
+    nsplit = tc_left(t, wg, c->k, c->scratch, c->status_dev, eff_sm(c), c->stream);
+  });
+  const int64_t nn = c->dims[n] * c->k;
+  launch(c, KC_REDUCE, [&] { reduce_splits(c->stream, c->scratch, nsplit, nn, nn, out); });
+}
+
+// Direct MTTKRP of mode n (common/tensor.hpp:246-327): FP64 contraction, or
+// on a tensor-core context the left contraction of mode n's view.
 void mttkrp_direct(planc_gpu_ctx* c, int n, double* out) {
-  if (!c->X64) fail(PLANC_GPU_ERR_UNSUPPORTED, "direct MTTKRP needs the FP64 tensor copy");
+  if (c->precision != PLANC_GPU_PREC_FP64) {
+    mttkrp_direct_tc(c, n, out);
+    return;
+  }
+  if (!c->X64) fail(PLANC_GPU_ERR_STATE, "no FP64 tensor copy");
   std::vector<int> modes;
   for (int m = 0; m < c->N; ++m)
     if (m != n) modes.push_back(m);
@@ -1158,6 +1225,7 @@ void free_all(planc_gpu_ctx* c) {
   };
   f(c->X64);
   tc_free(c->tct);
+  for (int n = 0; n < kMaxModes; ++n) tc_free(c->tcd[n]);
   f(c->normX2);
   for (int n = 0; n < kMaxModes; ++n) {
     f(c->F[n]);
@@ -1311,6 +1379,10 @@ int planc_gpu_set_tensor(planc_gpu_ctx* c, const void* X, int dtype, const int64
     c->s = nmodes / 2;  // ntf/auntf.hpp:122-123
     // a matrix (NMF): rows = mode 0 (L), columns = mode 1 (R)
     if (nmodes == 2) c->s = 0;
+    // no tree above four modes: the tensor-core copy splits before the last
+    // mode, whose direct MTTKRP it then serves as is
+    if (nmodes > 4 && c->precision != PLANC_GPU_PREC_FP64) c->s = nmodes - 2;
+    for (int n = 0; n < kMaxModes; ++n) tc_free(c->tcd[n]);
     // PLANC_GPU_DIMTREE_SPLIT=reference keeps the reference's split everywhere
     const char* split_env = getenv("PLANC_GPU_DIMTREE_SPLIT");
     const bool ref_split = split_env && strcmp(split_env, "reference") == 0;
@@ -1367,6 +1439,7 @@ int planc_gpu_set_tensor(planc_gpu_ctx* c, const void* X, int dtype, const int64
         if (te == cudaErrorInvalidValue)
           fail(PLANC_GPU_ERR_CUDA, "cuTensorMapEncodeTiled rejected the tensor map");
         CK(te);
+        c->tct.left_nf = c->s + 1;
       }
       CK(cudaGetLastError());
       CK(cudaStreamSynchronize(c->stream));
@@ -1386,8 +1459,6 @@ int planc_gpu_set_factors(planc_gpu_ctx* c, const double* const* F, const double
     if (!c->have_tensor) fail(PLANC_GPU_ERR_STATE, "set the tensor before the factors");
     if (k < 1 || k > kMaxRank)
       fail(PLANC_GPU_ERR_UNSUPPORTED, "rank must be in [1, " + std::to_string(kMaxRank) + "]");
-    if (c->precision != PLANC_GPU_PREC_FP64 && (c->N != 3 && c->N != 4))
-      fail(PLANC_GPU_ERR_UNSUPPORTED, "tensor-core precisions run the dimension tree (N in {3,4})");
     set_device(c);
     reset_graph(c);
     if (k != c->k) {
@@ -1487,11 +1558,10 @@ int planc_gpu_run(planc_gpu_ctx* c, int algo, int iters, int dimtree, int comput
     if (iters < 0) fail(PLANC_GPU_ERR_ARG, "iters < 0");
     if (!known_algo(algo)) fail(PLANC_GPU_ERR_ARG, "unknown algorithm " + std::to_string(algo));
     bool dt = dimtree && (c->N == 3 || c->N == 4);
-    if (c->precision != PLANC_GPU_PREC_FP64 && !dt)
-      fail(PLANC_GPU_ERR_UNSUPPORTED, "tensor-core precisions run the dimension tree only");
     if (iters == 0) return;
     set_device(c);
     ensure_buffers(c);
+    if (!dt) ensure_direct(c);
     // NTFNES evaluates the error every iteration (accelerated(true),
     // ntf/ntfnes.hpp:193): its acceleration compares against it
     const bool nes = algo == PLANC_GPU_NESTEROV;
@@ -1543,8 +1613,7 @@ int planc_gpu_mttkrp(planc_gpu_ctx* c, int mode, int dimtree, double* out) {
     set_device(c);
     ensure_buffers(c);
     bool dt = dimtree && (c->N == 3 || c->N == 4);
-    if (c->precision != PLANC_GPU_PREC_FP64 && !dt)
-      fail(PLANC_GPU_ERR_UNSUPPORTED, "tensor-core precisions run the dimension tree only");
+    if (!dt) ensure_direct(c);
     if (dt) {
       // the tree state for `mode` comes from the current factors
       dimtree_prereq(c, mode);
@@ -1580,7 +1649,9 @@ int planc_gpu_objective_error(planc_gpu_ctx* c, double* err) {
     // <X, model> needs the MTTKRP of the last mode from the current factors:
     // directly on the FP64 tensor, through the tree on the tensor-core copy
     // (whose 4-way form is the balanced tree)
-    last_mode_mttkrp(c, c->precision != PLANC_GPU_PREC_FP64);
+    const bool tree = c->precision != PLANC_GPU_PREC_FP64 && (c->N == 3 || c->N == 4);
+    if (c->precision != PLANC_GPU_PREC_FP64 && !tree) ensure_direct(c);
+    last_mode_mttkrp(c, tree);
     CK(cudaMemsetAsync(c->counter_dev, 0, sizeof(int), c->stream));
     error_kernel(c);
     CK(cudaMemcpyAsync(err, c->errs_dev, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -1597,8 +1668,7 @@ int planc_gpu_mode_begin(planc_gpu_ctx* c, int mode, int dimtree, double* gram_o
     set_device(c);
     ensure_buffers(c);
     bool dt = dimtree && (c->N == 3 || c->N == 4);
-    if (c->precision != PLANC_GPU_PREC_FP64 && !dt)
-      fail(PLANC_GPU_ERR_UNSUPPORTED, "tensor-core precisions run the dimension tree only");
+    if (!dt) ensure_direct(c);
     gram_loo(c, mode);
     mttkrp_any(c, mode, dt, c->M[mode]);
     if (gram_out)
@@ -1686,8 +1756,7 @@ int planc_gpu_mttkrp_device(planc_gpu_ctx* c, int mode, const double* const* F_d
     ensure_buffers(c);
     const bool dt = (flags & 1) && (c->N == 3 || c->N == 4);
     const bool reuse = (flags & 2) != 0;
-    if (c->precision != PLANC_GPU_PREC_FP64 && !dt)
-      fail(PLANC_GPU_ERR_UNSUPPORTED, "tensor-core precisions run the dimension tree only");
+    if (!dt) ensure_direct(c);
     double* saved[kMaxModes];
     for (int n = 0; n < c->N; ++n) {
       saved[n] = c->F[n];

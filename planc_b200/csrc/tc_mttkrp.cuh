@@ -1223,6 +1223,57 @@ __global__ void k_tc_convert(const T* __restrict__ X, int64_t L, int64_t R, int6
   }
 }
 
+// Copy of the tensor-core operand with mode n moved last, for the direct
+// (non-tree) MTTKRP of mode n as one left contraction. Element (i_0..i_{N-1})
+// sits at l + Lpad * j in the source view (l over modes <= s, j over the
+// others, lowest mode fastest in each) and goes to l' + Lpad' * i_n, l' over
+// the modes other than n in increasing order, lowest fastest (the row order
+// of the reference's krp_leave_out_one, common/ncpfactors.hpp:171-233). A
+// permutation of the stored BF16 values: the copies hold exactly the numbers
+// the tree's copy holds. Rows l' >= L' (padding) are zero.
+struct TcPermDesc {
+  int64_t dims[kMaxModes];
+  int N, n, s;
+  int64_t Lpad;         // source row stride
+  int64_t Lp, Lppad;    // target rows (numel / I_n) and row stride
+};
+
+__global__ void k_tc_permute(const __nv_bfloat16* __restrict__ hi, const __nv_bfloat16* __restrict__ lo,
+                             TcPermDesc d, __nv_bfloat16* __restrict__ ohi,
+                             __nv_bfloat16* __restrict__ olo) {
+  const int64_t total = d.Lppad * d.dims[d.n];
+  const __nv_bfloat16 zero = __ushort_as_bfloat16((unsigned short)0);
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t lp = e % d.Lppad, in = e / d.Lppad;
+    __nv_bfloat16 vh = zero, vl = zero;
+    if (lp < d.Lp) {
+      int64_t rem = lp, l = 0, j = 0, sl = 1, sj = 1;
+      for (int m = 0; m < d.N; ++m) {
+        int64_t im;
+        if (m == d.n) {
+          im = in;
+        } else {
+          im = rem % d.dims[m];
+          rem /= d.dims[m];
+        }
+        if (m <= d.s) {
+          l += im * sl;
+          sl *= d.dims[m];
+        } else {
+          j += im * sj;
+          sj *= d.dims[m];
+        }
+      }
+      const int64_t src = l + d.Lpad * j;
+      vh = hi[src];
+      if (lo) vl = lo[src];
+    }
+    ohi[e] = vh;
+    if (olo) olo[e] = vl;
+  }
+}
+
 // Self-test of the bounded-wait path: one thread waits on an mbarrier that no
 // one ever arrives on, with a limit of `limit` cycles; the wait runs out, sets
 // *status = kStTimeout and the kernel returns normally.
@@ -1255,6 +1306,7 @@ struct TcTensor {
   size_t bimg0_bytes = 0;
   int kpad = 0;
   int64_t I0 = 0;            // mode-0 size (factored left contraction when I0 % 64 == 0)
+  int left_nf = 0;           // modes the left contraction's Khatri-Rao rows span
   uint8_t* wimg = nullptr;   // Khatri-Rao image of the long-K kernel (k_tc_long)
   size_t wimg_bytes = 0;
   int64_t wimg_K = 0;        // longest K it must hold (0: long-K kernel unused)
@@ -1304,7 +1356,11 @@ inline void tc_free(TcTensor& t) {
   t.bimg_bytes = t.bimg0_bytes = t.wimg_bytes = 0;
 }
 
-inline bool tc_left_factored(const TcTensor& t) { return t.I0 > 0 && t.I0 % TC_BK == 0; }
+// The factored left contraction takes W = F_first x tail with a tail of one
+// or two factors: views whose left contraction lists two or three modes.
+inline bool tc_left_factored(const TcTensor& t) {
+  return t.I0 > 0 && t.I0 % TC_BK == 0 && t.left_nf >= 2 && t.left_nf <= 3;
+}
 
 // Returns cudaSuccess or an error; false map creation is reported as
 // cudaErrorInvalidValue.
@@ -1337,6 +1393,55 @@ inline cudaError_t tc_set_tensor(TcTensor& t, const void* src, bool src_f64, int
   else if (ok) {
     t.mR_lo = t.mR_hi;
     t.mL_lo = t.mL_hi;
+  }
+  return ok ? cudaSuccess : cudaErrorInvalidValue;
+}
+
+// Direct-MTTKRP copy of mode n (k_tc_permute) from the tree's copy `src`
+// whose view splits at s. dst's view: L' = numel / I_n rows, R' = I_n, with
+// I0 the size of the fastest remaining mode (the factored left contraction
+// applies when it is a multiple of 64). Returns cudaSuccess or an error;
+// failed map creation is reported as cudaErrorInvalidValue.
+inline cudaError_t tc_direct_copy(TcTensor& dst, const TcTensor& src, const int64_t* dims, int N,
+                                  int n, int s, cudaStream_t st) {
+  tc_free(dst);
+  TcPermDesc d;
+  memset(&d, 0, sizeof(d));
+  int64_t numel = 1;
+  for (int m = 0; m < N; ++m) {
+    d.dims[m] = dims[m];
+    numel *= dims[m];
+  }
+  d.N = N;
+  d.n = n;
+  d.s = s;
+  d.Lpad = src.Lpad;
+  d.Lp = numel / dims[n];
+  d.Lppad = (d.Lp + 7) / 8 * 8;
+  dst.L = d.Lp;
+  dst.R = dims[n];
+  dst.Lpad = d.Lppad;
+  dst.prec = src.prec;
+  dst.I0 = dims[n == 0 ? 1 : 0];
+  dst.left_nf = N - 1;
+  const size_t cnt = (size_t)d.Lppad * dims[n];
+  cudaError_t e = cudaMalloc(&dst.hi, cnt * 2);
+  if (e != cudaSuccess) return e;
+  if (src.lo) {
+    e = cudaMalloc(&dst.lo, cnt * 2);
+    if (e != cudaSuccess) return e;
+  }
+  k_tc_permute<<<4096, 256, 0, st>>>(src.hi, src.lo, d, dst.hi, dst.lo);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) return e;
+  bool ok = tc_make_map(&dst.mR_hi, dst.hi, dst.L, dst.R, dst.Lpad, 64, 64) &&
+            tc_make_map(&dst.mL_hi, dst.hi, dst.L, dst.R, dst.Lpad, 64, 128);
+  if (ok && dst.lo)
+    ok = tc_make_map(&dst.mR_lo, dst.lo, dst.L, dst.R, dst.Lpad, 64, 64) &&
+         tc_make_map(&dst.mL_lo, dst.lo, dst.L, dst.R, dst.Lpad, 64, 128);
+  else if (ok) {
+    dst.mR_lo = dst.mR_hi;
+    dst.mL_lo = dst.mL_hi;
   }
   return ok ? cudaSuccess : cudaErrorInvalidValue;
 }

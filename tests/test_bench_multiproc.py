@@ -55,3 +55,39 @@ def test_replica_value_single_process():
     import bench
     value, ms = bench.replica_value(200.0, steps=20, world=1)
     assert ms == 200.0 and value == pytest.approx(100.0)
+
+
+def _bench(args, env_extra=None):
+    import json
+    import subprocess
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    env = dict(os.environ, **(env_extra or {}))
+    r = subprocess.run([sys.executable, os.path.join(root, "bench.py")] + args, cwd=root,
+                       env=env, capture_output=True, text=True, timeout=600)
+    assert r.returncode == 0, r.stderr[-2000:]
+    lines = [l for l in r.stdout.splitlines() if l.startswith("{")]
+    return [json.loads(l) for l in lines]
+
+
+def test_reference_arm_line_on_cpu():
+    # --impl reference runs the reference's CPU implementation (or the
+    # oracle's restatement) on the host only: one JSON line with the
+    # contract's keys, the e2e key repeating the value with no copies
+    out = _bench(["--impl", "reference", "--dims", "24,20,16", "--rank", "4", "--steps", "3",
+                  "--warmup", "1"], {"CUDA_VISIBLE_DEVICES": ""})
+    assert len(out) == 1
+    line = out[0]
+    assert line["impl"] == "reference" and line["unit"] == "iters/s" and line["steps"] == 3
+    assert line["value"] > 0 and line["higher_is_better"] is True
+    assert line["e2e"] == {"value": line["value"], "unit": "iters/s", "h2d_bytes_per_step": 0,
+                           "d2h_bytes_per_step": 0}
+    assert line["cpu_baseline"]["kind"] in ("reference", "port")
+    assert line["cpu_baseline"]["value"] == line["value"]
+    assert 0 < line["final_rel_error"] < 1
+
+
+def test_reference_arm_other_ranks_exit_without_output():
+    out = _bench(["--impl", "reference", "--dims", "12,10,8", "--rank", "3", "--steps", "1",
+                  "--warmup", "0"], {"RANK": "1", "WORLD_SIZE": "2", "CUDA_VISIBLE_DEVICES": ""})
+    assert out == []

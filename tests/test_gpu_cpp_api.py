@@ -122,3 +122,26 @@ def test_dense_nmf_driver_matches_oracle(gpu, oracle_lib, tmp_path, algo, code):
     W = np.loadtxt(out + "_W", ndmin=2)
     H = np.loadtxt(out + "_H", ndmin=2)
     assert rel(W, Wo) < 1e-10 and rel(H, Ho) < 1e-10
+
+
+@pytest.mark.parametrize("prec", ["bf16", "bf16x2"])
+def test_dense_ntf_direct_mttkrp_mixed_precision(gpu, oracle_lib, tmp_path, prec):
+    # AUNTF's default dim_tree(false) (the reference's direct MTTKRP,
+    # common/tensor.hpp:246-327) on the tensor-core precisions:
+    # dense_ntf --dimtree 0 --precision bf16|bf16x2 against the FP64 oracle
+    exe = str(tmp_path / "dense_ntf")
+    _compile(os.path.join(PKG, "cpp", "ntf.cpp"), exe)
+    dims, k, iters = (48, 40, 36), 4, 8
+    F0 = init_factors(dims, k, seed=65)
+    init, out = str(tmp_path / "init"), str(tmp_path / "out")
+    _write_init(init, F0)
+    res = subprocess.run([exe, "-a", "1", "-d", " ".join(map(str, dims)), "-k", str(k), "-t",
+                          str(iters), "-e", "1", "--dimtree", "0", "--precision", prec, "--init",
+                          init, "-o", out], capture_output=True, text=True, check=True)
+    errs = [float(m) for m in re.findall(r"relative_error at it::\d+::([0-9.eE+-]+)", res.stdout)]
+    assert len(errs) == iters
+    X = oracle_lib.tensor_randu(dims, 103)
+    Fo, lo, eo = oracle_lib.ntf_run(X, F0, "hals", iters, dimtree=False)
+    # the tensor is uniform noise (error ~0.5): BF16 rounding moves the
+    # reported error by ~1e-4
+    assert abs(errs[-1] - eo[-1]) < (1e-3 if prec == "bf16" else 1e-5)

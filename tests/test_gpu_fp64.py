@@ -198,3 +198,38 @@ def test_synth_generator_matches_model(gpu):
     gpu.synth_cp_tensor(0, y.data_ptr(), "f64", dims, A, 0.5, 42, clip=False)
     z = (y - x).cpu().numpy() / 0.5
     assert abs(z.mean()) < 0.05 and abs(z.std() - 1) < 0.05
+
+
+def _golden():
+    import importlib.util
+    import os
+    gold = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+    spec = importlib.util.spec_from_file_location("make_golden", os.path.join(gold, "make_golden.py"))
+    mg = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mg)
+    return mg, np.load(os.path.join(gold, "ref_ntf_runs.npz"))
+
+
+_MG, _G = _golden()
+
+
+@pytest.mark.parametrize("name,algo", [(n, a) for n, _, _, _, _, al, _, _ in _MG.RUNS for a in al])
+def test_ntf_run_matches_reference_golden(gpu, name, algo):
+    # the FP64 GPU path against whole runs of the reference's own AUNTF
+    # (tests/golden/ref_ntf_runs.npz; the 64^3 rank-8 HALS/MU/BPP runs of
+    # 20 iterations are the benchmark's configuration 1)
+    dims = tuple(int(d) for d in _G[name + "_dims"])
+    k, iters, dt, seed = (int(v) for v in _G[name + "_meta"])
+    X, F0 = _MG.run_inputs(dims, k, float(_G[name + "_noise"][0]), seed)
+    with _ctx(gpu, X, F0) as c:
+        e = c.run(algo, iters, dimtree=bool(dt), compute_error=True)
+        F, lam = c.get_factors()
+    pre = "%s_%s_" % (name, algo)
+    for i in range(len(dims)):
+        assert rel(F[i], _G[pre + "F%d" % i]) < TOL, i
+    assert rel(lam, _G[pre + "lam"]) < TOL
+    ref_err = _G[pre + "err"]
+    if algo == "nesterov":
+        assert abs(e[-1] - ref_err[-1]) <= TOL * ref_err[-1]
+    else:
+        assert np.max(np.abs(e - ref_err) / ref_err) < TOL

@@ -159,3 +159,50 @@ def test_tc_ntf_fused_ttv_matches_fp64_error(gpu):
             c.set_factors(F0)
             errs[p] = c.run("hals", iters)
     assert abs(errs["bf16x2"][-1] - errs["fp64"][-1]) < 1e-4
+
+
+# ---- direct (non-tree) MTTKRP on the tensor cores: AUNTF's default
+# dim_tree(false) path (common/tensor.hpp:246-327) and tensors of 2 or 5+ modes.
+# Each mode is the left contraction of a copy of the BF16 tensor with that
+# mode moved last (a permutation of the stored values).
+@pytest.mark.parametrize("prec", ["bf16", "bf16x2"])
+@pytest.mark.parametrize("dims,k", [((64, 64, 64), 8), ((40, 33, 21), 32), ((13, 7, 20), 5),
+                                    ((9, 8, 7, 10), 64), ((128, 5, 9, 64), 16),
+                                    ((5, 4, 6, 3, 4), 6), ((4, 3, 5, 2, 3, 4), 12),
+                                    ((300, 70), 20), ((64, 128), 64)])
+def test_tc_direct_mttkrp_all_modes(gpu, oracle_lib, prec, dims, k):
+    X, _ = cp_tensor(dims, 3, seed=25)
+    F = init_factors(dims, k, seed=26)
+    Fn = _normalized(F)
+    with gpu.Context(0, prec) as c:
+        c.set_tensor(X)
+        c.set_factors(F)
+        for n in range(len(dims)):
+            ref = oracle_lib.mttkrp_direct(X, Fn, n)
+            got = c.mttkrp(n, dimtree=False)
+            assert rel(got, ref) < BOUND[prec], (n, rel(got, ref))
+        if len(dims) in (3, 4):  # the tree and the direct path agree as well
+            for n in range(len(dims)):
+                assert rel(c.mttkrp(n, dimtree=True), c.mttkrp(n, dimtree=False)) < 2 * BOUND[prec]
+
+
+@pytest.mark.parametrize("prec", ["bf16", "bf16x2"])
+@pytest.mark.parametrize("dims,k,algo", [((64, 64, 64), 8, "hals"), ((30, 24, 20, 16), 5, "anlsbpp"),
+                                         ((12, 10, 9, 8, 7), 4, "mu")])
+def test_tc_direct_ntf_matches_fp64(gpu, prec, dims, k, algo):
+    # whole runs with dimtree = false (and 5 modes, where no tree exists):
+    # final relative error within the mixed-precision bounds of the FP64 path
+    iters = 12
+    X, _ = cp_tensor(dims, k, noise=0.01, seed=27)
+    F0 = init_factors(dims, k, seed=28)
+    with gpu.Context(0, "fp64") as c:
+        c.set_tensor(X)
+        c.set_factors(F0)
+        e64 = c.run(algo, iters, dimtree=False)
+    with gpu.Context(0, prec) as c:
+        c.set_tensor(X.astype(np.float32))
+        c.set_factors(F0)
+        e = c.run(algo, iters, dimtree=False)
+        assert abs(c.objective_error() - e[-1]) < 1e-3
+    bound = 1e-3 if prec == "bf16" else 1e-4
+    assert abs(e[-1] - e64[-1]) < bound, (e[-1], e64[-1])
