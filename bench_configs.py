@@ -199,7 +199,7 @@ def cfg4(args, gpu, torch, dev):
 
 
 def cfg5(args, gpu, torch, dev):
-    from planc_b200.autograd import CPLoss
+    from planc_b200.autograd import CPLoss, projected_accelerated_step
     dims, k, T = (512, 512, 512), 32, 200
     rng = np.random.default_rng(501)
     A = [rng.random((d, k)) for d in dims]
@@ -216,12 +216,15 @@ def cfg5(args, gpu, torch, dev):
             y.grad = None
         loss = lossf(*Y)
         loss.backward()
+        t_next = 0.5 * (1 + (1 + 4 * t * t) ** 0.5)
+        mom = (t - 1) / t_next
         with torch.no_grad():
-            newF = [(y - eta * y.grad).clamp_(min=0.0) for y in Y]
-            t_next = 0.5 * (1 + (1 + 4 * t * t) ** 0.5)
-            mom = (t - 1) / t_next
-            newY = [nf + mom * (nf - fp) for nf, fp in zip(newF, Fprev)]
-        return newF, [y.detach() for y in newY], t_next, loss.detach()
+            # F = max(Y - eta grad, 0), Y = F + mom (F - F_prev): one launch
+            newF = [torch.empty_like(y) for y in Y]
+            newY = [torch.empty_like(y) for y in Y]
+            projected_accelerated_step(lossf, [y.detach() for y in Y], [y.grad for y in Y], Fprev,
+                                       eta, mom, newF, newY)
+        return newF, newY, t_next, loss.detach()
 
     with torch.no_grad():
         Lmax = max(float(torch.linalg.matrix_norm((F[1].T @ F[1]) * (F[2].T @ F[2]), 2)),

@@ -150,6 +150,69 @@ int planc_gpu_bpp_solve(planc_gpu_ctx* ctx, const double* AtA, const double* AtB
                         int n, int64_t ncols, double* X, int32_t* passive,
                         int32_t* iters);
 
+/* ---- The differentiable CP loss 1/2 ||X - [[F_0..F_{N-1}]]||^2 on the
+ * context's tensor, for caller-supplied DEVICE factors (row-major I_n x k
+ * FP64; k and the mode sizes those of the context). Its gradient is the
+ * reference's NTF gradient form (ntf/ntfnes.hpp:138-147, G_{-n} H^T - M^T in
+ * the reference's k x I layout). Ordered on the context's stream. */
+
+/* G_out (device, N x k x k) = F_n^T F_n of every factor, and *loss_out
+ * (device) = 1/2 ||X||^2 - <M0, F_0> + 1/2 sum_ab prod_n G_n[a, b], with M0
+ * the mode-0 MTTKRP of these factors (planc_gpu_mttkrp_device). */
+int planc_gpu_cp_loss_device(planc_gpu_ctx* ctx, const double* const* F_dev, const double* M0_dev,
+                             double* G_out, double* loss_out);
+
+/* grad_dev[n] = g (F_n (prod_{m != n} G_m) - M_dev[n]) for every mode, with
+ * G from planc_gpu_cp_loss_device, M_dev[n] the mode-n MTTKRPs and g the
+ * device scalar at g_dev (the upstream gradient). */
+int planc_gpu_cp_grads_device(planc_gpu_ctx* ctx, const double* const* F_dev, const double* G,
+                              const double* const* M_dev, const double* g_dev,
+                              double* const* grad_dev);
+
+/* One projected accelerated gradient step on every factor:
+ * Fnew[n] = max(Y[n] - eta grad[n], 0), Ynew[n] = Fnew[n] + mom (Fnew[n] - Fprev[n])
+ * (element-wise; outputs may alias the inputs of the same factor). */
+int planc_gpu_cp_step_device(planc_gpu_ctx* ctx, const double* const* Y, const double* const* grad,
+                             const double* const* Fprev, double eta, double mom, double* const* Fnew,
+                             double* const* Ynew);
+
+/* ---- Device building blocks of the distributed NTF iteration (one slab of
+ * the tensor per GPU; the caller runs the collectives between them). The
+ * reference's distributed loop, distntf/distauntf.hpp, reduce-scatters the
+ * partial MTTKRP (:305-315), updates its rows, all-reduces the column norms
+ * and the k x k Grams (:92-115, ncpfactors.hpp distributed_normalize) and
+ * all-gathers the factor (:164-234). All buffers are DEVICE memory, FP64,
+ * row-major rows x k (k x k for Grams), on the context's device; the calls
+ * are ordered on the context's stream and return without synchronising
+ * (planc_gpu_sync waits and reports device-side failures). */
+
+/* Updates `rows` rows of the factor block H in place from the matching rows
+ * of the MTTKRP block M and the leave-one-out Gram G (k x k): NTFMU /
+ * NTFHALS / NTFANLSBPP::update (ntf/ntfmu.hpp:11-16, ntfhals.hpp:13-29,
+ * ntfanlsbpp.hpp:15-57) restricted to the block; the updates are row-separable. */
+int planc_gpu_update_device(planc_gpu_ctx* ctx, int algo, double* H, const double* M,
+                            const double* G, int64_t rows, int k);
+
+/* G = F^T F of a rows x k block (un-normalised; deterministic order). */
+int planc_gpu_gram_device(planc_gpu_ctx* ctx, const double* F, int64_t rows, int k, double* G);
+
+/* From G_in = the factor's whole un-normalised Gram (summed over every block):
+ * lambda_r = sqrt(G_in_rr), G_out = Gram of the normalised factor, and the
+ * block F (rows x k) scaled column by column (NCPFactors::normalize(mode),
+ * common/ncpfactors.hpp:346-351, columns of zero norm left as they are).
+ * rows may be 0 (no block on this device). */
+int planc_gpu_normalize_device(planc_gpu_ctx* ctx, double* F, int64_t rows, int k,
+                               const double* G_in, double* lambda, double* G_out);
+
+/* out_r = sum_i A[i, r] B[i, r] (k values): a block's share of <X, model>
+ * in the Gram-form error (distntf/distauntf.hpp:685-727). */
+int planc_gpu_coldot_device(planc_gpu_ctx* ctx, const double* A, const double* B, int64_t rows,
+                            int k, double* out);
+
+/* Waits for the context's stream and reports a device-side failure of the
+ * work queued before it (BPP cap, non-finite values, ...), as the run calls do. */
+int planc_gpu_sync(planc_gpu_ctx* ctx);
+
 /* MTTKRP of `mode` for caller-supplied DEVICE factors F_dev[n] (row-major
  * I_n x k FP64, k = the rank set by planc_gpu_set_factors, on the context's
  * device), written to the device buffer M_dev (row-major I_mode x k FP64).
@@ -280,6 +343,15 @@ int planc_gpu_reset_update_state(planc_gpu_ctx* ctx);
  * status the device wrote is returned in *status_out (PLANC_GPU_ERR_TIMEOUT
  * when the bounded-wait path works) and the device stays usable. */
 int planc_gpu_selftest_wait_timeout(int device, double seconds, int* status_out);
+
+/* Self-test of the cooperative NMF W sweep's bounded waits (its per-column
+ * wait for every CTA's partial sum, the routine the sweep itself runs): a
+ * cooperative launch of four CTAs in which one CTA never stores its sum. The
+ * other CTAs' waits run out after a few thousand polls, raise the sweep's
+ * error flag and the timeout status, and every CTA returns. *status_out
+ * receives the status the device wrote (PLANC_GPU_ERR_TIMEOUT when the
+ * bounded-wait path works); the device stays usable. */
+int planc_gpu_selftest_coop_timeout(int device, int* status_out);
 
 /* Kernel timing, for roofline measurement: while enabled, CUDA events bracket
  * every launch of each kernel class on the context's stream. Class ids:

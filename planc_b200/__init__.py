@@ -44,6 +44,9 @@ EXPORTS = [
     "planc_gpu_batch_create", "planc_gpu_batch_add", "planc_gpu_batch_count",
     "planc_gpu_batch_set_factors", "planc_gpu_batch_run", "planc_gpu_batch_get_factors",
     "planc_gpu_batch_autotune", "planc_gpu_batch_destroy", "planc_gpu_mttkrp_last_mode_noalloc",
+    "planc_gpu_update_device", "planc_gpu_gram_device", "planc_gpu_normalize_device",
+    "planc_gpu_coldot_device", "planc_gpu_sync", "planc_gpu_selftest_coop_timeout",
+    "planc_gpu_cp_loss_device", "planc_gpu_cp_grads_device", "planc_gpu_cp_step_device",
 ]
 
 
@@ -108,6 +111,15 @@ def load():
     L.planc_gpu_batch_destroy.argtypes = [vp]
     L.planc_gpu_mttkrp_last_mode_noalloc.argtypes = [vp, pi64, i32, P(vp), i32, vp, vp]
     L.planc_gpu_selftest_wait_timeout.argtypes = [i32, d, P(i32)]
+    L.planc_gpu_update_device.argtypes = [vp, i32, vp, vp, vp, i64, i32]
+    L.planc_gpu_gram_device.argtypes = [vp, vp, i64, i32, vp]
+    L.planc_gpu_normalize_device.argtypes = [vp, vp, i64, i32, vp, vp, vp]
+    L.planc_gpu_coldot_device.argtypes = [vp, vp, vp, i64, i32, vp]
+    L.planc_gpu_sync.argtypes = [vp]
+    L.planc_gpu_selftest_coop_timeout.argtypes = [i32, P(i32)]
+    L.planc_gpu_cp_loss_device.argtypes = [vp, P(vp), vp, vp, vp]
+    L.planc_gpu_cp_grads_device.argtypes = [vp, P(vp), vp, P(vp), vp, P(vp)]
+    L.planc_gpu_cp_step_device.argtypes = [vp, P(vp), P(vp), P(vp), d, d, P(vp), P(vp)]
     for name in EXPORTS:
         getattr(L, name).restype = getattr(L, name).restype or i32
     L.planc_gpu_last_error.restype = ctypes.c_char_p
@@ -131,6 +143,10 @@ def _fptrs(F):
     for i, f in enumerate(F):
         arr[i] = _pd(f)
     return arr
+
+
+def _vps(ptrs):
+    return (ctypes.c_void_p * len(ptrs))(*[int(p) for p in ptrs])
 
 
 def _c64(a):
@@ -294,6 +310,47 @@ class Context:
         _check(load().planc_gpu_mttkrp_device(self.h, mode, arr, ctypes.c_void_p(int(out_ptr)),
                                               int(dimtree) | (2 if reuse else 0)))
 
+    # ---- device building blocks of the distributed iteration (device
+    # pointers, row-major rows x k FP64 blocks; ordered on the context's stream)
+    def update_device(self, algo, H_ptr, M_ptr, G_ptr, rows, k):
+        _check(load().planc_gpu_update_device(self.h, ALGO[algo] if isinstance(algo, str) else int(algo),
+                                              ctypes.c_void_p(int(H_ptr)), ctypes.c_void_p(int(M_ptr)),
+                                              ctypes.c_void_p(int(G_ptr)), int(rows), int(k)))
+
+    def gram_device(self, F_ptr, rows, k, G_ptr):
+        _check(load().planc_gpu_gram_device(self.h, ctypes.c_void_p(int(F_ptr)), int(rows), int(k),
+                                            ctypes.c_void_p(int(G_ptr))))
+
+    def normalize_device(self, F_ptr, rows, k, Gin_ptr, lam_ptr, Gout_ptr):
+        _check(load().planc_gpu_normalize_device(self.h, ctypes.c_void_p(int(F_ptr) if F_ptr else None),
+                                                 int(rows), int(k), ctypes.c_void_p(int(Gin_ptr)),
+                                                 ctypes.c_void_p(int(lam_ptr)),
+                                                 ctypes.c_void_p(int(Gout_ptr))))
+
+    def coldot_device(self, A_ptr, B_ptr, rows, k, out_ptr):
+        _check(load().planc_gpu_coldot_device(self.h, ctypes.c_void_p(int(A_ptr) if A_ptr else None),
+                                              ctypes.c_void_p(int(B_ptr) if B_ptr else None),
+                                              int(rows), int(k), ctypes.c_void_p(int(out_ptr))))
+
+    def sync(self):
+        _check(load().planc_gpu_sync(self.h))
+
+    # ---- differentiable CP loss on device factors (pointers)
+    def cp_loss_device(self, F_ptrs, M0_ptr, G_ptr, loss_ptr):
+        _check(load().planc_gpu_cp_loss_device(self.h, _vps(F_ptrs), ctypes.c_void_p(int(M0_ptr)),
+                                               ctypes.c_void_p(int(G_ptr)),
+                                               ctypes.c_void_p(int(loss_ptr))))
+
+    def cp_grads_device(self, F_ptrs, G_ptr, M_ptrs, g_ptr, grad_ptrs):
+        _check(load().planc_gpu_cp_grads_device(self.h, _vps(F_ptrs), ctypes.c_void_p(int(G_ptr)),
+                                                _vps(M_ptrs), ctypes.c_void_p(int(g_ptr)),
+                                                _vps(grad_ptrs)))
+
+    def cp_step_device(self, Y_ptrs, grad_ptrs, Fprev_ptrs, eta, mom, Fnew_ptrs, Ynew_ptrs):
+        _check(load().planc_gpu_cp_step_device(self.h, _vps(Y_ptrs), _vps(grad_ptrs), _vps(Fprev_ptrs),
+                                               float(eta), float(mom), _vps(Fnew_ptrs),
+                                               _vps(Ynew_ptrs)))
+
     def tensor_norm2(self):
         v = ctypes.c_double()
         _check(load().planc_gpu_tensor_norm2(self.h, ctypes.byref(v)))
@@ -386,6 +443,14 @@ def selftest_wait_timeout(device=0, seconds=0.05):
     """Runs the bounded-wait self-test; returns the status the kernel wrote."""
     st = ctypes.c_int32()
     _check(load().planc_gpu_selftest_wait_timeout(device, float(seconds), ctypes.byref(st)))
+    return st.value
+
+
+def selftest_coop_timeout(device=0):
+    """Runs the cooperative NMF sweep's bounded wait with one CTA that never
+    reports; returns the device status (-6, PLANC_GPU_ERR_TIMEOUT, expected)."""
+    st = ctypes.c_int32(0)
+    _check(load().planc_gpu_selftest_coop_timeout(device, ctypes.byref(st)))
     return st.value
 
 

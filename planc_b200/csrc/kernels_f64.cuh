@@ -768,6 +768,55 @@ __global__ void __launch_bounds__(256) k_scale_cols(double* __restrict__ F, int6
   }
 }
 
+// From an un-normalised Gram G_in = U^T U (summed over every row block of the
+// factor, possibly on other devices): lambda_r = sqrt((U^T U)_rr) and the Gram
+// of the normalised factor, G_out_ab = G_in_ab / (lambda_a lambda_b) (entries
+// of a zero column kept), the same arithmetic as k_gram_finalize. One CTA.
+__global__ void __launch_bounds__(1024) k_norm_from_gram(const double* __restrict__ Gin, int k,
+                                                         double* __restrict__ lambda,
+                                                         double* __restrict__ Gout) {
+  __shared__ double lam[kMaxRank];
+  const int tid = threadIdx.x;
+  if (tid < k) {
+    const double nrm = sqrt(Gin[tid * k + tid]);
+    lam[tid] = nrm;
+    lambda[tid] = nrm;
+  }
+  __syncthreads();
+  for (int e = tid; e < k * k; e += 1024) {
+    const double la = lam[e / k], lb = lam[e % k];
+    Gout[e] = (la > 0 && lb > 0) ? Gin[e] / (la * lb) : Gin[e];
+  }
+}
+
+// out_r = sum_i A[i, r] B[i, r] over row-major I x k blocks, in a fixed order
+// (two running sums per lane, then a tree over the lanes). One CTA.
+__global__ void __launch_bounds__(1024) k_coldot(const double* __restrict__ A,
+                                                 const double* __restrict__ B, int64_t I, int k,
+                                                 double* __restrict__ out) {
+  __shared__ double red[1024];
+  const int tid = threadIdx.x;
+  const int r = tid % k, lane = tid / k, lanes = 1024 / k;
+  double v = 0.0;
+  if (lane < lanes) {
+    double s0 = 0.0, s1 = 0.0;
+    int64_t i = lane;
+    for (; i + lanes < I; i += 2 * lanes) {
+      s0 = fma(A[i * k + r], B[i * k + r], s0);
+      s1 = fma(A[(i + lanes) * k + r], B[(i + lanes) * k + r], s1);
+    }
+    if (i < I) s0 = fma(A[i * k + r], B[i * k + r], s0);
+    v = s0 + s1;
+  }
+  red[tid] = v;
+  __syncthreads();
+  if (tid < k) {
+    double s = 0.0;
+    for (int l = 0; l < lanes; ++l) s += red[l * k + tid];
+    out[tid] = s;
+  }
+}
+
 // ---------------------------------------------------------------------------
 // Normalise mode n (NCPFactors::normalize(int), common/ncpfactors.hpp:346-351:
 // lambda_r = ||F(:,r)||, F(:,r) /= lambda_r when > 0), then G_n = F^T F of the
@@ -932,6 +981,148 @@ __global__ void __launch_bounds__(256) k_sumsq_partial(const T* __restrict__ X, 
     __syncthreads();
   }
   if (threadIdx.x == 0) part[blockIdx.x] = red[0];
+}
+
+// ---------------------------------------------------------------------------
+// Differentiable CP loss, 1/2 ||X - [[F_0..F_{N-1}]]||^2, in three fused
+// launches around the MTTKRPs (the gradient form of ntf/ntfnes.hpp:138-147).
+// ---------------------------------------------------------------------------
+constexpr int CPG_BLOCKS = 8;  // row blocks per factor of the Gram kernel
+
+struct CpFactors {
+  const double* F[kMaxModes];
+  int64_t I[kMaxModes];
+  int N, k;
+};
+
+// Grams G_n = F_n^T F_n of every factor: block (b, n) sums its share of the
+// rows of F_n into part[n][b]; the last block of factor n to finish (counter
+// ctr[n], left at 0 again) adds the CPG_BLOCKS partials in order into G_n.
+__global__ void __launch_bounds__(256) k_cp_grams(CpFactors f, double* __restrict__ part,
+                                                  double* __restrict__ G, unsigned* __restrict__ ctr) {
+  __shared__ bool last;
+  const int n = blockIdx.y, b = blockIdx.x, k = f.k, kk2 = k * k;
+  const int64_t I = f.I[n];
+  const int64_t per = (I + CPG_BLOCKS - 1) / CPG_BLOCKS;
+  const int64_t r0 = b * per, r1 = (r0 + per) < I ? (r0 + per) : I;
+  const double* F = f.F[n];
+  double* dst = part + ((int64_t)n * CPG_BLOCKS + b) * kk2;
+  for (int e = threadIdx.x; e < kk2; e += 256) {
+    const int a = e / k, c = e % k;
+    double s0 = 0.0, s1 = 0.0;
+    int64_t i = r0;
+    for (; i + 1 < r1; i += 2) {
+      s0 = fma(F[i * k + a], F[i * k + c], s0);
+      s1 = fma(F[(i + 1) * k + a], F[(i + 1) * k + c], s1);
+    }
+    if (i < r1) s0 = fma(F[i * k + a], F[i * k + c], s0);
+    dst[e] = s0 + s1;
+  }
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) last = atomicAdd(ctr + n, 1u) == CPG_BLOCKS - 1;
+  __syncthreads();
+  if (!last) return;
+  __threadfence();
+  const double* src = part + (int64_t)n * CPG_BLOCKS * kk2;
+  for (int e = threadIdx.x; e < kk2; e += 256) {
+    double t = 0.0;
+    for (int q = 0; q < CPG_BLOCKS; ++q) t += __ldcg(src + (int64_t)q * kk2 + e);
+    G[(int64_t)n * kk2 + e] = t;
+  }
+  if (threadIdx.x == 0) ctr[n] = 0;
+}
+
+// loss = 1/2 ||X||^2 - <M_0, F_0> + 1/2 sum_ab prod_n G_n[a, b]  (one CTA)
+__global__ void __launch_bounds__(1024) k_cp_loss(const double* __restrict__ M0,
+                                                  const double* __restrict__ F0, int64_t I0,
+                                                  const double* __restrict__ G, int N, int k,
+                                                  const double* __restrict__ normX2,
+                                                  double* __restrict__ loss) {
+  __shared__ double red[1024];
+  const int tid = threadIdx.x;
+  double v = 0.0;
+  for (int64_t e = tid; e < I0 * k; e += 1024) v = fma(M0[e], F0[e], v);
+  double mm = 0.0;
+  for (int e = tid; e < k * k; e += 1024) {
+    double g = 1.0;
+    for (int n = 0; n < N; ++n) g *= G[(int64_t)n * k * k + e];
+    mm += g;
+  }
+  red[tid] = 0.5 * mm - v;
+  __syncthreads();
+  for (int st = 512; st > 0; st >>= 1) {
+    if (tid < st) red[tid] += red[tid + st];
+    __syncthreads();
+  }
+  if (tid == 0) *loss = 0.5 * (*normX2) + red[0];
+}
+
+// grad_n = g * (F_n H_n - M_n), H_n = prod_{m != n} G_m (Hadamard), for every
+// mode: block (b, n) forms H_n in shared memory and does its rows.
+struct CpGrad {
+  const double* M[kMaxModes];
+  double* grad[kMaxModes];
+};
+__global__ void __launch_bounds__(256) k_cp_grads(CpFactors f, const double* __restrict__ G,
+                                                  CpGrad d, const double* __restrict__ gscale) {
+  __shared__ double H[kMaxRank * kMaxRank];
+  const int n = blockIdx.y, k = f.k, kk2 = k * k;
+  for (int e = threadIdx.x; e < kk2; e += 256) {
+    double h = 1.0;
+    for (int m = 0; m < f.N; ++m)
+      if (m != n) h *= G[(int64_t)m * kk2 + e];
+    H[e] = h;
+  }
+  __syncthreads();
+  const double g = *gscale;
+  const int64_t I = f.I[n];
+  const double* F = f.F[n];
+  const double* Mn = d.M[n];
+  double* out = d.grad[n];
+  for (int64_t e = (int64_t)blockIdx.x * 256 + threadIdx.x; e < I * k;
+       e += (int64_t)gridDim.x * 256) {
+    const int64_t i = e / k;
+    const int r = (int)(e % k);
+    double s = 0.0;
+    for (int c = 0; c < k; ++c) s = fma(F[i * k + c], H[c * k + r], s);
+    out[e] = g * (s - Mn[e]);
+  }
+}
+
+// One projected accelerated gradient step on every factor:
+//   F_new = max(Y - eta * grad, 0),  Y_new = F_new + mom * (F_new - F_prev)
+struct CpStep {
+  const double* Y[kMaxModes];
+  const double* grad[kMaxModes];
+  const double* Fprev[kMaxModes];
+  double* Fnew[kMaxModes];
+  double* Ynew[kMaxModes];
+  int64_t n[kMaxModes];  // elements of each factor
+  int N;
+};
+__global__ void __launch_bounds__(256) k_cp_step(CpStep s, double eta, double mom) {
+  const int m = blockIdx.y;
+  for (int64_t e = (int64_t)blockIdx.x * 256 + threadIdx.x; e < s.n[m];
+       e += (int64_t)gridDim.x * 256) {
+    double v = s.Y[m][e] - eta * s.grad[m][e];
+    v = v > 0.0 ? v : 0.0;
+    const double fp = s.Fprev[m][e];
+    s.Fnew[m][e] = v;
+    s.Ynew[m][e] = v + mom * (v - fp);
+  }
+}
+
+// acc = (first ? 0 : acc) + the nb partials summed in a fixed order (one
+// warp: lane l adds partials l, l + 32, ..., then a fixed shuffle tree).
+__global__ void k_accum_norm(const double* __restrict__ part, int nb, double* __restrict__ acc,
+                             int first) {
+  const int lane = threadIdx.x & 31;
+  double s = 0.0;
+  for (int b = lane; b < nb; b += 32) s += part[b];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if (lane == 0) *acc = first ? s : *acc + s;
 }
 
 template <typename T>

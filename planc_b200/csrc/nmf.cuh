@@ -273,6 +273,56 @@ inline size_t nmfc_smem_bytes(int KP, int rows) {
   return ((size_t)rows * (KP + 1) + (size_t)KP * KP + NMFC_THREADS) * sizeof(double);
 }
 
+// Warp 0's bounded wait for the nslots per-CTA sums of one column: polls the
+// slots until none holds NMFC_EMPTY, or another CTA raised the error flag, or
+// `limit` polls went by (then it raises the flag and kStTimeout itself).
+// Returns 1 with q = the fixed-order sum (lane l: slots l, l + 32, ...; then a
+// fixed shuffle tree), or 0 when the sweep must stop.
+__device__ __forceinline__ int nmfc_wait_slots(const double* slot, int nslots, unsigned* flag,
+                                               int* status, unsigned limit, double& q) {
+  const int lane = threadIdx.x & 31;
+  int ok = 1;
+  for (unsigned spins = 0;; ++spins) {
+    bool have = true;
+    q = 0.0;
+    for (int b = lane; b < nslots; b += 32) {
+      const double v = __ldcv(slot + b);
+      have = have && (__double_as_longlong(v) != NMFC_EMPTY);
+      q += v;
+    }
+    if (__all_sync(0xffffffffu, have)) break;
+    if (*(volatile unsigned*)flag) {
+      ok = 0;
+      break;
+    }
+    if (spins > limit) {
+      if (lane == 0) {
+        atomicExch(flag, 1u);
+        atomicCAS(status, 0, kStTimeout);
+      }
+      ok = 0;
+      break;
+    }
+    __nanosleep(20);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+  return ok;
+}
+
+// Self-test of that wait: every CTA but `skip` stores its slot, then warp 0
+// of every CTA waits with a limit of `limit` polls. The skipped slot never
+// fills, so the waits run out, the flag and kStTimeout are raised and every
+// CTA returns (no fault, no hang). Launched cooperatively, as the sweep is.
+__global__ void k_nmfc_wait_selftest(double* part, unsigned* flag, int* status, unsigned limit,
+                                     int skip) {
+  if (threadIdx.x == 0 && (int)blockIdx.x != skip) __stcg(part + blockIdx.x, 1.0);
+  if (threadIdx.x < 32) {
+    double q = 0.0;
+    nmfc_wait_slots(part, (int)gridDim.x, flag, status, limit, q);
+  }
+}
+
 template <int KP>
 __global__ void __launch_bounds__(NMFC_THREADS) k_nmf_hals_w_coop(
     double* __restrict__ W, const double* __restrict__ AH, const double* __restrict__ G, int64_t m,
@@ -353,33 +403,8 @@ __global__ void __launch_bounds__(NMFC_THREADS) k_nmf_hals_w_coop(
     // ||Wx||: warp 0 waits for every CTA's slot, adds them (lane l: CTAs l,
     // l + 32, ...; then a fixed shuffle tree), the same sum in every CTA
     if (tid < 32) {
-      int ok = 1;
       double q = 0.0;
-      for (unsigned spins = 0;; ++spins) {
-        bool have = true;
-        q = 0.0;
-        for (int b = tid; b < (int)gridDim.x; b += 32) {
-          const double v = __ldcv(slot + b);
-          have = have && (__double_as_longlong(v) != NMFC_EMPTY);
-          q += v;
-        }
-        if (__all_sync(0xffffffffu, have)) break;
-        if (*(volatile unsigned*)flag) {
-          ok = 0;
-          break;
-        }
-        if (spins > NMFC_SPINS) {
-          if (tid == 0) {
-            atomicExch(flag, 1u);
-            atomicCAS(status, 0, kStTimeout);
-          }
-          ok = 0;
-          break;
-        }
-        __nanosleep(20);
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+      const int ok = nmfc_wait_slots(slot, (int)gridDim.x, flag, status, NMFC_SPINS, q);
       if (tid == 0) {
         s_ok = ok;
         s_norm = sqrt(q);

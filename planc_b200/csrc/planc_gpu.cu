@@ -71,6 +71,12 @@ constexpr int64_t kBal4MaxK = int64_t(1) << 17;
 
 }  // namespace
 
+// Host tensors are uploaded through a staging buffer of this size, in chunks
+// of the natural element order; the sum of squares takes this many per-chunk
+// partials.
+constexpr int64_t kStageBytes = 64ll << 20;
+constexpr int kNormBlocks = 1184;
+
 struct planc_gpu_ctx {
   int device = 0;
   int precision = PLANC_GPU_PREC_FP64;
@@ -94,6 +100,11 @@ struct planc_gpu_ctx {
   bool have_tensor = false, have_factors = false;
 
   double* X64 = nullptr;         // FP64 tensor (plain path)
+  int64_t x64_elems = 0;
+  void* stage = nullptr;         // host-upload staging buffer (kStageBytes), made on first use
+  double* cp_part = nullptr;     // CP-loss Gram partials (N x CPG_BLOCKS x k x k)
+  unsigned* cp_ctr = nullptr;    // their per-factor completion counters
+  double* norm_part = nullptr;   // per-block partial sums of squares of one chunk
   TcTensor tct;                  // tensor-core operand copy (BF16 paths)
   // copies with mode n moved last for the direct (non-tree) MTTKRP on the
   // tensor cores, made on first use; the last mode uses tct when its view
@@ -1224,6 +1235,13 @@ void free_all(planc_gpu_ctx* c) {
     p = nullptr;
   };
   f(c->X64);
+  c->x64_elems = 0;
+  if (c->stage) cudaFree(c->stage);
+  c->stage = nullptr;
+  f(c->cp_part);
+  if (c->cp_ctr) cudaFree(c->cp_ctr);
+  c->cp_ctr = nullptr;
+  f(c->norm_part);
   tc_free(c->tct);
   for (int n = 0; n < kMaxModes; ++n) tc_free(c->tcd[n]);
   f(c->normX2);
@@ -1392,63 +1410,78 @@ int planc_gpu_set_tensor(planc_gpu_ctx* c, const void* X, int dtype, const int64
     c->L = 1;
     c->R = 1;
     for (int i = 0; i < nmodes; ++i) (i <= c->s ? c->L : c->R) *= dims[i];
-    size_t esz = dtype == PLANC_GPU_F64 ? 8 : 4;
-    const void* src = X;
-    void* staged = nullptr;
-    if (!x_on_device) {
-      CK(cudaMalloc(&staged, numel * esz));
-      cudaError_t e = cudaMemcpyAsync(staged, X, numel * esz, cudaMemcpyHostToDevice, c->stream);
-      if (e != cudaSuccess) {
-        cudaFree(staged);
-        cuda_check(e, "upload tensor");
-      }
-      src = staged;
-    }
-    try {
-      // ||X||^2 in FP64 from the values given
-      const int nb = 1184;
-      double* part = nullptr;
-      CK(cudaMalloc(&part, nb * sizeof(double)));
-      if (dtype == PLANC_GPU_F64)
-        k_sumsq_partial<double><<<nb, 256, 0, c->stream>>>((const double*)src, numel, part);
-      else
-        k_sumsq_partial<float><<<nb, 256, 0, c->stream>>>((const float*)src, numel, part);
-      k_reduce_splits<<<1, 32, 0, c->stream>>>(part, nb, 1, 1, c->normX2);
-      CK(cudaGetLastError());
-      double nx = 0.0;
-      CK(cudaMemcpyAsync(&nx, c->normX2, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
-      CK(cudaStreamSynchronize(c->stream));
-      if (!std::isfinite(nx)) {
-        cudaFree(part);
-        fail(PLANC_GPU_ERR_NONFINITE, "the tensor holds NaN or Inf values");
-      }
-      if (c->precision == PLANC_GPU_PREC_FP64) {
+    c->have_tensor = false;  // until the new tensor is in place
+    const size_t esz = dtype == PLANC_GPU_F64 ? 8 : 4;
+    // The tensor goes through in chunks of the natural order: from host memory
+    // through one fixed staging buffer (no allocation per call), from device
+    // memory in place. Each chunk adds its FP64 sum of squares (in a fixed
+    // order, the same for both sources) and is converted into the resident
+    // copy: FP64, or the tensor-core view (BF16 or a BF16 pair).
+    const int64_t chunk = kStageBytes / (int64_t)esz;
+    const bool f64 = c->precision == PLANC_GPU_PREC_FP64;
+    if (!x_on_device && !c->stage) CK(cudaMalloc(&c->stage, kStageBytes));
+    if (!c->norm_part) CK(cudaMalloc(&c->norm_part, kNormBlocks * sizeof(double)));
+    if (f64) {
+      if (!c->X64 || c->x64_elems != numel) {
         dalloc(&c->X64, (size_t)numel);
-        if (dtype == PLANC_GPU_F64)
-          CK(cudaMemcpyAsync(c->X64, src, numel * 8, cudaMemcpyDeviceToDevice, c->stream));
-        else
-          k_copy_to_f64<float><<<4096, 256, 0, c->stream>>>((const float*)src, numel, c->X64);
-      } else {
-        if (c->X64) {
-          cudaFree(c->X64);
-          c->X64 = nullptr;
+        c->x64_elems = numel;
+      }
+      tc_free(c->tct);
+    } else {
+      if (c->X64) {
+        cudaFree(c->X64);
+        c->X64 = nullptr;
+        c->x64_elems = 0;
+      }
+      CK(tc_prepare(c->tct, c->L, c->R, c->dims[0], c->precision));
+    }
+    for (int64_t e0 = 0; e0 < numel; e0 += chunk) {
+      const int64_t n = std::min<int64_t>(chunk, numel - e0);
+      const char* src = (const char*)X + (size_t)e0 * esz;
+      if (!x_on_device) {
+        if (f64 && dtype == PLANC_GPU_F64) {  // straight into the resident copy
+          CK(cudaMemcpyAsync(c->X64 + e0, src, n * esz, cudaMemcpyHostToDevice, c->stream));
+          src = (const char*)(c->X64 + e0);
+        } else {
+          CK(cudaMemcpyAsync(c->stage, src, n * esz, cudaMemcpyHostToDevice, c->stream));
+          src = (const char*)c->stage;
         }
-        cudaError_t te =
-            tc_set_tensor(c->tct, src, dtype == PLANC_GPU_F64, c->L, c->R, c->dims[0], c->precision,
-                          c->stream);
-        if (te == cudaErrorInvalidValue)
-          fail(PLANC_GPU_ERR_CUDA, "cuTensorMapEncodeTiled rejected the tensor map");
-        CK(te);
-        c->tct.left_nf = c->s + 1;
+      }
+      const unsigned nb = (unsigned)std::min<int64_t>(kNormBlocks, (n + 255) / 256);
+      if (dtype == PLANC_GPU_F64)
+        k_sumsq_partial<double><<<nb, 256, 0, c->stream>>>((const double*)src, n, c->norm_part);
+      else
+        k_sumsq_partial<float><<<nb, 256, 0, c->stream>>>((const float*)src, n, c->norm_part);
+      k_accum_norm<<<1, 32, 0, c->stream>>>(c->norm_part, (int)nb, c->normX2, e0 == 0);
+      const unsigned cb = (unsigned)std::min<int64_t>(4096, (n + 255) / 256);
+      if (f64) {
+        if (dtype == PLANC_GPU_F64) {
+          if ((const double*)src != c->X64 + e0)
+            CK(cudaMemcpyAsync(c->X64 + e0, src, n * 8, cudaMemcpyDeviceToDevice, c->stream));
+        } else {
+          k_copy_to_f64<float><<<cb, 256, 0, c->stream>>>((const float*)src, n, c->X64 + e0);
+        }
+      } else if (dtype == PLANC_GPU_F64) {
+        k_tc_convert_range<double><<<cb, 256, 0, c->stream>>>((const double*)src, e0, n, c->L,
+                                                              c->tct.Lpad, c->tct.hi, c->tct.lo);
+      } else {
+        k_tc_convert_range<float><<<cb, 256, 0, c->stream>>>((const float*)src, e0, n, c->L,
+                                                             c->tct.Lpad, c->tct.hi, c->tct.lo);
       }
       CK(cudaGetLastError());
-      CK(cudaStreamSynchronize(c->stream));
-      cudaFree(part);
-    } catch (...) {
-      if (staged) cudaFree(staged);
-      throw;
     }
-    if (staged) cudaFree(staged);
+    if (!f64) {
+      if (!tc_make_maps(c->tct))
+        fail(PLANC_GPU_ERR_CUDA, "cuTensorMapEncodeTiled rejected the tensor map");
+      c->tct.left_nf = c->s + 1;
+    }
+    double nx = 0.0;
+    CK(cudaMemcpyAsync(&nx, c->normX2, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    if (!std::isfinite(nx)) {
+      c->have_tensor = false;
+      fail(PLANC_GPU_ERR_NONFINITE, "the tensor holds NaN or Inf values");
+    }
     c->have_tensor = true;
   });
 }
@@ -1745,6 +1778,199 @@ int planc_gpu_bpp_solve(planc_gpu_ctx* c, const double* AtA, const double* AtB, 
   });
 }
 
+// ---- device building blocks of the distributed iteration
+int planc_gpu_update_device(planc_gpu_ctx* c, int algo, double* H, const double* M,
+                            const double* G, int64_t rows, int k) {
+  return guarded([&] {
+    if (!c || !H || !M || !G) fail(PLANC_GPU_ERR_ARG, "null argument");
+    if (rows < 0 || k < 1 || k > kMaxRank) fail(PLANC_GPU_ERR_ARG, "bad shape");
+    if (algo != PLANC_GPU_HALS && algo != PLANC_GPU_MU && algo != PLANC_GPU_ANLSBPP)
+      fail(PLANC_GPU_ERR_UNSUPPORTED, "row-block updates are MU, HALS and ANLS/BPP");
+    if (rows == 0) return;
+    set_device(c);
+    const unsigned blocks = (unsigned)((rows + 7) / 8);
+    if (algo == PLANC_GPU_HALS || algo == PLANC_GPU_MU) {
+      launch(c, KC_UPDATE, [&] {
+        if (k <= 32) {
+          if (algo == PLANC_GPU_HALS)
+            k_hals_warp<32><<<blocks, 256, 0, c->stream>>>(H, M, G, rows, k);
+          else
+            k_mu_warp<32><<<blocks, 256, 0, c->stream>>>(H, M, G, rows, k, kEps6);
+        } else {
+          if (algo == PLANC_GPU_HALS)
+            k_hals_warp<64><<<blocks, 256, 0, c->stream>>>(H, M, G, rows, k);
+          else
+            k_mu_warp<64><<<blocks, 256, 0, c->stream>>>(H, M, G, rows, k, kEps6);
+        }
+      });
+      return;
+    }
+    const unsigned bb = (unsigned)((rows + BPP_WARPS - 1) / BPP_WARPS);
+    launch(c, KC_BPP, [&] {
+      switch (kpad(k)) {
+#define CASE(KP)                                                                          \
+  case KP:                                                                                \
+    k_bpp<KP><<<bb, 32 * BPP_WARPS, bpp_smem_bytes(KP), c->stream>>>(                  \
+        G, M, k, rows, H, nullptr, nullptr, c->status_dev, c->bpp_max_iter,               \
+        c->bpp_warm ? H : nullptr);                                                       \
+    break;
+        CASE(8) CASE(16) CASE(32) CASE(64)
+#undef CASE
+      }
+    });
+  });
+}
+
+int planc_gpu_gram_device(planc_gpu_ctx* c, const double* F, int64_t rows, int k, double* G) {
+  return guarded([&] {
+    if (!c || !F || !G) fail(PLANC_GPU_ERR_ARG, "null argument");
+    if (rows < 0 || k < 1 || k > kMaxRank) fail(PLANC_GPU_ERR_ARG, "bad shape");
+    set_device(c);
+    if (rows == 0) {
+      CK(cudaMemsetAsync(G, 0, (size_t)k * k * 8, c->stream));
+      return;
+    }
+    const int rpb = gram_rows_per_block(rows);
+    const int nblk = (int)((rows + rpb - 1) / rpb);
+    if ((size_t)nblk * k * k > c->gram_part_elems) {
+      if (c->capturing) fail(PLANC_GPU_ERR_STATE, "Gram partials would grow during capture");
+      dalloc(&c->gram_part, (size_t)nblk * k * k);
+      c->gram_part_elems = (size_t)nblk * k * k;
+      c->buf_epoch++;
+    }
+    launch(c, KC_NORMGRAM, [&] {
+      k_gram_partial<<<nblk, 256, 0, c->stream>>>(F, rows, k, rpb, c->gram_part);
+    });
+    launch(c, KC_REDUCE, [&] {
+      reduce_splits(c->stream, c->gram_part, nblk, (int64_t)k * k, (int64_t)k * k, G);
+    });
+  });
+}
+
+int planc_gpu_normalize_device(planc_gpu_ctx* c, double* F, int64_t rows, int k,
+                               const double* G_in, double* lambda, double* G_out) {
+  return guarded([&] {
+    if (!c || !G_in || !lambda || !G_out || (rows > 0 && !F)) fail(PLANC_GPU_ERR_ARG, "null argument");
+    if (rows < 0 || k < 1 || k > kMaxRank) fail(PLANC_GPU_ERR_ARG, "bad shape");
+    set_device(c);
+    launch(c, KC_NORMGRAM, [&] { k_norm_from_gram<<<1, 1024, 0, c->stream>>>(G_in, k, lambda, G_out); });
+    if (rows > 0) {
+      const unsigned nb = (unsigned)std::min<int64_t>((rows * k + 255) / 256, 4096);
+      launch(c, KC_NORMGRAM, [&] { k_scale_cols<<<nb, 256, 0, c->stream>>>(F, rows, k, lambda); });
+    }
+  });
+}
+
+int planc_gpu_coldot_device(planc_gpu_ctx* c, const double* A, const double* B, int64_t rows, int k,
+                            double* out) {
+  return guarded([&] {
+    if (!c || !out || (rows > 0 && (!A || !B))) fail(PLANC_GPU_ERR_ARG, "null argument");
+    if (rows < 0 || k < 1 || k > kMaxRank) fail(PLANC_GPU_ERR_ARG, "bad shape");
+    set_device(c);
+    launch(c, KC_ERROR, [&] { k_coldot<<<1, 1024, 0, c->stream>>>(A, B, rows, k, out); });
+  });
+}
+
+int planc_gpu_sync(planc_gpu_ctx* c) {
+  return guarded([&] {
+    if (!c) fail(PLANC_GPU_ERR_ARG, "null context");
+    set_device(c);
+    CK(cudaStreamSynchronize(c->stream));
+    check_status(c);
+    drain_timing(c);
+  });
+}
+
+// ---- the differentiable CP loss
+namespace {
+CpFactors cp_factors(planc_gpu_ctx* c, const double* const* F) {
+  CpFactors f;
+  memset(&f, 0, sizeof(f));
+  f.N = c->N;
+  f.k = c->k;
+  for (int n = 0; n < c->N; ++n) {
+    if (!F[n]) fail(PLANC_GPU_ERR_ARG, "null factor");
+    f.F[n] = F[n];
+    f.I[n] = c->dims[n];
+  }
+  return f;
+}
+}  // namespace
+
+int planc_gpu_cp_loss_device(planc_gpu_ctx* c, const double* const* F_dev, const double* M0_dev,
+                             double* G_out, double* loss_out) {
+  return guarded([&] {
+    require_ready(c);
+    if (!F_dev || !M0_dev || !G_out || !loss_out) fail(PLANC_GPU_ERR_ARG, "null argument");
+    set_device(c);
+    CpFactors f = cp_factors(c, F_dev);
+    const int k = c->k;
+    if (!c->cp_part) {
+      if (c->capturing) fail(PLANC_GPU_ERR_STATE, "CP-loss buffers would be made during capture");
+      CK(cudaMalloc(&c->cp_part, (size_t)kMaxModes * CPG_BLOCKS * kMaxRank * kMaxRank * 8));
+      CK(cudaMalloc(&c->cp_ctr, kMaxModes * sizeof(unsigned)));
+      CK(cudaMemsetAsync(c->cp_ctr, 0, kMaxModes * sizeof(unsigned), c->stream));
+    }
+    launch(c, KC_NORMGRAM, [&] {
+      k_cp_grams<<<dim3(CPG_BLOCKS, c->N), 256, 0, c->stream>>>(f, c->cp_part, G_out, c->cp_ctr);
+    });
+    launch(c, KC_ERROR, [&] {
+      k_cp_loss<<<1, 1024, 0, c->stream>>>(M0_dev, F_dev[0], c->dims[0], G_out, c->N, k, c->normX2,
+                                            loss_out);
+    });
+  });
+}
+
+int planc_gpu_cp_grads_device(planc_gpu_ctx* c, const double* const* F_dev, const double* G,
+                              const double* const* M_dev, const double* g_dev,
+                              double* const* grad_dev) {
+  return guarded([&] {
+    require_ready(c);
+    if (!F_dev || !G || !M_dev || !g_dev || !grad_dev) fail(PLANC_GPU_ERR_ARG, "null argument");
+    set_device(c);
+    CpFactors f = cp_factors(c, F_dev);
+    CpGrad d;
+    memset(&d, 0, sizeof(d));
+    int64_t maxI = 1;
+    for (int n = 0; n < c->N; ++n) {
+      if (!M_dev[n] || !grad_dev[n]) fail(PLANC_GPU_ERR_ARG, "null MTTKRP or gradient");
+      d.M[n] = M_dev[n];
+      d.grad[n] = grad_dev[n];
+      maxI = std::max(maxI, c->dims[n]);
+    }
+    const unsigned gx = (unsigned)std::min<int64_t>((maxI * c->k + 255) / 256, 1024);
+    launch(c, KC_UPDATE, [&] {
+      k_cp_grads<<<dim3(gx, c->N), 256, 0, c->stream>>>(f, G, d, g_dev);
+    });
+  });
+}
+
+int planc_gpu_cp_step_device(planc_gpu_ctx* c, const double* const* Y, const double* const* grad,
+                             const double* const* Fprev, double eta, double mom, double* const* Fnew,
+                             double* const* Ynew) {
+  return guarded([&] {
+    require_ready(c);
+    if (!Y || !grad || !Fprev || !Fnew || !Ynew) fail(PLANC_GPU_ERR_ARG, "null argument");
+    set_device(c);
+    CpStep s;
+    memset(&s, 0, sizeof(s));
+    s.N = c->N;
+    int64_t maxn = 1;
+    for (int n = 0; n < c->N; ++n) {
+      if (!Y[n] || !grad[n] || !Fprev[n] || !Fnew[n] || !Ynew[n]) fail(PLANC_GPU_ERR_ARG, "null factor");
+      s.Y[n] = Y[n];
+      s.grad[n] = grad[n];
+      s.Fprev[n] = Fprev[n];
+      s.Fnew[n] = Fnew[n];
+      s.Ynew[n] = Ynew[n];
+      s.n[n] = c->dims[n] * c->k;
+      maxn = std::max(maxn, s.n[n]);
+    }
+    const unsigned gx = (unsigned)std::min<int64_t>((maxn + 255) / 256, 1024);
+    launch(c, KC_UPDATE, [&] { k_cp_step<<<dim3(gx, c->N), 256, 0, c->stream>>>(s, eta, mom); });
+  });
+}
+
 int planc_gpu_mttkrp_device(planc_gpu_ctx* c, int mode, const double* const* F_dev, double* M_dev,
                             int flags) {
   return guarded([&] {
@@ -1832,6 +2058,43 @@ int planc_gpu_selftest_wait_timeout(int device, double seconds, int* status_out)
     cudaFree(st);
     cuda_check(e, "wait self-test");
     *status_out = h;
+  });
+}
+
+int planc_gpu_selftest_coop_timeout(int device, int* status_out) {
+  return guarded([&] {
+    if (!status_out) fail(PLANC_GPU_ERR_ARG, "null argument");
+    CK(cudaSetDevice(device));
+    const int nct = 4;
+    double* part = nullptr;
+    unsigned* flag = nullptr;
+    int* st = nullptr;
+    auto cleanup = [&] {
+      cudaFree(part);
+      cudaFree(flag);
+      cudaFree(st);
+    };
+    try {
+      CK(cudaMalloc(&part, nct * sizeof(double)));
+      CK(cudaMalloc(&flag, sizeof(unsigned)));
+      CK(cudaMalloc(&st, sizeof(int)));
+      CK(cudaMemset(part, 0xff, nct * sizeof(double)));  // NMFC_EMPTY in every slot
+      CK(cudaMemset(flag, 0, sizeof(unsigned)));
+      CK(cudaMemset(st, 0, sizeof(int)));
+      unsigned limit = 1u << 12;
+      int skip = 1;
+      void* args[] = {&part, &flag, &st, &limit, &skip};
+      CK(cudaLaunchCooperativeKernel((const void*)k_nmfc_wait_selftest, dim3(nct), dim3(64), args,
+                                     0, nullptr));
+      CK(cudaDeviceSynchronize());
+      int h = 0;
+      CK(cudaMemcpy(&h, st, sizeof(int), cudaMemcpyDeviceToHost));
+      *status_out = h;
+    } catch (...) {
+      cleanup();
+      throw;
+    }
+    cleanup();
   });
 }
 

@@ -1201,28 +1201,6 @@ __device__ __forceinline__ __nv_bfloat16 bf16_stochastic(float x, uint32_t r) {
   return __ushort_as_bfloat16((unsigned short)(v >> 16));
 }
 
-// X (f32/f64, L x R column-major) -> BF16 hi (and lo) with leading dim Lpad.
-// Split-BF16 (lo != null): hi = RN(x), lo = RN(x - hi), residual ~2^-17 |x|.
-// Single BF16: stochastic rounding of RN_f32(x), seeded by the element index
-// (deterministic).
-template <typename T>
-__global__ void k_tc_convert(const T* __restrict__ X, int64_t L, int64_t R, int64_t Lpad,
-                             __nv_bfloat16* __restrict__ hi, __nv_bfloat16* __restrict__ lo) {
-  const int64_t total = Lpad * R;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t l = e % Lpad, j = e / Lpad;
-    double x = l < L ? (double)X[l + L * j] : 0.0;
-    if (lo) {
-      __nv_bfloat16 h = __double2bfloat16(x);
-      hi[e] = h;
-      lo[e] = __double2bfloat16(x - (double)__bfloat162float(h));
-    } else {
-      hi[e] = bf16_stochastic((float)x, sr_hash((uint64_t)e));
-    }
-  }
-}
-
 // Copy of the tensor-core operand with mode n moved last, for the direct
 // (non-tree) MTTKRP of mode n as one left contraction. Element (i_0..i_{N-1})
 // sits at l + Lpad * j in the source view (l over modes <= s, j over the
@@ -1271,6 +1249,41 @@ __global__ void k_tc_permute(const __nv_bfloat16* __restrict__ hi, const __nv_bf
     }
     ohi[e] = vh;
     if (olo) olo[e] = vl;
+  }
+}
+
+// The tensor-core copy of the tensor, converted over a range of its elements
+// in their natural order (mode 0 fastest): bf16x2 (lo != nullptr) stores the
+// BF16 pair hi = RN(x), lo = RN(x - hi); single BF16 rounds RN_f32(x)
+// stochastically, seeded by the destination index (deterministic, unbiased:
+// round-to-nearest of a nonnegative tensor is biased low). Source element
+// e0 + i is src[i]; it lands at l + Lpad * j (l = index % L, j = index / L),
+// and the element that ends a column (l = L - 1) also zeroes that column's
+// padding rows. The result does not depend on how the tensor is cut into
+// ranges.
+template <typename T>
+__global__ void k_tc_convert_range(const T* __restrict__ src, int64_t e0, int64_t n, int64_t L,
+                                   int64_t Lpad, __nv_bfloat16* __restrict__ hi,
+                                   __nv_bfloat16* __restrict__ lo) {
+  const __nv_bfloat16 zero = __ushort_as_bfloat16((unsigned short)0);
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t g = e0 + i;
+    const int64_t l = g % L, j = g / L;
+    const int64_t e = l + Lpad * j;
+    const double x = (double)src[i];
+    if (lo) {
+      __nv_bfloat16 h = __double2bfloat16(x);
+      hi[e] = h;
+      lo[e] = __double2bfloat16(x - (double)__bfloat162float(h));
+    } else {
+      hi[e] = bf16_stochastic((float)x, sr_hash((uint64_t)e));
+    }
+    if (l == L - 1)
+      for (int64_t pl = L; pl < Lpad; ++pl) {
+        hi[pl + Lpad * j] = zero;
+        if (lo) lo[pl + Lpad * j] = zero;
+      }
   }
 }
 
@@ -1362,40 +1375,42 @@ inline bool tc_left_factored(const TcTensor& t) {
   return t.I0 > 0 && t.I0 % TC_BK == 0 && t.left_nf >= 2 && t.left_nf <= 3;
 }
 
-// Returns cudaSuccess or an error; false map creation is reported as
-// cudaErrorInvalidValue.
-inline cudaError_t tc_set_tensor(TcTensor& t, const void* src, bool src_f64, int64_t L, int64_t R,
-                                 int64_t I0, int prec, cudaStream_t st) {
+// Storage of the BF16 view (L rows, R columns, row stride L rounded up to 8)
+// for conversion in ranges (k_tc_convert_range); buffers of the same view and
+// precision are kept (with their images).
+inline cudaError_t tc_prepare(TcTensor& t, int64_t L, int64_t R, int64_t I0, int prec) {
+  const int64_t Lpad = (L + 7) / 8 * 8;
+  if (t.hi && t.L == L && t.R == R && t.prec == prec) {
+    t.I0 = I0;
+    return cudaSuccess;
+  }
   tc_free(t);
   t.I0 = I0;
   t.L = L;
   t.R = R;
-  t.Lpad = (L + 7) / 8 * 8;
+  t.Lpad = Lpad;
   t.prec = prec;
-  size_t n = (size_t)t.Lpad * R;
+  const size_t n = (size_t)Lpad * R;
   cudaError_t e = cudaMalloc(&t.hi, n * 2);
-  if (e != cudaSuccess) return e;
-  if (prec == 2) {
-    e = cudaMalloc(&t.lo, n * 2);
-    if (e != cudaSuccess) return e;
-  }
-  if (src_f64)
-    k_tc_convert<double><<<4096, 256, 0, st>>>((const double*)src, L, R, t.Lpad, t.hi, t.lo);
-  else
-    k_tc_convert<float><<<4096, 256, 0, st>>>((const float*)src, L, R, t.Lpad, t.hi, t.lo);
-  e = cudaGetLastError();
-  if (e != cudaSuccess) return e;
-  bool ok = tc_make_map(&t.mR_hi, t.hi, L, R, t.Lpad, 64, 64) &&
-            tc_make_map(&t.mL_hi, t.hi, L, R, t.Lpad, 64, 128);
+  if (e == cudaSuccess && prec == 2) e = cudaMalloc(&t.lo, n * 2);
+  return e;
+}
+
+// Tensor maps of a prepared view (host-side encodes). False when the driver
+// rejects a map.
+inline bool tc_make_maps(TcTensor& t) {
+  bool ok = tc_make_map(&t.mR_hi, t.hi, t.L, t.R, t.Lpad, 64, 64) &&
+            tc_make_map(&t.mL_hi, t.hi, t.L, t.R, t.Lpad, 64, 128);
   if (ok && t.lo)
-    ok = tc_make_map(&t.mR_lo, t.lo, L, R, t.Lpad, 64, 64) &&
-         tc_make_map(&t.mL_lo, t.lo, L, R, t.Lpad, 64, 128);
+    ok = tc_make_map(&t.mR_lo, t.lo, t.L, t.R, t.Lpad, 64, 64) &&
+         tc_make_map(&t.mL_lo, t.lo, t.L, t.R, t.Lpad, 64, 128);
   else if (ok) {
     t.mR_lo = t.mR_hi;
     t.mL_lo = t.mL_hi;
   }
-  return ok ? cudaSuccess : cudaErrorInvalidValue;
+  return ok;
 }
+
 
 // Direct-MTTKRP copy of mode n (k_tc_permute) from the tree's copy `src`
 // whose view splits at s. dst's view: L' = numel / I_n rows, R' = I_n, with

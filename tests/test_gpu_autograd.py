@@ -147,3 +147,26 @@ def test_cp_loss_backward_after_second_forward(gpu, dims):
         for g, r in zip(got, R):
             assert rel(g.grad.cpu().numpy(), r.grad.cpu().numpy()) < 1e-10
     lossf.close()
+
+
+def test_projected_accelerated_step_kernel(gpu):
+    # the fused step against the same arithmetic in torch, with outputs in
+    # place of inputs of the same factor
+    import torch
+    from planc_b200.autograd import projected_accelerated_step
+    X, F, lossf, Ft = _setup("fp64", dims=(30, 20, 10), k=4, seed=41)
+    rng = np.random.default_rng(42)
+    Y = [torch.tensor(rng.random(f.shape), device="cuda", dtype=torch.float64) for f in F]
+    Gr = [torch.tensor(rng.standard_normal(f.shape), device="cuda", dtype=torch.float64) for f in F]
+    P = [torch.tensor(rng.random(f.shape), device="cuda", dtype=torch.float64) for f in F]
+    eta, mom = 0.37, 0.61
+    refF = [(y - eta * g).clamp(min=0.0) for y, g in zip(Y, Gr)]
+    refY = [nf + mom * (nf - p) for nf, p in zip(refF, P)]
+    Fn = [torch.empty_like(y) for y in Y]
+    projected_accelerated_step(lossf, Y, Gr, P, eta, mom, Fn, Y)  # Ynew written over Y
+    torch.cuda.synchronize()
+    for a, b in zip(Fn, refF):
+        assert torch.equal(a, b)
+    for a, b in zip(Y, refY):
+        assert torch.allclose(a, b, rtol=0, atol=1e-15)
+    lossf.close()

@@ -19,6 +19,20 @@ def test_bounded_wait_times_out_and_reports(gpu):
         c.run("hals", 1)
 
 
+def test_cooperative_sweep_wait_times_out_and_reports(gpu):
+    # the cooperative NMF W sweep's per-column wait (the routine the sweep
+    # runs) with one CTA that never stores its sum: the waits run out and
+    # report the timeout; no fault, no hang, the device stays usable
+    assert gpu.selftest_coop_timeout(0) == -6
+    with gpu.Context(0, "fp64") as c:
+        rng = np.random.default_rng(9)
+        A = np.asfortranarray(rng.random((300, 40)))
+        c.set_tensor(A)
+        c.nmf_set_factors(rng.random((300, 4)), rng.random((40, 4)))
+        obj, rel = c.nmf_run("hals", 2)
+        assert np.all(np.isfinite(rel))
+
+
 def test_bpp_iteration_cap_reports_failure_and_recovers(gpu):
     X, _ = cp_tensor((20, 18, 16), 6, seed=3)
     F0 = init_factors(X.shape, 6, seed=4)

@@ -233,3 +233,31 @@ def test_ntf_run_matches_reference_golden(gpu, name, algo):
         assert abs(e[-1] - ref_err[-1]) <= TOL * ref_err[-1]
     else:
         assert np.max(np.abs(e - ref_err) / ref_err) < TOL
+
+
+@pytest.mark.parametrize("prec,dtype", [("fp64", np.float64), ("fp64", np.float32),
+                                        ("bf16", np.float32), ("bf16x2", np.float64)])
+def test_set_tensor_host_and_device_sources_agree(gpu, prec, dtype):
+    # a tensor of several upload chunks (64 MiB each), with a ragged last one:
+    # host memory (through the staging buffer) and device memory (in place)
+    # give the same resident copy bit for bit, and re-uploading a tensor of the
+    # same shape into the same context reuses its buffers
+    import torch
+    dims, k = (301, 283, 203), 4
+    rng = np.random.default_rng(91)
+    X = np.asfortranarray(rng.random(dims).astype(dtype))
+    F = init_factors(dims, k, seed=92)
+    xd = torch.tensor(X.ravel(order="F"), device="cuda")
+    with gpu.Context(0, prec) as a, gpu.Context(0, prec) as b:
+        a.set_tensor(X)
+        b.set_tensor(xd.data_ptr(), dims=dims, dtype="f64" if dtype == np.float64 else "f32")
+        a.set_factors(F)
+        b.set_factors(F)
+        assert a.tensor_norm2() == b.tensor_norm2()
+        assert abs(a.tensor_norm2() - float(np.sum(X.astype(np.float64) ** 2))) < 1e-12 * a.tensor_norm2()
+        for n in range(3):
+            assert np.array_equal(a.mttkrp(n), b.mttkrp(n))
+        m0 = a.mttkrp(0)
+        a.set_tensor(X)
+        a.set_factors(F)
+        assert np.array_equal(a.mttkrp(0), m0)
