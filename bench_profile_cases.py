@@ -7,6 +7,7 @@ prints one line of timings. The cases are sized so that a profiler capture of
 one launch holds a few GB of device memory at most while the tensors stay
 larger than the 126 MB L2 (DRAM counters stay meaningful):
 
+  f64     k_contract_f64 (FP64 path, DMMA): 512^3 tensor (FP64 copy), rank 32, HALS
   bpp     k_bpp: ANLS/BPP normal equations of a 192-row mode at rank 64 taken
           from a 192 x 96 x 96 x 96 sparse-factor CP tensor after 10
           iterations (passive sets of ~45, ~3 BPP steps per row)
@@ -80,6 +81,19 @@ def case_bpp(gpu, torch):
             c.set_timing(False)
     print("bpp: 192 rows, k=64: kernel %.1f us, BPP steps mean %.2f max %d, passive mean %.1f"
           % (ms * 1e3, its.mean(), its.max(), P.sum(axis=0).mean()))
+    print("bpp: rows per BPP step count:", dict(enumerate(np.bincount(its).tolist())))
+
+
+def case_f64(gpu, torch):
+    # the FP64 path's DMMA contractions (right: P = X F_2, left: X^T KRP(F_0, F_1)):
+    # 512^3 FP64 (1.07 GB), rank 32, HALS iterations
+    dims, k = (512, 512, 512), 32
+    X, F0 = _synth(gpu, torch, dims, k, 61)
+    with gpu.Context(0, "fp64") as c:
+        c.set_tensor(X.data_ptr(), dims=dims, dtype="f32")
+        c.set_factors(F0)
+        ms = _timed(torch, c, lambda: c.run("hals", 1, compute_error=False), 3)
+    print("f64: 512^3 k=32 HALS FP64: %.3f ms per iteration" % ms)
 
 
 def case_tc3(gpu, torch):
@@ -172,7 +186,7 @@ def case_nes(gpu, torch):
     print("nes: 512^3 k=32 Nesterov: %.3f ms per iteration (8 in one call)" % ms)
 
 
-CASES = {"bpp": case_bpp, "nes": case_nes, "tc3": case_tc3, "tc4": case_tc4, "cfg3it": case_cfg3it,
+CASES = {"bpp": case_bpp, "f64": case_f64, "nes": case_nes, "tc3": case_tc3, "tc4": case_tc4, "cfg3it": case_cfg3it,
          "ttv": case_ttv, "nmf": case_nmf, "upd": case_upd}
 
 

@@ -336,9 +336,13 @@ __global__ void __launch_bounds__(32 * BPP_WARPS, 1) k_bpp(const double* __restr
   unsigned iter = 0;
   int st = 0;
   if (Pinit) {
-    // warm start from the previous solution's passive set: BPP reaches the
-    // unique NNLS optimum from any starting set (Kim & Park), so the result
-    // is the reference's; only the number of exchange steps changes
+    // warm start from the previous solution's passive set: with AtA positive
+    // definite BPP reaches the unique NNLS optimum from any starting set (Kim
+    // & Park), so the result is the reference's; only the number of exchange
+    // steps changes. When AtA is singular (a component whose factor column
+    // collapsed to zero leaves a zero row and column) the optimum is not
+    // unique and the warm set's system may be singular: a failed warm solve
+    // restarts from the reference's start, X = 0 (bppnnls.hpp:73-74).
     const bool lo = has_lo && Pinit[c * n + lane] > 0.0;
     const bool hi = has_hi && Pinit[c * n + lane + 32] > 0.0;
     passive = warp_mask64(lo, hi);
@@ -346,6 +350,16 @@ __global__ void __launch_bounds__(32 * BPP_WARPS, 1) k_bpp(const double* __restr
     if (passive) {
       ++iter;
       st = solve_passive();
+      if (st != 0) {
+        st = 0;
+        iter = 0;
+        passive = 0;
+        for (int i = lane; i < n; i += 32) {
+          x[i] = 0.0;
+          y[i] = -b[i];
+        }
+        __syncwarp();
+      }
     }
   }
   uint64_t nonopt = 0, infea = 0;

@@ -1113,6 +1113,22 @@ __global__ void __launch_bounds__(256) k_cp_step(CpStep s, double eta, double mo
   }
 }
 
+// Rows of a Khatri-Rao product, out[g, r] = W(g, r) of `wg` (the product
+// order of wgen_eval), g < rows: the tail image of a long direct MTTKRP.
+__global__ void __launch_bounds__(256) k_krp_rows(WGen wg, int64_t rows, int k,
+                                                  double* __restrict__ out) {
+  for (int64_t e = (int64_t)blockIdx.x * 256 + threadIdx.x; e < rows * k;
+       e += (int64_t)gridDim.x * 256)
+    out[e] = wgen_eval(wg, e / k, (int)(e % k), k);
+}
+
+// out[e] = v for e < n
+__global__ void k_fill(double* __restrict__ out, int64_t n, double v) {
+  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n;
+       e += (int64_t)gridDim.x * blockDim.x)
+    out[e] = v;
+}
+
 // acc = (first ? 0 : acc) + the nb partials summed in a fixed order (one
 // warp: lane l adds partials l, l + 32, ..., then a fixed shuffle tree).
 __global__ void k_accum_norm(const double* __restrict__ part, int nb, double* __restrict__ acc,

