@@ -25,10 +25,8 @@ namespace pg {
 // The products run on the FP64 tensor cores: warp-level
 // mma.sync.m8n8k4.f64 (the only FP64 MMA of sm_100a), each warp owning a
 // (128 / WARPS_M) x (KP / WARPS_N) block of the output as 8 x 8 accumulator
-// tiles. Tiles of X stream through a ring of CT_STAGES shared-memory buffers
-// filled by cp.async (three tiles in flight while one is multiplied); the
-// Khatri-Rao tile is generated into registers one tile ahead and stored
-// into one of two buffers. Shared-memory layouts are chosen so
+// tiles. The next reduction tile is loaded into registers while the current
+// one is multiplied out of shared memory. Shared-memory layouts are chosen so
 // that every fragment load is two 128-byte wavefronts (no bank conflicts):
 //   RIGHT: Xs[kk][m], row stride 128 + 8 doubles (X is m-contiguous);
 //   LEFT : Xs[m][kk], row stride BK + 4 doubles (X is kk-contiguous);
@@ -59,54 +57,21 @@ __device__ __forceinline__ void dmma_m8n8k4(double (&c)[2], double a, double b) 
                : "d"(a), "d"(b));
 }
 
-// Shared-memory ring of the contraction: CT_STAGES tiles of X in flight
-// (cp.async), two Khatri-Rao tiles (register-staged one tile ahead).
-constexpr int CT_STAGES = 4;
 template <int KP, bool LEFT>
-constexpr int ct_sx() { return LEFT ? ct_bk<KP>() + 4 : CT_BM + 8; }
-template <int KP, bool LEFT>
-constexpr size_t ct_smem_bytes() {
-  return ((size_t)CT_STAGES * (LEFT ? CT_BM * ct_sx<KP, LEFT>() : ct_bk<KP>() * ct_sx<KP, LEFT>()) +
-          2 * (size_t)ct_bk<KP>() * ct_ws<KP>()) *
-         sizeof(double);
-}
-
-// cp.async of `bytes` (16 or 8) from global to shared memory; src_bytes <
-// bytes zero-fills the rest (src_bytes = 0: nothing is read).
-__device__ __forceinline__ void cp_async16(void* dst, const void* src, int src_bytes) {
-  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src), "r"(src_bytes)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async8(void* dst, const void* src, int src_bytes) {
-  const uint32_t d = (uint32_t)__cvta_generic_to_shared(dst);
-  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src), "r"(src_bytes)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
-}
-
-// vec2: X is read in 16-byte pieces (two doubles); the caller sets it when
-// every piece is 16-byte aligned (RIGHT: ldx even; LEFT: ldx and ldb even).
-template <int KP, bool LEFT>
-__global__ void __launch_bounds__(256, 1) k_contract_f64(const double* __restrict__ X,
+__global__ void __launch_bounds__(256, 2) k_contract_f64(const double* __restrict__ X,
                                                          ContractGeom g, WGen wg, int k,
-                                                         double* __restrict__ out, int vec2) {
+                                                         double* __restrict__ out) {
   constexpr int BK = ct_bk<KP>();
+  constexpr int XPT = BK * CT_BM / 256;  // X elements per thread per tile
   constexpr int WPT = (BK * KP + 255) / 256;
   constexpr int WARPS_M = KP >= 32 ? 4 : 8;
   constexpr int WARPS_N = 8 / WARPS_M;
   constexpr int MT = CT_BM / WARPS_M / 8;  // 8-row MMA tiles per warp
   constexpr int NT = KP / WARPS_N / 8;     // 8-rank MMA tiles per warp
-  constexpr int SX = ct_sx<KP, LEFT>();
+  constexpr int SX = LEFT ? BK + 4 : CT_BM + 8;
   constexpr int SW = ct_ws<KP>();
-  constexpr int XT = LEFT ? CT_BM * SX : BK * SX;  // doubles of one X stage
-  extern __shared__ __align__(16) double ct_sm[];
-  double* Xs = ct_sm;                       // CT_STAGES x XT
-  double* Wsb = ct_sm + CT_STAGES * XT;     // 2 x BK x SW
+  __shared__ __align__(16) double Xs[LEFT ? CT_BM * SX : BK * SX];
+  __shared__ __align__(16) double Ws[BK * SW];
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   const int fg = lane >> 2, ft = lane & 3;
@@ -124,149 +89,121 @@ __global__ void __launch_bounds__(256, 1) k_contract_f64(const double* __restric
 #pragma unroll
     for (int j = 0; j < NT; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
-  // X tile t -> stage buffer xs (asynchronous; out-of-range elements are 0)
-  auto issue_x = [&](int64_t t, double* xs) {
+  double xr[XPT];
+  double wr[WPT];
+
+  auto load_tile = [&](int64_t t) {
     if constexpr (!LEFT) {
       const int64_t j0 = t * BK;
-      if (vec2) {
-        // BK rows of 128 m: 64 pieces a row
+      const int mm = tid & 127;
+      const int64_t gm = m0 + mm;
 #pragma unroll
-        for (int u = 0; u < BK * 64 / 256; ++u) {
-          const int c = tid + 256 * u, jj = c >> 6, mm = (c & 63) * 2;
-          const int64_t gm = m0 + mm, gj = j0 + jj;
-          const int64_t left = g.M - gm;
-          const int nb = (gj < g.A && left > 0) ? (left >= 2 ? 16 : 8) : 0;
-          cp_async16(xs + jj * SX + mm, nb ? (const void*)(X + gm + g.ldx * gj) : (const void*)X, nb);
-        }
-      } else {
+      for (int i = 0; i < XPT; ++i) {
+        int kk = (tid >> 7) + 2 * i;
+        int64_t gj = j0 + kk;
+        xr[i] = (gm < g.M && gj < g.A) ? X[gm + g.ldx * gj] : 0.0;
+      }
+      WIdx base;
+      if (wg.nf > 1) widx_init(wg, j0, base);
 #pragma unroll
-        for (int u = 0; u < BK * 128 / 256; ++u) {
-          const int c = tid + 256 * u, jj = c >> 7, mm = c & 127;
-          const int64_t gm = m0 + mm, gj = j0 + jj;
-          const int nb = (gj < g.A && gm < g.M) ? 8 : 0;
-          cp_async8(xs + jj * SX + mm, nb ? (const void*)(X + gm + g.ldx * gj) : (const void*)X, nb);
+      for (int i = 0; i < WPT; ++i) {
+        int e = tid + 256 * i;
+        double v = 0.0;
+        if (e < BK * KP) {
+          int kk = e / KP, r = e % KP;
+          int64_t gj = j0 + kk;
+          if (r < k && gj < g.A) {
+            if (wg.nf == 1) {
+              v = wg.f[0][gj * k + r];
+            } else {
+              WIdx w = base;
+              widx_advance(wg, w, kk);
+              v = wgen_row(wg, w, r, k);
+            }
+          }
         }
+        wr[i] = v;
       }
     } else {
       const int64_t b = t / tilesA;
       const int64_t a0 = (t % tilesA) * BK;
-      const double* Xb = X + g.ldb * b;
-      if (vec2) {
-        // 128 rows m of BK a: BK/2 pieces a row
+      const int aa = tid % BK;
+      const int64_t ga = a0 + aa;
 #pragma unroll
-        for (int u = 0; u < CT_BM * (BK / 2) / 256; ++u) {
-          const int c = tid + 256 * u, mm = c / (BK / 2), aa = (c % (BK / 2)) * 2;
-          const int64_t gm = m0 + mm, ga = a0 + aa;
-          const int64_t left = g.A - ga;
-          const int nb = (gm < g.M && left > 0) ? (left >= 2 ? 16 : 8) : 0;
-          cp_async16(xs + mm * SX + aa, nb ? (const void*)(Xb + ga + g.ldx * gm) : (const void*)X, nb);
-        }
-      } else {
-#pragma unroll
-        for (int u = 0; u < CT_BM * BK / 256; ++u) {
-          const int c = tid + 256 * u, mm = c / BK, aa = c % BK;
-          const int64_t gm = m0 + mm, ga = a0 + aa;
-          const int nb = (gm < g.M && ga < g.A) ? 8 : 0;
-          cp_async8(xs + mm * SX + aa, nb ? (const void*)(Xb + ga + g.ldx * gm) : (const void*)X, nb);
-        }
+      for (int i = 0; i < XPT; ++i) {
+        int mm = tid / BK + (256 / BK) * i;
+        int64_t gm = m0 + mm;
+        xr[i] = (gm < g.M && ga < g.A) ? X[ga + g.ldx * gm + g.ldb * b] : 0.0;
       }
-    }
-  };
-
-  // Khatri-Rao rows of tile t into registers, then into a W buffer
-  double wr[WPT];
-  auto load_w = [&](int64_t t) {
-    int64_t r0;  // first Khatri-Rao row of the tile
-    int64_t lim;
-    if constexpr (!LEFT) {
-      r0 = t * BK;
-      lim = g.A;
-    } else {
-      const int64_t b = t / tilesA;
-      const int64_t a0 = (t % tilesA) * BK;
-      r0 = a0 + g.A * b;
-      lim = a0;  // rows a0 .. g.A - 1 of this batch are in range
-    }
-    WIdx base;
-    if (wg.nf > 1) widx_init(wg, r0, base);
+      WIdx base;
+      widx_init(wg, a0 + g.A * b, base);
 #pragma unroll
-    for (int i = 0; i < WPT; ++i) {
-      const int e = tid + 256 * i;
-      double v = 0.0;
-      if (e < BK * KP) {
-        const int kk = e / KP, r = e % KP;
-        const bool inr = LEFT ? (lim + kk < g.A) : (r0 + kk < lim);
-        if (r < k && inr) {
-          if (wg.nf == 1) {
-            v = wg.f[0][(r0 + kk) * k + r];
-          } else {
+      for (int i = 0; i < WPT; ++i) {
+        int e = tid + 256 * i;
+        double v = 0.0;
+        if (e < BK * KP) {
+          int kk = e / KP, r = e % KP;
+          int64_t gaa = a0 + kk;
+          if (r < k && gaa < g.A) {
             WIdx w = base;
             widx_advance(wg, w, kk);
             v = wgen_row(wg, w, r, k);
           }
         }
+        wr[i] = v;
       }
-      wr[i] = v;
     }
   };
-  auto store_w = [&](double* ws) {
+  auto store_tile = [&]() {
+    if constexpr (!LEFT) {
+      const int mm = tid & 127;
+#pragma unroll
+      for (int i = 0; i < XPT; ++i) Xs[((tid >> 7) + 2 * i) * SX + mm] = xr[i];
+    } else {
+      const int aa = tid % BK;
+#pragma unroll
+      for (int i = 0; i < XPT; ++i) Xs[(tid / BK + (256 / BK) * i) * SX + aa] = xr[i];
+    }
 #pragma unroll
     for (int i = 0; i < WPT; ++i) {
-      const int e = tid + 256 * i;
-      if (e < BK * KP) ws[(e / KP) * SW + (e % KP)] = wr[i];
+      int e = tid + 256 * i;
+      if (e < BK * KP) Ws[(e / KP) * SW + (e % KP)] = wr[i];
     }
   };
 
-  const int64_t ntl = t_end - t_begin;
-  // prologue: the first CT_STAGES - 1 X tiles in flight (one group each,
-  // empty groups past the end keep the count uniform)
-#pragma unroll
-  for (int i = 0; i < CT_STAGES - 1; ++i) {
-    if (i < ntl) issue_x(t_begin + i, Xs + i * XT);
-    cp_async_commit();
-  }
-  if (ntl > 0) load_w(t_begin);
-  for (int64_t i = 0; i < ntl; ++i) {
-    const int st = (int)(i % CT_STAGES);
-    double* ws = Wsb + (int)(i & 1) * (BK * SW);
-    cp_async_wait<CT_STAGES - 2>();  // this thread's pieces of tile i have landed
-    store_w(ws);
-    __syncthreads();  // tile i visible to all; every thread is done with tile i - 1
-    {
-      const int64_t nx = i + CT_STAGES - 1;
-      if (nx < ntl) issue_x(t_begin + nx, Xs + (int)(nx % CT_STAGES) * XT);
-      cp_async_commit();
-    }
-    if (i + 1 < ntl) load_w(t_begin + i + 1);
-    const double* xs = Xs + st * XT;
+  if (t_begin < t_end) load_tile(t_begin);
+  for (int64_t t = t_begin; t < t_end; ++t) {
+    __syncthreads();
+    store_tile();
+    __syncthreads();
+    if (t + 1 < t_end) load_tile(t + 1);
 #pragma unroll
     for (int s4 = 0; s4 < BK / 4; ++s4) {
       const int kk = s4 * 4 + ft;
       double af[MT], bf[NT];
 #pragma unroll
-      for (int q = 0; q < MT; ++q) {
-        const int m = wm0 + q * 8 + fg;
-        af[q] = LEFT ? xs[m * SX + kk] : xs[kk * SX + m];
+      for (int i = 0; i < MT; ++i) {
+        const int m = wm0 + i * 8 + fg;
+        af[i] = LEFT ? Xs[m * SX + kk] : Xs[kk * SX + m];
       }
 #pragma unroll
-      for (int j = 0; j < NT; ++j) bf[j] = ws[kk * SW + wn0 + j * 8 + fg];
+      for (int j = 0; j < NT; ++j) bf[j] = Ws[kk * SW + wn0 + j * 8 + fg];
 #pragma unroll
-      for (int q = 0; q < MT; ++q)
+      for (int i = 0; i < MT; ++i)
 #pragma unroll
-        for (int j = 0; j < NT; ++j) dmma_m8n8k4(acc[q][j], af[q], bf[j]);
+        for (int j = 0; j < NT; ++j) dmma_m8n8k4(acc[i][j], af[i], bf[j]);
     }
   }
-  cp_async_wait<0>();
   double* o = out + (int64_t)blockIdx.y * g.split_stride;
 #pragma unroll
-  for (int q = 0; q < MT; ++q) {
-    const int64_t gm = m0 + wm0 + q * 8 + fg;
+  for (int i = 0; i < MT; ++i) {
+    const int64_t gm = m0 + wm0 + i * 8 + fg;
     if (gm >= g.M) continue;
 #pragma unroll
     for (int j = 0; j < NT; ++j) {
       const int r = wn0 + j * 8 + 2 * ft;
-      if (r < k) o[gm * k + r] = acc[q][j][0];
-      if (r + 1 < k) o[gm * k + r + 1] = acc[q][j][1];
+      if (r < k) o[gm * k + r] = acc[i][j][0];
+      if (r + 1 < k) o[gm * k + r + 1] = acc[i][j][1];
     }
   }
 }

@@ -377,48 +377,6 @@ WGen make_wgen(planc_gpu_ctx* c, const std::vector<int>& modes) {
   return g;
 }
 
-// ---------------------------------------------------------------- FP64 contraction launch
-// The contraction kernels take more than 48 KB of dynamic shared memory: the
-// attribute is set once per device (outside any graph capture).
-std::mutex g_ct_attr_mutex;
-bool g_ct_attr_done[64] = {false};
-
-void ct_ensure_attrs(int dev) {
-  std::lock_guard<std::mutex> lock(g_ct_attr_mutex);
-  if (dev < 0 || dev >= 64 || g_ct_attr_done[dev]) return;
-#define CT_ATTR(KP, LEFT)                                                                    \
-  CK(cudaFuncSetAttribute(k_contract_f64<KP, LEFT>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                          (int)ct_smem_bytes<KP, LEFT>()));
-  CT_ATTR(8, false) CT_ATTR(8, true) CT_ATTR(16, false) CT_ATTR(16, true)
-  CT_ATTR(32, false) CT_ATTR(32, true) CT_ATTR(64, false) CT_ATTR(64, true)
-#undef CT_ATTR
-  g_ct_attr_done[dev] = true;
-}
-
-// X read in 16-byte pieces when every piece is aligned: X itself, the
-// column (RIGHT) or row and batch (LEFT) strides even.
-int ct_vec2(const double* X, const ContractGeom& g, bool left) {
-  if (((uintptr_t)X & 15) != 0 || (g.ldx & 1)) return 0;
-  if (left && (g.ldb & 1)) return 0;
-  return 1;
-}
-
-void ct_launch(int KP, bool left, dim3 grid, cudaStream_t st, const double* X, const ContractGeom& g,
-               const WGen& wg, int k, double* out) {
-  const int v2 = ct_vec2(X, g, left);
-#define CT_L(KPV)                                                                             \
-  case KPV:                                                                                   \
-    if (left)                                                                                 \
-      k_contract_f64<KPV, true><<<grid, 256, ct_smem_bytes<KPV, true>(), st>>>(X, g, wg, k, out, v2);   \
-    else                                                                                      \
-      k_contract_f64<KPV, false><<<grid, 256, ct_smem_bytes<KPV, false>(), st>>>(X, g, wg, k, out, v2); \
-    break;
-  switch (KP) {
-    CT_L(8) CT_L(16) CT_L(32) CT_L(64)
-  }
-#undef CT_L
-}
-
 // ---------------------------------------------------------------- planning
 struct ContractPlan {
   ContractGeom g;
@@ -439,8 +397,8 @@ ContractPlan plan_contract(planc_gpu_ctx* c, bool left, int64_t M, int64_t ldx, 
   int64_t tilesA = (A + bk - 1) / bk;
   p.g.ktiles = left ? tilesA * B : tilesA;
   int64_t mtiles = (M + CT_BM - 1) / CT_BM;
-  // one CTA per SM is resident: split K only to fill the SMs once
-  int64_t ns = mtiles < eff_sm(c) ? eff_sm(c) / mtiles : 1;
+  int64_t target = 2 * (int64_t)eff_sm(c);
+  int64_t ns = (target + mtiles - 1) / mtiles;
   ns = std::max<int64_t>(1, std::min<int64_t>(ns, p.g.ktiles));
   ns = std::min<int64_t>(ns, 1024);
   p.g.tiles_per_split = (p.g.ktiles + ns - 1) / ns;
@@ -570,7 +528,17 @@ void run_contract(planc_gpu_ctx* c, const ContractPlan& p, bool left, const doub
     fail(PLANC_GPU_ERR_STATE, "internal: contraction scratch larger than planned");
   double* dst = p.nsplit > 1 ? c->scratch : out;
   launch(c, left ? KC_CONTRACT_LEFT : KC_CONTRACT, [&] {
-    ct_launch(kpad(k), left, p.grid, c->stream, X, p.g, wg, k, dst);
+    switch (kpad(k)) {
+#define CASE(KP)                                                                      \
+  case KP:                                                                            \
+    if (left)                                                                         \
+      k_contract_f64<KP, true><<<p.grid, 256, 0, c->stream>>>(X, p.g, wg, k, dst);    \
+    else                                                                              \
+      k_contract_f64<KP, false><<<p.grid, 256, 0, c->stream>>>(X, p.g, wg, k, dst);   \
+    break;
+      CASE(8) CASE(16) CASE(32) CASE(64)
+#undef CASE
+    }
   });
   if (p.nsplit > 1) {
     int64_t n = p.g.M * k;
@@ -1396,7 +1364,6 @@ int planc_gpu_create(planc_gpu_ctx** out, int device, int precision, void* cuda_
         attrs_set[device] = true;
       }
     }
-    ct_ensure_attrs(device);
     planc_gpu_ctx* c = new planc_gpu_ctx();
     c->device = device;
     c->precision = precision;
@@ -2613,7 +2580,6 @@ extern "C" int planc_gpu_mttkrp_last_mode_noalloc(const double* X_dev, const int
     CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kNoAllocMaxDevices) fail(PLANC_GPU_ERR_UNSUPPORTED, "device index too large");
     double* scratch = noalloc_scratch(dev);
-    ct_ensure_attrs(dev);
     int sms = 148;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     // Khatri-Rao operand over modes 0..N-2, lowest mode fastest
@@ -2639,7 +2605,7 @@ extern "C" int planc_gpu_mttkrp_last_mode_noalloc(const double* X_dev, const int
     const int bk = k > 32 ? ct_bk<64>() : ct_bk<32>();
     g.ktiles = (A + bk - 1) / bk;
     const int64_t mtiles = (R + CT_BM - 1) / CT_BM;
-    int64_t ns = mtiles < sms ? sms / mtiles : 1;
+    int64_t ns = (2 * (int64_t)sms + mtiles - 1) / mtiles;
     ns = std::max<int64_t>(1, std::min<int64_t>(ns, g.ktiles));
     ns = std::min<int64_t>(ns, (int64_t)(kNoAllocScratchDoubles / ((size_t)R * k)));
     g.tiles_per_split = (g.ktiles + ns - 1) / ns;
@@ -2649,7 +2615,12 @@ extern "C" int planc_gpu_mttkrp_last_mode_noalloc(const double* X_dev, const int
     cudaStream_t st = (cudaStream_t)cuda_stream;
     // every split writes its whole R x k partial (zeros when it has no tiles),
     // so nothing left in the scratch by an earlier call is read
-    ct_launch(kpad(k), true, grid, st, X_dev, g, wg, k, scratch);
+    switch (kpad(k)) {
+      case 8: k_contract_f64<8, true><<<grid, 256, 0, st>>>(X_dev, g, wg, k, scratch); break;
+      case 16: k_contract_f64<16, true><<<grid, 256, 0, st>>>(X_dev, g, wg, k, scratch); break;
+      case 32: k_contract_f64<32, true><<<grid, 256, 0, st>>>(X_dev, g, wg, k, scratch); break;
+      default: k_contract_f64<64, true><<<grid, 256, 0, st>>>(X_dev, g, wg, k, scratch); break;
+    }
     CK(cudaGetLastError());
     const int64_t n = R * k;
     reduce_splits(st, scratch, (int)ns, n, n, out_dev);
