@@ -342,6 +342,8 @@ def main():
         "right": (kt["contract"], numel * EB[args.precision] + L * k * 4),
         "left": (kt["contract_left"], numel * EB[args.precision] + nsplit_left * R * k * 8),
     }
+    # the left contraction's kernel: the factored form when I0 is a multiple of 64
+    kname = {"right": "k_tc_right", "left": "k_tc_left_fac" if dims[0] % 64 == 0 else "k_tc_left"}
     peak, peak_kind = peaks()
     per_kernel = {}
     for name, ((kms, kn), kbytes) in kern.items():
@@ -358,7 +360,7 @@ def main():
                 "frac": d["achieved_gbs"] / peak if d["achieved_gbs"] else None,
                 "traffic": traffic_from_profiles(args.precision, dims, k, dom),
                 "peak_source": peak_kind,
-                "kernel": "partial MTTKRP, %s contraction (k_tc_%s)" % (dom, dom),
+                "kernel": "partial MTTKRP, %s contraction (%s)" % (dom, kname[dom]),
                 "algorithmic_bytes_per_launch": d["algorithmic_bytes_per_launch"],
                 "avg_launch_ms": d["avg_launch_ms"], "launches": d["launches"],
                 "per_kernel": per_kernel}

@@ -8,15 +8,18 @@ one launch holds a few GB of device memory at most while the tensors stay
 larger than the 126 MB L2 (DRAM counters stay meaningful):
 
   f64     k_contract_f64 (FP64 path, DMMA): 512^3 tensor (FP64 copy), rank 32, HALS
-  bpp     k_bpp: ANLS/BPP normal equations of a 192-row mode at rank 64 taken
-          from a 192 x 96 x 96 x 96 sparse-factor CP tensor after 10
-          iterations (passive sets of ~45, ~3 BPP steps per row)
+  bpp     k_bpp / k_bpp_cta: ANLS/BPP normal equations of a 192-row mode at
+          rank 64 taken from a 192 x 96 x 96 x 96 sparse-factor CP tensor
+          after 10 iterations (passive sets of ~40, ~3 BPP steps per row),
+          also repeated to 768 and 3072 right-hand sides, with either kernel
   tc3     k_tc_right / k_tc_left_fac: 512^3 FP32 tensor (BF16 copy), rank 32,
           HALS iterations
   tc4     k_tc_long (both sides) + the multi-TTVs of the balanced 4-way tree:
           128^4 FP32 tensor (BF16 copy), rank 64, HALS iterations
   cfg3it  three ANLS/BPP iterations of the 192^4 rank-64 workload (BF16), for
           a one-pass launch list at full size
+  cfg4it  the 256-tensor batched HALS workload (dims U{32..256}, ranks
+          U{4,8,16,32}, BF16 copies), three batched iterations, no autotuning
   nmf     shared-memory NMF of a dense 16384 x 16384 FP32 matrix (BF16 copy),
           rank 32: three iterations each of MU, HALS and ANLS/BPP
   upd     AO-ADMM and Nesterov NTF updates on the 1024^3 rank-32 headline
@@ -65,6 +68,7 @@ def _timed(torch, ctx, fn, reps):
 
 
 def case_bpp(gpu, torch):
+    import os
     dims, k = (192, 96, 96, 96), 64
     X, F0 = _synth(gpu, torch, dims, k, 11, sparse=True)
     with gpu.Context(0, "bf16") as c:
@@ -72,16 +76,29 @@ def case_bpp(gpu, torch):
         c.set_factors(F0)
         c.run("anlsbpp", 10, compute_error=False)
         G, M = c.mode_begin(0)
-    with gpu.Context(0, "fp64") as c:
-        for _ in range(3):
-            c.set_timing(True)
-            c.kernel_times()
-            _, P, its = c.bpp_solve(G, M.T)
-            ms = c.kernel_times()["bpp"][0]
-            c.set_timing(False)
-    print("bpp: 192 rows, k=64: kernel %.1f us, BPP steps mean %.2f max %d, passive mean %.1f"
-          % (ms * 1e3, its.mean(), its.max(), P.sum(axis=0).mean()))
-    print("bpp: rows per BPP step count:", dict(enumerate(np.bincount(its).tolist())))
+    res = {}
+    # the mode's 192 right-hand sides, then the same rows repeated (more
+    # right-hand sides per launch), with each batched BPP kernel
+    for reps in (1, 4, 16):
+        B = np.tile(M.T, (1, reps))
+        for kern in ("warp", "cta"):
+            os.environ["PLANC_GPU_BPP_KERNEL"] = kern
+            with gpu.Context(0, "fp64") as c:
+                for _ in range(3):
+                    c.set_timing(True)
+                    c.kernel_times()
+                    Xs, P, its = c.bpp_solve(G, B)
+                    ms = c.kernel_times()["bpp"][0]
+                    c.set_timing(False)
+            del os.environ["PLANC_GPU_BPP_KERNEL"]
+            res[(reps, kern)] = (Xs, P)
+            print("bpp: %d rows, k=64, %s kernel: %.1f us, BPP steps mean %.2f max %d, passive mean %.1f"
+                  % (B.shape[1], kern, ms * 1e3, its.mean(), its.max(), P.sum(axis=0).mean()))
+        (xw, pw), (xc, pc) = res[(reps, "warp")], res[(reps, "cta")]
+        print("bpp: %d rows: masks differ in %d entries, max |X_warp - X_cta| / max |X| = %.2e"
+              % (B.shape[1], int((pw != pc).sum()), np.abs(xw - xc).max() / max(np.abs(xw).max(), 1e-300)))
+        if reps == 1:
+            print("bpp: rows per BPP step count:", dict(enumerate(np.bincount(its).tolist())))
 
 
 def case_f64(gpu, torch):
@@ -186,7 +203,37 @@ def case_nes(gpu, torch):
     print("nes: 512^3 k=32 Nesterov: %.3f ms per iteration (8 in one call)" % ms)
 
 
-CASES = {"bpp": case_bpp, "f64": case_f64, "nes": case_nes, "tc3": case_tc3, "tc4": case_tc4, "cfg3it": case_cfg3it,
+def case_cfg4it(gpu, torch):
+    # the batched workload of 256 uneven 3-way FP32 tensors (dims U{32..256},
+    # ranks U{4,8,16,32}, BF16 copies), two HALS iterations without the
+    # autotuner: a launch list of one batched iteration's per-member kernels
+    import time
+    rng = np.random.default_rng(401)
+    specs = [(tuple(int(d) for d in rng.integers(32, 257, size=3)), int(rng.choice([4, 8, 16, 32])))
+             for _ in range(256)]
+    b = gpu.Batch(0, "bf16", nstreams=64)
+    for i, (dims, k) in enumerate(specs):
+        r = np.random.default_rng(1000 + i)
+        A = [r.random((d, k)) for d in dims]
+        G = np.ones((k, k))
+        for a in A:
+            G *= a.T @ a
+        sigma = 0.01 * np.sqrt(G.sum() / float(np.prod(dims)))
+        X = torch.empty(int(np.prod(dims)), dtype=torch.float32, device="cuda:0")
+        gpu.synth_cp_tensor(0, X.data_ptr(), "f32", dims, A, sigma, 2000 + i, clip=True)
+        b.add(X.data_ptr(), [r.random((d, k)) for d in dims], dims=dims, dtype="f32")
+        del X
+    b.run("hals", 1, compute_error=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    b.run("hals", 2, compute_error=True)
+    torch.cuda.synchronize()
+    print("cfg4it: 256 tensors, HALS: %.3f ms per batched iteration (2 iterations, untuned)"
+          % ((time.perf_counter() - t0) * 500))
+    b.close()
+
+
+CASES = {"bpp": case_bpp, "cfg4it": case_cfg4it, "f64": case_f64, "nes": case_nes, "tc3": case_tc3, "tc4": case_tc4, "cfg3it": case_cfg3it,
          "ttv": case_ttv, "nmf": case_nmf, "upd": case_upd}
 
 

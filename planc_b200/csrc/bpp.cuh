@@ -397,4 +397,312 @@ __global__ void __launch_bounds__(32 * BPP_WARPS, 1) k_bpp(const double* __restr
   }
 }
 
+// ------------------------------------------------------------ CTA per row
+// The same BPP trajectory with one CTA per right-hand side (k_bpp gives each
+// one warp): for the few-hundred-row modes of a 4-way tensor a warp per row
+// leaves most SMs and schedulers idle and every step waits on one warp's
+// dependency chain, so the passive solve is spread over the whole CTA.
+//
+// Passive solve: right-looking Cholesky of the passive principal submatrix
+// bordered by the right-hand side, [S; z^T] (rows 0..m-1 the compacted
+// passive indices, row KP the right-hand side). Eliminating column j
+// subtracts S(i, j) S(c, j) / S(j, j) from every later entry (i, c); the
+// bordered row then holds y = L^{-1} z, and one warp finishes with the back
+// substitution L^T x = y. The lower triangle is held in registers: the
+// thread of segment t owns SEGW consecutive entries (row i, columns c0 ..
+// c0+SEGW-1) for the whole factorisation. After its update of column j the
+// owner of column j+1 publishes it to cbuf(:, j+1), and the owner of the
+// diagonal entry also publishes s = 1 / sqrt(pivot) and s^2 (or marks the
+// pivot as failed), so each column costs one barrier of the threads that own
+// segments; cbuf keeps every column, which is the factor the back
+// substitution reads (L(i, j) = cbuf(i, j) * s_j). Column entries sit at
+// i + i / 8, so the eight entries a segment reads lie in distinct banks for
+// the segments of one warp. Segments are numbered row by row (row i has
+// i / SEGW + 1 of them), so the segments of an m-row system are the first
+// ones for every m, followed by the ceil(m / SEGW) segments of the bordered
+// row.
+template <int KP, int SEGW>
+struct BppCta {
+  static constexpr int NBLK = KP / SEGW;                       // segments of a full row
+  static constexpr int NSEG = SEGW * NBLK * (NBLK + 1) / 2 + NBLK;
+  static constexpr int THREADS = (NSEG + 31) / 32 * 32;
+  // column stride of cbuf: entries 0..KP at i + i / 8; odd, so that walking a
+  // row across columns is conflict-free too
+  static constexpr int LDC = KP + KP / 8 + 1;
+  // threads per row of the Y = AtA X - AtB product (a power of two <= 32)
+  static constexpr int TPR = THREADS / KP >= 8 ? 8 : THREADS / KP >= 4 ? 4 : THREADS / KP >= 2 ? 2 : 1;
+  static constexpr size_t SMEM = ((size_t)KP * KP + (size_t)KP * LDC + 6 * (size_t)KP) * 8 + (size_t)KP * 4 + 16;
+};
+
+// segments of the rows 0..m-1 (row i has i / segw + 1)
+__host__ __device__ constexpr int bppc_row_segments(int m, int segw) {
+  return segw * (m / segw) * (m / segw + 1) / 2 + (m % segw) * (m / segw + 1);
+}
+
+template <int KP, int SEGW>
+__global__ void __launch_bounds__(BppCta<KP, SEGW>::THREADS, 2)
+    k_bpp_cta(const double* __restrict__ AtA_g, const double* __restrict__ Bm, int n, int64_t ncols,
+              double* __restrict__ Xout, int* __restrict__ passive_out, int* __restrict__ iters_out,
+              int* __restrict__ status, int max_iter_override, const double* __restrict__ Pinit) {
+  using C = BppCta<KP, SEGW>;
+  constexpr int LDC = C::LDC, TPR = C::TPR, NT = C::THREADS;
+  extern __shared__ __align__(16) unsigned char bppc_smem[];
+  double* AtA = reinterpret_cast<double*>(bppc_smem);  // n x n, leading dimension n
+  double* cbuf = AtA + KP * KP;                         // column j: cbuf[j * LDC + i + i / 8], i <= KP
+  double* sv = cbuf + KP * LDC;                         // 1 / sqrt(pivot j)
+  double* qv = sv + KP;                                 // 1 / pivot j
+  double* x = qv + KP;
+  double* y = x + KP;
+  double* b = y + KP;
+  double* z = b + KP;  // compacted solution
+  int* idx = reinterpret_cast<int*>(z + KP);
+  __shared__ int lu_rc;
+  __shared__ int bad_at;  // first pivot that is not positive and finite (KP + 1: none)
+  const int tid = threadIdx.x, lane = tid & 31;
+  for (int e = tid; e < n * n; e += NT) AtA[e] = __ldg(AtA_g + e);
+  // this thread's segment of the full triangle: row block q holds rows
+  // q*SEGW .. q*SEGW+SEGW-1 with q+1 segments each
+  int seg_row = -1, seg_c0 = 0;
+  {
+    int base = 0;
+    for (int q = 0; q < C::NBLK; ++q) {
+      const int cnt = SEGW * (q + 1);
+      if (tid >= base && tid < base + cnt) {
+        seg_row = q * SEGW + (tid - base) / (q + 1);
+        seg_c0 = SEGW * ((tid - base) % (q + 1));
+      }
+      base += cnt;
+    }
+  }
+  const bool has_lo = lane < n, has_hi = lane + 32 < n;
+  const int pbar = 3;
+  const unsigned max_it = max_iter_override > 0 ? (unsigned)max_iter_override : 5u * (unsigned)n;
+
+  for (int64_t c = blockIdx.x; c < ncols; c += gridDim.x) {
+    __syncthreads();  // AtA staged / the previous row's buffers are free
+    for (int i = tid; i < n; i += NT) {
+      b[i] = Bm[c * n + i];
+      x[i] = 0.0;
+      y[i] = -b[i];  // Y = AtA*0 - AtB, bppnnls.hpp:73
+    }
+    uint64_t passive = 0;  // bppnnls.hpp:74
+    int P = pbar, Ninf = n + 1;  // bppnnls.hpp:76-81
+
+    // X(P) = solve(AtA(P,P), AtB(P)), X(~P) = 0, Y = AtA X - AtB and the
+    // 1e-12 zeroing (bppnnls.hpp:163-172); uniform across the CTA
+    auto solve_passive = [&]() -> int {
+      const int m = __popcll(passive);
+      __syncthreads();  // x, y, b of the previous step read by every warp
+      if (tid < 32) {
+        if ((passive >> lane) & 1) idx[__popcll(passive & ((1ull << lane) - 1ull))] = lane;
+        if ((passive >> (lane + 32)) & 1)
+          idx[__popcll(passive & ((1ull << (lane + 32)) - 1ull))] = lane + 32;
+        if (lane == 0) bad_at = KP + 1;
+      }
+      __syncthreads();
+      const int nrow = bppc_row_segments(m, SEGW);
+      const int nact = nrow + (m + SEGW - 1) / SEGW;
+      int row = -1, c0 = 0;
+      if (tid < nrow) {
+        row = seg_row;
+        c0 = seg_c0;
+      } else if (tid < nact) {
+        row = KP;  // the bordered right-hand-side row
+        c0 = SEGW * (tid - nrow);
+      }
+      const int cb0 = c0 + (c0 >> 3);  // position of column c0 in a cbuf column
+      const int rpos = row + (row >> 3);
+      auto publish_pivot = [&](int j, double d) {
+        if (!(d > 0.0) || !isfinite(d)) {
+          bad_at = j;
+        } else {
+          const double sj = rsqrt(d);
+          sv[j] = sj;
+          qv[j] = sj * sj;
+        }
+      };
+      double v[SEGW];
+      {
+        const int gi = (row >= 0 && row < KP) ? idx[row] : 0;
+#pragma unroll
+        for (int u = 0; u < SEGW; ++u) {
+          const int cc = c0 + u;
+          double e = 0.0;
+          if (row == KP) {
+            if (cc < m) e = b[idx[cc]];
+          } else if (row >= 0 && cc <= row) {
+            e = AtA[gi + n * idx[cc]];
+          }
+          v[u] = e;
+        }
+      }
+      if (row >= 0 && c0 == 0) {
+        cbuf[rpos] = v[0];
+        if (row == 0) publish_pivot(0, v[0]);
+      }
+      __syncthreads();
+      // the warps that own segments step through the columns; bad_at only
+      // ever changes to j + 1 during step j, so every thread takes the same
+      // exit
+      const int nthr = (nact + 31) & ~31;
+      if (tid < nthr) {
+        for (int j = 0; j < m; ++j) {
+          if (bad_at <= j) break;
+          const double* col = cbuf + j * LDC;
+          if (row >= 0 && (row == KP || row > j) && c0 + SEGW - 1 > j) {
+            const double w = col[rpos] * qv[j];
+            // entries left of column j + 1, right of the row's last column,
+            // or past m are never read again: updating them unconditionally
+            // keeps the inner loop free of predicates
+#pragma unroll
+            for (int u = 0; u < SEGW; ++u) v[u] = fma(-w, col[cb0 + u], v[u]);
+            const int jn = j + 1;
+            if (jn < m && jn >= c0 && jn < c0 + SEGW && (row == KP || row >= jn)) {
+#pragma unroll
+              for (int u = 0; u < SEGW; ++u)
+                if (c0 + u == jn) {
+                  cbuf[jn * LDC + rpos] = v[u];
+                  if (row == jn) publish_pivot(jn, v[u]);
+                }
+            }
+          }
+          asm volatile("bar.sync 1, %0;" ::"r"(nthr) : "memory");
+        }
+      }
+      __syncthreads();
+      const bool chol_ok = bad_at > KP;
+      if (chol_ok) {
+        if (tid < 32 && m > 0) {  // L^T x = y, y_j = cbuf(KP, j) * s_j
+          double r[2], sl[2];
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            const int cc = lane + 32 * q;
+            sl[q] = cc < m ? sv[cc] : 0.0;
+            r[q] = cc < m ? cbuf[cc * LDC + KP + KP / 8] * sl[q] : 0.0;
+          }
+          for (int j = m - 1; j >= 0; --j) {
+            const double t = (j < 32 ? r[0] : r[1]) * sv[j];
+            const double xj = __shfl_sync(0xffffffffu, t, j & 31);
+            const int jpos = j + (j >> 3);
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+              const int cc = lane + 32 * q;
+              if (cc < j) r[q] = fma(-(cbuf[cc * LDC + jpos] * sl[q]), xj, r[q]);
+              else if (cc == j) r[q] = xj;
+            }
+          }
+#pragma unroll
+          for (int q = 0; q < 2; ++q) {
+            const int cc = lane + 32 * q;
+            if (cc < m) z[cc] = r[q];
+          }
+        }
+      } else {
+        // not positive definite: the general solver, as arma::solve falls back
+        __syncthreads();  // every thread has read the failing pivot before cbuf is reused
+        double* Ls = cbuf;
+        for (int e = tid; e < m * m; e += NT) {
+          const int ii = e % m, jj = e / m;
+          Ls[ii + LDC * jj] = AtA[idx[ii] + n * idx[jj]];
+        }
+        for (int i = tid; i < m; i += NT) z[i] = b[idx[i]];
+        __syncthreads();
+        if (tid < 32) {
+          const int rc = warp_lu_solve(Ls, LDC, m, z);
+          if (lane == 0) lu_rc = rc;
+        }
+        __syncthreads();
+        if (lu_rc != 0) return lu_rc;
+      }
+      __syncthreads();  // z complete
+      // Y = AtA*X - AtB over the passive columns (bppnnls.hpp:167-168), then
+      // the 1e-12 zeroing of X and Y (bppnnls.hpp:170-172)
+      int bad = 0;
+      for (int base = 0; base < n; base += NT / TPR) {
+        const int i = base + tid / TPR, part = tid % TPR;
+        double acc = 0.0;
+        if (i < n)
+          for (int q = part; q < m; q += TPR) acc = fma(AtA[i + n * idx[q]], z[q], acc);
+#pragma unroll
+        for (int off = TPR / 2; off > 0; off >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, off);
+        if (i < n && part == 0) {
+          const double yi = acc - b[i];
+          y[i] = (fabs(yi) < kEps12) ? 0.0 : yi;
+          const double xi =
+              ((passive >> i) & 1) ? z[__popcll(passive & ((1ull << i) - 1ull))] : 0.0;
+          if (!isfinite(xi) || !isfinite(yi)) bad = 1;
+          x[i] = (fabs(xi) < kEps12) ? 0.0 : xi;
+        }
+      }
+      return __syncthreads_or(bad) ? kStNonFinite : 0;
+    };
+    auto classify = [&](uint64_t& nonopt, uint64_t& infea) {
+      bool lo_no = has_lo && (y[lane] < 0) && !((passive >> lane) & 1);
+      bool hi_no = has_hi && (y[lane + 32] < 0) && !((passive >> (lane + 32)) & 1);
+      bool lo_in = has_lo && (x[lane] < 0) && ((passive >> lane) & 1);
+      bool hi_in = has_hi && (x[lane + 32] < 0) && ((passive >> (lane + 32)) & 1);
+      nonopt = warp_mask64(lo_no, hi_no);
+      infea = warp_mask64(lo_in, hi_in);
+    };
+
+    unsigned iter = 0;
+    int st = 0;
+    if (Pinit) {
+      // warm start from the previous solution's passive set (see k_bpp): a
+      // failed warm solve restarts from the reference's X = 0
+      const bool lo = has_lo && Pinit[c * n + lane] > 0.0;
+      const bool hi = has_hi && Pinit[c * n + lane + 32] > 0.0;
+      passive = warp_mask64(lo, hi);
+      if (passive) {
+        ++iter;
+        st = solve_passive();
+        if (st != 0) {
+          st = 0;
+          iter = 0;
+          passive = 0;
+          __syncthreads();
+          for (int i = tid; i < n; i += NT) {
+            x[i] = 0.0;
+            y[i] = -b[i];
+          }
+        }
+      }
+    }
+    __syncthreads();  // b, x, y visible to every warp
+    uint64_t nonopt = 0, infea = 0;
+    int notgood = 0;
+    if (st == 0) {
+      classify(nonopt, infea);
+      notgood = __popcll(nonopt) + __popcll(infea);
+    }
+    while (st == 0 && notgood > 0) {
+      ++iter;
+      if (iter > max_it) { st = kStBppMaxIter; break; }
+      if (notgood < Ninf) {  // Cols1, bppnnls.hpp:109, 115-129
+        P = pbar;
+        Ninf = notgood;
+        passive = (passive | nonopt) & ~infea;
+      } else if (P >= 1) {  // Cols2, bppnnls.hpp:110, 133-146
+        P -= 1;
+        passive = (passive | nonopt) & ~infea;
+      } else {  // backup rule, bppnnls.hpp:149-160
+        int rowidx = 63 - __clzll(nonopt | infea);
+        passive ^= (1ull << rowidx);
+      }
+      st = solve_passive();
+      if (st != 0) break;
+      classify(nonopt, infea);
+      notgood = __popcll(nonopt) + __popcll(infea);
+    }
+    for (int i = tid; i < n; i += NT) {
+      Xout[c * n + i] = x[i];
+      if (passive_out) passive_out[c * n + i] = (int)((passive >> i) & 1);
+    }
+    if (tid == 0) {
+      if (iters_out) iters_out[c] = (int)iter;
+      if (st != 0) atomicMin(status, st);
+    }
+  }
+}
+
 }  // namespace pg

@@ -25,20 +25,35 @@ namespace pg {
 // The products run on the FP64 tensor cores: warp-level
 // mma.sync.m8n8k4.f64 (the only FP64 MMA of sm_100a), each warp owning a
 // (128 / WARPS_M) x (KP / WARPS_N) block of the output as 8 x 8 accumulator
-// tiles. The next reduction tile is loaded into registers while the current
-// one is multiplied out of shared memory. Shared-memory layouts are chosen so
+// tiles (a warp whose rows all lie past M skips its products). The next
+// reduction tile is loaded into registers while the current one is
+// multiplied out of shared memory, then stored into the other of two
+// shared-memory stages: one CTA barrier per tile. Dynamic shared memory:
+// ct_smem_bytes<KP, LEFT>(). Shared-memory layouts are chosen so
 // that every fragment load is two 128-byte wavefronts (no bank conflicts):
-//   RIGHT: Xs[kk][m], row stride 128 + 8 doubles (X is m-contiguous);
+//   RIGHT: Xs[kk][m], row stride 128 + 4 doubles (X is m-contiguous);
 //   LEFT : Xs[m][kk], row stride BK + 4 doubles (X is kk-contiguous);
-//   both : Ws[kk][r], row stride KP + 8 (KP + 16 at KP = 8).
+//   both : Ws[kk][r], row stride KP + 4.
 // Fragment layouts of m8n8k4 (f64): A element (row g, col t), B element
 // (row t, col g), C elements (row g, cols 2t, 2t+1), g = lane / 4, t = lane % 4.
 // ---------------------------------------------------------------------------
 constexpr int CT_BM = 128;
 template <int KP>
 constexpr int ct_bk() { return KP == 64 ? 16 : 32; }
+// Row strides (in doubles) of the shared-memory tiles. A fragment load of
+// lane (g, t) = (lane / 4, lane % 4) reads word t * S + g (+ a constant);
+// a half warp (g < 4 or g >= 4) is one 128-byte wavefront when t * S mod 16
+// takes the values 0, 4, 8, 12, i.e. when S = 4 or 12 (mod 16) doubles.
 template <int KP>
-constexpr int ct_ws() { return KP % 16 == 0 ? KP + 8 : KP + 16; }
+constexpr int ct_ws() { return KP + 4; }
+constexpr int CT_SXR = CT_BM + 4;  // RIGHT: Xs[kk][m]
+// doubles of one shared-memory stage (X tile + W tile)
+template <int KP, bool LEFT>
+constexpr int ct_stage_elems() {
+  return (LEFT ? CT_BM * (ct_bk<KP>() + 4) : ct_bk<KP>() * CT_SXR) + ct_bk<KP>() * ct_ws<KP>();
+}
+template <int KP, bool LEFT>
+constexpr size_t ct_smem_bytes() { return 2 * sizeof(double) * (size_t)ct_stage_elems<KP, LEFT>(); }
 
 struct ContractGeom {
   int64_t M;        // output rows
@@ -57,7 +72,62 @@ __device__ __forceinline__ void dmma_m8n8k4(double (&c)[2], double a, double b) 
                : "d"(a), "d"(b));
 }
 
-template <int KP, bool LEFT>
+// W(row, r) of a Khatri-Rao generator with NF = 1, 2 or 3 factors, digits
+// in registers (NF = 0: any number of factors, wgen_eval). The product order
+// is wgen_eval's, F_0 * (F_1 * F_2). `row` must be below the product of the
+// dims (the caller checks its range).
+template <int NF>
+__device__ __forceinline__ double wgen_at(const WGen& wg, int64_t row, int r, int k) {
+  if constexpr (NF == 1) {
+    return wg.f[0][row * k + r];
+  } else if constexpr (NF == 2) {
+    const int64_t i1 = row / wg.dim[0], i0 = row - i1 * wg.dim[0];
+    return wg.f[0][i0 * k + r] * wg.f[1][i1 * k + r];
+  } else if constexpr (NF == 3) {
+    const int64_t q = row / wg.dim[0], i0 = row - q * wg.dim[0];
+    const int64_t i2 = q / wg.dim[1], i1 = q - i2 * wg.dim[1];
+    return wg.f[0][i0 * k + r] * (wg.f[1][i1 * k + r] * wg.f[2][i2 * k + r]);
+  } else {
+    return wgen_eval(wg, row, r, k);
+  }
+}
+// Division by a divisor fixed for the whole kernel (Granlund and Montgomery,
+// "Division by invariant integers using multiplication", PLDI 1994):
+// l = ceil(log2 d), m = floor(2^32 (2^l - d) / d) + 1, and for n < 2^31
+// n / d = (umulhi(n, m) + n) >> l (the sum stays below 2^32).
+struct FastDiv {
+  uint32_t d, m;
+  int l;
+};
+__device__ __forceinline__ FastDiv make_fastdiv(uint32_t d) {
+  int l = 0;
+  while (l < 31 && (1u << l) < d) ++l;
+  const uint64_t num = ((uint64_t)1 << 32) * (((uint64_t)1 << l) - d);
+  return FastDiv{d, (uint32_t)(num / d + 1), l};
+}
+__device__ __forceinline__ uint32_t fast_div(uint32_t n, const FastDiv& f) {
+  return (__umulhi(n, f.m) + n) >> f.l;
+}
+
+// W(row, r) as wgen_at with 32-bit digit arithmetic (the product of the dims
+// < 2^31) and the digit divisions by dims 0 and 1 precomputed
+template <int NF>
+__device__ __forceinline__ double wgen_at32(const WGen& wg, const FastDiv& f0, const FastDiv& f1,
+                                            uint32_t row, int r, int k) {
+  if constexpr (NF == 2) {
+    const uint32_t i1 = fast_div(row, f0), i0 = row - i1 * f0.d;
+    return wg.f[0][(int64_t)i0 * k + r] * wg.f[1][(int64_t)i1 * k + r];
+  } else if constexpr (NF == 3) {
+    const uint32_t q = fast_div(row, f0), i0 = row - q * f0.d;
+    const uint32_t i2 = fast_div(q, f1), i1 = q - i2 * f1.d;
+    return wg.f[0][(int64_t)i0 * k + r] *
+           (wg.f[1][(int64_t)i1 * k + r] * wg.f[2][(int64_t)i2 * k + r]);
+  } else {
+    return wgen_at<NF>(wg, (int64_t)row, r, k);
+  }
+}
+
+template <int KP, bool LEFT, int NF>
 __global__ void __launch_bounds__(256, 2) k_contract_f64(const double* __restrict__ X,
                                                          ContractGeom g, WGen wg, int k,
                                                          double* __restrict__ out) {
@@ -68,10 +138,11 @@ __global__ void __launch_bounds__(256, 2) k_contract_f64(const double* __restric
   constexpr int WARPS_N = 8 / WARPS_M;
   constexpr int MT = CT_BM / WARPS_M / 8;  // 8-row MMA tiles per warp
   constexpr int NT = KP / WARPS_N / 8;     // 8-rank MMA tiles per warp
-  constexpr int SX = LEFT ? BK + 4 : CT_BM + 8;
+  constexpr int SX = LEFT ? BK + 4 : CT_SXR;
   constexpr int SW = ct_ws<KP>();
-  __shared__ __align__(16) double Xs[LEFT ? CT_BM * SX : BK * SX];
-  __shared__ __align__(16) double Ws[BK * SW];
+  constexpr int XS_ELEMS = LEFT ? CT_BM * SX : BK * SX;
+  constexpr int STAGE = ct_stage_elems<KP, LEFT>();
+  extern __shared__ __align__(16) double ct_smem[];
   const int tid = threadIdx.x;
   const int lane = tid & 31, warp = tid >> 5;
   const int fg = lane >> 2, ft = lane & 3;
@@ -82,6 +153,14 @@ __global__ void __launch_bounds__(256, 2) k_contract_f64(const double* __restric
   int64_t t_end = t_begin + g.tiles_per_split;
   if (t_end > g.ktiles) t_end = g.ktiles;
   const int64_t tilesA = (g.A + BK - 1) / BK;
+  // Khatri-Rao row indices fit 32-bit digit arithmetic
+  const bool small_rows = (LEFT ? g.A * g.B : g.A) < ((int64_t)1 << 31);
+  FastDiv fd0{1, 1, 0}, fd1{1, 1, 0};
+  if (NF >= 2 && small_rows) {
+    fd0 = make_fastdiv((uint32_t)wg.dim[0]);
+    if (NF >= 3) fd1 = make_fastdiv((uint32_t)wg.dim[1]);
+  }
+  const bool warp_live = m0 + wm0 < g.M;  // warp-uniform
 
   double acc[MT][NT][2];
 #pragma unroll
@@ -95,34 +174,51 @@ __global__ void __launch_bounds__(256, 2) k_contract_f64(const double* __restric
   auto load_tile = [&](int64_t t) {
     if constexpr (!LEFT) {
       const int64_t j0 = t * BK;
-      const int mm = tid & 127;
-      const int64_t gm = m0 + mm;
+      const int64_t gm = m0 + (tid & 127);
+      const bool mrow = gm < g.M;
+      // rows kk = (tid >> 7) + 2 i of the tile through one running pointer
+      const int64_t jt = j0 + (tid >> 7);
+      const double* xp = X + gm + g.ldx * jt;
+      const int64_t xstep = 2 * g.ldx;
+      if (mrow && j0 + BK <= g.A) {
 #pragma unroll
-      for (int i = 0; i < XPT; ++i) {
-        int kk = (tid >> 7) + 2 * i;
-        int64_t gj = j0 + kk;
-        xr[i] = (gm < g.M && gj < g.A) ? X[gm + g.ldx * gj] : 0.0;
-      }
-      WIdx base;
-      if (wg.nf > 1) widx_init(wg, j0, base);
-#pragma unroll
-      for (int i = 0; i < WPT; ++i) {
-        int e = tid + 256 * i;
-        double v = 0.0;
-        if (e < BK * KP) {
-          int kk = e / KP, r = e % KP;
-          int64_t gj = j0 + kk;
-          if (r < k && gj < g.A) {
-            if (wg.nf == 1) {
-              v = wg.f[0][gj * k + r];
-            } else {
-              WIdx w = base;
-              widx_advance(wg, w, kk);
-              v = wgen_row(wg, w, r, k);
-            }
-          }
+        for (int i = 0; i < XPT; ++i) {
+          xr[i] = *xp;
+          xp += xstep;
         }
-        wr[i] = v;
+      } else {
+#pragma unroll
+        for (int i = 0; i < XPT; ++i) {
+          xr[i] = (mrow && jt + 2 * i < g.A) ? *xp : 0.0;
+          xp += xstep;
+        }
+      }
+      if constexpr (NF == 1) {
+        // 256 is a multiple of KP: entry i of this thread is (kk, r) =
+        // (tid / KP + (256 / KP) i, tid % KP)
+        const int r = tid % KP;
+        const int64_t jw = j0 + tid / KP;
+        const double* wp = wg.f[0] + jw * k + r;
+        const int64_t wstep = (int64_t)(256 / KP) * k;
+#pragma unroll
+        for (int i = 0; i < WPT; ++i) {
+          wr[i] = (r < k && jw + (256 / KP) * i < g.A) ? *wp : 0.0;
+          wp += wstep;
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < WPT; ++i) {
+          int e = tid + 256 * i;
+          double v = 0.0;
+          if (e < BK * KP) {
+            int kk = e / KP, r = e % KP;
+            int64_t gj = j0 + kk;
+            if (r < k && gj < g.A)
+              v = small_rows ? wgen_at32<NF>(wg, fd0, fd1, (uint32_t)gj, r, k)
+                             : wgen_at<NF>(wg, gj, r, k);
+          }
+          wr[i] = v;
+        }
       }
     } else {
       const int64_t b = t / tilesA;
@@ -135,8 +231,7 @@ __global__ void __launch_bounds__(256, 2) k_contract_f64(const double* __restric
         int64_t gm = m0 + mm;
         xr[i] = (gm < g.M && ga < g.A) ? X[ga + g.ldx * gm + g.ldb * b] : 0.0;
       }
-      WIdx base;
-      widx_init(wg, a0 + g.A * b, base);
+      const int64_t wrow0 = a0 + g.A * b;
 #pragma unroll
       for (int i = 0; i < WPT; ++i) {
         int e = tid + 256 * i;
@@ -144,17 +239,17 @@ __global__ void __launch_bounds__(256, 2) k_contract_f64(const double* __restric
         if (e < BK * KP) {
           int kk = e / KP, r = e % KP;
           int64_t gaa = a0 + kk;
-          if (r < k && gaa < g.A) {
-            WIdx w = base;
-            widx_advance(wg, w, kk);
-            v = wgen_row(wg, w, r, k);
-          }
+          if (r < k && gaa < g.A)
+            v = small_rows ? wgen_at32<NF>(wg, fd0, fd1, (uint32_t)(wrow0 + kk), r, k)
+                           : wgen_at<NF>(wg, wrow0 + kk, r, k);
         }
         wr[i] = v;
       }
     }
   };
-  auto store_tile = [&]() {
+  auto store_tile = [&](int stage) {
+    double* Xs = ct_smem + stage * STAGE;
+    double* Ws = Xs + XS_ELEMS;
     if constexpr (!LEFT) {
       const int mm = tid & 127;
 #pragma unroll
@@ -171,28 +266,36 @@ __global__ void __launch_bounds__(256, 2) k_contract_f64(const double* __restric
     }
   };
 
-  if (t_begin < t_end) load_tile(t_begin);
+  if (t_begin < t_end) {
+    load_tile(t_begin);
+    store_tile(0);
+  }
   for (int64_t t = t_begin; t < t_end; ++t) {
-    __syncthreads();
-    store_tile();
+    const int stage = (int)((t - t_begin) & 1);
+    // stage `stage` is complete and every warp is done with the other one
     __syncthreads();
     if (t + 1 < t_end) load_tile(t + 1);
+    if (warp_live) {
+      const double* Xs = ct_smem + stage * STAGE;
+      const double* Ws = Xs + XS_ELEMS;
 #pragma unroll
-    for (int s4 = 0; s4 < BK / 4; ++s4) {
-      const int kk = s4 * 4 + ft;
-      double af[MT], bf[NT];
+      for (int s4 = 0; s4 < BK / 4; ++s4) {
+        const int kk = s4 * 4 + ft;
+        double af[MT], bf[NT];
 #pragma unroll
-      for (int i = 0; i < MT; ++i) {
-        const int m = wm0 + i * 8 + fg;
-        af[i] = LEFT ? Xs[m * SX + kk] : Xs[kk * SX + m];
+        for (int i = 0; i < MT; ++i) {
+          const int m = wm0 + i * 8 + fg;
+          af[i] = LEFT ? Xs[m * SX + kk] : Xs[kk * SX + m];
+        }
+#pragma unroll
+        for (int j = 0; j < NT; ++j) bf[j] = Ws[kk * SW + wn0 + j * 8 + fg];
+#pragma unroll
+        for (int i = 0; i < MT; ++i)
+#pragma unroll
+          for (int j = 0; j < NT; ++j) dmma_m8n8k4(acc[i][j], af[i], bf[j]);
       }
-#pragma unroll
-      for (int j = 0; j < NT; ++j) bf[j] = Ws[kk * SW + wn0 + j * 8 + fg];
-#pragma unroll
-      for (int i = 0; i < MT; ++i)
-#pragma unroll
-        for (int j = 0; j < NT; ++j) dmma_m8n8k4(acc[i][j], af[i], bf[j]);
     }
+    if (t + 1 < t_end) store_tile(stage ^ 1);
   }
   double* o = out + (int64_t)blockIdx.y * g.split_stride;
 #pragma unroll

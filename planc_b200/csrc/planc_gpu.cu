@@ -198,6 +198,7 @@ struct planc_gpu_ctx {
   int64_t launch_count = 0;
   int bpp_max_iter = 0;  // 0: the reference's 5k cap
   bool bpp_warm = true;  // ANLS/BPP rows start from the replaced factor's passive set
+  int bpp_kernel = 0;    // 0: by size, 1: a warp per right-hand side, 2: a CTA per right-hand side
   // Fraction of the GPU one launch of this context aims to fill (split-K and
   // grid sizing). 1 for a context alone on the GPU; the batch autotuner lowers
   // it when many contexts run concurrently.
@@ -216,6 +217,43 @@ void set_device(planc_gpu_ctx* c) { CK(cudaSetDevice(c->device)); }
 int eff_sm(const planc_gpu_ctx* c) {
   int v = (int)(c->sm_count * c->par_scale);
   return v < 1 ? 1 : v;
+}
+
+// Batched BPP of ncols right-hand sides with the k x k matrix AtA (k_bpp: a
+// warp per right-hand side; k_bpp_cta: a CTA per right-hand side, for k > 16
+// while the right-hand sides are too few to give every SM several warps).
+// Launched on the context's stream; the caller times it.
+void launch_bpp(planc_gpu_ctx* c, const double* AtA, const double* B, int n, int64_t ncols,
+                double* X, int* P, int* I, const double* warm) {
+  if (ncols <= 0) return;
+  const int kp = kpad(n);
+  bool cta = kp >= 32 && ncols <= 4 * (int64_t)c->sm_count;
+  if (c->bpp_kernel == 1) cta = false;
+  if (c->bpp_kernel == 2) cta = kp >= 32;
+  if (cta) {
+    const unsigned grid = (unsigned)std::min<int64_t>(ncols, 2 * (int64_t)c->sm_count);
+    if (kp == 32) {
+      using C = BppCta<32, 8>;
+      k_bpp_cta<32, 8><<<grid, C::THREADS, C::SMEM, c->stream>>>(AtA, B, n, ncols, X, P, I, c->status_dev,
+                                                                c->bpp_max_iter, warm);
+    } else {
+      using C = BppCta<64, 8>;
+      k_bpp_cta<64, 8><<<grid, C::THREADS, C::SMEM, c->stream>>>(AtA, B, n, ncols, X, P, I, c->status_dev,
+                                                                c->bpp_max_iter, warm);
+    }
+    return;
+  }
+  const unsigned blocks = (unsigned)((ncols + BPP_WARPS - 1) / BPP_WARPS);
+  switch (kp) {
+#define CASE(KP)                                                                                    \
+  case KP:                                                                                          \
+    k_bpp<KP><<<blocks, 32 * BPP_WARPS, bpp_smem_bytes(KP), c->stream>>>(AtA, B, n, ncols, X, P, I, \
+                                                                         c->status_dev,             \
+                                                                         c->bpp_max_iter, warm);    \
+    break;
+    CASE(8) CASE(16) CASE(32) CASE(64)
+#undef CASE
+  }
 }
 
 template <typename T>
@@ -521,6 +559,47 @@ void ensure_buffers_impl(planc_gpu_ctx* c) {
   }
 }
 
+// k_contract_f64 specialised on the Khatri-Rao factor count (1, 2, 3; any
+// other count takes the generic generator)
+template <int KP, bool LEFT>
+void launch_contract_f64(dim3 grid, cudaStream_t st, const double* X, const ContractGeom& g,
+                         const WGen& wg, int k, double* dst) {
+  constexpr size_t sm = ct_smem_bytes<KP, LEFT>();
+  switch (wg.nf) {
+    case 1: k_contract_f64<KP, LEFT, 1><<<grid, 256, sm, st>>>(X, g, wg, k, dst); break;
+    case 2: k_contract_f64<KP, LEFT, 2><<<grid, 256, sm, st>>>(X, g, wg, k, dst); break;
+    case 3: k_contract_f64<KP, LEFT, 3><<<grid, 256, sm, st>>>(X, g, wg, k, dst); break;
+    default: k_contract_f64<KP, LEFT, 0><<<grid, 256, sm, st>>>(X, g, wg, k, dst); break;
+  }
+}
+
+template <int KP, bool LEFT>
+void contract_f64_attrs_kp() {
+  constexpr int sm = (int)ct_smem_bytes<KP, LEFT>();
+  CK(cudaFuncSetAttribute(k_contract_f64<KP, LEFT, 0>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  CK(cudaFuncSetAttribute(k_contract_f64<KP, LEFT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  CK(cudaFuncSetAttribute(k_contract_f64<KP, LEFT, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  CK(cudaFuncSetAttribute(k_contract_f64<KP, LEFT, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+}
+
+// Dynamic shared-memory limits of every k_contract_f64 instance (up to 92 KB)
+// on device dev, set once per device before its first launch.
+std::mutex g_contract_attr_mutex;
+bool g_contract_attr_set[64] = {false};
+void contract_f64_attrs(int dev) {
+  std::lock_guard<std::mutex> lock(g_contract_attr_mutex);
+  if (dev < 0 || dev >= 64 || g_contract_attr_set[dev]) return;
+  contract_f64_attrs_kp<8, false>();
+  contract_f64_attrs_kp<8, true>();
+  contract_f64_attrs_kp<16, false>();
+  contract_f64_attrs_kp<16, true>();
+  contract_f64_attrs_kp<32, false>();
+  contract_f64_attrs_kp<32, true>();
+  contract_f64_attrs_kp<64, false>();
+  contract_f64_attrs_kp<64, true>();
+  g_contract_attr_set[dev] = true;
+}
+
 void run_contract(planc_gpu_ctx* c, const ContractPlan& p, bool left, const double* X,
                   const WGen& wg, double* out) {
   const int k = c->k;
@@ -532,9 +611,9 @@ void run_contract(planc_gpu_ctx* c, const ContractPlan& p, bool left, const doub
 #define CASE(KP)                                                                      \
   case KP:                                                                            \
     if (left)                                                                         \
-      k_contract_f64<KP, true><<<p.grid, 256, 0, c->stream>>>(X, p.g, wg, k, dst);    \
+      launch_contract_f64<KP, true>(p.grid, c->stream, X, p.g, wg, k, dst);           \
     else                                                                              \
-      k_contract_f64<KP, false><<<p.grid, 256, 0, c->stream>>>(X, p.g, wg, k, dst);   \
+      launch_contract_f64<KP, false>(p.grid, c->stream, X, p.g, wg, k, dst);          \
     break;
       CASE(8) CASE(16) CASE(32) CASE(64)
 #undef CASE
@@ -900,18 +979,8 @@ void run_update(planc_gpu_ctx* c, int algo, int n) {
   } else if (algo == PLANC_GPU_ANLSBPP) {
     // NTFANLSBPP::update (ntf/ntfanlsbpp.hpp:15-57): all I_n right-hand sides
     // in one launch; the 2000-column chunking does not change values.
-    unsigned blocks = (unsigned)((I + BPP_WARPS - 1) / BPP_WARPS);
     launch(c, KC_BPP, [&] {
-      switch (kpad(k)) {
-#define CASE(KP)                                                                                   \
-  case KP:                                                                                         \
-    k_bpp<KP><<<blocks, 32 * BPP_WARPS, bpp_smem_bytes(KP), c->stream>>>(                      \
-        c->Gloo, c->M[n], k, I, c->F[n], nullptr, nullptr, c->status_dev, c->bpp_max_iter,         \
-        c->bpp_warm ? c->F[n] : nullptr);                                                          \
-    break;
-        CASE(8) CASE(16) CASE(32) CASE(64)
-#undef CASE
-      }
+      launch_bpp(c, c->Gloo, c->M[n], k, I, c->F[n], nullptr, nullptr, c->bpp_warm ? c->F[n] : nullptr);
     });
   } else if (algo == PLANC_GPU_AOADMM) {
     if (!c->admm_ready) fail(PLANC_GPU_ERR_STATE, "internal: AO-ADMM state not allocated");
@@ -1356,6 +1425,11 @@ int planc_gpu_create(planc_gpu_ctx** out, int device, int precision, void* cuda_
                                 (int)bpp_smem_bytes(64)));
         CK(cudaFuncSetAttribute(k_bpp<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)bpp_smem_bytes(32)));
+        contract_f64_attrs(device);
+        CK(cudaFuncSetAttribute(k_bpp_cta<64, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)BppCta<64, 8>::SMEM));
+        CK(cudaFuncSetAttribute(k_bpp_cta<32, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)BppCta<32, 8>::SMEM));
         // the opt-in limit covers static and dynamic shared memory together
         CK(cudaFuncSetAttribute(k_nmf_hals_w_coop<32>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)nmfc_smem_limit(prop.sharedMemPerBlockOptin)));
@@ -1375,6 +1449,12 @@ int planc_gpu_create(planc_gpu_ctx** out, int device, int precision, void* cuda_
     if (const char* e = getenv("PLANC_GPU_NES_MAX_STEPS")) {
       const int v = atoi(e);
       if (v >= 1 && v <= NES_MAX_STEPS) c->nes_max_steps = v;
+    }
+    // PLANC_GPU_BPP_KERNEL=warp|cta fixes the batched BPP kernel for contexts
+    // created while it is set (default: chosen by the number of right-hand sides)
+    if (const char* e = getenv("PLANC_GPU_BPP_KERNEL")) {
+      if (!strcmp(e, "warp")) c->bpp_kernel = 1;
+      if (!strcmp(e, "cta")) c->bpp_kernel = 2;
     }
     c->coop_launch = prop.cooperativeLaunch != 0;
     if (cuda_stream) {
@@ -1810,18 +1890,7 @@ int planc_gpu_bpp_solve(planc_gpu_ctx* c, const double* AtA, const double* AtB, 
       CK(cudaMalloc(&dI, (size_t)ncols * 4));
       CK(cudaMemcpyAsync(dA, AtA, (size_t)n * n * 8, cudaMemcpyHostToDevice, c->stream));
       CK(cudaMemcpyAsync(dB, AtB, (size_t)n * ncols * 8, cudaMemcpyHostToDevice, c->stream));
-      unsigned blocks = (unsigned)((ncols + BPP_WARPS - 1) / BPP_WARPS);
-      launch(c, KC_BPP, [&] {
-        switch (kpad(n)) {
-#define CASE(KP)                                                                            \
-  case KP:                                                                                  \
-    k_bpp<KP><<<blocks, 32 * BPP_WARPS, bpp_smem_bytes(KP), c->stream>>>(                    \
-        dA, dB, n, ncols, dX, dP, dI, c->status_dev, c->bpp_max_iter, nullptr);                  \
-    break;
-          CASE(8) CASE(16) CASE(32) CASE(64)
-#undef CASE
-        }
-      });
+      launch(c, KC_BPP, [&] { launch_bpp(c, dA, dB, n, ncols, dX, dP, dI, nullptr); });
       CK(cudaMemcpyAsync(X, dX, (size_t)n * ncols * 8, cudaMemcpyDeviceToHost, c->stream));
       if (passive)
         CK(cudaMemcpyAsync(passive, dP, (size_t)n * ncols * 4, cudaMemcpyDeviceToHost, c->stream));
@@ -1863,18 +1932,8 @@ int planc_gpu_update_device(planc_gpu_ctx* c, int algo, double* H, const double*
       });
       return;
     }
-    const unsigned bb = (unsigned)((rows + BPP_WARPS - 1) / BPP_WARPS);
     launch(c, KC_BPP, [&] {
-      switch (kpad(k)) {
-#define CASE(KP)                                                                          \
-  case KP:                                                                                \
-    k_bpp<KP><<<bb, 32 * BPP_WARPS, bpp_smem_bytes(KP), c->stream>>>(                  \
-        G, M, k, rows, H, nullptr, nullptr, c->status_dev, c->bpp_max_iter,               \
-        c->bpp_warm ? H : nullptr);                                                       \
-    break;
-        CASE(8) CASE(16) CASE(32) CASE(64)
-#undef CASE
-      }
+      launch_bpp(c, G, M, k, rows, H, nullptr, nullptr, c->bpp_warm ? H : nullptr);
     });
   });
 }
@@ -2580,6 +2639,7 @@ extern "C" int planc_gpu_mttkrp_last_mode_noalloc(const double* X_dev, const int
     CK(cudaGetDevice(&dev));
     if (dev < 0 || dev >= kNoAllocMaxDevices) fail(PLANC_GPU_ERR_UNSUPPORTED, "device index too large");
     double* scratch = noalloc_scratch(dev);
+    contract_f64_attrs(dev);
     int sms = 148;
     CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
     // Khatri-Rao operand over modes 0..N-2, lowest mode fastest
@@ -2616,10 +2676,10 @@ extern "C" int planc_gpu_mttkrp_last_mode_noalloc(const double* X_dev, const int
     // every split writes its whole R x k partial (zeros when it has no tiles),
     // so nothing left in the scratch by an earlier call is read
     switch (kpad(k)) {
-      case 8: k_contract_f64<8, true><<<grid, 256, 0, st>>>(X_dev, g, wg, k, scratch); break;
-      case 16: k_contract_f64<16, true><<<grid, 256, 0, st>>>(X_dev, g, wg, k, scratch); break;
-      case 32: k_contract_f64<32, true><<<grid, 256, 0, st>>>(X_dev, g, wg, k, scratch); break;
-      default: k_contract_f64<64, true><<<grid, 256, 0, st>>>(X_dev, g, wg, k, scratch); break;
+      case 8: launch_contract_f64<8, true>(grid, st, X_dev, g, wg, k, scratch); break;
+      case 16: launch_contract_f64<16, true>(grid, st, X_dev, g, wg, k, scratch); break;
+      case 32: launch_contract_f64<32, true>(grid, st, X_dev, g, wg, k, scratch); break;
+      default: launch_contract_f64<64, true>(grid, st, X_dev, g, wg, k, scratch); break;
     }
     CK(cudaGetLastError());
     const int64_t n = R * k;
@@ -2746,18 +2806,8 @@ void nmf_row_update(planc_gpu_ctx* c, int algo, double* U, const double* M, int6
       }
     });
   } else {
-    const unsigned blocks = (unsigned)((I + BPP_WARPS - 1) / BPP_WARPS);
     launch(c, KC_BPP, [&] {
-      switch (kpad(k)) {
-#define CASE(KP)                                                                               \
-  case KP:                                                                                     \
-    k_bpp<KP><<<blocks, 32 * BPP_WARPS, bpp_smem_bytes(KP), c->stream>>>(                      \
-        c->nmf_G, M, k, I, U, nullptr, nullptr, c->status_dev, c->bpp_max_iter,                \
-        c->bpp_warm ? U : nullptr);                                                            \
-    break;
-        CASE(8) CASE(16) CASE(32) CASE(64)
-#undef CASE
-      }
+      launch_bpp(c, c->nmf_G, M, k, I, U, nullptr, nullptr, c->bpp_warm ? U : nullptr);
     });
   }
 }

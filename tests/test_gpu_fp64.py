@@ -111,8 +111,16 @@ def test_host_update_extension_point(gpu, oracle_lib):
     assert abs(err - eo[-1]) / eo[-1] < TOL
 
 
+# the batched BPP kernels: a warp per right-hand side, a CTA per right-hand
+# side (k > 16), and the library's choice by size
+BPP_KERNELS = ["warp", "cta", None]
+
+
+@pytest.mark.parametrize("kern", BPP_KERNELS)
 @pytest.mark.parametrize("n", [3, 8, 17, 40, 64])
-def test_bpp_solve_masks_and_values(gpu, oracle_lib, n):
+def test_bpp_solve_masks_and_values(gpu, oracle_lib, n, kern, monkeypatch):
+    if kern:
+        monkeypatch.setenv("PLANC_GPU_BPP_KERNEL", kern)
     rng = np.random.default_rng(100 + n)
     A = rng.random((2 * n, n))
     A[:, rng.random(n) < 0.3] *= 0.1
@@ -124,6 +132,27 @@ def test_bpp_solve_masks_and_values(gpu, oracle_lib, n):
     assert rel(Xg.T, Xo) < 1e-9
     assert np.array_equal(Pg.T, Po)
     assert itg.max() <= 5 * n
+
+
+@pytest.mark.parametrize("kern", ["warp", "cta"])
+def test_bpp_kernels_ntf_match_oracle(gpu, oracle_lib, kern, monkeypatch):
+    # rank 36 (the CTA kernel's 64-column instance) with warm starts from the
+    # second iteration on, against the oracle's cold-start run
+    monkeypatch.setenv("PLANC_GPU_BPP_KERNEL", kern)
+    dims, k, iters = (60, 50, 45), 36, 6
+    rng = np.random.default_rng(81)
+    A = [rng.random((d, k)) * (rng.random((d, k)) < 0.6) for d in dims]
+    X = np.einsum("az,bz,cz->abc", *A)
+    X = np.asfortranarray(np.maximum(X + 0.01 * X.std() * rng.standard_normal(dims), 0.0))
+    F0 = init_factors(dims, k, seed=82)
+    with gpu.Context(0, "fp64") as c:
+        c.set_tensor(X)
+        c.set_factors(F0)
+        e = c.run("anlsbpp", iters)
+        F, lam = c.get_factors()
+    Fo, lo, eo = oracle_lib.ntf_run(X, F0, "anlsbpp", iters)
+    assert all(rel(a, b) < 1e-10 for a, b in zip(F, Fo))
+    assert np.max(np.abs(e - eo) / eo) < 1e-10
 
 
 def test_bpp_warm_start_reaches_the_same_factors(gpu, oracle_lib):
@@ -152,11 +181,13 @@ def test_bpp_warm_start_reaches_the_same_factors(gpu, oracle_lib):
         assert np.max(np.abs(e - eo) / eo) < 1e-10, warm
 
 
-def test_bpp_singular_normal_equations_reports_status(gpu):
+@pytest.mark.parametrize("n,kern", [(4, None), (40, "warp"), (40, "cta")])
+def test_bpp_singular_normal_equations_reports_status(gpu, n, kern, monkeypatch):
     # AtA with a zero row/column at an index that enters the passive set:
     # the solve has no pivot; the call returns ERR_SINGULAR and the context
     # stays usable.
-    n = 4
+    if kern:
+        monkeypatch.setenv("PLANC_GPU_BPP_KERNEL", kern)
     AtA = np.eye(n)
     AtA[2, 2] = 0.0
     B = np.ones((n, 3))
