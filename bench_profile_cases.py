@@ -19,7 +19,7 @@ larger than the 126 MB L2 (DRAM counters stay meaningful):
   cfg3it  three ANLS/BPP iterations of the 192^4 rank-64 workload (BF16), for
           a one-pass launch list at full size
   cfg4it  the 256-tensor batched HALS workload (dims U{32..256}, ranks
-          U{4,8,16,32}, BF16 copies), three batched iterations, no autotuning
+          U{4,8,16,32}, BF16 copies), 3 + 3 batched iterations, no autotuning
   nmf     shared-memory NMF of a dense 16384 x 16384 FP32 matrix (BF16 copy),
           rank 32: three iterations each of MU, HALS and ANLS/BPP
   upd     AO-ADMM and Nesterov NTF updates on the 1024^3 rank-32 headline
@@ -223,13 +223,13 @@ def case_cfg4it(gpu, torch):
         gpu.synth_cp_tensor(0, X.data_ptr(), "f32", dims, A, sigma, 2000 + i, clip=True)
         b.add(X.data_ptr(), [r.random((d, k)) for d in dims], dims=dims, dtype="f32")
         del X
-    b.run("hals", 1, compute_error=True)
+    b.run("hals", 3, compute_error=True)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    b.run("hals", 2, compute_error=True)
+    b.run("hals", 3, compute_error=True)
     torch.cuda.synchronize()
-    print("cfg4it: 256 tensors, HALS: %.3f ms per batched iteration (2 iterations, untuned)"
-          % ((time.perf_counter() - t0) * 500))
+    print("cfg4it: 256 tensors, HALS: %.3f ms per batched iteration (3 iterations, untuned)"
+          % ((time.perf_counter() - t0) * 1e3 / 3))
     b.close()
 
 

@@ -249,9 +249,16 @@ int planc_gpu_batch_set_factors(planc_gpu_batch* b, int index, const double* con
  * count x iters relative errors, member-major. */
 int planc_gpu_batch_run(planc_gpu_batch* b, int algo, int iters, int compute_error, double* errs);
 int planc_gpu_batch_get_factors(planc_gpu_batch* b, int index, double* const* F, double* lambda);
-/* Times the batch graph under candidate per-launch parallelism settings per
- * member size class and keeps the fastest; members' factors are unchanged.
- * best_ms (may be NULL) receives the tuned time of one batched iteration. */
+/* Times the batch graph under candidate settings per member size class and
+ * keeps the fastest: the per-launch parallelism (fraction of the SMs a
+ * member's launch is sized for) and, for the tensor-core precisions, the
+ * split-K length of the left contraction (fewest 64-element chunks per
+ * partial: 0, 8, 32 or 128). Members' factors are unchanged; a tensor-core
+ * batch's later results may differ from the untuned ones by the rounding of
+ * the reordered FP32 partial sums. best_ms (may be NULL) receives the tuned
+ * time of one batched iteration. A batch whose members are all 3-way
+ * tensor-core contexts running MU or HALS runs each phase of an iteration as
+ * one launch for all members (PLANC_GPU_BATCH_GROUPED=0 turns that off). */
 int planc_gpu_batch_autotune(planc_gpu_batch* b, int algo, int trials, double* best_ms);
 int planc_gpu_batch_destroy(planc_gpu_batch* b);
 

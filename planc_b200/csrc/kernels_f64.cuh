@@ -315,12 +315,13 @@ __global__ void __launch_bounds__(256, 2) k_contract_f64(const double* __restric
 // lanes per output each sum the splits s = lane8, lane8 + 8, ... and a fixed
 // shuffle tree adds the eight (deterministic run to run; eight times the
 // loads in flight of a thread-per-output loop).
-__global__ void k_reduce_splits(const double* __restrict__ part, int nsplit, int64_t stride,
-                                int64_t n, double* __restrict__ out) {
+__device__ __forceinline__ void reduce_splits_body(const double* __restrict__ part, int nsplit,
+                                                   int64_t stride, int64_t n,
+                                                   double* __restrict__ out, int64_t bx, int64_t gx) {
   const int sub = threadIdx.x & 7;
-  const int64_t step = ((int64_t)gridDim.x * blockDim.x) >> 3;
+  const int64_t step = (gx * blockDim.x) >> 3;
   // every lane of a warp runs the same number of iterations (shuffles below)
-  const int64_t base = (((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) << 2;
+  const int64_t base = ((bx * blockDim.x + threadIdx.x) >> 5) << 2;
   for (int64_t i0 = base; i0 < n; i0 += step) {
     const int64_t i = i0 + ((threadIdx.x >> 3) & 3);
     double s = 0.0;
@@ -342,6 +343,10 @@ __global__ void k_reduce_splits(const double* __restrict__ part, int nsplit, int
     if (sub == 0 && i < n) out[i] = s;
   }
 }
+__global__ void k_reduce_splits(const double* __restrict__ part, int nsplit, int64_t stride,
+                                int64_t n, double* __restrict__ out) {
+  reduce_splits_body(part, nsplit, stride, n, out, blockIdx.x, gridDim.x);
+}
 
 // Grid of k_reduce_splits for n outputs (256-thread blocks, 8 lanes each).
 inline unsigned reduce_grid(int64_t n) {
@@ -353,15 +358,32 @@ inline unsigned reduce_grid(int64_t n) {
 // warp, adding the partials with the same pairwise tree the eight lanes of
 // k_reduce_splits form ((p0 + p1) + (p2 + p3)) + ((p4 + p5) + (p6 + p7)),
 // absent partials reading as 0, so both kernels give the same bits.
-__global__ void __launch_bounds__(256) k_reduce_splits_few(const double* __restrict__ part,
-                                                           int nsplit, int64_t stride, int64_t n,
-                                                           double* __restrict__ out) {
-  for (int64_t i = (int64_t)blockIdx.x * 256 + threadIdx.x; i < n; i += (int64_t)gridDim.x * 256) {
+__device__ __forceinline__ void reduce_splits_few_body(const double* __restrict__ part, int nsplit,
+                                                       int64_t stride, int64_t n,
+                                                       double* __restrict__ out, int64_t bx,
+                                                       int64_t gx) {
+  for (int64_t i = bx * 256 + threadIdx.x; i < n; i += gx * 256) {
     double v[8];
 #pragma unroll
     for (int p = 0; p < 8; ++p) v[p] = p < nsplit ? part[p * stride + i] : 0.0;
     out[i] = ((v[0] + v[1]) + (v[2] + v[3])) + ((v[4] + v[5]) + (v[6] + v[7]));
   }
+}
+__global__ void __launch_bounds__(256) k_reduce_splits_few(const double* __restrict__ part,
+                                                           int nsplit, int64_t stride, int64_t n,
+                                                           double* __restrict__ out) {
+  reduce_splits_few_body(part, nsplit, stride, n, out, blockIdx.x, gridDim.x);
+}
+
+// Grid of the split-K sum for n outputs of nsplit partials (the launch
+// reduce_splits makes): 0 selects k_reduce_splits_few, 1 k_reduce_splits.
+inline int reduce_kind(int nsplit) { return nsplit <= 8 ? 0 : 1; }
+inline unsigned reduce_blocks(int nsplit, int64_t n) {
+  if (nsplit <= 8) {
+    const int64_t b = (n + 255) / 256;
+    return (unsigned)(b < 1 ? 1 : (b > 4096 ? 4096 : b));
+  }
+  return reduce_grid(n);
 }
 
 // out[i] = sum over the nsplit partials part[p * stride + i], i < n.
@@ -382,15 +404,17 @@ inline void reduce_splits(cudaStream_t st, const double* part, int nsplit, int64
 //   left : out[b, r] = sum_a T[(a + A*b)*k + r] * F[a*k + r]
 //   right: out[a, r] = sum_b T[(a + A*b)*k + r] * W(b, r)
 // ---------------------------------------------------------------------------
+// (kernel bodies take the CTA's index and the grid size as arguments, so that
+// the grouped launches of a batch run every member through the same code)
 template <typename TT>
-__global__ void __launch_bounds__(256) k_ttv_left(const TT* __restrict__ T, int64_t A, int64_t B,
-                                                  int k, const double* __restrict__ F,
-                                                  double* __restrict__ out) {
+__device__ __forceinline__ void ttv_left_body(const TT* __restrict__ T, int64_t A, int64_t B, int k,
+                                              const double* __restrict__ F, double* __restrict__ out,
+                                              int64_t bx, int64_t gx) {
   __shared__ double red[256];
   const int lanes = 256 / k;
   const int tid = threadIdx.x;
   const int r = tid % k, lane = tid / k;
-  for (int64_t b = blockIdx.x; b < B; b += gridDim.x) {
+  for (int64_t b = bx; b < B; b += gx) {
     double s = 0.0;
     if (lane < lanes) {
       const TT* Tb = T + (A * b) * k + r;
@@ -418,6 +442,12 @@ __global__ void __launch_bounds__(256) k_ttv_left(const TT* __restrict__ T, int6
     __syncthreads();
   }
 }
+template <typename TT>
+__global__ void __launch_bounds__(256) k_ttv_left(const TT* __restrict__ T, int64_t A, int64_t B,
+                                                  int k, const double* __restrict__ F,
+                                                  double* __restrict__ out) {
+  ttv_left_body<TT>(T, A, B, k, F, out, blockIdx.x, gridDim.x);
+}
 
 // k_ttv_left for an FP32 T with k a multiple of 4: a CTA takes TTVL_NB
 // consecutive b at once, so each F row it loads serves TTVL_NB rows of T. A
@@ -426,10 +456,9 @@ __global__ void __launch_bounds__(256) k_ttv_left(const TT* __restrict__ T, int6
 // the CTA adds its RL row lanes in order through shared memory. Four CTAs
 // an SM (64 registers a thread): the loop is bound by loads in flight.
 constexpr int TTVL_NB = 2;
-__global__ void __launch_bounds__(256, 4) k_ttv_left_f4(const float* __restrict__ T, int64_t A,
-                                                        int64_t B, int k,
-                                                        const double* __restrict__ F,
-                                                        double* __restrict__ out) {
+__device__ __forceinline__ void ttv_left_f4_body(const float* __restrict__ T, int64_t A, int64_t B,
+                                                 int k, const double* __restrict__ F,
+                                                 double* __restrict__ out, int64_t bx) {
   __shared__ double red[256 * TTVL_NB * 4];
   const int q = k >> 2;                  // float4 per row
   const int tpr = q <= 8 ? 8 : 16;       // threads per row
@@ -437,7 +466,7 @@ __global__ void __launch_bounds__(256, 4) k_ttv_left_f4(const float* __restrict_
   const int tid = threadIdx.x;
   const int r4 = tid % tpr, rl = tid / tpr;
   const bool active = r4 < q;
-  const int64_t b0 = (int64_t)blockIdx.x * TTVL_NB;
+  const int64_t b0 = bx * TTVL_NB;
   const int nb = (int)((B - b0) < TTVL_NB ? (B - b0) : TTVL_NB);
   double acc[TTVL_NB][4];
 #pragma unroll
@@ -475,6 +504,12 @@ __global__ void __launch_bounds__(256, 4) k_ttv_left_f4(const float* __restrict_
     for (int l = 0; l < RL; ++l) t += red[l * (TTVL_NB * k) + e];
     out[b0 * k + e] = t;
   }
+}
+__global__ void __launch_bounds__(256, 4) k_ttv_left_f4(const float* __restrict__ T, int64_t A,
+                                                        int64_t B, int k,
+                                                        const double* __restrict__ F,
+                                                        double* __restrict__ out) {
+  ttv_left_f4_body(T, A, B, k, F, out, blockIdx.x);
 }
 
 template <typename TT>
@@ -525,10 +560,10 @@ __global__ void __launch_bounds__(256) k_ttv_right(const TT* __restrict__ T, int
 // and 16 rows. W(b, r) comes from the row digits of b, advanced per step.
 // Writes one partial (A x k) per b-range; k_reduce_splits sums them.
 template <typename TT, int KP>
-__global__ void __launch_bounds__(256) k_ttv_right_tiled(const TT* __restrict__ T, int64_t A,
-                                                         int64_t B, int k, WGen wg,
-                                                         int64_t b_per_split,
-                                                         double* __restrict__ out) {
+__device__ __forceinline__ void ttv_right_tiled_body(const TT* __restrict__ T, int64_t A, int64_t B,
+                                                     int k, const WGen& wg, int64_t b_per_split,
+                                                     double* __restrict__ out, int64_t bx,
+                                                     int64_t by) {
   constexpr int J = 16;
   constexpr int AT = J * 256 / KP;
   constexpr int BC = 32;  // b values per shared-memory W chunk
@@ -536,8 +571,8 @@ __global__ void __launch_bounds__(256) k_ttv_right_tiled(const TT* __restrict__ 
   const int tid = threadIdx.x;
   const int r = tid % KP;
   const int arow = tid / KP;  // 0 .. 256/KP - 1
-  const int64_t a0 = (int64_t)blockIdx.x * AT;
-  const int64_t b0 = (int64_t)blockIdx.y * b_per_split;
+  const int64_t a0 = bx * AT;
+  const int64_t b0 = by * b_per_split;
   int64_t b1 = b0 + b_per_split;
   if (b1 > B) b1 = B;
   double acc[J];
@@ -582,12 +617,19 @@ __global__ void __launch_bounds__(256) k_ttv_right_tiled(const TT* __restrict__ 
     }
   }
   if (!rok) return;
-  double* o = out + (int64_t)blockIdx.y * A * k;
+  double* o = out + by * A * k;
 #pragma unroll
   for (int j = 0; j < J; ++j) {
     const int64_t a = a0 + arow + (int64_t)(256 / KP) * j;
     if (a < A) o[a * k + r] = acc[j];
   }
+}
+template <typename TT, int KP>
+__global__ void __launch_bounds__(256) k_ttv_right_tiled(const TT* __restrict__ T, int64_t A,
+                                                         int64_t B, int k, WGen wg,
+                                                         int64_t b_per_split,
+                                                         double* __restrict__ out) {
+  ttv_right_tiled_body<TT, KP>(T, A, B, k, wg, b_per_split, out, blockIdx.x, blockIdx.y);
 }
 
 // ---------------------------------------------------------------------------
@@ -665,14 +707,15 @@ __global__ void __launch_bounds__(128) k_mu_rows(double* __restrict__ H, const d
 // by delta, g += delta * G(i,:), so g(i) always equals the reference's
 // H(row,:) * G(:,i) with columns < i already replaced (ntf/ntfhals.hpp:17-18).
 template <int KP>
-__global__ void __launch_bounds__(256) k_hals_warp(double* __restrict__ H, const double* __restrict__ M,
-                                                   const double* __restrict__ G, int64_t I, int k) {
+__device__ __forceinline__ void hals_warp_body(double* __restrict__ H, const double* __restrict__ M,
+                                               const double* __restrict__ G, int64_t I, int k,
+                                               int64_t bx) {
   constexpr int PER = KP / 32;
   __shared__ double Gs[KP * KP];
   for (int e = threadIdx.x; e < k * k; e += blockDim.x) Gs[e] = G[e];
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int64_t row = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int64_t row = bx * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (row >= I) return;
   double h[PER], m[PER], g[PER];
 #pragma unroll
@@ -717,19 +760,24 @@ __global__ void __launch_bounds__(256) k_hals_warp(double* __restrict__ H, const
     if (c < k) H[row * k + c] = h[p];
   }
 }
+template <int KP>
+__global__ void __launch_bounds__(256) k_hals_warp(double* __restrict__ H, const double* __restrict__ M,
+                                                   const double* __restrict__ G, int64_t I, int k) {
+  hals_warp_body<KP>(H, M, G, I, k, blockIdx.x);
+}
 
 // MU: H = (H .* M) ./ (H G + eps); eps is 1e-6 for NTF (ntf/ntfmu.hpp:14) and
 // 1e-17 for NMF (nmf/mu.hpp:68, 80).
 template <int KP>
-__global__ void __launch_bounds__(256) k_mu_warp(double* __restrict__ H, const double* __restrict__ M,
-                                                 const double* __restrict__ G, int64_t I, int k,
-                                                 double eps) {
+__device__ __forceinline__ void mu_warp_body(double* __restrict__ H, const double* __restrict__ M,
+                                             const double* __restrict__ G, int64_t I, int k,
+                                             double eps, int64_t bx) {
   constexpr int PER = KP / 32;
   __shared__ double Gs[KP * KP];
   for (int e = threadIdx.x; e < k * k; e += blockDim.x) Gs[e] = G[e];
   __syncthreads();
   const int lane = threadIdx.x & 31;
-  const int64_t row = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int64_t row = bx * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (row >= I) return;
   double h[PER], t[PER];
 #pragma unroll
@@ -752,6 +800,12 @@ __global__ void __launch_bounds__(256) k_mu_warp(double* __restrict__ H, const d
     const int c = lane + 32 * p;
     if (c < k) H[row * k + c] = (h[p] * M[row * k + c]) / (t[p] + eps);
   }
+}
+template <int KP>
+__global__ void __launch_bounds__(256) k_mu_warp(double* __restrict__ H, const double* __restrict__ M,
+                                                 const double* __restrict__ G, int64_t I, int k,
+                                                 double eps) {
+  mu_warp_body<KP>(H, M, G, I, k, eps, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -1019,12 +1073,12 @@ __global__ void k_gram_loo(const double* __restrict__ Gall, int N, int k, int n,
 // Writes errs[*counter] and increments *counter (so one captured graph can be
 // replayed across iterations). One CTA of 256 threads.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(1024) k_error(const double* __restrict__ Mlast,
-                                                const double* __restrict__ Flast, int64_t I,
-                                                const double* __restrict__ lambda,
-                                                const double* __restrict__ Gall, int N, int k,
-                                                const double* __restrict__ normX2,
-                                                double* __restrict__ errs, int* __restrict__ counter) {
+__device__ __forceinline__ void error_body(const double* __restrict__ Mlast,
+                                           const double* __restrict__ Flast, int64_t I,
+                                           const double* __restrict__ lambda,
+                                           const double* __restrict__ Gall, int N, int k,
+                                           const double* __restrict__ normX2,
+                                           double* __restrict__ errs, int* __restrict__ counter) {
   __shared__ double red[1024];
   __shared__ double red2[1024];
   const int tid = threadIdx.x;
@@ -1064,6 +1118,14 @@ __global__ void __launch_bounds__(1024) k_error(const double* __restrict__ Mlast
     errs[c] = err;
     *counter = c + 1;
   }
+}
+__global__ void __launch_bounds__(1024) k_error(const double* __restrict__ Mlast,
+                                                const double* __restrict__ Flast, int64_t I,
+                                                const double* __restrict__ lambda,
+                                                const double* __restrict__ Gall, int N, int k,
+                                                const double* __restrict__ normX2,
+                                                double* __restrict__ errs, int* __restrict__ counter) {
+  error_body(Mlast, Flast, I, lambda, Gall, N, k, normX2, errs, counter);
 }
 
 // Sum of squares in FP64 (Tensor::norm, common/tensor.hpp:350-356), per-block

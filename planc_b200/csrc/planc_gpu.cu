@@ -24,6 +24,8 @@
 #include "tc_mttkrp.cuh"
 #include "nmf.cuh"
 #include "updates_iter.cuh"
+#include "batch_group.cuh"
+#include "tc_group.cuh"
 
 using namespace pg;
 
@@ -203,6 +205,9 @@ struct planc_gpu_ctx {
   // grid sizing). 1 for a context alone on the GPU; the batch autotuner lowers
   // it when many contexts run concurrently.
   double par_scale = 1.0;
+  // fewest chunks per split-K partial of the tensor-core left contraction
+  // (0: the default plan); the batch autotuner raises it for small members
+  int left_chunks = 0;
   // Incremented whenever a device buffer that a captured graph may reference
   // is (re)allocated; cached graphs are rebuilt when it changes.
   int64_t buf_epoch = 0;
@@ -768,7 +773,7 @@ void mttkrp_direct_tc(planc_gpu_ctx* c, int n, double* out) {
     fail(PLANC_GPU_ERR_STATE, "internal: split-K scratch larger than planned");
   int nsplit = 0;
   launch(c, KC_CONTRACT_LEFT, [&] {
-    nsplit = tc_left(t, wg, c->k, c->scratch, c->status_dev, eff_sm(c), c->stream);
+    nsplit = tc_left(t, wg, c->k, c->scratch, c->status_dev, eff_sm(c), c->stream, c->left_chunks);
   });
   const int64_t nn = c->dims[n] * c->k;
   launch(c, KC_REDUCE, [&] { reduce_splits(c->stream, c->scratch, nsplit, nn, nn, out); });
@@ -826,7 +831,8 @@ void partial_left(planc_gpu_ctx* c, double* out) {
     if (tc_scratch_elems(c->tct, eff_sm(c), c->k) > c->scratch_elems)
       fail(PLANC_GPU_ERR_STATE, "internal: split-K scratch larger than planned");
     launch(c, KC_CONTRACT_LEFT, [&] {
-      nsplit = tc_left(c->tct, wg, c->k, c->scratch, c->status_dev, eff_sm(c), c->stream);
+      nsplit = tc_left(c->tct, wg, c->k, c->scratch, c->status_dev, eff_sm(c), c->stream,
+                       c->left_chunks);
     });
     int64_t n = c->R * c->k;
     launch(c, KC_REDUCE, [&] {
@@ -1449,6 +1455,12 @@ int planc_gpu_create(planc_gpu_ctx** out, int device, int precision, void* cuda_
     if (const char* e = getenv("PLANC_GPU_NES_MAX_STEPS")) {
       const int v = atoi(e);
       if (v >= 1 && v <= NES_MAX_STEPS) c->nes_max_steps = v;
+    }
+    // PLANC_GPU_LEFT_CHUNKS=n: fewest chunks per split-K partial of the
+    // tensor-core left contraction for contexts created while it is set
+    if (const char* e = getenv("PLANC_GPU_LEFT_CHUNKS")) {
+      const int v = atoi(e);
+      if (v >= 0 && v <= (1 << 20)) c->left_chunks = v;
     }
     // PLANC_GPU_BPP_KERNEL=warp|cta fixes the batched BPP kernel for contexts
     // created while it is set (default: chosen by the number of right-hand sides)
@@ -2305,6 +2317,11 @@ struct planc_gpu_batch {
   cudaGraphExec_t gexec = nullptr;
   int g_algo = -1, g_err = -1;
   int64_t g_epoch = -1;  // sum of the members' buffer epochs at capture
+  // grouped iterations: argument tables of the grouped launches (device copy)
+  bool group = true;     // PLANC_GPU_BATCH_GROUPED=0 turns grouped phases off
+  uint8_t* grp_dev = nullptr;
+  size_t grp_cap = 0;
+  bool g_grouped = false;  // the cached graph runs grouped phases
 };
 
 namespace {
@@ -2337,8 +2354,16 @@ int batch_class(const planc_gpu_ctx* c) {
   return c->numel < (1 << 20) ? 0 : c->numel < (1 << 23) ? 1 : 2;
 }
 
+bool batch_groupable(const planc_gpu_batch* b, int algo);
+void batch_capture_grouped(planc_gpu_batch* b, int algo, bool err);
+
 void batch_capture(planc_gpu_batch* b, int algo, bool err) {
+  if (batch_groupable(b, algo)) {
+    batch_capture_grouped(b, algo, err);
+    return;
+  }
   batch_reset_graph(b);
+  b->g_grouped = false;
   cudaGraph_t graph = nullptr;
   CK(cudaStreamBeginCapture(b->master, cudaStreamCaptureModeThreadLocal));
   try {
@@ -2366,6 +2391,362 @@ void batch_capture(planc_gpu_batch* b, int algo, bool err) {
   b->g_algo = algo;
   b->g_err = err ? 1 : 0;
   b->g_epoch = batch_epoch(b);
+}
+
+// ---------------------------------------------------------------- grouped phases
+// A batch whose members are all 3-way tensor-core contexts running MU or HALS
+// on the dimension tree (factors of at most NGC_MAX_ROWS rows) runs each
+// outer iteration as phases: the tensor-core contractions of every member on
+// the worker streams (one per member, as before), and every other step of
+// the iteration -- the multi-TTVs, split-K sums, factor updates,
+// normalisation + Gram and error -- as ONE launch for all members (blockIdx.z
+// = member, batch_group.cuh). The members' arithmetic is that of their own
+// iteration (mttkrp_dimtree + run_update + normalize_gram + error_kernel);
+// a batched iteration is ~15 launches plus the contractions instead of
+// ~15 launches per member.
+bool batch_groupable(const planc_gpu_batch* b, int algo) {
+  if (!b->group || (algo != PLANC_GPU_HALS && algo != PLANC_GPU_MU)) return false;
+  for (auto* m : b->members) {
+    if (m->N != 3 || m->precision == PLANC_GPU_PREC_FP64 || m->bal4 || m->ngc_ctas <= 0) return false;
+    for (int n = 0; n < 3; ++n)
+      if (m->dims[n] > NGC_MAX_ROWS) return false;
+  }
+  return true;
+}
+
+// Host copies of the argument tables, laid out as they are copied to the
+// batch's device buffer after capture (the captured launches hold device
+// addresses inside that buffer).
+struct GrpTables {
+  std::vector<uint8_t> host;
+  uint8_t* dev = nullptr;
+  size_t cap = 0;
+  template <typename T>
+  const T* put(const std::vector<T>& v) {
+    size_t off = (host.size() + 255) & ~(size_t)255;
+    const size_t bytes = v.size() * sizeof(T);
+    if (off + bytes > cap) fail(PLANC_GPU_ERR_STATE, "internal: grouped argument tables too large");
+    host.resize(off + bytes);
+    memcpy(host.data() + off, v.data(), bytes);
+    return reinterpret_cast<const T*>(dev + off);
+  }
+};
+
+void grp_check(cudaError_t e) { cuda_check(e, "grouped launch"); }
+
+template <typename T>
+unsigned grp_max(const std::vector<T>& v, unsigned T::*f) {
+  unsigned g = 1;
+  for (const T& x : v) g = std::max(g, x.*f);
+  return g;
+}
+
+void grp_reduce(GrpTables& tab, cudaStream_t st, const std::vector<GrpRed>& all) {
+  std::vector<GrpRed> few, many;
+  for (const GrpRed& r : all) (reduce_kind(r.nsplit) == 0 ? few : many).push_back(r);
+  if (!few.empty())
+    k_grp_reduce_few<<<dim3(grp_max(few, &GrpRed::gx), 1, (unsigned)few.size()), 256, 0, st>>>(tab.put(few));
+  if (!many.empty())
+    k_grp_reduce<<<dim3(grp_max(many, &GrpRed::gx), 1, (unsigned)many.size()), 256, 0, st>>>(tab.put(many));
+  grp_check(cudaGetLastError());
+}
+
+GrpRed grp_red(const double* part, int nsplit, int64_t n, double* out) {
+  return GrpRed{part, nsplit, n, n, out, reduce_blocks(nsplit, n)};
+}
+
+// run_update for every member (MU / HALS, one warp per row)
+void grp_update(GrpTables& tab, cudaStream_t st, const std::vector<planc_gpu_ctx*>& ms, int algo, int n) {
+  std::vector<GrpUpd> u32, u64;
+  for (auto* m : ms) {
+    const int64_t I = m->dims[n];
+    GrpUpd u{m->F[n], m->M[n], m->Gloo, I, m->k, (unsigned)((I + 7) / 8)};
+    (m->k <= 32 ? u32 : u64).push_back(u);
+  }
+  if (!u32.empty()) {
+    const dim3 g(grp_max(u32, &GrpUpd::gx), 1, (unsigned)u32.size());
+    if (algo == PLANC_GPU_HALS) k_grp_hals<32><<<g, 256, 0, st>>>(tab.put(u32));
+    else k_grp_mu<32><<<g, 256, 0, st>>>(tab.put(u32), kEps6);
+  }
+  if (!u64.empty()) {
+    const dim3 g(grp_max(u64, &GrpUpd::gx), 1, (unsigned)u64.size());
+    if (algo == PLANC_GPU_HALS) k_grp_hals<64><<<g, 256, 0, st>>>(tab.put(u64));
+    else k_grp_mu<64><<<g, 256, 0, st>>>(tab.put(u64), kEps6);
+  }
+  grp_check(cudaGetLastError());
+}
+
+// normalize_gram(n, next, lambda) for every member (its cluster path)
+void grp_normgram(GrpTables& tab, cudaStream_t st, const std::vector<planc_gpu_ctx*>& ms, int n, int next) {
+  std::vector<GrpNg> g2, g4;
+  int cl2 = 1, cl4 = 1;
+  for (auto* m : ms) {
+    const int64_t I = m->dims[n];
+    const int64_t rpc = m->k > 32 ? 16 : NGC_TILE;
+    const int cl = (int)std::min<int64_t>(m->ngc_ctas, std::max<int64_t>(1, (I + rpc - 1) / rpc));
+    GrpNg g{m->F[n], I, m->k, m->lambda, m->Gall, m->N, n, next, m->Gloo, cl};
+    if (m->k <= 32) {
+      g2.push_back(g);
+      cl2 = std::max(cl2, cl);
+    } else {
+      g4.push_back(g);
+      cl4 = std::max(cl4, cl);
+    }
+  }
+  auto go = [&](auto kern, const std::vector<GrpNg>& v, int cl, int kp) {
+    if (v.empty()) return;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3((unsigned)cl, 1, (unsigned)v.size());
+    cfg.blockDim = dim3(NGC_THREADS, 1, 1);
+    cfg.dynamicSmemBytes = ngc_smem_bytes(kp);
+    cfg.stream = st;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = (unsigned)cl;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    grp_check(cudaLaunchKernelEx(&cfg, kern, tab.put(v)));
+  };
+  go(k_grp_normgram<2>, g2, cl2, 32);
+  go(k_grp_normgram<4>, g4, cl4, 64);
+}
+
+void batch_capture_grouped(planc_gpu_batch* b, int algo, bool err) {
+  batch_reset_graph(b);
+  const auto& ms = b->members;
+  const size_t cap = 32 * ((size_t)ms.size() * 512 + 256);
+  if (b->grp_cap < cap) {
+    dalloc(&b->grp_dev, cap);
+    b->grp_cap = cap;
+  }
+  GrpTables tab;
+  tab.dev = b->grp_dev;
+  tab.cap = b->grp_cap;
+  cudaStream_t st = b->master;
+  auto fork = [&] {
+    CK(cudaEventRecord(b->fork, st));
+    for (auto w : b->workers) CK(cudaStreamWaitEvent(w, b->fork, 0));
+  };
+  auto join = [&] {
+    for (size_t i = 0; i < b->workers.size(); ++i) {
+      CK(cudaEventRecord(b->joins[i], b->workers[i]));
+      CK(cudaStreamWaitEvent(st, b->joins[i], 0));
+    }
+  };
+  if (b->precision == PLANC_GPU_PREC_BF16X2) {
+    CK((tcg_set_attrs<16, true>()));
+    CK((tcg_set_attrs<32, true>()));
+    CK((tcg_set_attrs<64, true>()));
+  } else {
+    CK((tcg_set_attrs<16, false>()));
+    CK((tcg_set_attrs<32, false>()));
+    CK((tcg_set_attrs<64, false>()));
+  }
+  cudaGraph_t graph = nullptr;
+  CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+  try {
+    for (auto* m : ms) m->capturing = true;
+    // every member's tensor maps: right hi, right lo, left hi, left lo
+    std::vector<CUtensorMap> maps(4 * ms.size());
+    for (size_t i = 0; i < ms.size(); ++i) {
+      maps[4 * i] = ms[i]->tct.mR_hi;
+      maps[4 * i + 1] = ms[i]->tct.mR_lo;
+      maps[4 * i + 2] = ms[i]->tct.mL_hi;
+      maps[4 * i + 3] = ms[i]->tct.mL_lo;
+    }
+    const CUtensorMap* dmaps = tab.put(maps);
+    const bool x2 = b->precision == PLANC_GPU_PREC_BF16X2;
+    const int sms = ms[0]->sm_count;
+    int* gst = ms[0]->status_dev;  // status word of the grouped contractions
+    auto kpi = [](int k) { return tc_kpad(k) == 16 ? 0 : tc_kpad(k) == 32 ? 1 : 2; };
+    // ---- mode 0: P = X F_2 for every member (one grouped launch per rank
+    // class; members whose right contraction also forms the mode-0 multi-TTV
+    // keep their own launches); M_0 from P or from the fused TTV partials
+    std::vector<GrpRed> red;
+    std::vector<GrpTtvR> ttvr[4];
+    std::vector<TcgRight> rmem(ms.size());
+    std::vector<TcgBimg> bim[3];
+    std::vector<int2> ritems[3];
+    fork();
+    for (size_t mi = 0; mi < ms.size(); ++mi) {
+      planc_gpu_ctx* m = ms[mi];
+      const int k = m->k;
+      const int64_t I0 = m->dims[0];
+      const int ns = tc_right_ttv_nsplit(m->tct, k, eff_sm(m));
+      if (ns > 0 && (size_t)ns * I0 * k <= m->scratch_elems) {
+        launch(m, KC_PREP, [&] { tc_right_prep(m->tct, m->F[2], k, m->stream); });
+        launch(m, KC_CONTRACT, [&] {
+          tc_right_ttv(m->tct, k, m->P32, m->F[1], m->scratch, m->status_dev, eff_sm(m), m->stream);
+        });
+        red.push_back(grp_red(m->scratch, ns, I0 * k, m->M[0]));
+      } else {
+        const int ci = kpi(k), kp = tc_kpad(k);
+        const int nk = (int)((m->tct.R + TC_BK - 1) / TC_BK);
+        bim[ci].push_back(TcgBimg{m->F[2], m->tct.R, k, nk, m->tct.bimg,
+                                  (unsigned)std::min<int64_t>(((int64_t)nk * kp * TC_BK + 255) / 256, 1024)});
+        rmem[mi] = TcgRight{m->tct.bimg, m->P32, m->tct.L, m->tct.R, k, 0};
+        const int64_t ntiles = (m->tct.L + TC_BM - 1) / TC_BM;
+        for (int64_t t = 0; t < ntiles; ++t) ritems[ci].push_back(make_int2((int)mi, (int)t));
+        const int64_t A = I0, B = m->L / I0;
+        TtvRightPlan p = plan_ttv_right(m, A, B);
+        if (p.nsplit > 1 && (size_t)p.nsplit * A * k > m->scratch_elems)
+          fail(PLANC_GPU_ERR_STATE, "internal: multi-TTV scratch larger than planned");
+        const int ki = kpad(k) == 8 ? 0 : kpad(k) == 16 ? 1 : kpad(k) == 32 ? 2 : 3;
+        ttvr[ki].push_back(GrpTtvR{m->P32, A, B, k, make_wgen(m, {1}), p.bper,
+                                   p.nsplit > 1 ? m->scratch : m->M[0], p.grid.x, p.grid.y});
+        if (p.nsplit > 1) red.push_back(grp_red(m->scratch, p.nsplit, A * k, m->M[0]));
+      }
+    }
+    {
+      const TcgRight* drm = tab.put(rmem);
+      for (int ci = 0; ci < 3; ++ci) {
+        if (ritems[ci].empty()) continue;
+        const auto& bv = bim[ci];
+        const dim3 gb(grp_max(bv, &TcgBimg::gx), 1, (unsigned)bv.size());
+        const TcgBimg* db = tab.put(bv);
+        const int2* di = tab.put(ritems[ci]);
+        const int n = (int)ritems[ci].size();
+        const int grid = std::min(n, sms);
+#define TCG_RIGHT(KP)                                                                           \
+  {                                                                                             \
+    constexpr uint32_t SR16 = 2 * KP * 128;                                                     \
+    const uint32_t stage = (x2 ? 2u : 1u) * TC_BM * TC_BK * 2 + SR16;                           \
+    const int stg = tc_stages(stage);                                                           \
+    const size_t smem = (size_t)stg * stage + 1024;                                             \
+    k_tc_bimage_grp<KP><<<gb, 256, 0, st>>>(db);                                                \
+    if (x2) k_tc_right_grp<KP, true><<<grid, TC_THREADS, smem, st>>>(dmaps, drm, di, n, stg, gst); \
+    else k_tc_right_grp<KP, false><<<grid, TC_THREADS, smem, st>>>(dmaps, drm, di, n, stg, gst); \
+  }
+        if (ci == 0) TCG_RIGHT(16) else if (ci == 1) TCG_RIGHT(32) else TCG_RIGHT(64)
+#undef TCG_RIGHT
+        grp_check(cudaGetLastError());
+      }
+    }
+    join();
+    for (int ki = 0; ki < 4; ++ki) {
+      const auto& v = ttvr[ki];
+      if (v.empty()) continue;
+      const dim3 g(grp_max(v, &GrpTtvR::gx), grp_max(v, &GrpTtvR::gy), (unsigned)v.size());
+      const GrpTtvR* t = tab.put(v);
+      if (ki == 0) k_grp_ttv_right<8><<<g, 256, 0, st>>>(t);
+      else if (ki == 1) k_grp_ttv_right<16><<<g, 256, 0, st>>>(t);
+      else if (ki == 2) k_grp_ttv_right<32><<<g, 256, 0, st>>>(t);
+      else k_grp_ttv_right<64><<<g, 256, 0, st>>>(t);
+      grp_check(cudaGetLastError());
+    }
+    grp_reduce(tab, st, red);
+    grp_update(tab, st, ms, algo, 0);
+    grp_normgram(tab, st, ms, 0, 1);
+    // ---- mode 1: M_1 = TTV of P with the updated F_0 (run_ttv_left<float>)
+    {
+      std::vector<GrpTtvL> plain, f4;
+      for (auto* m : ms) {
+        const int k = m->k;
+        const int64_t A = m->dims[0], B = m->dims[1];
+        const int64_t g2 = (B + TTVL_NB - 1) / TTVL_NB;
+        if (k % 4 == 0 && g2 >= m->sm_count && g2 <= 65535)
+          f4.push_back(GrpTtvL{m->P32, A, B, k, m->F[0], m->M[1], (unsigned)g2});
+        else
+          plain.push_back(GrpTtvL{m->P32, A, B, k, m->F[0], m->M[1],
+                                  (unsigned)std::min<int64_t>(B, 65535)});
+      }
+      if (!plain.empty())
+        k_grp_ttv_left<<<dim3(grp_max(plain, &GrpTtvL::gx), 1, (unsigned)plain.size()), 256, 0, st>>>(
+            tab.put(plain));
+      if (!f4.empty())
+        k_grp_ttv_left_f4<<<dim3(grp_max(f4, &GrpTtvL::gx), 1, (unsigned)f4.size()), 256, 0, st>>>(
+            tab.put(f4));
+      grp_check(cudaGetLastError());
+    }
+    grp_update(tab, st, ms, algo, 1);
+    grp_normgram(tab, st, ms, 1, 2);
+    // ---- mode 2: M_2 = X^T KRP(F_0, F_1) per member (split-K partials), then the sums
+    // one grouped launch per (rank class, row tiles per CTA) for the generic
+    // left contractions; the factored ones (I_0 % 64 == 0) keep their own
+    red.clear();
+    std::vector<TcgLeft> lmem(ms.size());
+    std::vector<TcgUnit> lunits[3][2];
+    fork();
+    for (size_t mi = 0; mi < ms.size(); ++mi) {
+      planc_gpu_ctx* m = ms[mi];
+      WGen wg = make_wgen(m, {0, 1});
+      if (tc_scratch_elems(m->tct, eff_sm(m), m->k) > m->scratch_elems)
+        fail(PLANC_GPU_ERR_STATE, "internal: split-K scratch larger than planned");
+      if (tc_left_factored(m->tct)) {
+        int nsplit = 0;
+        launch(m, KC_CONTRACT_LEFT, [&] {
+          nsplit = tc_left(m->tct, wg, m->k, m->scratch, m->status_dev, eff_sm(m), m->stream,
+                           m->left_chunks);
+        });
+        red.push_back(grp_red(m->scratch, nsplit, m->R * m->k, m->M[2]));
+        continue;
+      }
+      int mg = 0, ns = 0;
+      tc_left_plan(m->tct, m->k, eff_sm(m), &mg, &ns, m->left_chunks);
+      const int MT = tc_left_mt(m->tct.R, m->k);
+      lmem[mi] = TcgLeft{wg, m->scratch, m->tct.L, m->tct.R, m->k, ns};
+      for (int jg = 0; jg < mg; ++jg)
+        for (int y = 0; y < ns; ++y) lunits[kpi(m->k)][MT - 1].push_back(TcgUnit{(int)mi, jg, y, 0});
+      red.push_back(grp_red(m->scratch, ns, m->R * m->k, m->M[2]));
+    }
+    {
+      const TcgLeft* dlm = tab.put(lmem);
+      for (int ci = 0; ci < 3; ++ci)
+        for (int mt = 1; mt <= 2; ++mt) {
+          const auto& uv = lunits[ci][mt - 1];
+          if (uv.empty()) continue;
+          const TcgUnit* du = tab.put(uv);
+          const int n = (int)uv.size();
+          const int grid = std::min(n, sms);
+#define TCG_LEFT(KP, MTV)                                                                            \
+  {                                                                                                  \
+    const uint32_t stage = (x2 ? 2u : 1u) * MTV * TC_BM * TC_BK * 2 + 2 * KP * 128;                  \
+    const int stg = tc_stages(stage);                                                                \
+    const size_t smem = (size_t)stg * stage + 1024;                                                  \
+    if (x2) k_tc_left_grp<KP, MTV, true><<<grid, TCL_THREADS, smem, st>>>(dmaps, dlm, du, n, stg, gst);  \
+    else k_tc_left_grp<KP, MTV, false><<<grid, TCL_THREADS, smem, st>>>(dmaps, dlm, du, n, stg, gst);    \
+  }
+          if (ci == 0) { if (mt == 1) TCG_LEFT(16, 1) else TCG_LEFT(16, 2) }
+          else if (ci == 1) { if (mt == 1) TCG_LEFT(32, 1) else TCG_LEFT(32, 2) }
+          else { if (mt == 1) TCG_LEFT(64, 1) else TCG_LEFT(64, 2) }
+#undef TCG_LEFT
+          grp_check(cudaGetLastError());
+        }
+    }
+    join();
+    grp_reduce(tab, st, red);
+    grp_update(tab, st, ms, algo, 2);
+    grp_normgram(tab, st, ms, 2, 0);
+    if (err) {
+      std::vector<GrpErr> e;
+      for (auto* m : ms)
+        e.push_back(GrpErr{m->M[2], m->F[2], m->dims[2], m->lambda, m->Gall, m->N, m->k, m->normX2,
+                           m->errs_dev, m->counter_dev});
+      k_grp_error<<<dim3(1, 1, (unsigned)e.size()), 1024, 0, st>>>(tab.put(e));
+      grp_check(cudaGetLastError());
+    }
+    for (auto* m : ms) m->capturing = false;
+  } catch (...) {
+    for (auto* m : ms) m->capturing = false;
+    cudaStreamEndCapture(st, &graph);
+    if (graph) cudaGraphDestroy(graph);
+    throw;
+  }
+  CK(cudaStreamEndCapture(st, &graph));
+  cudaError_t e = cudaGraphInstantiate(&b->gexec, graph, 0);
+  cudaGraphDestroy(graph);
+  cuda_check(e, "cudaGraphInstantiate (grouped batch)");
+  // the captured launches read their tables from grp_dev from the first replay
+  // on (no earlier replay of this batch is still running: the master stream
+  // is drained first)
+  CK(cudaStreamSynchronize(st));
+  CK(cudaMemcpy(b->grp_dev, tab.host.data(), tab.host.size(), cudaMemcpyHostToDevice));
+  b->g_algo = algo;
+  b->g_err = err ? 1 : 0;
+  b->g_epoch = batch_epoch(b);
+  b->g_grouped = true;
 }
 
 // per-run set-up of every member (error counters, first leave-one-out Gram),
@@ -2401,7 +2782,18 @@ int planc_gpu_batch_create(planc_gpu_batch** out, int device, int precision, int
     planc_gpu_batch* b = new planc_gpu_batch();
     b->device = device;
     b->precision = precision;
+    // PLANC_GPU_BATCH_GROUPED=0: per-member launches only (no grouped phases)
+    if (const char* e = getenv("PLANC_GPU_BATCH_GROUPED")) b->group = strcmp(e, "0") != 0;
     try {
+      // the grouped normalisation + Gram runs clusters of up to 16 CTAs with
+      // up to 64 KB of dynamic shared memory (as k_normgram_cluster)
+      for (auto kern : {k_grp_normgram<2>, k_grp_normgram<4>}) {
+        if (cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+            cudaSuccess)
+          cudaGetLastError();
+        CK(cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)ngc_smem_bytes(64)));
+      }
       CK(cudaStreamCreateWithFlags(&b->master, cudaStreamNonBlocking));
       CK(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
       for (int i = 0; i < nstreams; ++i) {
@@ -2517,11 +2909,17 @@ int planc_gpu_batch_autotune(planc_gpu_batch* b, int algo, int trials, double* b
     }
     const double cand[] = {1.0, 0.5, 0.25, 0.125, 0.0625, 0.03125};
     double scale[3] = {1.0, 1.0, 1.0};
+    // fewest 64-element chunks per split-K partial of the left contraction
+    const int lcand[] = {0, 8, 32, 128};
+    int lch[3] = {0, 0, 0};
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
     auto time_cfg = [&]() -> float {
-      for (auto* m : b->members) m->par_scale = scale[batch_class(m)];
+      for (auto* m : b->members) {
+        m->par_scale = scale[batch_class(m)];
+        m->left_chunks = lch[batch_class(m)];
+      }
       batch_ensure(b, 1, false);
       batch_capture(b, algo, false);
       batch_prepare(b);
@@ -2550,8 +2948,25 @@ int planc_gpu_batch_autotune(planc_gpu_batch* b, int algo, int trials, double* b
         }
       }
       scale[cls] = keep;
+      // then the split-K length of the tensor-core left contraction
+      if (b->precision != PLANC_GPU_PREC_FP64) {
+        int lkeep = lch[cls];
+        for (int lc : lcand) {
+          if (lc == lkeep) continue;
+          lch[cls] = lc;
+          float t = time_cfg();
+          if (t < best) {
+            best = t;
+            lkeep = lc;
+          }
+        }
+        lch[cls] = lkeep;
+      }
     }
-    for (auto* m : b->members) m->par_scale = scale[batch_class(m)];
+    for (auto* m : b->members) {
+      m->par_scale = scale[batch_class(m)];
+      m->left_chunks = lch[batch_class(m)];
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     batch_reset_graph(b);
@@ -2577,6 +2992,7 @@ int planc_gpu_batch_destroy(planc_gpu_batch* b) {
     for (auto e : b->joins) cudaEventDestroy(e);
     cudaEventDestroy(b->fork);
     cudaStreamDestroy(b->master);
+    if (b->grp_dev) cudaFree(b->grp_dev);
     delete b;
   });
 }

@@ -424,12 +424,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 // 128 bytes (K-major, 128B swizzle); row r < KP holds hi(F[j, r]) and row
 // KP + r holds lo(F[j, r]) for j = kb*64 .. kb*64+63 (zero beyond R or k).
 template <int KP>
-__global__ void k_tc_bimage(const double* __restrict__ F, int64_t R, int k, int nk,
-                            uint8_t* __restrict__ img) {
+__device__ __forceinline__ void tc_bimage_body(const double* __restrict__ F, int64_t R, int k, int nk,
+                                               uint8_t* __restrict__ img, int64_t bx, int64_t gx) {
   constexpr int NCOL = 2 * KP;
   const int64_t total = (int64_t)nk * KP * TC_BK;
-  for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < total;
-       e += (int64_t)gridDim.x * blockDim.x) {
+  for (int64_t e = bx * blockDim.x + threadIdx.x; e < total; e += gx * blockDim.x) {
     const int kk = (int)(e % TC_BK);
     const int r = (int)((e / TC_BK) % KP);
     const int kb = (int)(e / ((int64_t)TC_BK * KP));
@@ -440,6 +439,11 @@ __global__ void k_tc_bimage(const double* __restrict__ F, int64_t R, int k, int 
     *reinterpret_cast<__nv_bfloat16*>(st + sw128_kmajor_off(r, kk)) = hi;
     *reinterpret_cast<__nv_bfloat16*>(st + sw128_kmajor_off(KP + r, kk)) = lo;
   }
+}
+template <int KP>
+__global__ void k_tc_bimage(const double* __restrict__ F, int64_t R, int k, int nk,
+                            uint8_t* __restrict__ img) {
+  tc_bimage_body<KP>(F, R, k, nk, img, blockIdx.x, gridDim.x);
 }
 
 // ------------------------------------------------------------ left kernel
@@ -1476,13 +1480,21 @@ inline int tc_stages(uint32_t stage_bytes) {
 // 64-wide rank (keeps the drain warps' running sums in registers)
 inline int tc_left_mt(int64_t R, int k) { return (R > 128 && k <= 32) ? 2 : 1; }
 
-inline void tc_left_plan(const TcTensor& t, int k, int sm_count, int* mgroups, int* nsplit) {
+// min_units > 0 caps the split count so that every split takes at least
+// that many chunks (runs): fewer, longer splits for small tensors whose
+// parallelism comes from elsewhere (a grouped batch)
+inline void tc_left_plan(const TcTensor& t, int k, int sm_count, int* mgroups, int* nsplit,
+                         int min_units = 0) {
   const int MT = tc_left_mt(t.R, k);
   *mgroups = (int)((t.R + MT * TC_BM - 1) / (MT * TC_BM));
   int ns = sm_count / *mgroups;
   if (ns < 1) ns = 1;
   const int64_t units = tc_left_factored(t) ? t.L / t.I0 : (t.L + TC_BK - 1) / TC_BK;
   if (ns > units) ns = (int)units;
+  if (min_units > 0) {
+    const int64_t cap = (units + min_units - 1) / min_units;
+    if (ns > cap) ns = (int)(cap < 1 ? 1 : cap);
+  }
   *nsplit = ns;
 }
 
@@ -1648,9 +1660,9 @@ inline void tc_right(const TcTensor& t, int k, float* P, int* status, int sm_cou
 
 template <int KP, int MT, bool X2>
 inline void tc_left_launch(const TcTensor& t, const WGen& wg, int k, double* part, int* status,
-                           int sm_count, cudaStream_t st, int* nsplit_out) {
+                           int sm_count, cudaStream_t st, int* nsplit_out, int min_units) {
   int mg, ns;
-  tc_left_plan(t, k, sm_count, &mg, &ns);
+  tc_left_plan(t, k, sm_count, &mg, &ns, min_units);
   constexpr uint32_t STAGE = (X2 ? 2 : 1) * MT * TC_BM * TC_BK * 2 + 2 * KP * 128;
   const int stages = tc_stages(STAGE);
   const size_t smem = (size_t)stages * STAGE + 1024;
@@ -1671,17 +1683,17 @@ inline void tc_left_launch(const TcTensor& t, const WGen& wg, int k, double* par
 
 // Returns the number of split-K partials written to `part`.
 inline int tc_left(const TcTensor& t, const WGen& wg, int k, double* part, int* status,
-                   int sm_count, cudaStream_t st) {
+                   int sm_count, cudaStream_t st, int min_units = 0) {
   const bool x2 = t.prec == 2;
   const int MT = tc_left_mt(t.R, k);
   int ns = 1;
 #define TCL(KP)                                                                                  \
   if (MT == 2) {                                                                                 \
-    x2 ? tc_left_launch<KP, 2, true>(t, wg, k, part, status, sm_count, st, &ns)                  \
-       : tc_left_launch<KP, 2, false>(t, wg, k, part, status, sm_count, st, &ns);                \
+    x2 ? tc_left_launch<KP, 2, true>(t, wg, k, part, status, sm_count, st, &ns, min_units)                  \
+       : tc_left_launch<KP, 2, false>(t, wg, k, part, status, sm_count, st, &ns, min_units);                \
   } else {                                                                                       \
-    x2 ? tc_left_launch<KP, 1, true>(t, wg, k, part, status, sm_count, st, &ns)                  \
-       : tc_left_launch<KP, 1, false>(t, wg, k, part, status, sm_count, st, &ns);                \
+    x2 ? tc_left_launch<KP, 1, true>(t, wg, k, part, status, sm_count, st, &ns, min_units)                  \
+       : tc_left_launch<KP, 1, false>(t, wg, k, part, status, sm_count, st, &ns, min_units);                \
   }
   switch (tc_kpad(k)) {
     case 16: TCL(16) break;

@@ -509,11 +509,14 @@ inline size_t ngc_smem_bytes(int k) {
   return ((size_t)NGC_TILE * kp + (size_t)kp * kp) * sizeof(double);
 }
 
+// The rows are split over the first CLm CTAs of the cluster (CLm <= the
+// cluster's size; a batch's grouped launch runs every member in a cluster of
+// the largest member's size, and the CTAs past a member's own CLm add zeros).
 template <int BE>  // edge of a thread's block of outputs: 2 (k <= 32) or 4
-__global__ void __launch_bounds__(NGC_THREADS, 1)
-    k_normgram_cluster(double* __restrict__ F, int64_t I, int k, double* __restrict__ lambda,
-                       double* __restrict__ Gall, int N, int n, int next,
-                       double* __restrict__ Gloo) {
+__device__ __forceinline__ void normgram_cluster_body(double* __restrict__ F, int64_t I, int k,
+                                                      double* __restrict__ lambda,
+                                                      double* __restrict__ Gall, int N, int n,
+                                                      int next, double* __restrict__ Gloo, int CLm) {
   cg::cluster_group cluster = cg::this_cluster();
   const int CL = (int)cluster.num_blocks(), me = (int)cluster.block_rank();
   extern __shared__ double ngc_sm[];
@@ -523,7 +526,7 @@ __global__ void __launch_bounds__(NGC_THREADS, 1)
   __shared__ double lam[kMaxRank];
   const int tid = threadIdx.x;
   const int kk2 = k * k;
-  const int64_t per = (I + CL - 1) / CL;
+  const int64_t per = (I + CLm - 1) / CLm;
   const int64_t r0 = (int64_t)me * per;
   const int64_t r1 = (r0 + per) < I ? (r0 + per) : I;
   const int kt = (k + BE - 1) / BE;
@@ -606,6 +609,14 @@ __global__ void __launch_bounds__(NGC_THREADS, 1)
       if (i != next) g = g * Gall[(int64_t)i * kk2 + e];
     Gloo[e] = g;
   }
+}
+template <int BE>
+__global__ void __launch_bounds__(NGC_THREADS, 1)
+    k_normgram_cluster(double* __restrict__ F, int64_t I, int k, double* __restrict__ lambda,
+                       double* __restrict__ Gall, int N, int n, int next,
+                       double* __restrict__ Gloo) {
+  normgram_cluster_body<BE>(F, I, k, lambda, Gall, N, n, next, Gloo,
+                            (int)cg::this_cluster().num_blocks());
 }
 
 // ---------------------------------------------------------------------------
