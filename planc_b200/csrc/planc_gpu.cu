@@ -211,6 +211,8 @@ struct planc_gpu_ctx {
   // Incremented whenever a device buffer that a captured graph may reference
   // is (re)allocated; cached graphs are rebuilt when it changes.
   int64_t buf_epoch = 0;
+  size_t gall_elems = 0;  // capacity of Gall
+  int kvec = 0;           // rank the k-sized buffers (Gloo, lambda, lam_tmp) hold
   int64_t g_epoch = -1;
 };
 
@@ -1643,8 +1645,11 @@ int planc_gpu_set_factors(planc_gpu_ctx* c, const double* const* F, const double
     if (k < 1 || k > kMaxRank)
       fail(PLANC_GPU_ERR_UNSUPPORTED, "rank must be in [1, " + std::to_string(kMaxRank) + "]");
     set_device(c);
-    reset_graph(c);
+    // Cached iteration graphs stay valid when no buffer moves: the new
+    // factors are copied into the same device arrays. Any reallocation below
+    // bumps the buffer epoch, which rebuilds the graphs before their next use.
     if (k != c->k) {
+      reset_graph(c);
       free_update_state(c);
       auto f = [](auto*& p) {
         if (p) cudaFree(p);
@@ -1663,19 +1668,32 @@ int planc_gpu_set_factors(planc_gpu_ctx* c, const double* const* F, const double
         dalloc(&c->F[n], need);
         dalloc(&c->M[n], need);
         c->factor_cap[n] = (int64_t)need;
+        c->buf_epoch++;
       }
       CK(cudaMemcpyAsync(c->F[n], F[n], need * 8, cudaMemcpyHostToDevice, c->stream));
     }
-    dalloc(&c->Gall, (size_t)c->N * k * k);
+    if (!c->Gall || c->gall_elems != (size_t)c->N * k * k) {
+      c->gall_elems = (size_t)c->N * k * k;
+      dalloc(&c->Gall, c->gall_elems);
+      c->buf_epoch++;
+    }
     {
       int64_t maxI = 1;
       for (int n = 0; n < c->N; ++n) maxI = std::max(maxI, c->dims[n]);
-      c->gram_part_elems = (size_t)((maxI + GP_ROWS - 1) / GP_ROWS) * k * k;
-      dalloc(&c->gram_part, c->gram_part_elems);
+      const size_t gp = (size_t)((maxI + GP_ROWS - 1) / GP_ROWS) * k * k;
+      if (!c->gram_part || c->gram_part_elems < gp) {
+        c->gram_part_elems = gp;
+        dalloc(&c->gram_part, c->gram_part_elems);
+        c->buf_epoch++;
+      }
     }
-    dalloc(&c->Gloo, (size_t)k * k);
-    dalloc(&c->lambda, (size_t)k);
-    dalloc(&c->lam_tmp, (size_t)k);
+    if (!c->Gloo || c->kvec != k) {
+      dalloc(&c->Gloo, (size_t)k * k);
+      dalloc(&c->lambda, (size_t)k);
+      dalloc(&c->lam_tmp, (size_t)k);
+      c->kvec = k;
+      c->buf_epoch++;
+    }
     // AUNTF::reset: update_factor_mode on every mode (normalise, Gram), then
     // set_lambda(new lambda)
     for (int n = 0; n < c->N; ++n) normalize_gram(c, n, n == c->N - 1 ? 0 : -1, c->lambda);
