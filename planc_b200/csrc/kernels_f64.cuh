@@ -225,13 +225,66 @@ __global__ void __launch_bounds__(256, 2) k_contract_f64(const double* __restric
       const int64_t a0 = (t % tilesA) * BK;
       const int aa = tid % BK;
       const int64_t ga = a0 + aa;
+      // rows mm = tid / BK + (256 / BK) i of the tile through one running pointer
+      constexpr int MSTEP = 256 / BK;
+      const int64_t gm0 = m0 + tid / BK;
+      const double* xp = X + ga + g.ldx * gm0 + g.ldb * b;
+      const int64_t xstep = MSTEP * g.ldx;
+      if (ga < g.A && m0 + CT_BM <= g.M) {
 #pragma unroll
-      for (int i = 0; i < XPT; ++i) {
-        int mm = tid / BK + (256 / BK) * i;
-        int64_t gm = m0 + mm;
-        xr[i] = (gm < g.M && ga < g.A) ? X[ga + g.ldx * gm + g.ldb * b] : 0.0;
+        for (int i = 0; i < XPT; ++i) {
+          xr[i] = *xp;
+          xp += xstep;
+        }
+      } else {
+#pragma unroll
+        for (int i = 0; i < XPT; ++i) {
+          xr[i] = (gm0 + MSTEP * i < g.M && ga < g.A) ? *xp : 0.0;
+          xp += xstep;
+        }
       }
       const int64_t wrow0 = a0 + g.A * b;
+      if constexpr (NF == 2 || NF == 3) {
+        if (small_rows) {
+          // 256 is a multiple of KP: entry i of this thread is row
+          // kk = tid / KP + (256 / KP) i, rank r = tid % KP; its Khatri-Rao
+          // digits advance by 256 / KP per entry (one division per tile)
+          constexpr uint32_t RSTEP = 256 / KP;
+          const int r = tid % KP;
+          const int kk0 = tid / KP;
+          const uint32_t d0 = fd0.d, d1 = fd1.d;
+          uint32_t row = (uint32_t)(wrow0 + kk0);
+          uint32_t i1 = fast_div(row, fd0), i0 = row - i1 * d0, i2 = 0;
+          if (NF == 3) {
+            const uint32_t q = i1;
+            i2 = fast_div(q, fd1);
+            i1 = q - i2 * d1;
+          }
+#pragma unroll
+          for (int i = 0; i < WPT; ++i) {
+            double v = 0.0;
+            if (r < k && a0 + kk0 + (int64_t)RSTEP * i < g.A) {
+              if (NF == 2)
+                v = wg.f[0][(int64_t)i0 * k + r] * wg.f[1][(int64_t)i1 * k + r];
+              else
+                v = wg.f[0][(int64_t)i0 * k + r] *
+                    (wg.f[1][(int64_t)i1 * k + r] * wg.f[2][(int64_t)i2 * k + r]);
+            }
+            wr[i] = v;
+            i0 += RSTEP;
+            while (i0 >= d0) {
+              i0 -= d0;
+              if (NF == 3 && ++i1 == d1) {
+                i1 = 0;
+                ++i2;
+              } else if (NF == 2) {
+                ++i1;
+              }
+            }
+          }
+          return;
+        }
+      }
 #pragma unroll
       for (int i = 0; i < WPT; ++i) {
         int e = tid + 256 * i;
@@ -706,14 +759,33 @@ __global__ void __launch_bounds__(128) k_mu_rows(double* __restrict__ H, const d
 // HALS keeps g = H(row,:) * G up to date incrementally: after column i moves
 // by delta, g += delta * G(i,:), so g(i) always equals the reference's
 // H(row,:) * G(:,i) with columns < i already replaced (ntf/ntfhals.hpp:17-18).
+// k x k matrix G into shared memory, four loads in flight per thread, then a
+// CTA barrier
+__device__ __forceinline__ void stage_gram(const double* __restrict__ G, int k, double* Gs) {
+  const int kk = k * k;
+  for (int e0 = threadIdx.x; e0 < kk; e0 += 4 * blockDim.x) {
+    double g[4];
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = e0 + u * blockDim.x;
+      g[u] = e < kk ? G[e] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+      const int e = e0 + u * blockDim.x;
+      if (e < kk) Gs[e] = g[u];
+    }
+  }
+  __syncthreads();
+}
+
 template <int KP>
 __device__ __forceinline__ void hals_warp_body(double* __restrict__ H, const double* __restrict__ M,
                                                const double* __restrict__ G, int64_t I, int k,
                                                int64_t bx) {
   constexpr int PER = KP / 32;
   __shared__ double Gs[KP * KP];
-  for (int e = threadIdx.x; e < k * k; e += blockDim.x) Gs[e] = G[e];
-  __syncthreads();
+  stage_gram(G, k, Gs);
   const int lane = threadIdx.x & 31;
   const int64_t row = bx * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (row >= I) return;
@@ -774,8 +846,7 @@ __device__ __forceinline__ void mu_warp_body(double* __restrict__ H, const doubl
                                              double eps, int64_t bx) {
   constexpr int PER = KP / 32;
   __shared__ double Gs[KP * KP];
-  for (int e = threadIdx.x; e < k * k; e += blockDim.x) Gs[e] = G[e];
-  __syncthreads();
+  stage_gram(G, k, Gs);
   const int lane = threadIdx.x & 31;
   const int64_t row = bx * (blockDim.x >> 5) + (threadIdx.x >> 5);
   if (row >= I) return;

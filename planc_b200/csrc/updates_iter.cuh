@@ -540,7 +540,20 @@ __device__ __forceinline__ void normgram_cluster_body(double* __restrict__ F, in
   for (int64_t c0 = r0; c0 < r1; c0 += NGC_TILE) {
     const int nrows = (int)((r1 - c0) < NGC_TILE ? (r1 - c0) : NGC_TILE);
     __syncthreads();
-    for (int e = tid; e < nrows * k; e += NGC_THREADS) tile[e] = F[c0 * k + e];
+    // eight loads in flight per thread before the stores
+    for (int e0 = tid; e0 < nrows * k; e0 += 8 * NGC_THREADS) {
+      double tv[8];
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int e = e0 + u * NGC_THREADS;
+        tv[u] = e < nrows * k ? F[c0 * k + e] : 0.0;
+      }
+#pragma unroll
+      for (int u = 0; u < 8; ++u) {
+        const int e = e0 + u * NGC_THREADS;
+        if (e < nrows * k) tile[e] = tv[u];
+      }
+    }
     __syncthreads();
     if (owner)
       for (int i = 0; i < nrows; ++i) {
@@ -589,9 +602,19 @@ __device__ __forceinline__ void normgram_cluster_body(double* __restrict__ F, in
   const double* gs = tile;
   if (tid < k) lam[tid] = sqrt(gs[tid * k + tid]);
   __syncthreads();
-  for (int64_t e = r0 * k + tid; e < r1 * k; e += NGC_THREADS) {
-    const double nrm = lam[e % k];
-    if (nrm > 0) F[e] = F[e] / nrm;
+  for (int64_t e0 = r0 * k + tid; e0 < r1 * k; e0 += 8 * NGC_THREADS) {
+    double fv[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int64_t e = e0 + (int64_t)u * NGC_THREADS;
+      fv[u] = e < r1 * k ? F[e] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      const int64_t e = e0 + (int64_t)u * NGC_THREADS;
+      const double nrm = lam[e % k];
+      if (e < r1 * k && nrm > 0) F[e] = fv[u] / nrm;
+    }
   }
   if (me != 0) return;
   if (tid < k && lambda) lambda[tid] = lam[tid];

@@ -206,3 +206,24 @@ def test_tc_direct_ntf_matches_fp64(gpu, prec, dims, k, algo):
         assert abs(c.objective_error() - e[-1]) < 1e-3
     bound = 1e-3 if prec == "bf16" else 1e-4
     assert abs(e[-1] - e64[-1]) < bound, (e[-1], e64[-1])
+
+
+@pytest.mark.parametrize("prec", ["bf16", "bf16x2"])
+@pytest.mark.parametrize("chunks", [1, 8, 1000])
+def test_tc_left_split_length_keeps_the_bound(gpu, oracle_lib, prec, chunks, monkeypatch):
+    # PLANC_GPU_LEFT_CHUNKS (the batch autotuner's split-K length of the left
+    # contraction) only reorders the FP32 partial sums: every mode stays
+    # within the precision's bound, for the generic (I0 % 64 != 0) and the
+    # factored (I0 % 64 == 0) left contraction
+    monkeypatch.setenv("PLANC_GPU_LEFT_CHUNKS", str(chunks))
+    for dims, k in (((40, 33, 96), 16), ((64, 20, 70), 32)):
+        X, _ = cp_tensor(dims, 4, seed=31)
+        F = init_factors(dims, k, seed=32)
+        Fn = _normalized(F)
+        with gpu.Context(0, prec) as c:
+            c.set_tensor(X)
+            c.set_factors(F)
+            for n in range(3):
+                ref = oracle_lib.mttkrp_direct(X, Fn, n)
+                got = c.mttkrp(n, dimtree=True)
+                assert rel(got, ref) < BOUND[prec], (dims, n, rel(got, ref))
