@@ -20,6 +20,8 @@ larger than the 126 MB L2 (DRAM counters stay meaningful):
           a one-pass launch list at full size
   cfg4it  the 256-tensor batched HALS workload (dims U{32..256}, ranks
           U{4,8,16,32}, BF16 copies), 3 + 3 batched iterations, no autotuning
+  cfg4small  the first 32 tensors of that workload (0.5 GB on the device),
+          for captures of the grouped kernels
   nmf     shared-memory NMF of a dense 16384 x 16384 FP32 matrix (BF16 copy),
           rank 32: three iterations each of MU, HALS and ANLS/BPP
   upd     AO-ADMM and Nesterov NTF updates on the 1024^3 rank-32 headline
@@ -203,14 +205,14 @@ def case_nes(gpu, torch):
     print("nes: 512^3 k=32 Nesterov: %.3f ms per iteration (8 in one call)" % ms)
 
 
-def case_cfg4it(gpu, torch):
+def case_cfg4it(gpu, torch, members=256):
     # the batched workload of 256 uneven 3-way FP32 tensors (dims U{32..256},
-    # ranks U{4,8,16,32}, BF16 copies), two HALS iterations without the
-    # autotuner: a launch list of one batched iteration's per-member kernels
+    # ranks U{4,8,16,32}, BF16 copies), HALS iterations without the
+    # autotuner: a launch list of one batched iteration's kernels
     import time
     rng = np.random.default_rng(401)
     specs = [(tuple(int(d) for d in rng.integers(32, 257, size=3)), int(rng.choice([4, 8, 16, 32])))
-             for _ in range(256)]
+             for _ in range(members)]
     b = gpu.Batch(0, "bf16", nstreams=64)
     for i, (dims, k) in enumerate(specs):
         r = np.random.default_rng(1000 + i)
@@ -228,12 +230,16 @@ def case_cfg4it(gpu, torch):
     t0 = time.perf_counter()
     b.run("hals", 3, compute_error=True)
     torch.cuda.synchronize()
-    print("cfg4it: 256 tensors, HALS: %.3f ms per batched iteration (3 iterations, untuned)"
-          % ((time.perf_counter() - t0) * 1e3 / 3))
+    print("cfg4it: %d tensors, HALS: %.3f ms per batched iteration (3 iterations, untuned)"
+          % (members, (time.perf_counter() - t0) * 1e3 / 3))
     b.close()
 
 
-CASES = {"bpp": case_bpp, "cfg4it": case_cfg4it, "f64": case_f64, "nes": case_nes, "tc3": case_tc3, "tc4": case_tc4, "cfg3it": case_cfg3it,
+def case_cfg4small(gpu, torch):
+    case_cfg4it(gpu, torch, members=32)
+
+
+CASES = {"bpp": case_bpp, "cfg4it": case_cfg4it, "cfg4small": case_cfg4small, "f64": case_f64, "nes": case_nes, "tc3": case_tc3, "tc4": case_tc4, "cfg3it": case_cfg3it,
          "ttv": case_ttv, "nmf": case_nmf, "upd": case_upd}
 
 
