@@ -171,3 +171,50 @@ def test_projected_accelerated_step_kernel(gpu):
     for a, b in zip(Y, refY):
         assert torch.allclose(a, b, rtol=0, atol=1e-14)
     lossf.close()
+
+
+@pytest.mark.parametrize("prec", ["fp64", "bf16"])
+def test_cp_loss_captures_as_cuda_graph(gpu, prec):
+    # forward + backward captured once on the loss's stream (static factor
+    # inputs, static loss and gradients) replay the eager computation's bits
+    import torch
+    X, F, lossf, Ft = _setup(prec, dims=(48, 40, 36), k=8, seed=51)
+    s = torch.cuda.ExternalStream(lossf.ctx.stream, device="cuda")
+    Ys = [f.detach().clone().requires_grad_(True) for f in Ft]
+    eager = []
+    with torch.cuda.stream(s):
+        for step in range(3):
+            for y in Ys:
+                y.grad = None
+            loss = lossf(*Ys)
+            loss.backward()
+            eager.append((loss.detach().clone(), [y.grad.clone() for y in Ys]))
+            with torch.no_grad():
+                for y in Ys:
+                    y.mul_(0.9)
+    torch.cuda.synchronize()
+    with torch.no_grad():
+        for y, f in zip(Ys, Ft):
+            y.copy_(f.detach())
+    for y in Ys:
+        y.grad = None
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph, stream=s, capture_error_mode="relaxed"):
+        static_loss = lossf(*Ys)
+        static_loss.backward()
+    grads = [y.grad for y in Ys]
+    with torch.no_grad():
+        for y, f in zip(Ys, Ft):
+            y.copy_(f.detach())
+    with torch.cuda.stream(s), torch.no_grad():
+        for step in range(3):
+            graph.replay()
+            torch.cuda.synchronize()
+            el, eg = eager[step]
+            assert torch.equal(static_loss, el), step
+            assert all(torch.equal(a, b) for a, b in zip(grads, eg)), step
+            for y in Ys:
+                y.mul_(0.9)
+    del graph
+    lossf.close()
