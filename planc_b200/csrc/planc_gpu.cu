@@ -208,6 +208,10 @@ struct planc_gpu_ctx {
   // fewest chunks per split-K partial of the tensor-core left contraction
   // (0: the default plan); the batch autotuner raises it for small members
   int left_chunks = 0;
+  // tensor tiles of the tensor-core right contraction through cp.async
+  // producer warps (default) or TMA (PLANC_GPU_TC_LOADS=tma); the left
+  // contractions always use TMA (their 128-byte row pieces stream faster so)
+  bool tc_cpa = true;
   // Incremented whenever a device buffer that a captured graph may reference
   // is (re)allocated; cached graphs are rebuilt when it changes.
   int64_t buf_epoch = 0;
@@ -813,7 +817,7 @@ void partial_right(planc_gpu_ctx* c) {
   } else {
     launch(c, KC_PREP, [&] { tc_right_prep(c->tct, c->F[c->N - 1], c->k, c->stream); });
     launch(c, KC_CONTRACT, [&] {
-      tc_right(c->tct, c->k, c->P32, c->status_dev, eff_sm(c), c->stream);
+      tc_right(c->tct, c->k, c->P32, c->status_dev, eff_sm(c), c->stream, c->tc_cpa);
     });
   }
 }
@@ -905,7 +909,7 @@ void mttkrp_dimtree(planc_gpu_ctx* c, int n, double* out) {
         launch(c, KC_PREP, [&] { tc_right_prep(c->tct, c->F[2], c->k, c->stream); });
         launch(c, KC_CONTRACT, [&] {
           tc_right_ttv(c->tct, c->k, c->P32, c->F[1], c->scratch, c->status_dev, eff_sm(c),
-                       c->stream);
+                       c->stream, c->tc_cpa);
         });
         const int64_t nn = c->dims[0] * c->k;
         launch(c, KC_REDUCE, [&] {
@@ -1463,6 +1467,12 @@ int planc_gpu_create(planc_gpu_ctx** out, int device, int precision, void* cuda_
     if (const char* e = getenv("PLANC_GPU_LEFT_CHUNKS")) {
       const int v = atoi(e);
       if (v >= 0 && v <= (1 << 20)) c->left_chunks = v;
+    }
+    // PLANC_GPU_TC_LOADS=tma|cpasync picks how the tensor-core right
+    // contraction fetches its tensor tiles, for contexts created while it is set
+    if (const char* e = getenv("PLANC_GPU_TC_LOADS")) {
+      if (!strcmp(e, "tma")) c->tc_cpa = false;
+      if (!strcmp(e, "cpasync")) c->tc_cpa = true;
     }
     // PLANC_GPU_BPP_KERNEL=warp|cta fixes the batched BPP kernel for contexts
     // created while it is set (default: chosen by the number of right-hand sides)
@@ -2596,7 +2606,8 @@ void batch_capture_grouped(planc_gpu_batch* b, int algo, bool err) {
       if (ns > 0 && (size_t)ns * I0 * k <= m->scratch_elems) {
         launch(m, KC_PREP, [&] { tc_right_prep(m->tct, m->F[2], k, m->stream); });
         launch(m, KC_CONTRACT, [&] {
-          tc_right_ttv(m->tct, k, m->P32, m->F[1], m->scratch, m->status_dev, eff_sm(m), m->stream);
+          tc_right_ttv(m->tct, k, m->P32, m->F[1], m->scratch, m->status_dev, eff_sm(m), m->stream,
+                       m->tc_cpa);
         });
         red.push_back(grp_red(m->scratch, ns, I0 * k, m->M[0]));
       } else {

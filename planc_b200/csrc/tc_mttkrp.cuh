@@ -245,6 +245,40 @@ __device__ __forceinline__ void split_bf16(double w, __nv_bfloat16& hi, __nv_bfl
 constexpr int TC_BM = 128;   // rows per MMA tile
 constexpr int TC_BK = 64;    // K per pipeline stage (one 128-byte swizzle row of BF16)
 constexpr int TC_THREADS = 192;  // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue / KRP producers
+// Stages of a TMA / cp.async ring of stage_bytes each in ~200 KB of shared
+// memory (2 .. 8).
+__host__ __device__ constexpr int tc_stages(uint32_t stage_bytes) {
+  return (int)(200u * 1024u / stage_bytes) < 2 ? 2
+         : (int)(200u * 1024u / stage_bytes) > 8 ? 8 : (int)(200u * 1024u / stage_bytes);
+}
+// cp.async groups (stages) each producer thread keeps in flight for a ring of
+// stage_bytes stages: up to 5, fewer than the ring holds; the cp.async
+// instances are used when this is at least 2.
+__host__ __device__ constexpr int tc_cpa_depth(uint32_t stage_bytes) {
+  return tc_stages(stage_bytes) - 1 < 5 ? tc_stages(stage_bytes) - 1 : 5;
+}
+
+// Shared memory the right contraction's four epilogue warps stage their rows
+// of P in (32 rows of KP floats each), after the stage ring; the 16-column
+// instance stores directly.
+template <int KP>
+__host__ __device__ constexpr uint32_t tc_right_pstage() {
+  return KP >= 32 ? 4u * 32u * (uint32_t)KP * 4u : 0u;
+}
+
+// 16-byte cp.async (L1 bypassed) that reads `bytes` (0..16) from src and
+// zero-fills the rest of the destination; src must be 16-byte aligned.
+__device__ __forceinline__ void cp_async16_zfill(uint32_t dst, const void* src, uint32_t bytes) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;" ::"r"(dst), "l"(src), "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
 
 // ------------------------------------------------------------ right kernel
 // P32[l*k + r] = sum_j X[l, j] * F[j, r], l < L, r < k.
@@ -256,12 +290,25 @@ constexpr int TC_THREADS = 192;  // warp 0 TMA, warp 1 MMA, warps 2-5 epilogue /
 //   sum_{i1 of its tiles} P[i0 + I0 i1, r] * F1[i1, r]   (FP64)
 // and writes them to part[blockIdx / tpb][i0][r]; k_reduce_splits adds the
 // gridDim / tpb partials into M_0 (the sum k_ttv_right_tiled forms from P).
-template <int KP, bool X2, bool TTV = false>
-__global__ void __launch_bounds__(TC_THREADS, 1)
+//
+// With CPA the A tiles are not fetched by TMA: four more warps (6-9) copy
+// them with 16-byte cp.async into the same 128B-swizzled MN-major layout,
+// tc_cpa_depth(STAGE) stages of copies in flight per thread (on B200 this
+// streams the 256-byte row pieces of a tile ~15 % faster than two {64, 64}
+// TMA boxes). Each producer thread waits for its oldest group, makes it
+// visible to the tensor cores' async proxy and arrives on the stage's full
+// barrier (count 1 + 128: warp 0's B-image expect_tx and the 128 producers).
+// Rows l >= L and columns j >= R are zero-filled through the copy's source
+// size. Needs stages = tc_stages(STAGE) and a row stride Lpad that is a
+// multiple of 8.
+template <int KP, bool X2, bool TTV = false, bool CPA = false>
+__global__ void __launch_bounds__(CPA ? TC_THREADS + 128 : TC_THREADS, 1)
     k_tc_right(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
                const uint8_t* __restrict__ bimg, int64_t L, int64_t R, int k, int stages,
                float* __restrict__ P, int* __restrict__ status, const double* __restrict__ F1 = nullptr,
-               int tpb = 1, int64_t I0 = 0, double* __restrict__ part = nullptr) {
+               int tpb = 1, int64_t I0 = 0, double* __restrict__ part = nullptr,
+               const __nv_bfloat16* __restrict__ xhi = nullptr,
+               const __nv_bfloat16* __restrict__ xlo = nullptr, int64_t Lpad = 0) {
   constexpr int NCOL = 2 * KP;                       // hi | lo columns
   constexpr uint32_t A_BYTES = TC_BM * TC_BK * 2;    // one BF16 A tile
   constexpr uint32_t A_STAGE = X2 ? 2 * A_BYTES : A_BYTES;
@@ -270,6 +317,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   constexpr int NBUF = 4;  // accumulators in flight
   constexpr uint32_t TMEM_COLS = NBUF * NCOL < 32 ? 32 : NBUF * NCOL;
   constexpr uint32_t IDESC = idesc_bf16(NCOL, true, false);
+  // P staging of one epilogue warp, after the stage ring (0: direct stores)
+  constexpr uint32_t PST_BYTES = tc_right_pstage<KP>() / 4;
+  constexpr int DEPTH = tc_cpa_depth(STAGE);
 
   extern __shared__ uint8_t smem_raw[];
   __shared__ uint64_t bars[2 * 8 + 2 * NBUF];
@@ -288,7 +338,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   if (threadIdx.x == 0) {
     abort_sh = 0;
     for (int s = 0; s < stages; ++s) {
-      mbar_init(full(s), 1);
+      mbar_init(full(s), CPA ? 1 + 128 : 1);
       mbar_init(empty(s), 1);
     }
     for (int b = 0; b < NBUF; ++b) {
@@ -313,12 +363,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         for (int kb = 0; kb < nk; ++kb) {
           if (!mbar_wait(empty(s), ph ^ 1, abort_flag, status)) { ok = false; break; }
           const uint32_t st = smem0 + s * STAGE;
-          mbar_expect_tx(full(s), STAGE);
-          tma_load_2d(st, &tm_hi, l0, kb * TC_BK, full(s));
-          tma_load_2d(st + A_BYTES / 2, &tm_hi, l0 + 64, kb * TC_BK, full(s));
-          if (X2) {
-            tma_load_2d(st + A_BYTES, &tm_lo, l0, kb * TC_BK, full(s));
-            tma_load_2d(st + A_BYTES + A_BYTES / 2, &tm_lo, l0 + 64, kb * TC_BK, full(s));
+          if (CPA) {
+            mbar_expect_tx(full(s), B_STAGE);
+          } else {
+            mbar_expect_tx(full(s), STAGE);
+            tma_load_2d(st, &tm_hi, l0, kb * TC_BK, full(s));
+            tma_load_2d(st + A_BYTES / 2, &tm_hi, l0 + 64, kb * TC_BK, full(s));
+            if (X2) {
+              tma_load_2d(st + A_BYTES, &tm_lo, l0, kb * TC_BK, full(s));
+              tma_load_2d(st + A_BYTES + A_BYTES / 2, &tm_lo, l0 + 64, kb * TC_BK, full(s));
+            }
           }
           bulk_load(st + A_STAGE, bimg + (size_t)kb * B_STAGE, B_STAGE, full(s));
           if (++s == stages) { s = 0; ph ^= 1; }
@@ -360,7 +414,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         buf = (buf + 1) % NBUF;
       }
     }
-  } else {
+  } else if (warp < 6) {
     // epilogue warps 2..5: TMEM lane quarter = warp % 4
     const int q = warp & 3;
     int buf = 0;
@@ -372,35 +426,65 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       if (!mbar_wait(accf(buf), (aph >> buf) & 1, abort_flag, status)) break;
       tc_fence_after();
       const int64_t row = t * TC_BM + q * 32 + lane;
-      float v[NCOL];
+      const uint32_t tacc_addr = tmem + ((uint32_t)(q * 32) << 16) + buf * NCOL;
+      // with k == KP (KP >= 32) the warp's 32 rows of P are one contiguous
+      // block: they are staged in shared memory (row lane's 16-byte chunk c
+      // at c ^ (lane % 8), no bank conflicts) and written back with coalesced
+      // stores; otherwise each thread stores its row. The accumulator is
+      // drained 16 columns at a time.
+      const bool staged = PST_BYTES > 0 && k == KP;
+      uint8_t* sp = smem + (size_t)stages * STAGE + (size_t)(warp - 2) * PST_BYTES;
+      const double* f = TTV ? F1 + (t / tpb) * k : nullptr;
 #pragma unroll
-      for (int c = 0; c < NCOL; c += 32)
-        tmem_ld32(tmem + ((uint32_t)(q * 32) << 16) + buf * NCOL + c, v + c);
+      for (int h = 0; h < KP / 16; ++h) {
+        float a[16], b[16];
+        tmem_ld16(tacc_addr + h * 16, a);
+        tmem_ld16(tacc_addr + KP + h * 16, b);
+        if (staged) {
+#pragma unroll
+          for (int c = 0; c < 4; ++c) {
+            const float4 o = make_float4(a[4 * c] + b[4 * c], a[4 * c + 1] + b[4 * c + 1],
+                                         a[4 * c + 2] + b[4 * c + 2], a[4 * c + 3] + b[4 * c + 3]);
+            *reinterpret_cast<float4*>(sp + lane * (KP * 4) + (((h * 4 + c) ^ (lane & 7)) << 4)) = o;
+          }
+        } else if (row < L) {
+          float* dst = P + row * k + h * 16;
+          if (k == KP) {
+#pragma unroll
+            for (int c = 0; c < 4; ++c)
+              *reinterpret_cast<float4*>(dst + 4 * c) =
+                  make_float4(a[4 * c] + b[4 * c], a[4 * c + 1] + b[4 * c + 1],
+                              a[4 * c + 2] + b[4 * c + 2], a[4 * c + 3] + b[4 * c + 3]);
+          } else {
+#pragma unroll
+            for (int r = 0; r < 16; ++r)
+              if (h * 16 + r < k) dst[r] = a[r] + b[r];
+          }
+        }
+        if constexpr (TTV) {
+          if (row < L) {
+#pragma unroll
+            for (int r = 0; r < 16; ++r)
+              if (h * 16 + r < k)
+                tacc[h * 16 + r] = fma((double)(a[r] + b[r]), f[h * 16 + r], tacc[h * 16 + r]);
+          }
+        }
+      }
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive(acce(buf));
       aph ^= 1u << buf;
       buf = (buf + 1) % NBUF;
-      if (row < L) {
-        float* dst = P + row * k;
-        if (k == KP && (KP % 4) == 0) {
+      if (staged) {
+        const int64_t row0 = t * TC_BM + q * 32;
 #pragma unroll
-          for (int r = 0; r < KP; r += 4) {
-            float4 o = make_float4(v[r] + v[KP + r], v[r + 1] + v[KP + r + 1],
-                                   v[r + 2] + v[KP + r + 2], v[r + 3] + v[KP + r + 3]);
-            *reinterpret_cast<float4*>(dst + r) = o;
-          }
-        } else {
-#pragma unroll
-          for (int r = 0; r < KP; ++r)
-            if (r < k) dst[r] = v[r] + v[KP + r];
+        for (int it = 0; it < KP / 4; ++it) {
+          const int u = it * 32 + lane;  // 16-byte unit of the block
+          const int j = u / (KP / 4), c = u % (KP / 4);
+          const float4 o = *reinterpret_cast<const float4*>(sp + j * (KP * 4) + ((c ^ (j & 7)) << 4));
+          if (row0 + j < L) *reinterpret_cast<float4*>(P + (row0 + j) * KP + 4 * c) = o;
         }
-        if constexpr (TTV) {
-          const double* f = F1 + (t / tpb) * k;
-#pragma unroll
-          for (int r = 0; r < KP; ++r)
-            if (r < k) tacc[r] = fma((double)(v[r] + v[KP + r]), f[r], tacc[r]);
-        }
+        __syncwarp();
       }
     }
     if constexpr (TTV) {
@@ -410,6 +494,55 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       for (int r = 0; r < KP; ++r)
         if (r < k) dst[r] = tacc[r];
     }
+  } else if (CPA) {
+    // A-tile producers, warps 6..9: per stage 1024 (2048 with X2) copies of
+    // 16 bytes; copy q = pt + 128 i takes the 16-byte piece c16 = q % 16 of
+    // row j = q / 16 of the K block (l = l0 + 8 c16), which lands in box
+    // c16 / 8, chunk (c16 % 8) ^ (j % 8) of the swizzled row j
+    // (c16 and j % 8 are fixed per thread: its copies step 8 rows = 1 KB)
+    const int pt = threadIdx.x - TC_THREADS;
+    const int c16 = pt & 15, jt = pt >> 4;
+    const uint32_t dofs = (uint32_t)(c16 >> 3) * (A_BYTES / 2) + (uint32_t)jt * 128u +
+                          ((uint32_t)((c16 & 7) ^ jt) << 4);
+    int s = 0;
+    uint32_t ph = 0;
+    int inflight = 0;  // copy groups committed, not yet announced
+    int ps = 0;        // stage of the oldest of them (groups go in stage order)
+    bool ok = true;
+    for (int64_t t = blockIdx.x; t < ntiles && ok; t += gridDim.x) {
+      const int64_t l = t * TC_BM + 8 * c16;
+      const int64_t left = L - l;
+      const uint32_t lbytes = left <= 0 ? 0u : left >= 8 ? 16u : (uint32_t)left * 2u;
+      for (int kb = 0; kb < nk; ++kb) {
+        if (!mbar_wait(empty(s), ph ^ 1, abort_flag, status)) { ok = false; break; }
+        const uint32_t dst = smem0 + s * STAGE + dofs;
+        const int64_t j0 = (int64_t)kb * TC_BK + jt;
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const int64_t jj = j0 + 8 * i;
+          const uint32_t bytes = jj < R ? lbytes : 0u;
+          const size_t off = bytes ? (size_t)jj * (size_t)Lpad + (size_t)l : 0;
+          cp_async16_zfill(dst + 1024u * i, xhi + off, bytes);
+          if (X2) cp_async16_zfill(dst + 1024u * i + A_BYTES, xlo + off, bytes);
+        }
+        cp_async_commit();
+        if (++inflight > DEPTH) {
+          cp_async_wait<DEPTH>();
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          mbar_arrive(full(ps));
+          if (++ps == stages) ps = 0;
+          --inflight;
+        }
+        if (++s == stages) { s = 0; ph ^= 1; }
+      }
+    }
+    cp_async_wait<0>();
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (ok)
+      for (; inflight > 0; --inflight) {
+        mbar_arrive(full(ps));
+        if (++ps == stages) ps = 0;
+      }
   }
   __syncthreads();
   if (abort_sh) tc_drain_after_abort();
@@ -1470,11 +1603,6 @@ inline cudaError_t tc_direct_copy(TcTensor& dst, const TcTensor& src, const int6
   return ok ? cudaSuccess : cudaErrorInvalidValue;
 }
 
-inline int tc_stages(uint32_t stage_bytes) {
-  const uint32_t budget = 200 * 1024;
-  int s = (int)(budget / stage_bytes);
-  return s < 2 ? 2 : (s > 8 ? 8 : s);
-}
 
 // j-tiles per CTA of the left contraction: 2 when R > 128, except at the
 // 64-wide rank (keeps the drain warps' running sums in registers)
@@ -1510,11 +1638,18 @@ inline cudaError_t tc_set_attrs() {
   constexpr uint32_t SR = (X2 ? 2 : 1) * TC_BM * TC_BK * 2 + 2 * KP * 128;
   constexpr uint32_t SL1 = (X2 ? 2 : 1) * 1 * TC_BM * TC_BK * 2 + 2 * KP * 128;
   constexpr uint32_t SL2 = (X2 ? 2 : 1) * 2 * TC_BM * TC_BK * 2 + 2 * KP * 128;
-  cudaError_t e = cudaFuncSetAttribute(k_tc_right<KP, X2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)(tc_stages(SR) * SR + 1024));
-  if (e == cudaSuccess && KP <= 32)
-    e = cudaFuncSetAttribute(k_tc_right<KP, X2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)(tc_stages(SR) * SR + 1024));
+  const int smr = (int)(tc_stages(SR) * SR + tc_right_pstage<KP>() + 1024);
+  cudaError_t e = cudaFuncSetAttribute(k_tc_right<KP, X2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smr);
+  if (e == cudaSuccess && tc_cpa_depth(SR) >= 2)
+    e = cudaFuncSetAttribute(k_tc_right<KP, X2, false, true>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, smr);
+  if constexpr (KP <= 32) {  // the multi-TTV instances (rank <= 32)
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_tc_right<KP, X2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smr);
+    if (e == cudaSuccess && tc_cpa_depth(SR) >= 2)
+      e = cudaFuncSetAttribute(k_tc_right<KP, X2, true, true>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, smr);
+  }
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_tc_left<KP, 1, X2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(tc_stages(SL1) * SL1 + 1024));
@@ -1588,16 +1723,24 @@ inline void tc_right_prep(const TcTensor& t, const double* F, int k, cudaStream_
     k_tc_bimage<64><<<blocks, 256, 0, st>>>(F, t.R, k, nk, t.bimg);
 }
 
+// cpa: A tiles through cp.async producer warps (when the stage ring holds at
+// least 3 stages) instead of TMA; the same shared-memory image, hence the
+// same results.
 template <int KP, bool X2>
 inline void tc_right_launch(const TcTensor& t, int k, float* P, int* status, int sm_count,
-                            cudaStream_t st) {
+                            cudaStream_t st, bool cpa) {
   constexpr uint32_t STAGE = (X2 ? 2 : 1) * TC_BM * TC_BK * 2 + 2 * KP * 128;
   const int stages = tc_stages(STAGE);
-  const size_t smem = (size_t)stages * STAGE + 1024;
+  const size_t smem = (size_t)stages * STAGE + tc_right_pstage<KP>() + 1024;
   const int64_t ntiles = (t.L + TC_BM - 1) / TC_BM;
   const int grid = (int)std::min<int64_t>(ntiles, sm_count);
-  k_tc_right<KP, X2><<<grid, TC_THREADS, smem, st>>>(t.mR_hi, t.mR_lo, t.bimg, t.L, t.R, k, stages,
-                                                     P, status);
+  if (cpa && tc_cpa_depth(STAGE) >= 2)
+    k_tc_right<KP, X2, false, true><<<grid, TC_THREADS + 128, smem, st>>>(
+        t.mR_hi, t.mR_lo, t.bimg, t.L, t.R, k, stages, P, status, nullptr, 1, 0, nullptr, t.hi,
+        t.lo, t.Lpad);
+  else
+    k_tc_right<KP, X2><<<grid, TC_THREADS, smem, st>>>(t.mR_hi, t.mR_lo, t.bimg, t.L, t.R, k,
+                                                       stages, P, status);
 }
 
 // Whether the mode-0 multi-TTV can ride on the right contraction: 3-way
@@ -1620,41 +1763,46 @@ inline int tc_right_ttv_nsplit(const TcTensor& t, int k, int sm_count) {
 
 template <int KP, bool X2>
 inline void tc_right_ttv_launch(const TcTensor& t, int k, float* P, const double* F1, double* part,
-                                int* status, int sm_count, cudaStream_t st) {
+                                int* status, int sm_count, cudaStream_t st, bool cpa) {
   constexpr uint32_t STAGE = (X2 ? 2 : 1) * TC_BM * TC_BK * 2 + 2 * KP * 128;
   const int stages = tc_stages(STAGE);
-  const size_t smem = (size_t)stages * STAGE + 1024;
+  const size_t smem = (size_t)stages * STAGE + tc_right_pstage<KP>() + 1024;
   const int tpb = tc_right_ttv_tpb(t, k, sm_count);
   const int grid = tc_right_ttv_nsplit(t, k, sm_count) * tpb;
-  k_tc_right<KP, X2, true><<<grid, TC_THREADS, smem, st>>>(t.mR_hi, t.mR_lo, t.bimg, t.L, t.R, k,
-                                                           stages, P, status, F1, tpb, t.I0, part);
+  if (cpa && tc_cpa_depth(STAGE) >= 2)
+    k_tc_right<KP, X2, true, true><<<grid, TC_THREADS + 128, smem, st>>>(
+        t.mR_hi, t.mR_lo, t.bimg, t.L, t.R, k, stages, P, status, F1, tpb, t.I0, part, t.hi, t.lo,
+        t.Lpad);
+  else
+    k_tc_right<KP, X2, true><<<grid, TC_THREADS, smem, st>>>(t.mR_hi, t.mR_lo, t.bimg, t.L, t.R, k,
+                                                             stages, P, status, F1, tpb, t.I0, part);
 }
 
 // P32 = X * F_{N-1} and the mode-0 multi-TTV partials against F1
 // (tc_right_ttv_tpb(...) != 0; call tc_right_prep first). Returns nsplit.
 inline int tc_right_ttv(const TcTensor& t, int k, float* P, const double* F1, double* part,
-                        int* status, int sm_count, cudaStream_t st) {
+                        int* status, int sm_count, cudaStream_t st, bool cpa = true) {
   const bool x2 = t.prec == 2;
   if (tc_kpad(k) == 16)
-    x2 ? tc_right_ttv_launch<16, true>(t, k, P, F1, part, status, sm_count, st)
-       : tc_right_ttv_launch<16, false>(t, k, P, F1, part, status, sm_count, st);
+    x2 ? tc_right_ttv_launch<16, true>(t, k, P, F1, part, status, sm_count, st, cpa)
+       : tc_right_ttv_launch<16, false>(t, k, P, F1, part, status, sm_count, st, cpa);
   else
-    x2 ? tc_right_ttv_launch<32, true>(t, k, P, F1, part, status, sm_count, st)
-       : tc_right_ttv_launch<32, false>(t, k, P, F1, part, status, sm_count, st);
+    x2 ? tc_right_ttv_launch<32, true>(t, k, P, F1, part, status, sm_count, st, cpa)
+       : tc_right_ttv_launch<32, false>(t, k, P, F1, part, status, sm_count, st, cpa);
   return tc_right_ttv_nsplit(t, k, sm_count);
 }
 
 // P32 = X * F_{N-1} on the tensor cores (call tc_right_prep first).
 inline void tc_right(const TcTensor& t, int k, float* P, int* status, int sm_count,
-                     cudaStream_t st) {
+                     cudaStream_t st, bool cpa = true) {
   const bool x2 = t.prec == 2;
   switch (tc_kpad(k)) {
-    case 16: x2 ? tc_right_launch<16, true>(t, k, P, status, sm_count, st)
-                : tc_right_launch<16, false>(t, k, P, status, sm_count, st); break;
-    case 32: x2 ? tc_right_launch<32, true>(t, k, P, status, sm_count, st)
-                : tc_right_launch<32, false>(t, k, P, status, sm_count, st); break;
-    default: x2 ? tc_right_launch<64, true>(t, k, P, status, sm_count, st)
-                : tc_right_launch<64, false>(t, k, P, status, sm_count, st); break;
+    case 16: x2 ? tc_right_launch<16, true>(t, k, P, status, sm_count, st, cpa)
+                : tc_right_launch<16, false>(t, k, P, status, sm_count, st, cpa); break;
+    case 32: x2 ? tc_right_launch<32, true>(t, k, P, status, sm_count, st, cpa)
+                : tc_right_launch<32, false>(t, k, P, status, sm_count, st, cpa); break;
+    default: x2 ? tc_right_launch<64, true>(t, k, P, status, sm_count, st, cpa)
+                : tc_right_launch<64, false>(t, k, P, status, sm_count, st, cpa); break;
   }
 }
 
