@@ -208,9 +208,11 @@ struct planc_gpu_ctx {
   // fewest chunks per split-K partial of the tensor-core left contraction
   // (0: the default plan); the batch autotuner raises it for small members
   int left_chunks = 0;
-  // tensor tiles of the tensor-core right contraction through cp.async
-  // producer warps (default) or TMA (PLANC_GPU_TC_LOADS=tma); the left
-  // contractions always use TMA (their 128-byte row pieces stream faster so)
+  // parts per run of I0 of the factored left contraction's work units
+  // (PLANC_GPU_LEFT_PARTS; 0: the default)
+  int left_parts = 0;
+  // tensor tiles of the tensor-core right and factored left contractions
+  // through cp.async producer warps (default) or TMA (PLANC_GPU_TC_LOADS=tma)
   bool tc_cpa = true;
   // Incremented whenever a device buffer that a captured graph may reference
   // is (re)allocated; cached graphs are rebuilt when it changes.
@@ -1468,8 +1470,16 @@ int planc_gpu_create(planc_gpu_ctx** out, int device, int precision, void* cuda_
       const int v = atoi(e);
       if (v >= 0 && v <= (1 << 20)) c->left_chunks = v;
     }
-    // PLANC_GPU_TC_LOADS=tma|cpasync picks how the tensor-core right
-    // contraction fetches its tensor tiles, for contexts created while it is set
+    // PLANC_GPU_LEFT_PARTS=n splits each run of the factored left
+    // contraction into n work units (a divisor of I0 / 64) for contexts
+    // created while it is set
+    if (const char* e = getenv("PLANC_GPU_LEFT_PARTS")) {
+      const int v = atoi(e);
+      if (v >= 1 && v <= 1024) c->left_parts = v;
+    }
+    // PLANC_GPU_TC_LOADS=tma|cpasync picks how the tensor-core right and
+    // factored left contractions fetch their tensor tiles, for contexts
+    // created while it is set
     if (const char* e = getenv("PLANC_GPU_TC_LOADS")) {
       if (!strcmp(e, "tma")) c->tc_cpa = false;
       if (!strcmp(e, "cpasync")) c->tc_cpa = true;
@@ -1596,6 +1606,8 @@ int planc_gpu_set_tensor(planc_gpu_ctx* c, const void* X, int dtype, const int64
         c->x64_elems = 0;
       }
       CK(tc_prepare(c->tct, c->L, c->R, c->dims[0], c->precision));
+      c->tct.left_parts = c->left_parts > 0 ? c->left_parts : 1;
+      c->tct.left_cpa = c->tc_cpa;
     }
     for (int64_t e0 = 0; e0 < numel; e0 += chunk) {
       const int64_t n = std::min<int64_t>(chunk, numel - e0);

@@ -849,22 +849,55 @@ __global__ void __launch_bounds__(TCL_THREADS, 1)
 // as in the right contraction); the accumulator of each run g is drained and
 // scaled by tail(g, .) in FP64 by four drain warps. No producer warps, and the
 // tensor-core accumulation chain is one run (I_0/64 chunks) long.
-// Split y takes runs y, y + nsplit, ..., so concurrent CTAs read adjacent
-// I_0-element pieces of the same rows of X.
+// Work units are parts of runs: with hp parts per run, unit u covers chunks
+// (u % hp) * G/hp .. of run u / hp (the accumulator is restarted and scaled
+// per unit, which the sum allows since tail(g, r) is common to the run).
+// Split y takes units y, y + nsplit, ..., so concurrent CTAs read adjacent
+// pieces of the same rows of X.
 constexpr int TCF_THREADS = 192;  // warp 0 TMA, 1 MMA, 2-5 drain
 
-template <int KP, int MT, bool X2>
-__global__ void __launch_bounds__(TCF_THREADS, 1)
+// Shared-memory stage of k_tc_left_fac: KBS 64-wide K blocks of MT 128-row
+// A tiles (a second set for the lo part with X2) and KBS B slabs.
+__host__ __device__ constexpr uint32_t tcf_stage_bytes(int kp, int mt, bool x2, int kbs) {
+  return (x2 ? 2u : 1u) * kbs * mt * (uint32_t)(TC_BM * TC_BK * 2) + kbs * 2u * kp * 128u;
+}
+
+// With CPA (MT = 1) the A tiles come from four cp.async producer warps
+// (6-9) instead of TMA: 16-byte copies written to the swizzled positions,
+// zero-filled past R. A copy group fills a pair of stages (two consecutive
+// K blocks), so each warp-wide copy reads two 256-byte row pieces of X (on
+// B200 cp.async streams this pattern at ~6.9 TB/s, 128-byte pieces at ~4.9
+// and TMA boxes of any shape at ~6.0); tcf_cpa_depth(stages) pairs are in
+// flight per thread (2: at 1024^3 rank 32 the kernel takes 0.340 ms with 2,
+// 0.363 with 1 and 0.54 with 3), which leaves stages to spare for the MMAs'
+// turnaround. Warp 0 then loads only the B slab of a stage, and the full
+// barrier counts its expect_tx and the 128 producers. Needs an even number
+// of stages and units of an even number of chunks.
+__host__ __device__ constexpr int tcf_cpa_depth(int stages) { return stages / 2 - 1 < 2 ? stages / 2 - 1 : 2; }
+// Whether the cp.async instance exists for (KP, X2): rank <= 32 (the drain
+// warps' sums within the 10-warp register budget) and an even ring of at
+// least 6 stages.
+__host__ __device__ constexpr bool tcf_cpa_ok(int kp, bool x2) {
+  return kp <= 32 && tc_stages(tcf_stage_bytes(kp, 1, x2, 1)) % 2 == 0 &&
+         tcf_cpa_depth(tc_stages(tcf_stage_bytes(kp, 1, x2, 1))) >= 2;
+}
+template <int KP, int MT, bool X2, bool CPA = false>
+__global__ void __launch_bounds__(CPA ? TCF_THREADS + 128 : TCF_THREADS, 1)
     k_tc_left_fac(const __grid_constant__ CUtensorMap tm_hi, const __grid_constant__ CUtensorMap tm_lo,
                   const uint8_t* __restrict__ img0, const double* __restrict__ F1,
                   const double* __restrict__ F2, int64_t D1, int64_t I0, int64_t L, int64_t R, int k,
-                  int stages, double* __restrict__ part, int* __restrict__ status) {
+                  int stages, double* __restrict__ part, int* __restrict__ status, int hp = 1,
+                  const __nv_bfloat16* __restrict__ xhi = nullptr,
+                  const __nv_bfloat16* __restrict__ xlo = nullptr, int64_t Lpad = 0) {
+  static_assert(!CPA || MT == 1, "the cp.async instance takes one 128-row tile");
+  constexpr int KBS = 1;                           // K blocks per stage
   constexpr int NCOL = 2 * KP;
   constexpr uint32_t A_TILE = TC_BM * TC_BK * 2;  // 16 KB
-  constexpr uint32_t A_BYTES = MT * A_TILE;
+  constexpr uint32_t A_BYTES = KBS * MT * A_TILE;  // tile (kb, mt) at (kb * MT + mt) * A_TILE
   constexpr uint32_t A_STAGE = X2 ? 2 * A_BYTES : A_BYTES;
-  constexpr uint32_t B_STAGE = NCOL * 128;
-  constexpr uint32_t STAGE = A_STAGE + B_STAGE;
+  constexpr uint32_t B_STAGE = NCOL * 128;         // one slab of the F_0 image
+  constexpr uint32_t STAGE = A_STAGE + KBS * B_STAGE;
+  static_assert(STAGE == tcf_stage_bytes(KP, MT, X2, KBS), "stage layout");
   constexpr uint32_t ACC_COLS = MT * NCOL;
   constexpr int NBUF = 4 * ACC_COLS <= 512 ? 4 : 2;  // accumulators in flight
   constexpr uint32_t TMEM_NEED = NBUF * ACC_COLS;
@@ -882,10 +915,11 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
   const uint32_t smem0 = smem_u32(smem);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int64_t G = I0 / TC_BK;          // chunks per run
-  const int64_t nruns = L / I0;
+  const int64_t GH = G / hp;             // chunks per unit (a part of a run)
+  const int64_t nunits = L / I0 * hp;
   const int64_t ns = gridDim.y;
   const int64_t y = blockIdx.y;
-  const int64_t my_runs = y < nruns ? (nruns - y + ns - 1) / ns : 0;
+  const int64_t my_units = y < nunits ? (nunits - y + ns - 1) / ns : 0;
   const int j0 = blockIdx.x * MT * TC_BM;
   auto full = [&](int s) { return smem_u32(&bars[s]); };
   auto empty = [&](int s) { return smem_u32(&bars[8 + s]); };
@@ -895,7 +929,7 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
   if (threadIdx.x == 0) {
     abort_sh = 0;
     for (int s = 0; s < stages; ++s) {
-      mbar_init(full(s), 1);
+      mbar_init(full(s), CPA ? 1 + 128 : 1);
       mbar_init(empty(s), 1);
     }
     for (int b = 0; b < NBUF; ++b) {
@@ -915,18 +949,22 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
       int s = 0;
       uint32_t ph = 0;
       bool ok = true;
-      for (int64_t i = 0; i < my_runs && ok; ++i) {
-        const int64_t g = y + i * ns;
-        for (int64_t q = 0; q < G; ++q) {
-          const int64_t c = g * G + q;
+      for (int64_t i = 0; i < my_units && ok; ++i) {
+        const int64_t u = y + i * ns;
+        for (int64_t q = (u % hp) * GH, qe = q + GH; q < qe; q += KBS) {
+          const int64_t c = (u / hp) * G + q;
           if (!mbar_wait(empty(s), ph ^ 1, abort_flag, status)) { ok = false; break; }
           const uint32_t st = smem0 + s * STAGE;
-          mbar_expect_tx(full(s), STAGE);
-          for (int mt = 0; mt < MT; ++mt) {
-            tma_load_2d(st + mt * A_TILE, &tm_hi, (int)(c * TC_BK), j0 + mt * TC_BM, full(s));
-            if (X2) tma_load_2d(st + A_BYTES + mt * A_TILE, &tm_lo, (int)(c * TC_BK), j0 + mt * TC_BM, full(s));
+          if (CPA) {
+            mbar_expect_tx(full(s), KBS * B_STAGE);
+          } else {
+            mbar_expect_tx(full(s), STAGE);
+            for (int mt = 0; mt < MT; ++mt) {
+              tma_load_2d(st + mt * A_TILE, &tm_hi, (int)(c * TC_BK), j0 + mt * TC_BM, full(s));
+              if (X2) tma_load_2d(st + A_BYTES + mt * A_TILE, &tm_lo, (int)(c * TC_BK), j0 + mt * TC_BM, full(s));
+            }
           }
-          bulk_load(st + A_STAGE, img0 + (size_t)q * B_STAGE, B_STAGE, full(s));
+          bulk_load(st + A_STAGE, img0 + (size_t)q * B_STAGE, KBS * B_STAGE, full(s));
           if (++s == stages) { s = 0; ph ^= 1; }
         }
       }
@@ -937,28 +975,28 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
       uint32_t ph = 0;
       uint32_t aph = 0;  // bit b: phase of accumulator b
       bool ok = true;
-      for (int64_t i = 0; i < my_runs && ok; ++i) {
+      for (int64_t i = 0; i < my_units && ok; ++i) {
         const int buf = (int)(i % NBUF);
         if (!mbar_wait(acce(buf), ((aph >> buf) & 1) ^ 1, abort_flag, status)) break;
         tc_fence_after();
         const uint32_t d = tmem + buf * ACC_COLS;
-        for (int64_t q = 0; q < G; ++q) {
+        for (int64_t q = 0; q < GH; q += KBS) {
           if (!mbar_wait(full(s), ph, abort_flag, status)) { ok = false; break; }
           tc_fence_after();
           const uint32_t st = smem0 + s * STAGE;
 #pragma unroll
-          for (int kk = 0; kk < TC_BK / 16; ++kk) {
-            const uint64_t bdesc = smem_desc(st + A_STAGE + kk * 32, 16, 1024);
+          for (int kb = 0; kb < KBS; ++kb)
 #pragma unroll
-            for (int mt = 0; mt < MT; ++mt) {
-              const uint64_t adesc = smem_desc(st + mt * A_TILE + kk * 32, 16, 1024);
-              umma_bf16(d + mt * NCOL, adesc, bdesc, IDESC, (q != 0 || kk != 0) ? 1u : 0u);
-              if (X2) {
-                const uint64_t adesc2 = smem_desc(st + A_BYTES + mt * A_TILE + kk * 32, 16, 1024);
-                umma_bf16(d + mt * NCOL, adesc2, bdesc, IDESC, 1);
+            for (int kk = 0; kk < TC_BK / 16; ++kk) {
+              const uint64_t bdesc = smem_desc(st + A_STAGE + kb * B_STAGE + kk * 32, 16, 1024);
+#pragma unroll
+              for (int mt = 0; mt < MT; ++mt) {
+                const uint32_t at = st + (kb * MT + mt) * A_TILE + kk * 32;
+                umma_bf16(d + mt * NCOL, smem_desc(at, 16, 1024), bdesc, IDESC,
+                          (q != 0 || kb != 0 || kk != 0) ? 1u : 0u);
+                if (X2) umma_bf16(d + mt * NCOL, smem_desc(at + A_BYTES, 16, 1024), bdesc, IDESC, 1);
               }
             }
-          }
           umma_commit(empty(s));
           if (++s == stages) { s = 0; ph ^= 1; }
         }
@@ -967,7 +1005,7 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
         aph ^= 1u << buf;
       }
     }
-  } else {
+  } else if (warp < 6) {
     // drain warps 2..5: TMEM lane quarter = warp % 4. Each warp stages the
     // run's tail(g, .) in its own shared-memory slice (no cross-warp wait).
     const int q4 = warp & 3;
@@ -979,9 +1017,9 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
       for (int r = 0; r < KP; ++r) sum[mt][r] = 0;
     uint32_t aph = 0;
     bool ok = true;
-    for (int64_t i = 0; i < my_runs; ++i) {
+    for (int64_t i = 0; i < my_units; ++i) {
       const int buf = (int)(i % NBUF);
-      const int64_t g = y + i * ns;
+      const int64_t g = (y + i * ns) / hp;
       const int64_t i1 = F2 ? g % D1 : g;
       const int64_t i2 = F2 ? g / D1 : 0;
       __syncwarp();
@@ -1034,6 +1072,60 @@ __global__ void __launch_bounds__(TCF_THREADS, 1)
         }
       }
     }
+  } else if (CPA) {
+    // A-tile producers, warps 6..9: per pair of stages 2048 (x2 with X2)
+    // copies of 16 bytes; copy u = pt + 128 i takes the 16-byte piece
+    // p = u % 16 (l = 64 c + 8 p, chunk c of the pair's first stage) of tile
+    // row u / 16 (j = j0 + u / 16), which lands in stage p / 8 of the pair,
+    // chunk (p % 8) ^ (row % 8) of the swizzled row. p and row % 8 are fixed
+    // per thread: its copies step 8 rows = 1 KB.
+    constexpr int DEPTH = tcf_cpa_depth(tc_stages(STAGE));
+    static_assert(!CPA || (tc_stages(STAGE) % 2 == 0 && DEPTH >= 2), "stage pairs");
+    const int pt = threadIdx.x - TCF_THREADS;
+    const int p = pt & 15, jt = pt >> 4;
+    const uint32_t dofs = (uint32_t)(p >> 3) * STAGE + (uint32_t)jt * 128u + ((uint32_t)((p & 7) ^ jt) << 4);
+    int s = 0;  // first stage of the pair (even)
+    uint32_t ph = 0;
+    int inflight = 0;  // copy groups (pairs) committed, not yet announced
+    int ps = 0;        // first stage of the oldest of them
+    bool ok = true;
+    for (int64_t i = 0; i < my_units && ok; ++i) {
+      const int64_t u = y + i * ns;
+      for (int64_t q = (u % hp) * GH, qe = q + GH; q < qe; q += 2) {
+        if (!mbar_wait(empty(s), ph ^ 1, abort_flag, status) ||
+            !mbar_wait(empty(s + 1), ph ^ 1, abort_flag, status)) { ok = false; break; }
+        const uint32_t dst = smem0 + s * STAGE + dofs;
+        const int64_t l = ((u / hp) * G + q) * TC_BK + 8 * p;
+        const int64_t left = L - l;
+        const uint32_t lbytes = left <= 0 ? 0u : left >= 8 ? 16u : (uint32_t)left * 2u;
+#pragma unroll
+        for (int i8 = 0; i8 < 16; ++i8) {
+          const int64_t j = (int64_t)j0 + jt + 8 * i8;
+          const uint32_t bytes = j < R ? lbytes : 0u;
+          const size_t off = bytes ? (size_t)j * (size_t)Lpad + (size_t)l : 0;
+          cp_async16_zfill(dst + 1024u * i8, xhi + off, bytes);
+          if (X2) cp_async16_zfill(dst + 1024u * i8 + A_BYTES, xlo + off, bytes);
+        }
+        cp_async_commit();
+        if (++inflight > DEPTH) {
+          cp_async_wait<DEPTH>();
+          asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          mbar_arrive(full(ps));
+          mbar_arrive(full(ps + 1));
+          if ((ps += 2) == stages) ps = 0;
+          --inflight;
+        }
+        if ((s += 2) == stages) { s = 0; ph ^= 1; }
+      }
+    }
+    cp_async_wait<0>();
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    if (ok)
+      for (; inflight > 0; --inflight) {
+        mbar_arrive(full(ps));
+        mbar_arrive(full(ps + 1));
+        if ((ps += 2) == stages) ps = 0;
+      }
   }
   __syncthreads();
   if (abort_sh) tc_drain_after_abort();
@@ -1457,6 +1549,8 @@ struct TcTensor {
   int kpad = 0;
   int64_t I0 = 0;            // mode-0 size (factored left contraction when I0 % 64 == 0)
   int left_nf = 0;           // factors of the left contraction's Khatri-Rao generator
+  int left_parts = 1;        // parts each run of I0 splits into (factored left contraction)
+  bool left_cpa = false;     // factored left contraction through cp.async producers when it applies
   uint8_t* wimg = nullptr;   // Khatri-Rao image of the long-K kernel (k_tc_long)
   size_t wimg_bytes = 0;
   int64_t wimg_K = 0;        // longest K it must hold (0: long-K kernel unused)
@@ -1515,6 +1609,12 @@ inline int tc_left_gen_nf(int listed) { return (listed == 2 || listed == 3) ? li
 // or two factors.
 inline bool tc_left_factored(const TcTensor& t) {
   return t.I0 > 0 && t.I0 % TC_BK == 0 && t.left_nf >= 2 && t.left_nf <= 3;
+}
+// Parts per run of the factored left contraction's work units: left_parts
+// when it divides the run's I0 / 64 chunks, else 1.
+inline int tc_left_hp(const TcTensor& t) {
+  const int64_t G = t.I0 / TC_BK;
+  return (t.left_parts > 1 && G > 0 && G % t.left_parts == 0) ? t.left_parts : 1;
 }
 
 // Storage of the BF16 view (L rows, R columns, row stride L rounded up to 8)
@@ -1581,6 +1681,8 @@ inline cudaError_t tc_direct_copy(TcTensor& dst, const TcTensor& src, const int6
   dst.prec = src.prec;
   dst.I0 = dims[n == 0 ? 1 : 0];
   dst.left_nf = tc_left_gen_nf(N - 1);
+  dst.left_parts = src.left_parts;
+  dst.left_cpa = src.left_cpa;
   const size_t cnt = (size_t)d.Lppad * dims[n];
   cudaError_t e = cudaMalloc(&dst.hi, cnt * 2);
   if (e != cudaSuccess) return e;
@@ -1608,16 +1710,27 @@ inline cudaError_t tc_direct_copy(TcTensor& dst, const TcTensor& src, const int6
 // 64-wide rank (keeps the drain warps' running sums in registers)
 inline int tc_left_mt(int64_t R, int k) { return (R > 128 && k <= 32) ? 2 : 1; }
 
+// Whether the factored left contraction runs its cp.async instance (one
+// 128-row tile a CTA): asked for (left_cpa), rank <= 32 (the drain warps'
+// sums within the 10-warp register budget), units of an even number of
+// chunks and an even ring of at least 6 stages.
+inline bool tc_left_cpa(const TcTensor& t, int k) {
+  if (!t.left_cpa || !tc_left_factored(t) || !tcf_cpa_ok(tc_kpad(k), t.prec == 2)) return false;
+  return (t.I0 / TC_BK / tc_left_hp(t)) % 2 == 0;
+}
+// j-tiles per CTA of the contraction tc_left launches for t
+inline int tc_left_tiles(const TcTensor& t, int k) { return tc_left_cpa(t, k) ? 1 : tc_left_mt(t.R, k); }
+
 // min_units > 0 caps the split count so that every split takes at least
 // that many chunks (runs): fewer, longer splits for small tensors whose
 // parallelism comes from elsewhere (a grouped batch)
 inline void tc_left_plan(const TcTensor& t, int k, int sm_count, int* mgroups, int* nsplit,
                          int min_units = 0) {
-  const int MT = tc_left_mt(t.R, k);
+  const int MT = tc_left_tiles(t, k);
   *mgroups = (int)((t.R + MT * TC_BM - 1) / (MT * TC_BM));
   int ns = sm_count / *mgroups;
   if (ns < 1) ns = 1;
-  const int64_t units = tc_left_factored(t) ? t.L / t.I0 : (t.L + TC_BK - 1) / TC_BK;
+  const int64_t units = tc_left_factored(t) ? t.L / t.I0 * tc_left_hp(t) : (t.L + TC_BK - 1) / TC_BK;
   if (ns > units) ns = (int)units;
   if (min_units > 0) {
     const int64_t cap = (units + min_units - 1) / min_units;
@@ -1662,6 +1775,12 @@ inline cudaError_t tc_set_attrs() {
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_tc_left_fac<KP, 2, X2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(tc_stages(SL2) * SL2 + 1024));
+  if constexpr (tcf_cpa_ok(KP, X2)) {
+    constexpr uint32_t SC = tcf_stage_bytes(KP, 1, X2, 1);
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_tc_left_fac<KP, 1, X2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)(tc_stages(SC) * SC + 1024));
+  }
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(k_tc_long<KP, 1, X2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(tc_stages(SL1) * SL1 + 1024));
@@ -1820,8 +1939,21 @@ inline void tc_left_launch(const TcTensor& t, const WGen& wg, int k, double* par
     k_tc_bimage<KP><<<(unsigned)std::min<int64_t>(((int64_t)nslab * KP * TC_BK + 255) / 256, 1024),
                       256, 0, st>>>(wg.f[0], t.I0, k, nslab, t.bimg0);
     const double* F2 = wg.nf > 2 ? wg.f[2] : nullptr;
-    k_tc_left_fac<KP, MT, X2><<<dim3(mg, ns), TCF_THREADS, smem, st>>>(
-        t.mL_hi, t.mL_lo, t.bimg0, wg.f[1], F2, wg.dim[1], t.I0, t.L, t.R, k, stages, part, status);
+    bool done = false;
+    if constexpr (MT == 1 && tcf_cpa_ok(KP, X2)) {
+      if (tc_left_cpa(t, k)) {
+        constexpr uint32_t SC = tcf_stage_bytes(KP, 1, X2, 1);
+        k_tc_left_fac<KP, 1, X2, true><<<dim3(mg, ns), TCF_THREADS + 128, (size_t)tc_stages(SC) * SC + 1024,
+                                         st>>>(t.mL_hi, t.mL_lo, t.bimg0, wg.f[1], F2, wg.dim[1], t.I0, t.L,
+                                               t.R, k, tc_stages(SC), part, status, tc_left_hp(t), t.hi,
+                                               t.lo, t.Lpad);
+        done = true;
+      }
+    }
+    if (!done)
+      k_tc_left_fac<KP, MT, X2><<<dim3(mg, ns), TCF_THREADS, smem, st>>>(
+          t.mL_hi, t.mL_lo, t.bimg0, wg.f[1], F2, wg.dim[1], t.I0, t.L, t.R, k, stages, part, status,
+          tc_left_hp(t));
   } else {
     k_tc_left<KP, MT, X2><<<dim3(mg, ns), TCL_THREADS, smem, st>>>(t.mL_hi, t.mL_lo, wg, t.L, t.R, k,
                                                                    stages, part, status);
@@ -1833,7 +1965,7 @@ inline void tc_left_launch(const TcTensor& t, const WGen& wg, int k, double* par
 inline int tc_left(const TcTensor& t, const WGen& wg, int k, double* part, int* status,
                    int sm_count, cudaStream_t st, int min_units = 0) {
   const bool x2 = t.prec == 2;
-  const int MT = tc_left_mt(t.R, k);
+  const int MT = tc_left_tiles(t, k);
   int ns = 1;
 #define TCL(KP)                                                                                  \
   if (MT == 2) {                                                                                 \

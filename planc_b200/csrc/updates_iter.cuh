@@ -495,9 +495,9 @@ __global__ void __launch_bounds__(256) k_colnorm_apply(double* __restrict__ U, i
 // c of the entries over the cluster's CTAs in rank order and stores the sums
 // into every CTA's copy of the Gram (distributed shared memory); after a
 // second barrier every CTA holds the same Gram, takes lambda_r =
-// sqrt((U^T U)_rr) and divides its own rows by lambda, and CTA 0 writes
-// lambda, G_n = (U^T U)_ab / (lambda_a lambda_b) and the leave-one-out
-// product. Meant for factors of up to NGC_MAX_ROWS rows, where three launches
+// sqrt((U^T U)_rr), divides its own rows by lambda and writes its slice of
+// G_n = (U^T U)_ab / (lambda_a lambda_b) and of the leave-one-out product;
+// CTA 0 writes lambda. Meant for factors of up to NGC_MAX_ROWS rows, where three launches
 // cost more than the work.
 constexpr int NGC_THREADS = 256;
 constexpr int NGC_TILE = 64;          // rows of a shared-memory tile
@@ -602,35 +602,43 @@ __device__ __forceinline__ void normgram_cluster_body(double* __restrict__ F, in
   const double* gs = tile;
   if (tid < k) lam[tid] = sqrt(gs[tid * k + tid]);
   __syncthreads();
-  for (int64_t e0 = r0 * k + tid; e0 < r1 * k; e0 += 8 * NGC_THREADS) {
-    double fv[8];
+  {
+    // a thread keeps one column c of rows r0 + rr, r0 + rr + rstep, ...
+    const int rstep = NGC_THREADS / k;
+    const int c = tid % k;
+    const int64_t rr = tid / k;
+    const double nrm = lam[c];
+    if (rr < rstep && nrm > 0)
+      for (int64_t ra = r0 + rr; ra < r1; ra += 8 * (int64_t)rstep) {
+        double fv[8];
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int64_t e = e0 + (int64_t)u * NGC_THREADS;
-      fv[u] = e < r1 * k ? F[e] : 0.0;
-    }
+        for (int u = 0; u < 8; ++u) {
+          const int64_t r = ra + (int64_t)u * rstep;
+          fv[u] = r < r1 ? F[r * k + c] : 0.0;
+        }
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
-      const int64_t e = e0 + (int64_t)u * NGC_THREADS;
-      const double nrm = lam[e % k];
-      if (e < r1 * k && nrm > 0) F[e] = fv[u] / nrm;
-    }
+        for (int u = 0; u < 8; ++u) {
+          const int64_t r = ra + (int64_t)u * rstep;
+          if (r < r1) F[r * k + c] = fv[u] / nrm;
+        }
+      }
   }
-  if (me != 0) return;
-  if (tid < k && lambda) lambda[tid] = lam[tid];
+  if (me == 0 && tid < k && lambda) lambda[tid] = lam[tid];
+  // G_n and the leave-one-out product: CTA me writes its slice of the entries
+  const int sl = (kk2 + CL - 1) / CL;
+  const int e0 = me * sl, e1 = (e0 + sl) < kk2 ? (e0 + sl) : kk2;
   double* Gn = Gall + (int64_t)n * kk2;
-  for (int e = tid; e < kk2; e += NGC_THREADS) {
+  for (int e = e0 + tid; e < e1; e += NGC_THREADS) {
     const int a = e / k, b = e % k;
     const double la = lam[a], lb = lam[b];
-    Gn[e] = (la > 0 && lb > 0) ? gs[e] / (la * lb) : gs[e];
-  }
-  if (next < 0) return;
-  __syncthreads();
-  for (int e = tid; e < kk2; e += NGC_THREADS) {
-    double g = 1.0;
-    for (int i = 0; i < N; ++i)
-      if (i != next) g = g * Gall[(int64_t)i * kk2 + e];
-    Gloo[e] = g;
+    const double gn = (la > 0 && lb > 0) ? gs[e] / (la * lb) : gs[e];
+    Gn[e] = gn;
+    if (next >= 0) {
+      double g = 1.0;
+      for (int i = 0; i < N; ++i)
+        if (i != next) g = g * (i == n ? gn : Gall[(int64_t)i * kk2 + e]);
+      Gloo[e] = g;
+    }
   }
 }
 template <int BE>

@@ -230,16 +230,22 @@ def test_tc_left_split_length_keeps_the_bound(gpu, oracle_lib, prec, chunks, mon
 
 
 @pytest.mark.parametrize("prec", ["bf16", "bf16x2"])
-def test_tc_tile_loads_give_the_same_bits(gpu, prec, monkeypatch):
-    # the right contraction's tensor tiles through cp.async producer warps
-    # (PLANC_GPU_TC_LOADS=cpasync) or TMA: the same shared-memory image and
-    # the same MMAs, so the same bits. Shapes cover ragged rows (L = I0*I1 not
-    # a multiple of 8 or of 128), ragged K (I2 < 64, I2 % 64 != 0), ranks of
-    # the 16-, 32- and 64-column instances, the fused mode-0 multi-TTV
-    # (I0 % 128 == 0), and the direct (non-tree) MTTKRP of every mode
+def test_tc_tile_loads_agree(gpu, prec, monkeypatch):
+    # the tensor tiles of the right and factored left contractions through
+    # cp.async producer warps (PLANC_GPU_TC_LOADS=cpasync) or TMA. The right
+    # contraction fills the same shared-memory image and runs the same MMAs,
+    # so mode 0 (formed from it alone) has the same bits; the factored left
+    # contraction's cp.async instance takes one 128-row tile a CTA (TMA: two
+    # when R > 128), so its split-K partials are summed in another order
+    # (FP64, relative 1e-12). Shapes cover ragged rows (L = I0*I1 not a
+    # multiple of 8 or of 128), ragged K (I2 < 64, I2 % 64 != 0), ranks of the
+    # 16-, 32- and 64-column instances, the fused mode-0 multi-TTV
+    # (I0 % 128 == 0), the factored left contraction (I0 % 64 == 0; I0 = 64 has
+    # runs of one chunk, which the cp.async instance does not take) with ragged
+    # j, and the direct (non-tree) MTTKRP of every mode
     cases = [((13, 7, 20), 5), ((40, 33, 21), 32), ((130, 3, 300), 16), ((256, 40, 50), 16),
              ((384, 17, 23), 24), ((9, 8, 7, 10), 64), ((64, 20, 90), 40), ((128, 12, 300), 32),
-             ((64, 10, 200), 64)]
+             ((64, 10, 200), 16), ((256, 6, 333), 8)]
     for dims, k in cases:
         X, _ = cp_tensor(dims, 4, seed=33)
         F = init_factors(dims, k, seed=34)
@@ -254,6 +260,7 @@ def test_tc_tile_loads_give_the_same_bits(gpu, prec, monkeypatch):
                 e = c.run("hals", 3)
                 res[loads] = (ms, e, c.get_factors()[0])
         (m1, e1, f1), (m2, e2, f2) = res["tma"], res["cpasync"]
-        assert all(np.array_equal(a, b) for a, b in zip(m1, m2)), dims
-        assert np.array_equal(e1, e2), dims
-        assert all(np.array_equal(a, b) for a, b in zip(f1, f2)), dims
+        assert np.array_equal(m1[0], m2[0]), dims
+        assert all(rel(a, b) < 1e-12 for a, b in zip(m1, m2)), (dims, [rel(a, b) for a, b in zip(m1, m2)])
+        assert np.max(np.abs(np.asarray(e1) - np.asarray(e2))) < 1e-10, dims
+        assert all(rel(a, b) < 1e-8 for a, b in zip(f1, f2)), dims
