@@ -160,14 +160,24 @@ def traffic_from_profiles(precision, dims, k, which):
     return None
 
 
-def left_splits(L, R, I0, k, sm_count):
+def left_splits(L, R, I0, k, sm_count, precision="bf16"):
     """Split-K count of the 3-way left contraction, as the library plans it
-    (tc_left_plan: 128-row tiles, two per CTA when R > 128 and k <= 32, the
-    SMs shared among the row groups, at most one split per run of I_0 rows)."""
-    mt = 2 if (R > 128 and k <= 32) else 1
+    (tc_left_plan: 128-row tiles, two per CTA when R > 128 and k <= 32 except
+    for the factored contraction's cp.async instance (I_0 % 64 == 0, rank <= 32,
+    BF16, an even number of 64-wide chunks per work unit), which takes one;
+    the SMs shared among the row groups, at most one split per work unit:
+    a run of I_0 rows, or a part of one with PLANC_GPU_LEFT_PARTS)."""
+    factored = I0 % 64 == 0
+    hp = int(os.environ.get("PLANC_GPU_LEFT_PARTS", "1") or 1)
+    if not factored or hp < 1 or (I0 // 64) % hp != 0:
+        hp = 1
+    kpad = 16 if k <= 16 else 32 if k <= 32 else 64
+    cpa = (factored and kpad <= 32 and precision == "bf16" and (I0 // 64 // hp) % 2 == 0
+           and os.environ.get("PLANC_GPU_TC_LOADS", "cpasync") != "tma")
+    mt = 1 if cpa else (2 if (R > 128 and k <= 32) else 1)
     groups = -(-R // (mt * 128))
     ns = max(1, sm_count // groups)
-    units = L // I0 if I0 % 64 == 0 else -(-L // 64)
+    units = L // I0 * hp if factored else -(-L // 64)
     return min(ns, units)
 
 
@@ -337,7 +347,8 @@ def main():
     # writes P in FP32; left: X^T*KRP, writes split-K FP64 partials)
     L = dims[0] * dims[1]
     R = numel // L
-    nsplit_left = left_splits(L, R, dims[0], k, torch.cuda.get_device_properties(dev).multi_processor_count)
+    nsplit_left = left_splits(L, R, dims[0], k, torch.cuda.get_device_properties(dev).multi_processor_count,
+                              args.precision)
     kern = {
         "right": (kt["contract"], numel * EB[args.precision] + L * k * 4),
         "left": (kt["contract_left"], numel * EB[args.precision] + nsplit_left * R * k * 8),

@@ -1156,22 +1156,14 @@ __device__ __forceinline__ void error_body(const double* __restrict__ Mlast,
   const int r = tid % k, lane = tid / k, lanes = 1024 / k;
   double inner = 0.0;
   if (lane < lanes) {
-    // eight rows' loads in flight, four running sums (row u of a batch goes
-    // to sum u % 4)
-    double s[4] = {0.0, 0.0, 0.0, 0.0};
+    double s0 = 0.0, s1 = 0.0;
     int64_t i = lane;
-    for (; i + 7 * lanes < I; i += 8 * lanes) {
-      double m[8], f[8];
-#pragma unroll
-      for (int u = 0; u < 8; ++u) {
-        m[u] = Mlast[(i + u * lanes) * k + r];
-        f[u] = Flast[(i + u * lanes) * k + r];
-      }
-#pragma unroll
-      for (int u = 0; u < 8; ++u) s[u & 3] = fma(m[u], f[u], s[u & 3]);
+    for (; i + lanes < I; i += 2 * lanes) {
+      s0 = fma(Mlast[i * k + r], Flast[i * k + r], s0);
+      s1 = fma(Mlast[(i + lanes) * k + r], Flast[(i + lanes) * k + r], s1);
     }
-    for (int u = 0; i < I; i += lanes, ++u) s[u & 3] = fma(Mlast[i * k + r], Flast[i * k + r], s[u & 3]);
-    inner = ((s[0] + s[1]) + (s[2] + s[3])) * lambda[r];
+    if (i < I) s0 = fma(Mlast[i * k + r], Flast[i * k + r], s0);
+    inner = (s0 + s1) * lambda[r];
   }
   double mn = 0.0;
   for (int e = tid; e < k * k; e += 1024) {
