@@ -252,10 +252,11 @@ __host__ __device__ constexpr int tc_stages(uint32_t stage_bytes) {
          : (int)(200u * 1024u / stage_bytes) > 8 ? 8 : (int)(200u * 1024u / stage_bytes);
 }
 // cp.async groups (stages) each producer thread keeps in flight for a ring of
-// stage_bytes stages: up to 5, fewer than the ring holds; the cp.async
-// instances are used when this is at least 2.
+// stage_bytes stages: up to 5, leaving at least 3 stages for the MMAs'
+// turnaround (with one or two to spare the producers wait on the MMAs); the
+// cp.async instances are used when this is at least 2.
 __host__ __device__ constexpr int tc_cpa_depth(uint32_t stage_bytes) {
-  return tc_stages(stage_bytes) - 1 < 5 ? tc_stages(stage_bytes) - 1 : 5;
+  return tc_stages(stage_bytes) - 3 < 5 ? tc_stages(stage_bytes) - 3 : 5;
 }
 
 // Shared memory the right contraction's four epilogue warps stage their rows
@@ -868,12 +869,12 @@ __host__ __device__ constexpr uint32_t tcf_stage_bytes(int kp, int mt, bool x2, 
 // K blocks), so each warp-wide copy reads two 256-byte row pieces of X (on
 // B200 cp.async streams this pattern at ~6.9 TB/s, 128-byte pieces at ~4.9
 // and TMA boxes of any shape at ~6.0); tcf_cpa_depth(stages) pairs are in
-// flight per thread (2: at 1024^3 rank 32 the kernel takes 0.340 ms with 2,
-// 0.363 with 1 and 0.54 with 3), which leaves stages to spare for the MMAs'
-// turnaround. Warp 0 then loads only the B slab of a stage, and the full
+// flight per thread (up to 2, leaving at least two pairs for the MMAs'
+// turnaround: at 1024^3 rank 32, an 8-stage ring, the kernel takes 0.340 ms
+// with 2, 0.363 with 1 and 0.54 with 3). Warp 0 then loads only the B slab of a stage, and the full
 // barrier counts its expect_tx and the 128 producers. Needs an even number
 // of stages and units of an even number of chunks.
-__host__ __device__ constexpr int tcf_cpa_depth(int stages) { return stages / 2 - 1 < 2 ? stages / 2 - 1 : 2; }
+__host__ __device__ constexpr int tcf_cpa_depth(int stages) { return stages / 2 - 2 < 2 ? stages / 2 - 2 : 2; }
 // Whether the cp.async instance exists for (KP, X2): rank <= 32 (the drain
 // warps' sums within the 10-warp register budget) and an even ring of at
 // least 6 stages.
