@@ -127,10 +127,18 @@ __device__ __forceinline__ double wgen_at32(const WGen& wg, const FastDiv& f0, c
   }
 }
 
-template <int KP, bool LEFT, int NF>
+// RUNS (LEFT, NF = 2 or 3): the reduction index is laid out as runs of
+// g.A = dim[0] values of the fastest generator mode (g.B = the runs, g.ldb =
+// g.A), so every reduction tile lies in one run b and its Khatri-Rao rows are
+// W(a + A b, r) = F_0[a, r] * tail(b, r), tail = F_1[b, r] (NF = 2) or
+// F_1[i1, r] * F_2[i2, r] with b = i1 + dim[1] i2 (NF = 3): a thread takes
+// tail once per tile, then one F_0 load and one multiply per entry (the same
+// products as wgen_at, so the same W).
+template <int KP, bool LEFT, int NF, bool RUNS = false>
 __global__ void __launch_bounds__(256, 2) k_contract_f64(const double* __restrict__ X,
                                                          ContractGeom g, WGen wg, int k,
                                                          double* __restrict__ out) {
+  static_assert(!RUNS || (LEFT && (NF == 2 || NF == 3)), "runs of the fastest mode");
   constexpr int BK = ct_bk<KP>();
   constexpr int XPT = BK * CT_BM / 256;  // X elements per thread per tile
   constexpr int WPT = (BK * KP + 255) / 256;
@@ -156,7 +164,7 @@ __global__ void __launch_bounds__(256, 2) k_contract_f64(const double* __restric
   // Khatri-Rao row indices fit 32-bit digit arithmetic
   const bool small_rows = (LEFT ? g.A * g.B : g.A) < ((int64_t)1 << 31);
   FastDiv fd0{1, 1, 0}, fd1{1, 1, 0};
-  if (NF >= 2 && small_rows) {
+  if (NF >= 2 && small_rows && !RUNS) {
     fd0 = make_fastdiv((uint32_t)wg.dim[0]);
     if (NF >= 3) fd1 = make_fastdiv((uint32_t)wg.dim[1]);
   }
@@ -244,6 +252,29 @@ __global__ void __launch_bounds__(256, 2) k_contract_f64(const double* __restric
         }
       }
       const int64_t wrow0 = a0 + g.A * b;
+      if constexpr (RUNS) {
+        // 256 is a multiple of KP: entry i of this thread is row
+        // a = a0 + tid / KP + (256 / KP) i, rank r = tid % KP
+        const int r = tid % KP;
+        const int64_t a = a0 + tid / KP;
+        double tail = 0.0;
+        if (r < k) {
+          if (NF == 2) {
+            tail = wg.f[1][b * k + r];
+          } else {
+            const int64_t i2 = b / wg.dim[1], i1 = b - i2 * wg.dim[1];
+            tail = wg.f[1][i1 * k + r] * wg.f[2][i2 * k + r];
+          }
+        }
+        const double* fp = wg.f[0] + a * k + r;
+        const int64_t fstep = (int64_t)(256 / KP) * k;
+#pragma unroll
+        for (int i = 0; i < WPT; ++i) {
+          wr[i] = (r < k && a + (256 / KP) * i < g.A) ? *fp * tail : 0.0;
+          fp += fstep;
+        }
+        return;
+      }
       if constexpr (NF == 2 || NF == 3) {
         if (small_rows) {
           // 256 is a multiple of KP: entry i of this thread is row

@@ -576,8 +576,18 @@ void ensure_buffers_impl(planc_gpu_ctx* c) {
 // other count takes the generic generator)
 template <int KP, bool LEFT>
 void launch_contract_f64(dim3 grid, cudaStream_t st, const double* X, const ContractGeom& g,
-                         const WGen& wg, int k, double* dst) {
+                         const WGen& wg, int k, double* dst, bool runs = false) {
   constexpr size_t sm = ct_smem_bytes<KP, LEFT>();
+  if constexpr (LEFT) {
+    if (runs && wg.nf == 2) {
+      k_contract_f64<KP, true, 2, true><<<grid, 256, sm, st>>>(X, g, wg, k, dst);
+      return;
+    }
+    if (runs && wg.nf == 3) {
+      k_contract_f64<KP, true, 3, true><<<grid, 256, sm, st>>>(X, g, wg, k, dst);
+      return;
+    }
+  }
   switch (wg.nf) {
     case 1: k_contract_f64<KP, LEFT, 1><<<grid, 256, sm, st>>>(X, g, wg, k, dst); break;
     case 2: k_contract_f64<KP, LEFT, 2><<<grid, 256, sm, st>>>(X, g, wg, k, dst); break;
@@ -593,6 +603,10 @@ void contract_f64_attrs_kp() {
   CK(cudaFuncSetAttribute(k_contract_f64<KP, LEFT, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   CK(cudaFuncSetAttribute(k_contract_f64<KP, LEFT, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   CK(cudaFuncSetAttribute(k_contract_f64<KP, LEFT, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  if constexpr (LEFT) {
+    CK(cudaFuncSetAttribute(k_contract_f64<KP, true, 2, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+    CK(cudaFuncSetAttribute(k_contract_f64<KP, true, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  }
 }
 
 // Dynamic shared-memory limits of every k_contract_f64 instance (up to 92 KB)
@@ -614,7 +628,7 @@ void contract_f64_attrs(int dev) {
 }
 
 void run_contract(planc_gpu_ctx* c, const ContractPlan& p, bool left, const double* X,
-                  const WGen& wg, double* out) {
+                  const WGen& wg, double* out, bool runs = false) {
   const int k = c->k;
   if (contract_scratch(p) > c->scratch_elems)
     fail(PLANC_GPU_ERR_STATE, "internal: contraction scratch larger than planned");
@@ -624,7 +638,7 @@ void run_contract(planc_gpu_ctx* c, const ContractPlan& p, bool left, const doub
 #define CASE(KP)                                                                      \
   case KP:                                                                            \
     if (left)                                                                         \
-      launch_contract_f64<KP, true>(p.grid, c->stream, X, p.g, wg, k, dst);           \
+      launch_contract_f64<KP, true>(p.grid, c->stream, X, p.g, wg, k, dst, runs);     \
     else                                                                              \
       launch_contract_f64<KP, false>(p.grid, c->stream, X, p.g, wg, k, dst);          \
     break;
@@ -805,8 +819,10 @@ void mttkrp_direct(planc_gpu_ctx* c, int n, double* out) {
     ContractPlan p = plan_contract(c, false, c->dims[0], c->dims[0], B, 1, 0);
     run_contract(c, p, false, c->X64, wg, out);
   } else {
+    // mode 1: the reduction index is already runs of I_0 (A = I_0), so each
+    // tile takes one Khatri-Rao tail of the slower modes
     ContractPlan p = plan_contract(c, true, c->dims[n], A, A, B, A * c->dims[n]);
-    run_contract(c, p, true, c->X64, wg, out);
+    run_contract(c, p, true, c->X64, wg, out, n == 1 && (wg.nf == 2 || wg.nf == 3));
   }
 }
 
@@ -830,8 +846,13 @@ void partial_left(planc_gpu_ctx* c, double* out) {
   for (int m = 0; m <= c->s; ++m) modes.push_back(m);
   if (c->precision == PLANC_GPU_PREC_FP64) {
     WGen wg = make_wgen(c, modes);
-    ContractPlan p = plan_contract(c, true, c->R, c->L, c->L, 1, 0);
-    run_contract(c, p, true, c->X64, wg, out);
+    // reduction tiles aligned to runs of I_0 (the same tiles and splits as the
+    // flat view when I_0 is a multiple of the tile): one Khatri-Rao tail per tile
+    const int64_t bk = kpad(c->k) == 64 ? ct_bk<64>() : ct_bk<32>();
+    const bool runs = (wg.nf == 2 || wg.nf == 3) && c->dims[0] % bk == 0;
+    ContractPlan p = runs ? plan_contract(c, true, c->R, c->L, c->dims[0], c->L / c->dims[0], c->dims[0])
+                          : plan_contract(c, true, c->R, c->L, c->L, 1, 0);
+    run_contract(c, p, true, c->X64, wg, out, runs);
   } else {
     WGen wg = make_wgen(c, modes);
     int nsplit = 0;
