@@ -558,8 +558,35 @@ __device__ __forceinline__ void ttv_left_f4_body(const float* __restrict__ T, in
 #pragma unroll
     for (int c = 0; c < 4; ++c) acc[j][c] = 0.0;
   if (active) {
-#pragma unroll 4
-    for (int64_t a = rl; a < A; a += RL) {
+    // rows a, a + RL, a + 2 RL: every load of the three rows is issued
+    // before the first product (then one row at a time for the rest; three
+    // rows' values fill the 64 registers of four CTAs an SM)
+    constexpr int U = 3;
+    int64_t a = rl;
+    for (; a + (U - 1) * RL < A; a += U * RL) {
+      double2 f01[U], f23[U];
+      float4 t[U][TTVL_NB];
+#pragma unroll
+      for (int u = 0; u < U; ++u) {
+        const int64_t au = a + u * RL;
+        f01[u] = *reinterpret_cast<const double2*>(F + au * k + 4 * r4);
+        f23[u] = *reinterpret_cast<const double2*>(F + au * k + 4 * r4 + 2);
+#pragma unroll
+        for (int j = 0; j < TTVL_NB; ++j)
+          t[u][j] = j < nb ? *reinterpret_cast<const float4*>(T + (au + A * (b0 + j)) * k + 4 * r4)
+                           : make_float4(0.f, 0.f, 0.f, 0.f);
+      }
+#pragma unroll
+      for (int u = 0; u < U; ++u)
+#pragma unroll
+        for (int j = 0; j < TTVL_NB; ++j) {
+          acc[j][0] = fma((double)t[u][j].x, f01[u].x, acc[j][0]);
+          acc[j][1] = fma((double)t[u][j].y, f01[u].y, acc[j][1]);
+          acc[j][2] = fma((double)t[u][j].z, f23[u].x, acc[j][2]);
+          acc[j][3] = fma((double)t[u][j].w, f23[u].y, acc[j][3]);
+        }
+    }
+    for (; a < A; a += RL) {
       const double2 f01 = *reinterpret_cast<const double2*>(F + a * k + 4 * r4);
       const double2 f23 = *reinterpret_cast<const double2*>(F + a * k + 4 * r4 + 2);
       float4 t[TTVL_NB];
