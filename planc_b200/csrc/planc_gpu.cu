@@ -211,6 +211,10 @@ struct planc_gpu_ctx {
   // parts per run of I0 of the factored left contraction's work units
   // (PLANC_GPU_LEFT_PARTS; 0: the default)
   int left_parts = 0;
+  // 3-way tensor-core left contraction without the factored form (I_0 not a
+  // multiple of 64): against a Khatri-Rao image with the long-K kernel
+  // (default) or with Khatri-Rao producer warps (PLANC_GPU_LEFT_FORM=producers)
+  bool left_long = true;
   // tensor tiles of the tensor-core right and factored left contractions
   // through cp.async producer warps (default) or TMA (PLANC_GPU_TC_LOADS=tma)
   bool tc_cpa = true;
@@ -521,6 +525,17 @@ void ensure_errs(planc_gpu_ctx* c, int n) {
   }
 }
 
+// Whether the 3-way tensor-core tree's left contraction runs as the long-K
+// kernel against a Khatri-Rao image (tc_long_prep + tc_long): when the
+// factored form does not apply (I_0 % 64 != 0) and the context asks for it.
+// The image (L rows of hi|lo BF16 values) is written once per call and read
+// by every row group, where the producer-warp form regenerates each
+// Khatri-Rao tile in every CTA that uses it.
+bool left_via_long(const planc_gpu_ctx* c) {
+  return c->left_long && c->N == 3 && !c->bal4 && c->precision != PLANC_GPU_PREC_FP64 &&
+         c->tct.hi && !tc_left_factored(c->tct);
+}
+
 void ensure_buffers_impl(planc_gpu_ctx* c) {
   const int k = c->k;
   size_t need = 0;
@@ -538,6 +553,10 @@ void ensure_buffers_impl(planc_gpu_ctx* c) {
       need = std::max(need, (size_t)t2.nsplit * c->dims[1] * k);
     }
     need = std::max(need, tc_scratch_elems(c->tct, eff_sm(c), k));
+    if (left_via_long(c)) {
+      need = std::max(need, tc_long_scratch_elems(c->tct, true, k, eff_sm(c)));
+      c->tct.wimg_K = std::max(c->tct.wimg_K, c->L);
+    }
     if (c->bal4) {
       TtvRightPlan t3 = plan_ttv_right(c, c->dims[2], c->dims[3]);
       need = std::max(need, (size_t)t3.nsplit * c->dims[2] * k);
@@ -841,9 +860,15 @@ void partial_right(planc_gpu_ctx* c) {
 }
 
 // Left contraction M_{N-1} = X^T * KRP(F_0..F_s) (dimtrees.hpp:250-271).
+void long_contract(planc_gpu_ctx* c, bool left, const std::vector<int>& modes, double* out);
+
 void partial_left(planc_gpu_ctx* c, double* out) {
   std::vector<int> modes;
   for (int m = 0; m <= c->s; ++m) modes.push_back(m);
+  if (left_via_long(c)) {
+    long_contract(c, true, modes, out);
+    return;
+  }
   if (c->precision == PLANC_GPU_PREC_FP64) {
     WGen wg = make_wgen(c, modes);
     // reduction tiles aligned to runs of I_0 (the same tiles and splits as the
@@ -1490,6 +1515,13 @@ int planc_gpu_create(planc_gpu_ctx** out, int device, int precision, void* cuda_
     if (const char* e = getenv("PLANC_GPU_LEFT_CHUNKS")) {
       const int v = atoi(e);
       if (v >= 0 && v <= (1 << 20)) c->left_chunks = v;
+    }
+    // PLANC_GPU_LEFT_FORM=image|producers picks how a 3-way tensor-core left
+    // contraction without the factored form forms its Khatri-Rao rows, for
+    // contexts created while it is set
+    if (const char* e = getenv("PLANC_GPU_LEFT_FORM")) {
+      if (!strcmp(e, "producers")) c->left_long = false;
+      if (!strcmp(e, "image")) c->left_long = true;
     }
     // PLANC_GPU_LEFT_PARTS=n splits each run of the factored left
     // contraction into n work units (a divisor of I0 / 64) for contexts
@@ -2743,6 +2775,20 @@ void batch_capture_grouped(planc_gpu_batch* b, int algo, bool err) {
                            m->left_chunks);
         });
         red.push_back(grp_red(m->scratch, nsplit, m->R * m->k, m->M[2]));
+        continue;
+      }
+      if (left_via_long(m)) {
+        // the member's own Khatri-Rao image and long-K contraction (as
+        // long_contract), the split-K sum in the grouped reduction
+        launch(m, KC_PREP, [&] { tc_long_prep(m->tct, true, wg, m->k, m->stream); });
+        if (tc_long_scratch_elems(m->tct, true, m->k, eff_sm(m)) > m->scratch_elems)
+          fail(PLANC_GPU_ERR_STATE, "internal: split-K scratch larger than planned");
+        int nsplit = 1;
+        launch(m, KC_CONTRACT_LEFT, [&] {
+          nsplit = tc_long(m->tct, true, m->k, m->M[2], m->scratch, m->status_dev, eff_sm(m),
+                           m->stream);
+        });
+        if (nsplit > 1) red.push_back(grp_red(m->scratch, nsplit, m->R * m->k, m->M[2]));
         continue;
       }
       int mg = 0, ns = 0;

@@ -216,6 +216,9 @@ def test_tc_left_split_length_keeps_the_bound(gpu, oracle_lib, prec, chunks, mon
     # within the precision's bound, for the generic (I0 % 64 != 0) and the
     # factored (I0 % 64 == 0) left contraction
     monkeypatch.setenv("PLANC_GPU_LEFT_CHUNKS", str(chunks))
+    # the producer-warp form of the generic left contraction (the default for
+    # I0 % 64 != 0 is the long-K kernel over a Khatri-Rao image)
+    monkeypatch.setenv("PLANC_GPU_LEFT_FORM", "producers")
     for dims, k in (((40, 33, 96), 16), ((64, 20, 70), 32)):
         X, _ = cp_tensor(dims, 4, seed=31)
         F = init_factors(dims, k, seed=32)
@@ -264,3 +267,26 @@ def test_tc_tile_loads_agree(gpu, prec, monkeypatch):
         assert all(rel(a, b) < 1e-12 for a, b in zip(m1, m2)), (dims, [rel(a, b) for a, b in zip(m1, m2)])
         assert np.max(np.abs(np.asarray(e1) - np.asarray(e2))) < 1e-10, dims
         assert all(rel(a, b) < 1e-8 for a, b in zip(f1, f2)), dims
+
+
+@pytest.mark.parametrize("prec", ["bf16", "bf16x2"])
+@pytest.mark.parametrize("form", ["image", "producers"])
+def test_tc_generic_left_forms_keep_the_bound(gpu, oracle_lib, prec, form, monkeypatch):
+    # 3-way tensors with I0 % 64 != 0: the left contraction (mode 2 of the
+    # tree) against a Khatri-Rao image with the long-K kernel, or with
+    # Khatri-Rao producer warps; both within the precision's bound, for one
+    # and two 128-row tiles per CTA (R > 128 at rank <= 32) and rank 64
+    monkeypatch.setenv("PLANC_GPU_LEFT_FORM", form)
+    for dims, k in (((40, 33, 96), 16), ((37, 45, 300), 32), ((50, 21, 140), 64), ((13, 7, 20), 5)):
+        X, _ = cp_tensor(dims, 4, seed=35)
+        F = init_factors(dims, k, seed=36)
+        Fn = _normalized(F)
+        with gpu.Context(0, prec) as c:
+            c.set_tensor(X)
+            c.set_factors(F)
+            for n in range(3):
+                ref = oracle_lib.mttkrp_direct(X, Fn, n)
+                got = c.mttkrp(n, dimtree=True)
+                assert rel(got, ref) < BOUND[prec], (dims, n, rel(got, ref))
+            e = c.run("hals", 3)
+            assert np.all(np.isfinite(e))
