@@ -535,6 +535,10 @@ bool left_via_long(const planc_gpu_ctx* c) {
   return c->left_long && c->N == 3 && !c->bal4 && c->precision != PLANC_GPU_PREC_FP64 &&
          c->tct.hi && !tc_left_factored(c->tct);
 }
+// The same choice for a direct-MTTKRP view (any number of modes).
+bool direct_via_long(const planc_gpu_ctx* c, const TcTensor& t) {
+  return c->left_long && c->precision != PLANC_GPU_PREC_FP64 && t.hi && !tc_left_factored(t);
+}
 
 void ensure_buffers_impl(planc_gpu_ctx* c) {
   const int k = c->k;
@@ -741,6 +745,10 @@ void ensure_direct(planc_gpu_ctx* c) {
     }
     TcTensor& t = const_cast<TcTensor&>(direct_view(c, n));
     uint8_t* before[3] = {t.bimg, t.bimg0, t.wimg};
+    if (direct_via_long(c, t)) {
+      t.wimg_K = std::max(t.wimg_K, t.L);
+      need = std::max(need, tc_long_scratch_elems(t, true, c->k, eff_sm(c)));
+    }
     CK(tc_ensure(t, c->k));
     if (before[0] != t.bimg || before[1] != t.bimg0 || before[2] != t.wimg) grew = true;
     need = std::max(need, tc_scratch_elems(t, eff_sm(c), c->k));
@@ -810,13 +818,28 @@ void mttkrp_direct_tc(planc_gpu_ctx* c, int n, double* out) {
   }
   const TcTensor& t = direct_view(c, n);
   if (t.left_nf != wg.nf) fail(PLANC_GPU_ERR_STATE, "internal: direct view generator mismatch");
+  const int64_t nn = c->dims[n] * c->k;
+  if (direct_via_long(c, t)) {
+    // the Khatri-Rao image of the generator, then the long-K contraction
+    if ((t.L + TC_BK - 1) / TC_BK > (t.wimg_K + TC_BK - 1) / TC_BK || !t.wimg)
+      fail(PLANC_GPU_ERR_STATE, "internal: Khatri-Rao image smaller than planned");
+    if (tc_long_scratch_elems(t, true, c->k, eff_sm(c)) > c->scratch_elems)
+      fail(PLANC_GPU_ERR_STATE, "internal: split-K scratch larger than planned");
+    launch(c, KC_PREP, [&] { tc_long_prep(t, true, wg, c->k, c->stream); });
+    int nsplit = 1;
+    launch(c, KC_CONTRACT_LEFT, [&] {
+      nsplit = tc_long(t, true, c->k, out, c->scratch, c->status_dev, eff_sm(c), c->stream);
+    });
+    if (nsplit > 1)
+      launch(c, KC_REDUCE, [&] { reduce_splits(c->stream, c->scratch, nsplit, nn, nn, out); });
+    return;
+  }
   if (tc_scratch_elems(t, eff_sm(c), c->k) > c->scratch_elems)
     fail(PLANC_GPU_ERR_STATE, "internal: split-K scratch larger than planned");
   int nsplit = 0;
   launch(c, KC_CONTRACT_LEFT, [&] {
     nsplit = tc_left(t, wg, c->k, c->scratch, c->status_dev, eff_sm(c), c->stream, c->left_chunks);
   });
-  const int64_t nn = c->dims[n] * c->k;
   launch(c, KC_REDUCE, [&] { reduce_splits(c->stream, c->scratch, nsplit, nn, nn, out); });
 }
 

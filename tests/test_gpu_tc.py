@@ -273,9 +273,10 @@ def test_tc_tile_loads_agree(gpu, prec, monkeypatch):
 @pytest.mark.parametrize("form", ["image", "producers"])
 def test_tc_generic_left_forms_keep_the_bound(gpu, oracle_lib, prec, form, monkeypatch):
     # 3-way tensors with I0 % 64 != 0: the left contraction (mode 2 of the
-    # tree) against a Khatri-Rao image with the long-K kernel, or with
-    # Khatri-Rao producer warps; both within the precision's bound, for one
-    # and two 128-row tiles per CTA (R > 128 at rank <= 32) and rank 64
+    # tree, and the direct MTTKRP of modes whose view lacks the factored form)
+    # against a Khatri-Rao image with the long-K kernel, or with Khatri-Rao
+    # producer warps; both within the precision's bound, for one and two
+    # 128-row tiles per CTA (R > 128 at rank <= 32) and rank 64
     monkeypatch.setenv("PLANC_GPU_LEFT_FORM", form)
     for dims, k in (((40, 33, 96), 16), ((37, 45, 300), 32), ((50, 21, 140), 64), ((13, 7, 20), 5)):
         X, _ = cp_tensor(dims, 4, seed=35)
@@ -286,7 +287,8 @@ def test_tc_generic_left_forms_keep_the_bound(gpu, oracle_lib, prec, form, monke
             c.set_factors(F)
             for n in range(3):
                 ref = oracle_lib.mttkrp_direct(X, Fn, n)
-                got = c.mttkrp(n, dimtree=True)
-                assert rel(got, ref) < BOUND[prec], (dims, n, rel(got, ref))
+                for tree in (True, False):
+                    got = c.mttkrp(n, dimtree=tree)
+                    assert rel(got, ref) < BOUND[prec], (dims, n, tree, rel(got, ref))
             e = c.run("hals", 3)
             assert np.all(np.isfinite(e))
