@@ -706,7 +706,9 @@ void run_ttv_left(planc_gpu_ctx* c, const TT* T, int64_t A, int64_t B, const dou
                   double* out) {
   int k = c->k;
   const int64_t g2 = (B + TTVL_NB - 1) / TTVL_NB;
-  if (std::is_same<TT, float>::value && k % 4 == 0 && g2 >= c->sm_count && g2 <= 65535) {
+  // the float4 kernel when its CTAs fill the SMs this context may use (a
+  // batch member's share after the autotuner's parallelism fraction)
+  if (std::is_same<TT, float>::value && k % 4 == 0 && g2 >= eff_sm(c) && g2 <= 65535) {
     launch(c, KC_TTV, [&] {
       k_ttv_left_f4<<<(unsigned)g2, 256, 0, c->stream>>>((const float*)T, A, B, k, Fa, out);
     });
@@ -2763,7 +2765,7 @@ void batch_capture_grouped(planc_gpu_batch* b, int algo, bool err) {
         const int k = m->k;
         const int64_t A = m->dims[0], B = m->dims[1];
         const int64_t g2 = (B + TTVL_NB - 1) / TTVL_NB;
-        if (k % 4 == 0 && g2 >= m->sm_count && g2 <= 65535)
+        if (k % 4 == 0 && g2 >= eff_sm(m) && g2 <= 65535)
           f4.push_back(GrpTtvL{m->P32, A, B, k, m->F[0], m->M[1], (unsigned)g2});
         else
           plain.push_back(GrpTtvL{m->P32, A, B, k, m->F[0], m->M[1],
