@@ -162,7 +162,8 @@ def traffic_from_profiles(precision, dims, k, which):
 
 def left_splits(L, R, I0, k, sm_count, precision="bf16"):
     """Split-K count of the 3-way left contraction, as the library plans it
-    (tc_left_plan: 128-row tiles, two per CTA when R > 128 and k <= 32 except
+    (without the factored form, I_0 % 64 != 0: the long-K kernel's plan;
+    tc_left_plan: 128-row tiles, two per CTA when R > 128 and k <= 32 except
     for the factored contraction's cp.async instance (I_0 % 64 == 0, rank <= 32,
     BF16, an even number of 64-wide chunks per work unit), which takes one;
     the SMs shared among the row groups, at most one split per work unit:
@@ -174,6 +175,13 @@ def left_splits(L, R, I0, k, sm_count, precision="bf16"):
     kpad = 16 if k <= 16 else 32 if k <= 32 else 64
     cpa = (factored and kpad <= 32 and precision == "bf16" and (I0 // 64 // hp) % 2 == 0
            and os.environ.get("PLANC_GPU_TC_LOADS", "cpasync") != "tma")
+    if not factored and os.environ.get("PLANC_GPU_LEFT_FORM", "image") != "producers":
+        # the long-K kernel against a Khatri-Rao image (tc_long_plan): K groups
+        # of two 64-wide blocks, one split per group at most
+        mt = 2 if (R > 128 and kpad <= 32) else 1
+        groups = -(-R // (mt * 128))
+        ns = max(1, sm_count // groups)
+        return min(ns, -(-(-(-L // 64)) // 2))
     mt = 1 if cpa else (2 if (R > 128 and k <= 32) else 1)
     groups = -(-R // (mt * 128))
     ns = max(1, sm_count // groups)
