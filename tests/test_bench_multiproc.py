@@ -91,3 +91,34 @@ def test_reference_arm_other_ranks_exit_without_output():
     out = _bench(["--impl", "reference", "--dims", "12,10,8", "--rank", "3", "--steps", "1",
                   "--warmup", "0"], {"RANK": "1", "WORLD_SIZE": "2", "CUDA_VISIBLE_DEVICES": ""})
     assert out == []
+
+
+@pytest.mark.parametrize("dims,k,prec,env,expect", [
+    # factored left contraction, cp.async instance: one 128-row tile a CTA,
+    # 1024 / 128 = 8 row groups, 148 // 8 = 18 splits
+    ((1024, 1024, 1024), 32, "bf16", {}, 18),
+    # TMA instance (two tiles a CTA): 4 row groups, 37 splits
+    ((1024, 1024, 1024), 32, "bf16", {"PLANC_GPU_TC_LOADS": "tma"}, 37),
+    # bf16x2 has no cp.async instance of the factored left contraction
+    ((1024, 1024, 1024), 32, "bf16x2", {}, 37),
+    # I0 % 64 != 0: the long-K kernel over a Khatri-Rao image, 4 row groups
+    ((1000, 1000, 1000), 32, "bf16", {}, 37),
+    # ... or the producer-warp kernel
+    ((1000, 1000, 1000), 32, "bf16", {"PLANC_GPU_LEFT_FORM": "producers"}, 37),
+    # small K: at most one split per K group of two 64-wide blocks (L = 1320:
+    # 21 blocks, 11 groups)
+    ((40, 33, 96), 16, "bf16", {}, 11),
+])
+def test_bench_left_split_estimate(monkeypatch, dims, k, prec, env, expect):
+    # bench.py's algorithmic bytes of the left contraction count the split-K
+    # partials the library writes; its estimate follows the library's plans
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    import bench
+    for name in ("PLANC_GPU_TC_LOADS", "PLANC_GPU_LEFT_FORM", "PLANC_GPU_LEFT_PARTS"):
+        monkeypatch.delenv(name, raising=False)
+    for name, v in env.items():
+        monkeypatch.setenv(name, v)
+    L = dims[0] * dims[1]
+    assert bench.left_splits(L, dims[2], dims[0], k, 148, prec) == expect
